@@ -1,0 +1,205 @@
+"""ctypes binding of the elsa_b200 C ABI (include/elsa_b200.h).
+
+Loading fails loudly when libelsa_b200.so has not been built: there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libelsa_b200.so")
+POSE_FLOATS = 40
+
+SUCCESS = 0
+STATUS_NAMES = {
+    0: "ELSA_SUCCESS",
+    1: "ELSA_ERROR_INVALID_ARGUMENT",
+    2: "ELSA_ERROR_LOGIC",
+    3: "ELSA_ERROR_BAD_ALLOC",
+    4: "ELSA_ERROR_CUDA",
+    5: "ELSA_ERROR_NOT_SUPPORTED",
+}
+
+PROJECTOR_JOSEPH = 0
+
+# Every function the header declares: name -> (restype, argtypes)
+_vp = ctypes.c_void_p
+_i32 = ctypes.c_int32
+_i64 = ctypes.c_int64
+_f32 = ctypes.c_float
+_st = ctypes.c_int
+SIGNATURES = {
+    "elsa_last_error": (ctypes.c_char_p, []),
+    "elsa_abi_version": (_i32, []),
+    "elsa_pose_2d": (_st, [_f32, _f32, _f32, _vp, _vp, _vp, _vp, _f32, _vp, _vp]),
+    "elsa_pose_3d": (_st, [_f32, _f32, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _vp, _vp, _vp]),
+    "elsa_circle_trajectory": (_st, [_i32, _vp, _vp, _i64, _f32, _f32, _f32, _vp, _vp, _vp,
+                                     _vp]),
+    "elsa_projector_create": (_st, [_i32, _i32, _vp, _vp, _vp, _vp, _i32,
+                                    ctypes.POINTER(_vp)]),
+    "elsa_projector_destroy": (_st, [_vp]),
+    "elsa_projector_sizes": (_st, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+    "elsa_projector_info": (_st, [_vp, _i32, ctypes.POINTER(_i32)]),
+    "elsa_projector_apply": (_st, [_vp, _vp, _vp, _vp]),
+    "elsa_projector_apply_adjoint": (_st, [_vp, _vp, _vp, _vp]),
+    "elsa_projector_apply_host": (_st, [_vp, _vp, _vp]),
+    "elsa_projector_apply_adjoint_host": (_st, [_vp, _vp, _vp]),
+    "elsa_dot": (_st, [_vp, _vp, _i64, _vp, _vp]),
+    "elsa_squared_l2_norm": (_st, [_vp, _i64, _vp, _vp]),
+    "elsa_lincomb": (_st, [_f32, _vp, _f32, _vp, _vp, _i64, _vp]),
+    "elsa_cgne_solve": (_st, [_vp, _vp, _vp, _i32, _i32, _vp]),
+}
+
+
+class ElsaError(RuntimeError):
+    """A failed C ABI call; .status is the elsa_status code."""
+
+    def __init__(self, status, message):
+        super().__init__("%s: %s" % (STATUS_NAMES.get(status, status), message))
+        self.status = status
+
+
+class InvalidArgumentError(ElsaError, ValueError):
+    pass
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("elsa_b200 native library not built (%s); run "
+                              "`python -m elsa_b200.build`" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != SUCCESS:
+        msg = lib().elsa_last_error().decode()
+        if status == 1:
+            raise InvalidArgumentError(status, msg)
+        raise ElsaError(status, msg)
+
+
+def call(name, *args):
+    check(getattr(lib(), name)(*args))
+
+
+def np_ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def circle_trajectory(vol_dims, num_poses, arc_degrees, s2c, c2d, det_size=None,
+                      vol_spacing=None, det_spacing=None):
+    """Poses (P x 40 float32) and detector dims of a circular trajectory."""
+    dim = len(vol_dims)
+    vd = np.asarray(vol_dims, np.int64)
+    vs = np.ascontiguousarray(vol_spacing if vol_spacing is not None else np.ones(dim),
+                              np.float32)
+    poses = np.zeros((num_poses, POSE_FLOATS), np.float32)
+    det_dims = np.zeros(dim, np.int64)
+    ds = np.asarray(det_size, np.int64) if det_size is not None else None
+    dsp = np.ascontiguousarray(det_spacing, np.float32) if det_spacing is not None else None
+    call("elsa_circle_trajectory", dim, np_ptr(vd), np_ptr(vs), int(num_poses),
+         float(arc_degrees), float(s2c), float(c2d), np_ptr(ds) if ds is not None else None,
+         np_ptr(dsp) if dsp is not None else None, np_ptr(poses), np_ptr(det_dims))
+    return poses, det_dims
+
+
+def pose_2d(s2c, c2d, angle_rad, vol_spacing, vol_origin, sino_spacing, sino_origin,
+            pp_offset=0.0, cor_offset=(0.0, 0.0)):
+    out = np.zeros(POSE_FLOATS, np.float32)
+    arrs = [np.ascontiguousarray(a, np.float32) for a in
+            (vol_spacing, vol_origin, sino_spacing, sino_origin, cor_offset)]
+    call("elsa_pose_2d", float(s2c), float(c2d), float(angle_rad), np_ptr(arrs[0]),
+         np_ptr(arrs[1]), np_ptr(arrs[2]), np_ptr(arrs[3]), float(pp_offset), np_ptr(arrs[4]),
+         np_ptr(out))
+    return out
+
+
+def pose_3d(s2c, c2d, vol_spacing, vol_origin, sino_spacing, sino_origin, gamma, beta=0.0,
+            alpha=0.0, pp_offset=(0.0, 0.0), cor_offset=(0.0, 0.0, 0.0)):
+    out = np.zeros(POSE_FLOATS, np.float32)
+    arrs = [np.ascontiguousarray(a, np.float32) for a in
+            (vol_spacing, vol_origin, sino_spacing, sino_origin, pp_offset, cor_offset)]
+    call("elsa_pose_3d", float(s2c), float(c2d), np_ptr(arrs[0]), np_ptr(arrs[1]),
+         np_ptr(arrs[2]), np_ptr(arrs[3]), float(gamma), float(beta), float(alpha),
+         np_ptr(arrs[4]), np_ptr(arrs[5]), np_ptr(out))
+    return out
+
+
+class Projector:
+    """Owning handle of an elsa_projector (device-side operator)."""
+
+    def __init__(self, kind, vol_dims, det_dims, poses, params=None):
+        self.dim = len(vol_dims)
+        self.vol_dims = tuple(int(v) for v in vol_dims)
+        self.det_dims = tuple(int(v) for v in det_dims)
+        vd = np.asarray(vol_dims, np.int64)
+        dd = np.asarray(det_dims, np.int64)
+        ps = np.ascontiguousarray(poses, np.float32)
+        if ps.size != POSE_FLOATS * self.det_dims[-1]:
+            raise InvalidArgumentError(1, "pose array does not match the number of poses")
+        prm = np.ascontiguousarray(params if params is not None else [], np.float32)
+        h = ctypes.c_void_p()
+        call("elsa_projector_create", int(kind), self.dim, np_ptr(vd), np_ptr(dd), np_ptr(ps),
+             np_ptr(prm) if prm.size else None, int(prm.size), ctypes.byref(h))
+        self._h = h
+        d = ctypes.c_int64()
+        r = ctypes.c_int64()
+        call("elsa_projector_sizes", self._h, ctypes.byref(d), ctypes.byref(r))
+        self.domain_size = d.value
+        self.range_size = r.value
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self, key):
+        v = ctypes.c_int32()
+        call("elsa_projector_info", self._h, int(key), ctypes.byref(v))
+        return v.value
+
+    def apply_ptr(self, x_ptr, y_ptr, stream=None):
+        call("elsa_projector_apply", self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
+             ctypes.c_void_p(stream or 0))
+
+    def apply_adjoint_ptr(self, y_ptr, x_ptr, stream=None):
+        call("elsa_projector_apply_adjoint", self._h, ctypes.c_void_p(y_ptr),
+             ctypes.c_void_p(x_ptr), ctypes.c_void_p(stream or 0))
+
+    def apply_host(self, x):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1)
+        if x.size != self.domain_size:
+            raise InvalidArgumentError(1, "input size does not match the domain")
+        y = np.empty(self.range_size, np.float32)
+        call("elsa_projector_apply_host", self._h, np_ptr(x), np_ptr(y))
+        return y
+
+    def apply_adjoint_host(self, y):
+        y = np.ascontiguousarray(y, np.float32).reshape(-1)
+        if y.size != self.range_size:
+            raise InvalidArgumentError(1, "input size does not match the range")
+        x = np.empty(self.domain_size, np.float32)
+        call("elsa_projector_apply_adjoint_host", self._h, np_ptr(y), np_ptr(x))
+        return x
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().elsa_projector_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

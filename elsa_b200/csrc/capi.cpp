@@ -1,0 +1,280 @@
+// C ABI of elsa_b200 (include/elsa_b200.h): argument checks, exception -> status translation.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/elsa_b200.h"
+#include "geometry.hpp"
+#include "internal.cuh"
+#include "projector.hpp"
+#include "solvers.hpp"
+
+struct elsa_projector {
+    std::unique_ptr<elsa_b200::Projector> impl;
+    // lazily allocated staging buffers of the host-buffer entry points
+    std::unique_ptr<elsa_b200::DeviceBuffer> hostIn, hostOut;
+};
+
+namespace
+{
+    thread_local std::string gLastError;
+
+    template <class Fn>
+    elsa_status guarded(Fn&& fn)
+    {
+        try {
+            fn();
+            gLastError.clear();
+            return ELSA_SUCCESS;
+        } catch (const elsa_b200::Error& e) {
+            gLastError = e.what();
+            return e.status;
+        } catch (const std::bad_alloc& e) {
+            gLastError = e.what();
+            return ELSA_ERROR_BAD_ALLOC;
+        } catch (const std::exception& e) {
+            gLastError = e.what();
+            return ELSA_ERROR_LOGIC;
+        } catch (...) {
+            gLastError = "unknown error";
+            return ELSA_ERROR_LOGIC;
+        }
+    }
+
+    void require(bool cond, const char* msg)
+    {
+        if (!cond)
+            throw elsa_b200::Error(ELSA_ERROR_INVALID_ARGUMENT, msg);
+    }
+
+    cudaStream_t asStream(void* s)
+    {
+        return static_cast<cudaStream_t>(s);
+    }
+
+    void onDevice(const elsa_projector* p)
+    {
+        int cur = 0;
+        ELSA_CUDA(cudaGetDevice(&cur));
+        if (cur != p->impl->device())
+            ELSA_CUDA(cudaSetDevice(p->impl->device()));
+    }
+} // namespace
+
+extern "C" {
+
+const char* elsa_last_error(void)
+{
+    return gLastError.c_str();
+}
+
+int32_t elsa_abi_version(void)
+{
+    return 1;
+}
+
+elsa_status elsa_pose_2d(float s2c, float c2d, float angle, const float* volSpacing,
+                         const float* volOrigin, const float* sinoSpacing, const float* sinoOrigin,
+                         float ppOffset, const float* corOffset, float* out)
+{
+    return guarded([&] {
+        require(volSpacing && volOrigin && sinoSpacing && sinoOrigin && corOffset && out,
+                "elsa_pose_2d: null argument");
+        const auto rec = elsa_b200::makePose2d(s2c, c2d, angle, volSpacing, volOrigin,
+                                               sinoSpacing, sinoOrigin, ppOffset, corOffset);
+        std::memcpy(out, rec.v, sizeof(rec.v));
+    });
+}
+
+elsa_status elsa_pose_3d(float s2c, float c2d, const float* volSpacing, const float* volOrigin,
+                         const float* sinoSpacing, const float* sinoOrigin, float gamma,
+                         float beta, float alpha, const float* ppOffset, const float* corOffset,
+                         float* out)
+{
+    return guarded([&] {
+        require(volSpacing && volOrigin && sinoSpacing && sinoOrigin && ppOffset && corOffset &&
+                    out,
+                "elsa_pose_3d: null argument");
+        const auto rec = elsa_b200::makePose3d(s2c, c2d, volSpacing, volOrigin, sinoSpacing,
+                                               sinoOrigin, gamma, beta, alpha, ppOffset,
+                                               corOffset);
+        std::memcpy(out, rec.v, sizeof(rec.v));
+    });
+}
+
+elsa_status elsa_circle_trajectory(int32_t dim, const int64_t* volDims, const float* volSpacing,
+                                   int64_t numPoses, float arc, float s2c, float c2d,
+                                   const int64_t* detSize, const float* detSpacing,
+                                   float* outPoses, int64_t* outDetDims)
+{
+    return guarded([&] {
+        require(dim == 2 || dim == 3, "CircleTrajectoryGenerator: can only handle 2d/3d");
+        require(volDims && volSpacing && outPoses && outDetDims,
+                "elsa_circle_trajectory: null argument");
+        require(numPoses > 0, "elsa_circle_trajectory: need at least one pose");
+        const auto poses = elsa_b200::circleTrajectory(dim, volDims, volSpacing, numPoses, arc,
+                                                       s2c, c2d, detSize, detSpacing, outDetDims);
+        std::memcpy(outPoses, poses.data(), sizeof(elsa_b200::PoseRecord) * poses.size());
+    });
+}
+
+elsa_status elsa_projector_create(int32_t kind, int32_t dim, const int64_t* volDims,
+                                  const int64_t* detDims, const float* poses, const float* params,
+                                  int32_t numParams, elsa_projector** out)
+{
+    (void)params;
+    (void)numParams;
+    return guarded([&] {
+        require(out != nullptr, "elsa_projector_create: null output handle");
+        *out = nullptr;
+        require(dim == 2 || dim == 3, "JosephsMethod: only supporting 2d/3d operations");
+        require(volDims && detDims && poses, "elsa_projector_create: null argument");
+        for (int i = 0; i < dim; ++i) {
+            require(volDims[i] > 0 && volDims[i] < (1 << 20),
+                    "elsa_projector_create: invalid volume size");
+            require(detDims[i] > 0 && detDims[i] < (1 << 24),
+                    "elsa_projector_create: invalid detector size");
+        }
+        require(detDims[dim - 1] > 0, "JosephsMethod: geometry list was empty");
+        elsa_b200::VolumeShape vol{dim, {static_cast<int>(volDims[0]),
+                                         static_cast<int>(volDims[1]),
+                                         dim == 3 ? static_cast<int>(volDims[2]) : 1}};
+        elsa_b200::DetectorShape det{static_cast<int>(detDims[0]),
+                                     dim == 3 ? static_cast<int>(detDims[1]) : 1,
+                                     static_cast<int>(detDims[dim - 1])};
+        std::vector<elsa_b200::PoseRecord> pv(static_cast<size_t>(det.np));
+        std::memcpy(pv.data(), poses, sizeof(elsa_b200::PoseRecord) * pv.size());
+        auto handle = std::make_unique<elsa_projector>();
+        switch (kind) {
+        case ELSA_PROJECTOR_JOSEPH:
+            handle->impl = elsa_b200::makeJosephProjector(vol, det, pv);
+            break;
+        default:
+            throw elsa_b200::Error(ELSA_ERROR_NOT_SUPPORTED, "unknown projector kind");
+        }
+        *out = handle.release();
+    });
+}
+
+elsa_status elsa_projector_destroy(elsa_projector* p)
+{
+    return guarded([&] { delete p; });
+}
+
+elsa_status elsa_projector_sizes(const elsa_projector* p, int64_t* domain, int64_t* range)
+{
+    return guarded([&] {
+        require(p && domain && range, "elsa_projector_sizes: null argument");
+        *domain = p->impl->domainSize();
+        *range = p->impl->rangeSize();
+    });
+}
+
+elsa_status elsa_projector_info(const elsa_projector* p, int32_t key, int32_t* value)
+{
+    return guarded([&] {
+        require(p && value, "elsa_projector_info: null argument");
+        *value = p->impl->info(key);
+    });
+}
+
+elsa_status elsa_projector_apply(elsa_projector* p, const float* x, float* y, void* stream)
+{
+    return guarded([&] {
+        require(p && x && y, "elsa_projector_apply: null argument");
+        onDevice(p);
+        p->impl->forward(x, y, asStream(stream));
+    });
+}
+
+elsa_status elsa_projector_apply_adjoint(elsa_projector* p, const float* y, float* x,
+                                         void* stream)
+{
+    return guarded([&] {
+        require(p && x && y, "elsa_projector_apply_adjoint: null argument");
+        onDevice(p);
+        p->impl->adjoint(y, x, asStream(stream));
+    });
+}
+
+static void hostApply(elsa_projector* p, const float* in, float* out, bool adjoint)
+{
+    onDevice(p);
+    const int64_t nin = adjoint ? p->impl->rangeSize() : p->impl->domainSize();
+    const int64_t nout = adjoint ? p->impl->domainSize() : p->impl->rangeSize();
+    const size_t need = sizeof(float) * static_cast<size_t>(std::max(nin, nout));
+    if (!p->hostIn || p->hostIn->bytes() < need) {
+        p->hostIn = std::make_unique<elsa_b200::DeviceBuffer>(need);
+        p->hostOut = std::make_unique<elsa_b200::DeviceBuffer>(need);
+    }
+    float* din = p->hostIn->as<float>();
+    float* dout = p->hostOut->as<float>();
+    ELSA_CUDA(cudaMemcpy(din, in, sizeof(float) * nin, cudaMemcpyHostToDevice));
+    if (adjoint)
+        p->impl->adjoint(din, dout, nullptr);
+    else
+        p->impl->forward(din, dout, nullptr);
+    ELSA_CUDA(cudaMemcpy(out, dout, sizeof(float) * nout, cudaMemcpyDeviceToHost));
+}
+
+elsa_status elsa_projector_apply_host(elsa_projector* p, const float* x, float* y)
+{
+    return guarded([&] {
+        require(p && x && y, "elsa_projector_apply_host: null argument");
+        hostApply(p, x, y, false);
+    });
+}
+
+elsa_status elsa_projector_apply_adjoint_host(elsa_projector* p, const float* y, float* x)
+{
+    return guarded([&] {
+        require(p && x && y, "elsa_projector_apply_adjoint_host: null argument");
+        hostApply(p, y, x, true);
+    });
+}
+
+elsa_status elsa_dot(const float* x, const float* y, int64_t n, double* result, void* stream)
+{
+    return guarded([&] {
+        require(x && y && result && n >= 0, "elsa_dot: invalid argument");
+        elsa_b200::DeviceBuffer partials(sizeof(double) * elsa_b200::kReduceBlocks);
+        elsa_b200::launchDot(x, y, n, partials.as<double>(), result, asStream(stream));
+        ELSA_CUDA(cudaStreamSynchronize(asStream(stream)));
+    });
+}
+
+elsa_status elsa_squared_l2_norm(const float* x, int64_t n, double* result, void* stream)
+{
+    return guarded([&] {
+        require(x && result && n >= 0, "elsa_squared_l2_norm: invalid argument");
+        elsa_b200::DeviceBuffer partials(sizeof(double) * elsa_b200::kReduceBlocks);
+        elsa_b200::launchSquaredNorm(x, n, partials.as<double>(), result, asStream(stream));
+        ELSA_CUDA(cudaStreamSynchronize(asStream(stream)));
+    });
+}
+
+elsa_status elsa_lincomb(float a, const float* x, float b, const float* y, float* out, int64_t n,
+                         void* stream)
+{
+    return guarded([&] {
+        require(x && y && out && n >= 0, "elsa_lincomb: invalid argument");
+        elsa_b200::launchLincomb(a, x, b, y, out, n, asStream(stream));
+    });
+}
+
+elsa_status elsa_cgne_solve(elsa_projector* p, const float* b, float* x, int32_t iterations,
+                            int32_t useX0, void* stream)
+{
+    return guarded([&] {
+        require(p && b && x && iterations >= 0, "elsa_cgne_solve: invalid argument");
+        onDevice(p);
+        elsa_b200::SolverWorkspace ws(p->impl->domainSize(), p->impl->rangeSize());
+        elsa_b200::cgneSolve(*p->impl, b, x, iterations, useX0 != 0, ws, asStream(stream));
+        ELSA_CUDA(cudaStreamSynchronize(asStream(stream)));
+    });
+}
+
+} // extern "C"

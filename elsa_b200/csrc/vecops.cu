@@ -1,0 +1,242 @@
+// Fused vector operations, see vecops.cuh.
+//
+// Reference semantics: storage/reductions/DotProduct.h:24-47 (dot), storage/reductions/L2.h:15-49
+// (squaredL2Norm), storage/transforms/Lincomb.h:28-33 (lincomb). The reference reduces in the data
+// type (float); these kernels keep float data and accumulate in float64.
+#include "internal.cuh"
+#include "vecops.cuh"
+
+namespace elsa_b200
+{
+    namespace
+    {
+        __device__ __forceinline__ double blockSum(double v)
+        {
+            __shared__ double warpSums[kReduceThreads / 32];
+            for (int o = 16; o > 0; o >>= 1)
+                v += __shfl_down_sync(0xffffffffu, v, o);
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            if (lane == 0)
+                warpSums[warp] = v;
+            __syncthreads();
+            double s = 0.0;
+            if (warp == 0) {
+                s = lane < kReduceThreads / 32 ? warpSums[lane] : 0.0;
+                for (int o = 16; o > 0; o >>= 1)
+                    s += __shfl_down_sync(0xffffffffu, s, o);
+            }
+            return s; // valid in thread 0
+        }
+
+        // Each thread handles float4 chunks i = tid, tid + T, ... (T = total threads), plus a
+        // scalar tail; fixed assignment -> fixed summation order.
+        template <bool kSquare>
+        __global__ void __launch_bounds__(kReduceThreads)
+            partialDotKernel(const float* __restrict__ x, const float* __restrict__ y, int64_t n,
+                             double* __restrict__ partials)
+        {
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            double acc = 0.0;
+            const bool vec = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) &
+                              15) == 0;
+            int64_t done = 0;
+            if (vec) {
+                const int64_t n4 = n / 4;
+                const float4* x4 = reinterpret_cast<const float4*>(x);
+                const float4* y4 = reinterpret_cast<const float4*>(y);
+                for (int64_t i = tid; i < n4; i += T) {
+                    const float4 a = __ldg(x4 + i);
+                    const float4 b = kSquare ? a : __ldg(y4 + i);
+                    acc += static_cast<double>(a.x) * b.x + static_cast<double>(a.y) * b.y +
+                           static_cast<double>(a.z) * b.z + static_cast<double>(a.w) * b.w;
+                }
+                done = n4 * 4;
+            }
+            for (int64_t i = done + tid; i < n; i += T) {
+                const float a = __ldg(x + i);
+                const float b = kSquare ? a : __ldg(y + i);
+                acc += static_cast<double>(a) * b;
+            }
+            const double s = blockSum(acc);
+            if (threadIdx.x == 0)
+                partials[blockIdx.x] = s;
+        }
+
+        __device__ __forceinline__ double sumPartials(const double* __restrict__ partials)
+        {
+            double v = 0.0;
+            for (int i = threadIdx.x; i < kReduceBlocks; i += blockDim.x)
+                v += partials[i];
+            return blockSum(v);
+        }
+
+        __global__ void __launch_bounds__(kReduceThreads)
+            finishSumKernel(const double* __restrict__ partials, double* __restrict__ out)
+        {
+            const double s = sumPartials(partials);
+            if (threadIdx.x == 0)
+                *out = s;
+        }
+
+        __global__ void lincombKernel(float a, const float* x, float b, const float* y, float* out,
+                                      int64_t n)
+        {
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < n; i += T)
+                out[i] = a * x[i] + b * y[i];
+        }
+
+        __global__ void lincombDevKernel(const double* sa, float ca, const float* x,
+                                         const double* sb, float cb, const float* y, float* out,
+                                         int64_t n)
+        {
+            const float a = sa ? static_cast<float>(*sa) : ca;
+            const float b = sb ? static_cast<float>(*sb) : cb;
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < n; i += T)
+                out[i] = a * x[i] + b * y[i];
+        }
+
+        __global__ void fillKernel(float* x, float v, int64_t n)
+        {
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < n; i += T)
+                x[i] = v;
+        }
+
+        __global__ void scaleKernel(float* x, float v, int64_t n)
+        {
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < n; i += T)
+                x[i] *= v;
+        }
+
+        __global__ void __launch_bounds__(kReduceThreads)
+            cgStepKernel(float* __restrict__ x, float* __restrict__ r, const float* __restrict__ c,
+                         const float* __restrict__ q, int64_t n, const SolverScalars* S,
+                         double* __restrict__ partials)
+        {
+            const float alpha = static_cast<float>(S->kold / S->den);
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            double acc = 0.0;
+            for (int64_t i = tid; i < n; i += T) {
+                x[i] = x[i] + alpha * c[i];
+                const float ri = r[i] - alpha * q[i];
+                r[i] = ri;
+                acc += static_cast<double>(ri) * ri;
+            }
+            const double s = blockSum(acc);
+            if (threadIdx.x == 0)
+                partials[blockIdx.x] = s;
+        }
+
+        __global__ void __launch_bounds__(kReduceThreads)
+            cgFinishNormKernel(const double* __restrict__ partials, SolverScalars* S)
+        {
+            const double s = sumPartials(partials);
+            if (threadIdx.x == 0) {
+                S->k = s;
+                S->beta = s / S->kold;
+                S->kold = s;
+            }
+        }
+
+        __global__ void __launch_bounds__(kReduceThreads)
+            finishDenKernel(const double* __restrict__ partials, SolverScalars* S)
+        {
+            const double s = sumPartials(partials);
+            if (threadIdx.x == 0)
+                S->den = s;
+        }
+
+        __global__ void cgDirectionKernel(const float* __restrict__ r, float* __restrict__ c,
+                                          int64_t n, const SolverScalars* S)
+        {
+            const float beta = static_cast<float>(S->beta);
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < n; i += T)
+                c[i] = r[i] + beta * c[i];
+        }
+
+        unsigned gridFor(int64_t n)
+        {
+            const int64_t b = (n + 255) / 256;
+            return static_cast<unsigned>(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
+        }
+    } // namespace
+
+    void launchDot(const float* x, const float* y, int64_t n, double* partials, double* result,
+                   cudaStream_t s)
+    {
+        partialDotKernel<false><<<kReduceBlocks, kReduceThreads, 0, s>>>(x, y, n, partials);
+        finishSumKernel<<<1, kReduceThreads, 0, s>>>(partials, result);
+        ELSA_LAUNCH_CHECK("dot");
+    }
+
+    void launchSquaredNorm(const float* x, int64_t n, double* partials, double* result,
+                           cudaStream_t s)
+    {
+        partialDotKernel<true><<<kReduceBlocks, kReduceThreads, 0, s>>>(x, x, n, partials);
+        finishSumKernel<<<1, kReduceThreads, 0, s>>>(partials, result);
+        ELSA_LAUNCH_CHECK("squaredL2Norm");
+    }
+
+    void launchLincomb(float a, const float* x, float b, const float* y, float* out, int64_t n,
+                       cudaStream_t s)
+    {
+        lincombKernel<<<gridFor(n), 256, 0, s>>>(a, x, b, y, out, n);
+        ELSA_LAUNCH_CHECK("lincomb");
+    }
+
+    void launchLincombDev(const double* sa, float ca, const float* x, const double* sb, float cb,
+                          const float* y, float* out, int64_t n, cudaStream_t s)
+    {
+        lincombDevKernel<<<gridFor(n), 256, 0, s>>>(sa, ca, x, sb, cb, y, out, n);
+        ELSA_LAUNCH_CHECK("lincombDev");
+    }
+
+    void launchFill(float* x, float value, int64_t n, cudaStream_t s)
+    {
+        fillKernel<<<gridFor(n), 256, 0, s>>>(x, value, n);
+        ELSA_LAUNCH_CHECK("fill");
+    }
+
+    void launchScale(float* x, float value, int64_t n, cudaStream_t s)
+    {
+        scaleKernel<<<gridFor(n), 256, 0, s>>>(x, value, n);
+        ELSA_LAUNCH_CHECK("scale");
+    }
+
+    void launchCgStep(float* x, float* r, const float* c, const float* q, int64_t n,
+                      SolverScalars* S, double* partials, cudaStream_t s)
+    {
+        cgStepKernel<<<kReduceBlocks, kReduceThreads, 0, s>>>(x, r, c, q, n, S, partials);
+        ELSA_LAUNCH_CHECK("cgStep");
+    }
+
+    void launchCgFinishNorm(const double* partials, SolverScalars* S, cudaStream_t s)
+    {
+        cgFinishNormKernel<<<1, kReduceThreads, 0, s>>>(partials, S);
+        ELSA_LAUNCH_CHECK("cgFinishNorm");
+    }
+
+    void launchFinishDen(const double* partials, SolverScalars* S, cudaStream_t s)
+    {
+        finishDenKernel<<<1, kReduceThreads, 0, s>>>(partials, S);
+        ELSA_LAUNCH_CHECK("finishDen");
+    }
+
+    void launchCgDirection(const float* r, float* c, int64_t n, const SolverScalars* S,
+                           cudaStream_t s)
+    {
+        cgDirectionKernel<<<gridFor(n), 256, 0, s>>>(r, c, n, S);
+        ELSA_LAUNCH_CHECK("cgDirection");
+    }
+} // namespace elsa_b200

@@ -1,0 +1,161 @@
+/*
+ * elsa_b200: C ABI of the B200-native X-ray projector + iterative-solver hot path.
+ *
+ * Plain pointers and sizes only. Device pointers are CUDA device memory of the current device;
+ * `stream` is a cudaStream_t (NULL = legacy default stream). Every call returns an elsa_status;
+ * on failure elsa_last_error() gives a message (thread-local). No C++ exception crosses this
+ * boundary.
+ *
+ * Data layout (elsa's, core/Descriptors/DataDescriptor.cpp:86-118):
+ *   volume   float[nx*ny(*nz)], x fastest
+ *   sinogram float[nu(*nv)*num_poses], u fastest, pose last
+ *     (core/Descriptors/DetectorDescriptor.cpp:20-52)
+ *   pose     40 floats: P (dim x dim+1, row-major) at 0, Pinv (dim+1 x dim) at 12,
+ *            camera centre C (dim) at 24, extrinsic ext (dim x dim+1) at 27,
+ *            source-detector distance at 39; all in voxel-index units
+ *            (core/Geometry.cpp:225-270).
+ */
+#ifndef ELSA_B200_H
+#define ELSA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ELSA_POSE_FLOATS 40
+
+typedef enum elsa_status {
+    ELSA_SUCCESS = 0,
+    /* dimension mismatch, empty geometry, unsupported dim (elsa: InvalidArgumentError) */
+    ELSA_ERROR_INVALID_ARGUMENT = 1,
+    /* elsa: LogicError */
+    ELSA_ERROR_LOGIC = 2,
+    /* device allocation failed (elsa: std::bad_alloc) */
+    ELSA_ERROR_BAD_ALLOC = 3,
+    /* CUDA runtime error */
+    ELSA_ERROR_CUDA = 4,
+    /* geometry or option this build does not handle */
+    ELSA_ERROR_NOT_SUPPORTED = 5
+} elsa_status;
+
+typedef enum elsa_projector_kind {
+    /* JosephsMethod / JosephsMethodCUDA (matched adjoint) */
+    ELSA_PROJECTOR_JOSEPH = 0
+} elsa_projector_kind;
+
+typedef struct elsa_projector elsa_projector;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* elsa_last_error(void);
+
+/* ABI version of this library. */
+int32_t elsa_abi_version(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Geometry
+ * ------------------------------------------------------------------------------------------- */
+
+/* One 2D pose. Replaces Geometry(SourceToCenterOfRotation, CenterOfRotationToDetector, Radian,
+ * VolumeData2D, SinogramData2D, PrincipalPointOffset, RotationOffset2D),
+ * core/Geometry.cpp:12-51. vol_spacing/vol_origin/cor_offset: 2 floats; sino_spacing/
+ * sino_origin: 2 floats (only [0] is used). */
+elsa_status elsa_pose_2d(float source_to_center, float center_to_detector, float angle_rad,
+                         const float* vol_spacing, const float* vol_origin,
+                         const float* sino_spacing, const float* sino_origin,
+                         float principal_point_offset, const float* cor_offset, float* out_pose);
+
+/* One 3D pose (YZY Euler angles gamma, beta, alpha). Replaces Geometry(..., VolumeData3D,
+ * SinogramData3D, RotationAngles3D, PrincipalPointOffset2D, RotationOffset3D),
+ * core/Geometry.cpp:53-109. */
+elsa_status elsa_pose_3d(float source_to_center, float center_to_detector,
+                         const float* vol_spacing, const float* vol_origin,
+                         const float* sino_spacing, const float* sino_origin, float gamma,
+                         float beta, float alpha, const float* principal_point_offset,
+                         const float* cor_offset, float* out_pose);
+
+/* Circular trajectory. Replaces CircleTrajectoryGenerator::createTrajectory,
+ * generators/CircleTrajectoryGenerator.cpp:9-24 (with BaseCircleTrajectoryGenerator.cpp:12-74,
+ * TrajectoryGenerator.cpp:9-47). det_size (dim-1) and det_spacing (dim-1) may be NULL for
+ * elsa's defaults. out_poses: num_poses*ELSA_POSE_FLOATS floats; out_det_dims: dim entries. */
+elsa_status elsa_circle_trajectory(int32_t dim, const int64_t* vol_dims, const float* vol_spacing,
+                                   int64_t num_poses, float arc_degrees, float source_to_center,
+                                   float center_to_detector, const int64_t* det_size,
+                                   const float* det_spacing, float* out_poses,
+                                   int64_t* out_det_dims);
+
+/* ---------------------------------------------------------------------------------------------
+ * Projectors (LinearOperator<float> on device buffers)
+ * ------------------------------------------------------------------------------------------- */
+
+/* Create a projector on the current device. vol_dims: dim entries; det_dims: dim entries
+ * (nu[, nv], num_poses); poses: host, num_poses*ELSA_POSE_FLOATS floats; params: kind-specific
+ * (unused for Joseph, may be NULL). Replaces the constructors JosephsMethodCUDA(VolumeDescriptor,
+ * DetectorDescriptor), projectors_cuda/JosephsMethodCUDA.cpp:9-92, and
+ * JosephsMethod(VolumeDescriptor, DetectorDescriptor), projectors/JosephsMethod.cpp:11-28. */
+elsa_status elsa_projector_create(int32_t kind, int32_t dim, const int64_t* vol_dims,
+                                  const int64_t* det_dims, const float* poses,
+                                  const float* params, int32_t num_params,
+                                  elsa_projector** out);
+
+/* Replaces the operator's destructor (JosephsMethodCUDA.cpp:94-107). */
+elsa_status elsa_projector_destroy(elsa_projector* projector);
+
+/* Domain (volume) and range (sinogram) coefficient counts
+ * (LinearOperator::getDomainDescriptor/getRangeDescriptor, core/LinearOperator.h:60-70). */
+elsa_status elsa_projector_sizes(const elsa_projector* projector, int64_t* domain_size,
+                                 int64_t* range_size);
+
+/* Diagnostics: key 0 = conflict-free ray class spacing of the adjoint, 1 = adjoint bricks. */
+elsa_status elsa_projector_info(const elsa_projector* projector, int32_t key, int32_t* value);
+
+/* y = A x on device buffers. Replaces LinearOperator::apply(x, Ax), core/LinearOperator.cpp:94-98
+ * -> XrayProjector::applyImpl -> JosephsMethodCUDA::forward, JosephsMethodCUDA.cpp:132-214. */
+elsa_status elsa_projector_apply(elsa_projector* projector, const float* x, float* y,
+                                 void* stream);
+
+/* x = A^T y on device buffers (matched, atomic-free, deterministic). Replaces
+ * LinearOperator::applyAdjoint(y, Aty), core/LinearOperator.cpp:182-186 ->
+ * JosephsMethodCUDA::backward, JosephsMethodCUDA.cpp:216-389. */
+elsa_status elsa_projector_apply_adjoint(elsa_projector* projector, const float* y, float* x,
+                                         void* stream);
+
+/* Host-buffer variants, synchronous: copy the input to the device, run, copy the output back
+ * (the call pattern of the reference's CUDA projectors, which copy in and out on every apply,
+ * JosephsMethodCUDA.cpp:132-214). */
+elsa_status elsa_projector_apply_host(elsa_projector* projector, const float* x, float* y);
+elsa_status elsa_projector_apply_adjoint_host(elsa_projector* projector, const float* y,
+                                              float* x);
+
+/* ---------------------------------------------------------------------------------------------
+ * Vector operations on device float buffers; scalar results are float64 in device memory
+ * ------------------------------------------------------------------------------------------- */
+
+/* *result = <x, y>. Replaces DataContainer::dot, core/DataContainer.cpp:403-417
+ * (storage/reductions/DotProduct.h:24-47). */
+elsa_status elsa_dot(const float* x, const float* y, int64_t n, double* result, void* stream);
+
+/* *result = |x|_2^2. Replaces DataContainer::squaredL2Norm (storage/reductions/L2.h:15-49). */
+elsa_status elsa_squared_l2_norm(const float* x, int64_t n, double* result, void* stream);
+
+/* out = a*x + b*y. Replaces lincomb(a, x, b, y, out), core/DataContainer.cpp:1075-1108
+ * (storage/transforms/Lincomb.h:28-33). */
+elsa_status elsa_lincomb(float a, const float* x, float b, const float* y, float* out, int64_t n,
+                         void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Solvers (device-resident iterations, float64 inner products)
+ * ------------------------------------------------------------------------------------------- */
+
+/* CG on the normal equations A^T A x = A^T b. x: device volume buffer, used as the start value
+ * when use_x0 != 0 and overwritten with the solution. Replaces CGNE<float>(A, b).solve(
+ * iterations, x0), solvers/CGNE.cpp:20-78. */
+elsa_status elsa_cgne_solve(elsa_projector* projector, const float* b, float* x,
+                            int32_t iterations, int32_t use_x0, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ELSA_B200_H */

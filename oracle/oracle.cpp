@@ -1,0 +1,981 @@
+// Oracle: a CPU restatement of elsa's reference algorithms for the projector + solver hot path.
+//
+// TEST INFRASTRUCTURE ONLY. Nothing in the product (the elsa_b200 package, its CUDA kernels or
+// its C ABI) may include, link or call this file. Tests, __graft_entry__.smoke() and the CPU
+// baseline leg of bench.py use it as the checker.
+//
+// Every function cites the reference file:line it follows (paths relative to the elsa source
+// tree). Eigen 3.4.0, which the reference uses for all small vector/matrix math, is not available
+// here, so its evaluation order is restated: small products are coefficient-wise sequential dot
+// products with separate multiply and add (no FMA), reductions of <4 elements are sequential.
+// Built with -ffp-contract=off so the compiler does not fuse what the reference keeps separate.
+//
+// Parity is pinned against the reference's own known-answer tests (projectors/tests/*.cpp,
+// core/tests/test_Geometry.cpp) re-expressed in tests/test_oracle_kat.py.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#include <omp.h>
+
+namespace orc
+{
+    using real_t = float;
+    using index_t = int64_t;
+
+    // pi as real_t, core/elsaDefines.h:61-66
+    constexpr float pi_f() { return static_cast<float>(3.14159265358979323846); }
+
+    // ------------------------------------------------------------------------------------------
+    // Small dense matrices, row-major, with Eigen's coefficient-based product order.
+    // ------------------------------------------------------------------------------------------
+    struct Mat {
+        int r = 0, c = 0;
+        float a[16] = {0};
+        float& operator()(int i, int j) { return a[i * c + j]; }
+        float operator()(int i, int j) const { return a[i * c + j]; }
+    };
+
+    static Mat zeros(int r, int c)
+    {
+        Mat m;
+        m.r = r;
+        m.c = c;
+        return m;
+    }
+
+    static Mat identity(int r, int c)
+    {
+        Mat m = zeros(r, c);
+        for (int i = 0; i < std::min(r, c); ++i)
+            m(i, i) = 1.0f;
+        return m;
+    }
+
+    // Coefficient-based lazy product (Eigen 3.4 for rows+cols+depth < 20): every coefficient is
+    // the sequential sum of lhs(i,k)*rhs(k,j), k = 0..depth-1.
+    static Mat mul(const Mat& A, const Mat& B)
+    {
+        Mat C = zeros(A.r, B.c);
+        for (int i = 0; i < A.r; ++i)
+            for (int j = 0; j < B.c; ++j) {
+                float s = A(i, 0) * B(0, j);
+                for (int k = 1; k < A.c; ++k)
+                    s = s + A(i, k) * B(k, j);
+                C(i, j) = s;
+            }
+        return C;
+    }
+
+    // Matrix-vector product (Eigen GEMV for tiny sizes): per row ((0 + a0*x0) + a1*x1) + ...
+    static void matvec(const Mat& A, const float* x, float* y)
+    {
+        for (int i = 0; i < A.r; ++i) {
+            float s = 0.0f;
+            for (int k = 0; k < A.c; ++k)
+                s = s + A(i, k) * x[k];
+            y[i] = s;
+        }
+    }
+
+    static float seqSqNorm(const float* v, int n)
+    {
+        float s = v[0] * v[0];
+        for (int i = 1; i < n; ++i)
+            s = s + v[i] * v[i];
+        return s;
+    }
+
+    // ------------------------------------------------------------------------------------------
+    // Column-pivoting Householder QR solve in float, restating Eigen 3.4's ColPivHouseholderQR
+    // (computeInPlace + _solve_impl), used for the camera centre at core/Geometry.cpp:244-246.
+    // ------------------------------------------------------------------------------------------
+    static void colPivQrSolve(const Mat& Ain, const float* b, float* x)
+    {
+        const int n = Ain.r; // square
+        Mat qr = Ain;
+        float hCoeffs[4] = {0};
+        int transp[4] = {0};
+        float normsUpd[4], normsDir[4];
+        for (int k = 0; k < n; ++k) {
+            float col[4];
+            for (int i = 0; i < n; ++i)
+                col[i] = qr(i, k);
+            normsDir[k] = std::sqrt(seqSqNorm(col, n));
+            normsUpd[k] = normsDir[k];
+        }
+        const float eps = std::numeric_limits<float>::epsilon();
+        float maxNorm = normsUpd[0];
+        for (int k = 1; k < n; ++k)
+            if (normsUpd[k] > maxNorm)
+                maxNorm = normsUpd[k];
+        const float thresholdHelper = (maxNorm * eps) * (maxNorm * eps) / float(n);
+        const float downdateThreshold = std::sqrt(eps);
+        int nonzeroPivots = n;
+        for (int k = 0; k < n; ++k) {
+            int big = k;
+            float bigNorm = normsUpd[k];
+            for (int j = k + 1; j < n; ++j)
+                if (normsUpd[j] > bigNorm) {
+                    bigNorm = normsUpd[j];
+                    big = j;
+                }
+            const float bigSq = bigNorm * bigNorm;
+            if (nonzeroPivots == n && bigSq < thresholdHelper * float(n - k))
+                nonzeroPivots = k;
+            transp[k] = big;
+            if (k != big) {
+                for (int i = 0; i < n; ++i)
+                    std::swap(qr(i, k), qr(i, big));
+                std::swap(normsUpd[k], normsUpd[big]);
+                std::swap(normsDir[k], normsDir[big]);
+            }
+            // makeHouseholderInPlace on qr.col(k).tail(n-k)
+            const int len = n - k;
+            float tailSq = 0.0f;
+            if (len > 1) {
+                tailSq = qr(k + 1, k) * qr(k + 1, k);
+                for (int i = k + 2; i < n; ++i)
+                    tailSq = tailSq + qr(i, k) * qr(i, k);
+            }
+            const float c0 = qr(k, k);
+            float tau, beta;
+            const float tol = std::numeric_limits<float>::min();
+            if (tailSq <= tol) {
+                tau = 0.0f;
+                beta = c0;
+                for (int i = k + 1; i < n; ++i)
+                    qr(i, k) = 0.0f;
+            } else {
+                beta = std::sqrt(c0 * c0 + tailSq);
+                if (c0 >= 0.0f)
+                    beta = -beta;
+                const float denom = c0 - beta;
+                for (int i = k + 1; i < n; ++i)
+                    qr(i, k) = qr(i, k) / denom;
+                tau = (beta - c0) / beta;
+            }
+            hCoeffs[k] = tau;
+            qr(k, k) = beta;
+            // applyHouseholderOnTheLeft to bottomRightCorner(n-k, n-k-1)
+            const int cols = n - k - 1;
+            if (cols > 0) {
+                if (len == 1) {
+                    for (int j = k + 1; j < n; ++j)
+                        qr(k, j) = qr(k, j) * (1.0f - tau);
+                } else if (tau != 0.0f) {
+                    float tmp[4];
+                    for (int j = k + 1; j < n; ++j) {
+                        float s = 0.0f;
+                        for (int i = k + 1; i < n; ++i)
+                            s = s + qr(i, k) * qr(i, j);
+                        tmp[j] = s + qr(k, j);
+                    }
+                    for (int j = k + 1; j < n; ++j)
+                        qr(k, j) = qr(k, j) - tau * tmp[j];
+                    float tauEss[4];
+                    for (int i = k + 1; i < n; ++i)
+                        tauEss[i] = tau * qr(i, k);
+                    for (int j = k + 1; j < n; ++j)
+                        for (int i = k + 1; i < n; ++i)
+                            qr(i, j) = qr(i, j) - tmp[j] * tauEss[i];
+                }
+            }
+            // norm downdate (LAPACK xGEQP3 style)
+            for (int j = k + 1; j < n; ++j) {
+                if (normsUpd[j] != 0.0f) {
+                    float temp = std::fabs(qr(k, j)) / normsUpd[j];
+                    temp = (1.0f + temp) * (1.0f - temp);
+                    temp = temp < 0.0f ? 0.0f : temp;
+                    const float ratio = normsUpd[j] / normsDir[j];
+                    const float temp2 = temp * (ratio * ratio);
+                    if (temp2 <= downdateThreshold) {
+                        float s = 0.0f;
+                        if (n - k - 1 > 0) {
+                            s = qr(k + 1, j) * qr(k + 1, j);
+                            for (int i = k + 2; i < n; ++i)
+                                s = s + qr(i, j) * qr(i, j);
+                        }
+                        normsDir[j] = std::sqrt(s);
+                        normsUpd[j] = normsDir[j];
+                    } else {
+                        normsUpd[j] = normsUpd[j] * std::sqrt(temp);
+                    }
+                }
+            }
+        }
+        int perm[4];
+        for (int i = 0; i < n; ++i)
+            perm[i] = i;
+        for (int k = 0; k < n; ++k)
+            std::swap(perm[k], perm[transp[k]]);
+        if (nonzeroPivots == 0) {
+            for (int i = 0; i < n; ++i)
+                x[i] = 0.0f;
+            return;
+        }
+        float c[4];
+        for (int i = 0; i < n; ++i)
+            c[i] = b[i];
+        // apply Q^T = H_{p-1} ... H_0
+        for (int k = 0; k < nonzeroPivots; ++k) {
+            const int len = n - k;
+            const float tau = hCoeffs[k];
+            if (len == 1) {
+                c[k] = c[k] * (1.0f - tau);
+            } else if (tau != 0.0f) {
+                float s = 0.0f;
+                for (int i = k + 1; i < n; ++i)
+                    s = s + qr(i, k) * c[i];
+                s = s + c[k];
+                c[k] = c[k] - tau * s;
+                for (int i = k + 1; i < n; ++i)
+                    c[i] = c[i] - s * (tau * qr(i, k));
+            }
+        }
+        // upper-triangular back substitution, column-major order
+        const int p = nonzeroPivots;
+        for (int kk = 0; kk < p; ++kk) {
+            const int i = p - kk - 1;
+            if (c[i] != 0.0f) {
+                c[i] = c[i] / qr(i, i);
+                for (int s = 0; s < i; ++s)
+                    c[s] = c[s] - c[i] * qr(s, i);
+            }
+        }
+        for (int i = 0; i < n; ++i)
+            x[i] = 0.0f;
+        for (int i = 0; i < p; ++i)
+            x[perm[i]] = c[i];
+    }
+
+    // ------------------------------------------------------------------------------------------
+    // Geometry, core/Geometry.cpp:12-51 (2D), :53-109 (3D), :225-270 (buildMatrices)
+    // ------------------------------------------------------------------------------------------
+    struct Geom {
+        int dim = 3;
+        Mat P, Pinv, ext, K, R, S;
+        float t[3] = {0, 0, 0};
+        float C[3] = {0, 0, 0};
+        float sdd = 0;
+    };
+
+    static void buildMatrices(Geom& g)
+    {
+        const int d = g.dim;
+        Mat tmpRt = zeros(d + 1, d + 1);
+        for (int i = 0; i < d; ++i) {
+            for (int j = 0; j < d; ++j)
+                tmpRt(i, j) = g.R(i, j);
+            tmpRt(i, d) = g.t[i];
+        }
+        tmpRt(d, d) = 1.0f;
+        Mat tmpId = identity(d, d + 1);
+        Mat extFull = mul(tmpRt, g.S);
+        g.ext = zeros(d, d + 1);
+        for (int i = 0; i < d; ++i)
+            for (int j = 0; j <= d; ++j)
+                g.ext(i, j) = extFull(i, j);
+        g.P = mul(mul(g.K, tmpId), extFull);
+        // camera centre C = -(P(0:d,0:d)^-1 P(:,d)) by column-pivoting QR
+        Mat P33 = zeros(d, d);
+        float p4[3];
+        for (int i = 0; i < d; ++i) {
+            for (int j = 0; j < d; ++j)
+                P33(i, j) = g.P(i, j);
+            p4[i] = g.P(i, d);
+        }
+        float sol[3];
+        colPivQrSolve(P33, p4, sol);
+        for (int i = 0; i < d; ++i)
+            g.C[i] = -sol[i];
+        // Pinv = Sinv * Rtinv * tmpIdinv * Kinv
+        Mat Sinv = zeros(d + 1, d + 1);
+        for (int i = 0; i <= d; ++i)
+            Sinv(i, i) = 1.0f / g.S(i, i);
+        Mat Kinv = identity(d, d);
+        Kinv(0, 0) = 1.0f / g.K(0, 0);
+        Kinv(0, d - 1) = -g.K(0, d - 1) / g.K(0, 0);
+        if (d == 3) {
+            Kinv(1, 1) = 1.0f / g.K(1, 1);
+            Kinv(1, d - 1) = -g.K(1, d - 1) / g.K(1, 1);
+        }
+        Mat Rtinv = zeros(d + 1, d + 1);
+        for (int i = 0; i < d; ++i)
+            for (int j = 0; j < d; ++j)
+                Rtinv(i, j) = g.R(j, i);
+        // -R^T * t (GEMV with the negation folded into alpha)
+        for (int i = 0; i < d; ++i) {
+            float s = 0.0f;
+            for (int k = 0; k < d; ++k)
+                s = s + g.R(k, i) * g.t[k];
+            Rtinv(i, d) = -s;
+        }
+        Rtinv(d, d) = 1.0f;
+        Mat tmpIdinv = identity(d + 1, d);
+        g.Pinv = mul(mul(mul(Sinv, Rtinv), tmpIdinv), Kinv);
+    }
+
+    // Geometry.cpp:12-51
+    static Geom geometry2d(float s2c, float c2d, float angle, const float* volSpacing,
+                           const float* volOrigin, const float* sinoSpacing,
+                           const float* sinoOrigin, float ppOffset, const float* corOffset)
+    {
+        Geom g;
+        g.dim = 2;
+        g.sdd = s2c + c2d;
+        const float c = std::cos(angle);
+        const float s = std::sin(angle);
+        g.R = zeros(2, 2);
+        g.R(0, 0) = c;
+        g.R(0, 1) = -s;
+        g.R(1, 0) = s;
+        g.R(1, 1) = c;
+        g.S = identity(3, 3);
+        g.S(0, 0) = volSpacing[0];
+        g.S(1, 1) = volSpacing[1];
+        float v[2] = {-corOffset[0] - volOrigin[0], -corOffset[1] - volOrigin[1]};
+        matvec(g.R, v, g.t);
+        g.t[1] = g.t[1] + s2c;
+        const float alpha = sinoSpacing[0];
+        g.K = identity(2, 2);
+        g.K(0, 0) = (s2c + c2d) / alpha;
+        g.K(0, 1) = sinoOrigin[0] / alpha + ppOffset;
+        buildMatrices(g);
+        return g;
+    }
+
+    // Geometry.cpp:53-109 (YZY convention, angles gamma, beta, alpha)
+    static Geom geometry3d(float s2c, float c2d, const float* volSpacing, const float* volOrigin,
+                           const float* sinoSpacing, const float* sinoOrigin, float gamma,
+                           float beta, float alpha, const float* ppOffset, const float* corOffset)
+    {
+        Geom g;
+        g.dim = 3;
+        g.sdd = s2c + c2d;
+        const float ca = std::cos(alpha), sa = std::sin(alpha);
+        const float cb = std::cos(beta), sb = std::sin(beta);
+        const float cg = std::cos(gamma), sg = std::sin(gamma);
+        Mat A = zeros(3, 3), B = zeros(3, 3), Cm = zeros(3, 3);
+        A(0, 0) = cg; A(0, 1) = 0; A(0, 2) = sg;
+        A(1, 0) = 0;  A(1, 1) = 1; A(1, 2) = 0;
+        A(2, 0) = -sg; A(2, 1) = 0; A(2, 2) = cg;
+        B(0, 0) = cb; B(0, 1) = -sb; B(0, 2) = 0;
+        B(1, 0) = sb; B(1, 1) = cb; B(1, 2) = 0;
+        B(2, 0) = 0;  B(2, 1) = 0;  B(2, 2) = 1;
+        Cm(0, 0) = ca; Cm(0, 1) = 0; Cm(0, 2) = sa;
+        Cm(1, 0) = 0;  Cm(1, 1) = 1; Cm(1, 2) = 0;
+        Cm(2, 0) = -sa; Cm(2, 1) = 0; Cm(2, 2) = ca;
+        g.R = mul(mul(A, B), Cm);
+        g.S = identity(4, 4);
+        for (int i = 0; i < 3; ++i)
+            g.S(i, i) = volSpacing[i];
+        float v[3] = {-corOffset[0] - volOrigin[0], -corOffset[1] - volOrigin[1],
+                      -corOffset[2] - volOrigin[2]};
+        matvec(g.R, v, g.t);
+        g.t[2] = g.t[2] + s2c;
+        const float a1 = sinoSpacing[0], a2 = sinoSpacing[1];
+        g.K = identity(3, 3);
+        g.K(0, 0) = (s2c + c2d) / a1;
+        g.K(0, 2) = sinoOrigin[0] / a1 + ppOffset[0];
+        g.K(1, 1) = (s2c + c2d) / a2;
+        g.K(1, 2) = sinoOrigin[1] / a2 + ppOffset[1];
+        buildMatrices(g);
+        return g;
+    }
+
+    // Pose record exchanged with the tests (same layout as the product's C ABI):
+    // P at 0 (d x d+1, row-major), Pinv at 12 (d+1 x d), C at 24, ext at 27 (d x d+1), sdd at 39.
+    constexpr int POSE_FLOATS = 40;
+
+    static void packPose(const Geom& g, float* out)
+    {
+        std::memset(out, 0, sizeof(float) * POSE_FLOATS);
+        const int d = g.dim;
+        for (int i = 0; i < d * (d + 1); ++i) {
+            out[i] = g.P.a[i];
+            out[12 + i] = g.Pinv.a[i];
+            out[27 + i] = g.ext.a[i];
+        }
+        for (int i = 0; i < d; ++i)
+            out[24 + i] = g.C[i];
+        out[39] = g.sdd;
+    }
+
+    struct PoseView {
+        int dim;
+        const float* p;
+        float P(int i, int j) const { return p[i * (dim + 1) + j]; }
+        float Pinv(int i, int j) const { return p[12 + i * dim + j]; }
+        float C(int i) const { return p[24 + i]; }
+        float ext(int i, int j) const { return p[27 + i * (dim + 1) + j]; }
+        float sdd() const { return p[39]; }
+    };
+
+    // ------------------------------------------------------------------------------------------
+    // Rays: core/Descriptors/DetectorDescriptor.cpp:20-52,90-128
+    // ------------------------------------------------------------------------------------------
+    struct Ray {
+        float o[3];
+        float d[3];
+    };
+
+    static Ray rayFromDetector(const PoseView& pv, const float* detCoord)
+    {
+        const int d = pv.dim;
+        float h[3] = {detCoord[0], d == 3 ? detCoord[1] : 1.0f, 1.0f};
+        Ray r{};
+        float dir[4];
+        for (int i = 0; i <= d; ++i) {
+            float s = 0.0f;
+            for (int k = 0; k < d; ++k)
+                s = s + pv.Pinv(i, k) * h[k];
+            dir[i] = s;
+        }
+        const float z = seqSqNorm(dir, d);
+        const float nrm = std::sqrt(z);
+        for (int i = 0; i < d; ++i) {
+            r.d[i] = z > 0.0f ? dir[i] / nrm : dir[i];
+            r.o[i] = pv.C(i);
+        }
+        return r;
+    }
+
+    static Ray rayForIndex(const PoseView* poses, int dim, const index_t* detDims, index_t ir)
+    {
+        // detector coordinate from index, x (u) fastest, pose last
+        float dc[2] = {0, 0};
+        index_t pose;
+        if (dim == 2) {
+            const index_t u = ir % detDims[0];
+            pose = ir / detDims[0];
+            dc[0] = static_cast<float>(u) + 0.5f;
+        } else {
+            const index_t u = ir % detDims[0];
+            const index_t v = (ir / detDims[0]) % detDims[1];
+            pose = ir / (detDims[0] * detDims[1]);
+            dc[0] = static_cast<float>(u) + 0.5f;
+            dc[1] = static_cast<float>(v) + 0.5f;
+        }
+        return rayFromDetector(poses[pose], dc);
+    }
+
+    // projectors/Intersection.h:179-198
+    template <typename T1, typename T2>
+    static T1 minNum(T1 x, T2 y)
+    {
+        return (y != y) ? x : (x < y ? x : static_cast<T1>(y));
+    }
+    template <typename T1, typename T2>
+    static T1 maxNum(T1 x, T2 y)
+    {
+        return (y != y) ? x : (x > y ? x : static_cast<T1>(y));
+    }
+
+    // projectors/Intersection.cpp:7-46; box is [0, dims]
+    static bool intersectRay(const float* boxMax, int dim, const Ray& r, float& tmin, float& tmax)
+    {
+        float invDir = 1 / r.d[0];
+        float t1 = (0.0f - r.o[0]) * invDir;
+        float t2 = (boxMax[0] - r.o[0]) * invDir;
+        tmin = invDir >= 0 ? t1 : t2;
+        tmax = invDir >= 0 ? t2 : t1;
+        for (int i = 1; i < dim; ++i) {
+            invDir = 1 / r.d[i];
+            t1 = (0.0f - r.o[i]) * invDir;
+            t2 = (boxMax[i] - r.o[i]) * invDir;
+            tmin = maxNum(tmin, invDir >= 0 ? t1 : t2);
+            tmax = minNum(tmax, invDir >= 0 ? t2 : t1);
+        }
+        if (tmax == 0.0f && tmin == 0.0f)
+            return false;
+        return tmax >= maxNum(tmin, 0.0f);
+    }
+
+    // ------------------------------------------------------------------------------------------
+    // Joseph: projectors/DrivingDirectionTraversal.cpp:6-106 + JosephsMethod.cpp:37-198
+    // ------------------------------------------------------------------------------------------
+    struct DDTraversal {
+        float pos[3], step[3];
+        float length = 0;
+        int driving = 0;
+        index_t numSteps = 0;
+    };
+
+    static DDTraversal ddSetup(const float* boxMax, int dim, const Ray& r)
+    {
+        DDTraversal t;
+        float tmin, tmax;
+        const bool hit = intersectRay(boxMax, dim, r, tmin, tmax);
+        // argmax |d| (first occurrence)
+        int drv = 0;
+        float best = std::fabs(r.d[0]);
+        for (int i = 1; i < dim; ++i)
+            if (std::fabs(r.d[i]) > best) {
+                best = std::fabs(r.d[i]);
+                drv = i;
+            }
+        t.driving = drv;
+        if (!hit) {
+            t.numSteps = 0;
+            return t;
+        }
+        float exitp[3] = {0, 0, 0};
+        for (int i = 0; i < dim; ++i) {
+            t.pos[i] = r.o[i] + r.d[i] * tmin;
+            exitp[i] = r.o[i] + r.d[i] * tmax;
+            if (t.pos[i] < 0.0f)
+                t.pos[i] = 0.0f;
+            if (t.pos[i] > boxMax[i])
+                t.pos[i] = boxMax[i];
+            if (exitp[i] < 0.0f)
+                exitp[i] = 0.0f;
+            if (exitp[i] > boxMax[i])
+                exitp[i] = boxMax[i];
+        }
+        const float absd = std::fabs(r.d[drv]);
+        for (int i = 0; i < dim; ++i)
+            t.step[i] = r.d[i] / absd;
+        const float dist = t.pos[drv] - std::floor(t.pos[drv]);
+        const float sgn = (t.step[drv] > 0.0f) ? 1.0f : ((t.step[drv] < 0.0f) ? -1.0f : 0.0f);
+        const float shift = 0.5f - dist;
+        for (int i = 0; i < dim; ++i)
+            t.pos[i] = t.pos[i] + (t.step[i] * shift) * sgn;
+        t.pos[drv] = std::floor(t.pos[drv]) + 0.5f;
+        t.numSteps = static_cast<index_t>(std::ceil(std::fabs(exitp[drv] - t.pos[drv])));
+        // fixed-size Eigen array norm: the unrolled reduction adds s0^2 + (s1^2 + s2^2)
+        t.length = dim == 3 ? std::sqrt(t.step[0] * t.step[0]
+                                        + (t.step[1] * t.step[1] + t.step[2] * t.step[2]))
+                            : std::sqrt(t.step[0] * t.step[0] + t.step[1] * t.step[1]);
+        return t;
+    }
+
+    // Visit the taps of one Joseph sample exactly as JosephsMethod.cpp:37-97 does: weights from
+    // the position, masked (weight 0) and clipped taps, in the reference's tap order.
+    template <class Fn>
+    static void josephTaps(const float* pos, int drv, int dim, const index_t* volDims, Fn fn)
+    {
+        index_t fl[3], ce[3];
+        float w[3], cw[3];
+        for (int i = 0; i < dim; ++i) {
+            const float p5 = pos[i] - 0.5f;
+            fl[i] = static_cast<index_t>(std::floor(p5));
+            ce[i] = static_cast<index_t>(std::ceil(p5));
+            cw[i] = (pos[i] - static_cast<float>(fl[i])) - 0.5f;
+            w[i] = 1.0f - cw[i];
+        }
+        w[drv] = 1.0f;
+        cw[drv] = 1.0f;
+        auto tap = [&](index_t i0, index_t i1, index_t i2, float w0, float w1, float w2) {
+            index_t c[3] = {i0, i1, i2};
+            bool in = true;
+            for (int k = 0; k < dim; ++k)
+                in = in && c[k] >= 0 && c[k] < volDims[k];
+            for (int k = 0; k < dim; ++k)
+                c[k] = std::max<index_t>(0, std::min<index_t>(c[k], volDims[k] - 1));
+            float wt = static_cast<float>(in) * w0;
+            wt = wt * w1;
+            if (dim == 3)
+                wt = wt * w2;
+            const index_t idx =
+                dim == 2 ? c[0] + c[1] * volDims[0] : c[0] + volDims[0] * (c[1] + volDims[1] * c[2]);
+            fn(idx, wt);
+        };
+        if (dim == 2) {
+            tap(fl[0], ce[1], 0, w[0], cw[1], 1.0f);
+            tap(ce[0], fl[1], 0, cw[0], w[1], 1.0f);
+        } else {
+            tap(fl[0], fl[1], fl[2], w[0], w[1], w[2]);
+            tap(fl[0], ce[1], ce[2], w[0], cw[1], cw[2]);
+            tap(ce[0], fl[1], ce[2], cw[0], w[1], cw[2]);
+            tap(ce[0], ce[1], fl[2], cw[0], cw[1], w[2]);
+        }
+    }
+
+    // mode 0: reference position update (pos += step each step, DrivingDirectionTraversal.cpp:265)
+    // mode 1: pos_j = fma(j, step, pos_0) (one rounding; used to isolate the accumulation drift)
+    template <typename data_t, bool adjoint>
+    static void josephTraverse(int dim, const index_t* volDims, const index_t* detDims,
+                               index_t numPoses, const float* poseData, const data_t* in,
+                               data_t* out, int mode)
+    {
+        std::vector<PoseView> poses(numPoses);
+        for (index_t p = 0; p < numPoses; ++p)
+            poses[p] = PoseView{dim, poseData + p * POSE_FLOATS};
+        float boxMax[3] = {0, 0, 0};
+        index_t nvol = 1;
+        for (int i = 0; i < dim; ++i) {
+            boxMax[i] = static_cast<float>(volDims[i]);
+            nvol *= volDims[i];
+        }
+        const index_t nrays = (dim == 2 ? detDims[0] : detDims[0] * detDims[1]) * numPoses;
+        if (adjoint)
+            std::fill(out, out + nvol, data_t(0));
+#pragma omp parallel for schedule(dynamic, 256)
+        for (index_t ir = 0; ir < nrays; ++ir) {
+            const Ray r = rayForIndex(poses.data(), dim, detDims, ir);
+            DDTraversal tr = ddSetup(boxMax, dim, r);
+            const data_t L = static_cast<data_t>(tr.length);
+            data_t acc = 0;
+            float pos[3] = {tr.pos[0], tr.pos[1], tr.pos[2]};
+            for (index_t s = 0; s < tr.numSteps; ++s) {
+                if (mode == 1) {
+                    for (int i = 0; i < dim; ++i)
+                        pos[i] = std::fma(static_cast<float>(s), tr.step[i], tr.pos[i]);
+                }
+                if (adjoint) {
+                    const data_t y = in[ir];
+                    josephTaps(pos, tr.driving, dim, volDims, [&](index_t idx, float wt) {
+                        const data_t v = y * L * static_cast<data_t>(wt);
+#pragma omp atomic
+                        out[idx] += v;
+                    });
+                } else {
+                    josephTaps(pos, tr.driving, dim, volDims, [&](index_t idx, float wt) {
+                        acc += in[idx] * L * static_cast<data_t>(wt);
+                    });
+                }
+                if (mode == 0)
+                    for (int i = 0; i < dim; ++i)
+                        pos[i] = pos[i] + tr.step[i];
+            }
+            if (!adjoint)
+                out[ir] = acc;
+        }
+    }
+
+    // ------------------------------------------------------------------------------------------
+    // Siddon: projectors/TraverseAABB.cpp:6-184 + SiddonsMethod.cpp:76-124
+    // ------------------------------------------------------------------------------------------
+    template <typename data_t, bool adjoint>
+    static void siddonTraverse(int dim, const index_t* volDims, const index_t* detDims,
+                               index_t numPoses, const float* poseData, const data_t* in,
+                               data_t* out)
+    {
+        std::vector<PoseView> poses(numPoses);
+        for (index_t p = 0; p < numPoses; ++p)
+            poses[p] = PoseView{dim, poseData + p * POSE_FLOATS};
+        float boxMax[3] = {0, 0, 0};
+        index_t nvol = 1;
+        index_t strides[3] = {1, volDims[0], dim == 3 ? volDims[0] * volDims[1] : 0};
+        for (int i = 0; i < dim; ++i) {
+            boxMax[i] = static_cast<float>(volDims[i]);
+            nvol *= volDims[i];
+        }
+        const index_t nrays = (dim == 2 ? detDims[0] : detDims[0] * detDims[1]) * numPoses;
+        if (adjoint)
+            std::fill(out, out + nvol, data_t(0));
+        const float EPS = std::numeric_limits<float>::epsilon();
+        const float MAXF = std::numeric_limits<float>::max();
+#pragma omp parallel for schedule(dynamic, 256)
+        for (index_t ir = 0; ir < nrays; ++ir) {
+            const Ray r = rayForIndex(poses.data(), dim, detDims, ir);
+            data_t acc = 0;
+            float tmin, tmax;
+            bool inBox = intersectRay(boxMax, dim, r, tmin, tmax);
+            if (inBox) {
+                float entry[3], cur[3], T[3], tDelta[3];
+                int stepDir[3];
+                for (int i = 0; i < dim; ++i) {
+                    entry[i] = r.o[i] + r.d[i] * tmin;
+                    if (entry[i] < 0.0f)
+                        entry[i] = 0.0f;
+                    if (entry[i] > boxMax[i])
+                        entry[i] = boxMax[i];
+                }
+                for (int i = 0; i < dim; ++i)
+                    stepDir[i] = (r.d[i] > 0.0f) ? 1 : ((r.d[i] < 0.0f) ? -1 : 0);
+                for (int i = 0; i < dim; ++i) {
+                    float lc = std::floor(entry[i]);
+                    if (lc == entry[i] && stepDir[i] < 0)
+                        lc = lc - 1.0f;
+                    cur[i] = lc;
+                }
+                for (int i = 0; i < dim; ++i)
+                    if (cur[i] >= boxMax[i] || cur[i] < 0.0f)
+                        inBox = false;
+                if (inBox) {
+                    for (int i = 0; i < dim; ++i) {
+                        const float td = static_cast<float>(stepDir[i]) / r.d[i];
+                        tDelta[i] = std::fabs(r.d[i]) > EPS ? td : MAXF;
+                        const float tt =
+                            ((r.d[i] > 0.0f ? cur[i] + 1.0f : cur[i]) - entry[i]) / r.d[i];
+                        T[i] = std::fabs(r.d[i]) > EPS ? tt : MAXF;
+                    }
+                    index_t idx = 0;
+                    for (int i = 0; i < dim; ++i)
+                        idx += strides[i] * static_cast<index_t>(cur[i]);
+                    float tExit = 0.0f;
+                    while (inBox) {
+                        const float tEntry = tExit;
+                        float tm = T[0];
+                        for (int i = 1; i < dim; ++i)
+                            tm = (T[i] < tm) ? T[i] : tm;
+                        tExit = tm;
+                        bool mask[3];
+                        for (int i = 0; i < dim; ++i) {
+                            bool m = true;
+                            for (int j = 0; j < dim; ++j)
+                                if (j != i)
+                                    m = m && (T[i] <= T[j]);
+                            mask[i] = m;
+                        }
+                        for (int i = 0; i < dim; ++i) {
+                            if (mask[i]) {
+                                cur[i] = cur[i] + static_cast<float>(stepDir[i]);
+                                T[i] = T[i] + tDelta[i];
+                            }
+                        }
+                        for (int i = 0; i < dim; ++i)
+                            if (!(cur[i] < boxMax[i] && cur[i] >= 0.0f))
+                                inBox = false;
+                        const float weight = tExit - tEntry;
+                        if (adjoint) {
+                            const data_t v = in[ir] * static_cast<data_t>(weight);
+#pragma omp atomic
+                            out[idx] += v;
+                        } else {
+                            acc += in[idx] * static_cast<data_t>(weight);
+                        }
+                        for (int i = 0; i < dim; ++i)
+                            if (mask[i])
+                                idx += stepDir[i] * strides[i];
+                    }
+                }
+            }
+            if (!adjoint)
+                out[ir] = acc;
+        }
+    }
+
+    // ------------------------------------------------------------------------------------------
+    // Vector operations (storage/reductions/DotProduct.h:24-47, L2.h:15-49,
+    // transforms/Lincomb.h:28-33): reductions accumulate in data_t, in 64 fixed blocks combined
+    // sequentially (a deterministic stand-in for Thrust's blocked reduction).
+    // ------------------------------------------------------------------------------------------
+    template <typename data_t>
+    static data_t blockedDot(const data_t* a, const data_t* b, index_t n)
+    {
+        const int NB = 64;
+        data_t part[NB];
+#pragma omp parallel for
+        for (int blk = 0; blk < NB; ++blk) {
+            const index_t lo = n * blk / NB, hi = n * (blk + 1) / NB;
+            data_t s = 0;
+            for (index_t i = lo; i < hi; ++i)
+                s += a[i] * b[i];
+            part[blk] = s;
+        }
+        data_t s = 0;
+        for (int blk = 0; blk < NB; ++blk)
+            s += part[blk];
+        return s;
+    }
+
+} // namespace orc
+
+// ----------------------------------------------------------------------------------------------
+// C ABI for the Python test harness (ctypes)
+// ----------------------------------------------------------------------------------------------
+using orc::index_t;
+
+extern "C" {
+
+int oracle_num_threads(void)
+{
+    return omp_get_max_threads();
+}
+
+void oracle_set_num_threads(int n)
+{
+    omp_set_num_threads(n);
+}
+
+// Single 2D pose (Geometry.cpp:12-51) packed into a 40-float pose record.
+void oracle_geometry2d(float s2c, float c2d, float angleRad, const float* volSpacing,
+                       const float* volOrigin, const float* sinoSpacing, const float* sinoOrigin,
+                       float ppOffset, const float* corOffset, float* out)
+{
+    orc::packPose(orc::geometry2d(s2c, c2d, angleRad, volSpacing, volOrigin, sinoSpacing,
+                                  sinoOrigin, ppOffset, corOffset),
+                  out);
+}
+
+// Single 3D pose (Geometry.cpp:53-109).
+void oracle_geometry3d(float s2c, float c2d, const float* volSpacing, const float* volOrigin,
+                       const float* sinoSpacing, const float* sinoOrigin, float gamma, float beta,
+                       float alpha, const float* ppOffset, const float* corOffset, float* out)
+{
+    orc::packPose(orc::geometry3d(s2c, c2d, volSpacing, volOrigin, sinoSpacing, sinoOrigin, gamma,
+                                  beta, alpha, ppOffset, corOffset),
+                  out);
+}
+
+// Circular trajectory: generators/CircleTrajectoryGenerator.cpp:9-24,
+// BaseCircleTrajectoryGenerator.cpp:12-74, TrajectoryGenerator.cpp:9-47.
+// volDims/volSpacing: dim entries; detSize: dim-1 entries (or NULL -> floor(N*sqrt(2)));
+// detSpacing: dim-1 entries (or NULL -> volume spacing). Writes numPoses pose records and the
+// detector coefficient counts (dim entries, last = numPoses).
+void oracle_circle_trajectory(int dim, const int64_t* volDims, const float* volSpacing,
+                              int64_t numPoses, float arcDegrees, float s2c, float c2d,
+                              const int64_t* detSize, const float* detSpacing, float* outPoses,
+                              int64_t* outDetDims)
+{
+    float volOrigin[3], spacing[3], coeffsF[3];
+    int64_t coeffs[3];
+    for (int i = 0; i < dim; ++i)
+        volOrigin[i] = 0.5f * (static_cast<float>(volDims[i]) * volSpacing[i]);
+    if (detSize) {
+        for (int i = 0; i < dim - 1; ++i)
+            coeffs[i] = detSize[i];
+    } else {
+        const float sqrt2 = std::sqrt(2.f);
+        for (int i = 0; i < dim - 1; ++i)
+            coeffs[i] = static_cast<int64_t>(static_cast<float>(volDims[i]) * sqrt2);
+    }
+    coeffs[dim - 1] = numPoses;
+    for (int i = 0; i < dim - 1; ++i)
+        spacing[i] = detSpacing ? detSpacing[i] : volSpacing[i];
+    spacing[dim - 1] = 1.0f;
+    for (int i = 0; i < dim; ++i) {
+        coeffsF[i] = static_cast<float>(coeffs[i]);
+        outDetDims[i] = coeffs[i];
+    }
+    float sinoOrigin[3];
+    for (int i = 0; i < dim; ++i)
+        sinoOrigin[i] = 0.5f * (coeffsF[i] * spacing[i]);
+    // Eigen LinSpaced(n, 0, arc) for float: low + i*step, last = high
+    const float arc = static_cast<float>(arcDegrees);
+    const float stepDeg = numPoses == 1 ? 0.0f : (arc - 0.0f) / static_cast<float>(numPoses - 1);
+    const float zero3[3] = {0, 0, 0};
+    for (int64_t p = 0; p < numPoses; ++p) {
+        float deg = (p == numPoses - 1) ? arc : 0.0f + static_cast<float>(p) * stepDeg;
+        if (numPoses == 1)
+            deg = arc;
+        const float rad = deg * orc::pi_f() / 180;
+        float* out = outPoses + p * orc::POSE_FLOATS;
+        if (dim == 2)
+            orc::packPose(orc::geometry2d(s2c, c2d, rad, volSpacing, volOrigin, spacing,
+                                          sinoOrigin, 0.0f, zero3),
+                          out);
+        else
+            orc::packPose(orc::geometry3d(s2c, c2d, volSpacing, volOrigin, spacing, sinoOrigin,
+                                          rad, 0.0f, 0.0f, zero3, zero3),
+                          out);
+    }
+}
+
+// Ray for one detector index: writes origin (dim) and direction (dim).
+void oracle_ray(int dim, const int64_t* detDims, const float* poses, int64_t ir, float* origin,
+                float* direction)
+{
+    std::vector<orc::PoseView> pv(detDims[dim - 1]);
+    for (int64_t p = 0; p < detDims[dim - 1]; ++p)
+        pv[p] = orc::PoseView{dim, poses + p * orc::POSE_FLOATS};
+    const orc::Ray r = orc::rayForIndex(pv.data(), dim, detDims, ir);
+    for (int i = 0; i < dim; ++i) {
+        origin[i] = r.o[i];
+        direction[i] = r.d[i];
+    }
+}
+
+// Driving-direction traversal setup for one ray: pos (dim), step (dim), length, driving axis,
+// number of steps.
+void oracle_dd_setup(int dim, const int64_t* volDims, const float* origin, const float* direction,
+                     float* pos, float* step, float* length, int* driving, int64_t* numSteps)
+{
+    float boxMax[3] = {0, 0, 0};
+    for (int i = 0; i < dim; ++i)
+        boxMax[i] = static_cast<float>(volDims[i]);
+    orc::Ray r{};
+    for (int i = 0; i < dim; ++i) {
+        r.o[i] = origin[i];
+        r.d[i] = direction[i];
+    }
+    const orc::DDTraversal t = orc::ddSetup(boxMax, dim, r);
+    for (int i = 0; i < dim; ++i) {
+        pos[i] = t.pos[i];
+        step[i] = t.step[i];
+    }
+    *length = t.length;
+    *driving = t.driving;
+    *numSteps = t.numSteps;
+}
+
+void oracle_joseph_f32(int adjoint, int dim, const int64_t* volDims, const int64_t* detDims,
+                       const float* poses, const float* in, float* out, int mode)
+{
+    const int64_t np = detDims[dim - 1];
+    if (adjoint)
+        orc::josephTraverse<float, true>(dim, volDims, detDims, np, poses, in, out, mode);
+    else
+        orc::josephTraverse<float, false>(dim, volDims, detDims, np, poses, in, out, mode);
+}
+
+void oracle_joseph_f64(int adjoint, int dim, const int64_t* volDims, const int64_t* detDims,
+                       const float* poses, const double* in, double* out, int mode)
+{
+    const int64_t np = detDims[dim - 1];
+    if (adjoint)
+        orc::josephTraverse<double, true>(dim, volDims, detDims, np, poses, in, out, mode);
+    else
+        orc::josephTraverse<double, false>(dim, volDims, detDims, np, poses, in, out, mode);
+}
+
+void oracle_siddon_f32(int adjoint, int dim, const int64_t* volDims, const int64_t* detDims,
+                       const float* poses, const float* in, float* out)
+{
+    const int64_t np = detDims[dim - 1];
+    if (adjoint)
+        orc::siddonTraverse<float, true>(dim, volDims, detDims, np, poses, in, out);
+    else
+        orc::siddonTraverse<float, false>(dim, volDims, detDims, np, poses, in, out);
+}
+
+void oracle_siddon_f64(int adjoint, int dim, const int64_t* volDims, const int64_t* detDims,
+                       const float* poses, const double* in, double* out)
+{
+    const int64_t np = detDims[dim - 1];
+    if (adjoint)
+        orc::siddonTraverse<double, true>(dim, volDims, detDims, np, poses, in, out);
+    else
+        orc::siddonTraverse<double, false>(dim, volDims, detDims, np, poses, in, out);
+}
+
+// Number of Joseph samples (sum over rays of numSteps) and Siddon voxel crossings, used for the
+// algorithmic-bytes figure of the roofline.
+int64_t oracle_joseph_sample_count(int dim, const int64_t* volDims, const int64_t* detDims,
+                                   const float* poseData)
+{
+    const int64_t np = detDims[dim - 1];
+    std::vector<orc::PoseView> poses(np);
+    for (int64_t p = 0; p < np; ++p)
+        poses[p] = orc::PoseView{dim, poseData + p * orc::POSE_FLOATS};
+    float boxMax[3] = {0, 0, 0};
+    for (int i = 0; i < dim; ++i)
+        boxMax[i] = static_cast<float>(volDims[i]);
+    const int64_t nrays = (dim == 2 ? detDims[0] : detDims[0] * detDims[1]) * np;
+    int64_t total = 0;
+#pragma omp parallel for reduction(+ : total)
+    for (int64_t ir = 0; ir < nrays; ++ir) {
+        const orc::Ray r = orc::rayForIndex(poses.data(), dim, detDims, ir);
+        total += orc::ddSetup(boxMax, dim, r).numSteps;
+    }
+    return total;
+}
+
+double oracle_dot_f32(const float* a, const float* b, int64_t n)
+{
+    return static_cast<double>(orc::blockedDot(a, b, n));
+}
+
+double oracle_dot_f64(const double* a, const double* b, int64_t n)
+{
+    return orc::blockedDot(a, b, n);
+}
+
+} // extern "C"
