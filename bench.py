@@ -1,0 +1,327 @@
+#!/usr/bin/env python3
+"""Benchmark of the elsa_b200 hot path: 3D cone-beam Joseph forward + matched adjoint inside CGNE
+iterations at 256^3 (360 views, 384 x 384 detector, source-centre 2560, centre-detector 640).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl elsa_b200|reference]
+
+One step is one CGNE iteration (solvers/CGNE.cpp:50-73 of elsa): a forward projection, the matched
+adjoint and the fused float64 vector updates, enqueued through the C ABI (elsa_solver_iterate).
+`value` counts the voxel-view updates of the forward + adjoint pass per second (GUPS = 2 * N_vox *
+N_views per step). `e2e` is the same metric through the host-buffer entry points (the reference's
+call pattern: volume in, sinogram out, sinogram in, volume out, every apply). Under torchrun every
+rank runs its own replica of the problem (the cone-beam problem has no exchange step at this size)
+and `value` is the sum over ranks, timed as the max over ranks.
+
+`--impl reference` times the CPU restatement of elsa's own algorithm (oracle/, the reference
+C++ library cannot be built here: Eigen 3.4 is absent) on the host cores, on a bounded subset of
+views per step, and reports the same metric.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "3D cone-beam fwd+back GUPS and CG iters/s at 256^3; batched vs plain, 1 GPU"
+WORKLOAD = dict(workload="cone-beam Joseph CGNE, 256^3 volume, 360 views, 384x384 detector",
+                volume=[256, 256, 256], views=360, detector=[384, 384], source_to_center=2560,
+                center_to_detector=640, phantom="modified Shepp-Logan 3D")
+# kernels launched per CGNE iteration: forward, adjoint, dot (2), step, finish-norm, direction
+LAUNCHES_PER_STEP = 7
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device_index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names[1:], parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline_sample(views_in_sample, vol, poses, det, x):
+    """Time the oracle (CPU restatement of elsa's Joseph path, all host threads) on a subset of
+    the views: forward + adjoint. Returns (GUPS, seconds, threads)."""
+    from oracle import oracle as O
+    O.build()
+    idx = np.linspace(0, poses.shape[0] - 1, views_in_sample).round().astype(int)
+    p = np.ascontiguousarray(poses[idx])
+    d = np.array([det[0], det[1], len(idx)])
+    t0 = time.perf_counter()
+    y = O.joseph(x, vol, d, p)
+    O.joseph_adjoint(y, vol, d, p)
+    dt = time.perf_counter() - t0
+    return 2.0 * np.prod(vol) * len(idx) / dt / 1e9, dt, O.num_threads()
+
+
+def _traffic_from_profiles():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "joseph_cone256_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def run_elsa(args):
+    import torch
+    import elsa_b200
+    from elsa_b200 import phantoms
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    vol = tuple(WORKLOAD["volume"])
+    poses, det = elsa_b200.circle_trajectory(vol, WORKLOAD["views"], 360,
+                                             WORKLOAD["source_to_center"],
+                                             WORKLOAD["center_to_detector"], WORKLOAD["detector"])
+    proj = elsa_b200.Projector(elsa_b200.PROJECTOR_JOSEPH, vol, det, poses)
+    x_true = phantoms.modified_shepp_logan(vol)
+    stream = torch.cuda.current_stream().cuda_stream
+    xt = torch.from_numpy(x_true.ravel()).cuda()
+    b = torch.empty(proj.range_size, dtype=torch.float32, device="cuda")
+    proj.apply_ptr(xt.data_ptr(), b.data_ptr(), stream)
+    x = torch.zeros(proj.domain_size, dtype=torch.float32, device="cuda")
+    solver = elsa_b200.Solver(elsa_b200.SOLVER_CGNE, proj, b.data_ptr(), x.data_ptr(),
+                              stream=stream)
+    solver.iterate(args.warmup, stream)
+    torch.cuda.synchronize()
+    res0 = solver.squared_residual(stream)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    solver.enable_timing(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    solver.iterate(args.steps, stream)
+    end.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = start.elapsed_time(end)
+    clock_info = clocks.stop()
+    fwd_ms, adj_ms, timed = solver.timing()
+    res1 = solver.squared_residual(stream)
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    updates = 2.0 * np.prod(vol) * WORKLOAD["views"]  # forward + adjoint voxel-view updates
+    ms_per_step = ms / args.steps
+    value = updates * args.steps * world / (ms / 1e3) / 1e9
+
+    # end to end through the host-buffer entry points (pinned host memory)
+    xh = torch.from_numpy(x_true.ravel()).pin_memory().numpy()
+    yh = torch.empty(proj.range_size, dtype=torch.float32).pin_memory().numpy()
+    bh = torch.empty(proj.domain_size, dtype=torch.float32).pin_memory().numpy()
+    import ctypes
+    from elsa_b200 import _capi
+
+    def e2e_step():
+        _capi.call("elsa_projector_apply_host", proj.handle, _capi.np_ptr(xh), _capi.np_ptr(yh))
+        _capi.call("elsa_projector_apply_adjoint_host", proj.handle, _capi.np_ptr(yh),
+                   _capi.np_ptr(bh))
+
+    e2e_steps = max(2, min(args.steps, 5))
+    e2e_step()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = updates * e2e_steps * world / e2e_s / 1e9
+    h2d = 4 * (proj.domain_size + proj.range_size)
+    d2h = 4 * (proj.range_size + proj.domain_size)
+
+    # roofline of the dominant kernel (algorithmic gather bytes)
+    samples = proj.info(2)
+    bytes_per_pass = 4.0 * (proj.domain_size + proj.range_size) + 16.0 * samples
+    fwd_avg, adj_avg = fwd_ms / max(timed, 1), adj_ms / max(timed, 1)
+    dominant = "josephAdjointKernel" if adj_avg >= fwd_avg else "josephForwardKernel"
+    dom_ms = max(fwd_avg, adj_avg)
+    peak, peak_kind = _peaks()
+    achieved = bytes_per_pass / (dom_ms / 1e3) / 1e9
+    traffic = None
+    prof = _traffic_from_profiles()
+    if prof and prof.get("kernel") == dominant:
+        traffic = prof.get("dram_bytes_per_launch")
+    compulsory = 4.0 * (proj.domain_size + proj.range_size)
+
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (modified Shepp-Logan 3D phantom, b = A x)",
+        "config": dict(WORKLOAD, parallelism="replicas" if world > 1 else "single GPU",
+                       l2="working set > L2 (1.7 GB ray table + 8 GB checkpoints + 212 MB "
+                          "sinogram per step)"),
+        "cg_iters_per_s": round(1e3 / ms_per_step, 3),
+        "forward_ms": round(fwd_avg, 4), "adjoint_ms": round(adj_avg, 4),
+        "cg_residual_sq": [res0, res1],
+        "e2e": {"value": round(e2e_value, 3), "unit": "GUPS", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "timing": "host wall clock, pinned buffers"},
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1),
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "algorithmic_bytes_per_launch": bytes_per_pass,
+                     "samples_per_launch": samples,
+                     "compulsory_frac": round(compulsory / (dom_ms / 1e3) / 1e9 / peak, 5)},
+        "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+        "clocks": clock_info,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        gups, dt, cores = cpu_baseline_sample(args.cpu_views, vol, poses, det, x_true)
+        out["cpu_baseline"] = {"value": round(gups, 5), "unit": "GUPS", "cores": cores,
+                               "kind": "port", "seconds": round(dt, 2),
+                               "sample": "Joseph forward + adjoint over %d of the 360 views "
+                                         "(256^3, 384^2 detector)" % args.cpu_views}
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def run_reference(args):
+    world, rank, local = _dist()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from elsa_b200 import phantoms
+    O.build()
+    vol = tuple(WORKLOAD["volume"])
+    poses, det = O.circle_trajectory(vol, WORKLOAD["views"], 360, WORKLOAD["source_to_center"],
+                                     WORKLOAD["center_to_detector"], WORKLOAD["detector"])
+    x = phantoms.modified_shepp_logan(vol)
+    times = []
+    for i in range(args.warmup + args.steps):
+        gups, dt, cores = cpu_baseline_sample(args.cpu_views, vol, poses, det, x)
+        if i >= args.warmup:
+            times.append(dt)
+    dt = float(np.mean(times))
+    value = 2.0 * np.prod(vol) * args.cpu_views / dt / 1e9
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": "GUPS",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dt * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (modified Shepp-Logan 3D phantom)",
+        "config": dict(WORKLOAD, parallelism="host cores"),
+        "cpu_baseline": {"value": round(value, 5), "unit": "GUPS", "cores": O.num_threads(),
+                         "kind": "port",
+                         "sample": "per step: Joseph forward + adjoint over %d of the 360 views"
+                                   % args.cpu_views},
+        "e2e": {"value": round(value, 5), "unit": "GUPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="elsa_b200", choices=["elsa_b200", "reference"])
+    ap.add_argument("--cpu-views", type=int, default=4,
+                    help="views per CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_elsa(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -7,7 +7,7 @@ does, and fails loudly when the library is missing.
 """
 from . import _capi  # noqa: F401
 from ._capi import (ElsaError, InvalidArgumentError, Projector, circle_trajectory,  # noqa: F401
-                    pose_2d, pose_3d, POSE_FLOATS, PROJECTOR_JOSEPH)
+                    pose_2d, pose_3d, POSE_FLOATS, PROJECTOR_JOSEPH, SOLVER_CGNE, Solver)
 
 __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "circle_trajectory", "pose_2d",
-           "pose_3d", "POSE_FLOATS", "PROJECTOR_JOSEPH"]
+           "pose_3d", "POSE_FLOATS", "PROJECTOR_JOSEPH", "SOLVER_CGNE", "Solver"]

@@ -22,6 +22,7 @@ STATUS_NAMES = {
 }
 
 PROJECTOR_JOSEPH = 0
+SOLVER_CGNE = 0
 
 # Every function the header declares: name -> (restype, argtypes)
 _vp = ctypes.c_void_p
@@ -40,7 +41,7 @@ SIGNATURES = {
                                     ctypes.POINTER(_vp)]),
     "elsa_projector_destroy": (_st, [_vp]),
     "elsa_projector_sizes": (_st, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
-    "elsa_projector_info": (_st, [_vp, _i32, ctypes.POINTER(_i32)]),
+    "elsa_projector_info": (_st, [_vp, _i32, ctypes.POINTER(_i64)]),
     "elsa_projector_apply": (_st, [_vp, _vp, _vp, _vp]),
     "elsa_projector_apply_adjoint": (_st, [_vp, _vp, _vp, _vp]),
     "elsa_projector_apply_host": (_st, [_vp, _vp, _vp]),
@@ -49,6 +50,13 @@ SIGNATURES = {
     "elsa_squared_l2_norm": (_st, [_vp, _i64, _vp, _vp]),
     "elsa_lincomb": (_st, [_f32, _vp, _f32, _vp, _vp, _i64, _vp]),
     "elsa_cgne_solve": (_st, [_vp, _vp, _vp, _i32, _i32, _vp]),
+    "elsa_solver_create": (_st, [_i32, _vp, _vp, _vp, _i32, _vp, ctypes.POINTER(_vp)]),
+    "elsa_solver_iterate": (_st, [_vp, _i32, _vp]),
+    "elsa_solver_squared_residual": (_st, [_vp, _vp, ctypes.POINTER(ctypes.c_double)]),
+    "elsa_solver_enable_timing": (_st, [_vp, _i32]),
+    "elsa_solver_timing": (_st, [_vp, ctypes.POINTER(ctypes.c_double),
+                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i64)]),
+    "elsa_solver_destroy": (_st, [_vp]),
 }
 
 
@@ -165,7 +173,7 @@ class Projector:
         return self._h
 
     def info(self, key):
-        v = ctypes.c_int32()
+        v = ctypes.c_int64()
         call("elsa_projector_info", self._h, int(key), ctypes.byref(v))
         return v.value
 
@@ -196,6 +204,47 @@ class Projector:
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             lib().elsa_projector_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Solver:
+    """Owning handle of an elsa_solver: a device-resident iterative solve on device buffers
+    (b: range, x: domain; both must outlive the solver)."""
+
+    def __init__(self, kind, projector, b_ptr, x_ptr, use_x0=False, stream=None):
+        self._proj = projector  # keep the operator alive
+        h = ctypes.c_void_p()
+        call("elsa_solver_create", int(kind), projector.handle, ctypes.c_void_p(b_ptr),
+             ctypes.c_void_p(x_ptr), int(bool(use_x0)), ctypes.c_void_p(stream or 0),
+             ctypes.byref(h))
+        self._h = h
+
+    def iterate(self, iterations, stream=None):
+        call("elsa_solver_iterate", self._h, int(iterations), ctypes.c_void_p(stream or 0))
+
+    def squared_residual(self, stream=None):
+        v = ctypes.c_double()
+        call("elsa_solver_squared_residual", self._h, ctypes.c_void_p(stream or 0),
+             ctypes.byref(v))
+        return v.value
+
+    def enable_timing(self, on=True):
+        call("elsa_solver_enable_timing", self._h, int(bool(on)))
+
+    def timing(self):
+        f, a, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
+        call("elsa_solver_timing", self._h, ctypes.byref(f), ctypes.byref(a), ctypes.byref(n))
+        return f.value, a.value, n.value
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().elsa_solver_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

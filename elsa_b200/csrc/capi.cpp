@@ -12,6 +12,11 @@
 #include "projector.hpp"
 #include "solvers.hpp"
 
+struct elsa_solver {
+    std::unique_ptr<elsa_b200::SolverSession> impl;
+    int device = 0;
+};
+
 struct elsa_projector {
     std::unique_ptr<elsa_b200::Projector> impl;
     // lazily allocated staging buffers of the host-buffer entry points
@@ -173,7 +178,7 @@ elsa_status elsa_projector_sizes(const elsa_projector* p, int64_t* domain, int64
     });
 }
 
-elsa_status elsa_projector_info(const elsa_projector* p, int32_t key, int32_t* value)
+elsa_status elsa_projector_info(const elsa_projector* p, int32_t key, int64_t* value)
 {
     return guarded([&] {
         require(p && value, "elsa_projector_info: null argument");
@@ -275,6 +280,64 @@ elsa_status elsa_cgne_solve(elsa_projector* p, const float* b, float* x, int32_t
         elsa_b200::cgneSolve(*p->impl, b, x, iterations, useX0 != 0, ws, asStream(stream));
         ELSA_CUDA(cudaStreamSynchronize(asStream(stream)));
     });
+}
+
+elsa_status elsa_solver_create(int32_t kind, elsa_projector* p, const float* b, float* x,
+                               int32_t useX0, void* stream, elsa_solver** out)
+{
+    return guarded([&] {
+        require(out != nullptr, "elsa_solver_create: null output handle");
+        *out = nullptr;
+        require(p && b && x, "elsa_solver_create: null argument");
+        require(kind == ELSA_SOLVER_CGNE, "elsa_solver_create: unknown solver kind");
+        onDevice(p);
+        auto h = std::make_unique<elsa_solver>();
+        h->device = p->impl->device();
+        h->impl = std::make_unique<elsa_b200::SolverSession>(
+            static_cast<elsa_b200::SolverKind>(kind), *p->impl, b, x, useX0 != 0,
+            asStream(stream));
+        *out = h.release();
+    });
+}
+
+elsa_status elsa_solver_iterate(elsa_solver* s, int32_t iterations, void* stream)
+{
+    return guarded([&] {
+        require(s && iterations >= 0, "elsa_solver_iterate: invalid argument");
+        ELSA_CUDA(cudaSetDevice(s->device));
+        s->impl->iterate(iterations, asStream(stream));
+    });
+}
+
+elsa_status elsa_solver_squared_residual(elsa_solver* s, void* stream, double* value)
+{
+    return guarded([&] {
+        require(s && value, "elsa_solver_squared_residual: null argument");
+        ELSA_CUDA(cudaSetDevice(s->device));
+        *value = s->impl->squaredResidual(asStream(stream));
+    });
+}
+
+elsa_status elsa_solver_enable_timing(elsa_solver* s, int32_t enable)
+{
+    return guarded([&] {
+        require(s != nullptr, "elsa_solver_enable_timing: null argument");
+        s->impl->timer().enable(enable != 0);
+    });
+}
+
+elsa_status elsa_solver_timing(elsa_solver* s, double* fwd, double* adj, int64_t* count)
+{
+    return guarded([&] {
+        require(s && fwd && adj && count, "elsa_solver_timing: null argument");
+        ELSA_CUDA(cudaSetDevice(s->device));
+        s->impl->timer().collect(*fwd, *adj, *count);
+    });
+}
+
+elsa_status elsa_solver_destroy(elsa_solver* s)
+{
+    return guarded([&] { delete s; });
 }
 
 } // extern "C"

@@ -32,7 +32,7 @@ namespace elsa_b200
         int device() const { return device_; }
         int kind() const { return kind_; }
         // Tunables reported for diagnostics (e.g. the conflict-free ray class spacing).
-        virtual int info(int key) const { (void)key; return -1; }
+        virtual int64_t info(int key) const { (void)key; return -1; }
 
     protected:
         Projector(int kind, const VolumeShape& vol, const DetectorShape& det,

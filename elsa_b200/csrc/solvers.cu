@@ -45,9 +45,50 @@ namespace elsa_b200
     {
     }
 
+    KernelTimer::~KernelTimer()
+    {
+        for (auto e : pending_)
+            cudaEventDestroy(e);
+        for (auto e : pool_)
+            cudaEventDestroy(e);
+    }
+
+    void KernelTimer::mark(cudaStream_t s)
+    {
+        if (!enabled_)
+            return;
+        cudaEvent_t e;
+        if (!pool_.empty()) {
+            e = pool_.back();
+            pool_.pop_back();
+        } else {
+            ELSA_CUDA(cudaEventCreate(&e));
+        }
+        ELSA_CUDA(cudaEventRecord(e, s));
+        pending_.push_back(e);
+    }
+
+    void KernelTimer::collect(double& fwdMs, double& adjMs, int64_t& count)
+    {
+        for (size_t i = 0; i + 2 < pending_.size(); i += 3) {
+            ELSA_CUDA(cudaEventSynchronize(pending_[i + 2]));
+            float a = 0, b = 0;
+            ELSA_CUDA(cudaEventElapsedTime(&a, pending_[i], pending_[i + 1]));
+            ELSA_CUDA(cudaEventElapsedTime(&b, pending_[i + 1], pending_[i + 2]));
+            fwdMs_ += a;
+            adjMs_ += b;
+            ++count_;
+        }
+        pool_.insert(pool_.end(), pending_.begin(), pending_.end());
+        pending_.clear();
+        fwdMs = fwdMs_;
+        adjMs = adjMs_;
+        count = count_;
+    }
+
     // CGNE: CG on the normal equations A^T A x = A^T b, solvers/CGNE.cpp:20-78.
-    void cgneSolve(Projector& A, const float* b, float* x, int iterations, bool useX0,
-                   SolverWorkspace& ws, cudaStream_t s)
+    static void cgneBegin(Projector& A, const float* b, float* x, bool useX0,
+                          SolverWorkspace& ws, cudaStream_t s)
     {
         const int64_t n = A.domainSize();
         float* r = ws.vol0.as<float>();
@@ -57,7 +98,6 @@ namespace elsa_b200
         double* partials = ws.partials.as<double>();
         SolverScalars* S = ws.scalars.as<SolverScalars>();
         ELSA_CUDA(cudaMemsetAsync(S, 0, sizeof(SolverScalars), s));
-
         A.adjoint(b, r, s); // A^T b
         if (useX0) {
             A.forward(x, sino, s);
@@ -68,19 +108,66 @@ namespace elsa_b200
         }
         ELSA_CUDA(cudaMemcpyAsync(c, r, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
         launchSquaredNorm(r, n, partials, &S->kold, s);
-        for (int it = 0; it < iterations; ++it)
-            cgneIteration(A, x, r, c, q, sino, partials, S, s);
     }
 
-    void cgneIteration(Projector& A, float* x, float* r, float* c, float* q, float* sino,
-                       double* partials, SolverScalars* S, cudaStream_t s)
+    static void cgneStep(Projector& A, float* x, SolverWorkspace& ws, KernelTimer& t,
+                         cudaStream_t s)
     {
         const int64_t n = A.domainSize();
+        float* r = ws.vol0.as<float>();
+        float* c = ws.vol1.as<float>();
+        float* q = ws.vol2.as<float>();
+        float* sino = ws.sino0.as<float>();
+        double* partials = ws.partials.as<double>();
+        SolverScalars* S = ws.scalars.as<SolverScalars>();
+        t.mark(s);
         A.forward(c, sino, s);
-        A.adjoint(sino, q, s);                         // q = A^T A c
-        launchDot(c, q, n, partials, &S->den, s);      // <c, A^T A c>
-        launchCgStep(x, r, c, q, n, S, partials, s);   // x += a c, r -= a q, |r|^2 partials
-        launchCgFinishNorm(partials, S, s);            // k, beta = k/kold, kold = k
-        launchCgDirection(r, c, n, S, s);              // c = r + beta c
+        t.mark(s);
+        A.adjoint(sino, q, s); // q = A^T A c
+        t.mark(s);
+        launchDot(c, q, n, partials, &S->den, s);    // <c, A^T A c>
+        launchCgStep(x, r, c, q, n, S, partials, s); // x += a c, r -= a q, |r|^2 partials
+        launchCgFinishNorm(partials, S, s);          // k, beta = k/kold, kold = k
+        launchCgDirection(r, c, n, S, s);            // c = r + beta c
+    }
+
+    void cgneSolve(Projector& A, const float* b, float* x, int iterations, bool useX0,
+                   SolverWorkspace& ws, cudaStream_t s)
+    {
+        KernelTimer off;
+        cgneBegin(A, b, x, useX0, ws, s);
+        for (int it = 0; it < iterations; ++it)
+            cgneStep(A, x, ws, off, s);
+    }
+
+    SolverSession::SolverSession(SolverKind kind, Projector& A, const float* b, float* x,
+                                 bool useX0, cudaStream_t s)
+        : kind_(kind), A_(A), b_(b), x_(x), ws_(A.domainSize(), A.rangeSize())
+    {
+        switch (kind_) {
+        case SolverKind::CGNE:
+            cgneBegin(A_, b_, x_, useX0, ws_, s);
+            break;
+        }
+    }
+
+    void SolverSession::iterate(int iterations, cudaStream_t s)
+    {
+        for (int it = 0; it < iterations; ++it) {
+            switch (kind_) {
+            case SolverKind::CGNE:
+                cgneStep(A_, x_, ws_, timer_, s);
+                break;
+            }
+        }
+    }
+
+    double SolverSession::squaredResidual(cudaStream_t s)
+    {
+        SolverScalars h;
+        ELSA_CUDA(cudaMemcpyAsync(&h, ws_.scalars.as<SolverScalars>(), sizeof(h),
+                                  cudaMemcpyDeviceToHost, s));
+        ELSA_CUDA(cudaStreamSynchronize(s));
+        return h.kold;
     }
 } // namespace elsa_b200

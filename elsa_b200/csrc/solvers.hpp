@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include "projector.hpp"
 #include "vecops.cuh"
@@ -40,6 +41,48 @@ namespace elsa_b200
 
     void cgneSolve(Projector& A, const float* b, float* x, int iterations, bool useX0,
                    SolverWorkspace& ws, cudaStream_t s);
-    void cgneIteration(Projector& A, float* x, float* r, float* c, float* q, float* sino,
-                       double* partials, SolverScalars* S, cudaStream_t s);
+
+    // CUDA-event timing of the projector kernels inside solver iterations.
+    class KernelTimer
+    {
+    public:
+        ~KernelTimer();
+        void enable(bool on) { enabled_ = on; }
+        bool enabled() const { return enabled_; }
+        // Record a marker on the stream; markers come in (begin, after forward, after adjoint)
+        // triples per timed iteration.
+        void mark(cudaStream_t s);
+        // Synchronize and fold all pending triples into the totals.
+        void collect(double& fwdMs, double& adjMs, int64_t& count);
+
+    private:
+        bool enabled_ = false;
+        std::vector<cudaEvent_t> pending_, pool_;
+        double fwdMs_ = 0.0, adjMs_ = 0.0;
+        int64_t count_ = 0;
+    };
+
+    enum class SolverKind { CGNE = 0 };
+
+    // A solver run split into setup and iterations: begin() computes the initial residual,
+    // iterate() enqueues iterations asynchronously on the stream (capturable in a CUDA graph
+    // when timing is off).
+    class SolverSession
+    {
+    public:
+        SolverSession(SolverKind kind, Projector& A, const float* b, float* x, bool useX0,
+                      cudaStream_t s);
+        void iterate(int iterations, cudaStream_t s);
+        double squaredResidual(cudaStream_t s); // synchronizes
+        KernelTimer& timer() { return timer_; }
+        Projector& op() { return A_; }
+
+    private:
+        SolverKind kind_;
+        Projector& A_;
+        const float* b_;
+        float* x_;
+        SolverWorkspace ws_;
+        KernelTimer timer_;
+    };
 } // namespace elsa_b200

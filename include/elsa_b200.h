@@ -107,8 +107,9 @@ elsa_status elsa_projector_destroy(elsa_projector* projector);
 elsa_status elsa_projector_sizes(const elsa_projector* projector, int64_t* domain_size,
                                  int64_t* range_size);
 
-/* Diagnostics: key 0 = conflict-free ray class spacing of the adjoint, 1 = adjoint bricks. */
-elsa_status elsa_projector_info(const elsa_projector* projector, int32_t key, int32_t* value);
+/* Diagnostics: key 0 = conflict-free ray class spacing of the adjoint, 1 = adjoint bricks,
+ * 2 = samples per forward pass (sum over rays of the Joseph step count). */
+elsa_status elsa_projector_info(const elsa_projector* projector, int32_t key, int64_t* value);
 
 /* y = A x on device buffers. Replaces LinearOperator::apply(x, Ax), core/LinearOperator.cpp:94-98
  * -> XrayProjector::applyImpl -> JosephsMethodCUDA::forward, JosephsMethodCUDA.cpp:132-214. */
@@ -147,6 +148,39 @@ elsa_status elsa_lincomb(float a, const float* x, float b, const float* y, float
 /* ---------------------------------------------------------------------------------------------
  * Solvers (device-resident iterations, float64 inner products)
  * ------------------------------------------------------------------------------------------- */
+
+typedef struct elsa_solver elsa_solver;
+
+typedef enum elsa_solver_kind {
+    /* CGNE<float>, solvers/CGNE.cpp:20-78 */
+    ELSA_SOLVER_CGNE = 0
+} elsa_solver_kind;
+
+/* Set up a solver run: allocate its scratch, compute the initial residual (x is zeroed unless
+ * use_x0 != 0). b (range) and x (domain) are device buffers that must stay valid until
+ * elsa_solver_destroy; x holds the current iterate. The constructor + first half of
+ * Solver::solve(iterations, x0), solvers/Solver.h:21-43 and solvers/CGNE.cpp:20-47. */
+elsa_status elsa_solver_create(int32_t kind, elsa_projector* projector, const float* b, float* x,
+                               int32_t use_x0, void* stream, elsa_solver** out);
+
+/* Enqueue `iterations` iterations on the stream without synchronizing (the loop body of
+ * CGNE::solve, solvers/CGNE.cpp:50-73). All scalars stay in device memory, so the enqueued
+ * work can be captured in a CUDA graph when timing is disabled. */
+elsa_status elsa_solver_iterate(elsa_solver* solver, int32_t iterations, void* stream);
+
+/* Squared residual norm |r|^2 of the current iterate (float64, synchronizes the stream). */
+elsa_status elsa_solver_squared_residual(elsa_solver* solver, void* stream, double* value);
+
+/* Record CUDA events around the forward and adjoint projections of every iteration
+ * (elsa's Timer around each apply, logging/Timer.h:25-38). */
+elsa_status elsa_solver_enable_timing(elsa_solver* solver, int32_t enable);
+
+/* Synchronize and return the total forward / adjoint milliseconds and the number of timed
+ * iterations since timing was enabled. */
+elsa_status elsa_solver_timing(elsa_solver* solver, double* forward_ms, double* adjoint_ms,
+                               int64_t* iterations);
+
+elsa_status elsa_solver_destroy(elsa_solver* solver);
 
 /* CG on the normal equations A^T A x = A^T b. x: device volume buffer, used as the start value
  * when use_x0 != 0 and overwritten with the solution. Replaces CGNE<float>(A, b).solve(

@@ -1,0 +1,121 @@
+"""Known-answer cases re-expressed from elsa's own projector tests.
+
+Each case gives the geometry (pose records built with the oracle's restatement of
+core/Geometry.cpp), an input volume with the expected forward projection, and a sinogram with the
+expected backprojection. Values are closed-form and come from the cited reference tests.
+Volumes are numpy arrays indexed [z, y, x] / [y, x] (x fastest), as elsa's DataContainer(x, y, z).
+"""
+import math
+
+import numpy as np
+
+PI_F = float(np.float32(math.pi))
+SQ3 = math.sqrt(3.0)
+
+
+def _rad(deg):
+    # Degree{d}.to_radian() = d * pi_t / 180 in float (core/StrongTypes.h:60)
+    return float(np.float32(np.float32(deg) * np.float32(PI_F)) / np.float32(180))
+
+
+def _pose2d(O, vol_dims, det_u, s2c, c2d, angle, cor=(0.0, 0.0)):
+    vo = [0.5 * v for v in vol_dims]
+    return O.geometry2d(s2c, c2d, angle, [1, 1], vo, [1, 1], [0.5 * det_u, 0.5], 0.0, cor)
+
+
+def _pose3d(O, vol_dims, det_uv, num_poses, s2c, c2d, gamma, beta=0.0, cor=(0.0, 0.0, 0.0)):
+    vo = [0.5 * v for v in vol_dims]
+    so = [0.5 * det_uv[0], 0.5 * det_uv[1]]
+    return O.geometry3d(s2c, c2d, [1, 1, 1], vo, [1, 1], so, gamma, beta, 0.0, [0.0, 0.0], cor)
+
+
+def joseph_cases(O):
+    """projectors/tests/test_JosephsMethod.cpp"""
+    cases = []
+    # :17-204 single ray through a 5x5 volume of ones at 0/180/90/270 degrees
+    for deg, axis in ((0, "col"), (180, "col"), (90, "row"), (270, "row")):
+        poses = _pose2d(O, (5, 5), 1, 100.0, 5.0, _rad(deg))[None]
+        x = np.ones((5, 5), np.float32)
+        bp = np.zeros((5, 5), np.float32)
+        if axis == "col":
+            bp[:, 2] = 5
+        else:
+            bp[2, :] = 5
+        cases.append(dict(name="joseph_single_ray_%d" % deg, vol=(5, 5), det=(1, 1),
+                          poses=poses, x=x, y_expect=np.array([5.0]), y=np.array([5.0]),
+                          bp_expect=bp))
+    # :1151-1214 x-, y- and z-axis aligned rays through a 3^3 volume
+    beta = [0.0, 0.0, 0.0, 0.0, PI_F / 2, 3 * PI_F / 2]
+    gamma = [0.0, PI_F, PI_F / 2, 3 * PI_F / 2, PI_F / 2, 3 * PI_F / 2]
+    poses = np.stack([_pose3d(O, (3, 3, 3), (1, 1), 6, 60.0, 3.0, float(np.float32(g)),
+                              float(np.float32(b))) for g, b in zip(gamma, beta)])
+    x = np.zeros((3, 3, 3), np.float32)
+    for i in range(3):
+        x[1, 1, i] = 1
+        x[1, i, 1] = 1
+        x[i, 1, 1] = 1
+    bp = np.array([0, 0, 0, 0, 6, 0, 0, 0, 0, 0, 6, 0, 6, 18, 6, 0, 6, 0, 0, 0, 0, 0, 6, 0, 0, 0,
+                   0], np.float32).reshape(3, 3, 3)
+    cases.append(dict(name="joseph_axis_aligned_3d", vol=(3, 3, 3), det=(1, 1, 6), poses=poses,
+                      x=x, y_expect=np.full(6, 3.0), y=np.full(6, 3.0), bp_expect=bp))
+    # :1217-1270 non-cubic volume 5x1x2, ray through the shorter dimension
+    poses = _pose3d(O, (5, 1, 2), (1, 1), 1, 100.0, 5.0, 0.0, 0.0, (1.6, 0.0, 0.0))[None]
+    x = np.zeros((2, 1, 5), np.float32)
+    x[0, 0, 4] = 1
+    x[1, 0, 4] = 1
+    bp = np.zeros((2, 1, 5), np.float32)
+    bp[0, 0, 4] = bp[1, 0, 4] = 0.6
+    bp[0, 0, 3] = bp[1, 0, 3] = 0.4
+    cases.append(dict(name="joseph_non_cubic", vol=(5, 1, 2), det=(1, 1, 1), poses=poses, x=x,
+                      y_expect=np.array([1.2]), y=np.array([1.0]), bp_expect=bp))
+    # :1273-1348 30 degree ray through the centre of a 4x4 volume
+    poses = _pose2d(O, (4, 4), 1, 80.0, 4.0, -PI_F / 6)[None]
+    w = 2 / math.sqrt(3.0)
+    x = np.zeros((4, 4), np.float32)
+    for (i, j) in ((3, 0), (1, 1), (1, 2), (1, 3)):
+        x[j, i] = 1
+    exp = np.array([0, 0, (3 - SQ3) / 2, (SQ3 - 1) / 2, 0, (SQ3 - 1) / (2 * SQ3),
+                    (SQ3 + 1) / (2 * SQ3), 0, 0, (SQ3 + 1) / (2 * SQ3), (SQ3 - 1) / (2 * SQ3), 0,
+                    (SQ3 - 1) / 2, (3 - SQ3) / 2, 0, 0]) * w
+    cases.append(dict(name="joseph_30deg_center", vol=(4, 4), det=(1, 1), poses=poses, x=x,
+                      y_expect=np.array([2 * w]), y=np.array([1.0]),
+                      bp_expect=exp.reshape(4, 4)))
+    # :1350-1390 30 degree ray through a single pixel
+    poses = _pose2d(O, (4, 4), 1, 80.0, 4.0, -PI_F / 6, (-2 - SQ3 / 2, 0.0))[None]
+    x = np.zeros((4, 4), np.float32)
+    x[0, 0] = 1
+    bp = np.zeros((4, 4), np.float32)
+    bp[0, 0] = 1 / SQ3
+    cases.append(dict(name="joseph_30deg_single_pixel", vol=(4, 4), det=(1, 1), poses=poses, x=x,
+                      y_expect=np.array([1 / SQ3]), y=np.array([1.0]), bp_expect=bp,
+                      tol=1e-4))
+    return cases
+
+
+def siddon_cases(O):
+    """projectors/tests/test_SiddonsMethod.cpp"""
+    cases = []
+    # :1166-1227 30 degree ray through the centre of a 4x4 volume
+    poses = _pose2d(O, (4, 4), 1, 80.0, 4.0, -PI_F / 6)[None]
+    x = np.zeros((4, 4), np.float32)
+    x[0, 3], x[0, 2], x[1, 2] = 1, 2, 3
+    exp = np.array([0, 0, 2 - 2 / SQ3, 4 / SQ3 - 2, 0, 0, 2 / SQ3, 0, 0, 2 / SQ3, 0, 0,
+                    4 / SQ3 - 2, 2 - 2 / SQ3, 0, 0])
+    cases.append(dict(name="siddon_30deg_center", vol=(4, 4), det=(1, 1), poses=poses, x=x,
+                      y_expect=np.array([2 * SQ3 + 2]), y=np.array([1.0]),
+                      bp_expect=exp.reshape(4, 4)))
+    # :1094-1141 x-, y- and z-axis aligned rays through a 3^3 volume
+    beta = [0.0, 0.0, 0.0, 0.0, PI_F / 2, 3 * PI_F / 2]
+    gamma = [0.0, PI_F, PI_F / 2, 3 * PI_F / 2, PI_F / 2, 3 * PI_F / 2]
+    poses = np.stack([_pose3d(O, (3, 3, 3), (1, 1), 6, 60.0, 3.0, float(np.float32(g)),
+                              float(np.float32(b))) for g, b in zip(gamma, beta)])
+    x = np.zeros((3, 3, 3), np.float32)
+    for i in range(3):
+        x[1, 1, i] = 1
+        x[1, i, 1] = 1
+        x[i, 1, 1] = 1
+    bp = np.array([0, 0, 0, 0, 6, 0, 0, 0, 0, 0, 6, 0, 6, 18, 6, 0, 6, 0, 0, 0, 0, 0, 6, 0, 0, 0,
+                   0], np.float32).reshape(3, 3, 3)
+    cases.append(dict(name="siddon_axis_aligned_3d", vol=(3, 3, 3), det=(1, 1, 6), poses=poses,
+                      x=x, y_expect=np.full(6, 3.0), y=np.full(6, 3.0), bp_expect=bp))
+    return cases
