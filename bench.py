@@ -138,6 +138,17 @@ def _traffic_from_profiles():
         return None
 
 
+def _apply_size(args):
+    """--size N scales the cone-beam problem (N^3 volume, 1.5 N detector, same ratios) for
+    profiling small cases; the default is the 256^3 workload."""
+    if args.size and args.size != 256:
+        n = args.size
+        WORKLOAD.update(volume=[n, n, n], detector=[3 * n // 2, 3 * n // 2],
+                        source_to_center=10 * n, center_to_detector=5 * n // 2,
+                        workload="cone-beam Joseph CGNE, %d^3 volume, 360 views, %dx%d detector"
+                                 % (n, 3 * n // 2, 3 * n // 2))
+
+
 def run_elsa(args):
     import torch
     import elsa_b200
@@ -151,6 +162,7 @@ def run_elsa(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    _apply_size(args)
     vol = tuple(WORKLOAD["volume"])
     poses, det = elsa_b200.circle_trajectory(vol, WORKLOAD["views"], 360,
                                              WORKLOAD["source_to_center"],
@@ -277,6 +289,7 @@ def run_reference(args):
     from oracle import oracle as O
     from elsa_b200 import phantoms
     O.build()
+    _apply_size(args)
     vol = tuple(WORKLOAD["volume"])
     poses, det = O.circle_trajectory(vol, WORKLOAD["views"], 360, WORKLOAD["source_to_center"],
                                      WORKLOAD["center_to_detector"], WORKLOAD["detector"])
@@ -314,6 +327,8 @@ def main():
     ap.add_argument("--cpu-views", type=int, default=4,
                     help="views per CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", type=int, default=256,
+                    help="volume edge (profiling only; the benchmark workload is 256)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

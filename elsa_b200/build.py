@@ -29,6 +29,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall",
 CUDA_UNITS = [
     ("raysetup.cu", ["--fmad=false"]),
     ("joseph.cu", []),
+    ("joseph_tma.cu", []),
     ("vecops.cu", []),
     ("solvers.cu", []),
 ]
@@ -36,7 +37,7 @@ CXX_UNITS = [
     ("geometry.cpp", []),
     ("capi.cpp", []),
 ]
-HEADERS = ["internal.cuh", "raysetup.cuh", "projector.hpp", "geometry.hpp", "vecops.cuh",
+HEADERS = ["internal.cuh", "raysetup.cuh", "joseph_tma.cuh", "projector.hpp", "geometry.hpp", "vecops.cuh",
            "solvers.hpp"]
 
 

@@ -26,6 +26,7 @@
 // bilinear taps never overlap and the threads update shared memory without atomics. Each thread
 // walks one ray through the brick; classes are separated by barriers. Every voxel receives its
 // contributions in a fixed order, with exactly the positions and weights of the forward kernel.
+#include "joseph_tma.cuh"
 #include "projector.hpp"
 #include "raysetup.cuh"
 
@@ -363,8 +364,8 @@ namespace elsa_b200
 
         // One CTA per brick of BX x BY x BZ voxels (BZ = 1 in 2D). The z stride is padded by one
         // word (2D: the y stride) so that threads on neighbouring rays hit distinct banks.
-        template <int DIM, int BX, int BY, int BZ, int CPD>
-        __global__ void __launch_bounds__(256)
+        template <int DIM, int BX, int BY, int BZ, int CPD, int NT>
+        __global__ void __launch_bounds__(NT)
             josephAdjointKernel(const JosephRay* __restrict__ rays,
                                 const float2* __restrict__ checkpoints, int cpStride,
                                 const float* __restrict__ y,
@@ -443,19 +444,19 @@ namespace elsa_b200
             }
         }
 
-        template <int DIM, int BX, int BY, int BZ, int CPD>
+        template <int DIM, int BX, int BY, int BZ, int CPD, int NT>
         struct AdjointConfig {
             static constexpr int kRow = DIM == 3 ? BX : BX + 1;
             static constexpr int kPlane = DIM == 3 ? BX * BY + 1 : kRow * BY;
             static constexpr size_t kSmem = sizeof(float) * kPlane * BZ;
-            static constexpr int kThreads = 256;
+            static constexpr int kThreads = NT;
             static constexpr int kCheckpointDepth = CPD;
             static_assert(BX % CPD == 0 && BY % CPD == 0 && (DIM == 2 || BZ % CPD == 0),
                           "brick edges must be multiples of the checkpoint depth");
             static int3 brick() { return make_int3(BX, BY, BZ); }
             static void prepare()
             {
-                ELSA_CUDA(cudaFuncSetAttribute(josephAdjointKernel<DIM, BX, BY, BZ, CPD>,
+                ELSA_CUDA(cudaFuncSetAttribute(josephAdjointKernel<DIM, BX, BY, BZ, CPD, NT>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(kSmem)));
             }
@@ -464,13 +465,13 @@ namespace elsa_b200
                                const RayWindow* win, const unsigned* axes, VolumeShape vol,
                                DetectorShape det, int m, int3 nb, float* x)
             {
-                josephAdjointKernel<DIM, BX, BY, BZ, CPD><<<nbricks, kThreads, kSmem, s>>>(
+                josephAdjointKernel<DIM, BX, BY, BZ, CPD, NT><<<nbricks, kThreads, kSmem, s>>>(
                     rays, cps, cpStride, y, win, axes, vol, det, m, nb, x);
             }
         };
 
-        using Adjoint3d = AdjointConfig<3, 32, 16, 32, 16>;
-        using Adjoint2d = AdjointConfig<2, 64, 64, 1, 64>;
+        using Adjoint3d = AdjointConfig<3, 16, 32, 16, 16, 128>;
+        using Adjoint2d = AdjointConfig<2, 64, 64, 1, 64, 256>;
 
         class JosephProjector final : public Projector
         {
@@ -539,6 +540,11 @@ namespace elsa_b200
                 josephWindowKernel<<<static_cast<unsigned>((nwin + 255) / 256), 256>>>(
                     dPoses_, vol_, det_, brick_, nBricks_, dWindows_);
                 ELSA_LAUNCH_CHECK("josephWindowKernel");
+                if (vol_.dim == 3) {
+                    std::vector<float> hp(poses_.size() * kPoseFloats);
+                    std::memcpy(hp.data(), poses_.data(), sizeof(float) * hp.size());
+                    tma_ = std::make_unique<JosephForwardTma>(vol_, det_, hp, dRays_);
+                }
                 ELSA_CUDA(cudaDeviceSynchronize());
             }
 
@@ -555,7 +561,9 @@ namespace elsa_b200
                 const int64_t nrays = rangeSize_;
                 const unsigned blocks =
                     static_cast<unsigned>((nrays + kForwardThreads - 1) / kForwardThreads);
-                if (vol_.dim == 3)
+                if (tma_)
+                    tma_->forward(x, y, s);
+                else if (vol_.dim == 3)
                     josephForwardKernel<3><<<blocks, kForwardThreads, 0, s>>>(dRays_, nrays, x,
                                                                                 vol_, y);
                 else
@@ -585,6 +593,10 @@ namespace elsa_b200
                     return nBricks_.x * nBricks_.y * nBricks_.z;
                 case 2:
                     return sampleCount_;
+                case 3: // error word of the TMA forward (synchronizes)
+                    return tma_ ? static_cast<int64_t>(tma_->errorWord()) : 0;
+                case 4: // parts per million of detector tiles on the gather fallback
+                    return tma_ ? static_cast<int64_t>(tma_->fallbackFraction() * 1e6) : -1;
                 default:
                     return -1;
                 }
@@ -598,6 +610,7 @@ namespace elsa_b200
             int cpStride_ = 0;
             int classSpacing_ = 0;
             int64_t sampleCount_ = 0;
+            std::unique_ptr<JosephForwardTma> tma_;
             int3 brick_{}, nBricks_{};
         };
     } // namespace

@@ -108,7 +108,9 @@ elsa_status elsa_projector_sizes(const elsa_projector* projector, int64_t* domai
                                  int64_t* range_size);
 
 /* Diagnostics: key 0 = conflict-free ray class spacing of the adjoint, 1 = adjoint bricks,
- * 2 = samples per forward pass (sum over rays of the Joseph step count). */
+ * 2 = samples per forward pass (sum over rays of the Joseph step count), 3 = error word of the
+ * device pipeline (0 = no timed-out wait; synchronizes), 4 = detector tiles on the gather
+ * fallback of the staged forward, in parts per million. */
 elsa_status elsa_projector_info(const elsa_projector* projector, int32_t key, int64_t* value);
 
 /* y = A x on device buffers. Replaces LinearOperator::apply(x, Ax), core/LinearOperator.cpp:94-98

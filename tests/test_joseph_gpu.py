@@ -68,7 +68,9 @@ def test_joseph_parity(cuda, oracle, name):
     e_fwd, e_adj = rel_l2(Ax, ref_Ax), rel_l2(Aty, ref_Aty)
     # the float64 instantiation of the oracle, for the record
     d_Ax = oracle.joseph(x.astype(np.float64), c["vol"], det, poses, dtype=np.float64)
-    print("%s: fwd %.3g adj %.3g (vs f64 fwd %.3g)" % (name, e_fwd, e_adj, rel_l2(Ax, d_Ax)))
+    print("%s: fwd %.3g adj %.3g (vs f64 fwd %.3g), fallback tiles %d ppm"
+          % (name, e_fwd, e_adj, rel_l2(Ax, d_Ax), proj.info(4)))
+    assert proj.info(3) == 0  # no timed-out pipeline wait
     assert e_fwd <= PARITY
     assert e_adj <= PARITY
 
@@ -86,9 +88,10 @@ def test_joseph_adjointness_and_determinism(cuda, oracle, name):
     lhs = float(Ax.astype(np.float64) @ y)
     rhs = float(x.astype(np.float64) @ Aty)
     assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
-    # atomic-free adjoint: bitwise reproducible
-    _, Aty2 = _gpu_pair(cuda, proj, x, y)
+    # atomic-free adjoint and forward: bitwise reproducible
+    Ax2, Aty2 = _gpu_pair(cuda, proj, x, y)
     assert np.array_equal(Aty.view(np.uint32), Aty2.view(np.uint32))
+    assert np.array_equal(Ax.view(np.uint32), Ax2.view(np.uint32))
 
 
 def test_joseph_host_entry_points(cuda, oracle):
