@@ -252,10 +252,12 @@ namespace elsa_b200
             atomicAdd(samples, static_cast<unsigned long long>(R.n));
             unsigned bad = 0;
             for (int m = kMinClass; m <= kMaxClass; ++m) {
-                const int noffs = dim == 3 ? 4 : 1;
+                // pairs that the adjoint may process concurrently: same row m apart, and rows m
+                // apart with any offset inside a 32-ray segment (plus one)
+                const int noffs = dim == 3 ? 2 + 65 : 1;
                 for (int o = 0; o < noffs; ++o) {
-                    const int du = (o == 1) ? 0 : m;
-                    const int dv = (o == 0) ? 0 : (o == 3 ? -m : m);
+                    const int du = o == 0 ? m : (o == 1 ? 33 : o - 2 - 32);
+                    const int dv = o < 2 ? 0 : m;
                     const int u2 = u + du, v2 = v + dv;
                     if (u2 < 0 || u2 >= det.nu || v2 < 0 || v2 >= det.nv)
                         continue;
@@ -272,9 +274,10 @@ namespace elsa_b200
         }
 
         // Exact accumulated position of every ray at its first sample in each driving-axis slab
-        // of `depth` planes (slab index floor(k/depth), visited in ray order).
+        // of `depth` planes. Slab-major layout: row floor(k/depth) + 1, column = ray index, so a
+        // warp of neighbouring rays reads one contiguous run.
         __global__ void josephCheckpointKernel(const JosephRay* __restrict__ rays, int64_t nrays,
-                                               int depth, int stride,
+                                               int depth, int slabRows,
                                                float2* __restrict__ checkpoints)
         {
             const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -284,40 +287,27 @@ namespace elsa_b200
             if (R.n == 0)
                 return;
             const int dir = (R.meta & 4) ? -1 : 1;
-            const int first = floorDiv(R.k0, depth);
-            float2* out = checkpoints + r * stride;
             float pa = R.pa, pb = R.pb;
-            int k = R.k0, slab = first - dir;
+            int k = R.k0, slab = floorDiv(R.k0, depth) - dir;
             for (int j = 0; j < R.n; ++j, k += dir) {
                 const int s = floorDiv(k, depth);
                 if (s != slab) {
                     slab = s;
-                    const int idx = (s - first) * dir;
-                    if (idx < stride) // always true: the host sizes stride for N + 1 samples
-                        out[idx] = make_float2(pa, pb);
+                    // rows 0 .. slabRows-1 cover k in [-depth, (slabRows-1)*depth); the host
+                    // sizes slabRows for every sample of an N-plane volume
+                    if (s + 1 >= 0 && s + 1 < slabRows)
+                        checkpoints[(s + 1) * nrays + r] = make_float2(pa, pb);
                 }
                 pa = __fadd_rn(pa, R.sa);
                 pb = __fadd_rn(pb, R.sb);
             }
         }
 
-        struct PassGeom {
-            int extG, extA, extB;
-            int orgG, orgA, orgB;
-            int strG, strA, strB;
-        };
-
-        // Walk ray r (one thread) through the brick and add its bilinear splats to the
-        // shared-memory accumulator. Positions start from the slab checkpoint at the ray's first
-        // sample inside the brick and are accumulated exactly as in the forward kernel.
-        template <int DIM, int CPD>
-        __device__ __forceinline__ void splatRay(float* acc, const JosephRay& R, float yl,
-                                                 const float2* __restrict__ cps,
-                                                 const PassGeom& pg)
+        // Sample range [jLo, jHi] of ray R inside driving planes [kLo, kHi]; false if empty.
+        __device__ __forceinline__ bool sampleRange(const JosephRay& R, int kLo, int kHi, int& jLo,
+                                                    int& jHi)
         {
             const int dir = (R.meta & 4) ? -1 : 1;
-            const int kLo = pg.orgG, kHi = pg.orgG + pg.extG - 1;
-            int jLo, jHi;
             if (dir > 0) {
                 jLo = max(0, kLo - R.k0);
                 jHi = min(R.n - 1, kHi - R.k0);
@@ -325,153 +315,516 @@ namespace elsa_b200
                 jLo = max(0, R.k0 - kHi);
                 jHi = min(R.n - 1, R.k0 - kLo);
             }
-            if (jLo > jHi)
-                return;
-            int k = R.k0 + jLo * dir;
-            const int first = floorDiv(R.k0, CPD);
-            const float2 cp = cps[(floorDiv(k, CPD) - first) * dir];
-            float pa = cp.x, pb = cp.y;
-            float* plane = acc + (k - pg.orgG) * pg.strG;
-            const int dPlane = dir * pg.strG;
-            for (int j = jLo; j <= jHi; ++j, plane += dPlane, pa = __fadd_rn(pa, R.sa),
-                     pb = __fadd_rn(pb, R.sb)) {
-                Weights w;
-                tapWeights(pa, pb, w);
-                const int ia = w.ia - pg.orgA;
-                const bool a0 = static_cast<unsigned>(ia) < static_cast<unsigned>(pg.extA);
-                const bool a1 = static_cast<unsigned>(ia + 1) < static_cast<unsigned>(pg.extA);
-                if (DIM == 2) {
-                    if (a0)
-                        plane[ia * pg.strA] += yl * w.wa;
-                    if (a1)
-                        plane[(ia + 1) * pg.strA] += yl * w.cwa;
-                } else {
-                    const int ib = w.ib - pg.orgB;
-                    const bool b0 = static_cast<unsigned>(ib) < static_cast<unsigned>(pg.extB);
-                    const bool b1 = static_cast<unsigned>(ib + 1) < static_cast<unsigned>(pg.extB);
-                    float* q = plane + ia * pg.strA + ib * pg.strB;
-                    if (a0 && b0)
-                        q[0] += yl * (w.wa * w.wb);
-                    if (a1 && b0)
-                        q[pg.strA] += yl * (w.cwa * w.wb);
-                    if (a0 && b1)
-                        q[pg.strB] += yl * (w.wa * w.cwb);
-                    if (a1 && b1)
-                        q[pg.strA + pg.strB] += yl * (w.cwa * w.cwb);
+            return jLo <= jHi;
+        }
+
+        // Strides of the shared-memory brick (x fastest; the plane stride is padded by one word
+        // so that neighbouring rays stepping along z or x hit different banks).
+        template <int DIM, int BX, int BY>
+        struct BrickLayout {
+            static constexpr int kRow = DIM == 3 ? BX : BX + 1;
+            static constexpr int kPlane = DIM == 3 ? BX * BY + 1 : kRow * BY;
+        };
+
+        // Axis roles for driving axis G: stride/extent of G and of the non-driving axes a < b.
+        template <int DIM, int G, int BX, int BY, int BZ>
+        struct AxisRoles {
+            using L = BrickLayout<DIM, BX, BY>;
+            static constexpr int strG = G == 0 ? 1 : (G == 1 ? L::kRow : L::kPlane);
+            static constexpr int extG = G == 0 ? BX : (G == 1 ? BY : BZ);
+            static constexpr int strA = G == 0 ? L::kRow : 1;
+            static constexpr int extA = G == 0 ? BY : BX;
+            static constexpr int strB = DIM == 2 ? 0 : (G == 2 ? L::kRow : L::kPlane);
+            static constexpr int extB = DIM == 2 ? 1 : (G == 2 ? BY : BZ);
+        };
+
+        // Add to the brick word at local lane-axis column L, row-axis row O (if inside).
+        template <int EXT_L, int EXT_O, int STR_L, int STR_O>
+        __device__ __forceinline__ void addTap(float* plane, int L, int O, float v)
+        {
+            if (static_cast<unsigned>(L) < static_cast<unsigned>(EXT_L) &&
+                static_cast<unsigned>(O) < static_cast<unsigned>(EXT_O)) {
+                float* q = plane + L * STR_L + O * STR_O;
+                *q = *q + v;
+            }
+        }
+
+        // One warp splats 32 neighbouring rays (u = uSeg0 + lane) of detector row v through the
+        // brick, plane by plane in ray order. Lanes spread along the "lane axis" (a, or b when
+        // LB); taps landing in the same column are merged across neighbouring lanes, then the
+        // first and the second column of every lane's bilinear footprint are written in two
+        // separate phases, so no two lanes touch the same word at the same time. When the merge
+        // precondition fails (two neighbours on one column but different rows, or three on one
+        // column) the plane falls back to m phases of lanes m apart, which the class check proves
+        // disjoint.
+        template <int DIM, int G, bool LB, int BX, int BY, int BZ, int CPD>
+        __device__ __forceinline__ void splatRowSegment(
+            float* acc, const JosephRay* __restrict__ rays, const float2* __restrict__ cps,
+            int64_t nrays, const float* __restrict__ y, const DetectorShape& det, int p, int v,
+            int uSeg0, int u1, int m, int orgG, int orgA, int orgB)
+        {
+            using AR = AxisRoles<DIM, G, BX, BY, BZ>;
+            constexpr int EXT_L = LB ? AR::extB : AR::extA;
+            constexpr int EXT_O = LB ? AR::extA : AR::extB;
+            constexpr int STR_L = LB ? AR::strB : AR::strA;
+            constexpr int STR_O = LB ? AR::strA : AR::strB;
+            const int lane = threadIdx.x & 31;
+            const int u = uSeg0 + lane;
+            const int kLo = orgG, kHi = orgG + AR::extG - 1;
+            const int64_t r =
+                u + static_cast<int64_t>(det.nu) * (v + static_cast<int64_t>(det.nv) * p);
+            JosephRay R{};
+            bool act = u <= u1;
+            if (act)
+                R = rays[r];
+            act = act && R.n > 0 && (R.meta & 3) == G;
+            int jLo = 0, jHi = -1;
+            if (act)
+                act = sampleRange(R, kLo, kHi, jLo, jHi);
+            const int dir = (R.meta & 4) ? -1 : 1;
+            float pa = 0.0f, pb = 0.0f, yl = 0.0f;
+            if (act) {
+                const int kFirst = R.k0 + jLo * dir;
+                const float2 cp = __ldg(cps + (floorDiv(kFirst, CPD) + 1) * nrays + r);
+                pa = cp.x, pb = cp.y;
+                yl = __ldg(y + r) * R.len;
+            }
+            for (int dsel = 1; dsel >= -1; dsel -= 2) {
+                const bool part = act && dir == dsel;
+                if (!__any_sync(0xffffffffu, part))
+                    continue;
+                // plane offsets t in ray order: k = kLo + t (dir > 0) or kHi - t (dir < 0)
+                const int kFirst = R.k0 + jLo * dir;
+                const int t0 = part ? (dsel > 0 ? kFirst - kLo : kHi - kFirst) : (1 << 20);
+                const int t1 = part ? t0 + (jHi - jLo) : -1;
+                int tMin = t0, tMax = t1;
+                for (int o = 16; o > 0; o >>= 1) {
+                    tMin = min(tMin, __shfl_xor_sync(0xffffffffu, tMin, o));
+                    tMax = max(tMax, __shfl_xor_sync(0xffffffffu, tMax, o));
+                }
+                for (int t = tMin; t <= tMax; ++t) {
+                    const bool on = part && t >= t0 && t <= t1;
+                    const int k = dsel > 0 ? kLo + t : kHi - t;
+                    float* plane = acc + (k - orgG) * AR::strG;
+                    int L = 0, O = 0;
+                    float A = 0.0f, B = 0.0f, C = 0.0f, D = 0.0f;
+                    if (on) {
+                        Weights w;
+                        tapWeights(pa, pb, w);
+                        const int la = w.ia - orgA, lb = w.ib - orgB;
+                        L = LB ? lb : la;
+                        O = DIM == 2 ? 0 : (LB ? la : lb);
+                        const float wl0 = LB ? w.wb : w.wa, wl1 = LB ? w.cwb : w.cwa;
+                        const float wo0 = LB ? w.wa : w.wb, wo1 = LB ? w.cwa : w.cwb;
+                        if (DIM == 2) {
+                            A = yl * wl0;
+                            B = yl * wl1;
+                        } else {
+                            A = yl * (wl0 * wo0);
+                            B = yl * (wl1 * wo0);
+                            C = yl * (wl0 * wo1);
+                            D = yl * (wl1 * wo1);
+                        }
+                        pa = __fadd_rn(pa, R.sa);
+                        pb = __fadd_rn(pb, R.sb);
+                    }
+                    // neighbour state packed in one word: bit 0 active, bits 1.. column + 2^20
+                    const int packed = on ? (((L + (1 << 20)) << 1) | 1) : 0;
+                    const int prev = __shfl_up_sync(0xffffffffu, packed, 1);
+                    const int prev2 = __shfl_up_sync(0xffffffffu, packed, 2);
+                    const bool pOn = lane > 0 && (prev & 1);
+                    const int pL = (prev >> 1) - (1 << 20);
+                    const bool p2On = lane > 1 && (prev2 & 1);
+                    const int p2L = (prev2 >> 1) - (1 << 20);
+                    const bool second = on && pOn && pL == L; // second ray on this column
+                    // columns must be monotone along the active lanes and hold at most two rays
+                    const bool inc = __any_sync(0xffffffffu, on && pOn && pL < L);
+                    const bool dec = __any_sync(0xffffffffu, on && pOn && pL > L);
+                    const bool triple = __any_sync(0xffffffffu, second && p2On && p2L == L);
+                    if (!(inc && dec) && !triple) {
+                        // first rays of distinct columns, then second rays: within one phase
+                        // all writers sit on distinct columns
+#pragma unroll
+                        for (int ph = 0; ph < 4; ++ph) {
+                            const bool mine = on && (second == (ph >= 2));
+                            const int col = L + (ph & 1);
+                            if (mine) {
+                                addTap<EXT_L, EXT_O, STR_L, STR_O>(plane, col, O, (ph & 1) ? B : A);
+                                if (DIM == 3)
+                                    addTap<EXT_L, EXT_O, STR_L, STR_O>(plane, col, O + 1,
+                                                                       (ph & 1) ? D : C);
+                            }
+                            __syncwarp();
+                        }
+                    } else {
+                        for (int ph = 0; ph < m; ++ph) {
+                            if (on && lane % m == ph) {
+                                addTap<EXT_L, EXT_O, STR_L, STR_O>(plane, L, O, A);
+                                addTap<EXT_L, EXT_O, STR_L, STR_O>(plane, L + 1, O, B);
+                                if (DIM == 3) {
+                                    addTap<EXT_L, EXT_O, STR_L, STR_O>(plane, L, O + 1, C);
+                                    addTap<EXT_L, EXT_O, STR_L, STR_O>(plane, L + 1, O + 1, D);
+                                }
+                            }
+                            __syncwarp();
+                        }
+                    }
                 }
             }
         }
 
-        // One CTA per brick of BX x BY x BZ voxels (BZ = 1 in 2D). The z stride is padded by one
-        // word (2D: the y stride) so that threads on neighbouring rays hit distinct banks.
-        template <int DIM, int BX, int BY, int BZ, int CPD, int NT>
-        __global__ void __launch_bounds__(NT)
+        // All row segments of one (view, driving axis G) for a brick. Warps take (row, 32-ray
+        // segment) units; units that run concurrently are rows at least m apart or segments
+        // separated by a whole segment, so their taps are disjoint. Phases end with barriers.
+        template <int DIM, int G, bool LB, int BX, int BY, int BZ, int CPD, int NW>
+        __device__ __forceinline__ void splatView(float* acc, const RayWindow& w, int p,
+                                                  const JosephRay* __restrict__ rays,
+                                                  const float2* __restrict__ cps, int64_t nrays,
+                                                  const float* __restrict__ y,
+                                                  const DetectorShape& det, int m, int org0,
+                                                  int org1, int org2)
+        {
+            const int orgG = G == 0 ? org0 : (G == 1 ? org1 : org2);
+            const int orgA = G == 0 ? org1 : org0;
+            const int orgB = DIM == 2 ? 0 : (G == 2 ? org1 : org2);
+            const int warp = threadIdx.x >> 5;
+            const int nseg = (w.u1 - w.u0) / 32 + 1;
+            const int rowPhases = DIM == 3 ? m : 1;
+            for (int pr = 0; pr < rowPhases; ++pr) {
+                const int vFirst = w.v0 + pr;
+                const int nRows = DIM == 3 ? (vFirst <= w.v1 ? (w.v1 - vFirst) / m + 1 : 0) : 1;
+                for (int ps = 0; ps < 2 && ps < nseg; ++ps) {
+                    const int nSegs = (nseg - ps + 1) / 2;
+                    const int units = nRows * nSegs;
+                    for (int unit = warp; unit < units; unit += NW) {
+                        const int row = unit / nSegs, seg = unit - row * nSegs;
+                        const int v = DIM == 3 ? vFirst + row * m : 0;
+                        splatRowSegment<DIM, G, LB, BX, BY, BZ, CPD>(
+                            acc, rays, cps, nrays, y, det, p, v, w.u0 + 32 * (ps + 2 * seg),
+                            w.u1, m, orgG, orgA, orgB);
+                    }
+                    __syncthreads();
+                }
+            }
+        }
+
+        // One CTA per brick of BX x BY x BZ voxels (BZ = 1 in 2D), NW warps. The brick
+        // accumulates every view in a fixed order and is written once.
+        template <int DIM, int BX, int BY, int BZ, int CPD, int NW>
+        __global__ void __launch_bounds__(NW * 32)
             josephAdjointKernel(const JosephRay* __restrict__ rays,
-                                const float2* __restrict__ checkpoints, int cpStride,
+                                const float2* __restrict__ checkpoints, int64_t nrays,
                                 const float* __restrict__ y,
                                 const RayWindow* __restrict__ windows,
                                 const unsigned* __restrict__ viewAxes, VolumeShape vol,
                                 DetectorShape det, int m, int3 nBricks, float* __restrict__ x)
         {
-            extern __shared__ float acc[];
-            constexpr int kRow = DIM == 3 ? BX : BX + 1;
-            constexpr int kPlane = DIM == 3 ? BX * BY + 1 : kRow * BY;
-            constexpr int kWords = kPlane * BZ;
-            for (int i = threadIdx.x; i < kWords; i += blockDim.x)
-                acc[i] = 0.0f;
+            extern __shared__ float smem[];
+            using L = BrickLayout<DIM, BX, BY>;
+            constexpr int NT = NW * 32;
+            constexpr int kWords = L::kPlane * BZ;
+            float* acc = smem;
+            RayWindow* win = reinterpret_cast<RayWindow*>(smem + ((kWords + 3) & ~3));
+            unsigned* axes = reinterpret_cast<unsigned*>(win + det.np);
             const int bi = blockIdx.x;
             const int org0 = (bi % nBricks.x) * BX, org1 = ((bi / nBricks.x) % nBricks.y) * BY,
                       org2 = (bi / (nBricks.x * nBricks.y)) * BZ;
             const int nb = nBricks.x * nBricks.y * nBricks.z;
+            for (int i = threadIdx.x; i < kWords; i += NT)
+                acc[i] = 0.0f;
+            for (int p = threadIdx.x; p < det.np; p += NT) {
+                const RayWindow w = windows[static_cast<int64_t>(p) * nb + bi];
+                win[p] = w;
+                axes[p] = (w.u0 > w.u1 || w.v0 > w.v1) ? 0u : viewAxes[p];
+            }
             __syncthreads();
             for (int p = 0; p < det.np; ++p) {
-                const RayWindow w = windows[static_cast<int64_t>(p) * nb + bi];
-                if (w.u0 > w.u1 || w.v0 > w.v1)
+                const unsigned ax = axes[p];
+                if (!(ax & 7u))
                     continue;
-                const unsigned axes = viewAxes[p];
-                for (int g = 0; g < DIM; ++g) {
-                    if (!((axes >> g) & 1u))
-                        continue;
-                    // axis g is driving; (a, b) are the remaining axes in increasing order
-                    PassGeom pg;
-                    if (g == 0) {
-                        pg.extG = BX, pg.orgG = org0, pg.strG = 1;
-                        pg.extA = BY, pg.orgA = org1, pg.strA = kRow;
-                        pg.extB = BZ, pg.orgB = org2, pg.strB = kPlane;
-                    } else if (g == 1) {
-                        pg.extG = BY, pg.orgG = org1, pg.strG = kRow;
-                        pg.extA = BX, pg.orgA = org0, pg.strA = 1;
-                        pg.extB = BZ, pg.orgB = org2, pg.strB = kPlane;
-                    } else {
-                        pg.extG = BZ, pg.orgG = org2, pg.strG = kPlane;
-                        pg.extA = BX, pg.orgA = org0, pg.strA = 1;
-                        pg.extB = BY, pg.orgB = org1, pg.strB = kRow;
-                    }
-                    if (DIM == 2)
-                        pg.extB = 1, pg.orgB = 0, pg.strB = 0;
-                    const int mv = DIM == 3 ? m : 1;
-                    for (int cv = 0; cv < mv; ++cv) {
-                        const int vStart = w.v0 + ((cv - w.v0 % m) % m + m) % m;
-                        const int nvc =
-                            DIM == 3 ? (vStart <= w.v1 ? (w.v1 - vStart) / m + 1 : 0) : 1;
-                        for (int cu = 0; cu < m; ++cu) {
-                            const int uStart = w.u0 + ((cu - w.u0 % m) % m + m) % m;
-                            const int nuc = uStart <= w.u1 ? (w.u1 - uStart) / m + 1 : 0;
-                            const int total = nuc * nvc;
-                            for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-                                const int u = uStart + (idx % nuc) * m;
-                                const int v = DIM == 3 ? vStart + (idx / nuc) * m : 0;
-                                const int64_t r = u + static_cast<int64_t>(det.nu) *
-                                                          (v + static_cast<int64_t>(det.nv) * p);
-                                const JosephRay R = rays[r];
-                                if (R.n == 0 || (R.meta & 3) != g)
-                                    continue;
-                                splatRay<DIM, CPD>(acc, R, __ldg(y + r) * R.len,
-                                                   checkpoints + r * cpStride, pg);
-                            }
-                            __syncthreads();
-                        }
-                    }
+                const RayWindow w = win[p];
+                // bit g: rays drive along g; bit 4+g: their lanes spread along axis b
+#define ELSA_SPLAT(G_)                                                                            \
+    if (ax & (1u << G_)) {                                                                        \
+        if (ax & (16u << G_))                                                                     \
+            splatView<DIM, G_, true, BX, BY, BZ, CPD, NW>(acc, w, p, rays, checkpoints, nrays, y, \
+                                                          det, m, org0, org1, org2);              \
+        else                                                                                      \
+            splatView<DIM, G_, false, BX, BY, BZ, CPD, NW>(acc, w, p, rays, checkpoints, nrays,   \
+                                                           y, det, m, org0, org1, org2);          \
+    }
+                ELSA_SPLAT(0)
+                ELSA_SPLAT(1)
+                if (DIM == 3) {
+                    ELSA_SPLAT((DIM == 3 ? 2 : 1))
                 }
+#undef ELSA_SPLAT
             }
-            for (int i = threadIdx.x; i < BX * BY * BZ; i += blockDim.x) {
+            for (int i = threadIdx.x; i < BX * BY * BZ; i += NT) {
                 const int lx = i % BX, ly = (i / BX) % BY, lz = i / (BX * BY);
                 const int gx = org0 + lx, gy = org1 + ly, gz = org2 + lz;
                 if (gx < vol.n[0] && gy < vol.n[1] && gz < vol.n[2])
                     x[gx + static_cast<int64_t>(vol.n[0]) *
                                (gy + static_cast<int64_t>(vol.n[1]) * gz)] =
-                        acc[lz * kPlane + ly * kRow + lx];
+                        acc[lz * L::kPlane + ly * L::kRow + lx];
             }
         }
 
-        template <int DIM, int BX, int BY, int BZ, int CPD, int NT>
+        template <int DIM, int BX, int BY, int BZ, int CPD, int NW>
         struct AdjointConfig {
-            static constexpr int kRow = DIM == 3 ? BX : BX + 1;
-            static constexpr int kPlane = DIM == 3 ? BX * BY + 1 : kRow * BY;
-            static constexpr size_t kSmem = sizeof(float) * kPlane * BZ;
-            static constexpr int kThreads = NT;
+            using L = BrickLayout<DIM, BX, BY>;
+            static constexpr size_t kAccBytes = sizeof(float) * ((L::kPlane * BZ + 3) & ~3);
+            static constexpr int kThreads = NW * 32;
             static constexpr int kCheckpointDepth = CPD;
             static_assert(BX % CPD == 0 && BY % CPD == 0 && (DIM == 2 || BZ % CPD == 0),
                           "brick edges must be multiples of the checkpoint depth");
             static int3 brick() { return make_int3(BX, BY, BZ); }
-            static void prepare()
+            // accumulator + per-view windows and axis masks
+            static size_t smemBytes(int np)
             {
-                ELSA_CUDA(cudaFuncSetAttribute(josephAdjointKernel<DIM, BX, BY, BZ, CPD, NT>,
+                return kAccBytes + (sizeof(RayWindow) + sizeof(unsigned)) * np;
+            }
+            static void prepare(int np)
+            {
+                ELSA_CUDA(cudaFuncSetAttribute(josephAdjointKernel<DIM, BX, BY, BZ, CPD, NW>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>(kSmem)));
+                                               static_cast<int>(smemBytes(np))));
             }
             static void launch(int nbricks, cudaStream_t s, const JosephRay* rays,
-                               const float2* cps, int cpStride, const float* y,
+                               const float2* cps, int64_t nrays, const float* y,
                                const RayWindow* win, const unsigned* axes, VolumeShape vol,
                                DetectorShape det, int m, int3 nb, float* x)
             {
-                josephAdjointKernel<DIM, BX, BY, BZ, CPD, NT><<<nbricks, kThreads, kSmem, s>>>(
-                    rays, cps, cpStride, y, win, axes, vol, det, m, nb, x);
+                josephAdjointKernel<DIM, BX, BY, BZ, CPD, NW>
+                    <<<nbricks, kThreads, smemBytes(det.np), s>>>(rays, cps, nrays, y, win, axes,
+                                                                  vol, det, m, nb, x);
             }
         };
 
-        using Adjoint3d = AdjointConfig<3, 16, 32, 16, 16, 128>;
-        using Adjoint2d = AdjointConfig<2, 64, 64, 1, 64, 256>;
+        // Shared-memory brick of one warp: x stride 1, row stride BX + 1, plane stride chosen
+        // congruent to 1 modulo 32, so the 8 x 4 patch of class rays a warp walks at once spreads
+        // over the banks for both x- and z-driving rays.
+        template <int BX, int BY>
+        struct WarpBrick {
+            static constexpr int kRow = BX + 1;
+            static constexpr int kPlaneMin = kRow * BY;
+            static constexpr int kPlane = kPlaneMin + ((33 - kPlaneMin % 32) % 32);
+        };
+
+        template <int G, int BX, int BY, int BZ>
+        struct WarpRoles {
+            using L = WarpBrick<BX, BY>;
+            static constexpr int strG = G == 0 ? 1 : (G == 1 ? L::kRow : L::kPlane);
+            static constexpr int extG = G == 0 ? BX : (G == 1 ? BY : BZ);
+            static constexpr int strA = G == 0 ? L::kRow : 1;
+            static constexpr int extA = G == 0 ? BY : BX;
+            static constexpr int strB = G == 2 ? L::kRow : L::kPlane;
+            static constexpr int extB = G == 2 ? BY : BZ;
+        };
+
+        // Bilinear footprint of one sample in the warp brick: four word addresses (taps outside
+        // the brick point at a dummy word past the brick) and their weights.
+        template <int G, int BX, int BY, int BZ>
+        __device__ __forceinline__ void warpTaps(float* plane, float* dummy, float pa, float pb,
+                                                 int orgA, int orgB, float* (&adr)[4],
+                                                 float (&wt)[4])
+        {
+            using AR = WarpRoles<G, BX, BY, BZ>;
+            Weights w;
+            tapWeights(pa, pb, w);
+            const int ia = w.ia - orgA, ib = w.ib - orgB;
+            const bool a0 = static_cast<unsigned>(ia) < static_cast<unsigned>(AR::extA);
+            const bool a1 = static_cast<unsigned>(ia + 1) < static_cast<unsigned>(AR::extA);
+            const bool b0 = static_cast<unsigned>(ib) < static_cast<unsigned>(AR::extB);
+            const bool b1 = static_cast<unsigned>(ib + 1) < static_cast<unsigned>(AR::extB);
+            float* q = plane + ia * AR::strA + ib * AR::strB;
+            adr[0] = (a0 && b0) ? q : dummy;
+            adr[1] = (a1 && b0) ? q + AR::strA : dummy;
+            adr[2] = (a0 && b1) ? q + AR::strB : dummy;
+            adr[3] = (a1 && b1) ? q + AR::strA + AR::strB : dummy;
+            wt[0] = w.wa * w.wb;
+            wt[1] = w.cwa * w.wb;
+            wt[2] = w.wa * w.cwb;
+            wt[3] = w.cwa * w.cwb;
+        }
+
+        // Walk samples jLo..jHi of ray R (position cp at sample jLo) through the brick. The loop
+        // is software-pipelined: the taps of sample j+1 (always on another plane) are read
+        // before the sums of sample j are written back.
+        template <int G, int BX, int BY, int BZ>
+        __device__ __forceinline__ void warpSplat(float* acc, float* dummy, const JosephRay& R,
+                                                  float yl, float2 cp, int jLo, int jHi,
+                                                  int orgG, int orgA, int orgB)
+        {
+            using AR = WarpRoles<G, BX, BY, BZ>;
+            const int dir = (R.meta & 4) ? -1 : 1;
+            float pa = cp.x, pb = cp.y;
+            float* plane = acc + (R.k0 + jLo * dir - orgG) * AR::strG;
+            const int dPlane = dir * AR::strG;
+            float* adr[4];
+            float wt[4], val[4];
+            warpTaps<G, BX, BY, BZ>(plane, dummy, pa, pb, orgA, orgB, adr, wt);
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+                val[t] = *adr[t];
+            for (int j = jLo; j < jHi; ++j) {
+                plane += dPlane;
+                pa = __fadd_rn(pa, R.sa);
+                pb = __fadd_rn(pb, R.sb);
+                float* adr2[4];
+                float wt2[4], val2[4];
+                warpTaps<G, BX, BY, BZ>(plane, dummy, pa, pb, orgA, orgB, adr2, wt2);
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                    val2[t] = *adr2[t];
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                    *adr[t] = val[t] + yl * wt[t];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    adr[t] = adr2[t];
+                    wt[t] = wt2[t];
+                    val[t] = val2[t];
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+                *adr[t] = val[t] + yl * wt[t];
+        }
+
+        // One (view, driving axis G) for a warp-owned brick: M x M ray classes, separated by
+        // __syncwarp; lane i takes class rays i, i + 32, ... (u fastest within the class grid).
+        template <int G, int BX, int BY, int BZ, int CPD>
+        __device__ __forceinline__ void warpView(float* acc, const RayWindow& w, int p, int m,
+                                                 const JosephRay* __restrict__ rays,
+                                                 const float2* __restrict__ cps, int64_t nrays,
+                                                 const float* __restrict__ y,
+                                                 const DetectorShape& det, int org0, int org1,
+                                                 int org2)
+        {
+            using AR = WarpRoles<G, BX, BY, BZ>;
+            const int orgG = G == 0 ? org0 : (G == 1 ? org1 : org2);
+            const int orgA = G == 0 ? org1 : org0;
+            const int orgB = G == 2 ? org1 : org2;
+            const int kLo = orgG, kHi = orgG + AR::extG - 1;
+            const int lane = threadIdx.x & 31;
+            const int64_t viewBase = static_cast<int64_t>(det.nu) * det.nv * p;
+            for (int ov = 0; ov < m; ++ov) {
+                const int vStart = w.v0 + ov;
+                const int nvc = vStart <= w.v1 ? (w.v1 - vStart) / m + 1 : 0;
+                for (int ou = 0; ou < m; ++ou) {
+                    const int uStart = w.u0 + ou;
+                    const int nuc = uStart <= w.u1 ? (w.u1 - uStart) / m + 1 : 0;
+                    const int total = nuc * nvc;
+                    const float invNuc = nuc > 0 ? 1.0f / static_cast<float>(nuc) : 0.0f;
+                    // up to kBatch class rays per lane are fetched together (record,
+                    // checkpoint and detector value are independent loads: the brick is one
+                    // checkpoint slab deep, so the checkpoint row is known up front)
+                    constexpr int kBatch = 2;
+                    const int64_t cpRow = static_cast<int64_t>(orgG / CPD + 1) * nrays;
+                    for (int base = lane; base < total; base += 32 * kBatch) {
+                        JosephRay Rb[kBatch];
+                        float2 cpb[kBatch];
+                        float yb[kBatch];
+#pragma unroll
+                        for (int q = 0; q < kBatch; ++q) {
+                            const int i = base + 32 * q;
+                            Rb[q].n = 0;
+                            if (i < total) {
+                                // i / nuc by a float reciprocal: exact for i < 2^20, nuc < 2^11
+                                const int iv =
+                                    static_cast<int>((static_cast<float>(i) + 0.5f) * invNuc);
+                                const int iu = i - iv * nuc;
+                                const int64_t r = viewBase + (uStart + iu * m) +
+                                                  static_cast<int64_t>(det.nu) * (vStart + iv * m);
+                                Rb[q] = rays[r];
+                                cpb[q] = __ldg(cps + cpRow + r);
+                                yb[q] = __ldg(y + r);
+                            }
+                        }
+#pragma unroll
+                        for (int q = 0; q < kBatch; ++q) {
+                            const JosephRay& R = Rb[q];
+                            if (R.n == 0 || (R.meta & 3) != G)
+                                continue;
+                            int jLo, jHi;
+                            if (!sampleRange(R, kLo, kHi, jLo, jHi))
+                                continue;
+                            warpSplat<G, BX, BY, BZ>(acc, acc + WarpBrick<BX, BY>::kPlane * BZ,
+                                                     R, yb[q] * R.len, cpb[q], jLo, jHi, orgG,
+                                                     orgA, orgB);
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+
+        // 3D adjoint: one warp per brick of BX x BY x BZ voxels; the brick accumulates every
+        // view in a fixed order (view, axis, class, lane round) and is written once.
+        template <int BX, int BY, int BZ, int CPD>
+        __global__ void __launch_bounds__(32)
+            josephAdjointWarpKernel(const JosephRay* __restrict__ rays,
+                                    const float2* __restrict__ checkpoints, int64_t nrays,
+                                    const float* __restrict__ y,
+                                    const RayWindow* __restrict__ windows,
+                                    const unsigned* __restrict__ viewAxes, VolumeShape vol,
+                                    DetectorShape det, int m, int3 nBricks, float* __restrict__ x)
+        {
+            using L = WarpBrick<BX, BY>;
+            __shared__ float acc[L::kPlane * BZ + 1]; // + dummy word for taps outside
+            const int lane = threadIdx.x;
+            const int bi = blockIdx.x;
+            const int org0 = (bi % nBricks.x) * BX, org1 = ((bi / nBricks.x) % nBricks.y) * BY,
+                      org2 = (bi / (nBricks.x * nBricks.y)) * BZ;
+            const int nb = nBricks.x * nBricks.y * nBricks.z;
+            for (int i = lane; i < L::kPlane * BZ; i += 32)
+                acc[i] = 0.0f;
+            __syncwarp();
+            for (int p = 0; p < det.np; ++p) {
+                const RayWindow w = windows[static_cast<int64_t>(p) * nb + bi];
+                if (w.u0 > w.u1 || w.v0 > w.v1)
+                    continue;
+                const unsigned ax = viewAxes[p];
+                if (ax & 1u)
+                    warpView<0, BX, BY, BZ, CPD>(acc, w, p, m, rays, checkpoints, nrays, y, det,
+                                                 org0, org1, org2);
+                if (ax & 2u)
+                    warpView<1, BX, BY, BZ, CPD>(acc, w, p, m, rays, checkpoints, nrays, y, det,
+                                                 org0, org1, org2);
+                if (ax & 4u)
+                    warpView<2, BX, BY, BZ, CPD>(acc, w, p, m, rays, checkpoints, nrays, y, det,
+                                                 org0, org1, org2);
+            }
+            for (int i = lane; i < BX * BY * BZ; i += 32) {
+                const int lx = i % BX, ly = (i / BX) % BY, lz = i / (BX * BY);
+                const int gx = org0 + lx, gy = org1 + ly, gz = org2 + lz;
+                if (gx < vol.n[0] && gy < vol.n[1] && gz < vol.n[2])
+                    x[gx + static_cast<int64_t>(vol.n[0]) *
+                               (gy + static_cast<int64_t>(vol.n[1]) * gz)] =
+                        acc[lz * L::kPlane + ly * L::kRow + lx];
+            }
+        }
+
+        template <int BX, int BY, int BZ, int CPD>
+        struct WarpAdjointConfig {
+            static constexpr int kCheckpointDepth = CPD;
+            static_assert(BX == CPD && BY == CPD && BZ == CPD,
+                          "a warp brick is exactly one checkpoint slab deep along every axis");
+            static int3 brick() { return make_int3(BX, BY, BZ); }
+            static void prepare(int) {}
+            static void launch(int nbricks, cudaStream_t s, const JosephRay* rays,
+                               const float2* cps, int64_t nrays, const float* y,
+                               const RayWindow* win, const unsigned* axes, VolumeShape vol,
+                               DetectorShape det, int m, int3 nb, float* x)
+            {
+                josephAdjointWarpKernel<BX, BY, BZ, CPD><<<nbricks, 32, 0, s>>>(
+                    rays, cps, nrays, y, win, axes, vol, det, m, nb, x);
+            }
+        };
+
+        using Adjoint3d = WarpAdjointConfig<16, 16, 16, 16>;
+        using Adjoint2d = AdjointConfig<2, 64, 64, 1, 64, 8>;
 
         class JosephProjector final : public Projector
         {
@@ -502,6 +855,7 @@ namespace elsa_b200
                 ELSA_CUDA(cudaMemcpy(&bad, dBad, sizeof(unsigned), cudaMemcpyDeviceToHost));
                 ELSA_CUDA(cudaMemcpy(&count, dCount, sizeof(count), cudaMemcpyDeviceToHost));
                 sampleCount_ = static_cast<int64_t>(count);
+                laneAxisBits();
                 classSpacing_ = 0;
                 for (int m = kMinClass; m <= kMaxClass; ++m)
                     if (!((bad >> m) & 1u)) {
@@ -518,11 +872,11 @@ namespace elsa_b200
                 if (vol_.dim == 3) {
                     brick_ = Adjoint3d::brick();
                     cpd = Adjoint3d::kCheckpointDepth;
-                    Adjoint3d::prepare();
+                    Adjoint3d::prepare(det_.np);
                 } else {
                     brick_ = Adjoint2d::brick();
                     cpd = Adjoint2d::kCheckpointDepth;
-                    Adjoint2d::prepare();
+                    Adjoint2d::prepare(det_.np);
                 }
                 const int maxDim = std::max(vol_.n[0], std::max(vol_.n[1], vol_.n[2]));
                 cpStride_ = maxDim / cpd + 3;
@@ -546,6 +900,47 @@ namespace elsa_b200
                     tma_ = std::make_unique<JosephForwardTma>(vol_, det_, hp, dRays_);
                 }
                 ELSA_CUDA(cudaDeviceSynchronize());
+            }
+
+            // Per view and driving axis g: set bit 4+g of the view's axis word when neighbouring
+            // pixels of a detector row spread along the second non-driving axis b on the planes
+            // of g (centre pixel and its right neighbour).
+            void laneAxisBits()
+            {
+                std::vector<unsigned> axes(det_.np);
+                ELSA_CUDA(cudaMemcpy(axes.data(), dViewAxes_, sizeof(unsigned) * det_.np,
+                                     cudaMemcpyDeviceToHost));
+                for (int p = 0; p < det_.np; ++p) {
+                    const float* P = poses_[p].v + kPoseOffPinv;
+                    const int d = vol_.dim;
+                    const float uc = det_.nu / 2 + 0.5f, vc = det_.nv / 2 + 0.5f;
+                    float D[3] = {0, 0, 0}, E[3] = {0, 0, 0};
+                    for (int i = 0; i < d; ++i) {
+                        if (d == 3) {
+                            D[i] = P[i * 3] * uc + P[i * 3 + 1] * vc + P[i * 3 + 2];
+                            E[i] = P[i * 3] * (uc + 1.0f) + P[i * 3 + 1] * vc + P[i * 3 + 2];
+                        } else {
+                            D[i] = P[i * 2] * uc + P[i * 2 + 1];
+                            E[i] = P[i * 2] * (uc + 1.0f) + P[i * 2 + 1];
+                        }
+                    }
+                    if (d == 3) {
+                        for (int g = 0; g < 3; ++g) {
+                            int a, b;
+                            nonDrivingAxes(g, a, b);
+                            if (std::fabs(D[g]) == 0.0f || std::fabs(E[g]) == 0.0f)
+                                continue;
+                            const float da =
+                                std::fabs(E[a] / std::fabs(E[g]) - D[a] / std::fabs(D[g]));
+                            const float db =
+                                std::fabs(E[b] / std::fabs(E[g]) - D[b] / std::fabs(D[g]));
+                            if (db > da)
+                                axes[p] |= 16u << g;
+                        }
+                    }
+                }
+                ELSA_CUDA(cudaMemcpy(dViewAxes_, axes.data(), sizeof(unsigned) * det_.np,
+                                     cudaMemcpyHostToDevice));
             }
 
             ~JosephProjector() override
@@ -576,10 +971,10 @@ namespace elsa_b200
             {
                 const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
                 if (vol_.dim == 3)
-                    Adjoint3d::launch(nb, s, dRays_, dCheckpoints_, cpStride_, y, dWindows_,
+                    Adjoint3d::launch(nb, s, dRays_, dCheckpoints_, rangeSize_, y, dWindows_,
                                       dViewAxes_, vol_, det_, classSpacing_, nBricks_, x);
                 else
-                    Adjoint2d::launch(nb, s, dRays_, dCheckpoints_, cpStride_, y, dWindows_,
+                    Adjoint2d::launch(nb, s, dRays_, dCheckpoints_, rangeSize_, y, dWindows_,
                                       dViewAxes_, vol_, det_, classSpacing_, nBricks_, x);
                 ELSA_LAUNCH_CHECK("josephAdjointKernel");
             }
