@@ -6,8 +6,12 @@ a C ABI, include/elsa_b200.h). Importing this package does not need a GPU; calli
 does, and fails loudly when the library is missing.
 """
 from . import _capi  # noqa: F401
-from ._capi import (ElsaError, InvalidArgumentError, Projector, circle_trajectory,  # noqa: F401
-                    pose_2d, pose_3d, POSE_FLOATS, PROJECTOR_JOSEPH, SOLVER_CGNE, Solver)
+from ._capi import (ElsaError, InvalidArgumentError, Projector, Solver,  # noqa: F401
+                    circle_trajectory, pose_2d, pose_3d, power_iterations, POSE_FLOATS,
+                    PROJECTOR_JOSEPH, SOLVER_CGNE, SOLVER_CGLS, SOLVER_LANDWEBER, SOLVER_APGD,
+                    PROX_IDENTITY, PROX_BOX, PROX_L1)
 
-__all__ = ["ElsaError", "InvalidArgumentError", "Projector", "circle_trajectory", "pose_2d",
-           "pose_3d", "POSE_FLOATS", "PROJECTOR_JOSEPH", "SOLVER_CGNE", "Solver"]
+__all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "circle_trajectory",
+           "pose_2d", "pose_3d", "power_iterations", "POSE_FLOATS", "PROJECTOR_JOSEPH",
+           "SOLVER_CGNE", "SOLVER_CGLS", "SOLVER_LANDWEBER", "SOLVER_APGD", "PROX_IDENTITY",
+           "PROX_BOX", "PROX_L1"]

@@ -23,6 +23,12 @@ STATUS_NAMES = {
 
 PROJECTOR_JOSEPH = 0
 SOLVER_CGNE = 0
+SOLVER_CGLS = 1
+SOLVER_LANDWEBER = 2
+SOLVER_APGD = 3
+PROX_IDENTITY = 0
+PROX_BOX = 1
+PROX_L1 = 2
 
 # Every function the header declares: name -> (restype, argtypes)
 _vp = ctypes.c_void_p
@@ -50,7 +56,10 @@ SIGNATURES = {
     "elsa_squared_l2_norm": (_st, [_vp, _i64, _vp, _vp]),
     "elsa_lincomb": (_st, [_f32, _vp, _f32, _vp, _vp, _i64, _vp]),
     "elsa_cgne_solve": (_st, [_vp, _vp, _vp, _i32, _i32, _vp]),
-    "elsa_solver_create": (_st, [_i32, _vp, _vp, _vp, _i32, _vp, ctypes.POINTER(_vp)]),
+    "elsa_solver_create": (_st, [_i32, _vp, _vp, _vp, _i32, ctypes.POINTER(ctypes.c_double),
+                                 _i32, _vp, ctypes.POINTER(_vp)]),
+    "elsa_solver_step_size": (_st, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    "elsa_power_iterations": (_st, [_vp, _i32, _vp, ctypes.POINTER(ctypes.c_double)]),
     "elsa_solver_iterate": (_st, [_vp, _i32, _vp]),
     "elsa_solver_squared_residual": (_st, [_vp, _vp, ctypes.POINTER(ctypes.c_double)]),
     "elsa_solver_enable_timing": (_st, [_vp, _i32]),
@@ -213,17 +222,34 @@ class Projector:
             pass
 
 
+def power_iterations(projector, iterations=5, stream=None):
+    """Largest eigenvalue of A^T A (powerIterations(adjoint(A) * A), PowerIterations.cpp:10-27)."""
+    v = ctypes.c_double()
+    call("elsa_power_iterations", projector.handle, int(iterations), ctypes.c_void_p(stream or 0),
+         ctypes.byref(v))
+    return v.value
+
+
 class Solver:
     """Owning handle of an elsa_solver: a device-resident iterative solve on device buffers
     (b: range, x: domain; both must outlive the solver)."""
 
-    def __init__(self, kind, projector, b_ptr, x_ptr, use_x0=False, stream=None):
+    def __init__(self, kind, projector, b_ptr, x_ptr, use_x0=False, stream=None, params=()):
+        """params: the solver's constructor arguments in the C ABI's order (elsa_b200.h):
+        CGLS (eps, tol), Landweber (step,), APGD (mu, epsilon, prox, lower, upper, sigma)."""
         self._proj = projector  # keep the operator alive
         h = ctypes.c_void_p()
+        params = [float(v) for v in params]
+        arr = (ctypes.c_double * max(1, len(params)))(*params)
         call("elsa_solver_create", int(kind), projector.handle, ctypes.c_void_p(b_ptr),
-             ctypes.c_void_p(x_ptr), int(bool(use_x0)), ctypes.c_void_p(stream or 0),
-             ctypes.byref(h))
+             ctypes.c_void_p(x_ptr), int(bool(use_x0)), arr, len(params),
+             ctypes.c_void_p(stream or 0), ctypes.byref(h))
         self._h = h
+
+    def step_size(self):
+        v = ctypes.c_double()
+        call("elsa_solver_step_size", self._h, ctypes.byref(v))
+        return v.value
 
     def iterate(self, iterations, stream=None):
         call("elsa_solver_iterate", self._h, int(iterations), ctypes.c_void_p(stream or 0))

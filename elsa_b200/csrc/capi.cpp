@@ -1,6 +1,8 @@
 // C ABI of elsa_b200 (include/elsa_b200.h): argument checks, exception -> status translation.
 #include <cuda_runtime.h>
 
+#include <cfloat>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -283,20 +285,82 @@ elsa_status elsa_cgne_solve(elsa_projector* p, const float* b, float* x, int32_t
 }
 
 elsa_status elsa_solver_create(int32_t kind, elsa_projector* p, const float* b, float* x,
-                               int32_t useX0, void* stream, elsa_solver** out)
+                               int32_t useX0, const double* params, int32_t numParams,
+                               void* stream, elsa_solver** out)
 {
     return guarded([&] {
         require(out != nullptr, "elsa_solver_create: null output handle");
         *out = nullptr;
         require(p && b && x, "elsa_solver_create: null argument");
-        require(kind == ELSA_SOLVER_CGNE, "elsa_solver_create: unknown solver kind");
+        require(kind >= ELSA_SOLVER_CGNE && kind <= ELSA_SOLVER_APGD,
+                "elsa_solver_create: unknown solver kind");
+        require(numParams >= 0 && (numParams == 0 || params != nullptr),
+                "elsa_solver_create: invalid parameter array");
+        static const int kMaxParams[] = {0, 2, 1, 6};
+        require(numParams <= kMaxParams[kind], "elsa_solver_create: too many parameters");
+        auto param = [&](int i, double dflt) { return i < numParams ? params[i] : dflt; };
+        elsa_b200::SolverOptions opt;
+        switch (kind) {
+        case ELSA_SOLVER_CGLS:
+            opt.cglsEps = param(0, 0.0);
+            opt.cglsTol = param(1, 1e-4);
+            require(std::isfinite(opt.cglsEps) && std::isfinite(opt.cglsTol),
+                    "elsa_solver_create: CGLS eps and tol must be finite");
+            break;
+        case ELSA_SOLVER_LANDWEBER:
+            opt.landweberStep = param(0, 0.0);
+            require(std::isfinite(opt.landweberStep),
+                    "elsa_solver_create: Landweber step must be finite");
+            break;
+        case ELSA_SOLVER_APGD: {
+            opt.apgdMu = param(0, 0.0);
+            opt.apgdEpsilon = param(1, static_cast<double>(FLT_EPSILON));
+            const double prox = param(2, 0.0);
+            require(prox == 0.0 || prox == 1.0 || prox == 2.0,
+                    "elsa_solver_create: APGD proximal operator must be 0, 1 or 2");
+            opt.prox.kind = static_cast<int>(prox);
+            const double lo = param(3, std::nan("")), hi = param(4, std::nan(""));
+            opt.prox.flags = (std::isnan(lo) ? 0 : 1) | (std::isnan(hi) ? 0 : 2);
+            opt.prox.lo = std::isnan(lo) ? 0.0f : static_cast<float>(lo);
+            opt.prox.hi = std::isnan(hi) ? 0.0f : static_cast<float>(hi);
+            opt.prox.sigma = static_cast<float>(param(5, 1.0));
+            require(std::isfinite(opt.apgdMu) && std::isfinite(opt.apgdEpsilon) &&
+                        std::isfinite(opt.prox.sigma),
+                    "elsa_solver_create: APGD parameters must be finite");
+            if (opt.prox.kind == 1 && (opt.prox.flags & 3) == 3)
+                require(opt.prox.lo <= opt.prox.hi,
+                        "elsa_solver_create: box constraint with lower > upper");
+            break;
+        }
+        default:
+            break;
+        }
         onDevice(p);
         auto h = std::make_unique<elsa_solver>();
         h->device = p->impl->device();
         h->impl = std::make_unique<elsa_b200::SolverSession>(
-            static_cast<elsa_b200::SolverKind>(kind), *p->impl, b, x, useX0 != 0,
+            static_cast<elsa_b200::SolverKind>(kind), *p->impl, b, x, useX0 != 0, opt,
             asStream(stream));
         *out = h.release();
+    });
+}
+
+elsa_status elsa_solver_step_size(elsa_solver* s, double* value)
+{
+    return guarded([&] {
+        require(s && value, "elsa_solver_step_size: null argument");
+        *value = s->impl->stepSize();
+    });
+}
+
+elsa_status elsa_power_iterations(elsa_projector* p, int32_t iterations, void* stream,
+                                  double* value)
+{
+    return guarded([&] {
+        require(p && value && iterations >= 0, "elsa_power_iterations: invalid argument");
+        onDevice(p);
+        elsa_b200::SolverWorkspace ws(p->impl->domainSize(), p->impl->rangeSize());
+        *value = elsa_b200::powerIterationsAtA(*p->impl, ws, iterations, asStream(stream));
     });
 }
 

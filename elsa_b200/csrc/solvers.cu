@@ -6,6 +6,8 @@
 #include "solvers.hpp"
 #include "vecops.cuh"
 
+#include <cmath>
+
 namespace elsa_b200
 {
     Projector::Projector(int kind, const VolumeShape& vol, const DetectorShape& det,
@@ -40,7 +42,8 @@ namespace elsa_b200
     SolverWorkspace::SolverWorkspace(int64_t domain, int64_t range)
         : vol0(sizeof(float) * domain), vol1(sizeof(float) * domain),
           vol2(sizeof(float) * domain), vol3(sizeof(float) * domain),
-          sino0(sizeof(float) * range), partials(sizeof(double) * kReduceBlocks),
+          sino0(sizeof(float) * range), sino1(sizeof(float) * range),
+          partials(sizeof(double) * kReduceBlocks),
           scalars(sizeof(SolverScalars))
     {
     }
@@ -140,13 +143,171 @@ namespace elsa_b200
             cgneStep(A, x, ws, off, s);
     }
 
+    double powerIterationsAtA(Projector& A, SolverWorkspace& ws, int iterations,
+                              cudaStream_t s)
+    {
+        const int64_t n = A.domainSize();
+        float* u = ws.vol0.as<float>();
+        float* v = ws.vol1.as<float>();
+        float* sino = ws.sino0.as<float>();
+        double* partials = ws.partials.as<double>();
+        SolverScalars* S = ws.scalars.as<SolverScalars>();
+        launchFill(u, 1.0f, n, s);
+        for (int i = 0; i < iterations; ++i) {
+            A.forward(u, sino, s);
+            A.adjoint(sino, u, s); // u = A^T A u
+            launchSquaredNorm(u, n, partials, &S->k, s);
+            launchScaleByInvNorm(u, &S->k, n, s);
+        }
+        A.forward(u, sino, s);
+        A.adjoint(sino, v, s);
+        launchDot(u, v, n, partials, &S->den, s);
+        launchSquaredNorm(u, n, partials, &S->k, s);
+        SolverScalars h;
+        ELSA_CUDA(cudaMemcpyAsync(&h, S, sizeof(h), cudaMemcpyDeviceToHost, s));
+        ELSA_CUDA(cudaStreamSynchronize(s));
+        return h.den / std::sqrt(h.k);
+    }
+
+    // CGLS: solvers/CGLS.cpp:19-91 (damping eps^2, stop once |r|^2 < tol).
+    static void cglsBegin(Projector& A, const float* b, float* x, bool useX0, float damp,
+                          SolverWorkspace& ws, cudaStream_t s)
+    {
+        const int64_t n = A.domainSize(), m = A.rangeSize();
+        float* r = ws.vol0.as<float>();
+        float* c = ws.vol1.as<float>();
+        float* sres = ws.sino0.as<float>();
+        double* partials = ws.partials.as<double>();
+        SolverScalars* S = ws.scalars.as<SolverScalars>();
+        ELSA_CUDA(cudaMemsetAsync(S, 0, sizeof(SolverScalars), s));
+        if (useX0) {
+            A.forward(x, sres, s);
+            launchSub(b, sres, sres, m, s); // s = b - A x
+            A.adjoint(sres, r, s);
+            launchDampNorm(r, x, damp, n, partials, s); // r -= damp x
+        } else {
+            launchFill(x, 0.0f, n, s);
+            ELSA_CUDA(cudaMemcpyAsync(sres, b, sizeof(float) * m, cudaMemcpyDeviceToDevice, s));
+            A.adjoint(sres, r, s);
+        }
+        ELSA_CUDA(cudaMemcpyAsync(c, r, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+        launchSquaredNorm(r, n, partials, &S->kold, s);
+    }
+
+    static void cglsStep(Projector& A, float* x, float damp, double tol, SolverWorkspace& ws,
+                         KernelTimer& t, cudaStream_t s)
+    {
+        const int64_t n = A.domainSize(), m = A.rangeSize();
+        float* r = ws.vol0.as<float>();
+        float* c = ws.vol1.as<float>();
+        float* sres = ws.sino0.as<float>();
+        float* q = ws.sino1.as<float>();
+        double* partials = ws.partials.as<double>();
+        SolverScalars* S = ws.scalars.as<SolverScalars>();
+        launchCheckTol(S, tol, s);
+        t.mark(s);
+        A.forward(c, q, s);
+        t.mark(s);
+        launchSquaredNorm(q, m, partials, &S->den, s);
+        if (damp != 0.0f)
+            launchSquaredNorm(c, n, partials, &S->aux[0], s);
+        launchCglsStep(x, sres, c, q, n, m, S, damp, s);
+        A.adjoint(sres, r, s);
+        t.mark(s);
+        launchDampNorm(r, x, damp, n, partials, s);
+        launchCgFinishNorm(partials, S, s);
+        launchCgDirectionGuarded(r, c, n, S, s);
+    }
+
+    // Landweber: solvers/LandweberIteration.cpp:26-72 with Landweber.cpp:20-25 (T = A^T).
+    static void landweberStep(Projector& A, const float* b, float* x, float step,
+                              SolverWorkspace& ws, KernelTimer& t, cudaStream_t s)
+    {
+        const int64_t n = A.domainSize(), m = A.rangeSize();
+        float* q = ws.vol2.as<float>();
+        float* sino = ws.sino0.as<float>();
+        t.mark(s);
+        A.forward(x, sino, s);
+        t.mark(s);
+        launchSub(sino, b, sino, m, s); // A x - b
+        A.adjoint(sino, q, s);
+        t.mark(s);
+        launchAxpyMinus(x, step, q, n, s); // x -= step A^T (A x - b)
+    }
+
+    // APGD (FISTA): solvers/APGD.cpp:34-102; gradient A^T (A y) - A^T b.
+    static void apgdGradient(Projector& A, SolverWorkspace& ws, KernelTimer& t, cudaStream_t s)
+    {
+        const int64_t n = A.domainSize();
+        float* y = ws.vol1.as<float>();
+        float* grad = ws.vol2.as<float>();
+        float* atb = ws.vol3.as<float>();
+        float* sino = ws.sino0.as<float>();
+        t.mark(s);
+        A.forward(y, sino, s);
+        t.mark(s);
+        A.adjoint(sino, grad, s);
+        t.mark(s);
+        launchSub(grad, atb, grad, n, s);
+    }
+
+    static void apgdBegin(Projector& A, const float* b, float* x, bool useX0,
+                          SolverWorkspace& ws, cudaStream_t s)
+    {
+        const int64_t n = A.domainSize();
+        SolverScalars* S = ws.scalars.as<SolverScalars>();
+        ELSA_CUDA(cudaMemsetAsync(S, 0, sizeof(SolverScalars), s));
+        static const double one = 1.0;
+        ELSA_CUDA(cudaMemcpyAsync(&S->tPrev, &one, sizeof(double), cudaMemcpyHostToDevice, s));
+        if (!useX0)
+            launchFill(x, 0.0f, n, s);
+        ELSA_CUDA(cudaMemcpyAsync(ws.vol0.as<float>(), x, sizeof(float) * n,
+                                  cudaMemcpyDeviceToDevice, s)); // xPrev
+        ELSA_CUDA(cudaMemcpyAsync(ws.vol1.as<float>(), x, sizeof(float) * n,
+                                  cudaMemcpyDeviceToDevice, s)); // y
+        A.adjoint(b, ws.vol3.as<float>(), s);                   // A^T b
+        KernelTimer off;
+        apgdGradient(A, ws, off, s);
+    }
+
+    static void apgdStep(Projector& A, float* x, float mu, const SolverOptions& opt,
+                         SolverWorkspace& ws, KernelTimer& t, cudaStream_t s)
+    {
+        const int64_t n = A.domainSize();
+        SolverScalars* S = ws.scalars.as<SolverScalars>();
+        double* partials = ws.partials.as<double>();
+        launchApgdStep(x, ws.vol0.as<float>(), ws.vol1.as<float>(), ws.vol2.as<float>(), mu,
+                       opt.prox, n, S, partials, s);
+        launchApgdFinish(partials, S, opt.apgdEpsilon, s);
+        apgdGradient(A, ws, t, s);
+    }
+
     SolverSession::SolverSession(SolverKind kind, Projector& A, const float* b, float* x,
-                                 bool useX0, cudaStream_t s)
-        : kind_(kind), A_(A), b_(b), x_(x), ws_(A.domainSize(), A.rangeSize())
+                                 bool useX0, const SolverOptions& opt, cudaStream_t s)
+        : kind_(kind), opt_(opt), A_(A), b_(b), x_(x), ws_(A.domainSize(), A.rangeSize())
     {
         switch (kind_) {
         case SolverKind::CGNE:
             cgneBegin(A_, b_, x_, useX0, ws_, s);
+            break;
+        case SolverKind::CGLS:
+            cglsBegin(A_, b_, x_, useX0, static_cast<float>(opt_.cglsEps * opt_.cglsEps), ws_,
+                      s);
+            break;
+        case SolverKind::LANDWEBER:
+            step_ = opt_.landweberStep > 0.0
+                        ? opt_.landweberStep
+                        : 0.9 * (2.0 / powerIterationsAtA(A_, ws_, opt_.powerIterations, s));
+            if (!useX0)
+                launchFill(x_, 0.0f, A_.domainSize(), s);
+            ELSA_CUDA(cudaMemsetAsync(ws_.scalars.as<SolverScalars>(), 0, sizeof(SolverScalars),
+                                      s));
+            break;
+        case SolverKind::APGD:
+            step_ = opt_.apgdMu > 0.0
+                        ? opt_.apgdMu
+                        : 0.45 / powerIterationsAtA(A_, ws_, opt_.powerIterations, s);
+            apgdBegin(A_, b_, x_, useX0, ws_, s);
             break;
         }
     }
@@ -158,6 +319,16 @@ namespace elsa_b200
             case SolverKind::CGNE:
                 cgneStep(A_, x_, ws_, timer_, s);
                 break;
+            case SolverKind::CGLS:
+                cglsStep(A_, x_, static_cast<float>(opt_.cglsEps * opt_.cglsEps), opt_.cglsTol,
+                         ws_, timer_, s);
+                break;
+            case SolverKind::LANDWEBER:
+                landweberStep(A_, b_, x_, static_cast<float>(step_), ws_, timer_, s);
+                break;
+            case SolverKind::APGD:
+                apgdStep(A_, x_, static_cast<float>(step_), opt_, ws_, timer_, s);
+                break;
             }
         }
     }
@@ -168,6 +339,10 @@ namespace elsa_b200
         ELSA_CUDA(cudaMemcpyAsync(&h, ws_.scalars.as<SolverScalars>(), sizeof(h),
                                   cudaMemcpyDeviceToHost, s));
         ELSA_CUDA(cudaStreamSynchronize(s));
+        if (kind_ == SolverKind::APGD)
+            return h.k;
+        if (kind_ == SolverKind::LANDWEBER)
+            return 0.0;
         return h.kold;
     }
 } // namespace elsa_b200

@@ -32,11 +32,11 @@ namespace elsa_b200
         size_t bytes_ = 0;
     };
 
-    // Scratch for one solver run: four volume-sized and one sinogram-sized float buffers, the
+    // Scratch for one solver run: four volume-sized and two sinogram-sized float buffers, the
     // reduction partials and the device scalars.
     struct SolverWorkspace {
         SolverWorkspace(int64_t domain, int64_t range);
-        DeviceBuffer vol0, vol1, vol2, vol3, sino0, partials, scalars;
+        DeviceBuffer vol0, vol1, vol2, vol3, sino0, sino1, partials, scalars;
     };
 
     void cgneSolve(Projector& A, const float* b, float* x, int iterations, bool useX0,
@@ -62,7 +62,23 @@ namespace elsa_b200
         int64_t count_ = 0;
     };
 
-    enum class SolverKind { CGNE = 0 };
+    enum class SolverKind { CGNE = 0, CGLS = 1, LANDWEBER = 2, APGD = 3 };
+
+    // Solver options (elsa's constructor arguments). Step sizes <= 0 mean "derive from power
+    // iterations", as the reference does when none is given.
+    struct SolverOptions {
+        double cglsEps = 0.0;  // CGLS damping eps (damp = eps^2), solvers/CGLS.cpp:12-17
+        double cglsTol = 1e-4; // CGLS stops once |r|^2 < tol, solvers/CGLS.h:46
+        double landweberStep = 0.0; // <= 0: 0.9 * 2 / lambda_max(A^T A)
+        double apgdMu = 0.0;        // <= 0: 0.45 / lambda_max(A^T A)
+        double apgdEpsilon = 1.1920928955078125e-07; // APGD stops once |grad|^2 <= epsilon
+        ProxSpec prox{0, 0, 0.0f, 0.0f, 0.0f};
+        int powerIterations = 5; // solvers/PowerIterations.h:11
+    };
+
+    // Largest eigenvalue of A^T A by power iterations, solvers/PowerIterations.cpp:10-27
+    // (synchronizes once at the end).
+    double powerIterationsAtA(Projector& A, SolverWorkspace& ws, int iterations, cudaStream_t s);
 
     // A solver run split into setup and iterations: begin() computes the initial residual,
     // iterate() enqueues iterations asynchronously on the stream (capturable in a CUDA graph
@@ -71,14 +87,17 @@ namespace elsa_b200
     {
     public:
         SolverSession(SolverKind kind, Projector& A, const float* b, float* x, bool useX0,
-                      cudaStream_t s);
+                      const SolverOptions& opt, cudaStream_t s);
         void iterate(int iterations, cudaStream_t s);
         double squaredResidual(cudaStream_t s); // synchronizes
         KernelTimer& timer() { return timer_; }
         Projector& op() { return A_; }
+        double stepSize() const { return step_; }
 
     private:
         SolverKind kind_;
+        SolverOptions opt_;
+        double step_ = 0.0;
         Projector& A_;
         const float* b_;
         float* x_;

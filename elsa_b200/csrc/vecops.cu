@@ -240,3 +240,213 @@ namespace elsa_b200
         ELSA_LAUNCH_CHECK("cgDirection");
     }
 } // namespace elsa_b200
+
+namespace elsa_b200
+{
+    namespace
+    {
+        __global__ void __launch_bounds__(kReduceThreads)
+            cglsStepKernel(float* __restrict__ x, float* __restrict__ sres,
+                           const float* __restrict__ c, const float* __restrict__ q, int64_t nx,
+                           int64_t ns, const SolverScalars* S, float damp)
+        {
+            if (S->done)
+                return;
+            const double den = S->den + (damp != 0.0f ? damp * S->aux[0] : 0.0);
+            const float alpha = static_cast<float>(S->kold / den);
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < nx; i += T)
+                x[i] = x[i] + alpha * c[i];
+            for (int64_t i = tid; i < ns; i += T)
+                sres[i] = sres[i] - alpha * q[i];
+        }
+
+        __global__ void __launch_bounds__(kReduceThreads)
+            dampNormKernel(float* __restrict__ r, const float* __restrict__ x, float damp,
+                           int64_t n, double* __restrict__ partials)
+        {
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            double acc = 0.0;
+            for (int64_t i = tid; i < n; i += T) {
+                float v = r[i];
+                if (damp != 0.0f) {
+                    v = v - damp * x[i];
+                    r[i] = v;
+                }
+                acc += static_cast<double>(v) * v;
+            }
+            const double sum = blockSum(acc);
+            if (threadIdx.x == 0)
+                partials[blockIdx.x] = sum;
+        }
+
+        __global__ void checkTolKernel(SolverScalars* S, double tol)
+        {
+            if (S->kold < tol)
+                S->done = 1;
+        }
+
+        __global__ void cgDirectionGuardedKernel(const float* __restrict__ r,
+                                                 float* __restrict__ c, int64_t n,
+                                                 const SolverScalars* S)
+        {
+            if (S->done)
+                return;
+            const float beta = static_cast<float>(S->beta);
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < n; i += T)
+                c[i] = r[i] + beta * c[i];
+        }
+
+        // out may alias a or b (element-wise read before write)
+        __global__ void subKernel(const float* a, const float* b, float* out, int64_t n)
+        {
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < n; i += T)
+                out[i] = a[i] - b[i];
+        }
+
+        __global__ void axpyMinusKernel(float* __restrict__ x, float step,
+                                        const float* __restrict__ q, int64_t n)
+        {
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < n; i += T)
+                x[i] = x[i] - step * q[i];
+        }
+
+        __global__ void scaleByInvNormKernel(float* __restrict__ u, const double* normSq,
+                                             int64_t n)
+        {
+            const float nrm = static_cast<float>(sqrt(*normSq));
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < n; i += T)
+                u[i] = u[i] / nrm;
+        }
+
+        __device__ __forceinline__ float applyProx(float z, const ProxSpec& p, float mu)
+        {
+            if (p.kind == 1) { // ProximalBoxConstraint.cpp:27-40 (clip / maximum / minimum)
+                if (p.flags & 1)
+                    z = fmaxf(z, p.lo);
+                if (p.flags & 2)
+                    z = fminf(z, p.hi);
+                return z;
+            }
+            if (p.kind == 2) { // ProximalL1.cpp:24-38 (soft threshold at mu * sigma)
+                float t = fabsf(z) - mu * p.sigma;
+                t = 0.5f * (t + fabsf(t));
+                const float sg = z > 0.0f ? 1.0f : (z < 0.0f ? -1.0f : 0.0f);
+                return sg * t;
+            }
+            return z;
+        }
+
+        __global__ void __launch_bounds__(kReduceThreads)
+            apgdStepKernel(float* __restrict__ x, float* __restrict__ xPrev, float* __restrict__ y,
+                           const float* __restrict__ grad, float mu, ProxSpec prox, int64_t n,
+                           const SolverScalars* S, double* __restrict__ partials)
+        {
+            const bool done = S->done != 0;
+            const double tp = S->tPrev;
+            const double t = (1.0 + sqrt(1.0 + 4.0 * tp * tp)) / 2.0;
+            const float coef = static_cast<float>((tp - 1.0) / t);
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            double acc = 0.0;
+            for (int64_t i = tid; i < n; i += T) {
+                const float g = grad[i];
+                acc += static_cast<double>(g) * g;
+                if (done)
+                    continue;
+                const float z = y[i] - mu * g;
+                const float xn = applyProx(z, prox, mu);
+                y[i] = xn + coef * (xn - xPrev[i]);
+                x[i] = xn;
+                xPrev[i] = xn;
+            }
+            const double sum = blockSum(acc);
+            if (threadIdx.x == 0)
+                partials[blockIdx.x] = sum;
+        }
+
+        __global__ void __launch_bounds__(kReduceThreads)
+            apgdFinishKernel(const double* __restrict__ partials, SolverScalars* S, double eps)
+        {
+            const double g2 = sumPartials(partials);
+            if (threadIdx.x == 0 && !S->done) {
+                const double tp = S->tPrev;
+                S->tPrev = (1.0 + sqrt(1.0 + 4.0 * tp * tp)) / 2.0;
+                S->k = g2;
+                if (g2 <= eps)
+                    S->done = 1;
+            }
+        }
+    } // namespace
+
+    void launchCglsStep(float* x, float* sres, const float* c, const float* q, int64_t nx,
+                        int64_t ns, SolverScalars* S, float damp, cudaStream_t s)
+    {
+        cglsStepKernel<<<gridFor(nx > ns ? nx : ns), kReduceThreads, 0, s>>>(x, sres, c, q, nx,
+                                                                             ns, S, damp);
+        ELSA_LAUNCH_CHECK("cglsStep");
+    }
+
+    void launchDampNorm(float* r, const float* x, float damp, int64_t n, double* partials,
+                        cudaStream_t s)
+    {
+        dampNormKernel<<<kReduceBlocks, kReduceThreads, 0, s>>>(r, x, damp, n, partials);
+        ELSA_LAUNCH_CHECK("dampNorm");
+    }
+
+    void launchCheckTol(SolverScalars* S, double tol, cudaStream_t s)
+    {
+        checkTolKernel<<<1, 1, 0, s>>>(S, tol);
+        ELSA_LAUNCH_CHECK("checkTol");
+    }
+
+    void launchCgDirectionGuarded(const float* r, float* c, int64_t n, const SolverScalars* S,
+                                  cudaStream_t s)
+    {
+        cgDirectionGuardedKernel<<<gridFor(n), 256, 0, s>>>(r, c, n, S);
+        ELSA_LAUNCH_CHECK("cgDirectionGuarded");
+    }
+
+    void launchSub(const float* in, const float* b, float* out, int64_t n, cudaStream_t s)
+    {
+        subKernel<<<gridFor(n), 256, 0, s>>>(in, b, out, n);
+        ELSA_LAUNCH_CHECK("sub");
+    }
+
+    void launchAxpyMinus(float* x, float step, const float* q, int64_t n, cudaStream_t s)
+    {
+        axpyMinusKernel<<<gridFor(n), 256, 0, s>>>(x, step, q, n);
+        ELSA_LAUNCH_CHECK("axpyMinus");
+    }
+
+    void launchScaleByInvNorm(float* u, const double* normSq, int64_t n, cudaStream_t s)
+    {
+        scaleByInvNormKernel<<<gridFor(n), 256, 0, s>>>(u, normSq, n);
+        ELSA_LAUNCH_CHECK("scaleByInvNorm");
+    }
+
+    void launchApgdStep(float* x, float* xPrev, float* y, const float* grad, float mu,
+                        ProxSpec prox, int64_t n, const SolverScalars* S, double* partials,
+                        cudaStream_t s)
+    {
+        apgdStepKernel<<<kReduceBlocks, kReduceThreads, 0, s>>>(x, xPrev, y, grad, mu, prox, n,
+                                                                S, partials);
+        ELSA_LAUNCH_CHECK("apgdStep");
+    }
+
+    void launchApgdFinish(const double* partials, SolverScalars* S, double eps, cudaStream_t s)
+    {
+        apgdFinishKernel<<<1, kReduceThreads, 0, s>>>(partials, S, eps);
+        ELSA_LAUNCH_CHECK("apgdFinish");
+    }
+} // namespace elsa_b200

@@ -23,7 +23,18 @@ namespace elsa_b200
         double alpha;  // step length
         double beta;   // direction update
         double tPrev;  // FISTA momentum t_{k-1}
-        double aux[2]; // spare
+        double aux[2]; // aux[0]: |c|^2 for damped CGLS
+        int done;      // set once a convergence test passed; later updates become no-ops
+        int pad;
+    };
+
+    // Proximal operators of APGD (proximal_operators/ProximalBoxConstraint.cpp,
+    // ProximalL1.cpp): kind 0 identity, 1 box [lo, hi] (flags bit 0 lower, bit 1 upper),
+    // 2 L1 with weight sigma.
+    struct ProxSpec {
+        int kind;
+        int flags;
+        float lo, hi, sigma;
     };
 
     // partials: device buffer of kReduceBlocks doubles.
@@ -51,4 +62,29 @@ namespace elsa_b200
     // c = r + beta*c
     void launchCgDirection(const float* r, float* c, int64_t n, const SolverScalars* S,
                            cudaStream_t s);
+
+    // CGLS: alpha = kold / (den (+ damp*|c|^2)); x += alpha c; s -= alpha q (no-op once done)
+    void launchCglsStep(float* x, float* sres, const float* c, const float* q, int64_t nx,
+                        int64_t ns, SolverScalars* S, float damp, cudaStream_t s);
+    // r -= damp*x (damping), partial |r|^2 -> partials
+    void launchDampNorm(float* r, const float* x, float damp, int64_t n, double* partials,
+                        cudaStream_t s);
+    // S->done |= (S->kold < tol)
+    void launchCheckTol(SolverScalars* S, double tol, cudaStream_t s);
+    // c = r + beta*c unless done
+    void launchCgDirectionGuarded(const float* r, float* c, int64_t n, const SolverScalars* S,
+                                  cudaStream_t s);
+    // out = in - b (out may alias in or b)
+    void launchSub(const float* in, const float* b, float* out, int64_t n, cudaStream_t s);
+    // x -= step*q (Landweber)
+    void launchAxpyMinus(float* x, float step, const float* q, int64_t n, cudaStream_t s);
+    // u = u / sqrt(*normSq) (power iterations)
+    void launchScaleByInvNorm(float* u, const double* normSq, int64_t n, cudaStream_t s);
+    // APGD iteration body on the domain: z = y - mu*grad; x = prox(z); t = (1+sqrt(1+4tp^2))/2;
+    // y = x + ((tp-1)/t)(x - xPrev); xPrev = x; partial |grad|^2 -> partials. No-op once done.
+    void launchApgdStep(float* x, float* xPrev, float* y, const float* grad, float mu,
+                        ProxSpec prox, int64_t n, const SolverScalars* S, double* partials,
+                        cudaStream_t s);
+    // S->tPrev = t; S->k = sum(partials); S->done |= (S->k <= eps)
+    void launchApgdFinish(const double* partials, SolverScalars* S, double eps, cudaStream_t s);
 } // namespace elsa_b200

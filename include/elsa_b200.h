@@ -154,23 +154,52 @@ elsa_status elsa_lincomb(float a, const float* x, float b, const float* y, float
 typedef struct elsa_solver elsa_solver;
 
 typedef enum elsa_solver_kind {
-    /* CGNE<float>, solvers/CGNE.cpp:20-78 */
-    ELSA_SOLVER_CGNE = 0
+    /* CGNE<float>, solvers/CGNE.cpp:20-78. params: none. */
+    ELSA_SOLVER_CGNE = 0,
+    /* CGLS<float>, solvers/CGLS.cpp:12-91. params[0] = eps (damping eps^2, default 0),
+     * params[1] = tol (stop once |A^T s - eps^2 x|^2 < tol, default 1e-4). */
+    ELSA_SOLVER_CGLS = 1,
+    /* Landweber<float>, solvers/LandweberIteration.cpp:26-72 + Landweber.cpp:20-25.
+     * params[0] = step size (<= 0 or absent: 0.9 * 2 / powerIterations(A^T A)). */
+    ELSA_SOLVER_LANDWEBER = 2,
+    /* APGD<float> (FISTA), solvers/APGD.cpp:14-102. params[0] = mu (<= 0 or absent:
+     * 0.45 / powerIterations(A^T A)), params[1] = epsilon (stop once |grad|^2 <= epsilon, default
+     * FLT_EPSILON), params[2] = proximal operator: 0 identity, 1 box constraint
+     * (proximal_operators/ProximalBoxConstraint.cpp:20-40), 2 L1
+     * (proximal_operators/ProximalL1.cpp:21-33); params[3] = lower bound, params[4] = upper
+     * bound (NaN = no bound; box only), params[5] = L1 weight sigma (default 1). */
+    ELSA_SOLVER_APGD = 3
 } elsa_solver_kind;
 
 /* Set up a solver run: allocate its scratch, compute the initial residual (x is zeroed unless
  * use_x0 != 0). b (range) and x (domain) are device buffers that must stay valid until
- * elsa_solver_destroy; x holds the current iterate. The constructor + first half of
- * Solver::solve(iterations, x0), solvers/Solver.h:21-43 and solvers/CGNE.cpp:20-47. */
+ * elsa_solver_destroy; x holds the current iterate. params (num_params doubles, may be NULL when
+ * num_params == 0) are the solver's constructor arguments, laid out per kind as above; missing
+ * trailing entries take the reference's defaults. The constructor + first half of
+ * Solver::solve(iterations, x0), solvers/Solver.h:21-43. Step sizes derived by power iterations
+ * synchronize the stream once. */
 elsa_status elsa_solver_create(int32_t kind, elsa_projector* projector, const float* b, float* x,
-                               int32_t use_x0, void* stream, elsa_solver** out);
+                               int32_t use_x0, const double* params, int32_t num_params,
+                               void* stream, elsa_solver** out);
 
-/* Enqueue `iterations` iterations on the stream without synchronizing (the loop body of
- * CGNE::solve, solvers/CGNE.cpp:50-73). All scalars stay in device memory, so the enqueued
- * work can be captured in a CUDA graph when timing is disabled. */
+/* Step size in use (Landweber step, APGD mu; 0 for the CG solvers). */
+elsa_status elsa_solver_step_size(elsa_solver* solver, double* value);
+
+/* Largest eigenvalue of A^T A by `iterations` power iterations from u = 1, in float with float64
+ * inner products. Replaces powerIterations(adjoint(A) * A, iterations),
+ * solvers/PowerIterations.cpp:10-27. Synchronizes the stream. */
+elsa_status elsa_power_iterations(elsa_projector* projector, int32_t iterations, void* stream,
+                                  double* value);
+
+/* Enqueue `iterations` iterations on the stream without synchronizing (the loop bodies of
+ * CGNE.cpp:50-73, CGLS.cpp:53-83, LandweberIteration.cpp:57-67, APGD.cpp:64-92). All scalars
+ * stay in device memory (a convergence test sets a device flag after which iterations leave the
+ * iterate unchanged), so the enqueued work can be captured in a CUDA graph when timing is
+ * disabled. */
 elsa_status elsa_solver_iterate(elsa_solver* solver, int32_t iterations, void* stream);
 
-/* Squared residual norm |r|^2 of the current iterate (float64, synchronizes the stream). */
+/* Squared norm used by the solver's convergence test (CGNE/CGLS: |r|^2 of the current iterate;
+ * APGD: |grad|^2 of the last iteration; Landweber: 0). float64, synchronizes the stream. */
 elsa_status elsa_solver_squared_residual(elsa_solver* solver, void* stream, double* value);
 
 /* Record CUDA events around the forward and adjoint projections of every iteration
