@@ -8,10 +8,11 @@ does, and fails loudly when the library is missing.
 from . import _capi  # noqa: F401
 from ._capi import (ElsaError, InvalidArgumentError, Projector, Solver,  # noqa: F401
                     circle_trajectory, pose_2d, pose_3d, power_iterations, POSE_FLOATS,
-                    PROJECTOR_JOSEPH, SOLVER_CGNE, SOLVER_CGLS, SOLVER_LANDWEBER, SOLVER_APGD,
-                    PROX_IDENTITY, PROX_BOX, PROX_L1)
+                    PROJECTOR_JOSEPH, PROJECTOR_SIDDON, SOLVER_CGNE, SOLVER_CGLS,
+                    SOLVER_LANDWEBER, SOLVER_APGD, PROX_IDENTITY, PROX_BOX, PROX_L1)
 
 __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "circle_trajectory",
            "pose_2d", "pose_3d", "power_iterations", "POSE_FLOATS", "PROJECTOR_JOSEPH",
-           "SOLVER_CGNE", "SOLVER_CGLS", "SOLVER_LANDWEBER", "SOLVER_APGD", "PROX_IDENTITY",
+           "PROJECTOR_SIDDON", "SOLVER_CGNE", "SOLVER_CGLS", "SOLVER_LANDWEBER", "SOLVER_APGD",
+           "PROX_IDENTITY",
            "PROX_BOX", "PROX_L1"]

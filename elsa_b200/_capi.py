@@ -22,6 +22,7 @@ STATUS_NAMES = {
 }
 
 PROJECTOR_JOSEPH = 0
+PROJECTOR_SIDDON = 1
 SOLVER_CGNE = 0
 SOLVER_CGLS = 1
 SOLVER_LANDWEBER = 2

@@ -30,6 +30,7 @@ CUDA_UNITS = [
     ("raysetup.cu", ["--fmad=false"]),
     ("joseph.cu", []),
     ("joseph_tma.cu", []),
+    ("siddon.cu", []),
     ("vecops.cu", []),
     ("solvers.cu", []),
 ]

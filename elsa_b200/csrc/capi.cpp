@@ -159,6 +159,9 @@ elsa_status elsa_projector_create(int32_t kind, int32_t dim, const int64_t* volD
         case ELSA_PROJECTOR_JOSEPH:
             handle->impl = elsa_b200::makeJosephProjector(vol, det, pv);
             break;
+        case ELSA_PROJECTOR_SIDDON:
+            handle->impl = elsa_b200::makeSiddonProjector(vol, det, pv);
+            break;
         default:
             throw elsa_b200::Error(ELSA_ERROR_NOT_SUPPORTED, "unknown projector kind");
         }
@@ -246,7 +249,7 @@ elsa_status elsa_projector_apply_adjoint_host(elsa_projector* p, const float* y,
 elsa_status elsa_dot(const float* x, const float* y, int64_t n, double* result, void* stream)
 {
     return guarded([&] {
-        require(x && y && result && n >= 0, "elsa_dot: invalid argument");
+        require(result && n >= 0 && ((x && y) || n == 0), "elsa_dot: invalid argument");
         elsa_b200::DeviceBuffer partials(sizeof(double) * elsa_b200::kReduceBlocks);
         elsa_b200::launchDot(x, y, n, partials.as<double>(), result, asStream(stream));
         ELSA_CUDA(cudaStreamSynchronize(asStream(stream)));
@@ -256,7 +259,7 @@ elsa_status elsa_dot(const float* x, const float* y, int64_t n, double* result, 
 elsa_status elsa_squared_l2_norm(const float* x, int64_t n, double* result, void* stream)
 {
     return guarded([&] {
-        require(x && result && n >= 0, "elsa_squared_l2_norm: invalid argument");
+        require(result && n >= 0 && (x || n == 0), "elsa_squared_l2_norm: invalid argument");
         elsa_b200::DeviceBuffer partials(sizeof(double) * elsa_b200::kReduceBlocks);
         elsa_b200::launchSquaredNorm(x, n, partials.as<double>(), result, asStream(stream));
         ELSA_CUDA(cudaStreamSynchronize(asStream(stream)));
@@ -267,7 +270,7 @@ elsa_status elsa_lincomb(float a, const float* x, float b, const float* y, float
                          void* stream)
 {
     return guarded([&] {
-        require(x && y && out && n >= 0, "elsa_lincomb: invalid argument");
+        require(n >= 0 && ((x && y && out) || n == 0), "elsa_lincomb: invalid argument");
         elsa_b200::launchLincomb(a, x, b, y, out, n, asStream(stream));
     });
 }

@@ -30,17 +30,30 @@ namespace elsa_b200
 
     // Per-ray traversal record of the Joseph projector (32 bytes). The driving axis d is the
     // axis of largest |direction|; a < b are the two other axes (2D: only a). Sample j
-    // (0 <= j < n) lies on the plane of driving index k0 + j*dir, at non-driving positions
-    //   pa_j = fma(j, sa, pa),  pb_j = fma(j, sb, pb).
-    // The forward and the adjoint kernels evaluate exactly this expression, which makes the
-    // pair an exact transpose. (elsa's CPU code accumulates pos += step instead,
-    // projectors/DrivingDirectionTraversal.cpp:265.)
+    // (0 <= j < n) lies on the plane of driving index k0 + j*dir; its non-driving positions are
+    // accumulated in float, pa_{j+1} = pa_j + sa (one rounding per step), exactly like elsa's
+    // CPU traversal (projectors/DrivingDirectionTraversal.cpp:265). Kernels that start a ray in
+    // the middle read the accumulated position from the slab checkpoints.
     struct __align__(16) JosephRay {
         float pa, pb, sa, sb;
         float len; // |step| = intersection length per sample
         int k0;    // driving-axis voxel index of sample 0
         int n;     // number of samples, 0 when the ray misses the volume
         int meta;  // bits 0-1 driving axis, bit 2 set when the ray runs towards lower indices
+    };
+
+    // Per-ray record of the Siddon projector (48 bytes): elsa's TraverseAABB state at the entry
+    // voxel (projectors/TraverseAABB.cpp:6-40,104-166). g is the axis of largest |direction|
+    // (used to cut rays into slabs); every visit advances the axes whose T is minimal.
+    struct __align__(16) SiddonRay {
+        float tDelta[3]; // |1/d| per axis, FLT_MAX when |d| <= FLT_EPSILON
+        int meta;        // bits 0-1 g; bit 2+i: step of axis i is -1; bit 5+i: step of axis i is 0;
+                         // bit 8: the ray crosses the volume
+        int kFirst;      // entry voxel index along g
+        int kLast;       // last voxel index along g
+        int cur[2];      // entry voxel indices of the two other axes a < b (2D: b unused)
+        float T[3];      // parameter of the first boundary crossing per axis (FLT_MAX if none)
+        int crossings;   // number of voxels visited
     };
 
     // Per (brick, view) detector window of the rays that can touch the brick, inclusive.

@@ -1010,6 +1010,17 @@ namespace elsa_b200
         };
     } // namespace
 
+    void launchBrickWindows(const float* poses, const VolumeShape& vol, const DetectorShape& det,
+                            int3 brick, int3 nBricks, RayWindow* out, cudaStream_t s)
+    {
+        const int64_t nwin = static_cast<int64_t>(nBricks.x) * nBricks.y * nBricks.z * det.np;
+        if (nwin == 0)
+            return;
+        josephWindowKernel<<<static_cast<unsigned>((nwin + 255) / 256), 256, 0, s>>>(
+            poses, vol, det, brick, nBricks, out);
+        ELSA_LAUNCH_CHECK("josephWindowKernel");
+    }
+
     std::unique_ptr<Projector> makeJosephProjector(const VolumeShape& vol,
                                                    const DetectorShape& det,
                                                    const std::vector<PoseRecord>& poses)

@@ -49,4 +49,13 @@ namespace elsa_b200
     std::unique_ptr<Projector> makeJosephProjector(const VolumeShape& vol,
                                                    const DetectorShape& det,
                                                    const std::vector<PoseRecord>& poses);
+    std::unique_ptr<Projector> makeSiddonProjector(const VolumeShape& vol,
+                                                   const DetectorShape& det,
+                                                   const std::vector<PoseRecord>& poses);
+
+    // Detector window of every (brick, view) for the brick-owner adjoints: the projection of the
+    // brick grown by one voxel, plus one pixel (joseph.cu). Windows are indexed view * nBricks +
+    // brick.
+    void launchBrickWindows(const float* poses, const VolumeShape& vol, const DetectorShape& det,
+                            int3 brick, int3 nBricks, RayWindow* out, cudaStream_t s);
 } // namespace elsa_b200

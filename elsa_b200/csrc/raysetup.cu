@@ -150,4 +150,90 @@ namespace elsa_b200
         }
         rays[r] = rec;
     }
+
+    __global__ void siddonSetupKernel(const float* __restrict__ poses, VolumeShape vol,
+                                      DetectorShape det, SiddonRay* __restrict__ rays,
+                                      SiddonLine* __restrict__ lines)
+    {
+        const int64_t nrays = static_cast<int64_t>(det.nu) * det.nv * det.np;
+        const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+        if (r >= nrays)
+            return;
+        const int dim = vol.dim;
+        const int u = static_cast<int>(r % det.nu);
+        const int v = static_cast<int>((r / det.nu) % det.nv);
+        const int p = static_cast<int>(r / (static_cast<int64_t>(det.nu) * det.nv));
+        float o[3] = {0, 0, 0}, d[3] = {0, 0, 0};
+        pixelRay(poses + static_cast<int64_t>(p) * 40, dim, u, v, o, d);
+        float boxMax[3] = {static_cast<float>(vol.n[0]), static_cast<float>(vol.n[1]),
+                           static_cast<float>(vol.n[2])};
+        float tmin, tmax;
+        bool inBox = slabIntersect(boxMax, dim, o, d, tmin, tmax);
+        int g = 0;
+        float best = fabsf(d[0]);
+        for (int i = 1; i < dim; ++i)
+            if (fabsf(d[i]) > best) {
+                best = fabsf(d[i]);
+                g = i;
+            }
+        int a, b;
+        nonDrivingAxes(g, a, b);
+        SiddonRay rec;
+        for (int i = 0; i < 3; ++i) {
+            rec.tDelta[i] = FLT_MAX;
+            rec.T[i] = FLT_MAX;
+        }
+        rec.meta = g;
+        rec.kFirst = rec.kLast = 0;
+        rec.cur[0] = rec.cur[1] = 0;
+        rec.crossings = 0;
+        SiddonLine line{0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        if (inBox) {
+            // entry point clamped to the box, TraverseAABB.cpp:13-20
+            float entry[3] = {0, 0, 0}, cur[3] = {0, 0, 0};
+            int stepDir[3] = {0, 0, 0};
+            for (int i = 0; i < dim; ++i) {
+                float e = o[i] + d[i] * tmin;
+                e = e < 0.0f ? 0.0f : e;
+                e = e > boxMax[i] ? boxMax[i] : e;
+                entry[i] = e;
+                stepDir[i] = d[i] > 0.0f ? 1 : (d[i] < 0.0f ? -1 : 0);
+            }
+            // entry voxel (one lower on a boundary when stepping down), :123-137
+            for (int i = 0; i < dim; ++i) {
+                float lc = floorf(entry[i]);
+                if (lc == entry[i] && stepDir[i] < 0)
+                    lc = lc - 1.0f;
+                cur[i] = lc;
+                if (cur[i] >= boxMax[i] || cur[i] < 0.0f)
+                    inBox = false;
+            }
+            if (inBox) {
+                for (int i = 0; i < dim; ++i) {
+                    const bool moves = fabsf(d[i]) > FLT_EPSILON;
+                    rec.tDelta[i] = moves ? static_cast<float>(stepDir[i]) / d[i] : FLT_MAX;
+                    const float bound = d[i] > 0.0f ? cur[i] + 1.0f : cur[i];
+                    rec.T[i] = moves ? (bound - entry[i]) / d[i] : FLT_MAX;
+                    if (stepDir[i] < 0)
+                        rec.meta |= 4 << i;
+                    if (stepDir[i] == 0)
+                        rec.meta |= 32 << i;
+                }
+                rec.meta |= 256;
+                rec.kFirst = rec.kLast = static_cast<int>(cur[g]);
+                rec.cur[0] = static_cast<int>(cur[a]);
+                rec.cur[1] = dim == 3 ? static_cast<int>(cur[b]) : 0;
+                line.g0 = entry[g];
+                line.a0 = entry[a];
+                line.sa = d[a] / d[g];
+                if (dim == 3) {
+                    line.b0 = entry[b];
+                    line.sb = d[b] / d[g];
+                }
+            }
+        }
+        rays[r] = rec;
+        if (lines)
+            lines[r] = line;
+    }
 } // namespace elsa_b200

@@ -1,0 +1,561 @@
+// Siddon's method (exact intersection lengths) for sm_100a.
+//
+// Reference semantics: projectors/SiddonsMethod.cpp:76-124 with projectors/TraverseAABB.cpp:6-184
+// (elsa's CPU path, the parity target). A ray visits the voxels it crosses in order; each visit
+// advances every axis whose next boundary parameter T is minimal, and the voxel's weight is the
+// parameter difference tExit - tEntry:
+//   forward  y[r] = sum_visits x[voxel] * (tExit - tEntry)
+//   adjoint  x[v] = sum_r sum_{visits of v} y[r] * (tExit - tEntry)
+// T advances by repeated float addition (T += tDelta), so both kernels replay the reference's
+// float operations one by one (no contraction): the visited voxels and weights are bit-identical
+// to the CPU traversal.
+//
+// Forward: one thread per ray, voxels gathered through the read-only cache.
+//
+// Adjoint: atomic-free and deterministic, on the brick-owner scheme of the Joseph adjoint. One
+// warp owns a 16^3 brick in shared memory for all views. Rays are cut into slabs of 16 voxels
+// along their axis g of largest |direction|; per (ray, slab) a checkpoint holds the traversal
+// state (T of every axis, entry parameter, voxel) at the ray's first visit inside the slab,
+// computed once per geometry. For each view the warp takes the rays of the brick's detector
+// window class by class (pixel indices congruent modulo m, m validated per geometry so that
+// same-class rays with the same g stay more than two voxels apart laterally on every slice);
+// each lane replays one ray's visits inside the slab from its checkpoint and adds the weights of
+// the visits that fall inside the brick. Same-class rays therefore never touch the same voxel,
+// and every voxel sums its contributions in a fixed order.
+#include "projector.hpp"
+#include "raysetup.cuh"
+#include "solvers.hpp"
+
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+#include <cstring>
+
+namespace elsa_b200
+{
+    namespace
+    {
+        constexpr int kForwardThreads = 128;
+        constexpr int kSlab = 16; // brick edge = checkpoint slab depth
+        constexpr int kMinClass = 2;
+        constexpr int kMaxClass = 8;
+        constexpr int kActive = 256;
+
+        __device__ __forceinline__ int floorDiv(int a, int b)
+        {
+            const int q = a / b;
+            return (a % b != 0 && ((a < 0) != (b < 0))) ? q - 1 : q;
+        }
+
+        __device__ __forceinline__ int axisStep(int meta, int i)
+        {
+            return ((meta >> (5 + i)) & 1) ? 0 : (((meta >> (2 + i)) & 1) ? -1 : 1);
+        }
+
+        // One visit: the parameter where the ray leaves the current voxel, and which axes cross
+        // (TraverseAABB.cpp:55-100: all axes whose T is minimal advance together).
+        template <int DIM>
+        __device__ __forceinline__ float nextCrossing(float T0, float T1, float T2, bool& m0,
+                                                      bool& m1, bool& m2)
+        {
+            float tm = T0;
+            tm = (T1 < tm) ? T1 : tm;
+            if (DIM == 3)
+                tm = (T2 < tm) ? T2 : tm;
+            m0 = (T0 <= T1) && (DIM < 3 || T0 <= T2);
+            m1 = (T1 <= T0) && (DIM < 3 || T1 <= T2);
+            m2 = DIM == 3 && (T2 <= T0) && (T2 <= T1);
+            return tm;
+        }
+
+        // Entry voxel in axis order from the record (g and the two other axes a < b).
+        __device__ __forceinline__ void entryVoxel(int g, int kg, int ca, int cb, int& c0,
+                                                   int& c1, int& c2)
+        {
+            c0 = g == 0 ? kg : ca;
+            c1 = g == 1 ? kg : (g == 0 ? ca : cb);
+            c2 = g == 2 ? kg : cb;
+        }
+
+        template <int DIM>
+        __global__ void __launch_bounds__(kForwardThreads)
+            siddonForwardKernel(const SiddonRay* __restrict__ rays, int64_t nrays,
+                                const float* __restrict__ x, VolumeShape vol,
+                                float* __restrict__ y)
+        {
+            const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (r >= nrays)
+                return;
+            const SiddonRay R = rays[r];
+            float acc = 0.0f;
+            if (R.meta & kActive) {
+                const int g = R.meta & 3;
+                int c0, c1, c2;
+                entryVoxel(g, R.kFirst, R.cur[0], R.cur[1], c0, c1, c2);
+                const int s0 = axisStep(R.meta, 0), s1 = axisStep(R.meta, 1),
+                          s2 = axisStep(R.meta, 2);
+                const int nx = vol.n[0], ny = vol.n[1], nz = vol.n[2];
+                const int64_t sy = nx, sz = static_cast<int64_t>(nx) * ny;
+                int64_t idx = c0 + sy * c1 + (DIM == 3 ? sz * c2 : 0);
+                float T0 = R.T[0], T1 = R.T[1], T2 = R.T[2];
+                float tExit = 0.0f;
+                const int maxVisits = nx + ny + (DIM == 3 ? nz : 0) + 3;
+                for (int it = 0; it < maxVisits; ++it) {
+                    const float tEntry = tExit;
+                    bool m0, m1, m2;
+                    tExit = nextCrossing<DIM>(T0, T1, T2, m0, m1, m2);
+                    if (m0) {
+                        c0 += s0;
+                        T0 = __fadd_rn(T0, R.tDelta[0]);
+                    }
+                    if (m1) {
+                        c1 += s1;
+                        T1 = __fadd_rn(T1, R.tDelta[1]);
+                    }
+                    if (m2) {
+                        c2 += s2;
+                        T2 = __fadd_rn(T2, R.tDelta[2]);
+                    }
+                    const bool inside =
+                        static_cast<unsigned>(c0) < static_cast<unsigned>(nx) &&
+                        static_cast<unsigned>(c1) < static_cast<unsigned>(ny) &&
+                        (DIM < 3 || static_cast<unsigned>(c2) < static_cast<unsigned>(nz));
+                    const float w = __fsub_rn(tExit, tEntry);
+                    acc = __fadd_rn(acc, __fmul_rn(__ldg(x + idx), w));
+                    if (!inside)
+                        break;
+                    idx += (m0 ? s0 : 0) + (m1 ? s1 * sy : 0) + (m2 ? s2 * sz : 0);
+                }
+            }
+            y[r] = acc;
+        }
+
+        // Replays every ray once: writes the traversal state at the ray's first visit in each
+        // slab of kSlab voxels along g (slab-major, row floor(k/kSlab) + 1, column = ray), the
+        // last visited index along g and the visit count (SiddonsMethod's sample count).
+        template <int DIM>
+        __global__ void siddonCheckpointKernel(SiddonRay* __restrict__ rays, int64_t nrays,
+                                               VolumeShape vol, int slabRows,
+                                               float4* __restrict__ cpState,
+                                               unsigned* __restrict__ cpVoxel,
+                                               unsigned long long* __restrict__ visits)
+        {
+            const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (r >= nrays)
+                return;
+            SiddonRay R = rays[r];
+            if (!(R.meta & kActive))
+                return;
+            const int g = R.meta & 3;
+            int a, b;
+            nonDrivingAxes(g, a, b);
+            int c0, c1, c2;
+            entryVoxel(g, R.kFirst, R.cur[0], R.cur[1], c0, c1, c2);
+            const int s0 = axisStep(R.meta, 0), s1 = axisStep(R.meta, 1), s2 = axisStep(R.meta, 2);
+            const int nx = vol.n[0], ny = vol.n[1], nz = vol.n[2];
+            float T0 = R.T[0], T1 = R.T[1], T2 = R.T[2];
+            float tExit = 0.0f;
+            int slab = INT_MIN, count = 0, kLast = R.kFirst;
+            const int maxVisits = nx + ny + (DIM == 3 ? nz : 0) + 3;
+            for (int it = 0; it < maxVisits; ++it) {
+                const float tEntry = tExit;
+                const int cg = g == 0 ? c0 : (g == 1 ? c1 : c2);
+                const int s = floorDiv(cg, kSlab);
+                if (s != slab) {
+                    slab = s;
+                    if (s + 1 >= 0 && s + 1 < slabRows) {
+                        const int ca = a == 0 ? c0 : c1;
+                        const int cb = DIM == 3 ? (b == 1 ? c1 : c2) : 0;
+                        const int64_t at = static_cast<int64_t>(s + 1) * nrays + r;
+                        cpState[at] = make_float4(T0, T1, T2, tEntry);
+                        cpVoxel[at] =
+                            static_cast<unsigned>(ca) | (static_cast<unsigned>(cb) << 16);
+                    }
+                }
+                kLast = cg;
+                ++count;
+                bool m0, m1, m2;
+                tExit = nextCrossing<DIM>(T0, T1, T2, m0, m1, m2);
+                if (m0) {
+                    c0 += s0;
+                    T0 = __fadd_rn(T0, R.tDelta[0]);
+                }
+                if (m1) {
+                    c1 += s1;
+                    T1 = __fadd_rn(T1, R.tDelta[1]);
+                }
+                if (m2) {
+                    c2 += s2;
+                    T2 = __fadd_rn(T2, R.tDelta[2]);
+                }
+                const bool inside =
+                    static_cast<unsigned>(c0) < static_cast<unsigned>(nx) &&
+                    static_cast<unsigned>(c1) < static_cast<unsigned>(ny) &&
+                    (DIM < 3 || static_cast<unsigned>(c2) < static_cast<unsigned>(nz));
+                if (!inside)
+                    break;
+            }
+            R.kLast = kLast;
+            R.crossings = count;
+            rays[r] = R;
+            atomicAdd(visits, static_cast<unsigned long long>(count));
+        }
+
+        // True when rays R and S (same axis g) stay more than two voxels apart in one lateral
+        // coordinate over the slices of g that both visit.
+        __device__ bool separated(const SiddonRay& R, const SiddonLine& LR, const SiddonRay& S,
+                                  const SiddonLine& LS, int dim)
+        {
+            const int lo = max(min(R.kFirst, R.kLast), min(S.kFirst, S.kLast));
+            const int hi = min(max(R.kFirst, R.kLast), max(S.kFirst, S.kLast));
+            if (lo > hi)
+                return true;
+            const float margin = 2.05f;
+            const float g0 = static_cast<float>(lo), g1 = static_cast<float>(hi + 1);
+            const float da0 = fmaf(g0 - LR.g0, LR.sa, LR.a0) - fmaf(g0 - LS.g0, LS.sa, LS.a0);
+            const float da1 = fmaf(g1 - LR.g0, LR.sa, LR.a0) - fmaf(g1 - LS.g0, LS.sa, LS.a0);
+            if ((da0 > margin && da1 > margin) || (da0 < -margin && da1 < -margin))
+                return true;
+            if (dim == 3) {
+                const float db0 = fmaf(g0 - LR.g0, LR.sb, LR.b0) - fmaf(g0 - LS.g0, LS.sb, LS.b0);
+                const float db1 = fmaf(g1 - LR.g0, LR.sb, LR.b0) - fmaf(g1 - LS.g0, LS.sb, LS.b0);
+                if ((db0 > margin && db1 > margin) || (db0 < -margin && db1 < -margin))
+                    return true;
+            }
+            return false;
+        }
+
+        // Axes present per view and, per candidate class spacing m, whether two rays that the
+        // adjoint may process concurrently could visit the same voxel. Neighbours checked: the
+        // same detector row m pixels apart, and the next class row (m rows down) within +-32
+        // pixels; rays further apart in a class are further apart on every slice (the pixel ->
+        // slice-position map of a flat detector is monotone for rays sharing g).
+        __global__ void siddonClassCheckKernel(const SiddonRay* __restrict__ rays,
+                                               const SiddonLine* __restrict__ lines,
+                                               DetectorShape det, int dim,
+                                               unsigned* __restrict__ viewAxes,
+                                               unsigned* __restrict__ badSpacing)
+        {
+            const int64_t nrays = static_cast<int64_t>(det.nu) * det.nv * det.np;
+            const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (r >= nrays)
+                return;
+            const SiddonRay R = rays[r];
+            if (!(R.meta & kActive))
+                return;
+            const SiddonLine LR = lines[r];
+            const int u = static_cast<int>(r % det.nu);
+            const int v = static_cast<int>((r / det.nu) % det.nv);
+            const int p = static_cast<int>(r / (static_cast<int64_t>(det.nu) * det.nv));
+            atomicOr(viewAxes + p, 1u << (R.meta & 3));
+            unsigned bad = 0;
+            for (int m = kMinClass; m <= kMaxClass; ++m) {
+                const int noffs = dim == 3 ? 1 + 65 : 1;
+                for (int o = 0; o < noffs; ++o) {
+                    const int du = o == 0 ? m : o - 1 - 32;
+                    const int dv = o == 0 ? 0 : m;
+                    const int u2 = u + du, v2 = v + dv;
+                    if (u2 < 0 || u2 >= det.nu || v2 < 0 || v2 >= det.nv)
+                        continue;
+                    const int64_t r2 =
+                        u2 + static_cast<int64_t>(det.nu) * (v2 + static_cast<int64_t>(det.nv) * p);
+                    const SiddonRay S = rays[r2];
+                    if (!(S.meta & kActive) || (S.meta & 3) != (R.meta & 3))
+                        continue;
+                    if (!separated(R, LR, S, lines[r2], dim))
+                        bad |= 1u << m;
+                }
+            }
+            if (bad)
+                atomicOr(badSpacing, bad);
+        }
+
+        // Shared-memory brick of one warp (x stride 1, row stride 17, plane stride = 1 mod 32).
+        template <int DIM>
+        struct SiddonBrick {
+            static constexpr int kBz = DIM == 3 ? kSlab : 1;
+            static constexpr int kRow = kSlab + 1;
+            static constexpr int kPlaneMin = kRow * kSlab;
+            static constexpr int kPlane = kPlaneMin + ((33 - kPlaneMin % 32) % 32);
+            static constexpr int kWords = kPlane * kBz + 1; // + dummy word
+        };
+
+        // Replays the visits of one ray inside the slab [kLo, kLo + 15] along G from its
+        // checkpoint and adds y * weight to the visited voxels of the brick (visits outside the
+        // brick go to the dummy word).
+        template <int DIM, int G>
+        __device__ __forceinline__ void splatSegment(float* acc, float3 tDelta, int meta,
+                                                     int kFirst, float4 cp, unsigned cpv, float yv,
+                                                     int kLo, int org0, int org1, int org2,
+                                                     const VolumeShape& vol)
+        {
+            using L = SiddonBrick<DIM>;
+            const int dirG = ((meta >> (2 + G)) & 1) ? -1 : 1;
+            const int kg = dirG > 0 ? max(kLo, kFirst) : min(kLo + kSlab - 1, kFirst);
+            int c0, c1, c2;
+            entryVoxel(G, kg, static_cast<int>(cpv & 0xffffu), static_cast<int>(cpv >> 16), c0,
+                       c1, c2);
+            const int s0 = axisStep(meta, 0), s1 = axisStep(meta, 1), s2 = axisStep(meta, 2);
+            float T0 = cp.x, T1 = cp.y, T2 = cp.z;
+            float tEntry = cp.w;
+            float* dummy = acc + L::kWords - 1;
+            for (int it = 0; it < 3 * kSlab + 3; ++it) {
+                bool m0, m1, m2;
+                const float tExit = nextCrossing<DIM>(T0, T1, T2, m0, m1, m2);
+                const int l0 = c0 - org0, l1 = c1 - org1, l2 = DIM == 3 ? c2 - org2 : 0;
+                const bool mine = static_cast<unsigned>(l0) < static_cast<unsigned>(kSlab) &&
+                                  static_cast<unsigned>(l1) < static_cast<unsigned>(kSlab) &&
+                                  static_cast<unsigned>(l2) < static_cast<unsigned>(L::kBz);
+                float* adr = mine ? acc + l2 * L::kPlane + l1 * L::kRow + l0 : dummy;
+                const float w = __fsub_rn(tExit, tEntry);
+                *adr = __fadd_rn(*adr, __fmul_rn(yv, w));
+                if (m0) {
+                    c0 += s0;
+                    T0 = __fadd_rn(T0, tDelta.x);
+                }
+                if (m1) {
+                    c1 += s1;
+                    T1 = __fadd_rn(T1, tDelta.y);
+                }
+                if (m2) {
+                    c2 += s2;
+                    T2 = __fadd_rn(T2, tDelta.z);
+                }
+                const bool inside =
+                    static_cast<unsigned>(c0) < static_cast<unsigned>(vol.n[0]) &&
+                    static_cast<unsigned>(c1) < static_cast<unsigned>(vol.n[1]) &&
+                    (DIM < 3 || static_cast<unsigned>(c2) < static_cast<unsigned>(vol.n[2]));
+                const int cg = G == 0 ? c0 : (G == 1 ? c1 : c2);
+                if (!inside || cg < kLo || cg >= kLo + kSlab)
+                    break;
+                tEntry = tExit;
+            }
+        }
+
+        // One (view, axis G) for a warp-owned brick: m x m ray classes separated by __syncwarp;
+        // lane i takes class rays i, i + 32, ... (u fastest within the class grid).
+        template <int DIM, int G>
+        __device__ __forceinline__ void siddonView(float* acc, const RayWindow& w, int p, int m,
+                                                   const SiddonRay* __restrict__ rays,
+                                                   const float4* __restrict__ cpState,
+                                                   const unsigned* __restrict__ cpVoxel,
+                                                   int64_t nrays, const float* __restrict__ y,
+                                                   const DetectorShape& det, int org0, int org1,
+                                                   int org2, const VolumeShape& vol)
+        {
+            const int kLo = G == 0 ? org0 : (G == 1 ? org1 : org2);
+            const int kHi = kLo + kSlab - 1;
+            const int lane = threadIdx.x & 31;
+            const int64_t viewBase = static_cast<int64_t>(det.nu) * det.nv * p;
+            const int64_t cpRow = static_cast<int64_t>(kLo / kSlab + 1) * nrays;
+            for (int ov = 0; ov < m; ++ov) {
+                const int vStart = w.v0 + ov;
+                const int nvc = vStart <= w.v1 ? (w.v1 - vStart) / m + 1 : 0;
+                for (int ou = 0; ou < m; ++ou) {
+                    const int uStart = w.u0 + ou;
+                    const int nuc = uStart <= w.u1 ? (w.u1 - uStart) / m + 1 : 0;
+                    const int total = nuc * nvc;
+                    for (int i = lane; i < total; i += 32) {
+                        const int iv = i / nuc;
+                        const int iu = i - iv * nuc;
+                        const int64_t r = viewBase + (uStart + iu * m) +
+                                          static_cast<int64_t>(det.nu) * (vStart + iv * m);
+                        const int4* rp = reinterpret_cast<const int4*>(rays + r);
+                        const int4 q0 = __ldg(rp);     // tDelta[3], meta
+                        const int4 q1 = __ldg(rp + 1); // kFirst, kLast, cur[2]
+                        const int meta = q0.w;
+                        if (!(meta & kActive) || (meta & 3) != G)
+                            continue;
+                        if (max(q1.x, q1.y) < kLo || min(q1.x, q1.y) > kHi)
+                            continue;
+                        const float3 td = make_float3(__int_as_float(q0.x), __int_as_float(q0.y),
+                                                      __int_as_float(q0.z));
+                        splatSegment<DIM, G>(acc, td, meta, q1.x, __ldg(cpState + cpRow + r),
+                                             __ldg(cpVoxel + cpRow + r), __ldg(y + r), kLo, org0,
+                                             org1, org2, vol);
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+
+        template <int DIM>
+        __global__ void __launch_bounds__(32)
+            siddonAdjointKernel(const SiddonRay* __restrict__ rays,
+                                const float4* __restrict__ cpState,
+                                const unsigned* __restrict__ cpVoxel, int64_t nrays,
+                                const float* __restrict__ y,
+                                const RayWindow* __restrict__ windows,
+                                const unsigned* __restrict__ viewAxes, VolumeShape vol,
+                                DetectorShape det, int m, int3 nBricks, float* __restrict__ x)
+        {
+            using L = SiddonBrick<DIM>;
+            __shared__ float acc[L::kWords];
+            const int lane = threadIdx.x;
+            const int bi = blockIdx.x;
+            const int org0 = (bi % nBricks.x) * kSlab;
+            const int org1 = ((bi / nBricks.x) % nBricks.y) * kSlab;
+            const int org2 = (bi / (nBricks.x * nBricks.y)) * L::kBz;
+            const int nb = nBricks.x * nBricks.y * nBricks.z;
+            for (int i = lane; i < L::kWords; i += 32)
+                acc[i] = 0.0f;
+            __syncwarp();
+            for (int p = 0; p < det.np; ++p) {
+                const RayWindow w = windows[static_cast<int64_t>(p) * nb + bi];
+                if (w.u0 > w.u1 || w.v0 > w.v1)
+                    continue;
+                const unsigned ax = viewAxes[p];
+                if (ax & 1u)
+                    siddonView<DIM, 0>(acc, w, p, m, rays, cpState, cpVoxel, nrays, y, det, org0,
+                                       org1, org2, vol);
+                if (ax & 2u)
+                    siddonView<DIM, 1>(acc, w, p, m, rays, cpState, cpVoxel, nrays, y, det, org0,
+                                       org1, org2, vol);
+                if (DIM == 3 && (ax & 4u))
+                    siddonView<DIM, DIM == 3 ? 2 : 0>(acc, w, p, m, rays, cpState, cpVoxel, nrays,
+                                                      y, det, org0, org1, org2, vol);
+            }
+            __syncwarp();
+            for (int i = lane; i < kSlab * kSlab * L::kBz; i += 32) {
+                const int lx = i % kSlab, ly = (i / kSlab) % kSlab, lz = i / (kSlab * kSlab);
+                const int gx = org0 + lx, gy = org1 + ly, gz = org2 + lz;
+                if (gx < vol.n[0] && gy < vol.n[1] && gz < vol.n[2])
+                    x[gx + static_cast<int64_t>(vol.n[0]) *
+                               (gy + static_cast<int64_t>(vol.n[1]) * gz)] =
+                        acc[lz * L::kPlane + ly * L::kRow + lx];
+            }
+        }
+
+        class SiddonProjector final : public Projector
+        {
+        public:
+            SiddonProjector(const VolumeShape& vol, const DetectorShape& det,
+                            const std::vector<PoseRecord>& poses)
+                : Projector(1, vol, det, poses)
+            {
+                const int maxDim = std::max(vol_.n[0], std::max(vol_.n[1], vol_.n[2]));
+                if (maxDim >= 65536)
+                    throw Error(ELSA_ERROR_NOT_SUPPORTED,
+                                "SiddonsMethod: volume edges must be below 65536 voxels");
+                const int64_t nrays = rangeSize_;
+                const int threads = 256;
+                const unsigned blocks = static_cast<unsigned>((nrays + threads - 1) / threads);
+                rays_ = std::make_unique<DeviceBuffer>(sizeof(SiddonRay) * nrays);
+                DeviceBuffer lines(sizeof(SiddonLine) * nrays);
+                siddonSetupKernel<<<blocks, threads>>>(dPoses_, vol_, det_, rays_->as<SiddonRay>(),
+                                                       lines.as<SiddonLine>());
+                ELSA_LAUNCH_CHECK("siddonSetupKernel");
+
+                cpRows_ = maxDim / kSlab + 3;
+                cpState_ = std::make_unique<DeviceBuffer>(sizeof(float4) * nrays * cpRows_);
+                cpVoxel_ = std::make_unique<DeviceBuffer>(sizeof(unsigned) * nrays * cpRows_);
+                // per-view axis masks, the bad-spacing mask and a 64-bit visit counter
+                const size_t words = static_cast<size_t>(det_.np) + 4;
+                viewAxes_ = std::make_unique<DeviceBuffer>(sizeof(unsigned) * words);
+                unsigned* dAxes = viewAxes_->as<unsigned>();
+                ELSA_CUDA(cudaMemset(dAxes, 0, sizeof(unsigned) * words));
+                unsigned* dBad = dAxes + det_.np;
+                auto* dCount =
+                    reinterpret_cast<unsigned long long*>(dAxes + ((det_.np + 2) & ~1));
+                if (vol_.dim == 3)
+                    siddonCheckpointKernel<3><<<blocks, threads>>>(
+                        rays_->as<SiddonRay>(), nrays, vol_, cpRows_, cpState_->as<float4>(),
+                        cpVoxel_->as<unsigned>(), dCount);
+                else
+                    siddonCheckpointKernel<2><<<blocks, threads>>>(
+                        rays_->as<SiddonRay>(), nrays, vol_, cpRows_, cpState_->as<float4>(),
+                        cpVoxel_->as<unsigned>(), dCount);
+                ELSA_LAUNCH_CHECK("siddonCheckpointKernel");
+                siddonClassCheckKernel<<<blocks, threads>>>(rays_->as<SiddonRay>(),
+                                                            lines.as<SiddonLine>(), det_,
+                                                            vol_.dim, dAxes, dBad);
+                ELSA_LAUNCH_CHECK("siddonClassCheckKernel");
+                unsigned bad = 0;
+                unsigned long long count = 0;
+                ELSA_CUDA(cudaMemcpy(&bad, dBad, sizeof(unsigned), cudaMemcpyDeviceToHost));
+                ELSA_CUDA(cudaMemcpy(&count, dCount, sizeof(count), cudaMemcpyDeviceToHost));
+                visits_ = static_cast<int64_t>(count);
+                for (int m = kMinClass; m <= kMaxClass; ++m)
+                    if (!((bad >> m) & 1u)) {
+                        classSpacing_ = m;
+                        break;
+                    }
+                if (classSpacing_ == 0)
+                    throw Error(ELSA_ERROR_NOT_SUPPORTED,
+                                "SiddonsMethod: neighbouring detector rays pass within two voxels "
+                                "of each other even eight pixels apart; the atomic-free adjoint "
+                                "needs a coarser detector");
+
+                const int bz = vol_.dim == 3 ? kSlab : 1;
+                nBricks_ = make_int3((vol_.n[0] + kSlab - 1) / kSlab,
+                                     (vol_.n[1] + kSlab - 1) / kSlab, (vol_.n[2] + bz - 1) / bz);
+                const int64_t nwin =
+                    static_cast<int64_t>(nBricks_.x) * nBricks_.y * nBricks_.z * det_.np;
+                windows_ = std::make_unique<DeviceBuffer>(sizeof(RayWindow) * nwin);
+                launchBrickWindows(dPoses_, vol_, det_, make_int3(kSlab, kSlab, bz), nBricks_,
+                                   windows_->as<RayWindow>(), nullptr);
+                ELSA_CUDA(cudaDeviceSynchronize());
+            }
+
+            void forward(const float* x, float* y, cudaStream_t s) override
+            {
+                const int64_t nrays = rangeSize_;
+                const unsigned blocks =
+                    static_cast<unsigned>((nrays + kForwardThreads - 1) / kForwardThreads);
+                if (vol_.dim == 3)
+                    siddonForwardKernel<3><<<blocks, kForwardThreads, 0, s>>>(
+                        rays_->as<SiddonRay>(), nrays, x, vol_, y);
+                else
+                    siddonForwardKernel<2><<<blocks, kForwardThreads, 0, s>>>(
+                        rays_->as<SiddonRay>(), nrays, x, vol_, y);
+                ELSA_LAUNCH_CHECK("siddonForwardKernel");
+            }
+
+            void adjoint(const float* y, float* x, cudaStream_t s) override
+            {
+                const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
+                if (vol_.dim == 3)
+                    siddonAdjointKernel<3><<<nb, 32, 0, s>>>(
+                        rays_->as<SiddonRay>(), cpState_->as<float4>(), cpVoxel_->as<unsigned>(),
+                        rangeSize_, y, windows_->as<RayWindow>(), viewAxes_->as<unsigned>(), vol_,
+                        det_, classSpacing_, nBricks_, x);
+                else
+                    siddonAdjointKernel<2><<<nb, 32, 0, s>>>(
+                        rays_->as<SiddonRay>(), cpState_->as<float4>(), cpVoxel_->as<unsigned>(),
+                        rangeSize_, y, windows_->as<RayWindow>(), viewAxes_->as<unsigned>(), vol_,
+                        det_, classSpacing_, nBricks_, x);
+                ELSA_LAUNCH_CHECK("siddonAdjointKernel");
+            }
+
+            int64_t info(int key) const override
+            {
+                switch (key) {
+                case 0:
+                    return classSpacing_;
+                case 1:
+                    return static_cast<int64_t>(nBricks_.x) * nBricks_.y * nBricks_.z;
+                case 2:
+                    return visits_;
+                case 3:
+                    return 0;
+                default:
+                    return -1;
+                }
+            }
+
+        private:
+            std::unique_ptr<DeviceBuffer> rays_, cpState_, cpVoxel_, viewAxes_, windows_;
+            int cpRows_ = 0;
+            int classSpacing_ = 0;
+            int64_t visits_ = 0;
+            int3 nBricks_{};
+        };
+    } // namespace
+
+    std::unique_ptr<Projector> makeSiddonProjector(const VolumeShape& vol,
+                                                   const DetectorShape& det,
+                                                   const std::vector<PoseRecord>& poses)
+    {
+        return std::make_unique<SiddonProjector>(vol, det, poses);
+    }
+} // namespace elsa_b200

@@ -41,8 +41,11 @@ typedef enum elsa_status {
 } elsa_status;
 
 typedef enum elsa_projector_kind {
-    /* JosephsMethod / JosephsMethodCUDA (matched adjoint) */
-    ELSA_PROJECTOR_JOSEPH = 0
+    /* JosephsMethod / JosephsMethodCUDA (matched adjoint), projectors/JosephsMethod.cpp:37-198 */
+    ELSA_PROJECTOR_JOSEPH = 0,
+    /* SiddonsMethod / SiddonsMethodCUDA, projectors/SiddonsMethod.cpp:76-124 with
+     * projectors/TraverseAABB.cpp:6-184 */
+    ELSA_PROJECTOR_SIDDON = 1
 } elsa_projector_kind;
 
 typedef struct elsa_projector elsa_projector;

@@ -651,10 +651,11 @@ namespace orc
     // ------------------------------------------------------------------------------------------
     // Siddon: projectors/TraverseAABB.cpp:6-184 + SiddonsMethod.cpp:76-124
     // ------------------------------------------------------------------------------------------
+    // visits (optional): per-ray number of visited voxels
     template <typename data_t, bool adjoint>
     static void siddonTraverse(int dim, const index_t* volDims, const index_t* detDims,
                                index_t numPoses, const float* poseData, const data_t* in,
-                               data_t* out)
+                               data_t* out, index_t* visits = nullptr)
     {
         std::vector<PoseView> poses(numPoses);
         for (index_t p = 0; p < numPoses; ++p)
@@ -734,6 +735,8 @@ namespace orc
                             if (!(cur[i] < boxMax[i] && cur[i] >= 0.0f))
                                 inBox = false;
                         const float weight = tExit - tEntry;
+                        if (visits)
+                            ++visits[ir];
                         if (adjoint) {
                             const data_t v = in[ir] * static_cast<data_t>(weight);
 #pragma omp atomic
@@ -965,6 +968,24 @@ int64_t oracle_joseph_sample_count(int dim, const int64_t* volDims, const int64_
         const orc::Ray r = orc::rayForIndex(poses.data(), dim, detDims, ir);
         total += orc::ddSetup(boxMax, dim, r).numSteps;
     }
+    return total;
+}
+
+int64_t oracle_siddon_visit_count(int dim, const int64_t* volDims, const int64_t* detDims,
+                                  const float* poseData)
+{
+    const int64_t np = detDims[dim - 1];
+    const int64_t nrays = (dim == 2 ? detDims[0] : detDims[0] * detDims[1]) * np;
+    int64_t nvol = 1;
+    for (int i = 0; i < dim; ++i)
+        nvol *= volDims[i];
+    std::vector<float> x(static_cast<size_t>(nvol), 0.0f), y(static_cast<size_t>(nrays));
+    std::vector<int64_t> visits(static_cast<size_t>(nrays), 0);
+    orc::siddonTraverse<float, false>(dim, volDims, detDims, np, poseData, x.data(), y.data(),
+                                      visits.data());
+    int64_t total = 0;
+    for (int64_t v : visits)
+        total += v;
     return total;
 }
 

@@ -64,6 +64,8 @@ def lib():
             fn.argtypes = [c_int, c_int, _i64p, _i64p, _f32p, fp, fp]
         L.oracle_joseph_sample_count.argtypes = [c_int, _i64p, _i64p, _f32p]
         L.oracle_joseph_sample_count.restype = c_i64
+        L.oracle_siddon_visit_count.argtypes = [c_int, _i64p, _i64p, _f32p]
+        L.oracle_siddon_visit_count.restype = c_i64
         L.oracle_dot_f32.argtypes = [_f32p, _f32p, c_i64]
         L.oracle_dot_f32.restype = ctypes.c_double
         L.oracle_dot_f64.argtypes = [_f64p, _f64p, c_i64]
@@ -184,6 +186,11 @@ def siddon_adjoint(y, vol_dims, det_dims, poses, dtype=np.float32):
 def joseph_sample_count(vol_dims, det_dims, poses):
     return int(lib().oracle_joseph_sample_count(len(vol_dims), np.asarray(vol_dims, np.int64),
                                                 np.asarray(det_dims, np.int64), _f32(poses)))
+
+
+def siddon_visit_count(vol_dims, det_dims, poses):
+    return int(lib().oracle_siddon_visit_count(len(vol_dims), np.asarray(vol_dims, np.int64),
+                                               np.asarray(det_dims, np.int64), _f32(poses)))
 
 
 def dot(a, b):
