@@ -25,13 +25,14 @@ _i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
 
 
 def build(force=False):
-    """Compile oracle.cpp into liboracle.so (g++, OpenMP, no FP contraction)."""
-    src = os.path.join(_HERE, "oracle.cpp")
+    """Compile oracle.cpp and voxel_oracle.cpp into liboracle.so (g++, OpenMP, no FP
+    contraction)."""
+    srcs = [os.path.join(_HERE, "oracle.cpp"), os.path.join(_HERE, "voxel_oracle.cpp")]
     if (not force and os.path.exists(_LIB_PATH)
-            and os.path.getmtime(_LIB_PATH) >= os.path.getmtime(src)):
+            and all(os.path.getmtime(_LIB_PATH) >= os.path.getmtime(f) for f in srcs)):
         return _LIB_PATH
     cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared",
-           "-o", _LIB_PATH, src]
+           "-o", _LIB_PATH] + srcs
     subprocess.check_call(cmd)
     return _LIB_PATH
 
@@ -66,6 +67,20 @@ def lib():
         L.oracle_joseph_sample_count.restype = c_i64
         L.oracle_siddon_visit_count.argtypes = [c_int, _i64p, _i64p, _f32p]
         L.oracle_siddon_visit_count.restype = c_i64
+        L.oracle_bessel.argtypes = [c_int, ctypes.c_double]
+        L.oracle_bessel.restype = ctypes.c_double
+        L.oracle_blob_projected.argtypes = [c_f, c_f, c_f, c_int, c_int]
+        L.oracle_blob_projected.restype = c_f
+        L.oracle_bspline1d.argtypes = [c_f, c_int]
+        L.oracle_bspline1d.restype = c_f
+        L.oracle_blob_lut.argtypes = [c_f, c_f, c_int, c_int, c_i64, _f32p]
+        L.oracle_bspline_lut.argtypes = [c_int, c_int, c_int, c_i64, _f32p]
+        L.oracle_lut_lerp.argtypes = [_f32p, c_i64, c_f, c_f]
+        L.oracle_lut_lerp.restype = c_f
+        for name, fp in (("f32", _f32p), ("f64", _f64p)):
+            fn = getattr(L, "oracle_voxel_" + name)
+            fn.argtypes = [c_int, c_int, _i64p, _i64p, _f32p, _f32p, c_i64, c_f, c_int, c_int,
+                           fp, fp]
         L.oracle_dot_f32.argtypes = [_f32p, _f32p, c_i64]
         L.oracle_dot_f32.restype = ctypes.c_double
         L.oracle_dot_f64.argtypes = [_f64p, _f64p, c_i64]
@@ -199,3 +214,68 @@ def dot(a, b):
     if a.dtype == np.float64:
         return lib().oracle_dot_f64(a, np.ascontiguousarray(b, np.float64), a.size)
     return lib().oracle_dot_f32(_f32(a), _f32(b), a.size)
+
+
+# ---- voxel (blob / B-spline) projectors: oracle/voxel_oracle.cpp --------------------------------
+LUT_SIZE = 100  # DEFAULT_PROJECTOR_LUT_SIZE, projectors/Luts.hpp:8
+WEIGHT_CLASSIC = 0
+WEIGHT_DIFFERENTIAL = 1
+
+
+def bessel(m, x):
+    return lib().oracle_bessel(int(m), float(x))
+
+
+def blob_projected(s, a, alpha, m, which=0):
+    """which: 0 value, 1 derivative, 2 normalized gradient (projectors/Blobs.h:67-210)."""
+    return lib().oracle_blob_projected(s, a, alpha, int(m), int(which))
+
+
+def bspline1d(x, m):
+    return lib().oracle_bspline1d(x, int(m))
+
+
+def blob_lut(radius=2.0, alpha=10.83, order=2, which=0, n=LUT_SIZE):
+    out = np.empty(n, np.float32)
+    lib().oracle_blob_lut(radius, alpha, int(order), int(which), int(n), out)
+    return out
+
+
+def bspline_lut(dim, order=2, which=0, n=LUT_SIZE):
+    out = np.empty(n, np.float32)
+    lib().oracle_bspline_lut(int(dim), int(order), int(which), int(n), out)
+    return out
+
+
+def bspline_support(order):
+    return float(np.float32((order + 1) * 0.5))
+
+
+def lut_lerp(lut, support, distance):
+    lut = _f32(lut)
+    return lib().oracle_lut_lerp(lut, lut.size, support, distance)
+
+
+def voxel_lut(kind, dim, radius=2.0, alpha=10.83, order=2):
+    """(lut, support, weight kind) of a voxel projector: kind one of 'blob', 'bspline',
+    'phase_blob', 'phase_bspline' (VoxelProjector.cpp, PhaseContrastProjector.cpp)."""
+    phase = kind.startswith("phase")
+    which = 0 if not phase else (1 if dim == 2 else 2)
+    if kind.endswith("blob"):
+        return blob_lut(radius, alpha, order, which), float(np.float32(radius)), int(phase)
+    return bspline_lut(dim, order, which), bspline_support(order), int(phase)
+
+
+def voxel_project(adjoint, data, vol_dims, det_dims, poses, lut, support, weight_kind,
+                  loop_mode=1, dtype=np.float32):
+    """Blob / B-spline voxel projector (projectors/VoxelComputation.h:116-184). loop_mode 1 visits
+    the footprint rectangle; 0 follows the reference CPU loop as written."""
+    dim = len(vol_dims)
+    n_out = int(np.prod(vol_dims)) if adjoint else int(np.prod(det_dims))
+    data = np.ascontiguousarray(data, dtype).ravel()
+    out = np.empty(n_out, dtype)
+    fn = lib().oracle_voxel_f64 if dtype == np.float64 else lib().oracle_voxel_f32
+    lut = _f32(lut)
+    fn(int(adjoint), dim, np.asarray(vol_dims, np.int64), np.asarray(det_dims, np.int64),
+       _f32(poses), lut, lut.size, float(support), int(weight_kind), int(loop_mode), data, out)
+    return out

@@ -11,19 +11,21 @@ It restates the reference solvers on float32 vectors, with the projector given a
              proximal_operators/ProximalL1.cpp:24-38
 * powerIterations  solvers/PowerIterations.cpp:10-27
 
-Inner products and norms are accumulated in float64 (the reference reduces in float32 with a
+Every solver takes dtype=np.float32 (the reference's float instantiation, the parity target) or
+np.float64 (the double instantiation, which shows how far the float32 result itself is from exact
+arithmetic). Inner products and norms accumulate in float64 (the reference reduces in float32 with a
 thrust transform_reduce whose order depends on the backend, storage/reductions/L2.h:15-33,
 DotProduct.h:26-47; a float64 sum is the order-independent limit of those sums). Vector updates
-are float32 like the reference's DataContainer arithmetic; scalars (alpha, beta, t) are rounded
-to float32 before they scale a vector, as data_t scalars are in the reference.
+are in dtype like the reference's DataContainer arithmetic; scalars (alpha, beta, t) are rounded
+to dtype before they scale a vector, as data_t scalars are in the reference.
 """
 import numpy as np
 
 F32_EPS = float(np.finfo(np.float32).eps)
 
 
-def _f(a):
-    return np.ascontiguousarray(a, dtype=np.float32)
+def _caster(dtype):
+    return lambda a: np.ascontiguousarray(a, dtype=dtype)
 
 
 def _sq(a):
@@ -36,19 +38,21 @@ def _dot(a, b):
                         np.asarray(b, dtype=np.float64).ravel()))
 
 
-def power_iterations(A, At, domain_size, iterations=5):
+def power_iterations(A, At, domain_size, iterations=5, dtype=np.float32):
     """Largest eigenvalue of A^T A, solvers/PowerIterations.cpp:10-27."""
-    u = np.ones(domain_size, np.float32)
+    _f = _caster(dtype)
+    u = np.ones(domain_size, dtype)
     for _ in range(iterations):
         u = _f(At(A(u)))
-        u = _f(u / np.float32(np.sqrt(_sq(u))))
+        u = _f(u / dtype(np.sqrt(_sq(u))))
     v = _f(At(A(u)))
     return _dot(u, v) / np.sqrt(_sq(u))
 
 
-def cgne(A, At, b, domain_size, iterations, x0=None):
+def cgne(A, At, b, domain_size, iterations, x0=None, dtype=np.float32):
     """CG on A^T A x = A^T b, solvers/CGNE.cpp:20-78. Returns (x, |r|^2 history)."""
-    x = np.zeros(domain_size, np.float32) if x0 is None else _f(x0).copy()
+    _f = _caster(dtype)
+    x = np.zeros(domain_size, dtype) if x0 is None else _f(x0).copy()
     atb = _f(At(b))
     r = _f(atb - _f(At(A(x))))
     c = r.copy()
@@ -56,27 +60,28 @@ def cgne(A, At, b, domain_size, iterations, x0=None):
     hist = []
     for _ in range(iterations):
         ac = _f(At(A(c)))
-        alpha = np.float32(kold / _dot(c, ac))
+        alpha = dtype(kold / _dot(c, ac))
         x = _f(x + alpha * c)
         r = _f(r - alpha * ac)
         k = _sq(r)
-        beta = np.float32(k / kold)
+        beta = dtype(k / kold)
         c = _f(r + beta * c)
         kold = k
         hist.append(k)
     return x, hist
 
 
-def cgls(A, At, b, domain_size, iterations, x0=None, eps=0.0, tol=1e-4):
+def cgls(A, At, b, domain_size, iterations, x0=None, eps=0.0, tol=1e-4, dtype=np.float32):
     """CGLS with damping eps^2, solvers/CGLS.cpp:19-91. Returns (x, |r|^2 history)."""
-    damp = np.float32(eps * eps)
+    _f = _caster(dtype)
+    damp = dtype(eps * eps)
     if x0 is not None:
         x = _f(x0).copy()
         s = _f(b - _f(A(x)))
         r = _f(At(s))
         r = _f(r - damp * x)
     else:
-        x = np.zeros(domain_size, np.float32)
+        x = np.zeros(domain_size, dtype)
         s = _f(b).copy()
         r = _f(At(s))
     c = r.copy()
@@ -88,58 +93,62 @@ def cgls(A, At, b, domain_size, iterations, x0=None, eps=0.0, tol=1e-4):
         q = _f(A(c))
         delta = _sq(q)
         den = delta if damp == 0 else delta + float(damp) * _sq(c)
-        alpha = np.float32(kold / den)
+        alpha = dtype(kold / den)
         x = _f(x + alpha * c)
         s = _f(s - alpha * q)
         r = _f(At(s))
         if damp != 0:
             r = _f(r - damp * x)
         k = _sq(r)
-        beta = np.float32(k / kold)
+        beta = dtype(k / kold)
         c = _f(r + beta * c)
         kold = k
         hist.append(k)
     return x, hist
 
 
-def landweber(A, At, b, domain_size, iterations, x0=None, step=None, power_iters=5):
+def landweber(A, At, b, domain_size, iterations, x0=None, step=None, power_iters=5,
+              dtype=np.float32):
     """Landweber iteration x -= step * A^T (A x - b), solvers/LandweberIteration.cpp:26-72.
     Returns (x, step)."""
-    x = np.zeros(domain_size, np.float32) if x0 is None else _f(x0).copy()
+    _f = _caster(dtype)
+    x = np.zeros(domain_size, dtype) if x0 is None else _f(x0).copy()
     if step is None or step <= 0:
-        step = 0.9 * (2.0 / power_iterations(A, At, domain_size, power_iters))
-    st = np.float32(step)
+        step = 0.9 * (2.0 / power_iterations(A, At, domain_size, power_iters, dtype))
+    st = dtype(step)
     for _ in range(iterations):
         res = _f(_f(A(x)) - b)
         x = _f(x - st * _f(At(res)))
     return x, float(step)
 
 
-def prox(z, mu, kind=0, lower=None, upper=None, sigma=1.0):
+def prox(z, mu, kind=0, lower=None, upper=None, sigma=1.0, dtype=np.float32):
     """Proximal operators: 0 identity, 1 box (ProximalBoxConstraint.cpp:27-40),
     2 L1 soft threshold (ProximalL1.cpp:24-38)."""
+    _f = _caster(dtype)
     z = _f(z)
     if kind == 1:
         if lower is not None:
-            z = np.maximum(z, np.float32(lower))
+            z = np.maximum(z, dtype(lower))
         if upper is not None:
-            z = np.minimum(z, np.float32(upper))
+            z = np.minimum(z, dtype(upper))
         return _f(z)
     if kind == 2:
-        t = _f(np.abs(z) - np.float32(mu) * np.float32(sigma))
+        t = _f(np.abs(z) - dtype(mu) * dtype(sigma))
         t = _f(0.5 * (t + np.abs(t)))
         return _f(np.sign(z) * t)
     return z
 
 
 def apgd(A, At, b, domain_size, iterations, x0=None, mu=None, epsilon=F32_EPS, kind=0,
-         lower=None, upper=None, sigma=1.0, power_iters=5):
+         lower=None, upper=None, sigma=1.0, power_iters=5, dtype=np.float32):
     """Accelerated proximal gradient (FISTA), solvers/APGD.cpp:34-102.
     Returns (x, mu, |grad|^2 history)."""
     if mu is None or mu <= 0:
-        mu = 0.45 / power_iterations(A, At, domain_size, power_iters)
-    m = np.float32(mu)
-    x = np.zeros(domain_size, np.float32) if x0 is None else _f(x0).copy()
+        mu = 0.45 / power_iterations(A, At, domain_size, power_iters, dtype)
+    _f = _caster(dtype)
+    m = dtype(mu)
+    x = np.zeros(domain_size, dtype) if x0 is None else _f(x0).copy()
     x_prev = x.copy()
     y = x.copy()
     t_prev = 1.0
@@ -152,9 +161,9 @@ def apgd(A, At, b, domain_size, iterations, x0=None, mu=None, epsilon=F32_EPS, k
     hist = []
     for _ in range(iterations):
         z = _f(y - m * grad)
-        x = prox(z, m, kind, lower, upper, sigma)
+        x = prox(z, m, kind, lower, upper, sigma, dtype)
         t = (1.0 + np.sqrt(1.0 + 4.0 * t_prev * t_prev)) / 2.0
-        coef = np.float32((t_prev - 1.0) / t)
+        coef = dtype((t_prev - 1.0) / t)
         y = _f(x + coef * _f(x - x_prev))
         x_prev = x
         t_prev = t
