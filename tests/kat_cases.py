@@ -18,15 +18,20 @@ def _rad(deg):
     return float(np.float32(np.float32(deg) * np.float32(PI_F)) / np.float32(180))
 
 
-def _pose2d(O, vol_dims, det_u, s2c, c2d, angle, cor=(0.0, 0.0)):
-    vo = [0.5 * v for v in vol_dims]
-    return O.geometry2d(s2c, c2d, angle, [1, 1], vo, [1, 1], [0.5 * det_u, 0.5], 0.0, cor)
+def _pose2d(O, vol_dims, det_u, s2c, c2d, angle, cor=(0.0, 0.0), spacing=1.0):
+    # VolumeData2D{Size2D, Spacing2D}: origin 0.5 * (size * spacing), core/StrongTypes.h:498-504
+    sp = float(np.float32(spacing))
+    vo = [0.5 * float(np.float32(v * sp)) for v in vol_dims]
+    return O.geometry2d(s2c, c2d, angle, [sp, sp], vo, [1, 1], [0.5 * det_u, 0.5], 0.0, cor)
 
 
-def _pose3d(O, vol_dims, det_uv, num_poses, s2c, c2d, gamma, beta=0.0, cor=(0.0, 0.0, 0.0)):
-    vo = [0.5 * v for v in vol_dims]
+def _pose3d(O, vol_dims, det_uv, num_poses, s2c, c2d, gamma, beta=0.0, cor=(0.0, 0.0, 0.0),
+            spacing=1.0):
+    sp = float(np.float32(spacing))
+    vo = [0.5 * float(np.float32(v * sp)) for v in vol_dims]
     so = [0.5 * det_uv[0], 0.5 * det_uv[1]]
-    return O.geometry3d(s2c, c2d, [1, 1, 1], vo, [1, 1], so, gamma, beta, 0.0, [0.0, 0.0], cor)
+    return O.geometry3d(s2c, c2d, [sp, sp, sp], vo, [1, 1], so, gamma, beta, 0.0, [0.0, 0.0],
+                        cor)
 
 
 def joseph_cases(O):
@@ -118,4 +123,54 @@ def siddon_cases(O):
                    0], np.float32).reshape(3, 3, 3)
     cases.append(dict(name="siddon_axis_aligned_3d", vol=(3, 3, 3), det=(1, 1, 6), poses=poses,
                       x=x, y_expect=np.full(6, 3.0), y=np.full(6, 3.0), bp_expect=bp))
+    return cases
+
+
+def voxel_cases(O):
+    """projectors/tests/test_BlobVoxelProjector.cpp:25-244: a centre voxel set to 1, projected
+    onto one, two or three detector pixels. Expected values are blob LUT weights at the stated
+    distances (op.blob(d) is the projected-blob LUT at d); tolerances are the reference's."""
+    lut, support, _ = O.voxel_lut("blob", 3)
+    lut2, support2, _ = O.voxel_lut("blob", 2)
+    w = lambda d: O.lut_lerp(lut, support, d)  # noqa: E731
+    cases = []
+    # :25-71 3D, 5^3 volume, one pixel, spacings 0.5/1/1.5, gamma = 0..356 (radians, as written)
+    for i in (1, 2, 3):
+        sp = i / 2.0
+        for ang in range(0, 360, 4):
+            poses = _pose3d(O, (5, 5, 5), (1, 1), 1, 100.0, 5.0, float(np.float32(ang)),
+                            spacing=sp)[None]
+            x = np.zeros((5, 5, 5), np.float32)
+            x[2, 2, 2] = 1
+            cases.append(dict(name="blob3d_1px_sp%g_g%d" % (sp, ang), dim=3, vol=(5, 5, 5),
+                              det=(1, 1, 1), poses=poses, x=x, y_expect=np.array([w(0.0)]),
+                              rtol=0.005))
+    # :74-121 2D, 5^2 volume, one pixel, spacings 0.5/1/1.5, Degree{0..356}
+    for i in (1, 2, 3):
+        sp = i / 2.0
+        for ang in range(0, 360, 4):
+            poses = _pose2d(O, (5, 5), 1, 100.0, 5.0, _rad(ang), spacing=sp)[None]
+            x = np.zeros((5, 5), np.float32)
+            x[2, 2] = 1
+            cases.append(dict(name="blob2d_1px_sp%g_a%d" % (sp, ang), dim=2, vol=(5, 5),
+                              det=(1, 1), poses=poses, x=x,
+                              y_expect=np.array([O.lut_lerp(lut2, support2, 0.0)]), rtol=1e-5))
+    # :124-170 2D, two pixels: both at distance 0.4761878 (1 % tolerance)
+    for ang in range(0, 360, 4):
+        poses = _pose2d(O, (5, 5), 2, 100.0, 5.0, _rad(ang))[None]
+        x = np.zeros((5, 5), np.float32)
+        x[2, 2] = 1
+        v = O.lut_lerp(lut2, support2, 0.4761878)
+        cases.append(dict(name="blob2d_2px_a%d" % ang, dim=2, vol=(5, 5), det=(2, 1),
+                          poses=poses, x=x, y_expect=np.array([v, v]), rtol=0.01))
+    # :173-244 2D, three pixels in 5 degree steps: centre weight(0), outer weight(0.95233786)
+    for ang in range(0, 360, 5):
+        poses = _pose2d(O, (5, 5), 3, 100.0, 5.0, _rad(ang))[None]
+        x = np.zeros((5, 5), np.float32)
+        x[2, 2] = 1
+        v0 = O.lut_lerp(lut2, support2, 0.0)
+        v1 = O.lut_lerp(lut2, support2, 0.95233786)
+        cases.append(dict(name="blob2d_3px_a%d" % ang, dim=2, vol=(5, 5), det=(3, 1),
+                          poses=poses, x=x, y_expect=np.array([v1, v0, v1]),
+                          rtol=np.array([0.01, 1e-5, 0.01])))
     return cases
