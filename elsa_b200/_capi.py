@@ -54,6 +54,7 @@ SIGNATURES = {
     "elsa_projector_apply_host": (_st, [_vp, _vp, _vp]),
     "elsa_projector_apply_adjoint_host": (_st, [_vp, _vp, _vp]),
     "elsa_dot": (_st, [_vp, _vp, _i64, _vp, _vp]),
+    "elsa_dot_no_alloc": (_st, [_vp, _vp, _i64, _vp, _vp]),
     "elsa_squared_l2_norm": (_st, [_vp, _i64, _vp, _vp]),
     "elsa_lincomb": (_st, [_f32, _vp, _f32, _vp, _vp, _i64, _vp]),
     "elsa_cgne_solve": (_st, [_vp, _vp, _vp, _i32, _i32, _vp]),

@@ -32,6 +32,7 @@ CUDA_UNITS = [
     ("joseph_tma.cu", []),
     ("siddon.cu", []),
     ("vecops.cu", []),
+    ("noalloc.cu", []),
     ("solvers.cu", []),
 ]
 CXX_UNITS = [

@@ -256,6 +256,12 @@ elsa_status elsa_dot(const float* x, const float* y, int64_t n, double* result, 
     });
 }
 
+elsa_status elsa_dot_no_alloc(const float* x, const float* y, int64_t n, double* result,
+                              void* stream)
+{
+    return guarded([&] { elsa_b200::dotNoAlloc(x, y, n, result, asStream(stream)); });
+}
+
 elsa_status elsa_squared_l2_norm(const float* x, int64_t n, double* result, void* stream)
 {
     return guarded([&] {

@@ -85,6 +85,9 @@ namespace elsa_b200
     void launchApgdStep(float* x, float* xPrev, float* y, const float* grad, float mu,
                         ProxSpec prox, int64_t n, const SolverScalars* S, double* partials,
                         cudaStream_t s);
+    // *result = <x, y> with the partial sums in a fixed device array instead of caller scratch
+    // (noalloc.cu; asynchronous, allocates nothing, n <= ELSA_DOT_NO_ALLOC_MAX_ELEMENTS).
+    void dotNoAlloc(const float* x, const float* y, int64_t n, double* result, cudaStream_t s);
     // S->tPrev = t; S->k = sum(partials); S->done |= (S->k <= eps)
     void launchApgdFinish(const double* partials, SolverScalars* S, double eps, cudaStream_t s);
 } // namespace elsa_b200

@@ -142,6 +142,21 @@ elsa_status elsa_projector_apply_adjoint_host(elsa_projector* projector, const f
  * (storage/reductions/DotProduct.h:24-47). */
 elsa_status elsa_dot(const float* x, const float* y, int64_t n, double* result, void* stream);
 
+/* Largest n accepted by elsa_dot_no_alloc. */
+#define ELSA_DOT_NO_ALLOC_MAX_ELEMENTS ((int64_t)67108864)
+
+/* *result = <x, y> like elsa_dot, but without allocating any device memory. No counterpart in
+ * the reference: it exists for callers that must not call cudaMalloc/cudaFree (those synchronize
+ * the whole device and stall other streams, and some hosts route all device memory through their
+ * own pool). The partial sums live in a fixed 128 KiB device array that the library keeps on
+ * every GPU that loads it, so n is limited to ELSA_DOT_NO_ALLOC_MAX_ELEMENTS (larger n returns
+ * ELSA_ERROR_INVALID_ARGUMENT). result is device memory; the call is asynchronous on `stream`.
+ * All calls on a device share the array: calls that may run at the same time on the GPU race and
+ * must be ordered on one stream. The first call on a device looks up the array's device address;
+ * make that first call before any stream capture. */
+elsa_status elsa_dot_no_alloc(const float* x, const float* y, int64_t n, double* result,
+                              void* stream);
+
 /* *result = |x|_2^2. Replaces DataContainer::squaredL2Norm (storage/reductions/L2.h:15-49). */
 elsa_status elsa_squared_l2_norm(const float* x, int64_t n, double* result, void* stream);
 
