@@ -23,6 +23,12 @@ STATUS_NAMES = {
 
 PROJECTOR_JOSEPH = 0
 PROJECTOR_SIDDON = 1
+PROJECTOR_BLOB = 2
+PROJECTOR_BSPLINE = 3
+PROJECTOR_PHASE_CONTRAST_BLOB = 4
+PROJECTOR_PHASE_CONTRAST_BSPLINE = 5
+FOOTPRINT_REFERENCE = 0
+FOOTPRINT_RECTANGLE = 1
 SOLVER_CGNE = 0
 SOLVER_CGLS = 1
 SOLVER_LANDWEBER = 2
@@ -55,6 +61,7 @@ SIGNATURES = {
     "elsa_projector_apply_adjoint_host": (_st, [_vp, _vp, _vp]),
     "elsa_dot": (_st, [_vp, _vp, _i64, _vp, _vp]),
     "elsa_dot_no_alloc": (_st, [_vp, _vp, _i64, _vp, _vp]),
+    "elsa_voxel_lut": (_st, [_i32, _i32, _vp, _i32, _i32, _vp, _vp]),
     "elsa_squared_l2_norm": (_st, [_vp, _i64, _vp, _vp]),
     "elsa_lincomb": (_st, [_f32, _vp, _f32, _vp, _vp, _i64, _vp]),
     "elsa_cgne_solve": (_st, [_vp, _vp, _vp, _i32, _i32, _vp]),
@@ -222,6 +229,18 @@ class Projector:
             self.close()
         except Exception:
             pass
+
+
+def voxel_lut(kind, dim, params=(), samples=100):
+    """(table, support) of a voxel projector kind (ProjectedBlob / ProjectedBSpline LUTs)."""
+    import numpy as _np
+    params = _np.ascontiguousarray(params, _np.float32)
+    out = _np.empty(int(samples), _np.float32)
+    sup = ctypes.c_float()
+    call("elsa_voxel_lut", int(kind), int(dim),
+         ctypes.c_void_p(params.ctypes.data if params.size else 0), int(params.size),
+         int(samples), ctypes.c_void_p(out.ctypes.data), ctypes.byref(sup))
+    return out, sup.value
 
 
 def power_iterations(projector, iterations=5, stream=None):

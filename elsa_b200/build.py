@@ -31,16 +31,18 @@ CUDA_UNITS = [
     ("joseph.cu", []),
     ("joseph_tma.cu", []),
     ("siddon.cu", []),
+    ("voxel.cu", ["--fmad=false"]),
     ("vecops.cu", []),
     ("noalloc.cu", []),
     ("solvers.cu", []),
 ]
 CXX_UNITS = [
     ("geometry.cpp", []),
+    ("luts.cpp", []),
     ("capi.cpp", []),
 ]
 HEADERS = ["internal.cuh", "raysetup.cuh", "joseph_tma.cuh", "projector.hpp", "geometry.hpp", "vecops.cuh",
-           "solvers.hpp"]
+           "solvers.hpp", "luts.hpp", "voxel.hpp"]
 
 
 def _stale(target, deps):

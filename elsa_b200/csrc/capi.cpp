@@ -13,6 +13,7 @@
 #include "internal.cuh"
 #include "projector.hpp"
 #include "solvers.hpp"
+#include "voxel.hpp"
 
 struct elsa_solver {
     std::unique_ptr<elsa_b200::SolverSession> impl;
@@ -68,6 +69,65 @@ namespace
         ELSA_CUDA(cudaGetDevice(&cur));
         if (cur != p->impl->device())
             ELSA_CUDA(cudaSetDevice(p->impl->device()));
+    }
+} // namespace
+
+namespace
+{
+    struct VoxelSpec {
+        elsa_b200::VoxelLut lut;
+        bool phase = false;
+        elsa_b200::FootprintMode mode = elsa_b200::FootprintMode::Reference;
+    };
+
+    // Parameters of the voxel projector kinds (elsa_b200.h): blob (radius, alpha, order, mode),
+    // B-spline (order, mode); the lookup table of the absorption or phase-contrast variant.
+    VoxelSpec voxelSpec(int32_t kind, int32_t dim, const float* params, int32_t numParams)
+    {
+        const bool blob = kind == ELSA_PROJECTOR_BLOB || kind == ELSA_PROJECTOR_PHASE_CONTRAST_BLOB;
+        const bool phase = kind == ELSA_PROJECTOR_PHASE_CONTRAST_BLOB ||
+                           kind == ELSA_PROJECTOR_PHASE_CONTRAST_BSPLINE;
+        if (!blob && kind != ELSA_PROJECTOR_BSPLINE && !phase)
+            throw elsa_b200::Error(ELSA_ERROR_NOT_SUPPORTED, "not a voxel projector kind");
+        if (dim != 2 && dim != 3)
+            throw elsa_b200::Error(ELSA_ERROR_INVALID_ARGUMENT,
+                                   "voxel projector: only supporting 2d/3d operations");
+        const int maxParams = blob ? 4 : 2;
+        if (numParams > maxParams)
+            throw elsa_b200::Error(ELSA_ERROR_INVALID_ARGUMENT,
+                                   "voxel projector: too many parameters");
+        auto param = [&](int i, float dflt) { return i < numParams ? params[i] : dflt; };
+        auto asInt = [](float v, const char* what) {
+            if (!(v == std::floor(v)) || v < 0.0f || v > 64.0f)
+                throw elsa_b200::Error(ELSA_ERROR_INVALID_ARGUMENT,
+                                       std::string("voxel projector: invalid ") + what);
+            return static_cast<int>(v);
+        };
+        const auto profile = !phase ? elsa_b200::LutProfile::Value
+                                    : (dim == 2 ? elsa_b200::LutProfile::Derivative
+                                                : elsa_b200::LutProfile::NormalizedGradient);
+        VoxelSpec spec;
+        spec.phase = phase;
+        int mode;
+        if (blob) {
+            const float radius = param(0, 2.0f);
+            const float alpha = param(1, 10.83f);
+            const int order = asInt(param(2, 2.0f), "blob order");
+            if (phase && order < 1)
+                throw elsa_b200::Error(ELSA_ERROR_INVALID_ARGUMENT,
+                                       "phase-contrast blob: order must be 1 or 2");
+            spec.lut = elsa_b200::blobLut(radius, alpha, order, profile);
+            mode = asInt(param(3, 0.0f), "footprint mode");
+        } else {
+            const int order = asInt(param(0, 2.0f), "B-spline order");
+            spec.lut = elsa_b200::bsplineLut(dim, order, profile);
+            mode = asInt(param(1, 0.0f), "footprint mode");
+        }
+        if (mode > 1)
+            throw elsa_b200::Error(ELSA_ERROR_INVALID_ARGUMENT,
+                                   "voxel projector: footprint mode must be 0 or 1");
+        spec.mode = static_cast<elsa_b200::FootprintMode>(mode);
+        return spec;
     }
 } // namespace
 
@@ -132,13 +192,13 @@ elsa_status elsa_projector_create(int32_t kind, int32_t dim, const int64_t* volD
                                   const int64_t* detDims, const float* poses, const float* params,
                                   int32_t numParams, elsa_projector** out)
 {
-    (void)params;
-    (void)numParams;
     return guarded([&] {
         require(out != nullptr, "elsa_projector_create: null output handle");
         *out = nullptr;
         require(dim == 2 || dim == 3, "JosephsMethod: only supporting 2d/3d operations");
         require(volDims && detDims && poses, "elsa_projector_create: null argument");
+        require(numParams >= 0 && (numParams == 0 || params != nullptr),
+                "elsa_projector_create: invalid parameter array");
         for (int i = 0; i < dim; ++i) {
             require(volDims[i] > 0 && volDims[i] < (1 << 20),
                     "elsa_projector_create: invalid volume size");
@@ -162,10 +222,46 @@ elsa_status elsa_projector_create(int32_t kind, int32_t dim, const int64_t* volD
         case ELSA_PROJECTOR_SIDDON:
             handle->impl = elsa_b200::makeSiddonProjector(vol, det, pv);
             break;
+        case ELSA_PROJECTOR_BLOB:
+        case ELSA_PROJECTOR_BSPLINE:
+        case ELSA_PROJECTOR_PHASE_CONTRAST_BLOB:
+        case ELSA_PROJECTOR_PHASE_CONTRAST_BSPLINE: {
+            const VoxelSpec spec = voxelSpec(kind, dim, params, numParams);
+            handle->impl = elsa_b200::makeVoxelProjector(kind, vol, det, pv, spec.lut,
+                                                         spec.phase, spec.mode);
+            break;
+        }
         default:
             throw elsa_b200::Error(ELSA_ERROR_NOT_SUPPORTED, "unknown projector kind");
         }
         *out = handle.release();
+    });
+}
+
+elsa_status elsa_voxel_lut(int32_t kind, int32_t dim, const float* params, int32_t numParams,
+                           int32_t samples, float* out, float* support)
+{
+    return guarded([&] {
+        require(out && support && samples >= 2 && samples <= 1 << 20,
+                "elsa_voxel_lut: invalid argument");
+        require(numParams >= 0 && (numParams == 0 || params != nullptr),
+                "elsa_voxel_lut: invalid parameter array");
+        VoxelSpec spec = voxelSpec(kind, dim, params, numParams);
+        if (samples != elsa_b200::kVoxelLutSize) {
+            // same profile with another sample count (the reference's Lut<data_t, N>)
+            const bool blob =
+                kind == ELSA_PROJECTOR_BLOB || kind == ELSA_PROJECTOR_PHASE_CONTRAST_BLOB;
+            const auto profile = !spec.phase ? elsa_b200::LutProfile::Value
+                                             : (dim == 2 ? elsa_b200::LutProfile::Derivative
+                                                         : elsa_b200::LutProfile::NormalizedGradient);
+            auto p = [&](int i, float d) { return i < numParams ? params[i] : d; };
+            spec.lut = blob ? elsa_b200::blobLut(p(0, 2.0f), p(1, 10.83f),
+                                                 static_cast<int>(p(2, 2.0f)), profile, samples)
+                            : elsa_b200::bsplineLut(dim, static_cast<int>(p(0, 2.0f)), profile,
+                                                    samples);
+        }
+        std::memcpy(out, spec.lut.values.data(), sizeof(float) * spec.lut.values.size());
+        *support = spec.lut.support;
     });
 }
 

@@ -1,0 +1,402 @@
+// Voxel-driven projectors (blob / B-spline basis functions, absorption and phase contrast).
+//
+// Reference semantics: projectors/VoxelComputation.h:20-185 (visitDetector, forwardVoxel,
+// backwardVoxel), projectors/VoxelProjector.cpp:30-114 and PhaseContrastProjector.cpp:30-119.
+// For every (voxel, pose) the voxel centre is projected onto the detector, centre
+// c = hnormalized(P [v + .5; 1]) - .5, scaling s = sdd / |ext [v + .5; 1]|, and every pixel in
+// [ceil(c - r s), floor(c + r s)] (clamped to the detector) receives the weight
+// lut(|c - pixel| / s) (phase contrast: times sgn(d0) in 2D, d0 in 3D).
+//
+// This unit is compiled with --fmad=false: the footprint and weight arithmetic rounds exactly
+// like elsa's float CPU path.
+//
+// Footprint loop. elsa's CPU loop (VoxelComputation.h:88-113) runs its outer loop over the u
+// extent and its inner loop over the v extent while stepping the pixel index along u, so for a
+// non-square clamped footprint it visits a sheared block instead of the footprint rectangle.
+// FootprintMode::Reference reproduces that loop (pixels it would address outside the view are
+// dropped); FootprintMode::Rectangle visits the rectangle. The two agree whenever the u and v
+// extents are equal.
+//
+// Adjoint: one thread per voxel gathers over poses and footprint pixels in the reference's order
+// (deterministic, bit-identical to the CPU loop). Forward: one CTA per (brick of voxels, pose)
+// splats its voxels into a shared-memory detector patch with shared atomics and adds the patch
+// to the sinogram with global atomics (the reference's CUDA path uses global atomics per pixel);
+// the order of the float additions is not fixed, so forward results agree with the CPU path to
+// rounding, not bit for bit.
+#include "luts.hpp"
+#include "projector.hpp"
+#include "solvers.hpp"
+#include "voxel.hpp"
+
+#include <algorithm>
+#include <climits>
+
+namespace elsa_b200
+{
+    namespace
+    {
+        constexpr int kVoxelThreads = 256;
+        constexpr int kPatchWords = 2304; // 9 KB shared detector patch (48 x 48 pixels)
+
+        struct VoxelParams {
+            int dim;
+            int weightKind; // 0 classic, 1 differential
+            int mode;       // FootprintMode
+            float radius;   // LUT support
+            int nu, nv;     // detector pixels per pose (nv = 1 in 2D)
+        };
+
+        struct Footprint {
+            float c0, c1, s;
+            int lo0, hi0, lo1, hi1;
+        };
+
+        // VoxelComputation.h:55-86 in float, sequential sums (no contraction in this unit).
+        template <int DIM>
+        __device__ __forceinline__ Footprint footprint(const float* __restrict__ pose, int ix,
+                                                       int iy, int iz, const VoxelParams& vp)
+        {
+            const float h0 = static_cast<float>(ix) + 0.5f;
+            const float h1 = static_cast<float>(iy) + 0.5f;
+            const float h2 = static_cast<float>(iz) + 0.5f;
+            Footprint f;
+            if (DIM == 3) {
+                const float* P = pose;
+                const float* E = pose + 27;
+                float p[3], e[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    float s = __ldg(P + 4 * i) * h0;
+                    s = s + __ldg(P + 4 * i + 1) * h1;
+                    s = s + __ldg(P + 4 * i + 2) * h2;
+                    s = s + __ldg(P + 4 * i + 3) * 1.0f;
+                    p[i] = s;
+                    float t = __ldg(E + 4 * i) * h0;
+                    t = t + __ldg(E + 4 * i + 1) * h1;
+                    t = t + __ldg(E + 4 * i + 2) * h2;
+                    t = t + __ldg(E + 4 * i + 3) * 1.0f;
+                    e[i] = t;
+                }
+                f.c0 = p[0] / p[2] - 0.5f;
+                f.c1 = p[1] / p[2] - 0.5f;
+                float n2 = e[0] * e[0];
+                n2 = n2 + e[1] * e[1];
+                n2 = n2 + e[2] * e[2];
+                f.s = __ldg(pose + 39) / sqrtf(n2);
+            } else {
+                const float* P = pose;
+                const float* E = pose + 27;
+                float p[2], e[2];
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    float s = __ldg(P + 3 * i) * h0;
+                    s = s + __ldg(P + 3 * i + 1) * h1;
+                    s = s + __ldg(P + 3 * i + 2) * 1.0f;
+                    p[i] = s;
+                    float t = __ldg(E + 3 * i) * h0;
+                    t = t + __ldg(E + 3 * i + 1) * h1;
+                    t = t + __ldg(E + 3 * i + 2) * 1.0f;
+                    e[i] = t;
+                }
+                f.c0 = p[0] / p[1] - 0.5f;
+                f.c1 = 0.0f;
+                float n2 = e[0] * e[0];
+                n2 = n2 + e[1] * e[1];
+                f.s = __ldg(pose + 39) / sqrtf(n2);
+            }
+            // clamping in float first keeps the integer conversion in range for voxels that
+            // project far off the detector (same result as clamping the integers)
+            const float r = f.s * vp.radius;
+            f.lo0 = static_cast<int>(fmaxf(ceilf(f.c0 - r), 0.0f));
+            f.hi0 = static_cast<int>(fminf(floorf(f.c0 + r), static_cast<float>(vp.nu - 1)));
+            if (DIM == 3) {
+                f.lo1 = static_cast<int>(fmaxf(ceilf(f.c1 - r), 0.0f));
+                f.hi1 = static_cast<int>(fminf(floorf(f.c1 + r), static_cast<float>(vp.nv - 1)));
+            } else {
+                f.lo1 = f.hi1 = 0;
+            }
+            return f;
+        }
+
+        // Lut::operator()(float), Luts.hpp:61-80, on a table in shared memory.
+        __device__ __forceinline__ float lutAt(const float* lut, float support, float distance)
+        {
+            const float index = (distance / support) * static_cast<float>(kVoxelLutSize - 1);
+            if (index < 0.0f || index > static_cast<float>(kVoxelLutSize - 1))
+                return 0.0f;
+            const int a = static_cast<int>(floorf(index));
+            const int b = static_cast<int>(ceilf(index));
+            const float fa = lut[a], fb = lut[b];
+            const float t = index - static_cast<float>(a);
+            return t * fb + (1.0f - t) * fa;
+        }
+
+        template <int DIM>
+        __device__ __forceinline__ float voxelWeight(const float* lut, const VoxelParams& vp,
+                                                     float d0, float d1)
+        {
+            float n2 = d0 * d0;
+            if (DIM == 3)
+                n2 = n2 + d1 * d1;
+            const float v = lutAt(lut, vp.radius, sqrtf(n2));
+            if (vp.weightKind == 0)
+                return v;
+            if (DIM == 2)
+                return v * static_cast<float>((0.0f < d0) - (d0 < 0.0f));
+            return v * d0;
+        }
+
+        // Visits the footprint pixels of one voxel in the reference's order; fn(linear pixel
+        // index within the pose, d0, d1).
+        template <int DIM, class Fn>
+        __device__ __forceinline__ void visitFootprint(const Footprint& f, const VoxelParams& vp,
+                                                       Fn fn)
+        {
+            if (DIM == 2) {
+                for (int u = f.lo0; u <= f.hi0; ++u)
+                    fn(u, (f.c0 - static_cast<float>(u)) / f.s, 0.0f);
+                return;
+            }
+            const int ext0 = f.hi0 - f.lo0 + 1, ext1 = f.hi1 - f.lo1 + 1;
+            if (ext0 <= 0 || ext1 <= 0)
+                return;
+            const bool ref = vp.mode == static_cast<int>(FootprintMode::Reference);
+            const int rows = ref ? ext0 : ext1;
+            const int cols = ref ? ext1 : ext0;
+            const int64_t npix = static_cast<int64_t>(vp.nu) * vp.nv;
+            int64_t lin = static_cast<int64_t>(f.lo1) * vp.nu + f.lo0;
+            float cur0 = static_cast<float>(f.lo0), cur1 = static_cast<float>(f.lo1);
+            for (int r = 0; r < rows; ++r) {
+                for (int c = 0; c < cols; ++c) {
+                    if (lin >= 0 && lin < npix)
+                        fn(lin, (f.c0 - cur0) / f.s, (f.c1 - cur1) / f.s);
+                    lin += 1;
+                    cur0 = cur0 + 1.0f;
+                }
+                lin += vp.nu - ext0;
+                cur0 = cur0 - static_cast<float>(ext0);
+                cur1 = cur1 + 1.0f;
+            }
+        }
+
+        // Adjoint: x[v] = sum over poses and footprint pixels of w * y[pixel], in the reference's
+        // order (VoxelComputation.h:152-183). One thread per voxel, x fastest within a block.
+        template <int DIM>
+        __global__ void __launch_bounds__(kVoxelThreads)
+            voxelAdjointKernel(const float* __restrict__ poses, int np,
+                               const float* __restrict__ lutIn, VoxelParams vp, VolumeShape vol,
+                               const float* __restrict__ y, float* __restrict__ x)
+        {
+            __shared__ float lut[kVoxelLutSize];
+            for (int i = threadIdx.x; i < kVoxelLutSize; i += blockDim.x)
+                lut[i] = lutIn[i];
+            __syncthreads();
+            const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
+            const int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (v >= nvox)
+                return;
+            const int ix = static_cast<int>(v % vol.n[0]);
+            const int iy = static_cast<int>((v / vol.n[0]) % vol.n[1]);
+            const int iz = DIM == 3 ? static_cast<int>(v / (static_cast<int64_t>(vol.n[0]) *
+                                                            vol.n[1]))
+                                    : 0;
+            const int64_t npix = static_cast<int64_t>(vp.nu) * vp.nv;
+            float acc = 0.0f;
+            for (int p = 0; p < np; ++p) {
+                const Footprint f = footprint<DIM>(poses + static_cast<int64_t>(p) * 40, ix, iy,
+                                                   iz, vp);
+                const float* view = y + p * npix;
+                visitFootprint<DIM>(f, vp, [&](int64_t pix, float d0, float d1) {
+                    const float w = voxelWeight<DIM>(lut, vp, d0, d1);
+                    acc = acc + w * __ldg(view + pix);
+                });
+            }
+            x[v] = acc;
+        }
+
+        // Bounding box (u0, u1, v0, v1) of the pixels a footprint visits; false when the visit
+        // wraps across detector rows (reference loop with a sheared block), which the patch
+        // cannot hold.
+        template <int DIM>
+        __device__ __forceinline__ bool visitBox(const Footprint& f, const VoxelParams& vp,
+                                                 int& u0, int& u1, int& v0, int& v1)
+        {
+            const int ext0 = f.hi0 - f.lo0 + 1, ext1 = f.hi1 - f.lo1 + 1;
+            if (DIM == 2 || vp.mode != static_cast<int>(FootprintMode::Reference) ||
+                ext0 == ext1) {
+                u0 = f.lo0, u1 = f.hi0, v0 = f.lo1, v1 = f.hi1;
+                return true;
+            }
+            // rows r = 0 .. ext0-1 start at u = lo0 + r * (ext1 - ext0) and span ext1 pixels
+            const int shift = (ext0 - 1) * (ext1 - ext0);
+            u0 = f.lo0 + min(0, shift);
+            u1 = f.lo0 + max(0, shift) + ext1 - 1;
+            v0 = f.lo1;
+            v1 = min(f.lo1 + ext0 - 1, vp.nv - 1);
+            return u0 >= 0 && u1 < vp.nu;
+        }
+
+        // Forward: one CTA per (brick of voxels, pose). Voxels splat into a shared patch of the
+        // detector (shared atomics); the patch is added to the sinogram with global atomics.
+        // Voxels whose footprint leaves the patch add to the sinogram directly.
+        template <int DIM, int BX, int BY, int BZ>
+        __global__ void __launch_bounds__(kVoxelThreads)
+            voxelForwardKernel(const float* __restrict__ poses, const float* __restrict__ lutIn,
+                               VoxelParams vp, VolumeShape vol, int3 nBricks,
+                               const float* __restrict__ x, float* __restrict__ y)
+        {
+            static_assert(BX * BY * BZ == kVoxelThreads, "one thread per brick voxel");
+            __shared__ float lut[kVoxelLutSize];
+            __shared__ float patch[kPatchWords];
+            __shared__ int box[4]; // u0, -u1, v0, -v1 (atomicMin on all four)
+            const int p = blockIdx.y;
+            const int b = blockIdx.x;
+            const int bx = b % nBricks.x, by = (b / nBricks.x) % nBricks.y,
+                      bz = b / (nBricks.x * nBricks.y);
+            const int tx = threadIdx.x % BX, ty = (threadIdx.x / BX) % BY,
+                      tz = threadIdx.x / (BX * BY);
+            const int ix = bx * BX + tx, iy = by * BY + ty, iz = bz * BZ + tz;
+            for (int i = threadIdx.x; i < kVoxelLutSize; i += blockDim.x)
+                lut[i] = lutIn[i];
+            if (threadIdx.x < 4)
+                box[threadIdx.x] = INT_MAX;
+            __syncthreads();
+
+            bool active = ix < vol.n[0] && iy < vol.n[1] && (DIM == 2 || iz < vol.n[2]);
+            float xv = 0.0f;
+            Footprint f{};
+            int u0 = 0, u1 = -1, v0 = 0, v1 = -1;
+            bool boxed = false;
+            if (active) {
+                xv = __ldg(x + ix + static_cast<int64_t>(vol.n[0]) *
+                                        (iy + static_cast<int64_t>(vol.n[1]) * iz));
+                active = xv != 0.0f;
+            }
+            if (active) {
+                f = footprint<DIM>(poses + static_cast<int64_t>(p) * 40, ix, iy, iz, vp);
+                active = f.lo0 <= f.hi0 && f.lo1 <= f.hi1;
+            }
+            if (active) {
+                boxed = visitBox<DIM>(f, vp, u0, u1, v0, v1) && u0 <= u1 && v0 <= v1;
+                if (boxed) {
+                    atomicMin(&box[0], u0);
+                    atomicMin(&box[1], -u1);
+                    atomicMin(&box[2], v0);
+                    atomicMin(&box[3], -v1);
+                }
+            }
+            __syncthreads();
+            const int bu0 = box[0], bu1 = -box[1], bv0 = box[2], bv1 = -box[3];
+            const int pw = bu1 - bu0 + 1, ph = bv1 - bv0 + 1;
+            const bool usePatch = bu0 != INT_MAX && pw > 0 && ph > 0 &&
+                                  static_cast<int64_t>(pw) * ph <= kPatchWords;
+            float* view = y + static_cast<int64_t>(p) * vp.nu * vp.nv;
+            if (usePatch) {
+                for (int i = threadIdx.x; i < pw * ph; i += blockDim.x)
+                    patch[i] = 0.0f;
+            }
+            __syncthreads();
+            if (active) {
+                const bool toPatch = usePatch && boxed;
+                visitFootprint<DIM>(f, vp, [&](int64_t pix, float d0, float d1) {
+                    const float w = voxelWeight<DIM>(lut, vp, d0, d1);
+                    const float c = xv * w;
+                    if (toPatch) {
+                        const int pu = static_cast<int>(pix % vp.nu) - bu0;
+                        const int pv = static_cast<int>(pix / vp.nu) - bv0;
+                        atomicAdd(&patch[pv * pw + pu], c);
+                    } else {
+                        atomicAdd(view + pix, c);
+                    }
+                });
+            }
+            if (usePatch) {
+                __syncthreads();
+                for (int i = threadIdx.x; i < pw * ph; i += blockDim.x) {
+                    const float v = patch[i];
+                    if (v != 0.0f)
+                        atomicAdd(view + static_cast<int64_t>(bv0 + i / pw) * vp.nu + bu0 + i % pw,
+                                  v);
+                }
+            }
+        }
+
+        template <int DIM>
+        class VoxelProjector final : public Projector
+        {
+        public:
+            VoxelProjector(int kind, const VolumeShape& vol, const DetectorShape& det,
+                           const std::vector<PoseRecord>& poses, const VoxelLut& lut,
+                           int weightKind, FootprintMode mode)
+                : Projector(kind, vol, det, poses), lut_(sizeof(float) * kVoxelLutSize)
+            {
+                if (static_cast<int>(lut.values.size()) != kVoxelLutSize)
+                    throw Error(ELSA_ERROR_LOGIC, "voxel projector: lookup table size");
+                ELSA_CUDA(cudaMemcpy(lut_.as<float>(), lut.values.data(),
+                                     sizeof(float) * kVoxelLutSize, cudaMemcpyHostToDevice));
+                vp_.dim = DIM;
+                vp_.weightKind = weightKind;
+                vp_.mode = static_cast<int>(mode);
+                vp_.radius = lut.support;
+                vp_.nu = det.nu;
+                vp_.nv = det.nv;
+                nBricks_ = make_int3((vol.n[0] + kBX - 1) / kBX, (vol.n[1] + kBY - 1) / kBY,
+                                     (vol.n[2] + kBZ - 1) / kBZ);
+                if (det.np > 65535)
+                    throw Error(ELSA_ERROR_NOT_SUPPORTED, "voxel projector: at most 65535 poses");
+            }
+
+            void forward(const float* x, float* y, cudaStream_t s) override
+            {
+                ELSA_CUDA(cudaMemsetAsync(y, 0, sizeof(float) * rangeSize_, s));
+                const dim3 grid(static_cast<unsigned>(nBricks_.x * nBricks_.y * nBricks_.z),
+                                static_cast<unsigned>(det_.np));
+                voxelForwardKernel<DIM, kBX, kBY, kBZ><<<grid, kVoxelThreads, 0, s>>>(
+                    dPoses_, lut_.as<float>(), vp_, vol_, nBricks_, x, y);
+                ELSA_LAUNCH_CHECK("voxelForwardKernel");
+            }
+
+            void adjoint(const float* y, float* x, cudaStream_t s) override
+            {
+                const unsigned blocks =
+                    static_cast<unsigned>((domainSize_ + kVoxelThreads - 1) / kVoxelThreads);
+                voxelAdjointKernel<DIM><<<blocks, kVoxelThreads, 0, s>>>(
+                    dPoses_, det_.np, lut_.as<float>(), vp_, vol_, y, x);
+                ELSA_LAUNCH_CHECK("voxelAdjointKernel");
+            }
+
+            int64_t info(int key) const override
+            {
+                switch (key) {
+                case 1:
+                    return static_cast<int64_t>(nBricks_.x) * nBricks_.y * nBricks_.z;
+                case 5:
+                    return vp_.mode;
+                default:
+                    return -1;
+                }
+            }
+
+        private:
+            // forward bricks: 8 x 8 x 4 voxels in 3D, 16 x 16 in 2D (one thread per voxel)
+            static constexpr int kBX = DIM == 3 ? 8 : 16;
+            static constexpr int kBY = DIM == 3 ? 8 : 16;
+            static constexpr int kBZ = DIM == 3 ? 4 : 1;
+            DeviceBuffer lut_;
+            VoxelParams vp_{};
+            int3 nBricks_{};
+        };
+    } // namespace
+
+    std::unique_ptr<Projector> makeVoxelProjector(int kind, const VolumeShape& vol,
+                                                  const DetectorShape& det,
+                                                  const std::vector<PoseRecord>& poses,
+                                                  const VoxelLut& lut, bool phaseContrast,
+                                                  FootprintMode mode)
+    {
+        const int wk = phaseContrast ? 1 : 0;
+        if (vol.dim == 3)
+            return std::make_unique<VoxelProjector<3>>(kind, vol, det, poses, lut, wk, mode);
+        return std::make_unique<VoxelProjector<2>>(kind, vol, det, poses, lut, wk, mode);
+    }
+} // namespace elsa_b200

@@ -45,8 +45,26 @@ typedef enum elsa_projector_kind {
     ELSA_PROJECTOR_JOSEPH = 0,
     /* SiddonsMethod / SiddonsMethodCUDA, projectors/SiddonsMethod.cpp:76-124 with
      * projectors/TraverseAABB.cpp:6-184 */
-    ELSA_PROJECTOR_SIDDON = 1
+    ELSA_PROJECTOR_SIDDON = 1,
+    /* BlobVoxelProjector / BlobVoxelProjectorCUDA, projectors/VoxelProjector.cpp:7-52.
+     * params: radius (2), alpha (10.83), order (2), footprint mode (0). */
+    ELSA_PROJECTOR_BLOB = 2,
+    /* BSplineVoxelProjector / BSplineVoxelProjectorCUDA, projectors/VoxelProjector.cpp:69-114.
+     * params: order (2), footprint mode (0). */
+    ELSA_PROJECTOR_BSPLINE = 3,
+    /* PhaseContrastBlobVoxelProjector(CUDA), projectors/PhaseContrastProjector.cpp:6-52.
+     * params as ELSA_PROJECTOR_BLOB. */
+    ELSA_PROJECTOR_PHASE_CONTRAST_BLOB = 4,
+    /* PhaseContrastBSplineVoxelProjector(CUDA), projectors/PhaseContrastProjector.cpp:72-119.
+     * params as ELSA_PROJECTOR_BSPLINE. */
+    ELSA_PROJECTOR_PHASE_CONTRAST_BSPLINE = 5
 } elsa_projector_kind;
+
+/* Footprint mode of the voxel projectors (last parameter): 0 visits the pixels of each voxel
+ * footprint exactly as elsa's CPU loop does (projectors/VoxelComputation.h:88-113, which visits a
+ * sheared block when the clamped footprint is not square); 1 visits the footprint rectangle. */
+#define ELSA_FOOTPRINT_REFERENCE 0
+#define ELSA_FOOTPRINT_RECTANGLE 1
 
 typedef struct elsa_projector elsa_projector;
 
@@ -164,6 +182,14 @@ elsa_status elsa_squared_l2_norm(const float* x, int64_t n, double* result, void
  * (storage/transforms/Lincomb.h:28-33). */
 elsa_status elsa_lincomb(float a, const float* x, float b, const float* y, float* out, int64_t n,
                          void* stream);
+
+/* Lookup table (100 samples on [0, support]) that a voxel projector kind uses for dimension dim:
+ * the projected blob / B-spline, its derivative (2D phase contrast) or its derivative / s (3D
+ * phase contrast). params as for elsa_projector_create. Replaces ProjectedBlob::get_lut,
+ * get_derivative_lut, get_normalized_gradient_lut (projectors/Blobs.h:233-300) and the
+ * ProjectedBSpline ones (projectors/BSplines.h:132-200). out: host array of `samples` floats. */
+elsa_status elsa_voxel_lut(int32_t kind, int32_t dim, const float* params, int32_t num_params,
+                           int32_t samples, float* out, float* support);
 
 /* ---------------------------------------------------------------------------------------------
  * Solvers (device-resident iterations, float64 inner products)
