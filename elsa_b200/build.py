@@ -25,6 +25,9 @@ CUDA_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall",
              "-I" + os.path.join(ROOT, "include"), "-I/usr/local/cuda/include"]
 
+# Extra nvcc flags for experiments (e.g. -DELSA_ADJ_NW=2); empty for the product build.
+CUDA_FLAGS += os.environ.get("ELSA_B200_NVCC_EXTRA", "").split()
+
 # (source, extra flags)
 CUDA_UNITS = [
     ("raysetup.cu", ["--fmad=false"]),
