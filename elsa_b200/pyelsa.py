@@ -1,0 +1,404 @@
+"""pyelsa-style Python API over the elsa_b200 C ABI.
+
+The names, arguments and defaults follow elsa's Python bindings (pyelsa/pyelsa/bind_core.cpp,
+bind_generators.cpp, bind_projectors_cuda.cpp, bind_solvers.cpp, bind_proximal_operators.cpp), so
+that a pyelsa script runs with ``import elsa_b200.pyelsa as elsa``:
+
+    vol = elsa.VolumeDescriptor([256, 256, 256])
+    sino = elsa.CircleTrajectoryGenerator.createTrajectory(360, vol, 360, 2560, 640,
+                                                           detectorSize=[384, 384])
+    A = elsa.JosephsMethodCUDA(vol, sino)
+    b = A.apply(phantom)                       # numpy (F-order, x fastest) or DataContainer
+    x = elsa.CGNE(A, b).solve(30)
+    np.asarray(x)                              # back to numpy, shape (256, 256, 256)
+
+Arrays follow elsa's layout: the first index is x (fastest), i.e. Fortran order, as pyelsa's
+buffer protocol does. Data lives on the GPU (torch tensors on cuda:0); every projector and solver
+call runs the native CUDA kernels. The float64 instantiations (…CUDAd) are not provided: the
+device path computes in float32 with float64 inner products.
+"""
+import math
+
+import numpy as np
+
+from . import _capi
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("elsa_b200.pyelsa needs a CUDA device")
+    return torch
+
+
+# ---- descriptors (core/Descriptors) ----------------------------------------------------------------
+
+class DataDescriptor:
+    """Shape and spacing of a data container (core/Descriptors/DataDescriptor.h)."""
+
+    def __init__(self, size, spacing=None):
+        self._size = np.asarray(size, np.int64).ravel()
+        if self._size.size < 1 or np.any(self._size <= 0):
+            raise _capi.InvalidArgumentError(1, "DataDescriptor: invalid size")
+        sp = np.ones(self._size.size) if spacing is None else np.asarray(spacing, np.float64)
+        if sp.size != self._size.size or np.any(sp <= 0):
+            raise _capi.InvalidArgumentError(1, "DataDescriptor: invalid spacing")
+        self._spacing = sp.astype(np.float32)
+
+    def getNumberOfDimensions(self):
+        return int(self._size.size)
+
+    def getNumberOfCoefficients(self):
+        return int(np.prod(self._size))
+
+    def getNumberOfCoefficientsPerDimension(self):
+        return self._size.copy()
+
+    def getSpacingPerDimension(self):
+        return self._spacing.astype(np.float64)
+
+    def getLocationOfOrigin(self):
+        # 0.5 * (size * spacing), DataDescriptor.cpp:21,49
+        return (0.5 * (self._size.astype(np.float32) * self._spacing)).astype(np.float64)
+
+    @property
+    def shape(self):
+        return tuple(int(v) for v in self._size)
+
+    def __eq__(self, other):
+        return (isinstance(other, DataDescriptor) and np.array_equal(self._size, other._size)
+                and np.array_equal(self._spacing, other._spacing))
+
+
+class VolumeDescriptor(DataDescriptor):
+    """core/Descriptors/VolumeDescriptor.h"""
+
+
+class PlanarDetectorDescriptor(DataDescriptor):
+    """Flat-panel detector with one geometry (pose record) per projection
+    (core/Descriptors/PlanarDetectorDescriptor.h). The last dimension counts the poses."""
+
+    def __init__(self, size, poses, spacing=None):
+        super().__init__(size, spacing)
+        self.poses = np.ascontiguousarray(poses, np.float32).reshape(-1, _capi.POSE_FLOATS)
+        if self.poses.shape[0] != self._size[-1]:
+            raise _capi.InvalidArgumentError(1, "PlanarDetectorDescriptor: poses != last dim")
+
+    def getNumberOfGeometryPoses(self):
+        return int(self.poses.shape[0])
+
+
+class CircleTrajectoryGenerator:
+    """generators/CircleTrajectoryGenerator.cpp:9-24."""
+
+    @staticmethod
+    def createTrajectory(numberOfPoses, volumeDescriptor, arcDegrees, sourceToCenter,
+                         centerToDetector, principalPointOffset=None, centerOfRotOffset=None,
+                         detectorSize=None, detectorSpacing=None):
+        if principalPointOffset is not None or centerOfRotOffset is not None:
+            raise NotImplementedError("createTrajectory: principal point / centre of rotation "
+                                      "offsets are not supported; build poses with pose_2d / "
+                                      "pose_3d instead")
+        vol = volumeDescriptor
+        poses, det = _capi.circle_trajectory(vol.shape, int(numberOfPoses), float(arcDegrees),
+                                             float(sourceToCenter), float(centerToDetector),
+                                             detectorSize, vol.getSpacingPerDimension(),
+                                             detectorSpacing)
+        dim = vol.getNumberOfDimensions()
+        spacing = list(detectorSpacing) if detectorSpacing is not None else \
+            list(vol.getSpacingPerDimension()[:dim - 1])
+        return PlanarDetectorDescriptor(det, poses, spacing + [1.0])
+
+
+# ---- DataContainer ---------------------------------------------------------------------------------
+
+class DataContainer:
+    """A float32 device buffer with a descriptor (core/DataContainer.h). Built from a numpy array
+    (x fastest: Fortran order for an array of shape (nx, ny[, nz])) or a flat torch tensor."""
+
+    def __init__(self, data, descriptor=None):
+        torch = _torch()
+        if isinstance(data, DataContainer):
+            descriptor = descriptor or data.descriptor
+            self.tensor = data.tensor.clone()
+        elif hasattr(data, "is_cuda") or hasattr(data, "device"):
+            t = data.detach().to(device="cuda", dtype=torch.float32).contiguous().reshape(-1)
+            self.tensor = t
+            if descriptor is None:
+                raise _capi.InvalidArgumentError(1, "DataContainer: a tensor needs a descriptor")
+        else:
+            arr = np.asarray(data, dtype=np.float32)
+            if descriptor is None:
+                descriptor = DataDescriptor(arr.shape)
+            flat = np.ascontiguousarray(arr.reshape(-1, order="F") if arr.ndim > 1 else
+                                        arr.reshape(-1))
+            self.tensor = torch.from_numpy(flat).cuda()
+        if self.tensor.numel() != descriptor.getNumberOfCoefficients():
+            raise _capi.InvalidArgumentError(1, "DataContainer: size does not match descriptor")
+        self.descriptor = descriptor
+
+    @classmethod
+    def zeros(cls, descriptor):
+        torch = _torch()
+        obj = cls.__new__(cls)
+        obj.tensor = torch.zeros(descriptor.getNumberOfCoefficients(), dtype=torch.float32,
+                                 device="cuda")
+        obj.descriptor = descriptor
+        return obj
+
+    def getDataDescriptor(self):
+        return self.descriptor
+
+    def getSize(self):
+        return self.tensor.numel()
+
+    def __array__(self, dtype=None, copy=None):
+        arr = self.tensor.cpu().numpy().reshape(self.descriptor.shape, order="F")
+        return arr.astype(dtype) if dtype is not None else arr
+
+    def _ptr(self):
+        return self.tensor.data_ptr()
+
+    def _stream(self):
+        return _torch().cuda.current_stream().cuda_stream
+
+    def dot(self, other):
+        """<self, other> with float64 accumulation (elsa_dot)."""
+        import ctypes
+        torch = _torch()
+        o = _as_dc(other, self.descriptor)
+        res = torch.empty(1, dtype=torch.float64, device="cuda")
+        _capi.call("elsa_dot", ctypes.c_void_p(self._ptr()), ctypes.c_void_p(o._ptr()),
+                   self.getSize(), ctypes.c_void_p(res.data_ptr()),
+                   ctypes.c_void_p(self._stream()))
+        return float(res.item())
+
+    def squaredL2Norm(self):
+        import ctypes
+        torch = _torch()
+        res = torch.empty(1, dtype=torch.float64, device="cuda")
+        _capi.call("elsa_squared_l2_norm", ctypes.c_void_p(self._ptr()), self.getSize(),
+                   ctypes.c_void_p(res.data_ptr()), ctypes.c_void_p(self._stream()))
+        return float(res.item())
+
+    def l2Norm(self):
+        return math.sqrt(self.squaredL2Norm())
+
+    def _lincomb(self, a, other, b):
+        """a * self + b * other (elsa_lincomb, core/DataContainer.cpp:1075-1108)."""
+        import ctypes
+        o = _as_dc(other, self.descriptor) if other is not None else self
+        out = DataContainer.zeros(self.descriptor)
+        _capi.call("elsa_lincomb", ctypes.c_float(a), ctypes.c_void_p(self._ptr()),
+                   ctypes.c_float(b), ctypes.c_void_p(o._ptr()), ctypes.c_void_p(out._ptr()),
+                   self.getSize(), ctypes.c_void_p(self._stream()))
+        return out
+
+    def __add__(self, other):
+        return self._lincomb(1.0, other, 1.0)
+
+    def __sub__(self, other):
+        return self._lincomb(1.0, other, -1.0)
+
+    def __mul__(self, other):
+        if isinstance(other, (int, float, np.floating)):
+            return self._lincomb(float(other), None, 0.0)
+        # element-wise product: a convenience outside the projector / solver path
+        obj = DataContainer.__new__(DataContainer)
+        obj.tensor = self.tensor * _as_dc(other, self.descriptor).tensor
+        obj.descriptor = self.descriptor
+        return obj
+
+    __rmul__ = __mul__
+
+
+def _as_dc(x, descriptor):
+    if isinstance(x, DataContainer):
+        if x.getSize() != descriptor.getNumberOfCoefficients():
+            raise _capi.InvalidArgumentError(1, "size does not match the operator")
+        return x
+    return DataContainer(x, descriptor)
+
+
+# ---- operators (core/LinearOperator.h, projectors_cuda/*) -------------------------------------------
+
+class LinearOperator:
+    """Base of the projectors: apply / applyAdjoint on DataContainers or numpy arrays."""
+
+    def __init__(self, kind, volumeDescriptor, detectorDescriptor, params=None):
+        if volumeDescriptor.getNumberOfDimensions() != \
+                detectorDescriptor.getNumberOfDimensions():
+            raise _capi.InvalidArgumentError(1, "domain and range dimension need to match")
+        if not isinstance(detectorDescriptor, PlanarDetectorDescriptor):
+            raise _capi.InvalidArgumentError(1, "range descriptor needs a geometry")
+        self._domain = volumeDescriptor
+        self._range = detectorDescriptor
+        self._op = _capi.Projector(kind, volumeDescriptor.shape, detectorDescriptor.shape,
+                                   detectorDescriptor.poses, params)
+
+    def getDomainDescriptor(self):
+        return self._domain
+
+    def getRangeDescriptor(self):
+        return self._range
+
+    @property
+    def native(self):
+        """The underlying elsa_b200.Projector (C ABI handle)."""
+        return self._op
+
+    def _stream(self):
+        return _torch().cuda.current_stream().cuda_stream
+
+    def apply(self, x, Ax=None):
+        x = _as_dc(x, self._domain)
+        out = Ax if Ax is not None else DataContainer.zeros(self._range)
+        self._op.apply_ptr(x._ptr(), _as_dc(out, self._range)._ptr(), self._stream())
+        return out
+
+    def applyAdjoint(self, y, Aty=None):
+        y = _as_dc(y, self._range)
+        out = Aty if Aty is not None else DataContainer.zeros(self._domain)
+        self._op.apply_adjoint_ptr(y._ptr(), _as_dc(out, self._domain)._ptr(), self._stream())
+        return out
+
+
+class JosephsMethodCUDA(LinearOperator):
+    """JosephsMethodCUDA(volume, detector, fast=True): the matched, deterministic adjoint is used
+    for both settings of `fast` (elsa's fast adjoint is an unmatched approximation)."""
+
+    def __init__(self, volumeDescriptor, detectorDescriptor, fast=True):
+        super().__init__(_capi.PROJECTOR_JOSEPH, volumeDescriptor, detectorDescriptor)
+
+
+class SiddonsMethodCUDA(LinearOperator):
+    def __init__(self, volumeDescriptor, detectorDescriptor):
+        super().__init__(_capi.PROJECTOR_SIDDON, volumeDescriptor, detectorDescriptor)
+
+
+class BlobVoxelProjectorCUDA(LinearOperator):
+    def __init__(self, volumeDescriptor, detectorDescriptor, radius=2.0, alpha=10.83, order=2,
+                 footprint=_capi.FOOTPRINT_REFERENCE):
+        super().__init__(_capi.PROJECTOR_BLOB, volumeDescriptor, detectorDescriptor,
+                         [radius, alpha, order, footprint])
+
+
+class BSplineVoxelProjectorCUDA(LinearOperator):
+    def __init__(self, volumeDescriptor, detectorDescriptor, order=2,
+                 footprint=_capi.FOOTPRINT_REFERENCE):
+        super().__init__(_capi.PROJECTOR_BSPLINE, volumeDescriptor, detectorDescriptor,
+                         [order, footprint])
+
+
+class PhaseContrastBlobVoxelProjectorCUDA(LinearOperator):
+    def __init__(self, volumeDescriptor, detectorDescriptor, radius=2.0, alpha=10.83, order=2,
+                 footprint=_capi.FOOTPRINT_REFERENCE):
+        super().__init__(_capi.PROJECTOR_PHASE_CONTRAST_BLOB, volumeDescriptor,
+                         detectorDescriptor, [radius, alpha, order, footprint])
+
+
+class PhaseContrastBSplineVoxelProjectorCUDA(LinearOperator):
+    def __init__(self, volumeDescriptor, detectorDescriptor, order=2,
+                 footprint=_capi.FOOTPRINT_REFERENCE):
+        super().__init__(_capi.PROJECTOR_PHASE_CONTRAST_BSPLINE, volumeDescriptor,
+                         detectorDescriptor, [order, footprint])
+
+
+# pyelsa aliases: the names without the CUDA suffix (CPU projectors in elsa) and the f-suffixed
+# float instantiations resolve to the same device operators
+JosephsMethod = JosephsMethodCUDAf = JosephsMethodCUDA
+SiddonsMethod = SiddonsMethodCUDAf = SiddonsMethodCUDA
+BlobVoxelProjector = BlobVoxelProjectorCUDAf = BlobVoxelProjectorCUDA
+BSplineVoxelProjector = BSplineVoxelProjectorCUDAf = BSplineVoxelProjectorCUDA
+PhaseContrastBlobVoxelProjector = PhaseContrastBlobVoxelProjectorCUDA
+PhaseContrastBSplineVoxelProjector = PhaseContrastBSplineVoxelProjectorCUDA
+
+
+# ---- proximal operators (proximal_operators/*) ------------------------------------------------------
+
+class ProximalIdentity:
+    params = (0.0, float("nan"), float("nan"), 1.0)
+
+
+class ProximalBoxConstraint:
+    def __init__(self, lower=None, upper=None):
+        self.params = (1.0, float("nan") if lower is None else float(lower),
+                       float("nan") if upper is None else float(upper), 1.0)
+
+
+class ProximalL1:
+    def __init__(self, sigma=1.0):
+        self.params = (2.0, float("nan"), float("nan"), float(sigma))
+
+
+# ---- solvers (solvers/*, bindings in pyelsa/pyelsa/bind_solvers.cpp) --------------------------------
+
+class _Solver:
+    _kind = None
+
+    def __init__(self, A, b):
+        self.A = A
+        self.b = _as_dc(b, A.getRangeDescriptor())
+        self.last = None  # the native session of the last solve (residual, timing)
+
+    def _params(self):
+        return ()
+
+    def solve(self, iterations, x0=None):
+        x = DataContainer.zeros(self.A.getDomainDescriptor()) if x0 is None else \
+            DataContainer(_as_dc(x0, self.A.getDomainDescriptor()))
+        s = self.A._stream()
+        self.last = _capi.Solver(self._kind, self.A.native, self.b._ptr(), x._ptr(),
+                                 use_x0=x0 is not None, stream=s, params=self._params())
+        self.last.iterate(int(iterations), s)
+        return x
+
+
+class CGNE(_Solver):
+    _kind = _capi.SOLVER_CGNE
+
+
+class CGLS(_Solver):
+    _kind = _capi.SOLVER_CGLS
+
+    def __init__(self, A, b, eps=0.0, tol=1e-4):
+        super().__init__(A, b)
+        self.eps, self.tol = float(eps), float(tol)
+
+    def _params(self):
+        return (self.eps, self.tol)
+
+
+class Landweber(_Solver):
+    _kind = _capi.SOLVER_LANDWEBER
+
+    def __init__(self, A, b, stepSize=None):
+        super().__init__(A, b)
+        self.stepSize = stepSize
+
+    def _params(self):
+        return (float(self.stepSize),) if self.stepSize is not None else ()
+
+
+class APGD(_Solver):
+    """APGD(A, b, prox, mu=None, eps=1e-6) (pyelsa's defaults, bind_solvers.cpp:222-228)."""
+    _kind = _capi.SOLVER_APGD
+
+    def __init__(self, A, b, prox=None, mu=None, eps=1e-6):
+        super().__init__(A, b)
+        self.prox = prox if prox is not None else ProximalIdentity()
+        self.mu, self.eps = mu, float(eps)
+
+    def _params(self):
+        kind, lo, hi, sigma = self.prox.params
+        return (float(self.mu) if self.mu is not None else 0.0, self.eps, kind, lo, hi, sigma)
+
+
+FISTA = APGD
+CGNEf, CGLSf, Landweberf, APGDf = CGNE, CGLS, Landweber, APGD
+
+
+def powerIterations(op, niters=5):
+    """Largest eigenvalue of op^T op (solvers/PowerIterations.cpp:10-27, applied to
+    adjoint(A) * A as elsa's solvers do)."""
+    return _capi.power_iterations(op.native, niters, op._stream())
