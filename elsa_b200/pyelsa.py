@@ -121,7 +121,7 @@ class DataContainer:
         if isinstance(data, DataContainer):
             descriptor = descriptor or data.descriptor
             self.tensor = data.tensor.clone()
-        elif hasattr(data, "is_cuda") or hasattr(data, "device"):
+        elif isinstance(data, torch.Tensor):
             t = data.detach().to(device="cuda", dtype=torch.float32).contiguous().reshape(-1)
             self.tensor = t
             if descriptor is None:
