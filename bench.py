@@ -33,8 +33,9 @@ METRIC = "3D cone-beam fwd+back GUPS and CG iters/s at 256^3; batched vs plain, 
 WORKLOAD = dict(workload="cone-beam Joseph CGNE, 256^3 volume, 360 views, 384x384 detector",
                 volume=[256, 256, 256], views=360, detector=[384, 384], source_to_center=2560,
                 center_to_detector=640, phantom="modified Shepp-Logan 3D")
-# kernels launched per CGNE iteration: forward, adjoint, dot (2), step, finish-norm, direction
-LAUNCHES_PER_STEP = 7
+# kernels launched per CGNE iteration besides the projections: dot (partials + finish), step,
+# finish-norm, direction (solvers.cu, cgneStep)
+VECTOR_LAUNCHES_PER_STEP = 5
 
 
 def _peaks():
@@ -267,9 +268,11 @@ def run_elsa(args):
                      "algorithmic_bytes_per_launch": bytes_per_pass,
                      "samples_per_launch": samples,
                      "compulsory_frac": round(compulsory / (dom_ms / 1e3) / 1e9 / peak, 5)},
-        "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+        "gpu_launches": (proj.info(6) + proj.info(7) + VECTOR_LAUNCHES_PER_STEP) * args.steps,
         "clocks": clock_info,
     }
+    if rank == 0 and world == 1 and not args.no_batched:
+        out["batched"] = batched_vs_plain(torch, elsa_b200, phantoms)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         gups, dt, cores = cpu_baseline_sample(args.cpu_views, vol, poses, det, x_true)
         out["cpu_baseline"] = {"value": round(gups, 5), "unit": "GUPS", "cores": cores,
@@ -280,6 +283,65 @@ def run_elsa(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out))
+
+
+def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, streams=8,
+                     seed=5):
+    """Many small independent reconstructions: one at a time (each solver's iterations enqueued
+    on one stream, one problem after the other) against elsa_solve_batch (every solver's
+    iterations as a CUDA graph, problems spread over concurrent streams). Seeded instances of the
+    batched workload with edges {64, 96, 128}, 60-180 views, a detector of 1.5 x edge; projector
+    and solver set-up is outside both timed regions."""
+    rng = np.random.default_rng(seed)
+    problems = []
+    for _ in range(instances):
+        n = int(rng.choice([64, 96, 128]))
+        views = int(rng.integers(60, 181))
+        vol = (n, n, n)
+        poses, det = elsa_b200.circle_trajectory(vol, views, 360, 10.0 * n, 2.5 * n,
+                                                 [int(1.5 * n), int(1.5 * n)])
+        proj = elsa_b200.Projector(elsa_b200.PROJECTOR_JOSEPH, vol, det, poses)
+        xt = torch.from_numpy(phantoms.modified_shepp_logan(vol).ravel()).cuda()
+        b = torch.empty(proj.range_size, dtype=torch.float32, device="cuda")
+        proj.apply_ptr(xt.data_ptr(), b.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        problems.append((proj, b))
+    torch.cuda.synchronize()
+
+    def make():
+        s = torch.cuda.current_stream().cuda_stream
+        xs, sols = [], []
+        for proj, b in problems:
+            x = torch.zeros(proj.domain_size, dtype=torch.float32, device="cuda")
+            sols.append(elsa_b200.Solver(elsa_b200.SOLVER_CGNE, proj, b.data_ptr(),
+                                         x.data_ptr(), stream=s))
+            xs.append(x)
+        torch.cuda.synchronize()
+        return xs, sols
+
+    xs, plain = make()
+    s = torch.cuda.current_stream().cuda_stream
+    for sol in plain:  # warm-up of every kernel shape
+        sol.iterate(1, s)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for sol in plain:
+        sol.iterate(iterations, s)
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    xs2, batch = make()
+    elsa_b200.solve_batch(batch, 1, streams)  # captures the one-iteration graphs (warm-up)
+    t0 = time.perf_counter()
+    elsa_b200.solve_batch(batch, iterations, streams)  # captures + runs the timed graphs
+    t_batch = time.perf_counter() - t0
+    for sol in plain + batch:
+        sol.close()
+    return {"instances": instances, "iterations": iterations, "streams": streams,
+            "workload": "seeded CGNE problems, edges {64, 96, 128}, 60-180 views, detector "
+                        "1.5 x edge, Joseph",
+            "plain_recon_per_s": round(instances / t_plain, 3),
+            "batched_recon_per_s": round(instances / t_batch, 3),
+            "speedup": round(t_plain / t_batch, 3),
+            "timing": "host wall clock around synchronized device work, graph capture included"}
 
 
 def run_reference(args):
@@ -327,6 +389,8 @@ def main():
     ap.add_argument("--cpu-views", type=int, default=4,
                     help="views per CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-vs-plain small-problem measurement")
     ap.add_argument("--size", type=int, default=256,
                     help="volume edge (profiling only; the benchmark workload is 256)")
     args = ap.parse_args()

@@ -9,7 +9,7 @@ from . import _capi  # noqa: F401
 from ._capi import (ElsaError, InvalidArgumentError, Projector, Solver,  # noqa: F401
                     voxel_lut, PROJECTOR_BLOB, PROJECTOR_BSPLINE, PROJECTOR_PHASE_CONTRAST_BLOB,
                     PROJECTOR_PHASE_CONTRAST_BSPLINE, FOOTPRINT_REFERENCE, FOOTPRINT_RECTANGLE,
-                    circle_trajectory, pose_2d, pose_3d, power_iterations, POSE_FLOATS,
+                    circle_trajectory, pose_2d, pose_3d, power_iterations, solve_batch, POSE_FLOATS,
                     PROJECTOR_JOSEPH, PROJECTOR_SIDDON, SOLVER_CGNE, SOLVER_CGLS,
                     SOLVER_LANDWEBER, SOLVER_APGD, PROX_IDENTITY, PROX_BOX, PROX_L1)
 
@@ -17,7 +17,7 @@ __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "voxel_lu
            "PROJECTOR_BLOB", "PROJECTOR_BSPLINE", "PROJECTOR_PHASE_CONTRAST_BLOB",
            "PROJECTOR_PHASE_CONTRAST_BSPLINE", "FOOTPRINT_REFERENCE", "FOOTPRINT_RECTANGLE",
            "circle_trajectory",
-           "pose_2d", "pose_3d", "power_iterations", "POSE_FLOATS", "PROJECTOR_JOSEPH",
+           "pose_2d", "pose_3d", "power_iterations", "solve_batch", "POSE_FLOATS", "PROJECTOR_JOSEPH",
            "PROJECTOR_SIDDON", "SOLVER_CGNE", "SOLVER_CGLS", "SOLVER_LANDWEBER", "SOLVER_APGD",
            "PROX_IDENTITY",
            "PROX_BOX", "PROX_L1"]

@@ -70,6 +70,8 @@ SIGNATURES = {
     "elsa_solver_step_size": (_st, [_vp, ctypes.POINTER(ctypes.c_double)]),
     "elsa_power_iterations": (_st, [_vp, _i32, _vp, ctypes.POINTER(ctypes.c_double)]),
     "elsa_solver_iterate": (_st, [_vp, _i32, _vp]),
+    "elsa_solver_iterate_graph": (_st, [_vp, _i32, _vp]),
+    "elsa_solve_batch": (_st, [ctypes.POINTER(_vp), _i32, _i32, _i32]),
     "elsa_solver_squared_residual": (_st, [_vp, _vp, ctypes.POINTER(ctypes.c_double)]),
     "elsa_solver_enable_timing": (_st, [_vp, _i32]),
     "elsa_solver_timing": (_st, [_vp, ctypes.POINTER(ctypes.c_double),
@@ -243,6 +245,13 @@ def voxel_lut(kind, dim, params=(), samples=100):
     return out, sup.value
 
 
+def solve_batch(solvers, iterations, streams=8):
+    """Run `iterations` iterations of every Solver concurrently, each as a CUDA graph, over
+    `streams` streams; returns when all are done."""
+    arr = (ctypes.c_void_p * max(1, len(solvers)))(*[s._h.value for s in solvers])
+    call("elsa_solve_batch", arr, len(solvers), int(iterations), int(streams))
+
+
 def power_iterations(projector, iterations=5, stream=None):
     """Largest eigenvalue of A^T A (powerIterations(adjoint(A) * A), PowerIterations.cpp:10-27)."""
     v = ctypes.c_double()
@@ -266,6 +275,9 @@ class Solver:
              ctypes.c_void_p(x_ptr), int(bool(use_x0)), arr, len(params),
              ctypes.c_void_p(stream or 0), ctypes.byref(h))
         self._h = h
+
+    def iterate_graph(self, iterations, stream):
+        call("elsa_solver_iterate_graph", self._h, int(iterations), ctypes.c_void_p(stream))
 
     def step_size(self):
         v = ctypes.c_double()

@@ -478,6 +478,35 @@ elsa_status elsa_solver_iterate(elsa_solver* s, int32_t iterations, void* stream
     });
 }
 
+elsa_status elsa_solver_iterate_graph(elsa_solver* s, int32_t iterations, void* stream)
+{
+    return guarded([&] {
+        require(s && iterations >= 0, "elsa_solver_iterate_graph: invalid argument");
+        ELSA_CUDA(cudaSetDevice(s->device));
+        s->impl->iterateGraph(iterations, asStream(stream));
+    });
+}
+
+elsa_status elsa_solve_batch(elsa_solver* const* solvers, int32_t n, int32_t iterations,
+                             int32_t numStreams)
+{
+    return guarded([&] {
+        require(n >= 0 && (n == 0 || solvers) && iterations >= 0 && numStreams >= 1 &&
+                    numStreams <= 64,
+                "elsa_solve_batch: invalid argument");
+        std::vector<elsa_b200::SolverSession*> sessions(static_cast<size_t>(n));
+        for (int i = 0; i < n; ++i) {
+            require(solvers[i] != nullptr, "elsa_solve_batch: null solver");
+            require(solvers[i]->device == solvers[0]->device,
+                    "elsa_solve_batch: solvers on different devices");
+            sessions[static_cast<size_t>(i)] = solvers[i]->impl.get();
+        }
+        if (n > 0)
+            ELSA_CUDA(cudaSetDevice(solvers[0]->device));
+        elsa_b200::solveBatch(sessions.data(), n, iterations, numStreams);
+    });
+}
+
 elsa_status elsa_solver_squared_residual(elsa_solver* s, void* stream, double* value)
 {
     return guarded([&] {

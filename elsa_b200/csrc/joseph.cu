@@ -992,6 +992,10 @@ namespace elsa_b200
                     return tma_ ? static_cast<int64_t>(tma_->errorWord()) : 0;
                 case 4: // parts per million of detector tiles on the gather fallback
                     return tma_ ? static_cast<int64_t>(tma_->fallbackFraction() * 1e6) : -1;
+                case 6: // kernel launches per forward call
+                    return tma_ ? tma_->launchesPerForward() : 1;
+                case 7: // kernel launches per adjoint call
+                    return 1;
                 default:
                     return -1;
                 }

@@ -38,6 +38,12 @@ namespace elsa_b200
         // Fraction of tiles that take the gather fallback, and the error word (0 = fine;
         // synchronizes).
         double fallbackFraction() const { return fallbackFraction_; }
+        // kernel launches of one forward(): one volume permutation per driving axis present,
+        // plus the projection kernel
+        int launchesPerForward() const
+        {
+            return 1 + (present_[0] ? 1 : 0) + (present_[1] ? 1 : 0) + (present_[2] ? 1 : 0);
+        }
         unsigned errorWord() const;
 
     private:

@@ -7,6 +7,7 @@
 #include "vecops.cuh"
 
 #include <cmath>
+#include <vector>
 
 namespace elsa_b200
 {
@@ -331,6 +332,67 @@ namespace elsa_b200
                 break;
             }
         }
+    }
+
+    SolverSession::~SolverSession()
+    {
+        if (graph_)
+            cudaGraphExecDestroy(graph_);
+    }
+
+    void SolverSession::iterateGraph(int iterations, cudaStream_t s)
+    {
+        if (s == nullptr || s == cudaStreamLegacy)
+            throw Error(ELSA_ERROR_INVALID_ARGUMENT,
+                        "solver graphs need an explicitly created stream");
+        if (timer_.enabled())
+            throw Error(ELSA_ERROR_INVALID_ARGUMENT, "solver graphs need timing disabled");
+        if (!graph_ || graphIterations_ != iterations) {
+            if (graph_) {
+                ELSA_CUDA(cudaGraphExecDestroy(graph_));
+                graph_ = nullptr;
+            }
+            cudaGraph_t g = nullptr;
+            ELSA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            try {
+                iterate(iterations, s);
+            } catch (...) {
+                cudaStreamEndCapture(s, &g);
+                if (g)
+                    cudaGraphDestroy(g);
+                throw;
+            }
+            ELSA_CUDA(cudaStreamEndCapture(s, &g));
+            const cudaError_t e = cudaGraphInstantiate(&graph_, g, 0);
+            cudaGraphDestroy(g);
+            ELSA_CUDA(e);
+            graphIterations_ = iterations;
+        }
+        ELSA_CUDA(cudaGraphLaunch(graph_, s));
+    }
+
+    void solveBatch(SolverSession* const* sessions, int n, int iterations, int streams)
+    {
+        if (n < 0 || iterations < 0 || streams < 1 || streams > 64)
+            throw Error(ELSA_ERROR_INVALID_ARGUMENT, "solveBatch: invalid argument");
+        std::vector<cudaStream_t> pool(static_cast<size_t>(streams), nullptr);
+        try {
+            for (auto& st : pool)
+                ELSA_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            for (int i = 0; i < n; ++i)
+                sessions[i]->iterateGraph(iterations, pool[static_cast<size_t>(i % streams)]);
+            for (auto st : pool)
+                ELSA_CUDA(cudaStreamSynchronize(st));
+        } catch (...) {
+            for (auto st : pool)
+                if (st) {
+                    cudaStreamSynchronize(st);
+                    cudaStreamDestroy(st);
+                }
+            throw;
+        }
+        for (auto st : pool)
+            cudaStreamDestroy(st);
     }
 
     double SolverSession::squaredResidual(cudaStream_t s)

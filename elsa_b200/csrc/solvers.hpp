@@ -88,7 +88,14 @@ namespace elsa_b200
     public:
         SolverSession(SolverKind kind, Projector& A, const float* b, float* x, bool useX0,
                       const SolverOptions& opt, cudaStream_t s);
+        ~SolverSession();
+        SolverSession(const SolverSession&) = delete;
+        SolverSession& operator=(const SolverSession&) = delete;
         void iterate(int iterations, cudaStream_t s);
+        // The same iterations as one CUDA graph: captured from iterate() on the first call (and
+        // again when `iterations` changes), then launched on s. s must not be the legacy default
+        // stream; timing must be off.
+        void iterateGraph(int iterations, cudaStream_t s);
         double squaredResidual(cudaStream_t s); // synchronizes
         KernelTimer& timer() { return timer_; }
         Projector& op() { return A_; }
@@ -103,5 +110,12 @@ namespace elsa_b200
         float* x_;
         SolverWorkspace ws_;
         KernelTimer timer_;
+        cudaGraphExec_t graph_ = nullptr;
+        int graphIterations_ = -1;
     };
+
+    // Runs `iterations` iterations of every session, each as its CUDA graph, spread round-robin
+    // over `streams` concurrent streams (the sessions must use distinct projectors and buffers);
+    // returns when all have finished.
+    void solveBatch(SolverSession* const* sessions, int n, int iterations, int streams);
 } // namespace elsa_b200

@@ -242,6 +242,18 @@ elsa_status elsa_power_iterations(elsa_projector* projector, int32_t iterations,
  * disabled. */
 elsa_status elsa_solver_iterate(elsa_solver* solver, int32_t iterations, void* stream);
 
+/* Like elsa_solver_iterate, but the iterations run as one CUDA graph: captured on the first call
+ * (and again whenever `iterations` changes), launched on every call. `stream` must be a created
+ * stream (not the legacy default stream) and timing must be off. */
+elsa_status elsa_solver_iterate_graph(elsa_solver* solver, int32_t iterations, void* stream);
+
+/* Batched solves: `iterations` iterations of each of the n solvers (distinct projectors and
+ * buffers), each as its CUDA graph, spread round-robin over `num_streams` concurrent streams (1 to
+ * 64); returns when all have finished. Replaces a loop of Solver::solve calls over independent
+ * problems (no reference counterpart for the concurrency). */
+elsa_status elsa_solve_batch(elsa_solver* const* solvers, int32_t n, int32_t iterations,
+                             int32_t num_streams);
+
 /* Squared norm used by the solver's convergence test (CGNE/CGLS: |r|^2 of the current iterate;
  * APGD: |grad|^2 of the last iteration; Landweber: 0). float64, synchronizes the stream. */
 elsa_status elsa_solver_squared_residual(elsa_solver* solver, void* stream, double* value);
