@@ -1,5 +1,7 @@
 """Graph-captured solver iterations and batched concurrent solves: bit-identical to plain
-iterations (the graph replays the same launches; streams only change the overlap)."""
+iterations for the deterministic projectors (the graph replays the same launches; streams only
+change the overlap). The voxel projectors' forward adds with float atomics, so there the batched
+iterate agrees to rounding only."""
 import numpy as np
 import pytest
 
@@ -51,15 +53,22 @@ def test_batch_matches_plain(cuda, oracle, solver_kind):
     torch.cuda.synchronize()
     xs_batch, batch = _solvers(torch, insts, solver_kind)
     elsa_b200.solve_batch(batch, 6, streams=3)
-    for a, b in zip(xs_plain, xs_batch):
-        assert torch.equal(a, b)
+    _compare(kinds, xs_plain, xs_batch)
     # more graph launches continue the iteration exactly like plain iterations
     elsa_b200.solve_batch(batch, 4, streams=2)
     for sol in plain:
         sol.iterate(4, s)
     torch.cuda.synchronize()
-    for a, b in zip(xs_plain, xs_batch):
-        assert torch.equal(a, b)
+    _compare(kinds, xs_plain, xs_batch)
+
+
+def _compare(kinds, xs_plain, xs_batch):
+    import elsa_b200
+    for (kind, _), a, b in zip(kinds, xs_plain, xs_batch):
+        if kind in (elsa_b200.PROJECTOR_JOSEPH, elsa_b200.PROJECTOR_SIDDON):
+            assert bool((a == b).all()), kind
+        else:
+            assert float((a - b).norm() / a.norm()) <= 1e-4, kind
 
 
 def test_graph_needs_created_stream(cuda, oracle):
