@@ -692,26 +692,6 @@ namespace elsa_b200
                 *adr[t] = val[t] + yl * wt[t];
         }
 
-        // Steps t in [0, tMax] at which the approximate position p0 + t*s lies in [lo, hi),
-        // widened by one step on each side; t0 > t1 when there is none. The caller's interval
-        // carries a positional margin far above the drift between this linear form and the
-        // exactly accumulated position (|t| <= 16 steps: a few 1e-4 voxel).
-        __device__ __forceinline__ void stepWindow(float p0, float s, float lo, float hi, int tMax,
-                                                   int& t0, int& t1)
-        {
-            if (fabsf(s) < 1e-12f) {
-                const bool in = p0 >= lo && p0 < hi;
-                t0 = in ? 0 : 1;
-                t1 = in ? tMax : 0;
-                return;
-            }
-            const float ta = (lo - p0) / s, tb = (hi - p0) / s;
-            const float tmin = fminf(fmaxf(fminf(ta, tb), -2.0f), static_cast<float>(tMax + 2));
-            const float tmax = fminf(fmaxf(fmaxf(ta, tb), -2.0f), static_cast<float>(tMax + 2));
-            t0 = max(0, static_cast<int>(floorf(tmin)) - 1);
-            t1 = min(tMax, static_cast<int>(ceilf(tmax)) + 1);
-        }
-
         // One (view, driving axis G) for a warp-owned brick: M x M ray classes, separated by
         // __syncwarp; lane i takes class rays i, i + 32, ... (u fastest within the class grid).
         template <int G, int BX, int BY, int BZ, int CPD>
@@ -770,25 +750,9 @@ namespace elsa_b200
                             int jLo, jHi;
                             if (!sampleRange(R, kLo, kHi, jLo, jHi))
                                 continue;
-                            // samples whose four taps all miss the brick contribute nothing:
-                            // step over them with the position accumulation alone
-                            float2 cp = cpb[q];
-                            int ta0, ta1, tb0, tb1;
-                            const float m = 0.01f;
-                            stepWindow(cp.x, R.sa, orgA - 0.5f - m, orgA + AR::extA + 0.5f + m,
-                                       jHi - jLo, ta0, ta1);
-                            stepWindow(cp.y, R.sb, orgB - 0.5f - m, orgB + AR::extB + 0.5f + m,
-                                       jHi - jLo, tb0, tb1);
-                            const int t0 = max(ta0, tb0), t1 = min(ta1, tb1);
-                            if (t0 > t1)
-                                continue;
-                            for (int t = 0; t < t0; ++t) {
-                                cp.x = __fadd_rn(cp.x, R.sa);
-                                cp.y = __fadd_rn(cp.y, R.sb);
-                            }
                             warpSplat<G, BX, BY, BZ>(acc, acc + WarpBrick<BX, BY>::kPlane * BZ,
-                                                     R, yb[q] * R.len, cp, jLo + t0, jLo + t1,
-                                                     orgG, orgA, orgB);
+                                                     R, yb[q] * R.len, cpb[q], jLo, jHi, orgG,
+                                                     orgA, orgB);
                         }
                     }
                     __syncwarp();
