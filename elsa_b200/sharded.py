@@ -1,0 +1,129 @@
+"""View-sharded CGNE across processes (one per GPU) with torch.distributed.
+
+Every rank holds the whole volume and the poses [lo, hi) of its block of views; A = [A_0; A_1; ...]
+stacks the ranks' projectors. CGNE (solvers/CGNE.cpp:20-78) works on volume-sized vectors only,
+so the one exchange per iteration is the sum A^T A c = sum_r A_r^T A_r c: an all-reduce of one
+volume (67 MB at 256^3, ~0.1 ms over NVLink against ~78 ms of projection). The right-hand side
+A^T b is all-reduced once. The all-reduce hands every rank the same sum, so the replicated vectors
+(x, r, c) and the scalars computed from them stay identical on all ranks without further
+exchange.
+
+With the "nccl" backend the vectors are CUDA tensors and the projections and vector updates run
+the native kernels (C ABI); with "gloo" the same code runs on CPU tensors with caller-supplied
+projections (used by the tests).
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+__all__ = ["view_block", "NativeVectorOps", "TorchVectorOps", "ShardedCGNE"]
+
+
+def view_block(num_views, rank, world):
+    """Contiguous block [lo, hi) of views for `rank`; blocks differ in size by at most one."""
+    base, extra = divmod(int(num_views), int(world))
+    lo = rank * base + min(rank, extra)
+    return lo, lo + base + (1 if rank < extra else 0)
+
+
+class TorchVectorOps:
+    """Vector operations on torch tensors (CPU testing; float64 inner products)."""
+
+    @staticmethod
+    def dot(a, b):
+        return float(torch.dot(a.double(), b.double()))
+
+    @staticmethod
+    def lincomb(a, x, b, y, out):
+        out.copy_((a * x + b * y).to(out.dtype))
+
+
+class NativeVectorOps:
+    """The C ABI's fused vector operations on CUDA tensors (float64 inner products)."""
+
+    def __init__(self):
+        from . import _capi
+        self._capi = _capi
+        self._res = torch.empty(1, dtype=torch.float64, device="cuda")
+
+    def _stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def dot(self, a, b):
+        self._capi.call("elsa_dot", ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(b.data_ptr()),
+                        a.numel(), ctypes.c_void_p(self._res.data_ptr()), self._stream())
+        return float(self._res.item())
+
+    def lincomb(self, a, x, b, y, out):
+        self._capi.call("elsa_lincomb", ctypes.c_float(a), ctypes.c_void_p(x.data_ptr()),
+                        ctypes.c_float(b), ctypes.c_void_p(y.data_ptr()),
+                        ctypes.c_void_p(out.data_ptr()), x.numel(), self._stream())
+
+
+class ShardedCGNE:
+    """CGNE on A^T A x = A^T b with A split by views over the ranks of `group`.
+
+    forward(x) -> local sinogram block, adjoint(y) -> volume: this rank's projector (for the
+    native path: an elsa_b200.Projector built on the rank's poses, see `native_ops`).
+    b_local: this rank's block of measurements."""
+
+    def __init__(self, forward, adjoint, b_local, domain_size, ops=None, group=None):
+        import torch.distributed as dist
+        self.dist = dist
+        self.group = group
+        self.forward, self.adjoint = forward, adjoint
+        self.ops = ops or TorchVectorOps()
+        self.n = int(domain_size)
+        self.b = b_local
+
+    def _normal(self, v):
+        q = self.adjoint(self.forward(v))
+        self.dist.all_reduce(q, group=self.group)  # sum over the view blocks
+        return q
+
+    def solve(self, iterations, x0=None):
+        like = self.b
+        x = torch.zeros(self.n, dtype=torch.float32, device=like.device) if x0 is None else \
+            x0.clone()
+        atb = self.adjoint(self.b)
+        self.dist.all_reduce(atb, group=self.group)
+        r = atb.clone()
+        if x0 is not None:
+            ata_x = self._normal(x)
+            self.ops.lincomb(1.0, r, -1.0, ata_x, r)
+        c = r.clone()
+        kold = self.ops.dot(r, r)
+        history = []
+        for _ in range(int(iterations)):
+            q = self._normal(c)
+            alpha = float(np.float32(kold / self.ops.dot(c, q)))
+            self.ops.lincomb(1.0, x, alpha, c, x)
+            self.ops.lincomb(1.0, r, -alpha, q, r)
+            k = self.ops.dot(r, r)
+            beta = float(np.float32(k / kold))
+            self.ops.lincomb(1.0, r, beta, c, c)
+            kold = k
+            history.append(k)
+        return x, history
+
+
+def native_ops(kind, vol_dims, poses, det_dims, rank, world, params=None):
+    """(forward, adjoint, projector, (lo, hi)) for this rank's block of views, running the native
+    kernels on CUDA tensors."""
+    from . import _capi
+    lo, hi = view_block(len(poses), rank, world)
+    det = list(det_dims[:-1]) + [hi - lo]
+    proj = _capi.Projector(kind, vol_dims, det, np.ascontiguousarray(poses[lo:hi]), params)
+
+    def forward(x):
+        y = torch.empty(proj.range_size, dtype=torch.float32, device="cuda")
+        proj.apply_ptr(x.data_ptr(), y.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        return y
+
+    def adjoint(y):
+        x = torch.empty(proj.domain_size, dtype=torch.float32, device="cuda")
+        proj.apply_adjoint_ptr(y.data_ptr(), x.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        return x
+
+    return forward, adjoint, proj, (lo, hi)
