@@ -95,22 +95,110 @@ def modified_shepp_logan(shape):
         n = shape[0]
         if shape[0] != shape[1]:
             raise ValueError("phantom::modifiedSheppLogan: 2d size has to be square")
-        img = np.zeros((n, n), np.float64)
-        yy, xx = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+        img = np.zeros((n, n), np.float32)
         for amp, (cx, cy), (a, b), ang in MODIFIED_SHEPP_LOGAN_2D:
-            A, B = _scale(n, a), _scale(n, b)
-            if A == 0 and B == 0:
-                continue
-            x0, y0 = _scale_shift(n, cx), _scale_shift(n, cy)
-            t = math.radians(ang)
-            dx = xx - x0
-            # the reference draws with the y axis flipped (EllipseGenerator.cpp)
-            dy = (n - yy) - y0
-            u = dx * math.cos(t) + dy * math.sin(t)
-            v = -dx * math.sin(t) + dy * math.cos(t)
-            img += amp * ((u / max(A, 1e-9)) ** 2 + (v / max(B, 1e-9)) ** 2 <= 1.0)
-        return img.astype(np.float32)
+            center = (_scale_shift(n, cx), _scale_shift(n, cy))
+            draw_filled_ellipse_2d(img, amp, center, (_scale(n, a), _scale(n, b)), ang)
+        return img
     raise ValueError("phantom::modifiedSheppLogan: only 2d or 3d supported")
+
+
+def _trunc_div(a, b):
+    """C++ integer division (truncation toward zero)."""
+    q = abs(a) // abs(b)
+    return q if (a >= 0) == (b >= 0) else -q
+
+
+def _sheared_line_pairs(img, amp, center, x_off, y_off, shear):
+    """One pair of horizontal lines of a sheared ellipse (EllipseGenerator.cpp:118-158), with the
+    y axis flipped as the reference draws it."""
+    ny, nx = img.shape
+    for x in range(center[0] - x_off, center[0] + x_off + 1):
+        shear_term = _trunc_div((x - center[0]) * shear[1], shear[0])
+        for sgn in ((1, -1) if y_off != 0 else (1,)):
+            y = ny - (center[1] + sgn * y_off + shear_term)
+            if not (0 <= x < nx and 0 <= y < ny):
+                raise ValueError("EllipseGenerator: drawing coordinate out of bounds")
+            img[y, x] = np.float32(img[y, x] + np.float32(amp))
+
+
+def _sheared_filled_ellipse(img, amp, center, sizes, shear):
+    """Midpoint ellipse rasterisation in integer arithmetic, filled with horizontal line pairs
+    (EllipseGenerator.cpp:50-116)."""
+    sx, sy = sizes
+    two_xx, two_yy = 2 * sx * sx, 2 * sy * sy
+    # first part: y advances every step
+    x, y = sx, 0
+    x_change, y_change = sy * sy * (1 - 2 * sx), sx * sx
+    err, x_stop, y_stop = 0, two_yy * sx, 0
+    while x_stop >= y_stop:
+        _sheared_line_pairs(img, amp, center, x, y, shear)
+        y += 1
+        y_stop += two_xx
+        err += y_change
+        y_change += two_xx
+        if 2 * err + x_change > 0:
+            x -= 1
+            x_stop -= two_yy
+            err += x_change
+            x_change += two_yy
+    # second part: x advances every step; a line pair is drawn whenever y changes
+    x, y = 0, sy
+    x_change, y_change = sy * sy, sx * sx * (1 - 2 * sy)
+    err, x_stop, y_stop = 0, 0, two_xx * sy
+    while x_stop < y_stop:
+        x += 1
+        x_stop += two_yy
+        err += x_change
+        x_change += two_yy
+        if 2 * err + y_change > 0:
+            _sheared_line_pairs(img, amp, center, x - 1, y, shear)
+            y -= 1
+            y_stop -= two_xx
+            err += y_change
+            y_change += two_xx
+
+
+def draw_filled_ellipse_2d(img, amp, center, sizes, angle_deg):
+    """Adds `amp` to the pixels of a filled ellipse (EllipseGenerator::drawFilledEllipse2d,
+    generators/EllipseGenerator.cpp:10-48): integer centre and half axes; a rotation is turned
+    into a shear of the axis-aligned rasterisation. img: float32 (ny, nx), x fastest."""
+    sx, sy = int(sizes[0]), int(sizes[1])
+    if sx == 0 and sy == 0:
+        return
+    ang = float(np.float32(angle_deg))
+    if sx == sy or math.fmod(ang, 180.0) == 0:
+        _sheared_filled_ellipse(img, amp, center, (sx, sy), (1, 0))
+        return
+    rad = ang * math.pi / 180.0
+    theta = math.atan2(float(np.float32(-sy)) * math.tan(rad), float(sx))
+    s0 = int(math.floor(float(np.float32(sx)) * math.cos(theta) * math.cos(rad)
+                        - float(np.float32(sy)) * math.sin(theta) * math.sin(rad)))
+    s1 = int(math.floor(float(np.float32(sx)) * math.cos(theta) * math.sin(rad)
+                        + float(np.float32(sy)) * math.sin(theta) * math.cos(rad)))
+    sheared = (abs(s0), _trunc_div(sy * sx, abs(s0)))
+    _sheared_filled_ellipse(img, amp, center, sheared, (s0, s1))
+
+
+def rectangle(shape, lower, upper):
+    """phantoms::rectangle (generators/Phantoms.cpp:56-69): ones on [lower, upper) per axis.
+    shape, lower, upper in elsa's axis order (x first); returns x-fastest C-order array."""
+    img = np.zeros(tuple(reversed([int(s) for s in shape])), np.float32)
+    sl = tuple(slice(int(lo), int(hi)) for lo, hi in zip(reversed(lower), reversed(upper)))
+    img[sl] = 1.0
+    return img
+
+
+def circular(shape, radius):
+    """phantoms::circular (generators/Phantoms.cpp:37-54): ones where |p - size/2| <= radius,
+    p the integer voxel index (x first); returns x-fastest C-order array."""
+    shape = [int(s) for s in shape]
+    grids = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in reversed(shape)],
+                        indexing="ij")
+    d2 = np.zeros(grids[0].shape)
+    for g, n in zip(grids, reversed(shape)):
+        d2 += (g - np.float32(n) / np.float32(2.0)) ** 2
+    return (np.sqrt(d2) <= radius).astype(np.float32)
 
 
 def random_ellipsoids(n, count=20, seed=0):
