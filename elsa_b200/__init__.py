@@ -11,7 +11,8 @@ from ._capi import (ElsaError, InvalidArgumentError, Projector, Solver,  # noqa:
                     PROJECTOR_PHASE_CONTRAST_BSPLINE, FOOTPRINT_REFERENCE, FOOTPRINT_RECTANGLE,
                     circle_trajectory, pose_2d, pose_3d, power_iterations, solve_batch, POSE_FLOATS,
                     PROJECTOR_JOSEPH, PROJECTOR_SIDDON, SOLVER_CGNE, SOLVER_CGLS,
-                    SOLVER_LANDWEBER, SOLVER_APGD, PROX_IDENTITY, PROX_BOX, PROX_L1)
+                    SOLVER_LANDWEBER, SOLVER_APGD, SOLVER_SIRT, SOLVER_FGM,
+                    SOLVER_OGM, PROX_IDENTITY, PROX_BOX, PROX_L1)
 
 __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "voxel_lut",
            "PROJECTOR_BLOB", "PROJECTOR_BSPLINE", "PROJECTOR_PHASE_CONTRAST_BLOB",
@@ -19,5 +20,6 @@ __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "voxel_lu
            "circle_trajectory",
            "pose_2d", "pose_3d", "power_iterations", "solve_batch", "POSE_FLOATS", "PROJECTOR_JOSEPH",
            "PROJECTOR_SIDDON", "SOLVER_CGNE", "SOLVER_CGLS", "SOLVER_LANDWEBER", "SOLVER_APGD",
+           "SOLVER_SIRT", "SOLVER_FGM", "SOLVER_OGM",
            "PROX_IDENTITY",
            "PROX_BOX", "PROX_L1"]

@@ -33,6 +33,9 @@ SOLVER_CGNE = 0
 SOLVER_CGLS = 1
 SOLVER_LANDWEBER = 2
 SOLVER_APGD = 3
+SOLVER_SIRT = 4
+SOLVER_FGM = 5
+SOLVER_OGM = 6
 PROX_IDENTITY = 0
 PROX_BOX = 1
 PROX_L1 = 2

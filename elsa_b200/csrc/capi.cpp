@@ -397,11 +397,11 @@ elsa_status elsa_solver_create(int32_t kind, elsa_projector* p, const float* b, 
         require(out != nullptr, "elsa_solver_create: null output handle");
         *out = nullptr;
         require(p && b && x, "elsa_solver_create: null argument");
-        require(kind >= ELSA_SOLVER_CGNE && kind <= ELSA_SOLVER_APGD,
+        require(kind >= ELSA_SOLVER_CGNE && kind <= ELSA_SOLVER_OGM,
                 "elsa_solver_create: unknown solver kind");
         require(numParams >= 0 && (numParams == 0 || params != nullptr),
                 "elsa_solver_create: invalid parameter array");
-        static const int kMaxParams[] = {0, 2, 1, 6};
+        static const int kMaxParams[] = {0, 2, 1, 6, 1, 1, 1};
         require(numParams <= kMaxParams[kind], "elsa_solver_create: too many parameters");
         auto param = [&](int i, double dflt) { return i < numParams ? params[i] : dflt; };
         elsa_b200::SolverOptions opt;
@@ -437,6 +437,16 @@ elsa_status elsa_solver_create(int32_t kind, elsa_projector* p, const float* b, 
                         "elsa_solver_create: box constraint with lower > upper");
             break;
         }
+        case ELSA_SOLVER_SIRT:
+            opt.sirtStep = param(0, 0.0);
+            require(std::isfinite(opt.sirtStep), "elsa_solver_create: SIRT step must be finite");
+            break;
+        case ELSA_SOLVER_FGM:
+        case ELSA_SOLVER_OGM:
+            opt.momentumEpsilon = param(0, static_cast<double>(FLT_EPSILON));
+            require(std::isfinite(opt.momentumEpsilon) && opt.momentumEpsilon >= 0.0,
+                    "elsa_solver_create: epsilon must be finite and >= 0");
+            break;
         default:
             break;
         }

@@ -144,8 +144,8 @@ namespace elsa_b200
             cgneStep(A, x, ws, off, s);
     }
 
-    double powerIterationsAtA(Projector& A, SolverWorkspace& ws, int iterations,
-                              cudaStream_t s)
+    double powerIterationsAtA(Projector& A, SolverWorkspace& ws, int iterations, cudaStream_t s,
+                              const float* rangeScale, const float* domainScale)
     {
         const int64_t n = A.domainSize();
         float* u = ws.vol0.as<float>();
@@ -154,14 +154,21 @@ namespace elsa_b200
         double* partials = ws.partials.as<double>();
         SolverScalars* S = ws.scalars.as<SolverScalars>();
         launchFill(u, 1.0f, n, s);
+        const int64_t m = A.rangeSize();
+        auto apply = [&](const float* in, float* out) {
+            A.forward(in, sino, s);
+            if (rangeScale)
+                launchMul(sino, rangeScale, m, s);
+            A.adjoint(sino, out, s);
+            if (domainScale)
+                launchMul(out, domainScale, n, s);
+        };
         for (int i = 0; i < iterations; ++i) {
-            A.forward(u, sino, s);
-            A.adjoint(sino, u, s); // u = A^T A u
+            apply(u, u); // u = A^T A u (scaled)
             launchSquaredNorm(u, n, partials, &S->k, s);
             launchScaleByInvNorm(u, &S->k, n, s);
         }
-        A.forward(u, sino, s);
-        A.adjoint(sino, v, s);
+        apply(u, v);
         launchDot(u, v, n, partials, &S->den, s);
         launchSquaredNorm(u, n, partials, &S->k, s);
         SolverScalars h;
@@ -283,6 +290,69 @@ namespace elsa_b200
         apgdGradient(A, ws, t, s);
     }
 
+    // SIRT: Landweber with T A^T M, M = 1 / (A 1 + 1e-10), T = 1 / (A^T 1),
+    // solvers/SIRT.cpp:20-45 with LandweberIteration.cpp:57-67. ws.vol0 = T, ws.sino1 = M.
+    static void sirtBegin(Projector& A, SolverWorkspace& ws, cudaStream_t s)
+    {
+        const int64_t n = A.domainSize(), m = A.rangeSize();
+        float* tinv = ws.vol0.as<float>();
+        float* minv = ws.sino1.as<float>();
+        launchFill(ws.vol1.as<float>(), 1.0f, n, s);
+        A.forward(ws.vol1.as<float>(), minv, s); // row sums
+        launchReciprocal(minv, 1e-10f, minv, m, s);
+        launchFill(ws.sino0.as<float>(), 1.0f, m, s);
+        A.adjoint(ws.sino0.as<float>(), tinv, s); // column sums
+        launchReciprocal(tinv, 0.0f, tinv, n, s);
+    }
+
+    static void sirtStep(Projector& A, const float* b, float* x, float step, SolverWorkspace& ws,
+                         KernelTimer& t, cudaStream_t s)
+    {
+        const int64_t n = A.domainSize(), m = A.rangeSize();
+        float* sino = ws.sino0.as<float>();
+        float* q = ws.vol2.as<float>();
+        t.mark(s);
+        A.forward(x, sino, s);
+        t.mark(s);
+        launchSubMul(sino, b, ws.sino1.as<float>(), sino, m, s); // M (A x - b)
+        A.adjoint(sino, q, s);
+        t.mark(s);
+        launchScaledStep(x, step, ws.vol0.as<float>(), q, n, s); // x -= step T A^T M (A x - b)
+    }
+
+    // FGM / OGM on the least-squares problem 0.5 |A x - b|^2 (solvers/FGM.cpp:33-78,
+    // OGM.cpp:40-95 with functionals/LeastSquares.cpp:45-59): gradient A^T (A x - b) into vol2,
+    // previous y in vol1; S->aux[1] holds |grad_0|^2.
+    static void lsqGradient(Projector& A, const float* b, const float* x, SolverWorkspace& ws,
+                            KernelTimer& t, cudaStream_t s)
+    {
+        const int64_t m = A.rangeSize();
+        float* sino = ws.sino0.as<float>();
+        t.mark(s);
+        A.forward(x, sino, s);
+        t.mark(s);
+        launchSub(sino, b, sino, m, s);
+        A.adjoint(sino, ws.vol2.as<float>(), s);
+        t.mark(s);
+    }
+
+    static void momentumBegin(Projector& A, const float* b, float* x, bool useX0,
+                              SolverWorkspace& ws, cudaStream_t s)
+    {
+        const int64_t n = A.domainSize();
+        SolverScalars* S = ws.scalars.as<SolverScalars>();
+        if (!useX0)
+            launchFill(x, 0.0f, n, s);
+        ELSA_CUDA(cudaMemcpyAsync(ws.vol1.as<float>(), x, sizeof(float) * n,
+                                  cudaMemcpyDeviceToDevice, s)); // yPrev = x
+        KernelTimer off;
+        lsqGradient(A, b, x, ws, off, s);
+        ELSA_CUDA(cudaMemsetAsync(S, 0, sizeof(SolverScalars), s));
+        launchSquaredNorm(ws.vol2.as<float>(), n, ws.partials.as<double>(), &S->aux[1], s);
+        static const double one = 1.0;
+        ELSA_CUDA(cudaMemcpyAsync(&S->tPrev, &one, sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+
     SolverSession::SolverSession(SolverKind kind, Projector& A, const float* b, float* x,
                                  bool useX0, const SolverOptions& opt, cudaStream_t s)
         : kind_(kind), opt_(opt), A_(A), b_(b), x_(x), ws_(A.domainSize(), A.rangeSize())
@@ -310,6 +380,27 @@ namespace elsa_b200
                         : 0.45 / powerIterationsAtA(A_, ws_, opt_.powerIterations, s);
             apgdBegin(A_, b_, x_, useX0, ws_, s);
             break;
+        case SolverKind::SIRT:
+            sirtBegin(A_, ws_, s);
+            step_ = opt_.sirtStep > 0.0
+                        ? opt_.sirtStep
+                        : 0.9 * (2.0 / powerIterationsAtA(A_, ws_, opt_.powerIterations, s,
+                                                          ws_.sino1.as<float>(),
+                                                          ws_.vol0.as<float>()));
+            if (!useX0)
+                launchFill(x_, 0.0f, A_.domainSize(), s);
+            ELSA_CUDA(cudaMemsetAsync(ws_.scalars.as<SolverScalars>(), 0, sizeof(SolverScalars),
+                                      s));
+            break;
+        case SolverKind::FGM:
+        case SolverKind::OGM: {
+            // FGM uses 5 power iterations, OGM 20 (OGM.cpp:57-60)
+            const int pi = kind_ == SolverKind::OGM ? 20 : 5;
+            lipschitz_ = static_cast<float>(powerIterationsAtA(A_, ws_, pi, s));
+            step_ = 1.0 / lipschitz_;
+            momentumBegin(A_, b_, x_, useX0, ws_, s);
+            break;
+        }
         }
     }
 
@@ -330,6 +421,23 @@ namespace elsa_b200
             case SolverKind::APGD:
                 apgdStep(A_, x_, static_cast<float>(step_), opt_, ws_, timer_, s);
                 break;
+            case SolverKind::SIRT:
+                sirtStep(A_, b_, x_, static_cast<float>(step_), ws_, timer_, s);
+                break;
+            case SolverKind::FGM:
+            case SolverKind::OGM: {
+                const bool ogm = kind_ == SolverKind::OGM;
+                // OGM's last iteration uses the factor 8 (OGM.cpp:73): the last of this call
+                const float f = (ogm && it == iterations - 1) ? 8.0f : 4.0f;
+                const int64_t n = A_.domainSize();
+                SolverScalars* S = ws_.scalars.as<SolverScalars>();
+                lsqGradient(A_, b_, x_, ws_, timer_, s);
+                launchMomentumStep(x_, ws_.vol1.as<float>(), ws_.vol2.as<float>(), lipschitz_,
+                                   f, ogm ? 1 : 0, n, S, ws_.partials.as<double>(), s);
+                launchMomentumFinish(ws_.partials.as<double>(), S, f,
+                                        opt_.momentumEpsilon * opt_.momentumEpsilon, s);
+                break;
+            }
             }
         }
     }
@@ -401,8 +509,10 @@ namespace elsa_b200
         ELSA_CUDA(cudaMemcpyAsync(&h, ws_.scalars.as<SolverScalars>(), sizeof(h),
                                   cudaMemcpyDeviceToHost, s));
         ELSA_CUDA(cudaStreamSynchronize(s));
-        if (kind_ == SolverKind::APGD)
+        if (kind_ == SolverKind::APGD || kind_ == SolverKind::FGM || kind_ == SolverKind::OGM)
             return h.k;
+        if (kind_ == SolverKind::SIRT)
+            return 0.0;
         if (kind_ == SolverKind::LANDWEBER)
             return 0.0;
         return h.kold;

@@ -62,7 +62,7 @@ namespace elsa_b200
         int64_t count_ = 0;
     };
 
-    enum class SolverKind { CGNE = 0, CGLS = 1, LANDWEBER = 2, APGD = 3 };
+    enum class SolverKind { CGNE = 0, CGLS = 1, LANDWEBER = 2, APGD = 3, SIRT = 4, FGM = 5, OGM = 6 };
 
     // Solver options (elsa's constructor arguments). Step sizes <= 0 mean "derive from power
     // iterations", as the reference does when none is given.
@@ -74,11 +74,18 @@ namespace elsa_b200
         double apgdEpsilon = 1.1920928955078125e-07; // APGD stops once |grad|^2 <= epsilon
         ProxSpec prox{0, 0, 0.0f, 0.0f, 0.0f};
         int powerIterations = 5; // solvers/PowerIterations.h:11
+        double sirtStep = 0.0;   // <= 0: 0.9 * 2 / lambda_max(T A^T M A), solvers/SIRT.cpp
+        double momentumEpsilon = 1.1920928955078125e-07; // FGM / OGM: stop once
+                                                          // |grad|^2 <= eps^2 |grad_0|^2
     };
 
     // Largest eigenvalue of A^T A by power iterations, solvers/PowerIterations.cpp:10-27
     // (synchronizes once at the end).
-    double powerIterationsAtA(Projector& A, SolverWorkspace& ws, int iterations, cudaStream_t s);
+    // With rangeScale / domainScale (element-wise, may be null) the operator is
+    // diag(domainScale) A^T diag(rangeScale) A (SIRT's T A^T M A).
+    double powerIterationsAtA(Projector& A, SolverWorkspace& ws, int iterations, cudaStream_t s,
+                              const float* rangeScale = nullptr,
+                              const float* domainScale = nullptr);
 
     // A solver run split into setup and iterations: begin() computes the initial residual,
     // iterate() enqueues iterations asynchronously on the stream (capturable in a CUDA graph
@@ -110,6 +117,7 @@ namespace elsa_b200
         float* x_;
         SolverWorkspace ws_;
         KernelTimer timer_;
+        float lipschitz_ = 0.0f;
         cudaGraphExec_t graph_ = nullptr;
         int graphIterations_ = -1;
     };

@@ -449,4 +449,130 @@ namespace elsa_b200
         apgdFinishKernel<<<1, kReduceThreads, 0, s>>>(partials, S, eps);
         ELSA_LAUNCH_CHECK("apgdFinish");
     }
+
+    namespace
+    {
+        __global__ void reciprocalKernel(const float* __restrict__ in, float lift,
+                                         float* __restrict__ out, int64_t n)
+        {
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < n; i += T)
+                out[i] = 1.0f / (in[i] + lift);
+        }
+
+        __global__ void subMulKernel(const float* a, const float* __restrict__ b,
+                                     const float* __restrict__ m, float* out, int64_t n)
+        {
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < n; i += T)
+                out[i] = (a[i] - b[i]) * m[i];
+        }
+
+        __global__ void scaledStepKernel(float* __restrict__ x, float step,
+                                         const float* __restrict__ t,
+                                         const float* __restrict__ q, int64_t n)
+        {
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < n; i += T)
+                x[i] = x[i] - step * (t[i] * q[i]);
+        }
+
+        __global__ void mulKernel(float* __restrict__ u, const float* __restrict__ m, int64_t n)
+        {
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < n; i += T)
+                u[i] = u[i] * m[i];
+        }
+
+        __global__ void __launch_bounds__(kReduceThreads)
+            momentumStepKernel(float* __restrict__ x, float* __restrict__ yPrev,
+                               const float* __restrict__ grad, float lipschitz, float f, int ogm,
+                               int64_t n, const SolverScalars* S, double* __restrict__ partials)
+        {
+            const bool done = S->done != 0;
+            const double tp = S->tPrev;
+            const double th = 0.5 * (1.0 + sqrt(1.0 + f * tp * tp));
+            const float c1 = static_cast<float>((tp - 1.0) / th);
+            const float c2 = static_cast<float>(tp / th);
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            double acc = 0.0;
+            for (int64_t i = tid; i < n; i += T) {
+                const float g = grad[i];
+                acc += static_cast<double>(g) * g;
+                if (done)
+                    continue;
+                const float gl = g / lipschitz;
+                const float y = x[i] - gl;
+                float xn = y + c1 * (y - yPrev[i]);
+                if (ogm)
+                    xn = xn - c2 * gl;
+                x[i] = xn;
+                yPrev[i] = y;
+            }
+            const double sum = blockSum(acc);
+            if (threadIdx.x == 0)
+                partials[blockIdx.x] = sum;
+        }
+
+        __global__ void __launch_bounds__(kReduceThreads)
+            momentumFinishKernel(const double* __restrict__ partials, SolverScalars* S, float f,
+                                 double relTol)
+        {
+            const double g2 = sumPartials(partials);
+            if (threadIdx.x == 0 && !S->done) {
+                const double tp = S->tPrev;
+                S->tPrev = 0.5 * (1.0 + sqrt(1.0 + f * tp * tp));
+                S->k = g2;
+                if (g2 <= relTol * S->aux[1])
+                    S->done = 1;
+            }
+        }
+    } // namespace
+
+    void launchReciprocal(const float* in, float lift, float* out, int64_t n, cudaStream_t s)
+    {
+        reciprocalKernel<<<gridFor(n), 256, 0, s>>>(in, lift, out, n);
+        ELSA_LAUNCH_CHECK("reciprocal");
+    }
+
+    void launchSubMul(const float* a, const float* b, const float* m, float* out, int64_t n,
+                      cudaStream_t s)
+    {
+        subMulKernel<<<gridFor(n), 256, 0, s>>>(a, b, m, out, n);
+        ELSA_LAUNCH_CHECK("subMul");
+    }
+
+    void launchScaledStep(float* x, float step, const float* t, const float* q, int64_t n,
+                          cudaStream_t s)
+    {
+        scaledStepKernel<<<gridFor(n), 256, 0, s>>>(x, step, t, q, n);
+        ELSA_LAUNCH_CHECK("scaledStep");
+    }
+
+    void launchMul(float* u, const float* m, int64_t n, cudaStream_t s)
+    {
+        mulKernel<<<gridFor(n), 256, 0, s>>>(u, m, n);
+        ELSA_LAUNCH_CHECK("mul");
+    }
+
+    void launchMomentumStep(float* x, float* yPrev, const float* grad, float lipschitz, float f,
+                            int ogm, int64_t n, const SolverScalars* S, double* partials,
+                            cudaStream_t s)
+    {
+        momentumStepKernel<<<kReduceBlocks, kReduceThreads, 0, s>>>(x, yPrev, grad, lipschitz, f,
+                                                                    ogm, n, S, partials);
+        ELSA_LAUNCH_CHECK("momentumStep");
+    }
+
+    void launchMomentumFinish(const double* partials, SolverScalars* S, float f, double relTol,
+                              cudaStream_t s)
+    {
+        momentumFinishKernel<<<1, kReduceThreads, 0, s>>>(partials, S, f, relTol);
+        ELSA_LAUNCH_CHECK("momentumFinish");
+    }
 } // namespace elsa_b200

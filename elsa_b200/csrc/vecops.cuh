@@ -88,6 +88,26 @@ namespace elsa_b200
     // *result = <x, y> with the partial sums in a fixed device array instead of caller scratch
     // (noalloc.cu; asynchronous, allocates nothing, n <= ELSA_DOT_NO_ALLOC_MAX_ELEMENTS).
     void dotNoAlloc(const float* x, const float* y, int64_t n, double* result, cudaStream_t s);
+    // out = 1 / (in + lift) (SIRT's row and column sums, solvers/SIRT.cpp:28-41)
+    void launchReciprocal(const float* in, float lift, float* out, int64_t n, cudaStream_t s);
+    // out = (a - b) * m (out may alias a)
+    void launchSubMul(const float* a, const float* b, const float* m, float* out, int64_t n,
+                      cudaStream_t s);
+    // x = x - step * (t * q) (SIRT update)
+    void launchScaledStep(float* x, float step, const float* t, const float* q, int64_t n,
+                          cudaStream_t s);
+    // u = u * m (element-wise, in place)
+    void launchMul(float* u, const float* m, int64_t n, cudaStream_t s);
+    // FGM / OGM body (solvers/FGM.cpp:48-73, OGM.cpp:62-90): y = x - grad / L;
+    // theta = 0.5 (1 + sqrt(1 + f theta_prev^2)); x = y + (theta_prev - 1) / theta (y - yPrev)
+    // [- ogm * theta_prev / theta * grad / L]; yPrev = y; partial |grad|^2. No-op once done.
+    void launchMomentumStep(float* x, float* yPrev, const float* grad, float lipschitz, float f,
+                            int ogm, int64_t n, const SolverScalars* S, double* partials,
+                            cudaStream_t s);
+    // S->tPrev = theta (with factor f); S->k = sum(partials);
+    // S->done |= (S->k <= relTol * S->aux[1])
+    void launchMomentumFinish(const double* partials, SolverScalars* S, float f, double relTol,
+                              cudaStream_t s);
     // S->tPrev = t; S->k = sum(partials); S->done |= (S->k <= eps)
     void launchApgdFinish(const double* partials, SolverScalars* S, double eps, cudaStream_t s);
 } // namespace elsa_b200

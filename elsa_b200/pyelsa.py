@@ -395,7 +395,43 @@ class APGD(_Solver):
 
 
 FISTA = APGD
+
+
+class SIRT(Landweber):
+    """SIRT(A, b, stepSize=None) (solvers/SIRT.cpp)."""
+    _kind = _capi.SOLVER_SIRT
+
+
+class LeastSquares:
+    """The functional 0.5 |A x - b|^2 (functionals/LeastSquares.h), the problem FGM / OGM solve."""
+
+    def __init__(self, A, b):
+        self.A = A
+        self.b = b
+
+
+class _MomentumSolver(_Solver):
+    def __init__(self, problem, epsilon=1.1920928955078125e-07):
+        super().__init__(problem.A, problem.b)
+        self.epsilon = float(epsilon)
+
+    def _params(self):
+        return (self.epsilon,)
+
+
+class FGM(_MomentumSolver):
+    """FGM(LeastSquares(A, b), epsilon) (solvers/FGM.cpp)."""
+    _kind = _capi.SOLVER_FGM
+
+
+class OGM(_MomentumSolver):
+    """OGM(LeastSquares(A, b), epsilon) (solvers/OGM.cpp); solve(n) applies OGM's final-step
+    factor on iteration n."""
+    _kind = _capi.SOLVER_OGM
+
+
 CGNEf, CGLSf, Landweberf, APGDf = CGNE, CGLS, Landweber, APGD
+SIRTf, FGMf, OGMf = SIRT, FGM, OGM
 
 
 def powerIterations(op, niters=5):

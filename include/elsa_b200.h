@@ -212,7 +212,19 @@ typedef enum elsa_solver_kind {
      * (proximal_operators/ProximalBoxConstraint.cpp:20-40), 2 L1
      * (proximal_operators/ProximalL1.cpp:21-33); params[3] = lower bound, params[4] = upper
      * bound (NaN = no bound; box only), params[5] = L1 weight sigma (default 1). */
-    ELSA_SOLVER_APGD = 3
+    ELSA_SOLVER_APGD = 3,
+    /* SIRT<float>, solvers/SIRT.cpp:8-45 (Landweber with T A^T M, M = 1/(A 1 + 1e-10),
+     * T = 1/(A^T 1)). params[0] = step size (<= 0 or absent: 0.9 * 2 / powerIterations(T A^T M A)).
+     */
+    ELSA_SOLVER_SIRT = 4,
+    /* FGM<float> on LeastSquares(A, b), solvers/FGM.cpp:33-78. params[0] = epsilon (stop once
+     * |grad|^2 <= epsilon^2 |grad_0|^2, default FLT_EPSILON). */
+    ELSA_SOLVER_FGM = 5,
+    /* OGM<float> on LeastSquares(A, b), solvers/OGM.cpp:40-95 (20 power iterations for the
+     * Lipschitz constant). params[0] = epsilon as FGM. The last iteration of each
+     * elsa_solver_iterate call uses OGM's final-step factor, so one call of n iterations matches
+     * OGM::solve(n). */
+    ELSA_SOLVER_OGM = 6
 } elsa_solver_kind;
 
 /* Set up a solver run: allocate its scratch, compute the initial residual (x is zeroed unless
@@ -226,7 +238,8 @@ elsa_status elsa_solver_create(int32_t kind, elsa_projector* projector, const fl
                                int32_t use_x0, const double* params, int32_t num_params,
                                void* stream, elsa_solver** out);
 
-/* Step size in use (Landweber step, APGD mu; 0 for the CG solvers). */
+/* Step size in use (Landweber / SIRT step, APGD mu, FGM / OGM 1 / Lipschitz; 0 for the CG
+ * solvers). */
 elsa_status elsa_solver_step_size(elsa_solver* solver, double* value);
 
 /* Largest eigenvalue of A^T A by `iterations` power iterations from u = 1, in float with float64

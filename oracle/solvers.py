@@ -9,6 +9,8 @@ It restates the reference solvers on float32 vectors, with the projector given a
 * Landweber  solvers/LandweberIteration.cpp:26-72, solvers/Landweber.cpp:20-25
 * APGD       solvers/APGD.cpp:14-102, proximal_operators/ProximalBoxConstraint.cpp:27-40,
              proximal_operators/ProximalL1.cpp:24-38
+* SIRT       solvers/SIRT.cpp:8-45 (Landweber with T A^T M)
+* FGM, OGM   solvers/FGM.cpp:33-78, solvers/OGM.cpp:40-95 on LeastSquares (A^T (A x - b))
 * powerIterations  solvers/PowerIterations.cpp:10-27
 
 Every solver takes dtype=np.float32 (the reference's float instantiation, the parity target) or
@@ -173,3 +175,70 @@ def apgd(A, At, b, domain_size, iterations, x0=None, mu=None, epsilon=F32_EPS, k
             break
         grad = gradient(y)
     return x, float(mu), hist
+
+
+def sirt(A, At, b, domain_size, iterations, x0=None, step=None, power_iters=5,
+         dtype=np.float32):
+    """SIRT: x -= step * T A^T M (A x - b) with M = 1/(A 1 + 1e-10), T = 1/(A^T 1),
+    solvers/SIRT.cpp:20-45 + LandweberIteration.cpp:26-72. Returns (x, step)."""
+    _f = _caster(dtype)
+    m = _f(1.0 / _f(_f(A(np.ones(domain_size, dtype))) + dtype(1e-10)))
+    t = _f(1.0 / _f(At(np.ones(np.asarray(b).size, dtype))))
+
+    def tam_a(v):
+        return _f(t * _f(At(_f(m * _f(A(v))))))
+
+    x = np.zeros(domain_size, dtype) if x0 is None else _f(x0).copy()
+    if step is None or step <= 0:
+        u = np.ones(domain_size, dtype)
+        for _ in range(power_iters):
+            u = tam_a(u)
+            u = _f(u / dtype(np.sqrt(_sq(u))))
+        lam = _dot(u, tam_a(u)) / np.sqrt(_sq(u))
+        step = 0.9 * (2.0 / lam)
+    st = dtype(step)
+    for _ in range(iterations):
+        res = _f(_f(A(x)) - b)
+        x = _f(x - st * _f(t * _f(At(_f(m * res)))))
+    return x, float(step)
+
+
+def _momentum(A, At, b, domain_size, iterations, x0, epsilon, ogm, dtype):
+    _f = _caster(dtype)
+    x = np.zeros(domain_size, dtype) if x0 is None else _f(x0).copy()
+    y_prev = x.copy()
+    lip = power_iterations(A, At, domain_size, 20 if ogm else 5, dtype)
+
+    def grad(v):
+        return _f(At(_f(_f(A(v)) - b)))
+
+    delta0 = _sq(grad(x))
+    theta_prev = 1.0
+    hist = []
+    for i in range(iterations):
+        g = grad(x)
+        gl = _f(g / dtype(lip))
+        y = _f(x - gl)
+        f = 8.0 if (ogm and i == iterations - 1) else 4.0
+        theta = 0.5 * (1.0 + np.sqrt(1.0 + f * theta_prev * theta_prev))
+        x = _f(y + dtype((theta_prev - 1.0) / theta) * _f(y - y_prev))
+        if ogm:
+            x = _f(x - dtype(theta_prev / theta) * gl)
+        theta_prev = theta
+        y_prev = y
+        g2 = _sq(g)
+        hist.append(g2)
+        if g2 <= epsilon * epsilon * delta0:
+            break
+    return x, lip, hist
+
+
+def fgm(A, At, b, domain_size, iterations, x0=None, epsilon=F32_EPS, dtype=np.float32):
+    """Fast gradient method on 0.5 |A x - b|^2, solvers/FGM.cpp:33-78. Returns
+    (x, lipschitz, |grad|^2 history)."""
+    return _momentum(A, At, b, domain_size, iterations, x0, epsilon, False, dtype)
+
+
+def ogm(A, At, b, domain_size, iterations, x0=None, epsilon=F32_EPS, dtype=np.float32):
+    """Optimized gradient method on 0.5 |A x - b|^2, solvers/OGM.cpp:40-95."""
+    return _momentum(A, At, b, domain_size, iterations, x0, epsilon, True, dtype)

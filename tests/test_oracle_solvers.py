@@ -59,3 +59,17 @@ def test_prox_operators():
                                atol=1e-7)
     np.testing.assert_allclose(S.prox(z, 0.5, 2, sigma=0.4), [-1.8, 0, 0, 0.1, 1.3], atol=1e-6)
     np.testing.assert_array_equal(S.prox(z, 0.5, 0), z)
+
+
+def test_sirt_fgm_ogm_converge():
+    M, A, At, b, x = _dense(4, 60, 16)
+    M = np.abs(M)  # SIRT's row / column sums need a non-negative system
+    A = lambda v: M @ np.asarray(v, np.float32)  # noqa: E731
+    At = lambda v: M.T @ np.asarray(v, np.float32)  # noqa: E731
+    b = (M @ x).astype(np.float32)
+    n = M.shape[1]
+    xs, _ = S.sirt(A, At, b, n, 4000, power_iters=200)
+    xf, _, _ = S.fgm(A, At, b, n, 3000, epsilon=0.0)
+    xo, _, _ = S.ogm(A, At, b, n, 3000, epsilon=0.0)
+    for sol in (xs, xf, xo):
+        assert np.linalg.norm(sol - x) <= 2e-2 * np.linalg.norm(x)

@@ -61,7 +61,8 @@ def test_pyelsa_solvers(cuda, oracle):
     r0 = b.squaredL2Norm()
     for solver in (elsa.CGNE(A, b), elsa.CGLS(A, b), elsa.Landweber(A, b),
                    elsa.APGD(A, b, elsa.ProximalBoxConstraint(0.0)),
-                   elsa.FISTA(A, b, elsa.ProximalL1(1e-3))):
+                   elsa.FISTA(A, b, elsa.ProximalL1(1e-3)), elsa.SIRT(A, b),
+                   elsa.FGM(elsa.LeastSquares(A, b)), elsa.OGM(elsa.LeastSquares(A, b))):
         sol = solver.solve(15)
         res = (A.apply(sol) - b).squaredL2Norm()
         assert res < 0.2 * r0, type(solver).__name__

@@ -254,3 +254,32 @@ def test_solver_argument_errors(cuda, oracle):
     with pytest.raises(elsa_b200.InvalidArgumentError):
         elsa_b200.Solver(elsa_b200.SOLVER_APGD, proj, bt.data_ptr(), x.data_ptr(),
                          params=(0.0, 1e-7, 1, 1.0, 0.0))
+
+
+@pytest.mark.parametrize("name", sorted(PROBLEMS))
+def test_sirt_parity(cuda, oracle, name):
+    import elsa_b200
+    from oracle import solvers as S
+    proj, A, At, b, n = _problem(cuda, oracle, name)
+    x, _, step = _run_solver(cuda, proj, elsa_b200.SOLVER_SIRT, b, 12)
+    xr, step_r = S.sirt(A, At, b, n, 12)
+    assert abs(step - step_r) <= 1e-5 * step_r
+    assert rel_l2(x, xr) <= GD_TOL
+
+
+@pytest.mark.parametrize("kind", ["fgm", "ogm"])
+@pytest.mark.parametrize("name", sorted(PROBLEMS))
+def test_fgm_ogm_parity(cuda, oracle, name, kind):
+    import elsa_b200
+    from oracle import solvers as S
+    proj, A, At, b, n = _problem(cuda, oracle, name)
+    sk = elsa_b200.SOLVER_FGM if kind == "fgm" else elsa_b200.SOLVER_OGM
+    x, g2, step = _run_solver(cuda, proj, sk, b, 10)
+    xr, lip, hist = getattr(S, kind)(A, At, b, n, 10)
+    assert abs(step - 1.0 / lip) <= 1e-5 / lip
+    # accelerated gradient methods amplify rounding like CG: same bound as the CG solvers
+    A64, At64 = _f64_ops(oracle, name)
+    x64, _, h64 = getattr(S, kind)(A64, At64, b, n, 10, dtype=np.float64)
+    bx, br = _cg_bound(xr, x64, hist, h64)
+    assert rel_l2(x, xr) <= bx
+    assert abs(g2 - hist[-1]) <= br
