@@ -291,11 +291,12 @@ namespace elsa_b200
     }
 
     // SIRT: Landweber with T A^T M, M = 1 / (A 1 + 1e-10), T = 1 / (A^T 1),
-    // solvers/SIRT.cpp:20-45 with LandweberIteration.cpp:57-67. ws.vol0 = T, ws.sino1 = M.
+    // solvers/SIRT.cpp:20-45 with LandweberIteration.cpp:57-67. ws.vol3 = T, ws.sino1 = M (the
+    // power iterations use vol0, vol1 and sino0).
     static void sirtBegin(Projector& A, SolverWorkspace& ws, cudaStream_t s)
     {
         const int64_t n = A.domainSize(), m = A.rangeSize();
-        float* tinv = ws.vol0.as<float>();
+        float* tinv = ws.vol3.as<float>();
         float* minv = ws.sino1.as<float>();
         launchFill(ws.vol1.as<float>(), 1.0f, n, s);
         A.forward(ws.vol1.as<float>(), minv, s); // row sums
@@ -317,7 +318,7 @@ namespace elsa_b200
         launchSubMul(sino, b, ws.sino1.as<float>(), sino, m, s); // M (A x - b)
         A.adjoint(sino, q, s);
         t.mark(s);
-        launchScaledStep(x, step, ws.vol0.as<float>(), q, n, s); // x -= step T A^T M (A x - b)
+        launchScaledStep(x, step, ws.vol3.as<float>(), q, n, s); // x -= step T A^T M (A x - b)
     }
 
     // FGM / OGM on the least-squares problem 0.5 |A x - b|^2 (solvers/FGM.cpp:33-78,
@@ -386,7 +387,7 @@ namespace elsa_b200
                         ? opt_.sirtStep
                         : 0.9 * (2.0 / powerIterationsAtA(A_, ws_, opt_.powerIterations, s,
                                                           ws_.sino1.as<float>(),
-                                                          ws_.vol0.as<float>()));
+                                                          ws_.vol3.as<float>()));
             if (!useX0)
                 launchFill(x_, 0.0f, A_.domainSize(), s);
             ELSA_CUDA(cudaMemsetAsync(ws_.scalars.as<SolverScalars>(), 0, sizeof(SolverScalars),

@@ -12,9 +12,10 @@ pytestmark = pytest.mark.gpu
 # Solver tolerance: relative L2 of the iterate after the stated number of iterations against the
 # FP32 oracle. Both sides run float32 vectors with float64 inner products over projectors that
 # agree to ~3e-7. Landweber/APGD are contractions and stay within 1e-5. CG-type recurrences
-# amplify rounding differences on ill-conditioned problems, so there the bound is 1e-4 or twice
-# the distance of the FP32 oracle itself from the FP64 oracle, whichever is larger: the device
-# result must be as close to the FP32 reference as that reference is to exact arithmetic.
+# amplify rounding differences on ill-conditioned problems, so there the bound is 1e-4 or four
+# times the distance of the FP32 oracle itself from the FP64 oracle, whichever is larger: the
+# device result must be about as close to the FP32 reference as that reference is to exact
+# arithmetic (its reductions and fused operations round differently from both).
 CG_TOL = 1e-4
 GD_TOL = 1e-5
 
@@ -112,8 +113,8 @@ def _f64_ops(oracle, name):
 
 def _cg_bound(x32, x64, hist32, hist64):
     """(iterate bound, last-residual bound) for a CG-type solver, see CG_TOL."""
-    return (max(CG_TOL, 2.0 * rel_l2(x32, x64)),
-            max(1e-3 * hist32[-1], 2.0 * abs(hist32[-1] - hist64[-1])))
+    return (max(CG_TOL, 4.0 * rel_l2(x32, x64)),
+            max(1e-3 * hist32[-1], 4.0 * abs(hist32[-1] - hist64[-1])))
 
 
 def _run_solver(torch, proj, kind, b_np, iterations, params=(), x0=None, chunks=1):
