@@ -29,6 +29,7 @@
 #include "joseph_tma.cuh"
 #include "projector.hpp"
 #include "raysetup.cuh"
+#include "solvers.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -522,8 +523,11 @@ namespace elsa_b200
                                 const float* __restrict__ y,
                                 const RayWindow* __restrict__ windows,
                                 const unsigned* __restrict__ viewAxes, VolumeShape vol,
-                                DetectorShape det, int m, int3 nBricks, float* __restrict__ x)
+                                DetectorShape det, int m, int3 nBricks, int viewsPerChunk,
+                                float* __restrict__ x)
         {
+            // blockIdx.y selects a chunk of views; with several chunks each CTA writes its
+            // partial brick to x + chunk * nvox and a second pass sums the chunks in order
             extern __shared__ float smem[];
             using L = BrickLayout<DIM, BX, BY>;
             constexpr int NT = NW * 32;
@@ -535,15 +539,19 @@ namespace elsa_b200
             const int org0 = (bi % nBricks.x) * BX, org1 = ((bi / nBricks.x) % nBricks.y) * BY,
                       org2 = (bi / (nBricks.x * nBricks.y)) * BZ;
             const int nb = nBricks.x * nBricks.y * nBricks.z;
+            const int pBegin = blockIdx.y * viewsPerChunk;
+            const int pEnd = min(det.np, pBegin + viewsPerChunk);
             for (int i = threadIdx.x; i < kWords; i += NT)
                 acc[i] = 0.0f;
-            for (int p = threadIdx.x; p < det.np; p += NT) {
+            for (int p = pBegin + threadIdx.x; p < pEnd; p += NT) {
                 const RayWindow w = windows[static_cast<int64_t>(p) * nb + bi];
                 win[p] = w;
                 axes[p] = (w.u0 > w.u1 || w.v0 > w.v1) ? 0u : viewAxes[p];
             }
             __syncthreads();
-            for (int p = 0; p < det.np; ++p) {
+            const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
+            float* out = x + blockIdx.y * nvox;
+            for (int p = pBegin; p < pEnd; ++p) {
                 const unsigned ax = axes[p];
                 if (!(ax & 7u))
                     continue;
@@ -569,10 +577,23 @@ namespace elsa_b200
                 const int lx = i % BX, ly = (i / BX) % BY, lz = i / (BX * BY);
                 const int gx = org0 + lx, gy = org1 + ly, gz = org2 + lz;
                 if (gx < vol.n[0] && gy < vol.n[1] && gz < vol.n[2])
-                    x[gx + static_cast<int64_t>(vol.n[0]) *
-                               (gy + static_cast<int64_t>(vol.n[1]) * gz)] =
+                    out[gx + static_cast<int64_t>(vol.n[0]) *
+                                 (gy + static_cast<int64_t>(vol.n[1]) * gz)] =
                         acc[lz * L::kPlane + ly * L::kRow + lx];
             }
+        }
+
+        // x[v] = sum over chunks c = 0, 1, ... of partial[c][v], in chunk order
+        __global__ void sumChunksKernel(const float* __restrict__ partial, int chunks,
+                                        int64_t nvox, float* __restrict__ x)
+        {
+            const int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (v >= nvox)
+                return;
+            float s = partial[v];
+            for (int c = 1; c < chunks; ++c)
+                s = s + partial[c * nvox + v];
+            x[v] = s;
         }
 
         template <int DIM, int BX, int BY, int BZ, int CPD, int NW>
@@ -595,14 +616,31 @@ namespace elsa_b200
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(smemBytes(np))));
             }
+            // Views per chunk so that bricks x chunks fills about two CTAs per SM.
+            static int chunks(int nbricks, int np)
+            {
+                const int want = (2 * 148 + nbricks - 1) / nbricks;
+                return want < 1 ? 1 : (want > np ? np : want);
+            }
+            // partial: scratch of chunks(nbricks, np) volumes (unused with one chunk)
             static void launch(int nbricks, cudaStream_t s, const JosephRay* rays,
                                const float2* cps, int64_t nrays, const float* y,
                                const RayWindow* win, const unsigned* axes, VolumeShape vol,
-                               DetectorShape det, int m, int3 nb, float* x)
+                               DetectorShape det, int m, int3 nb, float* x, float* partial)
             {
+                const int nc = chunks(nbricks, det.np);
+                const int per = (det.np + nc - 1) / nc;
+                const int used = (det.np + per - 1) / per;
+                const dim3 grid(static_cast<unsigned>(nbricks), static_cast<unsigned>(used));
                 josephAdjointKernel<DIM, BX, BY, BZ, CPD, NW>
-                    <<<nbricks, kThreads, smemBytes(det.np), s>>>(rays, cps, nrays, y, win, axes,
-                                                                  vol, det, m, nb, x);
+                    <<<grid, kThreads, smemBytes(det.np), s>>>(rays, cps, nrays, y, win, axes,
+                                                               vol, det, m, nb, per,
+                                                               used > 1 ? partial : x);
+                if (used > 1) {
+                    const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
+                    sumChunksKernel<<<static_cast<unsigned>((nvox + 255) / 256), 256, 0, s>>>(
+                        partial, used, nvox, x);
+                }
             }
         };
 
@@ -900,6 +938,13 @@ namespace elsa_b200
                 josephWindowKernel<<<static_cast<unsigned>((nwin + 255) / 256), 256>>>(
                     dPoses_, vol_, det_, brick_, nBricks_, dWindows_);
                 ELSA_LAUNCH_CHECK("josephWindowKernel");
+                if (vol_.dim == 2) {
+                    const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
+                    const int nc = Adjoint2d::chunks(nb, det_.np);
+                    if (nc > 1)
+                        partial_ = std::make_unique<DeviceBuffer>(sizeof(float) * domainSize_ *
+                                                                  static_cast<size_t>(nc));
+                }
                 if (vol_.dim == 3) {
                     std::vector<float> hp(poses_.size() * kPoseFloats);
                     std::memcpy(hp.data(), poses_.data(), sizeof(float) * hp.size());
@@ -981,7 +1026,8 @@ namespace elsa_b200
                                       dViewAxes_, vol_, det_, classSpacing_, nBricks_, x);
                 else
                     Adjoint2d::launch(nb, s, dRays_, dCheckpoints_, rangeSize_, y, dWindows_,
-                                      dViewAxes_, vol_, det_, classSpacing_, nBricks_, x);
+                                      dViewAxes_, vol_, det_, classSpacing_, nBricks_, x,
+                                      partial_ ? partial_->as<float>() : nullptr);
                 ELSA_LAUNCH_CHECK("josephAdjointKernel");
             }
 
@@ -1016,6 +1062,7 @@ namespace elsa_b200
             int classSpacing_ = 0;
             int64_t sampleCount_ = 0;
             std::unique_ptr<JosephForwardTma> tma_;
+            std::unique_ptr<DeviceBuffer> partial_; // 2D adjoint: per view-chunk partial volumes
             int3 brick_{}, nBricks_{};
         };
     } // namespace
