@@ -596,6 +596,11 @@ namespace elsa_b200
             x[v] = s;
         }
 
+#ifndef ELSA_ADJ2D_CTAS_PER_SM
+#define ELSA_ADJ2D_CTAS_PER_SM 16
+#endif
+        constexpr int kAdjoint2dCtasPerSm = ELSA_ADJ2D_CTAS_PER_SM;
+
         template <int DIM, int BX, int BY, int BZ, int CPD, int NW>
         struct AdjointConfig {
             using L = BrickLayout<DIM, BX, BY>;
@@ -616,10 +621,12 @@ namespace elsa_b200
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(smemBytes(np))));
             }
-            // Views per chunk so that bricks x chunks fills about two CTAs per SM.
+            // Views per chunk so that bricks x chunks fills about kAdjoint2dCtasPerSm CTAs per SM
+            // (16 measured best among 1-16 at 128^2 x 180 views and 512^2 x 720 views). The
+            // partial volumes then hold fewer than 2 x 16 x 148 tiles of 64 x 64 floats (78 MB).
             static int chunks(int nbricks, int np)
             {
-                const int want = (2 * 148 + nbricks - 1) / nbricks;
+                const int want = (kAdjoint2dCtasPerSm * 148 + nbricks - 1) / nbricks;
                 return want < 1 ? 1 : (want > np ? np : want);
             }
             // partial: scratch of chunks(nbricks, np) volumes (unused with one chunk)
