@@ -35,6 +35,12 @@
 #include <cmath>
 #include <cstring>
 
+#ifndef ELSA_ADJ_BZ
+#define ELSA_ADJ_BZ 16 // z depth of the 3D adjoint's warp brick (x and y: one checkpoint slab)
+#endif
+#ifndef ELSA_ADJ_MIN_BLOCKS
+#define ELSA_ADJ_MIN_BLOCKS 1 // resident one-warp blocks per SM asked of the register allocator
+#endif
 #ifndef ELSA_SPLAT_UNROLL
 #define ELSA_SPLAT_UNROLL 2 // unroll factor of the adjoint's per-sample loop (1: 72.8 ms, 2: 63.4 ms, 4: 68.9 ms at 256^3)
 #endif
@@ -600,6 +606,10 @@ namespace elsa_b200
 #define ELSA_ADJ2D_CTAS_PER_SM 16
 #endif
         constexpr int kAdjoint2dCtasPerSm = ELSA_ADJ2D_CTAS_PER_SM;
+#ifndef ELSA_ADJ3D_WARPS_PER_SM
+#define ELSA_ADJ3D_WARPS_PER_SM 22
+#endif
+        constexpr int kAdjoint3dWarpsPerSm = ELSA_ADJ3D_WARPS_PER_SM;
 
         template <int DIM, int BX, int BY, int BZ, int CPD, int NW>
         struct AdjointConfig {
@@ -758,6 +768,10 @@ namespace elsa_b200
             const int orgA = G == 0 ? org1 : org0;
             const int orgB = G == 2 ? org1 : org2;
             const int kLo = orgG, kHi = orgG + AR::extG - 1;
+            // a brick thinner than a checkpoint slab along G starts its rays from the slab's
+            // checkpoint and advances them to the brick's first plane
+            constexpr bool kPartialSlab = AR::extG < CPD;
+            const int slabLo = (orgG / CPD) * CPD, slabHi = slabLo + CPD - 1;
             const int lane = threadIdx.x & 31;
             const int64_t viewBase = static_cast<int64_t>(det.nu) * det.nv * p;
             for (int ov = 0; ov < m; ++ov) {
@@ -801,8 +815,17 @@ namespace elsa_b200
                             int jLo, jHi;
                             if (!sampleRange(R, kLo, kHi, jLo, jHi))
                                 continue;
+                            float2 cp = cpb[q];
+                            if (kPartialSlab) {
+                                int jS0, jS1;
+                                sampleRange(R, slabLo, slabHi, jS0, jS1);
+                                for (int j = jS0; j < jLo; ++j) {
+                                    cp.x = __fadd_rn(cp.x, R.sa);
+                                    cp.y = __fadd_rn(cp.y, R.sb);
+                                }
+                            }
                             warpSplat<G, BX, BY, BZ>(acc, acc + WarpBrick<BX, BY>::kPlane * BZ,
-                                                     R, yb[q] * R.len, cpb[q], jLo, jHi, orgG,
+                                                     R, yb[q] * R.len, cp, jLo, jHi, orgG,
                                                      orgA, orgB);
                         }
                     }
@@ -814,14 +837,17 @@ namespace elsa_b200
         // 3D adjoint: one warp per brick of BX x BY x BZ voxels; the brick accumulates every
         // view in a fixed order (view, axis, class, lane round) and is written once.
         template <int BX, int BY, int BZ, int CPD>
-        __global__ void __launch_bounds__(32)
+        __global__ void __launch_bounds__(32, ELSA_ADJ_MIN_BLOCKS)
             josephAdjointWarpKernel(const JosephRay* __restrict__ rays,
                                     const float2* __restrict__ checkpoints, int64_t nrays,
                                     const float* __restrict__ y,
                                     const RayWindow* __restrict__ windows,
                                     const unsigned* __restrict__ viewAxes, VolumeShape vol,
-                                    DetectorShape det, int m, int3 nBricks, float* __restrict__ x)
+                                    DetectorShape det, int m, int3 nBricks, int viewsPerChunk,
+                                    float* __restrict__ x)
         {
+            // blockIdx.y selects a chunk of views, as in the 2D kernel: with several chunks the
+            // brick goes to x + chunk * nvox and sumChunksKernel adds the chunks in order
             using L = WarpBrick<BX, BY>;
             __shared__ float acc[L::kPlane * BZ + 1]; // + dummy word for taps outside
             const int lane = threadIdx.x;
@@ -832,7 +858,9 @@ namespace elsa_b200
             for (int i = lane; i < L::kPlane * BZ; i += 32)
                 acc[i] = 0.0f;
             __syncwarp();
-            for (int p = 0; p < det.np; ++p) {
+            const int pBegin = blockIdx.y * viewsPerChunk;
+            const int pEnd = min(det.np, pBegin + viewsPerChunk);
+            for (int p = pBegin; p < pEnd; ++p) {
                 const RayWindow w = windows[static_cast<int64_t>(p) * nb + bi];
                 if (w.u0 > w.u1 || w.v0 > w.v1)
                     continue;
@@ -847,12 +875,14 @@ namespace elsa_b200
                     warpView<2, BX, BY, BZ, CPD>(acc, w, p, m, rays, checkpoints, nrays, y, det,
                                                  org0, org1, org2);
             }
+            const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
+            float* out = x + blockIdx.y * nvox;
             for (int i = lane; i < BX * BY * BZ; i += 32) {
                 const int lx = i % BX, ly = (i / BX) % BY, lz = i / (BX * BY);
                 const int gx = org0 + lx, gy = org1 + ly, gz = org2 + lz;
                 if (gx < vol.n[0] && gy < vol.n[1] && gz < vol.n[2])
-                    x[gx + static_cast<int64_t>(vol.n[0]) *
-                               (gy + static_cast<int64_t>(vol.n[1]) * gz)] =
+                    out[gx + static_cast<int64_t>(vol.n[0]) *
+                                 (gy + static_cast<int64_t>(vol.n[1]) * gz)] =
                         acc[lz * L::kPlane + ly * L::kRow + lx];
             }
         }
@@ -860,21 +890,41 @@ namespace elsa_b200
         template <int BX, int BY, int BZ, int CPD>
         struct WarpAdjointConfig {
             static constexpr int kCheckpointDepth = CPD;
-            static_assert(BX == CPD && BY == CPD && BZ == CPD,
-                          "a warp brick is exactly one checkpoint slab deep along every axis");
+            static_assert(BX == CPD && BY == CPD && BZ <= CPD && CPD % BZ == 0,
+                          "a warp brick is one checkpoint slab deep along x and y and a whole "
+                          "fraction of one along z");
             static int3 brick() { return make_int3(BX, BY, BZ); }
             static void prepare(int) {}
+            // View chunks so that bricks x chunks reach kAdjoint3dWarpsPerSm one-warp CTAs per
+            // SM (about two waves of the 11 bricks that fit in shared memory at once); a 256^3
+            // volume has 4096 bricks and keeps one chunk.
+            static int chunks(int nbricks, int np)
+            {
+                const int want = (kAdjoint3dWarpsPerSm * 148 + nbricks - 1) / nbricks;
+                return want < 1 ? 1 : (want > np ? np : want);
+            }
+            // partial: scratch of chunks(nbricks, np) volumes (unused with one chunk)
             static void launch(int nbricks, cudaStream_t s, const JosephRay* rays,
                                const float2* cps, int64_t nrays, const float* y,
                                const RayWindow* win, const unsigned* axes, VolumeShape vol,
-                               DetectorShape det, int m, int3 nb, float* x)
+                               DetectorShape det, int m, int3 nb, float* x, float* partial)
             {
-                josephAdjointWarpKernel<BX, BY, BZ, CPD><<<nbricks, 32, 0, s>>>(
-                    rays, cps, nrays, y, win, axes, vol, det, m, nb, x);
+                const int nc = chunks(nbricks, det.np);
+                const int per = (det.np + nc - 1) / nc;
+                const int used = (det.np + per - 1) / per;
+                const dim3 grid(static_cast<unsigned>(nbricks), static_cast<unsigned>(used));
+                josephAdjointWarpKernel<BX, BY, BZ, CPD><<<grid, 32, 0, s>>>(
+                    rays, cps, nrays, y, win, axes, vol, det, m, nb, per,
+                    used > 1 ? partial : x);
+                if (used > 1) {
+                    const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
+                    sumChunksKernel<<<static_cast<unsigned>((nvox + 255) / 256), 256, 0, s>>>(
+                        partial, used, nvox, x);
+                }
             }
         };
 
-        using Adjoint3d = WarpAdjointConfig<16, 16, 16, 16>;
+        using Adjoint3d = WarpAdjointConfig<16, 16, ELSA_ADJ_BZ, 16>;
         using Adjoint2d = AdjointConfig<2, 64, 64, 1, 64, 8>;
 
         class JosephProjector final : public Projector
@@ -945,9 +995,10 @@ namespace elsa_b200
                 josephWindowKernel<<<static_cast<unsigned>((nwin + 255) / 256), 256>>>(
                     dPoses_, vol_, det_, brick_, nBricks_, dWindows_);
                 ELSA_LAUNCH_CHECK("josephWindowKernel");
-                if (vol_.dim == 2) {
+                {
                     const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
-                    const int nc = Adjoint2d::chunks(nb, det_.np);
+                    const int nc = vol_.dim == 2 ? Adjoint2d::chunks(nb, det_.np)
+                                                 : Adjoint3d::chunks(nb, det_.np);
                     if (nc > 1)
                         partial_ = std::make_unique<DeviceBuffer>(sizeof(float) * domainSize_ *
                                                                   static_cast<size_t>(nc));
@@ -1030,7 +1081,8 @@ namespace elsa_b200
                 const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
                 if (vol_.dim == 3)
                     Adjoint3d::launch(nb, s, dRays_, dCheckpoints_, rangeSize_, y, dWindows_,
-                                      dViewAxes_, vol_, det_, classSpacing_, nBricks_, x);
+                                      dViewAxes_, vol_, det_, classSpacing_, nBricks_, x,
+                                      partial_ ? partial_->as<float>() : nullptr);
                 else
                     Adjoint2d::launch(nb, s, dRays_, dCheckpoints_, rangeSize_, y, dWindows_,
                                       dViewAxes_, vol_, det_, classSpacing_, nBricks_, x,
@@ -1053,8 +1105,8 @@ namespace elsa_b200
                     return tma_ ? static_cast<int64_t>(tma_->fallbackFraction() * 1e6) : -1;
                 case 6: // kernel launches per forward call
                     return tma_ ? tma_->launchesPerForward() : 1;
-                case 7: // kernel launches per adjoint call
-                    return 1;
+                case 7: // kernel launches per adjoint call (with view chunks: + the chunk sum)
+                    return partial_ ? 2 : 1;
                 default:
                     return -1;
                 }
@@ -1069,7 +1121,7 @@ namespace elsa_b200
             int classSpacing_ = 0;
             int64_t sampleCount_ = 0;
             std::unique_ptr<JosephForwardTma> tma_;
-            std::unique_ptr<DeviceBuffer> partial_; // 2D adjoint: per view-chunk partial volumes
+            std::unique_ptr<DeviceBuffer> partial_; // adjoint: per view-chunk partial volumes
             int3 brick_{}, nBricks_{};
         };
     } // namespace
