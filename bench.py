@@ -248,6 +248,7 @@ def run_elsa(args):
     if prof and prof.get("kernel") == dominant:
         traffic = prof.get("dram_bytes_per_launch")
     compulsory = 4.0 * (proj.domain_size + proj.range_size)
+    pair_achieved = 2.0 * bytes_per_pass / ((fwd_avg + adj_avg) / 1e3) / 1e9
 
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "GUPS", "n_gpus": world,
@@ -267,7 +268,11 @@ def run_elsa(args):
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "algorithmic_bytes_per_launch": bytes_per_pass,
                      "samples_per_launch": samples,
-                     "compulsory_frac": round(compulsory / (dom_ms / 1e3) / 1e9 / peak, 5)},
+                     "compulsory_frac": round(compulsory / (dom_ms / 1e3) / 1e9 / peak, 5),
+                     # forward + matched adjoint together: two passes of gather bytes over
+                     # the sum of the two kernels' mean durations
+                     "forward_back_achieved": round(pair_achieved, 1),
+                     "forward_back_frac": round(pair_achieved / peak, 4)},
         "gpu_launches": (proj.info(6) + proj.info(7) + VECTOR_LAUNCHES_PER_STEP) * args.steps,
         "clocks": clock_info,
     }
