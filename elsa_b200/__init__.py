@@ -12,7 +12,10 @@ from ._capi import (ElsaError, InvalidArgumentError, Projector, Solver,  # noqa:
                     circle_trajectory, pose_2d, pose_3d, power_iterations, solve_batch, POSE_FLOATS,
                     PROJECTOR_JOSEPH, PROJECTOR_SIDDON, SOLVER_CGNE, SOLVER_CGLS,
                     SOLVER_LANDWEBER, SOLVER_APGD, SOLVER_SIRT, SOLVER_FGM,
-                    SOLVER_OGM, PROX_IDENTITY, PROX_BOX, PROX_L1)
+                    SOLVER_OGM, PROX_IDENTITY, PROX_BOX, PROX_L1, KNOB_FORWARD_THREADS,
+                    KNOB_ADJOINT_CHUNKS, KNOB_ADJOINT_THREADS, tune_cache_size,
+                    tune_cache_clear, tune_cache_save, tune_cache_load, tune_cache_put,
+                    tune_cache_get)
 
 __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "voxel_lut",
            "PROJECTOR_BLOB", "PROJECTOR_BSPLINE", "PROJECTOR_PHASE_CONTRAST_BLOB",
@@ -22,4 +25,6 @@ __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "voxel_lu
            "PROJECTOR_SIDDON", "SOLVER_CGNE", "SOLVER_CGLS", "SOLVER_LANDWEBER", "SOLVER_APGD",
            "SOLVER_SIRT", "SOLVER_FGM", "SOLVER_OGM",
            "PROX_IDENTITY",
-           "PROX_BOX", "PROX_L1"]
+           "PROX_BOX", "PROX_L1", "KNOB_FORWARD_THREADS", "KNOB_ADJOINT_CHUNKS",
+           "KNOB_ADJOINT_THREADS", "tune_cache_size", "tune_cache_clear", "tune_cache_save",
+           "tune_cache_load", "tune_cache_put", "tune_cache_get"]

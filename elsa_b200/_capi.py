@@ -39,6 +39,11 @@ SOLVER_OGM = 6
 PROX_IDENTITY = 0
 PROX_BOX = 1
 PROX_L1 = 2
+KNOB_FORWARD_THREADS = 0
+KNOB_ADJOINT_CHUNKS = 1
+KNOB_ADJOINT_THREADS = 2
+KNOB_COUNT = 3
+KNOB_NAMES = ("forward_threads", "adjoint_chunks", "adjoint_threads")
 
 # Every function the header declares: name -> (restype, argtypes)
 _vp = ctypes.c_void_p
@@ -58,6 +63,16 @@ SIGNATURES = {
     "elsa_projector_destroy": (_st, [_vp]),
     "elsa_projector_sizes": (_st, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "elsa_projector_info": (_st, [_vp, _i32, ctypes.POINTER(_i64)]),
+    "elsa_projector_get_knob": (_st, [_vp, _i32, ctypes.POINTER(_i32)]),
+    "elsa_projector_knob_candidates": (_st, [_vp, _i32, _vp, _i32, ctypes.POINTER(_i32)]),
+    "elsa_projector_set_knob": (_st, [_vp, _i32, _i32]),
+    "elsa_projector_autotune": (_st, [_vp, _vp, _i32, _vp, ctypes.POINTER(_i32)]),
+    "elsa_tune_cache_size": (_st, [ctypes.POINTER(_i64)]),
+    "elsa_tune_cache_clear": (_st, []),
+    "elsa_tune_cache_save": (_st, [ctypes.c_char_p]),
+    "elsa_tune_cache_load": (_st, [ctypes.c_char_p]),
+    "elsa_tune_cache_put": (_st, [ctypes.c_char_p, _vp]),
+    "elsa_tune_cache_get": (_st, [ctypes.c_char_p, _vp, ctypes.POINTER(_i32)]),
     "elsa_projector_apply": (_st, [_vp, _vp, _vp, _vp]),
     "elsa_projector_apply_adjoint": (_st, [_vp, _vp, _vp, _vp]),
     "elsa_projector_apply_host": (_st, [_vp, _vp, _vp]),
@@ -200,6 +215,33 @@ class Projector:
         call("elsa_projector_info", self._h, int(key), ctypes.byref(v))
         return v.value
 
+    def knob(self, knob):
+        """Current value of a launch knob (KNOB_*), -1 when this projector does not use it."""
+        v = ctypes.c_int32()
+        call("elsa_projector_get_knob", self._h, int(knob), ctypes.byref(v))
+        return v.value
+
+    def knob_candidates(self, knob):
+        """Values the autotuner may try for `knob` on this geometry ([] when fixed)."""
+        n = ctypes.c_int32()
+        call("elsa_projector_knob_candidates", self._h, int(knob), None, 0, ctypes.byref(n))
+        out = np.zeros(max(1, n.value), np.int32)
+        call("elsa_projector_knob_candidates", self._h, int(knob), np_ptr(out), int(out.size),
+             ctypes.byref(n))
+        return [int(v) for v in out[:n.value]]
+
+    def set_knob(self, knob, value):
+        call("elsa_projector_set_knob", self._h, int(knob), int(value))
+
+    def autotune(self, stream=None, force=False):
+        """Time the candidates of every knob and keep the fastest (or take the tuning cache's
+        entry for this shape). Returns ({knob name: value}, from_cache)."""
+        vals = np.full(KNOB_COUNT, -1, np.int32)
+        hit = ctypes.c_int32()
+        call("elsa_projector_autotune", self._h, ctypes.c_void_p(stream or 0), int(bool(force)),
+             np_ptr(vals), ctypes.byref(hit))
+        return {KNOB_NAMES[k]: int(vals[k]) for k in range(KNOB_COUNT)}, bool(hit.value)
+
     def apply_ptr(self, x_ptr, y_ptr, stream=None):
         call("elsa_projector_apply", self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
              ctypes.c_void_p(stream or 0))
@@ -234,6 +276,41 @@ class Projector:
             self.close()
         except Exception:
             pass
+
+
+def tune_cache_size():
+    n = ctypes.c_int64()
+    call("elsa_tune_cache_size", ctypes.byref(n))
+    return n.value
+
+
+def tune_cache_clear():
+    call("elsa_tune_cache_clear")
+
+
+def tune_cache_save(path):
+    """Write the process-wide tuning cache to a text file (one line per projector shape)."""
+    call("elsa_tune_cache_save", os.fsencode(path))
+
+
+def tune_cache_load(path):
+    """Add the entries of a file written by tune_cache_save to the tuning cache."""
+    call("elsa_tune_cache_load", os.fsencode(path))
+
+
+def tune_cache_put(key, values):
+    v = np.ascontiguousarray(values, np.int32)
+    if v.size != KNOB_COUNT:
+        raise InvalidArgumentError(1, "tune_cache_put: need %d knob values" % KNOB_COUNT)
+    call("elsa_tune_cache_put", key.encode(), np_ptr(v))
+
+
+def tune_cache_get(key):
+    """Knob values cached under `key` ("kind:dim:nx,ny,nz:nu,nv,np"), or None."""
+    v = np.zeros(KNOB_COUNT, np.int32)
+    found = ctypes.c_int32()
+    call("elsa_tune_cache_get", key.encode(), np_ptr(v), ctypes.byref(found))
+    return [int(a) for a in v] if found.value else None
 
 
 def voxel_lut(kind, dim, params=(), samples=100):

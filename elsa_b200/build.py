@@ -43,9 +43,10 @@ CXX_UNITS = [
     ("geometry.cpp", []),
     ("luts.cpp", []),
     ("capi.cpp", []),
+    ("tune.cpp", []),
 ]
 HEADERS = ["internal.cuh", "raysetup.cuh", "joseph_tma.cuh", "projector.hpp", "geometry.hpp", "vecops.cuh",
-           "solvers.hpp", "luts.hpp", "voxel.hpp"]
+           "solvers.hpp", "luts.hpp", "voxel.hpp", "tune.hpp"]
 
 
 def _stale(target, deps):

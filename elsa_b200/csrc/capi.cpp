@@ -13,6 +13,7 @@
 #include "internal.cuh"
 #include "projector.hpp"
 #include "solvers.hpp"
+#include "tune.hpp"
 #include "voxel.hpp"
 
 struct elsa_solver {
@@ -284,6 +285,114 @@ elsa_status elsa_projector_info(const elsa_projector* p, int32_t key, int64_t* v
     return guarded([&] {
         require(p && value, "elsa_projector_info: null argument");
         *value = p->impl->info(key);
+    });
+}
+
+elsa_status elsa_projector_get_knob(const elsa_projector* p, int32_t knob, int32_t* value)
+{
+    return guarded([&] {
+        require(p && value, "elsa_projector_get_knob: null argument");
+        require(knob >= 0 && knob < ELSA_KNOB_COUNT, "elsa_projector_get_knob: unknown knob");
+        *value = p->impl->knob(knob);
+    });
+}
+
+elsa_status elsa_projector_knob_candidates(const elsa_projector* p, int32_t knob,
+                                           int32_t* values, int32_t capacity, int32_t* count)
+{
+    return guarded([&] {
+        require(p && count, "elsa_projector_knob_candidates: null argument");
+        require(knob >= 0 && knob < ELSA_KNOB_COUNT,
+                "elsa_projector_knob_candidates: unknown knob");
+        require(capacity >= 0 && (capacity == 0 || values),
+                "elsa_projector_knob_candidates: bad output buffer");
+        const std::vector<int> c = p->impl->knobCandidates(knob);
+        *count = static_cast<int32_t>(c.size());
+        for (int32_t i = 0; i < capacity && i < static_cast<int32_t>(c.size()); ++i)
+            values[i] = c[i];
+    });
+}
+
+elsa_status elsa_projector_set_knob(elsa_projector* p, int32_t knob, int32_t value)
+{
+    return guarded([&] {
+        require(p, "elsa_projector_set_knob: null argument");
+        require(knob >= 0 && knob < ELSA_KNOB_COUNT, "elsa_projector_set_knob: unknown knob");
+        onDevice(p);
+        ELSA_CUDA(cudaDeviceSynchronize()); // no launch of the old configuration in flight
+        p->impl->setKnob(knob, value);
+    });
+}
+
+elsa_status elsa_projector_autotune(elsa_projector* p, void* stream, int32_t force,
+                                    int32_t* values, int32_t* fromCache)
+{
+    return guarded([&] {
+        require(p, "elsa_projector_autotune: null argument");
+        onDevice(p);
+        ELSA_CUDA(cudaStreamSynchronize(asStream(stream)));
+        const elsa_b200::TuneResult r =
+            elsa_b200::autotune(*p->impl, asStream(stream), force != 0);
+        if (values)
+            for (int k = 0; k < ELSA_KNOB_COUNT; ++k)
+                values[k] = r.values[k];
+        if (fromCache)
+            *fromCache = r.fromCache ? 1 : 0;
+    });
+}
+
+elsa_status elsa_tune_cache_size(int64_t* entries)
+{
+    return guarded([&] {
+        require(entries != nullptr, "elsa_tune_cache_size: null argument");
+        *entries = static_cast<int64_t>(elsa_b200::tuneCacheSize());
+    });
+}
+
+elsa_status elsa_tune_cache_clear(void)
+{
+    return guarded([&] { elsa_b200::tuneCacheClear(); });
+}
+
+elsa_status elsa_tune_cache_save(const char* path)
+{
+    return guarded([&] {
+        require(path != nullptr, "elsa_tune_cache_save: null path");
+        elsa_b200::tuneCacheSave(path);
+    });
+}
+
+elsa_status elsa_tune_cache_load(const char* path)
+{
+    return guarded([&] {
+        require(path != nullptr, "elsa_tune_cache_load: null path");
+        elsa_b200::tuneCacheLoad(path);
+    });
+}
+
+elsa_status elsa_tune_cache_put(const char* key, const int32_t* values)
+{
+    return guarded([&] {
+        require(key && values, "elsa_tune_cache_put: null argument");
+        elsa_b200::KnobValues v{};
+        for (int k = 0; k < ELSA_KNOB_COUNT; ++k) {
+            require(values[k] >= -1, "elsa_tune_cache_put: knob values must be >= -1");
+            v[k] = values[k];
+        }
+        elsa_b200::tuneCachePut(key, v);
+    });
+}
+
+elsa_status elsa_tune_cache_get(const char* key, int32_t* values, int32_t* found)
+{
+    return guarded([&] {
+        require(key && values && found, "elsa_tune_cache_get: null argument");
+        elsa_b200::KnobValues v{};
+        const bool hit = elsa_b200::tuneCacheGet(key, v);
+        *found = hit ? 1 : 0;
+        if (hit)
+            for (int k = 0; k < ELSA_KNOB_COUNT; ++k)
+                values[k] = v[k];
     });
 }
 

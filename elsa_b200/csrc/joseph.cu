@@ -49,7 +49,8 @@ namespace elsa_b200
 {
     namespace
     {
-        constexpr int kForwardThreads = 256;
+        constexpr int kForwardThreads = 256;    // default rays per block of the gather forward
+        constexpr int kMaxForwardThreads = 512; // largest block the autotuner may choose
         constexpr int kSplatUnroll = ELSA_SPLAT_UNROLL;
         constexpr int kMinClass = 2;
         constexpr int kMaxClass = 8;
@@ -79,7 +80,7 @@ namespace elsa_b200
         }
 
         template <int DIM>
-        __global__ void __launch_bounds__(kForwardThreads)
+        __global__ void __launch_bounds__(kMaxForwardThreads)
             josephForwardKernel(const JosephRay* __restrict__ rays, int64_t nrays,
                                 const float* __restrict__ x, VolumeShape vol,
                                 float* __restrict__ y)
@@ -639,13 +640,12 @@ namespace elsa_b200
                 const int want = (kAdjoint2dCtasPerSm * 148 + nbricks - 1) / nbricks;
                 return want < 1 ? 1 : (want > np ? np : want);
             }
-            // partial: scratch of chunks(nbricks, np) volumes (unused with one chunk)
-            static void launch(int nbricks, cudaStream_t s, const JosephRay* rays,
+            // nc view chunks; partial: scratch of nc volumes (unused with one chunk)
+            static void launch(int nbricks, int nc, cudaStream_t s, const JosephRay* rays,
                                const float2* cps, int64_t nrays, const float* y,
                                const RayWindow* win, const unsigned* axes, VolumeShape vol,
                                DetectorShape det, int m, int3 nb, float* x, float* partial)
             {
-                const int nc = chunks(nbricks, det.np);
                 const int per = (det.np + nc - 1) / nc;
                 const int used = (det.np + per - 1) / per;
                 const dim3 grid(static_cast<unsigned>(nbricks), static_cast<unsigned>(used));
@@ -653,11 +653,9 @@ namespace elsa_b200
                     <<<grid, kThreads, smemBytes(det.np), s>>>(rays, cps, nrays, y, win, axes,
                                                                vol, det, m, nb, per,
                                                                used > 1 ? partial : x);
-                if (used > 1) {
-                    const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
-                    sumChunksKernel<<<static_cast<unsigned>((nvox + 255) / 256), 256, 0, s>>>(
-                        partial, used, nvox, x);
-                }
+                if (used > 1)
+                    launchSumChunks(partial, used,
+                                    static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2], x, s);
             }
         };
 
@@ -903,24 +901,21 @@ namespace elsa_b200
                 const int want = (kAdjoint3dWarpsPerSm * 148 + nbricks - 1) / nbricks;
                 return want < 1 ? 1 : (want > np ? np : want);
             }
-            // partial: scratch of chunks(nbricks, np) volumes (unused with one chunk)
-            static void launch(int nbricks, cudaStream_t s, const JosephRay* rays,
+            // nc view chunks; partial: scratch of nc volumes (unused with one chunk)
+            static void launch(int nbricks, int nc, cudaStream_t s, const JosephRay* rays,
                                const float2* cps, int64_t nrays, const float* y,
                                const RayWindow* win, const unsigned* axes, VolumeShape vol,
                                DetectorShape det, int m, int3 nb, float* x, float* partial)
             {
-                const int nc = chunks(nbricks, det.np);
                 const int per = (det.np + nc - 1) / nc;
                 const int used = (det.np + per - 1) / per;
                 const dim3 grid(static_cast<unsigned>(nbricks), static_cast<unsigned>(used));
                 josephAdjointWarpKernel<BX, BY, BZ, CPD><<<grid, 32, 0, s>>>(
                     rays, cps, nrays, y, win, axes, vol, det, m, nb, per,
                     used > 1 ? partial : x);
-                if (used > 1) {
-                    const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
-                    sumChunksKernel<<<static_cast<unsigned>((nvox + 255) / 256), 256, 0, s>>>(
-                        partial, used, nvox, x);
-                }
+                if (used > 1)
+                    launchSumChunks(partial, used,
+                                    static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2], x, s);
             }
         };
 
@@ -995,14 +990,7 @@ namespace elsa_b200
                 josephWindowKernel<<<static_cast<unsigned>((nwin + 255) / 256), 256>>>(
                     dPoses_, vol_, det_, brick_, nBricks_, dWindows_);
                 ELSA_LAUNCH_CHECK("josephWindowKernel");
-                {
-                    const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
-                    const int nc = vol_.dim == 2 ? Adjoint2d::chunks(nb, det_.np)
-                                                 : Adjoint3d::chunks(nb, det_.np);
-                    if (nc > 1)
-                        partial_ = std::make_unique<DeviceBuffer>(sizeof(float) * domainSize_ *
-                                                                  static_cast<size_t>(nc));
-                }
+                setKnob(kKnobAdjointChunks, defaultChunks());
                 if (vol_.dim == 3) {
                     std::vector<float> hp(poses_.size() * kPoseFloats);
                     std::memcpy(hp.data(), poses_.data(), sizeof(float) * hp.size());
@@ -1064,14 +1052,14 @@ namespace elsa_b200
             {
                 const int64_t nrays = rangeSize_;
                 const unsigned blocks =
-                    static_cast<unsigned>((nrays + kForwardThreads - 1) / kForwardThreads);
+                    static_cast<unsigned>((nrays + forwardThreads_ - 1) / forwardThreads_);
                 if (tma_)
                     tma_->forward(x, y, s);
                 else if (vol_.dim == 3)
-                    josephForwardKernel<3><<<blocks, kForwardThreads, 0, s>>>(dRays_, nrays, x,
+                    josephForwardKernel<3><<<blocks, forwardThreads_, 0, s>>>(dRays_, nrays, x,
                                                                                 vol_, y);
                 else
-                    josephForwardKernel<2><<<blocks, kForwardThreads, 0, s>>>(dRays_, nrays, x,
+                    josephForwardKernel<2><<<blocks, forwardThreads_, 0, s>>>(dRays_, nrays, x,
                                                                                 vol_, y);
                 ELSA_LAUNCH_CHECK("josephForwardKernel");
             }
@@ -1079,15 +1067,65 @@ namespace elsa_b200
             void adjoint(const float* y, float* x, cudaStream_t s) override
             {
                 const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
+                float* partial = partial_ ? partial_->as<float>() : nullptr;
                 if (vol_.dim == 3)
-                    Adjoint3d::launch(nb, s, dRays_, dCheckpoints_, rangeSize_, y, dWindows_,
-                                      dViewAxes_, vol_, det_, classSpacing_, nBricks_, x,
-                                      partial_ ? partial_->as<float>() : nullptr);
+                    Adjoint3d::launch(nb, adjointChunks_, s, dRays_, dCheckpoints_, rangeSize_, y,
+                                      dWindows_, dViewAxes_, vol_, det_, classSpacing_, nBricks_,
+                                      x, partial);
                 else
-                    Adjoint2d::launch(nb, s, dRays_, dCheckpoints_, rangeSize_, y, dWindows_,
-                                      dViewAxes_, vol_, det_, classSpacing_, nBricks_, x,
-                                      partial_ ? partial_->as<float>() : nullptr);
+                    Adjoint2d::launch(nb, adjointChunks_, s, dRays_, dCheckpoints_, rangeSize_, y,
+                                      dWindows_, dViewAxes_, vol_, det_, classSpacing_, nBricks_,
+                                      x, partial);
                 ELSA_LAUNCH_CHECK("josephAdjointKernel");
+            }
+
+            std::vector<int> knobCandidates(int knob) const override
+            {
+                if (knob == kKnobAdjointChunks) {
+                    // partial volumes limited to 1 GiB
+                    const int64_t byMemory =
+                        std::max<int64_t>(1, (int64_t(1) << 30) / (4 * domainSize_));
+                    const int limit = static_cast<int>(
+                        std::min<int64_t>(std::min<int64_t>(det_.np, 256), byMemory));
+                    return chunkCandidates(limit, std::min(limit, defaultChunks()));
+                }
+                if (knob == kKnobForwardThreads && !tma_)
+                    return {64, 128, 256, 512};
+                return {};
+            }
+
+            int knob(int knob) const override
+            {
+                if (knob == kKnobAdjointChunks)
+                    return adjointChunks_;
+                if (knob == kKnobForwardThreads)
+                    return tma_ ? -1 : forwardThreads_;
+                return -1;
+            }
+
+            void setKnob(int knob, int value) override
+            {
+                const std::vector<int> c = knobCandidates(knob);
+                if (knob == kKnobAdjointChunks && value == defaultChunks()) {
+                    // the default is always allowed, also past the tuning limits
+                } else if (std::find(c.begin(), c.end(), value) == c.end()) {
+                    throw Error(ELSA_ERROR_INVALID_ARGUMENT,
+                                "JosephsMethod: value " + std::to_string(value) +
+                                    " is not a candidate of knob " + std::to_string(knob));
+                }
+                if (knob == kKnobForwardThreads) {
+                    forwardThreads_ = value;
+                    return;
+                }
+                const size_t need = sizeof(float) * static_cast<size_t>(domainSize_) *
+                                    static_cast<size_t>(value);
+                if (value <= 1)
+                    partial_.reset();
+                else if (!partial_ || partial_->bytes() < need) {
+                    partial_.reset();
+                    partial_ = std::make_unique<DeviceBuffer>(need);
+                }
+                adjointChunks_ = value;
             }
 
             int64_t info(int key) const override
@@ -1106,7 +1144,7 @@ namespace elsa_b200
                 case 6: // kernel launches per forward call
                     return tma_ ? tma_->launchesPerForward() : 1;
                 case 7: // kernel launches per adjoint call (with view chunks: + the chunk sum)
-                    return partial_ ? 2 : 1;
+                    return adjointChunks_ > 1 ? 2 : 1;
                 default:
                     return -1;
                 }
@@ -1122,6 +1160,16 @@ namespace elsa_b200
             int64_t sampleCount_ = 0;
             std::unique_ptr<JosephForwardTma> tma_;
             std::unique_ptr<DeviceBuffer> partial_; // adjoint: per view-chunk partial volumes
+            int adjointChunks_ = 1;                 // view chunks of the adjoint
+            int forwardThreads_ = kForwardThreads;  // rays per block of the gather forward
+
+            // Views per chunk so that bricks x chunks fill the GPU (see the launch configs).
+            int defaultChunks() const
+            {
+                const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
+                return vol_.dim == 2 ? Adjoint2d::chunks(nb, det_.np)
+                                     : Adjoint3d::chunks(nb, det_.np);
+            }
             int3 brick_{}, nBricks_{};
         };
     } // namespace
@@ -1135,6 +1183,16 @@ namespace elsa_b200
         josephWindowKernel<<<static_cast<unsigned>((nwin + 255) / 256), 256, 0, s>>>(
             poses, vol, det, brick, nBricks, out);
         ELSA_LAUNCH_CHECK("josephWindowKernel");
+    }
+
+    void launchSumChunks(const float* partial, int chunks, int64_t nvox, float* x,
+                         cudaStream_t s)
+    {
+        if (nvox == 0)
+            return;
+        sumChunksKernel<<<static_cast<unsigned>((nvox + 255) / 256), 256, 0, s>>>(partial, chunks,
+                                                                                  nvox, x);
+        ELSA_LAUNCH_CHECK("sumChunksKernel");
     }
 
     std::unique_ptr<Projector> makeJosephProjector(const VolumeShape& vol,

@@ -18,6 +18,16 @@
 
 namespace elsa_b200
 {
+    // Launch parameters ("knobs") that change how a projector's kernels are launched, not the
+    // operator: every value gives the same forward and adjoint up to float rounding (adjoint
+    // view chunks only change the order in which per-chunk partial volumes are added).
+    enum Knob : int {
+        kKnobForwardThreads = 0, // rays per block of a thread-per-ray forward kernel
+        kKnobAdjointChunks = 1,  // view chunks of a brick-owner adjoint (partial volumes)
+        kKnobAdjointThreads = 2, // voxels per block of a thread-per-voxel adjoint kernel
+        kKnobCount = 3
+    };
+
     class Projector
     {
     public:
@@ -33,6 +43,19 @@ namespace elsa_b200
         int kind() const { return kind_; }
         // Tunables reported for diagnostics (e.g. the conflict-free ray class spacing).
         virtual int64_t info(int key) const { (void)key; return -1; }
+        // Values the autotuner may try for `knob` on this geometry (empty: fixed here), the
+        // current value (-1: not used by this projector) and setting one of the candidates.
+        virtual std::vector<int> knobCandidates(int knob) const
+        {
+            (void)knob;
+            return {};
+        }
+        virtual int knob(int knob) const
+        {
+            (void)knob;
+            return -1;
+        }
+        virtual void setKnob(int knob, int value);
 
     protected:
         Projector(int kind, const VolumeShape& vol, const DetectorShape& det,
@@ -58,4 +81,13 @@ namespace elsa_b200
     // brick.
     void launchBrickWindows(const float* poses, const VolumeShape& vol, const DetectorShape& det,
                             int3 brick, int3 nBricks, RayWindow* out, cudaStream_t s);
+
+    // x[v] = sum over c = 0 .. chunks-1 of partial[c * nvox + v], added in chunk order
+    // (joseph.cu).
+    void launchSumChunks(const float* partial, int chunks, int64_t nvox, float* x,
+                         cudaStream_t s);
+
+    // Powers of two up to `limit` plus `extra` (sorted, unique, each >= 1): the candidate
+    // view-chunk counts of a brick-owner adjoint.
+    std::vector<int> chunkCandidates(int limit, int extra);
 } // namespace elsa_b200

@@ -35,7 +35,9 @@ namespace elsa_b200
 {
     namespace
     {
-        constexpr int kForwardThreads = 128;
+        constexpr int kForwardThreads = 128;    // default rays per block of the forward
+        constexpr int kMaxForwardThreads = 512; // largest block the autotuner may choose
+        constexpr int kAdjointWarpsPerSm = 22;  // view-chunk target of the warp-brick adjoint
         constexpr int kSlab = 16; // brick edge = checkpoint slab depth
         constexpr int kMinClass = 2;
         constexpr int kMaxClass = 8;
@@ -78,7 +80,7 @@ namespace elsa_b200
         }
 
         template <int DIM>
-        __global__ void __launch_bounds__(kForwardThreads)
+        __global__ void __launch_bounds__(kMaxForwardThreads)
             siddonForwardKernel(const SiddonRay* __restrict__ rays, int64_t nrays,
                                 const float* __restrict__ x, VolumeShape vol,
                                 float* __restrict__ y)
@@ -387,8 +389,11 @@ namespace elsa_b200
                                 const float* __restrict__ y,
                                 const RayWindow* __restrict__ windows,
                                 const unsigned* __restrict__ viewAxes, VolumeShape vol,
-                                DetectorShape det, int m, int3 nBricks, float* __restrict__ x)
+                                DetectorShape det, int m, int3 nBricks, int viewsPerChunk,
+                                float* __restrict__ x)
         {
+            // blockIdx.y selects a chunk of views; with several chunks the brick goes to
+            // x + chunk * nvox and launchSumChunks adds the chunks in order
             using L = SiddonBrick<DIM>;
             __shared__ float acc[L::kWords];
             const int lane = threadIdx.x;
@@ -400,7 +405,9 @@ namespace elsa_b200
             for (int i = lane; i < L::kWords; i += 32)
                 acc[i] = 0.0f;
             __syncwarp();
-            for (int p = 0; p < det.np; ++p) {
+            const int pBegin = blockIdx.y * viewsPerChunk;
+            const int pEnd = min(det.np, pBegin + viewsPerChunk);
+            for (int p = pBegin; p < pEnd; ++p) {
                 const RayWindow w = windows[static_cast<int64_t>(p) * nb + bi];
                 if (w.u0 > w.u1 || w.v0 > w.v1)
                     continue;
@@ -416,12 +423,14 @@ namespace elsa_b200
                                                       y, det, org0, org1, org2, vol);
             }
             __syncwarp();
+            const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
+            float* out = x + blockIdx.y * nvox;
             for (int i = lane; i < kSlab * kSlab * L::kBz; i += 32) {
                 const int lx = i % kSlab, ly = (i / kSlab) % kSlab, lz = i / (kSlab * kSlab);
                 const int gx = org0 + lx, gy = org1 + ly, gz = org2 + lz;
                 if (gx < vol.n[0] && gy < vol.n[1] && gz < vol.n[2])
-                    x[gx + static_cast<int64_t>(vol.n[0]) *
-                               (gy + static_cast<int64_t>(vol.n[1]) * gz)] =
+                    out[gx + static_cast<int64_t>(vol.n[0]) *
+                                 (gy + static_cast<int64_t>(vol.n[1]) * gz)] =
                         acc[lz * L::kPlane + ly * L::kRow + lx];
             }
         }
@@ -494,6 +503,7 @@ namespace elsa_b200
                 windows_ = std::make_unique<DeviceBuffer>(sizeof(RayWindow) * nwin);
                 launchBrickWindows(dPoses_, vol_, det_, make_int3(kSlab, kSlab, bz), nBricks_,
                                    windows_->as<RayWindow>(), nullptr);
+                setKnob(kKnobAdjointChunks, defaultChunks());
                 ELSA_CUDA(cudaDeviceSynchronize());
             }
 
@@ -501,12 +511,12 @@ namespace elsa_b200
             {
                 const int64_t nrays = rangeSize_;
                 const unsigned blocks =
-                    static_cast<unsigned>((nrays + kForwardThreads - 1) / kForwardThreads);
+                    static_cast<unsigned>((nrays + forwardThreads_ - 1) / forwardThreads_);
                 if (vol_.dim == 3)
-                    siddonForwardKernel<3><<<blocks, kForwardThreads, 0, s>>>(
+                    siddonForwardKernel<3><<<blocks, forwardThreads_, 0, s>>>(
                         rays_->as<SiddonRay>(), nrays, x, vol_, y);
                 else
-                    siddonForwardKernel<2><<<blocks, kForwardThreads, 0, s>>>(
+                    siddonForwardKernel<2><<<blocks, forwardThreads_, 0, s>>>(
                         rays_->as<SiddonRay>(), nrays, x, vol_, y);
                 ELSA_LAUNCH_CHECK("siddonForwardKernel");
             }
@@ -514,17 +524,23 @@ namespace elsa_b200
             void adjoint(const float* y, float* x, cudaStream_t s) override
             {
                 const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
+                const int per = (det_.np + adjointChunks_ - 1) / adjointChunks_;
+                const int used = (det_.np + per - 1) / per;
+                const dim3 grid(static_cast<unsigned>(nb), static_cast<unsigned>(used));
+                float* out = used > 1 ? partial_->as<float>() : x;
                 if (vol_.dim == 3)
-                    siddonAdjointKernel<3><<<nb, 32, 0, s>>>(
+                    siddonAdjointKernel<3><<<grid, 32, 0, s>>>(
                         rays_->as<SiddonRay>(), cpState_->as<float4>(), cpVoxel_->as<unsigned>(),
                         rangeSize_, y, windows_->as<RayWindow>(), viewAxes_->as<unsigned>(), vol_,
-                        det_, classSpacing_, nBricks_, x);
+                        det_, classSpacing_, nBricks_, per, out);
                 else
-                    siddonAdjointKernel<2><<<nb, 32, 0, s>>>(
+                    siddonAdjointKernel<2><<<grid, 32, 0, s>>>(
                         rays_->as<SiddonRay>(), cpState_->as<float4>(), cpVoxel_->as<unsigned>(),
                         rangeSize_, y, windows_->as<RayWindow>(), viewAxes_->as<unsigned>(), vol_,
-                        det_, classSpacing_, nBricks_, x);
+                        det_, classSpacing_, nBricks_, per, out);
                 ELSA_LAUNCH_CHECK("siddonAdjointKernel");
+                if (used > 1)
+                    launchSumChunks(partial_->as<float>(), used, domainSize_, x, s);
             }
 
             int64_t info(int key) const override
@@ -538,12 +554,76 @@ namespace elsa_b200
                     return visits_;
                 case 3:
                     return 0;
+                case 6: // kernel launches per forward call
+                    return 1;
+                case 7: // kernel launches per adjoint call (with view chunks: + the chunk sum)
+                    return adjointChunks_ > 1 ? 2 : 1;
                 default:
                     return -1;
                 }
             }
 
+            std::vector<int> knobCandidates(int knob) const override
+            {
+                if (knob == kKnobAdjointChunks) {
+                    // partial volumes limited to 1 GiB
+                    const int64_t byMemory =
+                        std::max<int64_t>(1, (int64_t(1) << 30) / (4 * domainSize_));
+                    const int limit = static_cast<int>(
+                        std::min<int64_t>(std::min<int64_t>(det_.np, 256), byMemory));
+                    return chunkCandidates(limit, std::min(limit, defaultChunks()));
+                }
+                if (knob == kKnobForwardThreads)
+                    return {64, 128, 256, 512};
+                return {};
+            }
+
+            int knob(int knob) const override
+            {
+                if (knob == kKnobAdjointChunks)
+                    return adjointChunks_;
+                if (knob == kKnobForwardThreads)
+                    return forwardThreads_;
+                return -1;
+            }
+
+            void setKnob(int knob, int value) override
+            {
+                const std::vector<int> c = knobCandidates(knob);
+                if (knob == kKnobAdjointChunks && value == defaultChunks()) {
+                    // the default is always allowed, also past the tuning limits
+                } else if (std::find(c.begin(), c.end(), value) == c.end()) {
+                    throw Error(ELSA_ERROR_INVALID_ARGUMENT,
+                                "SiddonsMethod: value " + std::to_string(value) +
+                                    " is not a candidate of knob " + std::to_string(knob));
+                }
+                if (knob == kKnobForwardThreads) {
+                    forwardThreads_ = value;
+                    return;
+                }
+                const size_t need = sizeof(float) * static_cast<size_t>(domainSize_) *
+                                    static_cast<size_t>(value);
+                if (value <= 1)
+                    partial_.reset();
+                else if (!partial_ || partial_->bytes() < need) {
+                    partial_.reset();
+                    partial_ = std::make_unique<DeviceBuffer>(need);
+                }
+                adjointChunks_ = value;
+            }
+
         private:
+            // View chunks so that bricks x chunks reach kAdjointWarpsPerSm one-warp CTAs per SM.
+            int defaultChunks() const
+            {
+                const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
+                const int want = (kAdjointWarpsPerSm * 148 + nb - 1) / nb;
+                return std::max(1, std::min(want, det_.np));
+            }
+
+            std::unique_ptr<DeviceBuffer> partial_; // adjoint: per view-chunk partial volumes
+            int adjointChunks_ = 1;
+            int forwardThreads_ = kForwardThreads;
             std::unique_ptr<DeviceBuffer> rays_, cpState_, cpVoxel_, viewAxes_, windows_;
             int cpRows_ = 0;
             int classSpacing_ = 0;

@@ -35,7 +35,8 @@ namespace elsa_b200
 {
     namespace
     {
-        constexpr int kVoxelThreads = 256;
+        constexpr int kVoxelThreads = 256;      // forward: one thread per brick voxel; adjoint default
+        constexpr int kMaxAdjointThreads = 512; // largest adjoint block the autotuner may choose
         constexpr int kPatchWords = 2304; // 9 KB shared detector patch (48 x 48 pixels)
 
         struct VoxelParams {
@@ -182,7 +183,7 @@ namespace elsa_b200
         // Adjoint: x[v] = sum over poses and footprint pixels of w * y[pixel], in the reference's
         // order (VoxelComputation.h:152-183). One thread per voxel, x fastest within a block.
         template <int DIM>
-        __global__ void __launch_bounds__(kVoxelThreads)
+        __global__ void __launch_bounds__(kMaxAdjointThreads)
             voxelAdjointKernel(const float* __restrict__ poses, int np,
                                const float* __restrict__ lutIn, VoxelParams vp, VolumeShape vol,
                                const float* __restrict__ y, float* __restrict__ x)
@@ -359,8 +360,8 @@ namespace elsa_b200
             void adjoint(const float* y, float* x, cudaStream_t s) override
             {
                 const unsigned blocks =
-                    static_cast<unsigned>((domainSize_ + kVoxelThreads - 1) / kVoxelThreads);
-                voxelAdjointKernel<DIM><<<blocks, kVoxelThreads, 0, s>>>(
+                    static_cast<unsigned>((domainSize_ + adjointThreads_ - 1) / adjointThreads_);
+                voxelAdjointKernel<DIM><<<blocks, adjointThreads_, 0, s>>>(
                     dPoses_, det_.np, lut_.as<float>(), vp_, vol_, y, x);
                 ELSA_LAUNCH_CHECK("voxelAdjointKernel");
             }
@@ -372,12 +373,39 @@ namespace elsa_b200
                     return static_cast<int64_t>(nBricks_.x) * nBricks_.y * nBricks_.z;
                 case 5:
                     return vp_.mode;
+                case 6: // kernel launches per forward call (after the output memset)
+                    return 1;
+                case 7: // kernel launches per adjoint call
+                    return 1;
                 default:
                     return -1;
                 }
             }
 
+            std::vector<int> knobCandidates(int knob) const override
+            {
+                if (knob == kKnobAdjointThreads)
+                    return {64, 128, 256, 512};
+                return {};
+            }
+
+            int knob(int knob) const override
+            {
+                return knob == kKnobAdjointThreads ? adjointThreads_ : -1;
+            }
+
+            void setKnob(int knob, int value) override
+            {
+                const std::vector<int> c = knobCandidates(knob);
+                if (std::find(c.begin(), c.end(), value) == c.end())
+                    throw Error(ELSA_ERROR_INVALID_ARGUMENT,
+                                "voxel projector: value " + std::to_string(value) +
+                                    " is not a candidate of knob " + std::to_string(knob));
+                adjointThreads_ = value;
+            }
+
         private:
+            int adjointThreads_ = kVoxelThreads; // voxels per block of the gather adjoint
             // forward bricks: 8 x 8 x 4 voxels in 3D, 16 x 16 in 2D (one thread per voxel)
             static constexpr int kBX = DIM == 3 ? 8 : 16;
             static constexpr int kBY = DIM == 3 ? 8 : 16;

@@ -131,8 +131,55 @@ elsa_status elsa_projector_sizes(const elsa_projector* projector, int64_t* domai
 /* Diagnostics: key 0 = conflict-free ray class spacing of the adjoint, 1 = adjoint bricks,
  * 2 = samples per forward pass (sum over rays of the Joseph step count), 3 = error word of the
  * device pipeline (0 = no timed-out wait; synchronizes), 4 = detector tiles on the gather
- * fallback of the staged forward, in parts per million. */
+ * fallback of the staged forward, in parts per million, 5 = footprint mode of a voxel
+ * projector, 6 / 7 = kernel launches per forward / adjoint call. */
 elsa_status elsa_projector_info(const elsa_projector* projector, int32_t key, int64_t* value);
+
+/* Launch parameters ("knobs") of a projector. None of them changes the operator: every value
+ * computes the same forward and adjoint up to float rounding (adjoint view chunks only change
+ * the order in which per-chunk partial volumes are added). The reference has no counterpart;
+ * its CUDA projectors launch fixed block shapes (JosephsMethodCUDA.cpp:132-214,
+ * ProjectVoxelsCUDA.cu:21-239). */
+#define ELSA_KNOB_FORWARD_THREADS 0 /* rays per block of a thread-per-ray forward (Siddon, 2D Joseph) */
+#define ELSA_KNOB_ADJOINT_CHUNKS 1  /* view chunks of a brick-owner adjoint (Joseph, Siddon) */
+#define ELSA_KNOB_ADJOINT_THREADS 2 /* voxels per block of a thread-per-voxel adjoint (blob, B-spline) */
+#define ELSA_KNOB_COUNT 3
+
+/* Current value of `knob` (-1: the projector does not use it). */
+elsa_status elsa_projector_get_knob(const elsa_projector* projector, int32_t knob,
+                                    int32_t* value);
+
+/* Candidate values of `knob` for this projector's geometry, ascending: *count receives their
+ * number (0: not tunable here) and the first min(*count, capacity) are written to values. */
+elsa_status elsa_projector_knob_candidates(const elsa_projector* projector, int32_t knob,
+                                           int32_t* values, int32_t capacity, int32_t* count);
+
+/* Set `knob` to one of its candidates (or, for the adjoint chunks, the default the projector
+ * chose at creation); other values return ELSA_ERROR_INVALID_ARGUMENT. May allocate or free the
+ * adjoint's partial volumes; synchronous with respect to the host. */
+elsa_status elsa_projector_set_knob(elsa_projector* projector, int32_t knob, int32_t value);
+
+/* Autotuner: time every candidate of every knob (the forward for the forward knob, the adjoint
+ * for the others) with CUDA events on `stream`, keep the fastest, and record the choice in the
+ * process-wide tuning cache under the key "kind:dim:nx,ny,nz:nu,nv,np". Unless `force` is
+ * non-zero, a key already in the cache is applied without timing. values (may be NULL) receives
+ * ELSA_KNOB_COUNT values (-1 for unused knobs); *from_cache (may be NULL) is set to 1 when the
+ * cache supplied them. Allocates one volume and one sinogram of scratch; synchronizes `stream`.
+ * No reference counterpart. */
+elsa_status elsa_projector_autotune(elsa_projector* projector, void* stream, int32_t force,
+                                    int32_t* values, int32_t* from_cache);
+
+/* The tuning cache (host memory, shared by all threads): number of entries, removal of all
+ * entries, writing it to a text file (one line per key: the key and ELSA_KNOB_COUNT integers)
+ * and reading such a file (adding to or replacing the entries; a malformed file changes
+ * nothing and returns ELSA_ERROR_INVALID_ARGUMENT). Set and look up one entry directly with
+ * elsa_tune_cache_put / elsa_tune_cache_get (*found = 0 when absent). No reference counterpart. */
+elsa_status elsa_tune_cache_size(int64_t* entries);
+elsa_status elsa_tune_cache_clear(void);
+elsa_status elsa_tune_cache_save(const char* path);
+elsa_status elsa_tune_cache_load(const char* path);
+elsa_status elsa_tune_cache_put(const char* key, const int32_t* values);
+elsa_status elsa_tune_cache_get(const char* key, int32_t* values, int32_t* found);
 
 /* y = A x on device buffers. Replaces LinearOperator::apply(x, Ax), core/LinearOperator.cpp:94-98
  * -> XrayProjector::applyImpl -> JosephsMethodCUDA::forward, JosephsMethodCUDA.cpp:132-214. */
