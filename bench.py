@@ -391,8 +391,10 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="elsa_b200", choices=["elsa_b200", "reference"])
-    ap.add_argument("--cpu-views", type=int, default=4,
-                    help="views per CPU baseline sample")
+    ap.add_argument("--cpu-views", type=int, default=None,
+                    help="views per CPU baseline sample (default: 60 for the cpu_baseline of "
+                         "this arm, about 10 s on 16 host threads; for --impl reference as many "
+                         "as keep the whole run near 90 s, 4 to 60)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-vs-plain small-problem measurement")
@@ -402,8 +404,13 @@ def main():
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
+        if args.cpu_views is None:
+            # about 0.17 s per view (forward + adjoint) on 16 host threads
+            args.cpu_views = max(4, min(60, int(90.0 / (args.steps + args.warmup) / 0.17)))
         run_reference(args)
     else:
+        if args.cpu_views is None:
+            args.cpu_views = 60
         run_elsa(args)
 
 

@@ -38,6 +38,8 @@ namespace elsa_b200
         constexpr int kForwardThreads = 128;    // default rays per block of the forward
         constexpr int kMaxForwardThreads = 512; // largest block the autotuner may choose
         constexpr int kAdjointWarpsPerSm = 22;  // view-chunk target of the warp-brick adjoint
+        constexpr int kMinAdjointChunks = 32;   // default floor of the view chunks
+        constexpr int64_t kChunkMemory = int64_t(1) << 31; // default partial-volume budget
         constexpr int kSlab = 16; // brick edge = checkpoint slab depth
         constexpr int kMinClass = 2;
         constexpr int kMaxClass = 8;
@@ -566,9 +568,9 @@ namespace elsa_b200
             std::vector<int> knobCandidates(int knob) const override
             {
                 if (knob == kKnobAdjointChunks) {
-                    // partial volumes limited to 1 GiB
+                    // partial volumes limited to 4 GiB
                     const int64_t byMemory =
-                        std::max<int64_t>(1, (int64_t(1) << 30) / (4 * domainSize_));
+                        std::max<int64_t>(1, (int64_t(1) << 32) / (4 * domainSize_));
                     const int limit = static_cast<int>(
                         std::min<int64_t>(std::min<int64_t>(det_.np, 256), byMemory));
                     return chunkCandidates(limit, std::min(limit, defaultChunks()));
@@ -613,12 +615,17 @@ namespace elsa_b200
             }
 
         private:
-            // View chunks so that bricks x chunks reach kAdjointWarpsPerSm one-warp CTAs per SM.
+            // View chunks: enough for bricks x chunks to reach kAdjointWarpsPerSm one-warp CTAs
+            // per SM and at least kMinAdjointChunks, within kChunkMemory of partial volumes
+            // (256^3 / 360 views: 103.8 ms with 1 chunk, 85.5 with 32).
             int defaultChunks() const
             {
                 const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
-                const int want = (kAdjointWarpsPerSm * 148 + nb - 1) / nb;
-                return std::max(1, std::min(want, det_.np));
+                const int want = std::max((kAdjointWarpsPerSm * 148 + nb - 1) / nb,
+                                          kMinAdjointChunks);
+                const int64_t cap = std::max<int64_t>(1, kChunkMemory / (4 * domainSize_));
+                return static_cast<int>(
+                    std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(want, det_.np), cap)));
             }
 
             std::unique_ptr<DeviceBuffer> partial_; // adjoint: per view-chunk partial volumes
