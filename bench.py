@@ -278,6 +278,12 @@ def run_elsa(args):
     }
     if rank == 0 and world == 1 and not args.no_batched:
         out["batched"] = batched_vs_plain(torch, elsa_b200, phantoms)
+    if rank == 0 and world == 1 and args.batched_full:
+        # the full batched workload: 64 instances, edges {64, ..., 256}, 60-360 views, 50
+        # CG iterations each (several minutes; not part of the default run)
+        out["batched_full"] = batched_vs_plain(torch, elsa_b200, phantoms, instances=64,
+                                               iterations=50, edges=(64, 96, 128, 192, 256),
+                                               views=(60, 360))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         gups, dt, cores = cpu_baseline_sample(args.cpu_views, vol, poses, det, x_true)
         out["cpu_baseline"] = {"value": round(gups, 5), "unit": "GUPS", "cores": cores,
@@ -291,58 +297,84 @@ def run_elsa(args):
 
 
 def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, streams=8,
-                     seed=5):
-    """Many small independent reconstructions: one at a time (each solver's iterations enqueued
-    on one stream, one problem after the other) against elsa_solve_batch (every solver's
-    iterations as a CUDA graph, problems spread over concurrent streams). Seeded instances of the
-    batched workload with edges {64, 96, 128}, 60-180 views, a detector of 1.5 x edge; projector
-    and solver set-up is outside both timed regions."""
+                     seed=5, edges=(64, 96, 128), views=(60, 180), free_floor_gb=24.0):
+    """Many independent reconstructions: one at a time (each solver's iterations enqueued on one
+    stream, one problem after the other) against elsa_solve_batch (every solver's iterations as
+    a CUDA graph, problems spread over concurrent streams). Seeded instances with volume edges
+    drawn from `edges`, views uniform in `views`, a detector of 1.5 x edge and a modified
+    Shepp-Logan phantom. Instances are built in waves that leave `free_floor_gb` of device
+    memory free; each wave is timed both ways and the times are summed. Projector and solver
+    set-up is outside both timed regions."""
     rng = np.random.default_rng(seed)
-    problems = []
+    specs = []
     for _ in range(instances):
-        n = int(rng.choice([64, 96, 128]))
-        views = int(rng.integers(60, 181))
-        vol = (n, n, n)
-        poses, det = elsa_b200.circle_trajectory(vol, views, 360, 10.0 * n, 2.5 * n,
-                                                 [int(1.5 * n), int(1.5 * n)])
-        proj = elsa_b200.Projector(elsa_b200.PROJECTOR_JOSEPH, vol, det, poses)
-        xt = torch.from_numpy(phantoms.modified_shepp_logan(vol).ravel()).cuda()
-        b = torch.empty(proj.range_size, dtype=torch.float32, device="cuda")
-        proj.apply_ptr(xt.data_ptr(), b.data_ptr(), torch.cuda.current_stream().cuda_stream)
-        problems.append((proj, b))
-    torch.cuda.synchronize()
+        n = int(rng.choice(list(edges)))
+        nv = int(rng.integers(views[0], views[1] + 1))
+        specs.append((n, nv))
+    t_plain = t_batch = 0.0
+    waves = 0
+    i = 0
+    while i < len(specs):
+        problems = []
+        while i < len(specs):
+            n, nv = specs[i]
+            vol = (n, n, n)
+            poses, det = elsa_b200.circle_trajectory(vol, nv, 360, 10.0 * n, 2.5 * n,
+                                                     [int(1.5 * n), int(1.5 * n)])
+            proj = elsa_b200.Projector(elsa_b200.PROJECTOR_JOSEPH, vol, det, poses)
+            xt = torch.from_numpy(phantoms.modified_shepp_logan(vol).ravel()).cuda()
+            b = torch.empty(proj.range_size, dtype=torch.float32, device="cuda")
+            proj.apply_ptr(xt.data_ptr(), b.data_ptr(), torch.cuda.current_stream().cuda_stream)
+            problems.append((proj, b))
+            i += 1
+            torch.cuda.synchronize()
+            free, _ = torch.cuda.mem_get_info()
+            # two solver workspaces per problem are still to come (4 volumes + 2 sinograms each)
+            ws = 2 * 4 * (4 * proj.domain_size + 2 * proj.range_size)
+            if free - ws < free_floor_gb * 1e9:
+                break
+        waves += 1
 
-    def make():
+        def make():
+            s = torch.cuda.current_stream().cuda_stream
+            xs, sols = [], []
+            for proj, b in problems:
+                x = torch.zeros(proj.domain_size, dtype=torch.float32, device="cuda")
+                sols.append(elsa_b200.Solver(elsa_b200.SOLVER_CGNE, proj, b.data_ptr(),
+                                             x.data_ptr(), stream=s))
+                xs.append(x)
+            torch.cuda.synchronize()
+            return xs, sols
+
+        xs, plain = make()
         s = torch.cuda.current_stream().cuda_stream
-        xs, sols = [], []
-        for proj, b in problems:
-            x = torch.zeros(proj.domain_size, dtype=torch.float32, device="cuda")
-            sols.append(elsa_b200.Solver(elsa_b200.SOLVER_CGNE, proj, b.data_ptr(),
-                                         x.data_ptr(), stream=s))
-            xs.append(x)
+        for sol in plain:  # warm-up of every kernel shape
+            sol.iterate(1, s)
         torch.cuda.synchronize()
-        return xs, sols
-
-    xs, plain = make()
-    s = torch.cuda.current_stream().cuda_stream
-    for sol in plain:  # warm-up of every kernel shape
-        sol.iterate(1, s)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for sol in plain:
-        sol.iterate(iterations, s)
-    torch.cuda.synchronize()
-    t_plain = time.perf_counter() - t0
-    xs2, batch = make()
-    elsa_b200.solve_batch(batch, 1, streams)  # captures the one-iteration graphs (warm-up)
-    t0 = time.perf_counter()
-    elsa_b200.solve_batch(batch, iterations, streams)  # captures + runs the timed graphs
-    t_batch = time.perf_counter() - t0
-    for sol in plain + batch:
-        sol.close()
+        t0 = time.perf_counter()
+        for sol in plain:
+            sol.iterate(iterations, s)
+        torch.cuda.synchronize()
+        t_plain += time.perf_counter() - t0
+        for sol in plain:
+            sol.close()
+        del xs, plain
+        xs2, batch = make()
+        elsa_b200.solve_batch(batch, 1, streams)  # captures the one-iteration graphs (warm-up)
+        t0 = time.perf_counter()
+        elsa_b200.solve_batch(batch, iterations, streams)  # captures + runs the timed graphs
+        t_batch += time.perf_counter() - t0
+        for sol in batch:
+            sol.close()
+        for proj, _ in problems:
+            proj.close()
+        del xs2, batch, problems
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
     return {"instances": instances, "iterations": iterations, "streams": streams,
-            "workload": "seeded CGNE problems, edges {64, 96, 128}, 60-180 views, detector "
-                        "1.5 x edge, Joseph",
+            "waves": waves,
+            "workload": "seeded CGNE problems, edges {%s}, %d-%d views, detector 1.5 x edge, "
+                        "Joseph" % (", ".join(str(e) for e in edges), views[0], views[1]),
             "plain_recon_per_s": round(instances / t_plain, 3),
             "batched_recon_per_s": round(instances / t_batch, 3),
             "speedup": round(t_plain / t_batch, 3),
@@ -398,6 +430,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-vs-plain small-problem measurement")
+    ap.add_argument("--batched-full", action="store_true",
+                    help="also time the full batched workload (64 reconstructions of edges "
+                         "64-256, 60-360 views, 50 CG iterations each; several minutes)")
     ap.add_argument("--size", type=int, default=256,
                     help="volume edge (profiling only; the benchmark workload is 256)")
     args = ap.parse_args()
