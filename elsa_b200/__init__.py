@@ -15,7 +15,8 @@ from ._capi import (ElsaError, InvalidArgumentError, Projector, Solver,  # noqa:
                     SOLVER_OGM, PROX_IDENTITY, PROX_BOX, PROX_L1, KNOB_FORWARD_THREADS,
                     KNOB_ADJOINT_CHUNKS, KNOB_ADJOINT_THREADS, tune_cache_size,
                     tune_cache_clear, tune_cache_save, tune_cache_load, tune_cache_put,
-                    tune_cache_get)
+                    tune_cache_get, SOLVER_SQS, SUBSET_ROUND_ROBIN,
+                    SUBSET_ROTATIONAL_CLUSTERING, subset_split, gather_views)
 
 __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "voxel_lut",
            "PROJECTOR_BLOB", "PROJECTOR_BSPLINE", "PROJECTOR_PHASE_CONTRAST_BLOB",
@@ -27,4 +28,5 @@ __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "voxel_lu
            "PROX_IDENTITY",
            "PROX_BOX", "PROX_L1", "KNOB_FORWARD_THREADS", "KNOB_ADJOINT_CHUNKS",
            "KNOB_ADJOINT_THREADS", "tune_cache_size", "tune_cache_clear", "tune_cache_save",
-           "tune_cache_load", "tune_cache_put", "tune_cache_get"]
+           "tune_cache_load", "tune_cache_put", "tune_cache_get", "SOLVER_SQS",
+           "SUBSET_ROUND_ROBIN", "SUBSET_ROTATIONAL_CLUSTERING", "subset_split", "gather_views"]

@@ -36,6 +36,9 @@ SOLVER_APGD = 3
 SOLVER_SIRT = 4
 SOLVER_FGM = 5
 SOLVER_OGM = 6
+SOLVER_SQS = 7
+SUBSET_ROUND_ROBIN = 0
+SUBSET_ROTATIONAL_CLUSTERING = 1
 PROX_IDENTITY = 0
 PROX_BOX = 1
 PROX_L1 = 2
@@ -86,6 +89,10 @@ SIGNATURES = {
     "elsa_solver_create": (_st, [_i32, _vp, _vp, _vp, _i32, ctypes.POINTER(ctypes.c_double),
                                  _i32, _vp, ctypes.POINTER(_vp)]),
     "elsa_solver_step_size": (_st, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    "elsa_sqs_create": (_st, [_vp, _vp, _vp, _vp, _i32, _vp, _i32, _i32, ctypes.c_double, _vp,
+                              _vp, ctypes.POINTER(_vp)]),
+    "elsa_subset_split": (_st, [_i32, _vp, _i32, _i32, _i32, _vp, _vp]),
+    "elsa_gather_views": (_st, [_vp, _i64, _vp, _i32, _i32, _vp, _vp]),
     "elsa_power_iterations": (_st, [_vp, _i32, _vp, ctypes.POINTER(ctypes.c_double)]),
     "elsa_solver_iterate": (_st, [_vp, _i32, _vp]),
     "elsa_solver_iterate_graph": (_st, [_vp, _i32, _vp]),
@@ -278,6 +285,30 @@ class Projector:
             pass
 
 
+def subset_split(dim, poses, num_subsets, strategy=SUBSET_ROUND_ROBIN):
+    """Ordered-subset partition of the poses (SubsetSampler): a list of num_subsets lists of
+    pose indices."""
+    ps = np.ascontiguousarray(poses, np.float32).reshape(-1)
+    n = ps.size // POSE_FLOATS
+    order = np.zeros(max(1, n), np.int32)
+    sizes = np.zeros(max(1, int(num_subsets)), np.int32)
+    call("elsa_subset_split", int(dim), np_ptr(ps), int(n), int(num_subsets), int(strategy),
+         np_ptr(order), np_ptr(sizes))
+    out, k = [], 0
+    for c in sizes[:int(num_subsets)]:
+        out.append([int(v) for v in order[k:k + int(c)]])
+        k += int(c)
+    return out
+
+
+def gather_views(sino_ptr, view_size, views, total_views, out_ptr, stream=None):
+    """Device copy of the sinogram views `views` (in that order) to out (elsa_gather_views)."""
+    idx = np.ascontiguousarray(views, np.int32)
+    call("elsa_gather_views", ctypes.c_void_p(sino_ptr), int(view_size),
+         np_ptr(idx) if idx.size else None, int(idx.size), int(total_views),
+         ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream or 0))
+
+
 def tune_cache_size():
     n = ctypes.c_int64()
     call("elsa_tune_cache_size", ctypes.byref(n))
@@ -355,6 +386,25 @@ class Solver:
              ctypes.c_void_p(x_ptr), int(bool(use_x0)), arr, len(params),
              ctypes.c_void_p(stream or 0), ctypes.byref(h))
         self._h = h
+
+    @classmethod
+    def sqs(cls, projector, b_ptr, x_ptr, subsets=(), use_x0=False, momentum=True,
+            epsilon=1.1920928955078125e-07, preconditioner_ptr=None, stream=None):
+        """SQS on LeastSquares(projector, b) (elsa_sqs_create). subsets: (Projector, b_ptr)
+        pairs of an ordered-subset split (none: the full problem)."""
+        self = cls.__new__(cls)
+        self._proj = projector
+        self._subsets = list(subsets)  # keep the subset operators alive
+        n = len(self._subsets)
+        projs = (ctypes.c_void_p * max(1, n))(*[p.handle.value for p, _ in self._subsets])
+        bs = (ctypes.c_void_p * max(1, n))(*[int(bp) for _, bp in self._subsets])
+        h = ctypes.c_void_p()
+        call("elsa_sqs_create", projector.handle, ctypes.c_void_p(b_ptr), projs, bs, n,
+             ctypes.c_void_p(x_ptr), int(bool(use_x0)), int(bool(momentum)), float(epsilon),
+             ctypes.c_void_p(preconditioner_ptr or 0), ctypes.c_void_p(stream or 0),
+             ctypes.byref(h))
+        self._h = h
+        return self
 
     def iterate_graph(self, iterations, stream):
         call("elsa_solver_iterate_graph", self._h, int(iterations), ctypes.c_void_p(stream))

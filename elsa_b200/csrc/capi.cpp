@@ -506,11 +506,11 @@ elsa_status elsa_solver_create(int32_t kind, elsa_projector* p, const float* b, 
         require(out != nullptr, "elsa_solver_create: null output handle");
         *out = nullptr;
         require(p && b && x, "elsa_solver_create: null argument");
-        require(kind >= ELSA_SOLVER_CGNE && kind <= ELSA_SOLVER_OGM,
+        require(kind >= ELSA_SOLVER_CGNE && kind <= ELSA_SOLVER_SQS,
                 "elsa_solver_create: unknown solver kind");
         require(numParams >= 0 && (numParams == 0 || params != nullptr),
                 "elsa_solver_create: invalid parameter array");
-        static const int kMaxParams[] = {0, 2, 1, 6, 1, 1, 1};
+        static const int kMaxParams[] = {0, 2, 1, 6, 1, 1, 1, 2};
         require(numParams <= kMaxParams[kind], "elsa_solver_create: too many parameters");
         auto param = [&](int i, double dflt) { return i < numParams ? params[i] : dflt; };
         elsa_b200::SolverOptions opt;
@@ -556,6 +556,16 @@ elsa_status elsa_solver_create(int32_t kind, elsa_projector* p, const float* b, 
             require(std::isfinite(opt.momentumEpsilon) && opt.momentumEpsilon >= 0.0,
                     "elsa_solver_create: epsilon must be finite and >= 0");
             break;
+        case ELSA_SOLVER_SQS: {
+            const double momentum = param(0, 1.0);
+            require(momentum == 0.0 || momentum == 1.0,
+                    "elsa_solver_create: SQS momentum must be 0 or 1");
+            opt.sqsMomentum = momentum == 1.0;
+            opt.sqsEpsilon = param(1, static_cast<double>(FLT_EPSILON));
+            require(std::isfinite(opt.sqsEpsilon) && opt.sqsEpsilon >= 0.0,
+                    "elsa_solver_create: epsilon must be finite and >= 0");
+            break;
+        }
         default:
             break;
         }
@@ -566,6 +576,95 @@ elsa_status elsa_solver_create(int32_t kind, elsa_projector* p, const float* b, 
             static_cast<elsa_b200::SolverKind>(kind), *p->impl, b, x, useX0 != 0, opt,
             asStream(stream));
         *out = h.release();
+    });
+}
+
+elsa_status elsa_sqs_create(elsa_projector* p, const float* b,
+                            elsa_projector* const* subsetProjectors, const float* const* subsetB,
+                            int32_t numSubsets, float* x, int32_t useX0, int32_t momentum,
+                            double epsilon, const float* preconditioner, void* stream,
+                            elsa_solver** out)
+{
+    return guarded([&] {
+        require(out != nullptr, "elsa_sqs_create: null output handle");
+        *out = nullptr;
+        require(p && b && x, "elsa_sqs_create: null argument");
+        require(numSubsets == 0 || numSubsets >= 2,
+                "elsa_sqs_create: use 0 subsets (full problem) or at least 2");
+        require(numSubsets == 0 || (subsetProjectors && subsetB),
+                "elsa_sqs_create: null subset arrays");
+        require(momentum == 0 || momentum == 1, "elsa_sqs_create: momentum must be 0 or 1");
+        require(std::isfinite(epsilon) && epsilon >= 0.0,
+                "elsa_sqs_create: epsilon must be finite and >= 0");
+        std::vector<elsa_b200::SubsetRef> subsets;
+        for (int32_t i = 0; i < numSubsets; ++i) {
+            require(subsetProjectors[i] && subsetB[i], "elsa_sqs_create: null subset");
+            subsets.push_back({subsetProjectors[i]->impl.get(), subsetB[i]});
+        }
+        elsa_b200::SolverOptions opt;
+        opt.sqsMomentum = momentum != 0;
+        opt.sqsEpsilon = epsilon;
+        opt.sqsPreconditioner = preconditioner;
+        onDevice(p);
+        auto h = std::make_unique<elsa_solver>();
+        h->device = p->impl->device();
+        h->impl = std::make_unique<elsa_b200::SolverSession>(
+            elsa_b200::SolverKind::SQS, *p->impl, b, x, useX0 != 0, opt, asStream(stream),
+            std::move(subsets));
+        *out = h.release();
+    });
+}
+
+elsa_status elsa_subset_split(int32_t dim, const float* poses, int32_t numPoses,
+                              int32_t numSubsets, int32_t strategy, int32_t* viewOrder,
+                              int32_t* subsetSizes)
+{
+    return guarded([&] {
+        require(poses && viewOrder && subsetSizes, "elsa_subset_split: null argument");
+        require(dim == 2 || dim == 3, "elsa_subset_split: dim must be 2 or 3");
+        require(numPoses >= 1, "elsa_subset_split: no poses");
+        require(numSubsets >= 2, "SubsetSampler: nSubsets must be >= 2");
+        require(strategy == ELSA_SUBSET_ROUND_ROBIN ||
+                    strategy == ELSA_SUBSET_ROTATIONAL_CLUSTERING,
+                "SubsetSampler: unsupported sampling strategy");
+        std::vector<elsa_b200::PoseRecord> recs(static_cast<size_t>(numPoses));
+        std::memcpy(recs.data(), poses, sizeof(float) * elsa_b200::kPoseFloats * recs.size());
+        std::vector<std::vector<int>> parts;
+        if (strategy == ELSA_SUBSET_ROUND_ROBIN) {
+            std::vector<int> idx(static_cast<size_t>(numPoses));
+            for (int32_t i = 0; i < numPoses; ++i)
+                idx[static_cast<size_t>(i)] = i;
+            parts = elsa_b200::splitRoundRobin(idx, numSubsets);
+        } else {
+            parts = elsa_b200::splitRotationalClustering(dim, recs, numSubsets);
+        }
+        int32_t k = 0;
+        for (int32_t i = 0; i < numSubsets; ++i) {
+            const auto& part = parts[static_cast<size_t>(i)];
+            subsetSizes[i] = static_cast<int32_t>(part.size());
+            for (int v : part)
+                viewOrder[k++] = v;
+        }
+    });
+}
+
+elsa_status elsa_gather_views(const float* sinogram, int64_t viewSize, const int32_t* viewOrder,
+                              int32_t numViews, int32_t totalViews, float* out, void* stream)
+{
+    return guarded([&] {
+        require(viewSize >= 0 && numViews >= 0 && totalViews >= 0,
+                "elsa_gather_views: negative size");
+        require(numViews == 0 || viewSize == 0 || (sinogram && out && viewOrder),
+                "elsa_gather_views: null argument");
+        for (int32_t j = 0; j < numViews; ++j) {
+            const int32_t v = viewOrder[j];
+            require(v >= 0 && v < totalViews, "elsa_gather_views: view index out of range");
+        }
+        for (int32_t j = 0; j < numViews && viewSize > 0; ++j)
+            ELSA_CUDA(cudaMemcpyAsync(out + static_cast<int64_t>(j) * viewSize,
+                                      sinogram + static_cast<int64_t>(viewOrder[j]) * viewSize,
+                                      sizeof(float) * static_cast<size_t>(viewSize),
+                                      cudaMemcpyDeviceToDevice, asStream(stream)));
     });
 }
 

@@ -7,6 +7,7 @@
 // compiled without floating-point contraction (-ffp-contract=off).
 #include "geometry.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -360,5 +361,45 @@ namespace elsa_b200
                                            rad, 0.0f, 0.0f, zero, zero));
         }
         return poses;
+    }
+
+    std::vector<std::vector<int>> splitRoundRobin(const std::vector<int>& indices, int nSubsets)
+    {
+        std::vector<std::vector<int>> out(static_cast<size_t>(nSubsets));
+        for (size_t i = 0; i < indices.size(); ++i)
+            out[i % static_cast<size_t>(nSubsets)].push_back(indices[i]);
+        return out;
+    }
+
+    std::vector<std::vector<int>> splitRotationalClustering(int dim,
+                                                            const std::vector<PoseRecord>& poses,
+                                                            int nSubsets)
+    {
+        // rotation block of the extrinsic matrix [R | t] (row stride dim + 1)
+        auto rot = [dim](const PoseRecord& r, int i, int j) {
+            return r.v[kPoseOffExt + i * (dim + 1) + j];
+        };
+        // R1 R2^T coefficient (i, j): k-sum in sequence, as a coefficient-based small product
+        auto prod = [&](const PoseRecord& a, const PoseRecord& b, int i, int j) {
+            float acc = rot(a, i, 0) * rot(b, j, 0);
+            for (int k = 1; k < dim; ++k)
+                acc = acc + rot(a, i, k) * rot(b, j, k);
+            return acc;
+        };
+        const PoseRecord first = poses.front();
+        auto dist = [&](const PoseRecord& g) {
+            if (dim == 2)
+                return static_cast<double>(std::atan2(prod(first, g, 1, 0), prod(first, g, 0, 0)));
+            float trace = prod(first, g, 0, 0) + prod(first, g, 1, 1);
+            trace = trace + prod(first, g, 2, 2);
+            return std::acos((trace - 1.0) / 2.0);
+        };
+        std::vector<int> idx(poses.size());
+        for (size_t i = 0; i < idx.size(); ++i)
+            idx[i] = static_cast<int>(i);
+        std::sort(idx.begin(), idx.end(), [&](int lhs, int rhs) {
+            return dist(poses[static_cast<size_t>(lhs)]) < dist(poses[static_cast<size_t>(rhs)]);
+        });
+        return splitRoundRobin(idx, nSubsets);
     }
 } // namespace elsa_b200

@@ -47,4 +47,14 @@ namespace elsa_b200
                                              float arcDegrees, float s2c, float c2d,
                                              const int64_t* detSize, const float* detSpacing,
                                              int64_t* detDims);
+
+    // Ordered-subset partitions of the poses (projectors/SubsetSampler.cpp:50-103): subset i of
+    // a round robin takes positions i, i + n, i + 2n, ... of `indices`; rotational clustering
+    // first sorts the pose indices by the rotation angle to the first pose (2D: the signed angle
+    // atan2(R0 R^T (1,0), R0 R^T (0,0)); 3D: acos((trace(R0 R^T) - 1) / 2)), with std::sort as
+    // the reference does, then splits them round robin.
+    std::vector<std::vector<int>> splitRoundRobin(const std::vector<int>& indices, int nSubsets);
+    std::vector<std::vector<int>> splitRotationalClustering(int dim,
+                                                            const std::vector<PoseRecord>& poses,
+                                                            int nSubsets);
 } // namespace elsa_b200

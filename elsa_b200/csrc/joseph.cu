@@ -32,6 +32,7 @@
 #include "solvers.hpp"
 
 #include <algorithm>
+#include <mutex>
 #include <cmath>
 #include <cstring>
 
@@ -628,11 +629,21 @@ namespace elsa_b200
             {
                 return kAccBytes + (sizeof(RayWindow) + sizeof(unsigned)) * np;
             }
+            // The dynamic shared-memory limit is an attribute of the kernel on the device, shared
+            // by every projector: it only ever grows, so a projector with fewer views created
+            // later leaves room for the earlier ones.
             static void prepare(int np)
             {
-                ELSA_CUDA(cudaFuncSetAttribute(josephAdjointKernel<DIM, BX, BY, BZ, CPD, NW>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>(smemBytes(np))));
+                static std::mutex mu;
+                std::lock_guard<std::mutex> lock(mu);
+                cudaFuncAttributes attr{};
+                ELSA_CUDA(cudaFuncGetAttributes(&attr,
+                                                josephAdjointKernel<DIM, BX, BY, BZ, CPD, NW>));
+                const int need = static_cast<int>(smemBytes(np));
+                if (need > attr.maxDynamicSharedSizeBytes)
+                    ELSA_CUDA(cudaFuncSetAttribute(josephAdjointKernel<DIM, BX, BY, BZ, CPD, NW>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   need));
             }
             // Views per chunk so that bricks x chunks fills about kAdjoint2dCtasPerSm CTAs per SM
             // (16 measured best among 1-16 at 128^2 x 180 views and 512^2 x 720 views). The

@@ -354,10 +354,107 @@ namespace elsa_b200
         ELSA_CUDA(cudaMemcpyAsync(&S->tPrev, &one, sizeof(double), cudaMemcpyHostToDevice, s));
     }
 
-    SolverSession::SolverSession(SolverKind kind, Projector& A, const float* b, float* x,
-                                 bool useX0, const SolverOptions& opt, cudaStream_t s)
-        : kind_(kind), opt_(opt), A_(A), b_(b), x_(x), ws_(A.domainSize(), A.rangeSize())
+    // SQS: solvers/SQS.cpp:87-170 on the least-squares problem 0.5 |A x - b|^2
+    // (functionals/LeastSquares.cpp:45-59: gradient A^T (A x - b), Hessian A^T A). ws.vol0 =
+    // prevX, vol1 = gradient, vol2 = D = 1 / (A^T A 1), vol3 = full gradient for the subset-mode
+    // convergence check; S->alpha = t, S->beta = prevT.
+    static void sqsGradient(Projector& A, const float* b, const float* x, float* g,
+                            SolverWorkspace& ws, KernelTimer& t, cudaStream_t s)
     {
+        float* sino = ws.sino0.as<float>();
+        t.mark(s);
+        A.forward(x, sino, s);
+        t.mark(s);
+        launchSub(sino, b, sino, A.rangeSize(), s);
+        A.adjoint(sino, g, s);
+        t.mark(s);
+    }
+
+    static void sqsBegin(Projector& A, const float* b, float* x, bool useX0, double eps,
+                         SolverWorkspace& ws, cudaStream_t s)
+    {
+        const int64_t n = A.domainSize();
+        SolverScalars* S = ws.scalars.as<SolverScalars>();
+        double* partials = ws.partials.as<double>();
+        ELSA_CUDA(cudaMemsetAsync(S, 0, sizeof(SolverScalars), s));
+        if (!useX0)
+            launchFill(x, 0.0f, n, s);
+        KernelTimer off;
+        sqsGradient(A, b, x, ws.vol1.as<float>(), ws, off, s);
+        launchSquaredNorm(ws.vol1.as<float>(), n, partials, &S->k, s);
+        launchSqsBegin(S, eps * eps, s);
+        float* D = ws.vol2.as<float>();
+        launchFill(D, 1.0f, n, s);
+        A.forward(D, ws.sino0.as<float>(), s);
+        A.adjoint(ws.sino0.as<float>(), D, s); // A^T A 1
+        launchReciprocal(D, 0.0f, D, n, s);
+        ELSA_CUDA(cudaMemcpyAsync(ws.vol0.as<float>(), x, sizeof(float) * n,
+                                  cudaMemcpyDeviceToDevice, s)); // prevX
+    }
+
+    void SolverSession::sqsIterate(int iterations, cudaStream_t s)
+    {
+        const int64_t n = A_.domainSize();
+        SolverScalars* S = ws_.scalars.as<SolverScalars>();
+        double* partials = ws_.partials.as<double>();
+        const bool subsetMode = !subsets_.empty();
+        const int nSub = subsetMode ? static_cast<int>(subsets_.size()) : 1;
+        const int momentum = opt_.sqsMomentum ? 1 : 0;
+        for (int it = 0; it < iterations && !hostDone_; ++it) {
+            for (int m = 0; m < nSub && !hostDone_; ++m) {
+                Projector& Am = subsetMode ? *subsets_[static_cast<size_t>(m)].A : A_;
+                const float* bm = subsetMode ? subsets_[static_cast<size_t>(m)].b : b_;
+                sqsGradient(Am, bm, x_, ws_.vol1.as<float>(), ws_, timer_, s);
+                launchSqsStep(x_, ws_.vol0.as<float>(), ws_.vol1.as<float>(),
+                              ws_.vol2.as<float>(), opt_.sqsPreconditioner,
+                              static_cast<float>(nSub), momentum, n, S, partials, s);
+                launchSqsFinish(partials, S, subsetMode ? 1 : 0, momentum, s);
+                if (!subsetMode)
+                    continue;
+                // the subset gradient passed the threshold: SQS.cpp:131-133 confirms with the
+                // full problem's gradient at the new iterate (one host synchronization per
+                // subset step)
+                double candidate = 0.0;
+                ELSA_CUDA(cudaMemcpyAsync(&candidate, &S->aux[0], sizeof(double),
+                                          cudaMemcpyDeviceToHost, s));
+                ELSA_CUDA(cudaStreamSynchronize(s));
+                if (candidate == 0.0)
+                    continue;
+                static const double zero = 0.0;
+                ELSA_CUDA(cudaMemcpyAsync(&S->aux[0], &zero, sizeof(double),
+                                          cudaMemcpyHostToDevice, s));
+                KernelTimer off;
+                sqsGradient(A_, b_, x_, ws_.vol3.as<float>(), ws_, off, s);
+                launchSquaredNorm(ws_.vol3.as<float>(), n, partials, &S->den, s);
+                SolverScalars h;
+                ELSA_CUDA(cudaMemcpyAsync(&h, S, sizeof(h), cudaMemcpyDeviceToHost, s));
+                ELSA_CUDA(cudaStreamSynchronize(s));
+                if (h.den <= h.aux[1]) {
+                    launchSetFlag(&S->done, s);
+                    hostDone_ = true;
+                }
+            }
+        }
+    }
+
+    SolverSession::SolverSession(SolverKind kind, Projector& A, const float* b, float* x,
+                                 bool useX0, const SolverOptions& opt, cudaStream_t s,
+                                 std::vector<SubsetRef> subsets)
+        : kind_(kind), opt_(opt), A_(A), b_(b), x_(x), ws_(A.domainSize(), A.rangeSize()),
+          subsets_(std::move(subsets))
+    {
+        if (!subsets_.empty() && kind_ != SolverKind::SQS)
+            throw Error(ELSA_ERROR_INVALID_ARGUMENT, "only SQS takes ordered subsets");
+        for (const SubsetRef& r : subsets_) {
+            if (!r.A || !r.b)
+                throw Error(ELSA_ERROR_INVALID_ARGUMENT, "SQS: null subset");
+            if (r.A->domainSize() != A.domainSize() || r.A->rangeSize() > A.rangeSize())
+                throw Error(ELSA_ERROR_INVALID_ARGUMENT,
+                            "SQS: a subset projector must share the volume and have at most "
+                            "the full problem's views");
+            if (r.A->device() != A.device())
+                throw Error(ELSA_ERROR_INVALID_ARGUMENT, "SQS: subsets on another device");
+        }
         switch (kind_) {
         case SolverKind::CGNE:
             cgneBegin(A_, b_, x_, useX0, ws_, s);
@@ -402,11 +499,18 @@ namespace elsa_b200
             momentumBegin(A_, b_, x_, useX0, ws_, s);
             break;
         }
+        case SolverKind::SQS:
+            sqsBegin(A_, b_, x_, useX0, opt_.sqsEpsilon, ws_, s);
+            break;
         }
     }
 
     void SolverSession::iterate(int iterations, cudaStream_t s)
     {
+        if (kind_ == SolverKind::SQS) {
+            sqsIterate(iterations, s);
+            return;
+        }
         for (int it = 0; it < iterations; ++it) {
             switch (kind_) {
             case SolverKind::CGNE:
@@ -439,6 +543,8 @@ namespace elsa_b200
                                         opt_.momentumEpsilon * opt_.momentumEpsilon, s);
                 break;
             }
+            case SolverKind::SQS:
+                break; // handled above
             }
         }
     }
@@ -456,6 +562,10 @@ namespace elsa_b200
                         "solver graphs need an explicitly created stream");
         if (timer_.enabled())
             throw Error(ELSA_ERROR_INVALID_ARGUMENT, "solver graphs need timing disabled");
+        if (!subsets_.empty())
+            throw Error(ELSA_ERROR_NOT_SUPPORTED,
+                        "SQS with ordered subsets confirms convergence on the host and cannot "
+                        "run as a CUDA graph");
         if (!graph_ || graphIterations_ != iterations) {
             if (graph_) {
                 ELSA_CUDA(cudaGraphExecDestroy(graph_));
@@ -510,7 +620,8 @@ namespace elsa_b200
         ELSA_CUDA(cudaMemcpyAsync(&h, ws_.scalars.as<SolverScalars>(), sizeof(h),
                                   cudaMemcpyDeviceToHost, s));
         ELSA_CUDA(cudaStreamSynchronize(s));
-        if (kind_ == SolverKind::APGD || kind_ == SolverKind::FGM || kind_ == SolverKind::OGM)
+        if (kind_ == SolverKind::APGD || kind_ == SolverKind::FGM || kind_ == SolverKind::OGM ||
+            kind_ == SolverKind::SQS)
             return h.k;
         if (kind_ == SolverKind::SIRT)
             return 0.0;

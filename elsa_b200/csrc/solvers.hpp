@@ -62,7 +62,22 @@ namespace elsa_b200
         int64_t count_ = 0;
     };
 
-    enum class SolverKind { CGNE = 0, CGLS = 1, LANDWEBER = 2, APGD = 3, SIRT = 4, FGM = 5, OGM = 6 };
+    enum class SolverKind {
+        CGNE = 0,
+        CGLS = 1,
+        LANDWEBER = 2,
+        APGD = 3,
+        SIRT = 4,
+        FGM = 5,
+        OGM = 6,
+        SQS = 7
+    };
+
+    // One ordered subset of an SQS problem: the subset's projector (its views) and measurements.
+    struct SubsetRef {
+        Projector* A;
+        const float* b;
+    };
 
     // Solver options (elsa's constructor arguments). Step sizes <= 0 mean "derive from power
     // iterations", as the reference does when none is given.
@@ -77,6 +92,9 @@ namespace elsa_b200
         double sirtStep = 0.0;   // <= 0: 0.9 * 2 / lambda_max(T A^T M A), solvers/SIRT.cpp
         double momentumEpsilon = 1.1920928955078125e-07; // FGM / OGM: stop once
                                                           // |grad|^2 <= eps^2 |grad_0|^2
+        bool sqsMomentum = true;                     // SQS momentum acceleration
+        double sqsEpsilon = 1.1920928955078125e-07;  // SQS: stop once |g|^2 <= eps^2 |grad_0|^2
+        const float* sqsPreconditioner = nullptr;    // SQS: diagonal applied to the gradient
     };
 
     // Largest eigenvalue of A^T A by power iterations, solvers/PowerIterations.cpp:10-27
@@ -93,8 +111,11 @@ namespace elsa_b200
     class SolverSession
     {
     public:
+        // subsets: SQS in ordered-subset mode (every subset projector has A's domain and at
+        // most A's range); empty for the full problem and for the other kinds.
         SolverSession(SolverKind kind, Projector& A, const float* b, float* x, bool useX0,
-                      const SolverOptions& opt, cudaStream_t s);
+                      const SolverOptions& opt, cudaStream_t s,
+                      std::vector<SubsetRef> subsets = {});
         ~SolverSession();
         SolverSession(const SolverSession&) = delete;
         SolverSession& operator=(const SolverSession&) = delete;
@@ -120,6 +141,9 @@ namespace elsa_b200
         float lipschitz_ = 0.0f;
         cudaGraphExec_t graph_ = nullptr;
         int graphIterations_ = -1;
+        std::vector<SubsetRef> subsets_;
+        bool hostDone_ = false; // SQS with subsets: convergence confirmed on the host
+        void sqsIterate(int iterations, cudaStream_t s);
     };
 
     // Runs `iterations` iterations of every session, each as its CUDA graph, spread round-robin

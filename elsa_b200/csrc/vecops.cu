@@ -534,6 +534,113 @@ namespace elsa_b200
         }
     } // namespace
 
+    namespace
+    {
+        // nextT of SQS.cpp:123-124, in float: 1 + sqrt(1 + 4 * t * t) / 2
+        __device__ __forceinline__ float sqsNextT(float t)
+        {
+            const float q = __fadd_rn(1.0f, __fmul_rn(__fmul_rn(4.0f, t), t));
+            return __fadd_rn(1.0f, __fdiv_rn(__fsqrt_rn(q), 2.0f));
+        }
+
+        __global__ void __launch_bounds__(kReduceThreads)
+            sqsStepKernel(float* __restrict__ x, float* __restrict__ prevX,
+                          const float* __restrict__ g, const float* __restrict__ D,
+                          const float* __restrict__ P, float nSub, int momentum, int64_t n,
+                          const SolverScalars* S, double* __restrict__ partials)
+        {
+            const bool done = S->done != 0;
+            const float t = static_cast<float>(S->alpha);
+            const float prevT = static_cast<float>(S->beta);
+            const float coef = __fdiv_rn(prevT, sqsNextT(t));
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            double acc = 0.0;
+            for (int64_t i = tid; i < n; i += T) {
+                float gi = g[i];
+                if (P)
+                    gi = __fmul_rn(P[i], gi);
+                acc += static_cast<double>(gi) * gi;
+                if (done)
+                    continue;
+                float xn = __fsub_rn(x[i], __fmul_rn(nSub, __fmul_rn(D[i], gi)));
+                if (momentum) {
+                    xn = __fadd_rn(xn, __fmul_rn(coef, __fsub_rn(xn, prevX[i])));
+                    prevX[i] = xn;
+                }
+                x[i] = xn;
+            }
+            const double sum = blockSum(acc);
+            if (threadIdx.x == 0)
+                partials[blockIdx.x] = sum;
+        }
+
+        __global__ void __launch_bounds__(kReduceThreads)
+            sqsFinishKernel(const double* __restrict__ partials, SolverScalars* S, int subsetMode,
+                            int momentum)
+        {
+            const double g2 = sumPartials(partials);
+            if (threadIdx.x == 0) {
+                S->k = g2;
+                if (!S->done) {
+                    if (g2 <= S->aux[1]) {
+                        if (subsetMode)
+                            S->aux[0] = 1.0;
+                        else
+                            S->done = 1;
+                    }
+                    if (momentum) {
+                        const float t = static_cast<float>(S->alpha);
+                        S->beta = t;
+                        S->alpha = sqsNextT(t);
+                    }
+                }
+            }
+        }
+
+        __global__ void sqsBeginKernel(SolverScalars* S, double eps2)
+        {
+            S->alpha = 1.0;
+            S->beta = 1.0;
+            S->aux[0] = 0.0;
+            S->aux[1] = S->k * eps2;
+            S->done = 0;
+        }
+
+        __global__ void setFlagKernel(int* flag)
+        {
+            *flag = 1;
+        }
+    } // namespace
+
+    void launchSqsStep(float* x, float* prevX, const float* g, const float* D, const float* P,
+                       float nSub, int momentum, int64_t n, const SolverScalars* S,
+                       double* partials, cudaStream_t s)
+    {
+        sqsStepKernel<<<kReduceBlocks, kReduceThreads, 0, s>>>(x, prevX, g, D, P, nSub, momentum,
+                                                               n, S, partials);
+        ELSA_LAUNCH_CHECK("sqsStep");
+    }
+
+    void launchSqsFinish(const double* partials, SolverScalars* S, int subsetMode, int momentum,
+                         cudaStream_t s)
+    {
+        sqsFinishKernel<<<1, kReduceThreads, 0, s>>>(partials, S, subsetMode, momentum);
+        ELSA_LAUNCH_CHECK("sqsFinish");
+    }
+
+    void launchSqsBegin(SolverScalars* S, double eps2, cudaStream_t s)
+    {
+        sqsBeginKernel<<<1, 1, 0, s>>>(S, eps2);
+        ELSA_LAUNCH_CHECK("sqsBegin");
+    }
+
+    void launchSetFlag(int* flag, cudaStream_t s)
+    {
+        setFlagKernel<<<1, 1, 0, s>>>(flag);
+        ELSA_LAUNCH_CHECK("setFlag");
+    }
+
     void launchReciprocal(const float* in, float lift, float* out, int64_t n, cudaStream_t s)
     {
         reciprocalKernel<<<gridFor(n), 256, 0, s>>>(in, lift, out, n);

@@ -110,4 +110,22 @@ namespace elsa_b200
                               cudaStream_t s);
     // S->tPrev = t; S->k = sum(partials); S->done |= (S->k <= eps)
     void launchApgdFinish(const double* partials, SolverScalars* S, double eps, cudaStream_t s);
+
+    // SQS (solvers/SQS.cpp:105-142), S->alpha = t, S->beta = prevT (float values), S->aux[1] =
+    // the convergence threshold. Step: g = P g (when P is given); partials = sum g^2; unless
+    // S->done: x = x - nSub * (D g) and, with momentum, nextT = 1 + sqrt(1 + 4 t t) / 2,
+    // x = x + prevT / nextT * (x - prevX), prevX = x. Float operations in the reference's order.
+    void launchSqsStep(float* x, float* prevX, const float* g, const float* D, const float* P,
+                       float nSub, int momentum, int64_t n, const SolverScalars* S,
+                       double* partials, cudaStream_t s);
+    // S->k = sum(partials); unless S->done: if S->k <= S->aux[1] set S->done (full problem) or
+    // S->aux[0] = 1 (ordered subsets: the caller confirms with the full gradient); with momentum
+    // prevT = t, t = nextT.
+    void launchSqsFinish(const double* partials, SolverScalars* S, int subsetMode, int momentum,
+                         cudaStream_t s);
+    // S->alpha = S->beta = 1, S->aux[0] = 0, S->done = 0, S->aux[1] = S->k * eps2 (S->k holds
+    // |grad_0|^2).
+    void launchSqsBegin(SolverScalars* S, double eps2, cudaStream_t s);
+    // *value = 1 (device int)
+    void launchSetFlag(int* flag, cudaStream_t s);
 } // namespace elsa_b200

@@ -271,7 +271,12 @@ typedef enum elsa_solver_kind {
      * Lipschitz constant). params[0] = epsilon as FGM. The last iteration of each
      * elsa_solver_iterate call uses OGM's final-step factor, so one call of n iterations matches
      * OGM::solve(n). */
-    ELSA_SOLVER_OGM = 6
+    ELSA_SOLVER_OGM = 6,
+    /* SQS<float> on LeastSquares(A, b) without subsets, solvers/SQS.cpp:87-170 (diagonal
+     * majorizer 1 / (A^T A 1)). params[0] = momentum acceleration (1 default, 0 off),
+     * params[1] = epsilon (stop once |grad|^2 <= epsilon^2 |grad_0|^2, default FLT_EPSILON).
+     * Ordered subsets and a preconditioner: elsa_sqs_create. */
+    ELSA_SOLVER_SQS = 7
 } elsa_solver_kind;
 
 /* Set up a solver run: allocate its scratch, compute the initial residual (x is zeroed unless
@@ -285,8 +290,45 @@ elsa_status elsa_solver_create(int32_t kind, elsa_projector* projector, const fl
                                int32_t use_x0, const double* params, int32_t num_params,
                                void* stream, elsa_solver** out);
 
+/* SQS with ordered subsets, solvers/SQS.cpp:10-22,87-170: the constructor
+ * SQS(problem, subsets, [preconditioner,] momentumAcceleration, epsilon) + the first half of
+ * solve(). projector / b: the full problem LeastSquares(A, b) (device buffer b); subset i:
+ * LeastSquares(subset_projectors[i], subset_b[i]) with subset_b[i] that subset's measurements
+ * (device buffers, e.g. from elsa_gather_views), every subset projector sharing the volume and
+ * having at most the full problem's views; num_subsets 0 solves the full problem, otherwise it
+ * must be >= 2. preconditioner: NULL or a device volume buffer p, the diagonal operator applied
+ * to every gradient (a Scaling preconditioner). With subsets, each subset step whose gradient
+ * passes the threshold is confirmed with the full gradient on the host (one stream
+ * synchronization per subset step), so such a solver cannot run as a CUDA graph
+ * (elsa_solver_iterate_graph / elsa_solve_batch return ELSA_ERROR_NOT_SUPPORTED). The
+ * projectors and buffers must outlive the solver. */
+elsa_status elsa_sqs_create(elsa_projector* projector, const float* b,
+                            elsa_projector* const* subset_projectors, const float* const* subset_b,
+                            int32_t num_subsets, float* x, int32_t use_x0, int32_t momentum,
+                            double epsilon, const float* preconditioner, void* stream,
+                            elsa_solver** out);
+
+/* Ordered-subset sampling strategies, projectors/SubsetSampler.h:28-31. */
+#define ELSA_SUBSET_ROUND_ROBIN 0
+#define ELSA_SUBSET_ROTATIONAL_CLUSTERING 1
+
+/* Split num_poses poses (pose records as elsa_projector_create takes them) into num_subsets >= 2
+ * subsets (SubsetSampler::splitRoundRobin / splitRotationalClustering,
+ * projectors/SubsetSampler.cpp:50-103). view_order (num_poses entries) receives the pose indices
+ * subset by subset, subset_sizes (num_subsets entries) the number of poses per subset. Host
+ * only. */
+elsa_status elsa_subset_split(int32_t dim, const float* poses, int32_t num_poses,
+                              int32_t num_subsets, int32_t strategy, int32_t* view_order,
+                              int32_t* subset_sizes);
+
+/* out[j] = sinogram view view_order[j] (view_size floats each; device buffers, host index array;
+ * asynchronous on `stream`): the per-subset measurement blocks of
+ * SubsetSampler::getPartitionedData, projectors/SubsetSampler.cpp:120-150. */
+elsa_status elsa_gather_views(const float* sinogram, int64_t view_size, const int32_t* view_order,
+                              int32_t num_views, int32_t total_views, float* out, void* stream);
+
 /* Step size in use (Landweber / SIRT step, APGD mu, FGM / OGM 1 / Lipschitz; 0 for the CG
- * solvers). */
+ * solvers and SQS). */
 elsa_status elsa_solver_step_size(elsa_solver* solver, double* value);
 
 /* Largest eigenvalue of A^T A by `iterations` power iterations from u = 1, in float with float64

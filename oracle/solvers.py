@@ -11,6 +11,8 @@ It restates the reference solvers on float32 vectors, with the projector given a
              proximal_operators/ProximalL1.cpp:24-38
 * SIRT       solvers/SIRT.cpp:8-45 (Landweber with T A^T M)
 * FGM, OGM   solvers/FGM.cpp:33-78, solvers/OGM.cpp:40-95 on LeastSquares (A^T (A x - b))
+* SQS        solvers/SQS.cpp:87-170 (ordered subsets, momentum, diagonal preconditioner) and the
+             subset splits of projectors/SubsetSampler.cpp:50-103
 * powerIterations  solvers/PowerIterations.cpp:10-27
 
 Every solver takes dtype=np.float32 (the reference's float instantiation, the parity target) or
@@ -242,3 +244,80 @@ def fgm(A, At, b, domain_size, iterations, x0=None, epsilon=F32_EPS, dtype=np.fl
 def ogm(A, At, b, domain_size, iterations, x0=None, epsilon=F32_EPS, dtype=np.float32):
     """Optimized gradient method on 0.5 |A x - b|^2, solvers/OGM.cpp:40-95."""
     return _momentum(A, At, b, domain_size, iterations, x0, epsilon, True, dtype)
+
+
+def sqs(A, At, b, domain_size, iterations, x0=None, subsets=None, momentum=True,
+        epsilon=F32_EPS, precond=None, dtype=np.float32):
+    """SQS on 0.5 |A x - b|^2, solvers/SQS.cpp:87-170. subsets: list of (A_m, At_m, b_m) for the
+    ordered-subset mode (None: the full problem); precond: diagonal applied to each gradient.
+    As in the reference, z is the same vector as x: the momentum update overwrites x, and
+    nextT = 1 + sqrt(1 + 4 t t) / 2. Returns (x, |g|^2 history, stopped early)."""
+    c = _caster(dtype)
+    one = dtype(1)
+    x = c(np.zeros(domain_size)) if x0 is None else c(x0).copy()
+    b = c(b)
+    grad = lambda A_, At_, b_, v: c(At_(c(c(A_(v)) - b_)))  # noqa: E731
+    threshold = _sq(grad(A, At, b, x)) * epsilon * epsilon
+    D = c(At(c(A(c(np.ones(domain_size))))))
+    with np.errstate(divide="ignore"):
+        D = c(one / D)
+    prev_t, t = one, one
+    prev_x = x.copy()
+    parts = subsets if subsets else [(A, At, b)]
+    n_sub = dtype(len(parts))
+    history = []
+    for _ in range(iterations):
+        for (Am, Atm, bm) in parts:
+            g = grad(Am, Atm, c(bm), x)
+            if precond is not None:
+                g = c(c(precond) * g)
+            g2 = _sq(g)
+            history.append(g2)
+            if momentum:
+                next_t = dtype(one + dtype(np.sqrt(dtype(one + dtype(dtype(4) * t) * t))) /
+                               dtype(2))
+                x = c(x - c(n_sub * c(D * g)))
+                x = c(x + c(dtype(prev_t / next_t) * c(x - prev_x)))
+            else:
+                x = c(x - c(n_sub * c(D * g)))
+            if g2 <= threshold:
+                if not subsets or _sq(grad(A, At, b, x)) <= threshold:
+                    return x, history, True
+            if momentum:
+                prev_t, t = t, next_t
+                prev_x = x.copy()
+    return x, history, False
+
+
+def subset_split_round_robin(indices, n_subsets):
+    """SubsetSampler::splitRoundRobin, projectors/SubsetSampler.cpp:56-69."""
+    out = [[] for _ in range(n_subsets)]
+    for i, v in enumerate(indices):
+        out[i % n_subsets].append(int(v))
+    return out
+
+
+def subset_split_rotational(dim, poses, n_subsets):
+    """SubsetSampler::splitRotationalClustering, projectors/SubsetSampler.cpp:71-103: pose
+    indices sorted by the rotation angle to the first pose, then round robin. Rotation blocks
+    come from the extrinsic matrix [R | t] of the 40-float pose records (offset 27, row stride
+    dim + 1); products and the trace in float32 with sequential sums, the angle as the reference
+    computes it (2D atan2 in float, 3D acos in double). Python's sort is stable where the
+    reference's std::sort is not: the two agree whenever the angles are distinct."""
+    P = np.asarray(poses, np.float32).reshape(-1, 40)
+    R = [P[i, 27:27 + dim * (dim + 1)].reshape(dim, dim + 1)[:, :dim] for i in range(len(P))]
+
+    def prod(a, b, i, j):
+        acc = np.float32(a[i, 0] * b[j, 0])
+        for k in range(1, dim):
+            acc = np.float32(acc + np.float32(a[i, k] * b[j, k]))
+        return acc
+
+    def dist(g):
+        if dim == 2:
+            return float(np.arctan2(prod(R[0], g, 1, 0), prod(R[0], g, 0, 0)))
+        tr = np.float32(np.float32(prod(R[0], g, 0, 0) + prod(R[0], g, 1, 1)) + prod(R[0], g, 2, 2))
+        return float(np.arccos((float(tr) - 1.0) / 2.0))
+
+    idx = sorted(range(len(P)), key=lambda i: dist(R[i]))
+    return subset_split_round_robin(idx, n_subsets)

@@ -121,3 +121,21 @@ def test_joseph_full_size_subset(cuda, oracle):
     Ax, Aty = _gpu_pair(cuda, proj, x, y)
     assert rel_l2(Ax, oracle.joseph(x, vol, det, poses)) <= PARITY
     assert rel_l2(Aty, oracle.joseph_adjoint(y, vol, det, poses)) <= PARITY
+
+
+def test_2d_adjoint_after_smaller_projector(cuda, oracle):
+    """The 2D adjoint's shared-memory limit is a per-kernel device attribute: a projector with
+    fewer views created later must not lower it below what an earlier one needs."""
+    vol = (64, 64)
+    poses, det = oracle.circle_trajectory(vol, 120, 360, 500, 125, [92])
+    big = _projector(vol, det, poses)
+    small_poses, small_det = oracle.circle_trajectory(vol, 10, 360, 500, 125, [92])
+    small = _projector(vol, small_det, small_poses)
+    rng = np.random.default_rng(5)
+    y = rng.uniform(0, 1, big.range_size).astype(np.float32)
+    x = rng.uniform(0, 1, big.domain_size).astype(np.float32)
+    _, bp = _gpu_pair(cuda, big, x, y)
+    assert rel_l2(bp, oracle.joseph_adjoint(y, vol, det, poses)) <= PARITY
+    ys = rng.uniform(0, 1, small.range_size).astype(np.float32)
+    _, bps = _gpu_pair(cuda, small, x, ys)
+    assert rel_l2(bps, oracle.joseph_adjoint(ys, vol, small_det, small_poses)) <= PARITY

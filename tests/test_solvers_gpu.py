@@ -254,7 +254,9 @@ def test_solver_argument_errors(cuda, oracle):
     bt = cuda.from_numpy(b).cuda()
     x = cuda.zeros(n, dtype=cuda.float32, device="cuda")
     with pytest.raises(elsa_b200.InvalidArgumentError):
-        elsa_b200.Solver(7, proj, bt.data_ptr(), x.data_ptr())
+        elsa_b200.Solver(elsa_b200.SOLVER_SQS + 1, proj, bt.data_ptr(), x.data_ptr())
+    with pytest.raises(elsa_b200.InvalidArgumentError):  # SQS momentum flag must be 0 or 1
+        elsa_b200.Solver(elsa_b200.SOLVER_SQS, proj, bt.data_ptr(), x.data_ptr(), params=(0.5,))
     with pytest.raises(elsa_b200.InvalidArgumentError):
         elsa_b200.Solver(elsa_b200.SOLVER_LANDWEBER, proj, bt.data_ptr(), x.data_ptr(),
                          params=(1.0, 2.0))
