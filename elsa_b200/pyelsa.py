@@ -430,8 +430,134 @@ class OGM(_MomentumSolver):
     _kind = _capi.SOLVER_OGM
 
 
+class Scaling:
+    """Diagonal operator (core/LinearOperators/Scaling.h), here as an SQS preconditioner:
+    Scaling(descriptor, factors) with a DataContainer or an array of factors."""
+
+    def __init__(self, descriptor, factors):
+        self.descriptor = descriptor
+        self.factors = _as_dc(factors, descriptor)
+
+    def getScaleFactors(self):
+        return self.factors
+
+
+class SQS:
+    """SQS on LeastSquares(A, b) (solvers/SQS.h:29-69) with elsa's constructor forms:
+    SQS(problem[, subsets][, preconditioner], momentumAcceleration=True, epsilon=FLT_EPSILON).
+    subsets: a list of LeastSquares problems, one per ordered subset (e.g. from a
+    SubsetSampler); preconditioner: a Scaling (or a DataContainer / array of its diagonal)."""
+
+    def __init__(self, problem, *args, momentumAcceleration=True,
+                 epsilon=1.1920928955078125e-07):
+        args = list(args)
+        self.subsets = args.pop(0) if args and isinstance(args[0], (list, tuple)) else []
+        self.preconditioner = None
+        if args and not isinstance(args[0], (bool, float, int)):
+            self.preconditioner = args.pop(0)
+        if args:
+            momentumAcceleration = bool(args.pop(0))
+        if args:
+            epsilon = float(args.pop(0))
+        if args:
+            raise TypeError("SQS: too many arguments")
+        self.problem = problem
+        self.momentum = bool(momentumAcceleration)
+        self.epsilon = float(epsilon)
+        self.last = None
+
+    def solve(self, iterations, x0=None):
+        A = self.problem.A
+        b = _as_dc(self.problem.b, A.getRangeDescriptor())
+        x = DataContainer.zeros(A.getDomainDescriptor()) if x0 is None else \
+            DataContainer(_as_dc(x0, A.getDomainDescriptor()))
+        subs = []
+        self._keep = [b]
+        for sp in self.subsets:
+            bm = _as_dc(sp.b, sp.A.getRangeDescriptor())
+            self._keep.append(bm)
+            subs.append((sp.A.native, bm._ptr()))
+        p = self.preconditioner
+        pdc = None
+        if p is not None:
+            pdc = p.getScaleFactors() if isinstance(p, Scaling) else \
+                _as_dc(p, A.getDomainDescriptor())
+            self._keep.append(pdc)
+        s = A._stream()
+        self.last = _capi.Solver.sqs(A.native, b._ptr(), x._ptr(), subsets=subs,
+                                     use_x0=x0 is not None, momentum=self.momentum,
+                                     epsilon=self.epsilon,
+                                     preconditioner_ptr=pdc._ptr() if pdc is not None else None,
+                                     stream=s)
+        self.last.iterate(int(iterations), s)
+        return x
+
+
+class SubsetSampler:
+    """SubsetSampler<PlanarDetectorDescriptor, float> (projectors/SubsetSampler.h:22-129):
+    ordered subsets of the poses of a detector descriptor. getPartitionedData returns one
+    DataContainer per subset (the blocks of the reference's PartitionDescriptor)."""
+
+    ROUND_ROBIN = _capi.SUBSET_ROUND_ROBIN
+    ROTATIONAL_CLUSTERING = _capi.SUBSET_ROTATIONAL_CLUSTERING
+
+    def __init__(self, volumeDescriptor, detectorDescriptor, nSubsets,
+                 samplingStrategy=ROUND_ROBIN):
+        if int(nSubsets) <= 1:
+            raise _capi.InvalidArgumentError(1, "SubsetSampler: nSubsets must be >= 2")
+        self._volume = volumeDescriptor
+        self._full = detectorDescriptor
+        self._n = int(nSubsets)
+        dim = detectorDescriptor.getNumberOfDimensions()
+        self._mapping = _capi.subset_split(dim, detectorDescriptor.poses, self._n,
+                                           samplingStrategy)
+        size = list(detectorDescriptor.getNumberOfCoefficientsPerDimension())
+        spacing = list(detectorDescriptor.getSpacingPerDimension())
+        self._detectors = [PlanarDetectorDescriptor(size[:-1] + [len(idx)],
+                                                    detectorDescriptor.poses[idx], spacing)
+                           for idx in self._mapping]
+
+    @staticmethod
+    def splitRoundRobin(indices, nSubsets):
+        """Subset i takes positions i, i + n, ... of indices (SubsetSampler.cpp:56-69)."""
+        out = [[] for _ in range(int(nSubsets))]
+        for i, v in enumerate(indices):
+            out[i % int(nSubsets)].append(int(v))
+        return out
+
+    @staticmethod
+    def splitRotationalClustering(detectorDescriptor, nSubsets):
+        """SubsetSampler.cpp:71-103, through elsa_subset_split."""
+        return _capi.subset_split(detectorDescriptor.getNumberOfDimensions(),
+                                  detectorDescriptor.poses, int(nSubsets),
+                                  _capi.SUBSET_ROTATIONAL_CLUSTERING)
+
+    def getIndexMapping(self):
+        return [list(m) for m in self._mapping]
+
+    def getSubsetDetectorDescriptors(self):
+        return list(self._detectors)
+
+    def getPartitionedData(self, sinogram):
+        sino = _as_dc(sinogram, self._full)
+        view = int(np.prod(self._full.getNumberOfCoefficientsPerDimension()[:-1]))
+        out = []
+        for idx, d in zip(self._mapping, self._detectors):
+            block = DataContainer.zeros(d)
+            _capi.gather_views(sino._ptr(), view, idx, self._full.getNumberOfGeometryPoses(),
+                               block._ptr(), sino._stream())
+            out.append(block)
+        return out
+
+    def getProjector(self, projectorClass):
+        return projectorClass(self._volume, self._full)
+
+    def getSubsetProjectors(self, projectorClass):
+        return [projectorClass(self._volume, d) for d in self._detectors]
+
+
 CGNEf, CGLSf, Landweberf, APGDf = CGNE, CGLS, Landweber, APGD
-SIRTf, FGMf, OGMf = SIRT, FGM, OGM
+SIRTf, FGMf, OGMf, SQSf = SIRT, FGM, OGM, SQS
 
 
 def powerIterations(op, niters=5):

@@ -62,7 +62,10 @@ def test_pyelsa_solvers(cuda, oracle):
     for solver in (elsa.CGNE(A, b), elsa.CGLS(A, b), elsa.Landweber(A, b),
                    elsa.APGD(A, b, elsa.ProximalBoxConstraint(0.0)),
                    elsa.FISTA(A, b, elsa.ProximalL1(1e-3)), elsa.SIRT(A, b),
-                   elsa.FGM(elsa.LeastSquares(A, b)), elsa.OGM(elsa.LeastSquares(A, b))):
+                   elsa.FGM(elsa.LeastSquares(A, b)), elsa.OGM(elsa.LeastSquares(A, b)),
+                   elsa.SQS(elsa.LeastSquares(A, b)),
+                   elsa.SQS(elsa.LeastSquares(A, b), elsa.Scaling(vol, np.ones((24, 24, 24))),
+                            False)):
         sol = solver.solve(15)
         res = (A.apply(sol) - b).squaredL2Norm()
         assert res < 0.2 * r0, type(solver).__name__
@@ -144,3 +147,31 @@ def test_unrolled_gradient_descent(cuda, oracle):
         with torch.no_grad():
             fd = (run(ap, False) - run(am, False)).item() / (2 * h)
         assert abs(fd - g[k]) <= 5e-2 * max(abs(fd), abs(g[k])) + 1e-3 * gmax, (k, fd, g[k])
+
+
+def test_pyelsa_ordered_subsets(cuda, oracle):
+    """SubsetSampler + SQS in ordered-subset mode (the reference's usage: subset projectors and
+    partitioned data as LeastSquares problems) against the C ABI run on the same subsets."""
+    import elsa_b200
+    elsa, vol, sino = _setup(oracle, 24, 30, 36)
+    A = elsa.JosephsMethodCUDA(vol, sino)
+    from elsa_b200 import phantoms
+    x = phantoms.modified_shepp_logan((24, 24, 24)).reshape(-1)
+    b = A.apply(elsa.DataContainer(cuda.from_numpy(x), vol))
+    sampler = elsa.SubsetSampler(vol, sino, 3, elsa.SubsetSampler.ROTATIONAL_CLUSTERING)
+    blocks = sampler.getPartitionedData(b)
+    projs = sampler.getSubsetProjectors(elsa.JosephsMethodCUDA)
+    subsets = [elsa.LeastSquares(p, d) for p, d in zip(projs, blocks)]
+    sol = elsa.SQS(elsa.LeastSquares(A, b), subsets).solve(4)
+    r0 = b.squaredL2Norm()
+    assert (A.apply(sol) - b).squaredL2Norm() < 0.2 * r0
+    # the same run through the C ABI
+    s = cuda.cuda.current_stream().cuda_stream
+    xd = cuda.zeros(A.native.domain_size, device="cuda")
+    sv = elsa_b200.Solver.sqs(A.native, b._ptr(), xd.data_ptr(),
+                              subsets=[(p.native, d._ptr()) for p, d in zip(projs, blocks)],
+                              stream=s)
+    sv.iterate(4, s)
+    cuda.cuda.synchronize()
+    assert np.array_equal(xd.cpu().numpy(), sol.tensor.cpu().numpy())
+    sv.close()
