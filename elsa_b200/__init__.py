@@ -16,7 +16,8 @@ from ._capi import (ElsaError, InvalidArgumentError, Projector, Solver,  # noqa:
                     KNOB_ADJOINT_CHUNKS, KNOB_ADJOINT_THREADS, tune_cache_size,
                     tune_cache_clear, tune_cache_save, tune_cache_load, tune_cache_put,
                     tune_cache_get, SOLVER_SQS, SUBSET_ROUND_ROBIN,
-                    SUBSET_ROTATIONAL_CLUSTERING, subset_split, gather_views)
+                    SUBSET_ROTATIONAL_CLUSTERING, subset_split, gather_views, edf_read,
+                    edf_write, mhd_read, mhd_write, pgm_write)
 
 __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "voxel_lut",
            "PROJECTOR_BLOB", "PROJECTOR_BSPLINE", "PROJECTOR_PHASE_CONTRAST_BLOB",
@@ -29,4 +30,5 @@ __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "voxel_lu
            "PROX_BOX", "PROX_L1", "KNOB_FORWARD_THREADS", "KNOB_ADJOINT_CHUNKS",
            "KNOB_ADJOINT_THREADS", "tune_cache_size", "tune_cache_clear", "tune_cache_save",
            "tune_cache_load", "tune_cache_put", "tune_cache_get", "SOLVER_SQS",
-           "SUBSET_ROUND_ROBIN", "SUBSET_ROTATIONAL_CLUSTERING", "subset_split", "gather_views"]
+           "SUBSET_ROUND_ROBIN", "SUBSET_ROTATIONAL_CLUSTERING", "subset_split", "gather_views",
+           "edf_read", "edf_write", "mhd_read", "mhd_write", "pgm_write"]

@@ -48,6 +48,16 @@ KNOB_ADJOINT_THREADS = 2
 KNOB_COUNT = 3
 KNOB_NAMES = ("forward_threads", "adjoint_chunks", "adjoint_threads")
 
+IO_MAX_DIMS = 8
+IO_TYPES = ("int8", "uint8", "int16", "uint16", "int32", "uint32", "float32", "float64")
+
+
+class ImageInfo(ctypes.Structure):
+    """elsa_image_info"""
+    _fields_ = [("ndim", ctypes.c_int32), ("data_type", ctypes.c_int32),
+                ("dims", ctypes.c_int64 * IO_MAX_DIMS), ("spacing", ctypes.c_float * IO_MAX_DIMS)]
+
+
 # Every function the header declares: name -> (restype, argtypes)
 _vp = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -92,6 +102,13 @@ SIGNATURES = {
     "elsa_sqs_create": (_st, [_vp, _vp, _vp, _vp, _i32, _vp, _i32, _i32, ctypes.c_double, _vp,
                               _vp, ctypes.POINTER(_vp)]),
     "elsa_subset_split": (_st, [_i32, _vp, _i32, _i32, _i32, _vp, _vp]),
+    "elsa_edf_info": (_st, [ctypes.c_char_p, ctypes.POINTER(ImageInfo)]),
+    "elsa_edf_read": (_st, [ctypes.c_char_p, _vp, _i64]),
+    "elsa_edf_write": (_st, [ctypes.c_char_p, _vp, _i32, _vp, _vp]),
+    "elsa_mhd_info": (_st, [ctypes.c_char_p, ctypes.POINTER(ImageInfo)]),
+    "elsa_mhd_read": (_st, [ctypes.c_char_p, _vp, _i64]),
+    "elsa_mhd_write": (_st, [ctypes.c_char_p, ctypes.c_char_p, _vp, _i32, _vp, _vp]),
+    "elsa_pgm_write": (_st, [ctypes.c_char_p, _vp, _i32, _vp]),
     "elsa_gather_views": (_st, [_vp, _i64, _vp, _i32, _i32, _vp, _vp]),
     "elsa_power_iterations": (_st, [_vp, _i32, _vp, ctypes.POINTER(ctypes.c_double)]),
     "elsa_solver_iterate": (_st, [_vp, _i32, _vp]),
@@ -307,6 +324,54 @@ def gather_views(sino_ptr, view_size, views, total_views, out_ptr, stream=None):
     call("elsa_gather_views", ctypes.c_void_p(sino_ptr), int(view_size),
          np_ptr(idx) if idx.size else None, int(idx.size), int(total_views),
          ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream or 0))
+
+
+def _image_read(fmt, path):
+    info = ImageInfo()
+    call("elsa_%s_info" % fmt, os.fsencode(path), ctypes.byref(info))
+    dims = [int(info.dims[i]) for i in range(info.ndim)]
+    spacing = [float(info.spacing[i]) for i in range(info.ndim)]
+    data = np.empty(int(np.prod(dims)), np.float32)
+    call("elsa_%s_read" % fmt, os.fsencode(path), np_ptr(data), int(data.size))
+    return data, dims, spacing, IO_TYPES[info.data_type]
+
+
+def edf_read(path):
+    """(flat float32 data x fastest, dims, spacing, stored type) of an EDF file."""
+    return _image_read("edf", path)
+
+
+def mhd_read(meta_path):
+    """(flat float32 data x fastest, dims, spacing, stored type) of an MHD meta + raw file."""
+    return _image_read("mhd", meta_path)
+
+
+def _shape_args(data, dims, spacing):
+    d = np.ascontiguousarray(dims, np.int64)
+    buf = np.ascontiguousarray(data, np.float32).reshape(-1)
+    if buf.size != int(np.prod(d)):
+        raise InvalidArgumentError(1, "image data does not match its dimensions")
+    sp = None if spacing is None else np.ascontiguousarray(spacing, np.float32)
+    if sp is not None and sp.size != d.size:
+        raise InvalidArgumentError(1, "one spacing per dimension")
+    return buf, d, sp
+
+
+def edf_write(path, data, dims, spacing=None):
+    buf, d, sp = _shape_args(data, dims, spacing)
+    call("elsa_edf_write", os.fsencode(path), np_ptr(buf), int(d.size), np_ptr(d),
+         np_ptr(sp) if sp is not None else None)
+
+
+def mhd_write(meta_path, raw_path, data, dims, spacing=None):
+    buf, d, sp = _shape_args(data, dims, spacing)
+    call("elsa_mhd_write", os.fsencode(meta_path), os.fsencode(raw_path), np_ptr(buf),
+         int(d.size), np_ptr(d), np_ptr(sp) if sp is not None else None)
+
+
+def pgm_write(path, data, dims):
+    buf, d, _ = _shape_args(data, dims, None)
+    call("elsa_pgm_write", os.fsencode(path), np_ptr(buf), int(d.size), np_ptr(d))
 
 
 def tune_cache_size():

@@ -44,9 +44,10 @@ CXX_UNITS = [
     ("luts.cpp", []),
     ("capi.cpp", []),
     ("tune.cpp", []),
+    ("io.cpp", []),
 ]
 HEADERS = ["internal.cuh", "raysetup.cuh", "joseph_tma.cuh", "projector.hpp", "geometry.hpp", "vecops.cuh",
-           "solvers.hpp", "luts.hpp", "voxel.hpp", "tune.hpp"]
+           "solvers.hpp", "luts.hpp", "voxel.hpp", "tune.hpp", "io.hpp"]
 
 
 def _stale(target, deps):

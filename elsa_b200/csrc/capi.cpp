@@ -11,6 +11,7 @@
 #include "../../include/elsa_b200.h"
 #include "geometry.hpp"
 #include "internal.cuh"
+#include "io.hpp"
 #include "projector.hpp"
 #include "solvers.hpp"
 #include "tune.hpp"
@@ -754,6 +755,99 @@ elsa_status elsa_solver_timing(elsa_solver* s, double* fwd, double* adj, int64_t
 elsa_status elsa_solver_destroy(elsa_solver* s)
 {
     return guarded([&] { delete s; });
+}
+
+} // extern "C"
+
+namespace
+{
+    void fillInfo(const elsa_b200::io::ImageInfo& in, elsa_image_info* out)
+    {
+        if (in.dims.size() > ELSA_IO_MAX_DIMS)
+            throw elsa_b200::Error(ELSA_ERROR_NOT_SUPPORTED, "image has too many dimensions");
+        std::memset(out, 0, sizeof(*out));
+        out->ndim = static_cast<int32_t>(in.dims.size());
+        out->data_type = static_cast<int32_t>(in.type);
+        for (size_t i = 0; i < in.dims.size(); ++i) {
+            out->dims[i] = in.dims[i];
+            out->spacing[i] = in.spacing[i];
+        }
+    }
+
+    std::vector<int64_t> shapeOf(int32_t ndim, const int64_t* dims, const char* who)
+    {
+        require(ndim >= 1 && ndim <= ELSA_IO_MAX_DIMS && dims != nullptr, who);
+        return std::vector<int64_t>(dims, dims + ndim);
+    }
+
+    std::vector<float> spacingOf(int32_t ndim, const float* spacing)
+    {
+        return spacing ? std::vector<float>(spacing, spacing + ndim)
+                       : std::vector<float>(static_cast<size_t>(ndim), 1.0f);
+    }
+} // namespace
+
+extern "C" {
+
+elsa_status elsa_edf_info(const char* path, elsa_image_info* info)
+{
+    return guarded([&] {
+        require(path && info, "elsa_edf_info: null argument");
+        fillInfo(elsa_b200::io::edfInfo(path), info);
+    });
+}
+
+elsa_status elsa_edf_read(const char* path, float* out, int64_t count)
+{
+    return guarded([&] {
+        require(path && (out || count == 0) && count >= 0, "elsa_edf_read: invalid argument");
+        elsa_b200::io::edfRead(path, out, count);
+    });
+}
+
+elsa_status elsa_edf_write(const char* path, const float* data, int32_t ndim, const int64_t* dims,
+                           const float* spacing)
+{
+    return guarded([&] {
+        require(path && data, "elsa_edf_write: null argument");
+        elsa_b200::io::edfWrite(path, data, shapeOf(ndim, dims, "elsa_edf_write: bad shape"),
+                                spacingOf(ndim, spacing));
+    });
+}
+
+elsa_status elsa_mhd_info(const char* metaPath, elsa_image_info* info)
+{
+    return guarded([&] {
+        require(metaPath && info, "elsa_mhd_info: null argument");
+        fillInfo(elsa_b200::io::mhdInfo(metaPath), info);
+    });
+}
+
+elsa_status elsa_mhd_read(const char* metaPath, float* out, int64_t count)
+{
+    return guarded([&] {
+        require(metaPath && (out || count == 0) && count >= 0, "elsa_mhd_read: invalid argument");
+        elsa_b200::io::mhdRead(metaPath, out, count);
+    });
+}
+
+elsa_status elsa_mhd_write(const char* metaPath, const char* rawPath, const float* data,
+                           int32_t ndim, const int64_t* dims, const float* spacing)
+{
+    return guarded([&] {
+        require(metaPath && rawPath && data, "elsa_mhd_write: null argument");
+        elsa_b200::io::mhdWrite(metaPath, rawPath, data,
+                                shapeOf(ndim, dims, "elsa_mhd_write: bad shape"),
+                                spacingOf(ndim, spacing));
+    });
+}
+
+elsa_status elsa_pgm_write(const char* path, const float* data, int32_t ndim, const int64_t* dims)
+{
+    return guarded([&] {
+        require(path && data, "elsa_pgm_write: null argument");
+        elsa_b200::io::pgmWrite(path, data, shapeOf(ndim, dims, "elsa_pgm_write: bad shape"));
+    });
 }
 
 } // extern "C"

@@ -556,6 +556,65 @@ class SubsetSampler:
         return [projectorClass(self._volume, d) for d in self._detectors]
 
 
+# ---- image files (io/, bindings in pyelsa/pyelsa/bind_io.cpp + hints/io_hints.cpp) ---------------
+
+def _host_flat(data):
+    dc = data if isinstance(data, DataContainer) else None
+    if dc is not None:
+        return dc.tensor.detach().cpu().numpy(), dc.descriptor
+    arr = np.asarray(data, np.float32)
+    return arr.reshape(-1, order="F"), DataDescriptor(arr.shape)
+
+
+def _to_container(flat, dims, spacing):
+    torch = _torch()
+    dc = DataContainer.__new__(DataContainer)
+    dc.tensor = torch.from_numpy(np.ascontiguousarray(flat, np.float32)).cuda()
+    dc.descriptor = VolumeDescriptor(dims, spacing)
+    return dc
+
+
+class EDF:
+    """EDF.readf(filename) -> DataContainer, EDF.write(data, filename) (io/EDFHandler.h)."""
+
+    @staticmethod
+    def readf(filename):
+        flat, dims, spacing, _ = _capi.edf_read(filename)
+        return _to_container(flat, dims, spacing)
+
+    @staticmethod
+    def write(data, filename):
+        flat, desc = _host_flat(data)
+        _capi.edf_write(filename, flat, desc.getNumberOfCoefficientsPerDimension(),
+                        desc.getSpacingPerDimension())
+
+
+class MHD:
+    """MHD.readf(filename) -> DataContainer, MHD.write(data, metaFilename, rawFilename)
+    (io/MHDHandler.h)."""
+
+    @staticmethod
+    def readf(filename):
+        flat, dims, spacing, _ = _capi.mhd_read(filename)
+        return _to_container(flat, dims, spacing)
+
+    @staticmethod
+    def write(data, metaFilename, rawFilename):
+        flat, desc = _host_flat(data)
+        _capi.mhd_write(metaFilename, rawFilename, flat,
+                        desc.getNumberOfCoefficientsPerDimension(),
+                        desc.getSpacingPerDimension())
+
+
+class PGM:
+    """PGM.write(data, filename) (io/PGMHandler.h)."""
+
+    @staticmethod
+    def write(data, filename):
+        flat, desc = _host_flat(data)
+        _capi.pgm_write(filename, flat, desc.getNumberOfCoefficientsPerDimension())
+
+
 CGNEf, CGLSf, Landweberf, APGDf = CGNE, CGLS, Landweber, APGD
 SIRTf, FGMf, OGMf, SQSf = SIRT, FGM, OGM, SQS
 

@@ -377,6 +377,54 @@ elsa_status elsa_solver_destroy(elsa_solver* solver);
 elsa_status elsa_cgne_solve(elsa_projector* projector, const float* b, float* x,
                             int32_t iterations, int32_t use_x0, void* stream);
 
+/* ---------------------------------------------------------------------------------------------
+ * Image files (io/EDFHandler, io/MHDHandler, io/PGMHandler). Host buffers of float; a caller
+ * copies them to or from device buffers. Headers are written byte for byte as the reference
+ * writes them; reading follows the reference's parse rules and rejects what it rejects
+ * (ELSA_ERROR_INVALID_ARGUMENT with the reference's message).
+ * ------------------------------------------------------------------------------------------- */
+
+#define ELSA_IO_MAX_DIMS 8
+
+/* Element types of the raw data, DataUtils::DataType (io/ioUtils.h:33-45). Readable: uint16,
+ * float32, float64 (converted to float); written: float32. */
+#define ELSA_IO_INT8 0
+#define ELSA_IO_UINT8 1
+#define ELSA_IO_INT16 2
+#define ELSA_IO_UINT16 3
+#define ELSA_IO_INT32 4
+#define ELSA_IO_UINT32 5
+#define ELSA_IO_FLOAT32 6
+#define ELSA_IO_FLOAT64 7
+
+typedef struct elsa_image_info {
+    int32_t ndim;      /* number of dimensions (<= ELSA_IO_MAX_DIMS) */
+    int32_t data_type; /* ELSA_IO_* of the stored data */
+    int64_t dims[ELSA_IO_MAX_DIMS];   /* coefficients per dimension, x first */
+    float spacing[ELSA_IO_MAX_DIMS];  /* spacing per dimension (1 when the file has none) */
+} elsa_image_info;
+
+/* Header of an EDF file (EDF::readHeader + parseHeader, io/EDFHandler.cpp:71-216). */
+elsa_status elsa_edf_info(const char* path, elsa_image_info* info);
+/* Its data, count = the product of the dimensions, converted to float (EDF::read,
+ * io/EDFHandler.cpp:9-41). */
+elsa_status elsa_edf_read(const char* path, float* out, int64_t count);
+/* EDF::write (io/EDFHandler.cpp:43-69,218-255) of float data; spacing may be NULL (ones). */
+elsa_status elsa_edf_write(const char* path, const float* data, int32_t ndim, const int64_t* dims,
+                           const float* spacing);
+
+/* MHD meta file + raw file (io/MHDHandler.cpp:9-66,68-194); the raw file named in the meta
+ * file is found relative to the meta file's directory. */
+elsa_status elsa_mhd_info(const char* meta_path, elsa_image_info* info);
+elsa_status elsa_mhd_read(const char* meta_path, float* out, int64_t count);
+elsa_status elsa_mhd_write(const char* meta_path, const char* raw_path, const float* data,
+                           int32_t ndim, const int64_t* dims, const float* spacing);
+
+/* PGM::write (io/PGMHandler.cpp:20-58): 2D data (or 3D with a last dimension of 1) as a P2
+ * grey-scale image scaled to [0, 255]. */
+elsa_status elsa_pgm_write(const char* path, const float* data, int32_t ndim,
+                           const int64_t* dims);
+
 #ifdef __cplusplus
 }
 #endif

@@ -175,3 +175,22 @@ def test_pyelsa_ordered_subsets(cuda, oracle):
     cuda.cuda.synchronize()
     assert np.array_equal(xd.cpu().numpy(), sol.tensor.cpu().numpy())
     sv.close()
+
+
+def test_pyelsa_image_files(cuda, oracle, tmp_path):
+    """EDF / MHD / PGM through pyelsa's names: a device DataContainer written and read back keeps
+    its values, sizes and spacing (io/tests/test_EDFHandler.cpp, test_MHDHandler.cpp)."""
+    import elsa_b200.pyelsa as elsa
+    vol = elsa.VolumeDescriptor([11, 17], [0.5, 2.0])
+    rng = np.random.default_rng(1)
+    arr = rng.standard_normal((11, 17)).astype(np.float32)
+    dc = elsa.DataContainer(arr, vol)
+    elsa.EDF.write(dc, str(tmp_path / "a.edf"))
+    back = elsa.EDF.readf(str(tmp_path / "a.edf"))
+    assert back.getDataDescriptor() == vol
+    assert np.array_equal(np.asarray(back), arr)
+    elsa.MHD.write(dc, str(tmp_path / "a.mhd"), str(tmp_path / "a.raw"))
+    back = elsa.MHD.readf(str(tmp_path / "a.mhd"))
+    assert back.getDataDescriptor() == vol and np.array_equal(np.asarray(back), arr)
+    elsa.PGM.write(dc, str(tmp_path / "a.pgm"))
+    assert open(tmp_path / "a.pgm").read().startswith("P2\n11 17\n255\n")
