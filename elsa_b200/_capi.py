@@ -27,6 +27,7 @@ PROJECTOR_BLOB = 2
 PROJECTOR_BSPLINE = 3
 PROJECTOR_PHASE_CONTRAST_BLOB = 4
 PROJECTOR_PHASE_CONTRAST_BSPLINE = 5
+PROJECTOR_BINARY = 6
 FOOTPRINT_REFERENCE = 0
 FOOTPRINT_RECTANGLE = 1
 SOLVER_CGNE = 0

@@ -224,6 +224,9 @@ elsa_status elsa_projector_create(int32_t kind, int32_t dim, const int64_t* volD
         case ELSA_PROJECTOR_SIDDON:
             handle->impl = elsa_b200::makeSiddonProjector(vol, det, pv);
             break;
+        case ELSA_PROJECTOR_BINARY:
+            handle->impl = elsa_b200::makeSiddonProjector(vol, det, pv, true);
+            break;
         case ELSA_PROJECTOR_BLOB:
         case ELSA_PROJECTOR_BSPLINE:
         case ELSA_PROJECTOR_PHASE_CONTRAST_BLOB:

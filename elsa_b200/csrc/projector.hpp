@@ -72,9 +72,11 @@ namespace elsa_b200
     std::unique_ptr<Projector> makeJosephProjector(const VolumeShape& vol,
                                                    const DetectorShape& det,
                                                    const std::vector<PoseRecord>& poses);
+    // binary: BinaryMethod, the Siddon visits with weight 1 (projectors/BinaryMethod.cpp)
     std::unique_ptr<Projector> makeSiddonProjector(const VolumeShape& vol,
                                                    const DetectorShape& det,
-                                                   const std::vector<PoseRecord>& poses);
+                                                   const std::vector<PoseRecord>& poses,
+                                                   bool binary = false);
 
     // Detector window of every (brick, view) for the brick-owner adjoints: the projection of the
     // brick grown by one voxel, plus one pixel (joseph.cu). Windows are indexed view * nBricks +

@@ -84,9 +84,10 @@ namespace elsa_b200
         template <int DIM>
         __global__ void __launch_bounds__(kMaxForwardThreads)
             siddonForwardKernel(const SiddonRay* __restrict__ rays, int64_t nrays,
-                                const float* __restrict__ x, VolumeShape vol,
+                                const float* __restrict__ x, VolumeShape vol, int binary,
                                 float* __restrict__ y)
         {
+            // binary: BinaryMethod (projectors/BinaryMethod.cpp:66-111), weight 1 per visit
             const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
             if (r >= nrays)
                 return;
@@ -124,7 +125,7 @@ namespace elsa_b200
                         static_cast<unsigned>(c0) < static_cast<unsigned>(nx) &&
                         static_cast<unsigned>(c1) < static_cast<unsigned>(ny) &&
                         (DIM < 3 || static_cast<unsigned>(c2) < static_cast<unsigned>(nz));
-                    const float w = __fsub_rn(tExit, tEntry);
+                    const float w = binary ? 1.0f : __fsub_rn(tExit, tEntry);
                     acc = __fadd_rn(acc, __fmul_rn(__ldg(x + idx), w));
                     if (!inside)
                         break;
@@ -291,7 +292,7 @@ namespace elsa_b200
         __device__ __forceinline__ void splatSegment(float* acc, float3 tDelta, int meta,
                                                      int kFirst, float4 cp, unsigned cpv, float yv,
                                                      int kLo, int org0, int org1, int org2,
-                                                     const VolumeShape& vol)
+                                                     const VolumeShape& vol, int binary)
         {
             using L = SiddonBrick<DIM>;
             const int dirG = ((meta >> (2 + G)) & 1) ? -1 : 1;
@@ -311,7 +312,7 @@ namespace elsa_b200
                                   static_cast<unsigned>(l1) < static_cast<unsigned>(kSlab) &&
                                   static_cast<unsigned>(l2) < static_cast<unsigned>(L::kBz);
                 float* adr = mine ? acc + l2 * L::kPlane + l1 * L::kRow + l0 : dummy;
-                const float w = __fsub_rn(tExit, tEntry);
+                const float w = binary ? 1.0f : __fsub_rn(tExit, tEntry);
                 *adr = __fadd_rn(*adr, __fmul_rn(yv, w));
                 if (m0) {
                     c0 += s0;
@@ -345,7 +346,7 @@ namespace elsa_b200
                                                    const unsigned* __restrict__ cpVoxel,
                                                    int64_t nrays, const float* __restrict__ y,
                                                    const DetectorShape& det, int org0, int org1,
-                                                   int org2, const VolumeShape& vol)
+                                                   int org2, const VolumeShape& vol, int binary)
         {
             const int kLo = G == 0 ? org0 : (G == 1 ? org1 : org2);
             const int kHi = kLo + kSlab - 1;
@@ -376,7 +377,7 @@ namespace elsa_b200
                                                       __int_as_float(q0.z));
                         splatSegment<DIM, G>(acc, td, meta, q1.x, __ldg(cpState + cpRow + r),
                                              __ldg(cpVoxel + cpRow + r), __ldg(y + r), kLo, org0,
-                                             org1, org2, vol);
+                                             org1, org2, vol, binary);
                     }
                     __syncwarp();
                 }
@@ -392,7 +393,7 @@ namespace elsa_b200
                                 const RayWindow* __restrict__ windows,
                                 const unsigned* __restrict__ viewAxes, VolumeShape vol,
                                 DetectorShape det, int m, int3 nBricks, int viewsPerChunk,
-                                float* __restrict__ x)
+                                int binary, float* __restrict__ x)
         {
             // blockIdx.y selects a chunk of views; with several chunks the brick goes to
             // x + chunk * nvox and launchSumChunks adds the chunks in order
@@ -416,13 +417,13 @@ namespace elsa_b200
                 const unsigned ax = viewAxes[p];
                 if (ax & 1u)
                     siddonView<DIM, 0>(acc, w, p, m, rays, cpState, cpVoxel, nrays, y, det, org0,
-                                       org1, org2, vol);
+                                       org1, org2, vol, binary);
                 if (ax & 2u)
                     siddonView<DIM, 1>(acc, w, p, m, rays, cpState, cpVoxel, nrays, y, det, org0,
-                                       org1, org2, vol);
+                                       org1, org2, vol, binary);
                 if (DIM == 3 && (ax & 4u))
                     siddonView<DIM, DIM == 3 ? 2 : 0>(acc, w, p, m, rays, cpState, cpVoxel, nrays,
-                                                      y, det, org0, org1, org2, vol);
+                                                      y, det, org0, org1, org2, vol, binary);
             }
             __syncwarp();
             const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
@@ -440,9 +441,10 @@ namespace elsa_b200
         class SiddonProjector final : public Projector
         {
         public:
+            // binary: BinaryMethod (kind 6), the same visits with weight 1
             SiddonProjector(const VolumeShape& vol, const DetectorShape& det,
-                            const std::vector<PoseRecord>& poses)
-                : Projector(1, vol, det, poses)
+                            const std::vector<PoseRecord>& poses, bool binary)
+                : Projector(binary ? 6 : 1, vol, det, poses), binary_(binary ? 1 : 0)
             {
                 const int maxDim = std::max(vol_.n[0], std::max(vol_.n[1], vol_.n[2]));
                 if (maxDim >= 65536)
@@ -516,10 +518,10 @@ namespace elsa_b200
                     static_cast<unsigned>((nrays + forwardThreads_ - 1) / forwardThreads_);
                 if (vol_.dim == 3)
                     siddonForwardKernel<3><<<blocks, forwardThreads_, 0, s>>>(
-                        rays_->as<SiddonRay>(), nrays, x, vol_, y);
+                        rays_->as<SiddonRay>(), nrays, x, vol_, binary_, y);
                 else
                     siddonForwardKernel<2><<<blocks, forwardThreads_, 0, s>>>(
-                        rays_->as<SiddonRay>(), nrays, x, vol_, y);
+                        rays_->as<SiddonRay>(), nrays, x, vol_, binary_, y);
                 ELSA_LAUNCH_CHECK("siddonForwardKernel");
             }
 
@@ -534,12 +536,12 @@ namespace elsa_b200
                     siddonAdjointKernel<3><<<grid, 32, 0, s>>>(
                         rays_->as<SiddonRay>(), cpState_->as<float4>(), cpVoxel_->as<unsigned>(),
                         rangeSize_, y, windows_->as<RayWindow>(), viewAxes_->as<unsigned>(), vol_,
-                        det_, classSpacing_, nBricks_, per, out);
+                        det_, classSpacing_, nBricks_, per, binary_, out);
                 else
                     siddonAdjointKernel<2><<<grid, 32, 0, s>>>(
                         rays_->as<SiddonRay>(), cpState_->as<float4>(), cpVoxel_->as<unsigned>(),
                         rangeSize_, y, windows_->as<RayWindow>(), viewAxes_->as<unsigned>(), vol_,
-                        det_, classSpacing_, nBricks_, per, out);
+                        det_, classSpacing_, nBricks_, per, binary_, out);
                 ELSA_LAUNCH_CHECK("siddonAdjointKernel");
                 if (used > 1)
                     launchSumChunks(partial_->as<float>(), used, domainSize_, x, s);
@@ -631,6 +633,7 @@ namespace elsa_b200
             std::unique_ptr<DeviceBuffer> partial_; // adjoint: per view-chunk partial volumes
             int adjointChunks_ = 1;
             int forwardThreads_ = kForwardThreads;
+            int binary_ = 0;
             std::unique_ptr<DeviceBuffer> rays_, cpState_, cpVoxel_, viewAxes_, windows_;
             int cpRows_ = 0;
             int classSpacing_ = 0;
@@ -641,8 +644,9 @@ namespace elsa_b200
 
     std::unique_ptr<Projector> makeSiddonProjector(const VolumeShape& vol,
                                                    const DetectorShape& det,
-                                                   const std::vector<PoseRecord>& poses)
+                                                   const std::vector<PoseRecord>& poses,
+                                                   bool binary)
     {
-        return std::make_unique<SiddonProjector>(vol, det, poses);
+        return std::make_unique<SiddonProjector>(vol, det, poses, binary);
     }
 } // namespace elsa_b200

@@ -276,6 +276,14 @@ class SiddonsMethodCUDA(LinearOperator):
         super().__init__(_capi.PROJECTOR_SIDDON, volumeDescriptor, detectorDescriptor)
 
 
+class BinaryMethod(LinearOperator):
+    """BinaryMethod(volume, detector) (projectors/BinaryMethod.h): the voxels a ray visits, each
+    with weight 1, on the device (the Siddon traversal kernels)."""
+
+    def __init__(self, volumeDescriptor, detectorDescriptor):
+        super().__init__(_capi.PROJECTOR_BINARY, volumeDescriptor, detectorDescriptor)
+
+
 class BlobVoxelProjectorCUDA(LinearOperator):
     def __init__(self, volumeDescriptor, detectorDescriptor, radius=2.0, alpha=10.83, order=2,
                  footprint=_capi.FOOTPRINT_REFERENCE):
@@ -308,6 +316,7 @@ class PhaseContrastBSplineVoxelProjectorCUDA(LinearOperator):
 # float instantiations resolve to the same device operators
 JosephsMethod = JosephsMethodCUDAf = JosephsMethodCUDA
 SiddonsMethod = SiddonsMethodCUDAf = SiddonsMethodCUDA
+BinaryMethodf = BinaryMethod
 BlobVoxelProjector = BlobVoxelProjectorCUDAf = BlobVoxelProjectorCUDA
 BSplineVoxelProjector = BSplineVoxelProjectorCUDAf = BSplineVoxelProjectorCUDA
 PhaseContrastBlobVoxelProjector = PhaseContrastBlobVoxelProjectorCUDA

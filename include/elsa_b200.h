@@ -57,7 +57,10 @@ typedef enum elsa_projector_kind {
     ELSA_PROJECTOR_PHASE_CONTRAST_BLOB = 4,
     /* PhaseContrastBSplineVoxelProjector(CUDA), projectors/PhaseContrastProjector.cpp:72-119.
      * params as ELSA_PROJECTOR_BSPLINE. */
-    ELSA_PROJECTOR_PHASE_CONTRAST_BSPLINE = 5
+    ELSA_PROJECTOR_PHASE_CONTRAST_BSPLINE = 5,
+    /* BinaryMethod, projectors/BinaryMethod.cpp:66-111: the voxels TraverseAABB visits, each
+     * with weight 1 (elsa has it on the CPU only). */
+    ELSA_PROJECTOR_BINARY = 6
 } elsa_projector_kind;
 
 /* Footprint mode of the voxel projectors (last parameter): 0 visits the pixels of each voxel

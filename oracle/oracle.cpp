@@ -651,11 +651,12 @@ namespace orc
     // ------------------------------------------------------------------------------------------
     // Siddon: projectors/TraverseAABB.cpp:6-184 + SiddonsMethod.cpp:76-124
     // ------------------------------------------------------------------------------------------
-    // visits (optional): per-ray number of visited voxels
+    // visits (optional): per-ray number of visited voxels. binary: BinaryMethod
+    // (projectors/BinaryMethod.cpp:66-111), the same TraverseAABB visits with weight 1.
     template <typename data_t, bool adjoint>
     static void siddonTraverse(int dim, const index_t* volDims, const index_t* detDims,
                                index_t numPoses, const float* poseData, const data_t* in,
-                               data_t* out, index_t* visits = nullptr)
+                               data_t* out, index_t* visits = nullptr, bool binary = false)
     {
         std::vector<PoseView> poses(numPoses);
         for (index_t p = 0; p < numPoses; ++p)
@@ -737,7 +738,15 @@ namespace orc
                         const float weight = tExit - tEntry;
                         if (visits)
                             ++visits[ir];
-                        if (adjoint) {
+                        if (binary) {
+                            if (adjoint) {
+                                const data_t v = in[ir];
+#pragma omp atomic
+                                out[idx] += v;
+                            } else {
+                                acc += in[idx];
+                            }
+                        } else if (adjoint) {
                             const data_t v = in[ir] * static_cast<data_t>(weight);
 #pragma omp atomic
                             out[idx] += v;
@@ -947,6 +956,29 @@ void oracle_siddon_f64(int adjoint, int dim, const int64_t* volDims, const int64
         orc::siddonTraverse<double, true>(dim, volDims, detDims, np, poses, in, out);
     else
         orc::siddonTraverse<double, false>(dim, volDims, detDims, np, poses, in, out);
+}
+
+void oracle_binary_f32(int adjoint, int dim, const int64_t* volDims, const int64_t* detDims,
+                       const float* poses, const float* in, float* out)
+{
+    const int64_t np = detDims[dim - 1];
+    if (adjoint)
+        orc::siddonTraverse<float, true>(dim, volDims, detDims, np, poses, in, out, nullptr, true);
+    else
+        orc::siddonTraverse<float, false>(dim, volDims, detDims, np, poses, in, out, nullptr,
+                                          true);
+}
+
+void oracle_binary_f64(int adjoint, int dim, const int64_t* volDims, const int64_t* detDims,
+                       const float* poses, const double* in, double* out)
+{
+    const int64_t np = detDims[dim - 1];
+    if (adjoint)
+        orc::siddonTraverse<double, true>(dim, volDims, detDims, np, poses, in, out, nullptr,
+                                          true);
+    else
+        orc::siddonTraverse<double, false>(dim, volDims, detDims, np, poses, in, out, nullptr,
+                                           true);
 }
 
 // Number of Joseph samples (sum over rays of numSteps) and Siddon voxel crossings, used for the

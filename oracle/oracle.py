@@ -63,6 +63,8 @@ def lib():
             fn.argtypes = [c_int, c_int, _i64p, _i64p, _f32p, fp, fp, c_int]
             fn = getattr(L, "oracle_siddon_" + name)
             fn.argtypes = [c_int, c_int, _i64p, _i64p, _f32p, fp, fp]
+            fn = getattr(L, "oracle_binary_" + name)
+            fn.argtypes = [c_int, c_int, _i64p, _i64p, _f32p, fp, fp]
         L.oracle_joseph_sample_count.argtypes = [c_int, _i64p, _i64p, _f32p]
         L.oracle_joseph_sample_count.restype = c_i64
         L.oracle_siddon_visit_count.argtypes = [c_int, _i64p, _i64p, _f32p]
@@ -196,6 +198,16 @@ def siddon(x, vol_dims, det_dims, poses, dtype=np.float32):
 
 def siddon_adjoint(y, vol_dims, det_dims, poses, dtype=np.float32):
     return _call_projector("siddon", True, vol_dims, det_dims, poses, y, dtype)
+
+
+def binary(x, vol_dims, det_dims, poses, dtype=np.float32):
+    """BinaryMethod forward projection (projectors/BinaryMethod.cpp:66-111): the sum of the voxels
+    that TraverseAABB visits."""
+    return _call_projector("binary", False, vol_dims, det_dims, poses, x, dtype)
+
+
+def binary_adjoint(y, vol_dims, det_dims, poses, dtype=np.float32):
+    return _call_projector("binary", True, vol_dims, det_dims, poses, y, dtype)
 
 
 def joseph_sample_count(vol_dims, det_dims, poses):

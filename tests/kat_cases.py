@@ -126,6 +126,37 @@ def siddon_cases(O):
     return cases
 
 
+def binary_cases(O):
+    """projectors/tests/test_BinaryMethod.cpp: one ray through a 5x5 volume of ones (source to
+    centre 100, centre to detector 5) at several angles; y = A x and bp = A^T y = A^T A x."""
+    cases = []
+    ones = np.ones((5, 5), np.float32)
+    column = np.zeros((5, 5), np.float32)
+    column[:, 2] = 5
+    row = np.zeros((5, 5), np.float32)
+    row[2, :] = 5
+    # :25-240 (cmp vectors in DataContainer order, x fastest)
+    diag45 = np.array([9, 0, 0, 0, 0, 9, 9, 0, 0, 0, 0, 9, 9, 0, 0, 0, 0, 9, 9, 0, 0, 0, 0, 9, 9],
+                      np.float32).reshape(5, 5)
+    diag225 = np.array([9, 9, 0, 0, 0, 0, 9, 9, 0, 0, 0, 0, 9, 9, 0, 0, 0, 0, 9, 9, 0, 0, 0, 0,
+                        9], np.float32).reshape(5, 5)
+    for name, angle, y, bp in (("0deg", 0.0, 5.0, column), ("180deg", _rad(180), 5.0, column),
+                               ("90deg", _rad(90), 5.0, row), ("270deg", _rad(270), 5.0, row),
+                               ("45deg", _rad(45), 9.0, diag45),
+                               ("225deg", _rad(225), 9.0, diag225)):
+        poses = _pose2d(O, (5, 5), 1, 100.0, 5.0, angle)[None]
+        cases.append(dict(name="binary_" + name, vol=(5, 5), det=(1, 1), poses=poses, x=ones,
+                          y_expect=np.array([y]), y=np.array([y]), bp_expect=bp))
+    # :242-325 one ray, four angles
+    poses = np.stack([_pose2d(O, (5, 5), 1, 100.0, 5.0, a)
+                      for a in (_rad(0), _rad(90), _rad(180), _rad(270))])
+    cross = np.array([0, 0, 10, 0, 0, 0, 0, 10, 0, 0, 10, 10, 20, 10, 10, 0, 0, 10, 0, 0, 0, 0,
+                      10, 0, 0], np.float32).reshape(5, 5)
+    cases.append(dict(name="binary_4angles", vol=(5, 5), det=(1, 4), poses=poses, x=ones,
+                      y_expect=np.full(4, 5.0), y=np.full(4, 5.0), bp_expect=cross))
+    return cases
+
+
 def voxel_cases(O):
     """projectors/tests/test_BlobVoxelProjector.cpp:25-244: a centre voxel set to 1, projected
     onto one, two or three detector pixels. Expected values are blob LUT weights at the stated

@@ -3,7 +3,7 @@ import numpy as np
 import pytest
 
 from conftest import rel_l2
-from kat_cases import joseph_cases, siddon_cases
+from kat_cases import binary_cases, joseph_cases, siddon_cases
 
 
 def _run(O, fn, case, dtype):
@@ -47,6 +47,23 @@ def test_siddon_kat(oracle, dtype):
         y, bp = _run(oracle, _Siddon(oracle), case, dtype)
         np.testing.assert_allclose(y, case["y_expect"], rtol=1e-5, err_msg=case["name"])
         assert rel_l2(bp, case["bp_expect"]) <= 1e-5, case["name"]
+
+
+class _Binary(_Joseph):
+    def __call__(self, x, vol, det, poses, dtype):
+        return self.O.binary(x, vol, det, poses, dtype=dtype)
+
+    def adjoint(self, y, vol, det, poses, dtype):
+        return self.O.binary_adjoint(y, vol, det, poses, dtype=dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_binary_kat(oracle, dtype):
+    for case in binary_cases(oracle):
+        y, bp = _run(oracle, _Binary(oracle), case, dtype)
+        np.testing.assert_array_equal(y, case["y_expect"], err_msg=case["name"])
+        np.testing.assert_array_equal(bp.reshape(case["bp_expect"].shape), case["bp_expect"],
+                                      err_msg=case["name"])
 
 
 def test_joseph_outputs_overwritten(oracle):

@@ -115,3 +115,40 @@ def test_siddon_cgls(cuda, oracle):
     torch.cuda.synchronize()
     xr, _ = S.cgls(A, At, b_np, x_true.size, 8)
     assert rel_l2(x.cpu().numpy(), xr) <= 1e-4
+
+
+def test_binary_kats_gpu(cuda, oracle):
+    """BinaryMethod (the Siddon kernels with weight 1) against test_BinaryMethod.cpp's cases:
+    exact, both directions."""
+    import elsa_b200
+    from kat_cases import binary_cases
+    for case in binary_cases(oracle):
+        proj = elsa_b200.Projector(elsa_b200.PROJECTOR_BINARY, case["vol"], case["det"],
+                                   case["poses"])
+        y, bp = _gpu_pair(cuda, proj, case["x"], case["y"])
+        np.testing.assert_array_equal(y, case["y_expect"], err_msg=case["name"])
+        np.testing.assert_array_equal(bp.reshape(case["bp_expect"].shape), case["bp_expect"],
+                                      err_msg=case["name"])
+
+
+@pytest.mark.parametrize("name", sorted(CONFIGS))
+def test_binary_parity(cuda, oracle, name):
+    """Forward bit-identical to the oracle (same visits and float sums), adjoint within 1e-5
+    (the oracle adds with atomics in varying order)."""
+    import elsa_b200
+    c = CONFIGS[name]
+    poses, det = oracle.circle_trajectory(c["vol"], c["views"], c.get("arc", 360), c["s2c"],
+                                          c["c2d"], c["det"])
+    proj = elsa_b200.Projector(elsa_b200.PROJECTOR_BINARY, c["vol"], det, poses)
+    rng = np.random.default_rng(21)
+    x = rng.uniform(0, 1, int(np.prod(c["vol"]))).astype(np.float32)
+    y = rng.uniform(0, 1, int(np.prod(det))).astype(np.float32)
+    Ax, Aty = _gpu_pair(cuda, proj, x, y)
+    ref_Ax = np.asarray(oracle.binary(x, c["vol"], det, poses), np.float32).ravel()
+    ref_Aty = oracle.binary_adjoint(y, c["vol"], det, poses)
+    assert np.array_equal(Ax.view(np.uint32), ref_Ax.view(np.uint32))
+    assert rel_l2(Aty, ref_Aty) <= PARITY
+    # adjointness <A x, y> = <x, A^T y>
+    lhs = float(np.dot(Ax.astype(np.float64), y))
+    rhs = float(np.dot(x.astype(np.float64), Aty))
+    assert abs(lhs - rhs) <= 1e-5 * abs(lhs)
