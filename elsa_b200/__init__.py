@@ -17,7 +17,8 @@ from ._capi import (ElsaError, InvalidArgumentError, Projector, Solver,  # noqa:
                     tune_cache_clear, tune_cache_save, tune_cache_load, tune_cache_put,
                     tune_cache_get, SOLVER_SQS, SUBSET_ROUND_ROBIN,
                     SUBSET_ROTATIONAL_CLUSTERING, subset_split, gather_views, edf_read,
-                    edf_write, mhd_read, mhd_write, pgm_write, PROJECTOR_BINARY)
+                    edf_write, mhd_read, mhd_write, pgm_write, PROJECTOR_BINARY,
+                    curved_detector_coords)
 
 __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "voxel_lut",
            "PROJECTOR_BLOB", "PROJECTOR_BSPLINE", "PROJECTOR_PHASE_CONTRAST_BLOB",
@@ -31,4 +32,5 @@ __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "voxel_lu
            "KNOB_ADJOINT_THREADS", "tune_cache_size", "tune_cache_clear", "tune_cache_save",
            "tune_cache_load", "tune_cache_put", "tune_cache_get", "SOLVER_SQS",
            "SUBSET_ROUND_ROBIN", "SUBSET_ROTATIONAL_CLUSTERING", "subset_split", "gather_views",
-           "edf_read", "edf_write", "mhd_read", "mhd_write", "pgm_write", "PROJECTOR_BINARY"]
+           "edf_read", "edf_write", "mhd_read", "mhd_write", "pgm_write", "PROJECTOR_BINARY",
+           "curved_detector_coords"]

@@ -74,6 +74,9 @@ SIGNATURES = {
                                      _vp]),
     "elsa_projector_create": (_st, [_i32, _i32, _vp, _vp, _vp, _vp, _i32,
                                     ctypes.POINTER(_vp)]),
+    "elsa_projector_create_curved": (_st, [_i32, _i32, _vp, _vp, _vp, _vp, _i32, _f32, _f32,
+                                           ctypes.POINTER(_vp)]),
+    "elsa_curved_detector_coords": (_st, [_i32, _i32, _i32, _f32, _f32, _vp]),
     "elsa_projector_destroy": (_st, [_vp]),
     "elsa_projector_sizes": (_st, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "elsa_projector_info": (_st, [_vp, _i32, ctypes.POINTER(_i64)]),
@@ -211,7 +214,9 @@ def pose_3d(s2c, c2d, vol_spacing, vol_origin, sino_spacing, sino_origin, gamma,
 class Projector:
     """Owning handle of an elsa_projector (device-side operator)."""
 
-    def __init__(self, kind, vol_dims, det_dims, poses, params=None):
+    def __init__(self, kind, vol_dims, det_dims, poses, params=None, curved=None):
+        """curved: (opening angle in radian, source-to-detector distance) of a curved detector,
+        None for a flat one."""
         self.dim = len(vol_dims)
         self.vol_dims = tuple(int(v) for v in vol_dims)
         self.det_dims = tuple(int(v) for v in det_dims)
@@ -222,8 +227,14 @@ class Projector:
             raise InvalidArgumentError(1, "pose array does not match the number of poses")
         prm = np.ascontiguousarray(params if params is not None else [], np.float32)
         h = ctypes.c_void_p()
-        call("elsa_projector_create", int(kind), self.dim, np_ptr(vd), np_ptr(dd), np_ptr(ps),
-             np_ptr(prm) if prm.size else None, int(prm.size), ctypes.byref(h))
+        self.curved = None if curved is None else (float(curved[0]), float(curved[1]))
+        if self.curved is None:
+            call("elsa_projector_create", int(kind), self.dim, np_ptr(vd), np_ptr(dd),
+                 np_ptr(ps), np_ptr(prm) if prm.size else None, int(prm.size), ctypes.byref(h))
+        else:
+            call("elsa_projector_create_curved", int(kind), self.dim, np_ptr(vd), np_ptr(dd),
+                 np_ptr(ps), np_ptr(prm) if prm.size else None, int(prm.size),
+                 self.curved[0], self.curved[1], ctypes.byref(h))
         self._h = h
         d = ctypes.c_int64()
         r = ctypes.c_int64()
@@ -301,6 +312,15 @@ class Projector:
             self.close()
         except Exception:
             pass
+
+
+def curved_detector_coords(dim, nu, nv, angle, s2d):
+    """Planar (u', v') of every pixel centre of a curved detector, shape (nv, nu, 2)."""
+    h = int(nv) if dim == 3 else 1
+    out = np.zeros(2 * int(nu) * h, np.float32)
+    call("elsa_curved_detector_coords", int(dim), int(nu), h, float(angle), float(s2d),
+         np_ptr(out))
+    return out.reshape(h, int(nu), 2)
 
 
 def subset_split(dim, poses, num_subsets, strategy=SUBSET_ROUND_ROBIN):

@@ -190,9 +190,10 @@ elsa_status elsa_circle_trajectory(int32_t dim, const int64_t* volDims, const fl
     });
 }
 
-elsa_status elsa_projector_create(int32_t kind, int32_t dim, const int64_t* volDims,
-                                  const int64_t* detDims, const float* poses, const float* params,
-                                  int32_t numParams, elsa_projector** out)
+static elsa_status projectorCreate(int32_t kind, int32_t dim, const int64_t* volDims,
+                                   const int64_t* detDims, const float* poses, const float* params,
+                                   int32_t numParams, const elsa_b200::CurvedDetector& curved,
+                                   elsa_projector** out)
 {
     return guarded([&] {
         require(out != nullptr, "elsa_projector_create: null output handle");
@@ -219,18 +220,21 @@ elsa_status elsa_projector_create(int32_t kind, int32_t dim, const int64_t* volD
         auto handle = std::make_unique<elsa_projector>();
         switch (kind) {
         case ELSA_PROJECTOR_JOSEPH:
-            handle->impl = elsa_b200::makeJosephProjector(vol, det, pv);
+            handle->impl = elsa_b200::makeJosephProjector(vol, det, pv, curved);
             break;
         case ELSA_PROJECTOR_SIDDON:
-            handle->impl = elsa_b200::makeSiddonProjector(vol, det, pv);
+            handle->impl = elsa_b200::makeSiddonProjector(vol, det, pv, false, curved);
             break;
         case ELSA_PROJECTOR_BINARY:
-            handle->impl = elsa_b200::makeSiddonProjector(vol, det, pv, true);
+            handle->impl = elsa_b200::makeSiddonProjector(vol, det, pv, true, curved);
             break;
         case ELSA_PROJECTOR_BLOB:
         case ELSA_PROJECTOR_BSPLINE:
         case ELSA_PROJECTOR_PHASE_CONTRAST_BLOB:
         case ELSA_PROJECTOR_PHASE_CONTRAST_BSPLINE: {
+            if (curved.enabled())
+                throw elsa_b200::Error(ELSA_ERROR_NOT_SUPPORTED,
+                                       "voxel projectors need a planar detector");
             const VoxelSpec spec = voxelSpec(kind, dim, params, numParams);
             handle->impl = elsa_b200::makeVoxelProjector(kind, vol, det, pv, spec.lut,
                                                          spec.phase, spec.mode);
@@ -240,6 +244,47 @@ elsa_status elsa_projector_create(int32_t kind, int32_t dim, const int64_t* volD
             throw elsa_b200::Error(ELSA_ERROR_NOT_SUPPORTED, "unknown projector kind");
         }
         *out = handle.release();
+    });
+}
+
+elsa_status elsa_projector_create(int32_t kind, int32_t dim, const int64_t* volDims,
+                                  const int64_t* detDims, const float* poses, const float* params,
+                                  int32_t numParams, elsa_projector** out)
+{
+    return projectorCreate(kind, dim, volDims, detDims, poses, params, numParams, {}, out);
+}
+
+elsa_status elsa_projector_create_curved(int32_t kind, int32_t dim, const int64_t* volDims,
+                                         const int64_t* detDims, const float* poses,
+                                         const float* params, int32_t numParams, float angle,
+                                         float s2d, elsa_projector** out)
+{
+    if (!(angle > 0.0f) || !(s2d > 0.0f)) {
+        gLastError = "CurvedDetectorDescriptor: angle and source-to-detector distance must be "
+                     "positive";
+        if (out)
+            *out = nullptr;
+        return ELSA_ERROR_INVALID_ARGUMENT;
+    }
+    elsa_b200::CurvedDetector c;
+    c.angle = angle;
+    c.s2d = s2d;
+    return projectorCreate(kind, dim, volDims, detDims, poses, params, numParams, c, out);
+}
+
+elsa_status elsa_curved_detector_coords(int32_t dim, int32_t nu, int32_t nv, float angle,
+                                        float s2d, float* out)
+{
+    return guarded([&] {
+        require(out != nullptr, "elsa_curved_detector_coords: null output");
+        require(dim == 2 || dim == 3, "elsa_curved_detector_coords: dim must be 2 or 3");
+        require(nu > 0 && (dim == 2 || nv > 0), "elsa_curved_detector_coords: empty detector");
+        require(angle > 0.0f && s2d > 0.0f,
+                "CurvedDetectorDescriptor: angle and source-to-detector distance must be "
+                "positive");
+        const std::vector<float> xy =
+            elsa_b200::curvedPlanarCoords(dim, nu, dim == 3 ? nv : 1, angle, s2d);
+        std::memcpy(out, xy.data(), sizeof(float) * xy.size());
     });
 }
 

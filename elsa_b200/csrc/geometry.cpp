@@ -402,4 +402,38 @@ namespace elsa_b200
         });
         return splitRoundRobin(idx, nSubsets);
     }
+
+    std::vector<float> curvedPlanarCoords(int dim, int nu, int nv, float angle, float s2d,
+                                          std::vector<float>* columnFactor)
+    {
+        if (columnFactor)
+            columnFactor->assign(static_cast<size_t>(nu), 1.0f);
+        const int height = dim == 3 ? nv : 1;
+        const float radius = static_cast<float>(nu) / angle;
+        const float angleDelta = angle / static_cast<float>(nu);
+        const float cx = static_cast<float>(nu) / 2.0f;
+        const float cy = static_cast<float>(height) / 2.0f;
+        const float circleX = cx, circleY = s2d - radius;
+        std::vector<float> out(static_cast<size_t>(nu) * height * 2, 0.0f);
+        for (int h = 0; h < height; ++h)
+            for (int l = 0; l < nu; ++l) {
+                const float c0 = static_cast<float>(l) + 0.5f;
+                const float c1 = static_cast<float>(h) + 0.5f;
+                const float rayAngle = (c0 - cx) * angleDelta;
+                // sin / cos of the float angle evaluated in double, as the unqualified calls on
+                // a float argument in the reference resolve
+                const float dx = static_cast<float>(std::sin(static_cast<double>(rayAngle))) *
+                                 radius;
+                const float dd = static_cast<float>(std::cos(static_cast<double>(rayAngle))) *
+                                 radius;
+                const float px = circleX + dx, py = circleY + dd;
+                const float factor = py == 0.0f ? 1.0f : s2d / py;
+                if (columnFactor)
+                    (*columnFactor)[static_cast<size_t>(l)] = factor;
+                const size_t i = (static_cast<size_t>(h) * nu + l) * 2;
+                out[i] = (px - cx) * factor + cx;
+                out[i + 1] = dim == 3 ? (c1 - cy) * factor + cy : 0.0f;
+            }
+        return out;
+    }
 } // namespace elsa_b200

@@ -57,4 +57,15 @@ namespace elsa_b200
     std::vector<std::vector<int>> splitRotationalClustering(int dim,
                                                             const std::vector<PoseRecord>& poses,
                                                             int nSubsets);
+
+    // Planar detector coordinates of the pixel centres of a curved (cylindrical) detector,
+    // CurvedDetectorDescriptor::setup / mapCurvedCoordToPlanarCoord
+    // (core/Descriptors/CurvedDetectorDescriptor.cpp:33-91): radius nu / angle, the circle centred
+    // s2d - radius in front of the source; every pixel centre on the arc is projected from the
+    // source onto the flat detector at distance s2d. Two floats (u', v') per pixel, u fastest
+    // (2D: v' = 0). A ray-driven projector casts the ray of pixel (u, v) through (u', v') instead
+    // of (u + 0.5, v + 0.5).
+    // columnFactor (optional): per column u the factor s2d / depth that stretches its rows.
+    std::vector<float> curvedPlanarCoords(int dim, int nu, int nv, float angle, float s2d,
+                                          std::vector<float>* columnFactor = nullptr);
 } // namespace elsa_b200

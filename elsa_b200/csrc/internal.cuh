@@ -56,6 +56,13 @@ namespace elsa_b200
         int crossings;   // number of voxels visited
     };
 
+    // Curved detector as the brick-window kernel sees it: planar coordinate of the ray of every
+    // detector column (ascending, null for a flat detector) and the range of the row stretch.
+    struct CurvedMap {
+        const float* planarU = nullptr;
+        float fmin = 1.0f, fmax = 1.0f;
+    };
+
     // Per (brick, view) detector window of the rays that can touch the brick, inclusive.
     struct __align__(16) RayWindow {
         int u0, u1, v0, v1; // empty when u0 > u1

@@ -138,9 +138,24 @@ namespace elsa_b200
         // Detector window of every (brick, view): projection of the brick grown by one voxel,
         // plus one pixel of margin. Falls back to the whole detector when a corner lies behind
         // the source.
+        // Number of entries of the ascending table t[0..n) that are < x (le: <= x).
+        __device__ __forceinline__ int countBelow(const float* __restrict__ t, int n, float x,
+                                                  bool le)
+        {
+            int lo = 0, hi = n;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (le ? (t[mid] <= x) : (t[mid] < x))
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            return lo;
+        }
+
         __global__ void josephWindowKernel(const float* __restrict__ poses, VolumeShape vol,
                                            DetectorShape det, int3 brick, int3 nBricks,
-                                           RayWindow* __restrict__ out)
+                                           CurvedMap cm, RayWindow* __restrict__ out)
         {
             const int nb = nBricks.x * nBricks.y * nBricks.z;
             const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -190,6 +205,25 @@ namespace elsa_b200
             RayWindow w;
             if (behind) {
                 w.u0 = 0, w.u1 = det.nu - 1, w.v0 = 0, w.v1 = det.nv - 1;
+            } else if (cm.planarU) {
+                // curved detector: the rays of pixel column u pass planar coordinate
+                // planarU[u] (ascending), and rows are stretched by a factor in [fmin, fmax]
+                // about the detector's centre row
+                const int below = countBelow(cm.planarU, det.nu, umin, true);
+                const int before = countBelow(cm.planarU, det.nu, umax, false);
+                w.u0 = max(0, below - 2);
+                w.u1 = min(det.nu - 1, before + 1);
+                if (vol.dim == 3) {
+                    const float cy = 0.5f * static_cast<float>(det.nv);
+                    const float lo = cy + fminf((vmin - cy) / cm.fmin, (vmin - cy) / cm.fmax);
+                    const float hi = cy + fmaxf((vmax - cy) / cm.fmin, (vmax - cy) / cm.fmax);
+                    const float vLo = fmaxf(floorf(lo - 0.5f) - 1.0f, -1.0f);
+                    const float vHi = fminf(ceilf(hi - 0.5f) + 1.0f, static_cast<float>(det.nv));
+                    w.v0 = max(0, static_cast<int>(vLo));
+                    w.v1 = min(det.nv - 1, static_cast<int>(vHi));
+                } else {
+                    w.v0 = 0, w.v1 = 0;
+                }
             } else {
                 // pixel i has its centre at i + 0.5
                 const float uLo = fmaxf(floorf(umin - 0.5f) - 1.0f, -1.0f);
@@ -939,14 +973,15 @@ namespace elsa_b200
         {
         public:
             JosephProjector(const VolumeShape& vol, const DetectorShape& det,
-                            const std::vector<PoseRecord>& poses)
-                : Projector(0, vol, det, poses)
+                            const std::vector<PoseRecord>& poses, const CurvedDetector& curved)
+                : Projector(0, vol, det, poses), curved_(vol.dim, det, curved)
             {
                 const int64_t nrays = rangeSize_;
                 ELSA_CUDA(cudaMalloc(&dRays_, sizeof(JosephRay) * nrays));
                 const int threads = 256;
                 const unsigned blocks = static_cast<unsigned>((nrays + threads - 1) / threads);
-                josephSetupKernel<<<blocks, threads>>>(dPoses_, vol_, det_, dRays_);
+                josephSetupKernel<<<blocks, threads>>>(dPoses_, vol_, det_, curved_.planar(),
+                                                       dRays_);
                 ELSA_LAUNCH_CHECK("josephSetupKernel");
 
                 // per-view axis masks, then (at +np) the bad-spacing mask and a 64-bit counter
@@ -1001,7 +1036,7 @@ namespace elsa_b200
                     static_cast<int64_t>(nBricks_.x) * nBricks_.y * nBricks_.z * det_.np;
                 ELSA_CUDA(cudaMalloc(&dWindows_, sizeof(RayWindow) * nwin));
                 josephWindowKernel<<<static_cast<unsigned>((nwin + 255) / 256), 256>>>(
-                    dPoses_, vol_, det_, brick_, nBricks_, dWindows_);
+                    dPoses_, vol_, det_, brick_, nBricks_, curved_.map(), dWindows_);
                 ELSA_LAUNCH_CHECK("josephWindowKernel");
                 setKnob(kKnobAdjointChunks, defaultChunks());
                 if (vol_.dim == 3) {
@@ -1010,6 +1045,7 @@ namespace elsa_b200
                     tma_ = std::make_unique<JosephForwardTma>(vol_, det_, hp, dRays_);
                 }
                 ELSA_CUDA(cudaDeviceSynchronize());
+                curved_.release(); // rays and windows are built
             }
 
             // Per view and driving axis g: set bit 4+g of the view's axis word when neighbouring
@@ -1172,6 +1208,7 @@ namespace elsa_b200
             int classSpacing_ = 0;
             int64_t sampleCount_ = 0;
             std::unique_ptr<JosephForwardTma> tma_;
+            CurvedTables curved_; // curved detector coordinates while the rays are set up
             std::unique_ptr<DeviceBuffer> partial_; // adjoint: per view-chunk partial volumes
             int adjointChunks_ = 1;                 // view chunks of the adjoint
             int forwardThreads_ = kForwardThreads;  // rays per block of the gather forward
@@ -1194,13 +1231,14 @@ namespace elsa_b200
     } // namespace
 
     void launchBrickWindows(const float* poses, const VolumeShape& vol, const DetectorShape& det,
-                            int3 brick, int3 nBricks, RayWindow* out, cudaStream_t s)
+                            int3 brick, int3 nBricks, RayWindow* out, cudaStream_t s,
+                            CurvedMap cm)
     {
         const int64_t nwin = static_cast<int64_t>(nBricks.x) * nBricks.y * nBricks.z * det.np;
         if (nwin == 0)
             return;
         josephWindowKernel<<<static_cast<unsigned>((nwin + 255) / 256), 256, 0, s>>>(
-            poses, vol, det, brick, nBricks, out);
+            poses, vol, det, brick, nBricks, cm, out);
         ELSA_LAUNCH_CHECK("josephWindowKernel");
     }
 
@@ -1216,8 +1254,9 @@ namespace elsa_b200
 
     std::unique_ptr<Projector> makeJosephProjector(const VolumeShape& vol,
                                                    const DetectorShape& det,
-                                                   const std::vector<PoseRecord>& poses)
+                                                   const std::vector<PoseRecord>& poses,
+                                                   const CurvedDetector& curved)
     {
-        return std::make_unique<JosephProjector>(vol, det, poses);
+        return std::make_unique<JosephProjector>(vol, det, poses, curved);
     }
 } // namespace elsa_b200

@@ -28,6 +28,36 @@ namespace elsa_b200
         kKnobCount = 3
     };
 
+    // A curved (cylindrical) detector: opening angle (radian) and source-to-detector distance
+    // (CurvedDetectorDescriptor); angle 0 is a flat detector.
+    struct CurvedDetector {
+        float angle = 0.0f;
+        float s2d = 0.0f;
+        bool enabled() const { return angle > 0.0f; }
+    };
+
+    class DeviceBuffer;
+
+    // Device copies of a curved detector's planar pixel coordinates (float2 per pixel) and of
+    // the per-column planar u for the brick windows; empty for a flat detector. Needed only
+    // while a projector sets up its rays and windows.
+    class CurvedTables
+    {
+    public:
+        CurvedTables();
+        CurvedTables(int dim, const DetectorShape& det, const CurvedDetector& c);
+        ~CurvedTables();
+        CurvedTables(CurvedTables&&) noexcept;
+        CurvedTables& operator=(CurvedTables&&) noexcept;
+        const float2* planar() const;
+        CurvedMap map() const;
+        void release();
+
+    private:
+        std::unique_ptr<DeviceBuffer> planar_, column_;
+        float fmin_ = 1.0f, fmax_ = 1.0f;
+    };
+
     class Projector
     {
     public:
@@ -71,18 +101,21 @@ namespace elsa_b200
 
     std::unique_ptr<Projector> makeJosephProjector(const VolumeShape& vol,
                                                    const DetectorShape& det,
-                                                   const std::vector<PoseRecord>& poses);
+                                                   const std::vector<PoseRecord>& poses,
+                                                   const CurvedDetector& curved = {});
     // binary: BinaryMethod, the Siddon visits with weight 1 (projectors/BinaryMethod.cpp)
     std::unique_ptr<Projector> makeSiddonProjector(const VolumeShape& vol,
                                                    const DetectorShape& det,
                                                    const std::vector<PoseRecord>& poses,
-                                                   bool binary = false);
+                                                   bool binary = false,
+                                                   const CurvedDetector& curved = {});
 
     // Detector window of every (brick, view) for the brick-owner adjoints: the projection of the
     // brick grown by one voxel, plus one pixel (joseph.cu). Windows are indexed view * nBricks +
     // brick.
     void launchBrickWindows(const float* poses, const VolumeShape& vol, const DetectorShape& det,
-                            int3 brick, int3 nBricks, RayWindow* out, cudaStream_t s);
+                            int3 brick, int3 nBricks, RayWindow* out, cudaStream_t s,
+                            CurvedMap cm = {});
 
     // x[v] = sum over c = 0 .. chunks-1 of partial[c * nvox + v], added in chunk order
     // (joseph.cu).

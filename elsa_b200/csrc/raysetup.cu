@@ -25,12 +25,22 @@ namespace elsa_b200
             return (y != y) ? x : (x > y ? x : y);
         }
 
-        // Ray through the centre of pixel (u, v) of a pose record.
-        __device__ void pixelRay(const float* pose, int dim, int u, int v, float* o, float* d)
+        // Ray through the centre of pixel (u, v) of a pose record, or, for a curved detector,
+        // through the planar coordinate planar[u + nu * v] of that pixel centre
+        // (CurvedDetectorDescriptor::computeRayFromDetectorCoord,
+        // core/Descriptors/CurvedDetectorDescriptor.cpp:93-120).
+        __device__ void pixelRay(const float* pose, int dim, int u, int v, const float2* planar,
+                                 int nu, float* o, float* d)
         {
             const float* Pinv = pose + 12;
-            const float h0 = static_cast<float>(u) + 0.5f;
-            const float h1 = (dim == 3) ? static_cast<float>(v) + 0.5f : 1.0f;
+            float h0 = static_cast<float>(u) + 0.5f;
+            float h1 = (dim == 3) ? static_cast<float>(v) + 0.5f : 1.0f;
+            if (planar) {
+                const float2 c = planar[u + static_cast<int64_t>(nu) * v];
+                h0 = c.x;
+                if (dim == 3)
+                    h1 = c.y;
+            }
             float dir[3];
             if (dim == 3) {
                 for (int i = 0; i < 3; ++i) {
@@ -82,7 +92,8 @@ namespace elsa_b200
     } // namespace
 
     __global__ void josephSetupKernel(const float* __restrict__ poses, VolumeShape vol,
-                                      DetectorShape det, JosephRay* __restrict__ rays)
+                                      DetectorShape det, const float2* __restrict__ planar,
+                                      JosephRay* __restrict__ rays)
     {
         const int64_t nrays = static_cast<int64_t>(det.nu) * det.nv * det.np;
         const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -93,7 +104,7 @@ namespace elsa_b200
         const int v = static_cast<int>((r / det.nu) % det.nv);
         const int p = static_cast<int>(r / (static_cast<int64_t>(det.nu) * det.nv));
         float o[3] = {0, 0, 0}, d[3] = {0, 0, 0};
-        pixelRay(poses + static_cast<int64_t>(p) * 40, dim, u, v, o, d);
+        pixelRay(poses + static_cast<int64_t>(p) * 40, dim, u, v, planar, det.nu, o, d);
         float boxMax[3] = {static_cast<float>(vol.n[0]), static_cast<float>(vol.n[1]),
                            static_cast<float>(vol.n[2])};
         float tmin, tmax;
@@ -152,7 +163,8 @@ namespace elsa_b200
     }
 
     __global__ void siddonSetupKernel(const float* __restrict__ poses, VolumeShape vol,
-                                      DetectorShape det, SiddonRay* __restrict__ rays,
+                                      DetectorShape det, const float2* __restrict__ planar,
+                                      SiddonRay* __restrict__ rays,
                                       SiddonLine* __restrict__ lines)
     {
         const int64_t nrays = static_cast<int64_t>(det.nu) * det.nv * det.np;
@@ -164,7 +176,7 @@ namespace elsa_b200
         const int v = static_cast<int>((r / det.nu) % det.nv);
         const int p = static_cast<int>(r / (static_cast<int64_t>(det.nu) * det.nv));
         float o[3] = {0, 0, 0}, d[3] = {0, 0, 0};
-        pixelRay(poses + static_cast<int64_t>(p) * 40, dim, u, v, o, d);
+        pixelRay(poses + static_cast<int64_t>(p) * 40, dim, u, v, planar, det.nu, o, d);
         float boxMax[3] = {static_cast<float>(vol.n[0]), static_cast<float>(vol.n[1]),
                            static_cast<float>(vol.n[2])};
         float tmin, tmax;

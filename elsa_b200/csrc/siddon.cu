@@ -443,9 +443,11 @@ namespace elsa_b200
         public:
             // binary: BinaryMethod (kind 6), the same visits with weight 1
             SiddonProjector(const VolumeShape& vol, const DetectorShape& det,
-                            const std::vector<PoseRecord>& poses, bool binary)
+                            const std::vector<PoseRecord>& poses, bool binary,
+                            const CurvedDetector& curved)
                 : Projector(binary ? 6 : 1, vol, det, poses), binary_(binary ? 1 : 0)
             {
+                CurvedTables tables(vol.dim, det, curved); // used while setting up
                 const int maxDim = std::max(vol_.n[0], std::max(vol_.n[1], vol_.n[2]));
                 if (maxDim >= 65536)
                     throw Error(ELSA_ERROR_NOT_SUPPORTED,
@@ -455,7 +457,8 @@ namespace elsa_b200
                 const unsigned blocks = static_cast<unsigned>((nrays + threads - 1) / threads);
                 rays_ = std::make_unique<DeviceBuffer>(sizeof(SiddonRay) * nrays);
                 DeviceBuffer lines(sizeof(SiddonLine) * nrays);
-                siddonSetupKernel<<<blocks, threads>>>(dPoses_, vol_, det_, rays_->as<SiddonRay>(),
+                siddonSetupKernel<<<blocks, threads>>>(dPoses_, vol_, det_, tables.planar(),
+                                                       rays_->as<SiddonRay>(),
                                                        lines.as<SiddonLine>());
                 ELSA_LAUNCH_CHECK("siddonSetupKernel");
 
@@ -506,7 +509,7 @@ namespace elsa_b200
                     static_cast<int64_t>(nBricks_.x) * nBricks_.y * nBricks_.z * det_.np;
                 windows_ = std::make_unique<DeviceBuffer>(sizeof(RayWindow) * nwin);
                 launchBrickWindows(dPoses_, vol_, det_, make_int3(kSlab, kSlab, bz), nBricks_,
-                                   windows_->as<RayWindow>(), nullptr);
+                                   windows_->as<RayWindow>(), nullptr, tables.map());
                 setKnob(kKnobAdjointChunks, defaultChunks());
                 ELSA_CUDA(cudaDeviceSynchronize());
             }
@@ -645,8 +648,8 @@ namespace elsa_b200
     std::unique_ptr<Projector> makeSiddonProjector(const VolumeShape& vol,
                                                    const DetectorShape& det,
                                                    const std::vector<PoseRecord>& poses,
-                                                   bool binary)
+                                                   bool binary, const CurvedDetector& curved)
     {
-        return std::make_unique<SiddonProjector>(vol, det, poses, binary);
+        return std::make_unique<SiddonProjector>(vol, det, poses, binary, curved);
     }
 } // namespace elsa_b200

@@ -2,10 +2,12 @@
 // residual norms accumulate in float64, and all scalars (alpha, beta, ...) stay in device memory,
 // so an iteration is a fixed sequence of asynchronous launches on one stream (capturable in a
 // CUDA graph).
+#include "geometry.hpp"
 #include "projector.hpp"
 #include "solvers.hpp"
 #include "vecops.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -26,6 +28,63 @@ namespace elsa_b200
     Projector::~Projector()
     {
         cudaFree(dPoses_);
+    }
+
+    CurvedTables::CurvedTables() = default;
+    CurvedTables::~CurvedTables() = default;
+    CurvedTables::CurvedTables(CurvedTables&&) noexcept = default;
+    CurvedTables& CurvedTables::operator=(CurvedTables&&) noexcept = default;
+
+    CurvedTables::CurvedTables(int dim, const DetectorShape& det, const CurvedDetector& c)
+    {
+        if (!c.enabled())
+            return;
+        if (!(c.s2d > 0.0f) || !std::isfinite(c.angle) || !std::isfinite(c.s2d))
+            throw Error(ELSA_ERROR_INVALID_ARGUMENT,
+                        "CurvedDetectorDescriptor: angle and source-to-detector distance must be "
+                        "positive");
+        std::vector<float> factor;
+        const std::vector<float> xy =
+            curvedPlanarCoords(dim, det.nu, det.nv, c.angle, c.s2d, &factor);
+        std::vector<float> column(static_cast<size_t>(det.nu));
+        for (int u = 0; u < det.nu; ++u) {
+            column[static_cast<size_t>(u)] = xy[static_cast<size_t>(u) * 2];
+            if (u > 0 && !(column[static_cast<size_t>(u)] > column[static_cast<size_t>(u - 1)]))
+                throw Error(ELSA_ERROR_NOT_SUPPORTED,
+                            "CurvedDetectorDescriptor: the pixel columns do not map to increasing "
+                            "planar coordinates (opening angle too large)");
+        }
+        fmin_ = *std::min_element(factor.begin(), factor.end());
+        fmax_ = *std::max_element(factor.begin(), factor.end());
+        if (!(fmin_ > 0.0f))
+            throw Error(ELSA_ERROR_NOT_SUPPORTED,
+                        "CurvedDetectorDescriptor: the arc reaches behind the source");
+        planar_ = std::make_unique<DeviceBuffer>(sizeof(float) * xy.size());
+        column_ = std::make_unique<DeviceBuffer>(sizeof(float) * column.size());
+        ELSA_CUDA(cudaMemcpy(planar_->as<float>(), xy.data(), sizeof(float) * xy.size(),
+                             cudaMemcpyHostToDevice));
+        ELSA_CUDA(cudaMemcpy(column_->as<float>(), column.data(), sizeof(float) * column.size(),
+                             cudaMemcpyHostToDevice));
+    }
+
+    const float2* CurvedTables::planar() const
+    {
+        return planar_ ? planar_->as<float2>() : nullptr;
+    }
+
+    CurvedMap CurvedTables::map() const
+    {
+        CurvedMap m;
+        m.planarU = column_ ? column_->as<float>() : nullptr;
+        m.fmin = fmin_;
+        m.fmax = fmax_;
+        return m;
+    }
+
+    void CurvedTables::release()
+    {
+        planar_.reset();
+        column_.reset();
     }
 
     DeviceBuffer::DeviceBuffer(size_t bytes) : bytes_(bytes)

@@ -88,6 +88,26 @@ class PlanarDetectorDescriptor(DataDescriptor):
         return int(self.poses.shape[0])
 
 
+class CurvedDetectorDescriptor(PlanarDetectorDescriptor):
+    """Cylindrical detector (core/Descriptors/CurvedDetectorDescriptor.h): the poses of a flat
+    detector plus the opening angle (radian) and the source-to-detector distance."""
+
+    def __init__(self, size, poses, angle, s2d, spacing=None):
+        super().__init__(size, poses, spacing)
+        self.angle = float(angle)
+        self.s2d = float(s2d)
+
+    def getPlanarCoords(self):
+        dim = self.getNumberOfDimensions()
+        nv = int(self._size[1]) if dim == 3 else 1
+        c = _capi.curved_detector_coords(dim, int(self._size[0]), nv, self.angle, self.s2d)
+        return [c[v, u, :dim - 1].astype(np.float64) for v in range(c.shape[0])
+                for u in range(c.shape[1])]
+
+    def getRadius(self):
+        return float(np.float32(np.float32(self._size[0]) / np.float32(self.angle)))
+
+
 class CircleTrajectoryGenerator:
     """generators/CircleTrajectoryGenerator.cpp:9-24."""
 
@@ -108,6 +128,23 @@ class CircleTrajectoryGenerator:
         spacing = list(detectorSpacing) if detectorSpacing is not None else \
             list(vol.getSpacingPerDimension()[:dim - 1])
         return PlanarDetectorDescriptor(det, poses, spacing + [1.0])
+
+
+class CurvedCircleTrajectoryGenerator:
+    """generators/CurvedCircleTrajectoryGenerator.cpp:8-30: the circle trajectory's poses with a
+    curved detector of opening angle `angle` (radian) at source-to-detector distance
+    sourceToCenter + centerToDetector."""
+
+    @staticmethod
+    def createTrajectory(numberOfPoses, volumeDescriptor, arcDegrees, sourceToCenter,
+                         centerToDetector, angle, principalPointOffset=None,
+                         centerOfRotOffset=None, detectorSize=None, detectorSpacing=None):
+        flat = CircleTrajectoryGenerator.createTrajectory(
+            numberOfPoses, volumeDescriptor, arcDegrees, sourceToCenter, centerToDetector,
+            principalPointOffset, centerOfRotOffset, detectorSize, detectorSpacing)
+        s2d = float(np.float32(np.float32(sourceToCenter) + np.float32(centerToDetector)))
+        return CurvedDetectorDescriptor(flat.shape, flat.poses, angle, s2d,
+                                        list(flat.getSpacingPerDimension()))
 
 
 # ---- DataContainer ---------------------------------------------------------------------------------
@@ -233,8 +270,11 @@ class LinearOperator:
             raise _capi.InvalidArgumentError(1, "range descriptor needs a geometry")
         self._domain = volumeDescriptor
         self._range = detectorDescriptor
+        curved = None
+        if isinstance(detectorDescriptor, CurvedDetectorDescriptor):
+            curved = (detectorDescriptor.angle, detectorDescriptor.s2d)
         self._op = _capi.Projector(kind, volumeDescriptor.shape, detectorDescriptor.shape,
-                                   detectorDescriptor.poses, params)
+                                   detectorDescriptor.poses, params, curved)
 
     def getDomainDescriptor(self):
         return self._domain

@@ -123,6 +123,24 @@ elsa_status elsa_projector_create(int32_t kind, int32_t dim, const int64_t* vol_
                                   const float* params, int32_t num_params,
                                   elsa_projector** out);
 
+/* As elsa_projector_create for a curved (cylindrical) detector, CurvedDetectorDescriptor
+ * (core/Descriptors/CurvedDetectorDescriptor.cpp:8-120) as CurvedCircleTrajectoryGenerator
+ * builds it (generators/CurvedCircleTrajectoryGenerator.cpp:8-30): the same poses, opening
+ * angle `angle` (radian, > 0) and source-to-detector distance `s2d` (source-to-centre plus
+ * centre-to-detector). The ray of pixel (u, v) passes the pixel centre's point on the arc.
+ * Kinds ELSA_PROJECTOR_JOSEPH, _SIDDON and _BINARY; the voxel projectors need a planar
+ * detector (ELSA_ERROR_NOT_SUPPORTED). */
+elsa_status elsa_projector_create_curved(int32_t kind, int32_t dim, const int64_t* vol_dims,
+                                         const int64_t* det_dims, const float* poses,
+                                         const float* params, int32_t num_params, float angle,
+                                         float s2d, elsa_projector** out);
+
+/* Planar detector coordinates of the pixel centres of a curved detector, two floats (u', v')
+ * per pixel, u fastest (v' = 0 in 2D): CurvedDetectorDescriptor::getPlanarCoords. out holds
+ * 2 * nu * nv floats (nv = 1 in 2D). Host only. */
+elsa_status elsa_curved_detector_coords(int32_t dim, int32_t nu, int32_t nv, float angle,
+                                        float s2d, float* out);
+
 /* Replaces the operator's destructor (JosephsMethodCUDA.cpp:94-107). */
 elsa_status elsa_projector_destroy(elsa_projector* projector);
 

@@ -445,23 +445,62 @@ namespace orc
         return r;
     }
 
-    static Ray rayForIndex(const PoseView* poses, int dim, const index_t* detDims, index_t ir)
+    // coords (optional): a curved detector's planar coordinate per pixel (2 floats, u fastest),
+    // used in place of the pixel centre (CurvedDetectorDescriptor.cpp:93-120)
+    static Ray rayForIndex(const PoseView* poses, int dim, const index_t* detDims, index_t ir,
+                           const float* coords = nullptr)
     {
         // detector coordinate from index, x (u) fastest, pose last
         float dc[2] = {0, 0};
         index_t pose;
+        index_t pixel;
         if (dim == 2) {
             const index_t u = ir % detDims[0];
             pose = ir / detDims[0];
+            pixel = u;
             dc[0] = static_cast<float>(u) + 0.5f;
         } else {
             const index_t u = ir % detDims[0];
             const index_t v = (ir / detDims[0]) % detDims[1];
             pose = ir / (detDims[0] * detDims[1]);
+            pixel = u + detDims[0] * v;
             dc[0] = static_cast<float>(u) + 0.5f;
             dc[1] = static_cast<float>(v) + 0.5f;
         }
+        if (coords) {
+            dc[0] = coords[2 * pixel];
+            if (dim == 3)
+                dc[1] = coords[2 * pixel + 1];
+        }
         return rayFromDetector(poses[pose], dc);
+    }
+
+    // CurvedDetectorDescriptor::setup / mapCurvedCoordToPlanarCoord
+    // (core/Descriptors/CurvedDetectorDescriptor.cpp:33-91): planar coordinates of the pixel
+    // centres, 2 floats per pixel (v' = 0 in 2D)
+    static void curvedCoords(int dim, index_t nu, index_t nv, float angle, float s2d, float* out)
+    {
+        const index_t height = dim == 3 ? nv : 1;
+        const float radius = static_cast<float>(nu) / angle;
+        const float angleDelta = angle / static_cast<float>(nu);
+        const float centre[2] = {static_cast<float>(nu) / 2.0f, static_cast<float>(height) / 2.0f};
+        const float circle[2] = {centre[0], s2d - radius};
+        for (index_t h = 0; h < height; ++h)
+            for (index_t l = 0; l < nu; ++l) {
+                const float coord0 = static_cast<float>(l) + 0.5f;
+                const float coord1 = static_cast<float>(h) + 0.5f;
+                const float rayAngle = (coord0 - centre[0]) * angleDelta;
+                // the reference's unqualified sin / cos of a float: evaluated in double here
+                const float deltaX =
+                    static_cast<float>(std::sin(static_cast<double>(rayAngle))) * radius;
+                const float deltaDepth =
+                    static_cast<float>(std::cos(static_cast<double>(rayAngle))) * radius;
+                const float onCurved[2] = {circle[0] + deltaX, circle[1] + deltaDepth};
+                const float factor = onCurved[1] == 0 ? 1.0f : s2d / onCurved[1];
+                float* o = out + 2 * (h * nu + l);
+                o[0] = (onCurved[0] - centre[0]) * factor + centre[0];
+                o[1] = dim == 3 ? (coord1 - centre[1]) * factor + centre[1] : 0.0f;
+            }
     }
 
     // projectors/Intersection.h:179-198
@@ -601,7 +640,7 @@ namespace orc
     template <typename data_t, bool adjoint>
     static void josephTraverse(int dim, const index_t* volDims, const index_t* detDims,
                                index_t numPoses, const float* poseData, const data_t* in,
-                               data_t* out, int mode)
+                               data_t* out, int mode, const float* coords = nullptr)
     {
         std::vector<PoseView> poses(numPoses);
         for (index_t p = 0; p < numPoses; ++p)
@@ -617,7 +656,7 @@ namespace orc
             std::fill(out, out + nvol, data_t(0));
 #pragma omp parallel for schedule(dynamic, 256)
         for (index_t ir = 0; ir < nrays; ++ir) {
-            const Ray r = rayForIndex(poses.data(), dim, detDims, ir);
+            const Ray r = rayForIndex(poses.data(), dim, detDims, ir, coords);
             DDTraversal tr = ddSetup(boxMax, dim, r);
             const data_t L = static_cast<data_t>(tr.length);
             data_t acc = 0;
@@ -656,7 +695,8 @@ namespace orc
     template <typename data_t, bool adjoint>
     static void siddonTraverse(int dim, const index_t* volDims, const index_t* detDims,
                                index_t numPoses, const float* poseData, const data_t* in,
-                               data_t* out, index_t* visits = nullptr, bool binary = false)
+                               data_t* out, index_t* visits = nullptr, bool binary = false,
+                               const float* coords = nullptr)
     {
         std::vector<PoseView> poses(numPoses);
         for (index_t p = 0; p < numPoses; ++p)
@@ -675,7 +715,7 @@ namespace orc
         const float MAXF = std::numeric_limits<float>::max();
 #pragma omp parallel for schedule(dynamic, 256)
         for (index_t ir = 0; ir < nrays; ++ir) {
-            const Ray r = rayForIndex(poses.data(), dim, detDims, ir);
+            const Ray r = rayForIndex(poses.data(), dim, detDims, ir, coords);
             data_t acc = 0;
             float tmin, tmax;
             bool inBox = intersectRay(boxMax, dim, r, tmin, tmax);
@@ -919,66 +959,71 @@ void oracle_dd_setup(int dim, const int64_t* volDims, const float* origin, const
 }
 
 void oracle_joseph_f32(int adjoint, int dim, const int64_t* volDims, const int64_t* detDims,
-                       const float* poses, const float* in, float* out, int mode)
+                       const float* poses, const float* in, float* out, int mode, const float* coords)
 {
     const int64_t np = detDims[dim - 1];
     if (adjoint)
-        orc::josephTraverse<float, true>(dim, volDims, detDims, np, poses, in, out, mode);
+        orc::josephTraverse<float, true>(dim, volDims, detDims, np, poses, in, out, mode, coords);
     else
-        orc::josephTraverse<float, false>(dim, volDims, detDims, np, poses, in, out, mode);
+        orc::josephTraverse<float, false>(dim, volDims, detDims, np, poses, in, out, mode, coords);
 }
 
 void oracle_joseph_f64(int adjoint, int dim, const int64_t* volDims, const int64_t* detDims,
-                       const float* poses, const double* in, double* out, int mode)
+                       const float* poses, const double* in, double* out, int mode, const float* coords)
 {
     const int64_t np = detDims[dim - 1];
     if (adjoint)
-        orc::josephTraverse<double, true>(dim, volDims, detDims, np, poses, in, out, mode);
+        orc::josephTraverse<double, true>(dim, volDims, detDims, np, poses, in, out, mode, coords);
     else
-        orc::josephTraverse<double, false>(dim, volDims, detDims, np, poses, in, out, mode);
+        orc::josephTraverse<double, false>(dim, volDims, detDims, np, poses, in, out, mode, coords);
 }
 
 void oracle_siddon_f32(int adjoint, int dim, const int64_t* volDims, const int64_t* detDims,
-                       const float* poses, const float* in, float* out)
+                       const float* poses, const float* in, float* out, const float* coords)
 {
     const int64_t np = detDims[dim - 1];
     if (adjoint)
-        orc::siddonTraverse<float, true>(dim, volDims, detDims, np, poses, in, out);
+        orc::siddonTraverse<float, true>(dim, volDims, detDims, np, poses, in, out, nullptr, false, coords);
     else
-        orc::siddonTraverse<float, false>(dim, volDims, detDims, np, poses, in, out);
+        orc::siddonTraverse<float, false>(dim, volDims, detDims, np, poses, in, out, nullptr, false, coords);
 }
 
 void oracle_siddon_f64(int adjoint, int dim, const int64_t* volDims, const int64_t* detDims,
-                       const float* poses, const double* in, double* out)
+                       const float* poses, const double* in, double* out, const float* coords)
 {
     const int64_t np = detDims[dim - 1];
     if (adjoint)
-        orc::siddonTraverse<double, true>(dim, volDims, detDims, np, poses, in, out);
+        orc::siddonTraverse<double, true>(dim, volDims, detDims, np, poses, in, out, nullptr, false, coords);
     else
-        orc::siddonTraverse<double, false>(dim, volDims, detDims, np, poses, in, out);
+        orc::siddonTraverse<double, false>(dim, volDims, detDims, np, poses, in, out, nullptr, false, coords);
 }
 
 void oracle_binary_f32(int adjoint, int dim, const int64_t* volDims, const int64_t* detDims,
-                       const float* poses, const float* in, float* out)
+                       const float* poses, const float* in, float* out, const float* coords)
 {
     const int64_t np = detDims[dim - 1];
     if (adjoint)
-        orc::siddonTraverse<float, true>(dim, volDims, detDims, np, poses, in, out, nullptr, true);
+        orc::siddonTraverse<float, true>(dim, volDims, detDims, np, poses, in, out, nullptr, true, coords);
     else
         orc::siddonTraverse<float, false>(dim, volDims, detDims, np, poses, in, out, nullptr,
-                                          true);
+                                          true, coords);
 }
 
 void oracle_binary_f64(int adjoint, int dim, const int64_t* volDims, const int64_t* detDims,
-                       const float* poses, const double* in, double* out)
+                       const float* poses, const double* in, double* out, const float* coords)
 {
     const int64_t np = detDims[dim - 1];
     if (adjoint)
         orc::siddonTraverse<double, true>(dim, volDims, detDims, np, poses, in, out, nullptr,
-                                          true);
+                                          true, coords);
     else
         orc::siddonTraverse<double, false>(dim, volDims, detDims, np, poses, in, out, nullptr,
-                                           true);
+                                           true, coords);
+}
+
+void oracle_curved_coords(int dim, int64_t nu, int64_t nv, float angle, float s2d, float* out)
+{
+    orc::curvedCoords(dim, nu, nv, angle, s2d, out);
 }
 
 // Number of Joseph samples (sum over rays of numSteps) and Siddon voxel crossings, used for the

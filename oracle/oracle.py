@@ -58,13 +58,15 @@ def lib():
         L.oracle_dd_setup.argtypes = [c_int, _i64p, _f32p, _f32p, _f32p, _f32p,
                                       ctypes.POINTER(c_f), ctypes.POINTER(c_int),
                                       ctypes.POINTER(c_i64)]
+        _vp = ctypes.c_void_p  # optional curved-detector coordinates (None: flat detector)
         for name, fp in (("f32", _f32p), ("f64", _f64p)):
             fn = getattr(L, "oracle_joseph_" + name)
-            fn.argtypes = [c_int, c_int, _i64p, _i64p, _f32p, fp, fp, c_int]
+            fn.argtypes = [c_int, c_int, _i64p, _i64p, _f32p, fp, fp, c_int, _vp]
             fn = getattr(L, "oracle_siddon_" + name)
-            fn.argtypes = [c_int, c_int, _i64p, _i64p, _f32p, fp, fp]
+            fn.argtypes = [c_int, c_int, _i64p, _i64p, _f32p, fp, fp, _vp]
             fn = getattr(L, "oracle_binary_" + name)
-            fn.argtypes = [c_int, c_int, _i64p, _i64p, _f32p, fp, fp]
+            fn.argtypes = [c_int, c_int, _i64p, _i64p, _f32p, fp, fp, _vp]
+        L.oracle_curved_coords.argtypes = [c_int, c_i64, c_i64, c_f, c_f, _f32p]
         L.oracle_joseph_sample_count.argtypes = [c_int, _i64p, _i64p, _f32p]
         L.oracle_joseph_sample_count.restype = c_i64
         L.oracle_siddon_visit_count.argtypes = [c_int, _i64p, _i64p, _f32p]
@@ -168,7 +170,8 @@ def _vol_count(vol_dims):
     return int(np.prod(vol_dims))
 
 
-def _call_projector(name, adjoint, vol_dims, det_dims, poses, data, dtype, extra=()):
+def _call_projector(name, adjoint, vol_dims, det_dims, poses, data, dtype, extra=(),
+                    coords=None):
     dim = len(vol_dims)
     vd = np.asarray(vol_dims, np.int64)
     dd = np.asarray(det_dims, np.int64)
@@ -176,38 +179,52 @@ def _call_projector(name, adjoint, vol_dims, det_dims, poses, data, dtype, extra
     n_out = _vol_count(vol_dims) if adjoint else _det_count(det_dims)
     out = np.zeros(n_out, dtype)
     suffix = "f32" if dtype == np.float32 else "f64"
-    getattr(lib(), "oracle_%s_%s" % (name, suffix))(int(adjoint), dim, vd, dd, _f32(poses), inp,
-                                                    out, *extra)
+    cc = None if coords is None else np.ascontiguousarray(coords, np.float32).reshape(-1)
+    if cc is not None and cc.size != 2 * int(np.prod(dd[:-1])):
+        raise ValueError("curved detector coordinates: 2 floats per detector pixel")
+    getattr(lib(), "oracle_%s_%s" % (name, suffix))(
+        int(adjoint), dim, vd, dd, _f32(poses), inp, out, *extra,
+        cc.ctypes.data_as(ctypes.c_void_p) if cc is not None else None)
     return out
 
 
-def joseph(x, vol_dims, det_dims, poses, dtype=np.float32, mode=0):
+def curved_coords(dim, nu, nv, angle, s2d):
+    """CurvedDetectorDescriptor::getPlanarCoords (core/Descriptors/CurvedDetectorDescriptor.cpp:
+    33-91): planar (u', v') of every pixel centre, shape (nv, nu, 2) (nv = 1 in 2D)."""
+    h = nv if dim == 3 else 1
+    out = np.zeros(2 * nu * h, np.float32)
+    lib().oracle_curved_coords(int(dim), int(nu), int(h), float(angle), float(s2d), out)
+    return out.reshape(h, nu, 2)
+
+
+def joseph(x, vol_dims, det_dims, poses, dtype=np.float32, mode=0, coords=None):
     """Joseph forward projection (projectors/JosephsMethod.cpp:140-198). mode 0 accumulates the
-    sample position like the reference; mode 1 evaluates it as fma(j, step, pos0)."""
-    return _call_projector("joseph", False, vol_dims, det_dims, poses, x, dtype, (mode,))
+    sample position like the reference; mode 1 evaluates it as fma(j, step, pos0). coords: a
+    curved detector's planar pixel coordinates (curved_coords)."""
+    return _call_projector("joseph", False, vol_dims, det_dims, poses, x, dtype, (mode,), coords)
 
 
-def joseph_adjoint(y, vol_dims, det_dims, poses, dtype=np.float32, mode=0):
-    return _call_projector("joseph", True, vol_dims, det_dims, poses, y, dtype, (mode,))
+def joseph_adjoint(y, vol_dims, det_dims, poses, dtype=np.float32, mode=0, coords=None):
+    return _call_projector("joseph", True, vol_dims, det_dims, poses, y, dtype, (mode,), coords)
 
 
-def siddon(x, vol_dims, det_dims, poses, dtype=np.float32):
+def siddon(x, vol_dims, det_dims, poses, dtype=np.float32, coords=None):
     """Siddon forward projection (projectors/SiddonsMethod.cpp:76-100)."""
-    return _call_projector("siddon", False, vol_dims, det_dims, poses, x, dtype)
+    return _call_projector("siddon", False, vol_dims, det_dims, poses, x, dtype, coords=coords)
 
 
-def siddon_adjoint(y, vol_dims, det_dims, poses, dtype=np.float32):
-    return _call_projector("siddon", True, vol_dims, det_dims, poses, y, dtype)
+def siddon_adjoint(y, vol_dims, det_dims, poses, dtype=np.float32, coords=None):
+    return _call_projector("siddon", True, vol_dims, det_dims, poses, y, dtype, coords=coords)
 
 
-def binary(x, vol_dims, det_dims, poses, dtype=np.float32):
+def binary(x, vol_dims, det_dims, poses, dtype=np.float32, coords=None):
     """BinaryMethod forward projection (projectors/BinaryMethod.cpp:66-111): the sum of the voxels
     that TraverseAABB visits."""
-    return _call_projector("binary", False, vol_dims, det_dims, poses, x, dtype)
+    return _call_projector("binary", False, vol_dims, det_dims, poses, x, dtype, coords=coords)
 
 
-def binary_adjoint(y, vol_dims, det_dims, poses, dtype=np.float32):
-    return _call_projector("binary", True, vol_dims, det_dims, poses, y, dtype)
+def binary_adjoint(y, vol_dims, det_dims, poses, dtype=np.float32, coords=None):
+    return _call_projector("binary", True, vol_dims, det_dims, poses, y, dtype, coords=coords)
 
 
 def joseph_sample_count(vol_dims, det_dims, poses):
