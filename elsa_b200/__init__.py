@@ -18,7 +18,7 @@ from ._capi import (ElsaError, InvalidArgumentError, Projector, Solver,  # noqa:
                     tune_cache_get, SOLVER_SQS, SUBSET_ROUND_ROBIN,
                     SUBSET_ROTATIONAL_CLUSTERING, subset_split, gather_views, edf_read,
                     edf_write, mhd_read, mhd_write, pgm_write, PROJECTOR_BINARY,
-                    curved_detector_coords)
+                    curved_detector_coords, PROJECTOR_RAY_BLOB, PROJECTOR_RAY_BSPLINE)
 
 __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "voxel_lut",
            "PROJECTOR_BLOB", "PROJECTOR_BSPLINE", "PROJECTOR_PHASE_CONTRAST_BLOB",
@@ -33,4 +33,4 @@ __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "voxel_lu
            "tune_cache_load", "tune_cache_put", "tune_cache_get", "SOLVER_SQS",
            "SUBSET_ROUND_ROBIN", "SUBSET_ROTATIONAL_CLUSTERING", "subset_split", "gather_views",
            "edf_read", "edf_write", "mhd_read", "mhd_write", "pgm_write", "PROJECTOR_BINARY",
-           "curved_detector_coords"]
+           "curved_detector_coords", "PROJECTOR_RAY_BLOB", "PROJECTOR_RAY_BSPLINE"]

@@ -28,6 +28,8 @@ PROJECTOR_BSPLINE = 3
 PROJECTOR_PHASE_CONTRAST_BLOB = 4
 PROJECTOR_PHASE_CONTRAST_BSPLINE = 5
 PROJECTOR_BINARY = 6
+PROJECTOR_RAY_BLOB = 7
+PROJECTOR_RAY_BSPLINE = 8
 FOOTPRINT_REFERENCE = 0
 FOOTPRINT_RECTANGLE = 1
 SOLVER_CGNE = 0

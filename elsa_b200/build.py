@@ -37,6 +37,7 @@ CUDA_UNITS = [
     ("voxel.cu", ["--fmad=false"]),
     ("vecops.cu", []),
     ("noalloc.cu", []),
+    ("lutproj.cu", []),
     ("solvers.cu", []),
 ]
 CXX_UNITS = [

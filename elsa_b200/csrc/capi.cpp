@@ -228,6 +228,21 @@ static elsa_status projectorCreate(int32_t kind, int32_t dim, const int64_t* vol
         case ELSA_PROJECTOR_BINARY:
             handle->impl = elsa_b200::makeSiddonProjector(vol, det, pv, true, curved);
             break;
+        case ELSA_PROJECTOR_RAY_BLOB:
+        case ELSA_PROJECTOR_RAY_BSPLINE: {
+            if (curved.enabled())
+                throw elsa_b200::Error(ELSA_ERROR_NOT_SUPPORTED,
+                                       "LutProjector: curved detectors are not supported");
+            const bool blob = kind == ELSA_PROJECTOR_RAY_BLOB;
+            require(numParams <= (blob ? 3 : 1), "LutProjector: too many parameters");
+            const VoxelSpec spec = voxelSpec(blob ? ELSA_PROJECTOR_BLOB : ELSA_PROJECTOR_BSPLINE,
+                                             dim, params, numParams);
+            // BlobProjector::support = ceil(radius), BSplineProjector::support = 2
+            // (projectors/LutProjector.h:199, LutProjector.cpp:77-80)
+            const int support = blob ? static_cast<int>(std::ceil(spec.lut.support)) : 2;
+            handle->impl = elsa_b200::makeLutProjector(kind, vol, det, pv, spec.lut, support);
+            break;
+        }
         case ELSA_PROJECTOR_BLOB:
         case ELSA_PROJECTOR_BSPLINE:
         case ELSA_PROJECTOR_PHASE_CONTRAST_BLOB:

@@ -110,6 +110,14 @@ namespace elsa_b200
                                                    bool binary = false,
                                                    const CurvedDetector& curved = {});
 
+    struct VoxelLut;
+    // Ray-driven blob / B-spline projector (LutProjector): lut on [0, lut.support], the
+    // neighbourhood half-width `support` in voxels.
+    std::unique_ptr<Projector> makeLutProjector(int kind, const VolumeShape& vol,
+                                                const DetectorShape& det,
+                                                const std::vector<PoseRecord>& poses,
+                                                const VoxelLut& lut, int support);
+
     // Detector window of every (brick, view) for the brick-owner adjoints: the projection of the
     // brick grown by one voxel, plus one pixel (joseph.cu). Windows are indexed view * nBricks +
     // brick.

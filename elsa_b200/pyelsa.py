@@ -324,6 +324,23 @@ class BinaryMethod(LinearOperator):
         super().__init__(_capi.PROJECTOR_BINARY, volumeDescriptor, detectorDescriptor)
 
 
+class BlobProjector(LinearOperator):
+    """BlobProjector(volume, detector, radius=2, alpha=10.83, order=2): elsa's ray-driven blob
+    projector (projectors/LutProjector.h), on the device."""
+
+    def __init__(self, volumeDescriptor, detectorDescriptor, radius=2.0, alpha=10.83, order=2):
+        super().__init__(_capi.PROJECTOR_RAY_BLOB, volumeDescriptor, detectorDescriptor,
+                         [radius, alpha, order])
+
+
+class BSplineProjector(LinearOperator):
+    """BSplineProjector(volume, detector, order=2): elsa's ray-driven B-spline projector."""
+
+    def __init__(self, volumeDescriptor, detectorDescriptor, order=2):
+        super().__init__(_capi.PROJECTOR_RAY_BSPLINE, volumeDescriptor, detectorDescriptor,
+                         [order])
+
+
 class BlobVoxelProjectorCUDA(LinearOperator):
     def __init__(self, volumeDescriptor, detectorDescriptor, radius=2.0, alpha=10.83, order=2,
                  footprint=_capi.FOOTPRINT_REFERENCE):
@@ -357,6 +374,7 @@ class PhaseContrastBSplineVoxelProjectorCUDA(LinearOperator):
 JosephsMethod = JosephsMethodCUDAf = JosephsMethodCUDA
 SiddonsMethod = SiddonsMethodCUDAf = SiddonsMethodCUDA
 BinaryMethodf = BinaryMethod
+BlobProjectorf, BSplineProjectorf = BlobProjector, BSplineProjector
 BlobVoxelProjector = BlobVoxelProjectorCUDAf = BlobVoxelProjectorCUDA
 BSplineVoxelProjector = BSplineVoxelProjectorCUDAf = BSplineVoxelProjectorCUDA
 PhaseContrastBlobVoxelProjector = PhaseContrastBlobVoxelProjectorCUDA

@@ -60,7 +60,16 @@ typedef enum elsa_projector_kind {
     ELSA_PROJECTOR_PHASE_CONTRAST_BSPLINE = 5,
     /* BinaryMethod, projectors/BinaryMethod.cpp:66-111: the voxels TraverseAABB visits, each
      * with weight 1 (elsa has it on the CPU only). */
-    ELSA_PROJECTOR_BINARY = 6
+    ELSA_PROJECTOR_BINARY = 6,
+    /* BlobProjector, the ray-driven blob projector of projectors/LutProjector.h:85-199 (the
+     * slice walk of SliceTraversal.cpp, lut(distance to the ray) for the voxels within
+     * ceil(radius) in each slice). params: radius (2), alpha (10.83), order (2). As in the
+     * reference, the adjoint walks a box grown by the support, so forward and adjoint are not
+     * exact transposes near the volume faces. */
+    ELSA_PROJECTOR_RAY_BLOB = 7,
+    /* BSplineProjector, the same with the projected B-spline (neighbourhood 2,
+     * LutProjector.cpp:48-90). params: order (2). */
+    ELSA_PROJECTOR_RAY_BSPLINE = 8
 } elsa_projector_kind;
 
 /* Footprint mode of the voxel projectors (last parameter): 0 visits the pixels of each voxel

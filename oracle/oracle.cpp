@@ -22,6 +22,12 @@
 
 #include <omp.h>
 
+namespace vox
+{
+    // Lut::operator() (voxel_oracle.cpp)
+    float lutLerp(const float* lut, int64_t N, float support, float distance);
+} // namespace vox
+
 namespace orc
 {
     using real_t = float;
@@ -805,6 +811,265 @@ namespace orc
     }
 
     // ------------------------------------------------------------------------------------------
+    // Ray-driven blob / B-spline projector: projectors/LutProjector.h:85-163 with
+    // SliceTraversal.cpp:7-200 (traversal coordinates: the leading axis of the ray rotated onto
+    // +x about the box centre), Intersection.cpp:47-119 (intersectXPlanes) and
+    // core/Utilities/CartesianIndices.cpp:341-356 (neighbours_in_slice, last axis fastest).
+    // ------------------------------------------------------------------------------------------
+    struct SliceWalk {
+        bool hit = false;
+        float start[3] = {0, 0, 0}; // ray.pointAt(t) of the first slice, original coordinates
+        float step[3] = {0, 0, 0};  // direction * tDelta
+        index_t count = 0;          // endIndex
+        int lead = 0;
+    };
+
+    // rotation of TransformToTraversal::create2DRotation / create3DRotation
+    static void traversalRotation(int dim, int lead, float coeff, float R[3][3])
+    {
+        const float pi = static_cast<float>(3.14159265358979323846);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                R[i][j] = i == j ? 1.0f : 0.0f;
+        if (dim == 2) {
+            float rad = 0.0f;
+            if (lead == 0 && coeff >= 0)
+                rad = 0.0f;
+            else if (lead == 0 && coeff < 0)
+                rad = pi;
+            else if (lead == 1 && coeff >= 0)
+                rad = 3 * pi / 2;
+            else if (lead == 1 && coeff <= 0)
+                rad = pi / 2;
+            const float c = std::cos(rad), sn = std::sin(rad);
+            R[0][0] = c, R[0][1] = -sn, R[1][0] = sn, R[1][1] = c;
+            return;
+        }
+        auto rotY = [&](float rad) {
+            const float c = std::cos(rad), sn = std::sin(rad);
+            R[0][0] = c, R[0][1] = 0, R[0][2] = sn;
+            R[1][0] = 0, R[1][1] = 1, R[1][2] = 0;
+            R[2][0] = -sn, R[2][1] = 0, R[2][2] = c;
+        };
+        auto rotZ = [&](float rad) {
+            const float c = std::cos(rad), sn = std::sin(rad);
+            R[0][0] = c, R[0][1] = -sn, R[0][2] = 0;
+            R[1][0] = sn, R[1][1] = c, R[1][2] = 0;
+            R[2][0] = 0, R[2][1] = 0, R[2][2] = 1;
+        };
+        const float half = static_cast<float>(0.5 * static_cast<double>(pi));
+        if (lead == 0 && coeff >= 0)
+            return;
+        else if (lead == 0 && coeff < 0)
+            rotY(pi);
+        else if (lead == 1 && coeff >= 0)
+            rotZ(-half);
+        else if (lead == 1 && coeff <= 0)
+            rotZ(half);
+        else if (lead == 2 && coeff >= 0)
+            rotY(half);
+        else if (lead == 2 && coeff <= 0)
+            rotY(-half);
+    }
+
+    // SliceTraversal(aabb, ray) for the box [bmin, bmax]
+    static SliceWalk sliceWalk(int dim, const float* bmin, const float* bmax, const Ray& r)
+    {
+        SliceWalk w;
+        int lead = 0;
+        float best = std::fabs(r.d[0]);
+        for (int i = 1; i < dim; ++i)
+            if (std::fabs(r.d[i]) > best) {
+                best = std::fabs(r.d[i]);
+                lead = i;
+            }
+        w.lead = lead;
+        float R[3][3];
+        traversalRotation(dim, lead, r.d[lead], R);
+        // T = rotation * translation(-centre): columns 0..dim-1 are R, column dim is R (-centre)
+        float centre[3] = {0, 0, 0}, tcol[3] = {0, 0, 0};
+        for (int i = 0; i < dim; ++i)
+            centre[i] = bmax[i] / 2;
+        for (int i = 0; i < dim; ++i) {
+            float acc = 0.0f;
+            for (int k = 0; k < dim; ++k)
+                acc = acc + R[i][k] * (-centre[k]);
+            tcol[i] = acc + 0.0f;
+        }
+        auto point = [&](const float* p, float* out) {
+            for (int i = 0; i < dim; ++i) {
+                float acc = 0.0f;
+                for (int k = 0; k < dim; ++k)
+                    acc = acc + R[i][k] * p[k];
+                out[i] = acc + tcol[i];
+            }
+        };
+        float o[3], d[3], lo[3], hi[3];
+        point(r.o, o);
+        for (int i = 0; i < dim; ++i) {
+            float acc = 0.0f;
+            for (int k = 0; k < dim; ++k)
+                acc = acc + R[i][k] * r.d[k];
+            d[i] = acc;
+        }
+        point(bmin, lo);
+        point(bmax, hi);
+        for (int i = 0; i < dim; ++i)
+            if (lo[i] > hi[i])
+                std::swap(lo[i], hi[i]);
+        // intersectXPlanes
+        lo[0] += 0.5f;
+        hi[0] -= 0.5f;
+        float invDir = 1 / d[0];
+        float t1 = (lo[0] - o[0]) * invDir, t2 = (hi[0] - o[0]) * invDir;
+        float tmin = invDir >= 0 ? t1 : t2, tmax = invDir >= 0 ? t2 : t1;
+        const float txmin = tmin, txmax = tmax;
+        for (int i = 1; i < dim; ++i) {
+            invDir = 1 / d[i];
+            t1 = (lo[i] - o[i]) * invDir;
+            t2 = (hi[i] - o[i]) * invDir;
+            tmin = maxNum(tmin, invDir >= 0 ? t1 : t2);
+            tmax = minNum(tmax, invDir >= 0 ? t2 : t1);
+        }
+        const float xcentre = std::fabs(lo[0] - static_cast<float>(static_cast<int>(std::round(lo[0]))));
+        auto fractional = [](float v) {
+            float trash = 0;
+            return std::modf(v, &trash);
+        };
+        if (txmin < tmin) {
+            const float e = o[0] + tmin * d[0];
+            const float tmp = std::fabs(fractional(e - xcentre));
+            const float frac = e < xcentre ? tmp : 1 - tmp;
+            tmin += (tmp > 0.00001 && frac > 0.00001) ? frac / d[0] : 0;
+        }
+        if (txmax > tmax) {
+            const float e = o[0] + tmax * d[0];
+            const float tmp = std::fabs(fractional(e - xcentre));
+            const float frac = e < xcentre ? 1 - tmp : tmp;
+            tmax -= (tmp > 0.00001 && frac > 0.00001) ? frac / d[0] : 0;
+        }
+        if (tmax == 0.0 && tmin == 0.0)
+            return w;
+        if (!(tmax - maxNum(tmin, 0.0f) > -0.000001))
+            return w;
+        const float first = o[0] + tmin * d[0], last = o[0] + tmax * d[0];
+        w.count = std::max<index_t>(1, static_cast<index_t>(std::ceil(last - first + 0.5f)));
+        const float tDelta = 1 / d[0];
+        for (int i = 0; i < dim; ++i) {
+            w.start[i] = r.o[i] + tmin * r.d[i];
+            w.step[i] = r.d[i] * tDelta;
+        }
+        w.hit = true;
+        return w;
+    }
+
+    // Visit the neighbourhood of every slice voxel: f(linear index, weight). backward: the walk
+    // uses the box grown by `support` in the non-leading axes (LutProjector.h:135-147).
+    template <class F>
+    static void lutRay(int dim, const index_t* volDims, const Ray& r, const float* lut,
+                       index_t lutN, float radius, int support, bool backward, F&& f)
+    {
+        float bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};
+        for (int i = 0; i < dim; ++i)
+            bmax[i] = static_cast<float>(volDims[i]);
+        int lead = 0;
+        {
+            float best = std::fabs(r.d[0]);
+            for (int i = 1; i < dim; ++i)
+                if (std::fabs(r.d[i]) > best) {
+                    best = std::fabs(r.d[i]);
+                    lead = i;
+                }
+        }
+        float wmin[3], wmax[3];
+        for (int i = 0; i < dim; ++i) {
+            wmin[i] = bmin[i], wmax[i] = bmax[i];
+            if (backward && i != lead) {
+                wmin[i] -= static_cast<float>(support);
+                wmax[i] += static_cast<float>(support);
+            }
+        }
+        const SliceWalk w = sliceWalk(dim, wmin, wmax, r);
+        if (!w.hit)
+            return;
+        float cur[3] = {w.start[0], w.start[1], w.start[2]};
+        for (index_t it = 0; it < w.count; ++it) {
+            index_t from[3] = {0, 0, 0}, to[3] = {1, 1, 1};
+            for (int i = 0; i < dim; ++i) {
+                const index_t pos = static_cast<index_t>(cur[i]);
+                const index_t dist = i == lead ? 0 : support;
+                from[i] = std::max<index_t>(pos - dist, 0);
+                to[i] = std::min<index_t>(pos + dist + 1, volDims[i]);
+                if (to[i] == from[i])
+                    from[i] -= 1;
+            }
+            for (index_t a = from[0]; a < to[0]; ++a)
+                for (index_t b = from[1]; b < to[1]; ++b)
+                    for (index_t c = from[2]; c < (dim == 3 ? to[2] : from[2] + 1); ++c) {
+                        const index_t nb[3] = {a, b, c};
+                        float diff[3], dot = 0.0f;
+                        for (int i = 0; i < dim; ++i)
+                            diff[i] = (static_cast<float>(nb[i]) + 0.5f) - r.o[i];
+                        for (int i = 0; i < dim; ++i)
+                            dot = dot + r.d[i] * diff[i];
+                        float sq = 0.0f;
+                        for (int i = 0; i < dim; ++i) {
+                            const float v = diff[i] - dot * r.d[i];
+                            sq = sq + v * v;
+                        }
+                        const float distance = std::sqrt(sq);
+                        const float wt = vox::lutLerp(lut, lutN, radius, distance);
+                        const index_t idx = a + volDims[0] * (b + (dim == 3 ? volDims[1] * c : 0));
+                        if (a >= 0 && b >= 0 && c >= 0)
+                            f(idx, wt);
+                    }
+            for (int i = 0; i < dim; ++i)
+                cur[i] = cur[i] + w.step[i];
+        }
+    }
+
+    template <typename data_t, bool adjoint>
+    static void lutTraverse(int dim, const index_t* volDims, const index_t* detDims,
+                            index_t numPoses, const float* poseData, const float* lut,
+                            index_t lutN, float radius, int support, const data_t* in,
+                            data_t* out)
+    {
+        std::vector<PoseView> poses(numPoses);
+        for (index_t p = 0; p < numPoses; ++p)
+            poses[p] = PoseView{dim, poseData + p * POSE_FLOATS};
+        index_t nvol = 1;
+        for (int i = 0; i < dim; ++i)
+            nvol *= volDims[i];
+        const index_t nrays = (dim == 2 ? detDims[0] : detDims[0] * detDims[1]) * numPoses;
+        if (adjoint)
+            std::fill(out, out + nvol, data_t(0));
+#pragma omp parallel for schedule(dynamic, 64)
+        for (index_t ir = 0; ir < nrays; ++ir) {
+            const Ray r = rayForIndex(poses.data(), dim, detDims, ir);
+            if (adjoint) {
+                const data_t y = in[ir];
+                lutRay(dim, volDims, r, lut, lutN, radius, support, true,
+                       [&](index_t idx, float wt) {
+                           if (idx < 0 || idx >= nvol)
+                               return;
+                           const data_t v = static_cast<data_t>(wt) * y;
+#pragma omp atomic
+                           out[idx] += v;
+                       });
+            } else {
+                data_t acc = 0;
+                lutRay(dim, volDims, r, lut, lutN, radius, support, false,
+                       [&](index_t idx, float wt) {
+                           if (idx < 0 || idx >= nvol)
+                               return;
+                           acc += static_cast<data_t>(wt) * in[idx];
+                       });
+                out[ir] = acc;
+            }
+        }
+    }
+
+    // ------------------------------------------------------------------------------------------
     // Vector operations (storage/reductions/DotProduct.h:24-47, L2.h:15-49,
     // transforms/Lincomb.h:28-33): reductions accumulate in data_t, in 64 fixed blocks combined
     // sequentially (a deterministic stand-in for Thrust's blocked reduction).
@@ -1019,6 +1284,32 @@ void oracle_binary_f64(int adjoint, int dim, const int64_t* volDims, const int64
     else
         orc::siddonTraverse<double, false>(dim, volDims, detDims, np, poses, in, out, nullptr,
                                            true, coords);
+}
+
+void oracle_lut_f32(int adjoint, int dim, const int64_t* volDims, const int64_t* detDims,
+                    const float* poses, const float* lut, int64_t lutN, float radius, int support,
+                    const float* in, float* out)
+{
+    const int64_t np = detDims[dim - 1];
+    if (adjoint)
+        orc::lutTraverse<float, true>(dim, volDims, detDims, np, poses, lut, lutN, radius,
+                                      support, in, out);
+    else
+        orc::lutTraverse<float, false>(dim, volDims, detDims, np, poses, lut, lutN, radius,
+                                       support, in, out);
+}
+
+void oracle_lut_f64(int adjoint, int dim, const int64_t* volDims, const int64_t* detDims,
+                    const float* poses, const float* lut, int64_t lutN, float radius, int support,
+                    const double* in, double* out)
+{
+    const int64_t np = detDims[dim - 1];
+    if (adjoint)
+        orc::lutTraverse<double, true>(dim, volDims, detDims, np, poses, lut, lutN, radius,
+                                       support, in, out);
+    else
+        orc::lutTraverse<double, false>(dim, volDims, detDims, np, poses, lut, lutN, radius,
+                                        support, in, out);
 }
 
 void oracle_curved_coords(int dim, int64_t nu, int64_t nv, float angle, float s2d, float* out)

@@ -67,6 +67,9 @@ def lib():
             fn = getattr(L, "oracle_binary_" + name)
             fn.argtypes = [c_int, c_int, _i64p, _i64p, _f32p, fp, fp, _vp]
         L.oracle_curved_coords.argtypes = [c_int, c_i64, c_i64, c_f, c_f, _f32p]
+        for name, fp in (("f32", _f32p), ("f64", _f64p)):
+            getattr(L, "oracle_lut_" + name).argtypes = [c_int, c_int, _i64p, _i64p, _f32p,
+                                                         _f32p, c_i64, c_f, c_int, fp, fp]
         L.oracle_joseph_sample_count.argtypes = [c_int, _i64p, _i64p, _f32p]
         L.oracle_joseph_sample_count.restype = c_i64
         L.oracle_siddon_visit_count.argtypes = [c_int, _i64p, _i64p, _f32p]
@@ -225,6 +228,23 @@ def binary(x, vol_dims, det_dims, poses, dtype=np.float32, coords=None):
 
 def binary_adjoint(y, vol_dims, det_dims, poses, dtype=np.float32, coords=None):
     return _call_projector("binary", True, vol_dims, det_dims, poses, y, dtype, coords=coords)
+
+
+def lut_project(adjoint, data, vol_dims, det_dims, poses, lut, radius, support,
+                dtype=np.float32):
+    """Ray-driven blob / B-spline projector (projectors/LutProjector.h:85-163): the slice walk of
+    SliceTraversal and lut(distance to the ray) for the voxels within `support` in each slice.
+    The backward walks the box grown by `support`, the forward the volume box, as the
+    reference does."""
+    dim = len(vol_dims)
+    n_out = int(np.prod(vol_dims)) if adjoint else int(np.prod(det_dims))
+    data = np.ascontiguousarray(data, dtype).ravel()
+    out = np.empty(n_out, dtype)
+    lut = _f32(lut)
+    fn = lib().oracle_lut_f64 if dtype == np.float64 else lib().oracle_lut_f32
+    fn(int(adjoint), dim, np.asarray(vol_dims, np.int64), np.asarray(det_dims, np.int64),
+       _f32(poses), lut, lut.size, float(radius), int(support), data, out)
+    return out
 
 
 def joseph_sample_count(vol_dims, det_dims, poses):

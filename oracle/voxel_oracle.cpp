@@ -284,8 +284,9 @@ namespace vox
             bsplineSupport(order), N, out);
     }
 
-    // Lut::operator()(float distance), Luts.hpp:61-80
-    static float lutLerp(const float* lut, index_t N, float support, float distance)
+    // Lut::operator()(float distance), Luts.hpp:61-80 (also used by the ray-driven LutProjector
+    // restatement in oracle.cpp)
+    float lutLerp(const float* lut, index_t N, float support, float distance)
     {
         const float index = (distance / support) * static_cast<float>(N - 1);
         if (index < 0 || index > static_cast<float>(N - 1))

@@ -157,6 +157,63 @@ def binary_cases(O):
     return cases
 
 
+def lut_cases(O):
+    """projectors/tests/test_LutProjector.cpp: the ray-driven blob projector (radius 2, alpha
+    10.83, order 2) on 5x5 / 5^3 volumes, source to centre 100, centre to detector 5. Each case
+    gives the expected detector values as multiples of the blob's weight at given distances and
+    the relative tolerance of the reference check."""
+    lut = O.blob_lut()
+
+    def w(d):
+        return float(O.lut_lerp(lut, 2.0, float(np.float32(d))))
+
+    cases = []
+    # :156-200 centre voxel, one ray, angles 0, 4, ..., 356 degrees
+    x = np.zeros((5, 5), np.float32)
+    x[2, 2] = 1
+    for a in range(0, 360, 4):
+        poses = _pose2d(O, (5, 5), 1, 100.0, 5.0, _rad(a))[None]
+        cases.append(dict(name="lut_center_%d" % a, vol=(5, 5), det=(1, 1), poses=poses, x=x,
+                          y_expect=np.array([w(0)]), tol=1.2e-5))
+    # :203-249 two rays, :252-306 three rays
+    for a in range(0, 360, 4):
+        poses = _pose2d(O, (5, 5), 2, 100.0, 5.0, _rad(a))[None]
+        cases.append(dict(name="lut_two_%d" % a, vol=(5, 5), det=(2, 1), poses=poses, x=x,
+                          y_expect=np.array([w(0.4761878)] * 2), tol=0.01))
+    for a in range(0, 360, 5):
+        poses = _pose2d(O, (5, 5), 3, 100.0, 5.0, _rad(a))[None]
+        cases.append(dict(name="lut_three_%d" % a, vol=(5, 5), det=(3, 1), poses=poses, x=x,
+                          y_expect=np.array([w(0.95233786), w(0), w(0.95233786)]), tol=0.01))
+    # :309-720 stepping of single rays (arrays indexed [y, x] = x(x, y) of the reference)
+    step = [(0, [(2, j) for j in range(5)], 5 * w(0), 1.2e-5),
+            (0, [(3, j) for j in range(5)], 5 * w(1), 1.2e-5),
+            (0, [(1, j) for j in range(5)], 5 * w(1), 1.2e-5),
+            (0, [(4, j) for j in range(5)], 5 * w(2), 1.2e-5),
+            (0, [(0, j) for j in range(5)], 5 * w(2), 1.2e-5),
+            (45, [(i, i) for i in range(5)], 5 * w(0), 1.2e-5),
+            (45, [(0, 1), (1, 2), (2, 3), (3, 4)], 4 * w(0.707106769084930), 0.01),
+            (45, [(1, 0), (2, 1), (3, 2), (4, 3)], 4 * w(0.707106769084930), 0.01),
+            (45, [(0, 2), (1, 3), (2, 4)], 3 * w(2 * 0.707106769084930), 1.2e-5),
+            (45, [(2, 0), (3, 1), (4, 2)], 3 * w(2 * 0.707106769084930), 1.2e-5),
+            (90, [(i, 2) for i in range(5)], 5 * w(0), 1.2e-5),
+            (90, [(i, 3) for i in range(5)], 5 * w(1), 1.2e-5)]
+    for k, (a, vox, val, tol) in enumerate(step):
+        xs = np.zeros((5, 5), np.float32)
+        for (i, j) in vox:
+            xs[j, i] = 1
+        poses = _pose2d(O, (5, 5), 1, 100.0, 5.0, _rad(a))[None]
+        cases.append(dict(name="lut_step_%d_%d" % (a, k), vol=(5, 5), det=(1, 1), poses=poses,
+                          x=xs, y_expect=np.array([val]), tol=tol))
+    # :110-153 3D: centre voxel of a 5^3 volume, Gamma of 0, 4, ..., 356 (radian)
+    x3 = np.zeros((5, 5, 5), np.float32)
+    x3[2, 2, 2] = 1
+    for a in range(0, 360, 4):
+        poses = _pose3d(O, (5, 5, 5), (1, 1), 1, 100.0, 5.0, float(np.float32(a)))[None]
+        cases.append(dict(name="lut_center3d_%d" % a, vol=(5, 5, 5), det=(1, 1, 1), poses=poses,
+                          x=x3, y_expect=np.array([w(0)]), tol=1.2e-5))
+    return cases
+
+
 def voxel_cases(O):
     """projectors/tests/test_BlobVoxelProjector.cpp:25-244: a centre voxel set to 1, projected
     onto one, two or three detector pixels. Expected values are blob LUT weights at the stated

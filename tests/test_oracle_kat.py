@@ -3,7 +3,7 @@ import numpy as np
 import pytest
 
 from conftest import rel_l2
-from kat_cases import binary_cases, joseph_cases, siddon_cases
+from kat_cases import binary_cases, joseph_cases, lut_cases, siddon_cases
 
 
 def _run(O, fn, case, dtype):
@@ -64,6 +64,23 @@ def test_binary_kat(oracle, dtype):
         np.testing.assert_array_equal(y, case["y_expect"], err_msg=case["name"])
         np.testing.assert_array_equal(bp.reshape(case["bp_expect"].shape), case["bp_expect"],
                                       err_msg=case["name"])
+
+
+def _approx_ok(got, want, tol):
+    # doctest Approx: |a - b| < eps * (1 + max(|a|, |b|))
+    return abs(got - want) < tol * (1.0 + max(abs(got), abs(want)))
+
+
+def test_lut_projector_kat(oracle):
+    lut = oracle.blob_lut()
+    bad = []
+    for case in lut_cases(oracle):
+        y = oracle.lut_project(False, case["x"], case["vol"], case["det"], case["poses"], lut,
+                               2.0, 2)
+        for got, want in zip(y, case["y_expect"]):
+            if not _approx_ok(float(got), float(want), case["tol"]):
+                bad.append((case["name"], float(got), float(want)))
+    assert not bad, bad[:10]
 
 
 def test_joseph_outputs_overwritten(oracle):
