@@ -148,14 +148,16 @@ namespace elsa_b200
         }
 
         // Visits the footprint pixels of one voxel in the reference's order; fn(linear pixel
-        // index within the pose, d0, d1).
+        // index within the pose, u, v, d0, d1) with (u, v) the pixel's unwrapped detector
+        // coordinates (u may leave [0, nu) where the reference's linear index wraps into the
+        // next row; visitBox rejects such footprints for the shared patch).
         template <int DIM, class Fn>
         __device__ __forceinline__ void visitFootprint(const Footprint& f, const VoxelParams& vp,
                                                        Fn fn)
         {
             if (DIM == 2) {
                 for (int u = f.lo0; u <= f.hi0; ++u)
-                    fn(u, (f.c0 - static_cast<float>(u)) / f.s, 0.0f);
+                    fn(u, u, 0, (f.c0 - static_cast<float>(u)) / f.s, 0.0f);
                 return;
             }
             const int ext0 = f.hi0 - f.lo0 + 1, ext1 = f.hi1 - f.lo1 + 1;
@@ -167,14 +169,19 @@ namespace elsa_b200
             const int64_t npix = static_cast<int64_t>(vp.nu) * vp.nv;
             int64_t lin = static_cast<int64_t>(f.lo1) * vp.nu + f.lo0;
             float cur0 = static_cast<float>(f.lo0), cur1 = static_cast<float>(f.lo1);
+            int u = f.lo0, v = f.lo1;
             for (int r = 0; r < rows; ++r) {
+                const float d1 = (f.c1 - cur1) / f.s;
                 for (int c = 0; c < cols; ++c) {
                     if (lin >= 0 && lin < npix)
-                        fn(lin, (f.c0 - cur0) / f.s, (f.c1 - cur1) / f.s);
+                        fn(lin, u, v, (f.c0 - cur0) / f.s, d1);
                     lin += 1;
+                    u += 1;
                     cur0 = cur0 + 1.0f;
                 }
                 lin += vp.nu - ext0;
+                u -= ext0;
+                v += 1;
                 cur0 = cur0 - static_cast<float>(ext0);
                 cur1 = cur1 + 1.0f;
             }
@@ -207,7 +214,7 @@ namespace elsa_b200
                 const Footprint f = footprint<DIM>(poses + static_cast<int64_t>(p) * 40, ix, iy,
                                                    iz, vp);
                 const float* view = y + p * npix;
-                visitFootprint<DIM>(f, vp, [&](int64_t pix, float d0, float d1) {
+                visitFootprint<DIM>(f, vp, [&](int64_t pix, int pu_, int pv_, float d0, float d1) {
                     const float w = voxelWeight<DIM>(lut, vp, d0, d1);
                     acc = acc + w * __ldg(view + pix);
                 });
@@ -299,13 +306,13 @@ namespace elsa_b200
             __syncthreads();
             if (active) {
                 const bool toPatch = usePatch && boxed;
-                visitFootprint<DIM>(f, vp, [&](int64_t pix, float d0, float d1) {
+                visitFootprint<DIM>(f, vp, [&](int64_t pix, int pu_, int pv_, float d0, float d1) {
                     const float w = voxelWeight<DIM>(lut, vp, d0, d1);
                     const float c = xv * w;
                     if (toPatch) {
-                        const int pu = static_cast<int>(pix % vp.nu) - bu0;
-                        const int pv = static_cast<int>(pix / vp.nu) - bv0;
-                        atomicAdd(&patch[pv * pw + pu], c);
+                        // a boxed footprint stays inside its rows: the unwrapped coordinates
+                        // are the pixel's own
+                        atomicAdd(&patch[(pv_ - bv0) * pw + (pu_ - bu0)], c);
                     } else {
                         atomicAdd(view + pix, c);
                     }
