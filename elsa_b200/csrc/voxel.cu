@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 
 namespace elsa_b200
 {
@@ -45,6 +46,7 @@ namespace elsa_b200
             int mode;       // FootprintMode
             float radius;   // LUT support
             int nu, nv;     // detector pixels per pose (nv = 1 in 2D)
+            float invRadius; // 1 / radius when radius is a power of two, else 0
         };
 
         struct Footprint {
@@ -119,16 +121,21 @@ namespace elsa_b200
             return f;
         }
 
-        // Lut::operator()(float), Luts.hpp:61-80, on a table in shared memory.
-        __device__ __forceinline__ float lutAt(const float* lut, float support, float distance)
+        // Lut::operator()(float), Luts.hpp:61-80, on a table in shared memory. invSupport: 1 /
+        // support when support is a power of two (then distance * invSupport is exactly
+        // distance / support), else 0. ceil(index) is floor(index) + (index > floor(index)).
+        __device__ __forceinline__ float lutAt(const float* lut, float support, float invSupport,
+                                               float distance)
         {
-            const float index = (distance / support) * static_cast<float>(kVoxelLutSize - 1);
+            const float q = invSupport != 0.0f ? distance * invSupport : distance / support;
+            const float index = q * static_cast<float>(kVoxelLutSize - 1);
             if (index < 0.0f || index > static_cast<float>(kVoxelLutSize - 1))
                 return 0.0f;
-            const int a = static_cast<int>(floorf(index));
-            const int b = static_cast<int>(ceilf(index));
+            const float af = floorf(index);
+            const int a = static_cast<int>(af);
+            const int b = a + (index > af ? 1 : 0);
             const float fa = lut[a], fb = lut[b];
-            const float t = index - static_cast<float>(a);
+            const float t = index - af;
             return t * fb + (1.0f - t) * fa;
         }
 
@@ -139,7 +146,7 @@ namespace elsa_b200
             float n2 = d0 * d0;
             if (DIM == 3)
                 n2 = n2 + d1 * d1;
-            const float v = lutAt(lut, vp.radius, sqrtf(n2));
+            const float v = lutAt(lut, vp.radius, vp.invRadius, sqrtf(n2));
             if (vp.weightKind == 0)
                 return v;
             if (DIM == 2)
@@ -348,6 +355,11 @@ namespace elsa_b200
                 vp_.radius = lut.support;
                 vp_.nu = det.nu;
                 vp_.nv = det.nv;
+                {
+                    int e = 0;
+                    const float m = std::frexp(lut.support, &e);
+                    vp_.invRadius = (m == 0.5f) ? std::ldexp(1.0f, 1 - e) : 0.0f;
+                }
                 nBricks_ = make_int3((vol.n[0] + kBX - 1) / kBX, (vol.n[1] + kBY - 1) / kBY,
                                      (vol.n[2] + kBZ - 1) / kBZ);
                 if (det.np > 65535)
