@@ -381,6 +381,62 @@ def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, st
             "timing": "host wall clock around synchronized device work, graph capture included"}
 
 
+SECONDARY = {
+    # name: (projector kind, volume, views, detector, params, source-centre, centre-detector)
+    "siddon256": ("SIDDON", (256, 256, 256), 360, [384, 384], None, 2560, 640),
+    "blob128": ("BLOB", (128, 128, 128), 180, [192, 192], [2.0, 10.83, 2.0], 1280, 320),
+    "bspline128": ("BSPLINE", (128, 128, 128), 180, [192, 192], [2.0], 1280, 320),
+    "phase_blob128": ("PHASE_CONTRAST_BLOB", (128, 128, 128), 180, [192, 192],
+                      [2.0, 10.83, 2.0], 1280, 320),
+    "phase_bspline128": ("PHASE_CONTRAST_BSPLINE", (128, 128, 128), 180, [192, 192], [2.0],
+                         1280, 320),
+    "joseph2d128": ("JOSEPH", (128, 128), 180, [182], None, 1000, 250),
+    "binary2d128": ("BINARY", (128, 128), 180, [182], None, 1000, 250),
+    "rayblob64": ("RAY_BLOB", (64, 64, 64), 60, [96, 96], [2.0, 10.83, 2.0], 640, 160),
+}
+
+
+def run_secondary(args):
+    """Forward / adjoint times of the other projector workloads (CUDA events, mean of 5 calls
+    after 3 warm-up calls, random inputs); one JSON line."""
+    import torch
+    import elsa_b200
+    torch.cuda.set_device(0)
+    names = list(SECONDARY) if args.secondary == "all" else args.secondary.split(",")
+    s = torch.cuda.current_stream().cuda_stream
+    out = {"secondary": {}}
+    for name in names:
+        kind, vol, views, det, params, s2c, c2d = SECONDARY[name]
+        poses, dd = elsa_b200.circle_trajectory(vol, views, 360, s2c, c2d, det)
+        p = elsa_b200.Projector(getattr(elsa_b200, "PROJECTOR_" + kind), vol, dd, poses, params)
+        x = torch.rand(p.domain_size, device="cuda")
+        y = torch.rand(p.range_size, device="cuda")
+        oy, ox = torch.empty_like(y), torch.empty_like(x)
+
+        def timed(fn):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(5):
+                fn()
+            b.record()
+            torch.cuda.synchronize()
+            return a.elapsed_time(b) / 5
+
+        fwd = timed(lambda: p.apply_ptr(x.data_ptr(), oy.data_ptr(), s))
+        adj = timed(lambda: p.apply_adjoint_ptr(y.data_ptr(), ox.data_ptr(), s))
+        nvox = int(np.prod(vol))
+        out["secondary"][name] = {
+            "volume": [int(v) for v in vol], "views": int(views),
+            "detector": [int(v) for v in dd[:-1]],
+            "forward_ms": round(fwd, 3), "adjoint_ms": round(adj, 3),
+            "gups": round(2 * nvox * views / ((fwd + adj) / 1e3) / 1e9, 3)}
+        p.close()
+    print(json.dumps(out))
+
+
 def run_reference(args):
     world, rank, local = _dist()
     if rank != 0:
@@ -433,11 +489,17 @@ def main():
     ap.add_argument("--batched-full", action="store_true",
                     help="also time the full batched workload (64 reconstructions of edges "
                          "64-256, 60-360 views, 50 CG iterations each; several minutes)")
+    ap.add_argument("--secondary", default=None,
+                    help="time other projector workloads instead ('all' or a comma list of: %s)"
+                         % ", ".join(SECONDARY))
     ap.add_argument("--size", type=int, default=256,
                     help="volume edge (profiling only; the benchmark workload is 256)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.secondary:
+        run_secondary(args)
+        return
     if args.impl == "reference":
         if args.cpu_views is None:
             # about 0.17 s per view (forward + adjoint) on 16 host threads
