@@ -25,7 +25,8 @@ namespace elsa_b200
         kKnobForwardThreads = 0, // rays per block of a thread-per-ray forward kernel
         kKnobAdjointChunks = 1,  // view chunks of a brick-owner adjoint (partial volumes)
         kKnobAdjointThreads = 2, // voxels per block of a thread-per-voxel adjoint kernel
-        kKnobCount = 3
+        kKnobAdjointScatter = 3, // 0: deterministic brick-owner adjoint, 1: atomic scatter
+        kKnobCount = 4
     };
 
     // A curved (cylindrical) detector: opening angle (radian) and source-to-detector distance

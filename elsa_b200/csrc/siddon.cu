@@ -12,7 +12,11 @@
 //
 // Forward: one thread per ray, voxels gathered through the read-only cache.
 //
-// Adjoint: atomic-free and deterministic, on the brick-owner scheme of the Joseph adjoint. One
+// Adjoint, two kernels (launch knob kKnobAdjointScatter). The scatter kernel replays each ray
+// like the forward, one thread per ray, and adds y * weight to every visited voxel with a
+// fire-and-forget atomic: the reference's own scheme, with an addition order that varies from run
+// to run. The brick-owner kernel is atomic-free and deterministic:
+// on the brick-owner scheme of the Joseph adjoint. One
 // warp owns a 16^3 brick in shared memory for all views. Rays are cut into slabs of 16 voxels
 // along their axis g of largest |direction|; per (ray, slab) a checkpoint holds the traversal
 // state (T of every axis, entry parameter, voxel) at the ray's first visit inside the slab,
@@ -36,6 +40,7 @@ namespace elsa_b200
     namespace
     {
         constexpr int kForwardThreads = 128;    // default rays per block of the forward
+        constexpr int kScatterThreads = 256;    // rays per block of the scatter adjoint
         constexpr int kMaxForwardThreads = 512; // largest block the autotuner may choose
         constexpr int kAdjointWarpsPerSm = 22;  // view-chunk target of the warp-brick adjoint
         constexpr int kMinAdjointChunks = 32;   // default floor of the view chunks
@@ -135,9 +140,63 @@ namespace elsa_b200
             y[r] = acc;
         }
 
+        // Adjoint by atomic scatter: the forward's visit loop, adding y[r] * weight to each
+        // visited voxel (x zeroed beforehand). The atomics' return values are unused, so they
+        // compile to reductions that do not wait for the memory system.
+        template <int DIM>
+        __global__ void __launch_bounds__(kScatterThreads)
+            siddonScatterKernel(const SiddonRay* __restrict__ rays, int64_t nrays,
+                                const float* __restrict__ y, VolumeShape vol, int binary,
+                                float* __restrict__ x)
+        {
+            const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (r >= nrays)
+                return;
+            const float yr = __ldg(y + r);
+            const SiddonRay R = rays[r];
+            if (!(R.meta & kActive) || yr == 0.0f)
+                return;
+            const int g = R.meta & 3;
+            int c0, c1, c2;
+            entryVoxel(g, R.kFirst, R.cur[0], R.cur[1], c0, c1, c2);
+            const int s0 = axisStep(R.meta, 0), s1 = axisStep(R.meta, 1), s2 = axisStep(R.meta, 2);
+            const int nx = vol.n[0], ny = vol.n[1], nz = vol.n[2];
+            const int64_t sy = nx, sz = static_cast<int64_t>(nx) * ny;
+            int64_t idx = c0 + sy * c1 + (DIM == 3 ? sz * c2 : 0);
+            float T0 = R.T[0], T1 = R.T[1], T2 = R.T[2];
+            float tExit = 0.0f;
+            const int maxVisits = nx + ny + (DIM == 3 ? nz : 0) + 3;
+            for (int it = 0; it < maxVisits; ++it) {
+                const float tEntry = tExit;
+                bool m0, m1, m2;
+                tExit = nextCrossing<DIM>(T0, T1, T2, m0, m1, m2);
+                if (m0) {
+                    c0 += s0;
+                    T0 = __fadd_rn(T0, R.tDelta[0]);
+                }
+                if (m1) {
+                    c1 += s1;
+                    T1 = __fadd_rn(T1, R.tDelta[1]);
+                }
+                if (m2) {
+                    c2 += s2;
+                    T2 = __fadd_rn(T2, R.tDelta[2]);
+                }
+                const bool inside = static_cast<unsigned>(c0) < static_cast<unsigned>(nx) &&
+                                    static_cast<unsigned>(c1) < static_cast<unsigned>(ny) &&
+                                    (DIM < 3 || static_cast<unsigned>(c2) < static_cast<unsigned>(nz));
+                const float w = binary ? 1.0f : __fsub_rn(tExit, tEntry);
+                atomicAdd(x + idx, __fmul_rn(yr, w));
+                if (!inside)
+                    break;
+                idx += (m0 ? s0 : 0) + (m1 ? s1 * sy : 0) + (m2 ? s2 * sz : 0);
+            }
+        }
+
         // Replays every ray once: writes the traversal state at the ray's first visit in each
-        // slab of kSlab voxels along g (slab-major, row floor(k/kSlab) + 1, column = ray), the
-        // last visited index along g and the visit count (SiddonsMethod's sample count).
+        // slab of kSlab voxels along g (slab-major, row floor(k/kSlab) + 1, column = ray; skipped
+        // when cpState is null), the last visited index along g and the visit count
+        // (SiddonsMethod's sample count; skipped when visits is null).
         template <int DIM>
         __global__ void siddonCheckpointKernel(SiddonRay* __restrict__ rays, int64_t nrays,
                                                VolumeShape vol, int slabRows,
@@ -168,7 +227,7 @@ namespace elsa_b200
                 const int s = floorDiv(cg, kSlab);
                 if (s != slab) {
                     slab = s;
-                    if (s + 1 >= 0 && s + 1 < slabRows) {
+                    if (cpState != nullptr && s + 1 >= 0 && s + 1 < slabRows) {
                         const int ca = a == 0 ? c0 : c1;
                         const int cb = DIM == 3 ? (b == 1 ? c1 : c2) : 0;
                         const int64_t at = static_cast<int64_t>(s + 1) * nrays + r;
@@ -203,7 +262,8 @@ namespace elsa_b200
             R.kLast = kLast;
             R.crossings = count;
             rays[r] = R;
-            atomicAdd(visits, static_cast<unsigned long long>(count));
+            if (visits != nullptr)
+                atomicAdd(visits, static_cast<unsigned long long>(count));
         }
 
         // True when rays R and S (same axis g) stay more than two voxels apart in one lateral
@@ -445,7 +505,8 @@ namespace elsa_b200
             SiddonProjector(const VolumeShape& vol, const DetectorShape& det,
                             const std::vector<PoseRecord>& poses, bool binary,
                             const CurvedDetector& curved)
-                : Projector(binary ? 6 : 1, vol, det, poses), binary_(binary ? 1 : 0)
+                : Projector(binary ? 6 : 1, vol, det, poses), binary_(binary ? 1 : 0),
+                  curved_(curved)
             {
                 CurvedTables tables(vol.dim, det, curved); // used while setting up
                 const int maxDim = std::max(vol_.n[0], std::max(vol_.n[1], vol_.n[2]));
@@ -463,8 +524,6 @@ namespace elsa_b200
                 ELSA_LAUNCH_CHECK("siddonSetupKernel");
 
                 cpRows_ = maxDim / kSlab + 3;
-                cpState_ = std::make_unique<DeviceBuffer>(sizeof(float4) * nrays * cpRows_);
-                cpVoxel_ = std::make_unique<DeviceBuffer>(sizeof(unsigned) * nrays * cpRows_);
                 // per-view axis masks, the bad-spacing mask and a 64-bit visit counter
                 const size_t words = static_cast<size_t>(det_.np) + 4;
                 viewAxes_ = std::make_unique<DeviceBuffer>(sizeof(unsigned) * words);
@@ -473,14 +532,14 @@ namespace elsa_b200
                 unsigned* dBad = dAxes + det_.np;
                 auto* dCount =
                     reinterpret_cast<unsigned long long*>(dAxes + ((det_.np + 2) & ~1));
+                // last visited slice and visit count of every ray; the checkpoints themselves are
+                // written once the brick-owner adjoint is selected (buildOwner)
                 if (vol_.dim == 3)
                     siddonCheckpointKernel<3><<<blocks, threads>>>(
-                        rays_->as<SiddonRay>(), nrays, vol_, cpRows_, cpState_->as<float4>(),
-                        cpVoxel_->as<unsigned>(), dCount);
+                        rays_->as<SiddonRay>(), nrays, vol_, cpRows_, nullptr, nullptr, dCount);
                 else
                     siddonCheckpointKernel<2><<<blocks, threads>>>(
-                        rays_->as<SiddonRay>(), nrays, vol_, cpRows_, cpState_->as<float4>(),
-                        cpVoxel_->as<unsigned>(), dCount);
+                        rays_->as<SiddonRay>(), nrays, vol_, cpRows_, nullptr, nullptr, dCount);
                 ELSA_LAUNCH_CHECK("siddonCheckpointKernel");
                 siddonClassCheckKernel<<<blocks, threads>>>(rays_->as<SiddonRay>(),
                                                             lines.as<SiddonLine>(), det_,
@@ -491,26 +550,18 @@ namespace elsa_b200
                 ELSA_CUDA(cudaMemcpy(&bad, dBad, sizeof(unsigned), cudaMemcpyDeviceToHost));
                 ELSA_CUDA(cudaMemcpy(&count, dCount, sizeof(count), cudaMemcpyDeviceToHost));
                 visits_ = static_cast<int64_t>(count);
+                // class spacing of the brick-owner adjoint; 0 when neighbouring detector rays pass
+                // within two voxels of each other even eight pixels apart (only the scatter
+                // adjoint is available then)
                 for (int m = kMinClass; m <= kMaxClass; ++m)
                     if (!((bad >> m) & 1u)) {
                         classSpacing_ = m;
                         break;
                     }
-                if (classSpacing_ == 0)
-                    throw Error(ELSA_ERROR_NOT_SUPPORTED,
-                                "SiddonsMethod: neighbouring detector rays pass within two voxels "
-                                "of each other even eight pixels apart; the atomic-free adjoint "
-                                "needs a coarser detector");
-
                 const int bz = vol_.dim == 3 ? kSlab : 1;
                 nBricks_ = make_int3((vol_.n[0] + kSlab - 1) / kSlab,
                                      (vol_.n[1] + kSlab - 1) / kSlab, (vol_.n[2] + bz - 1) / bz);
-                const int64_t nwin =
-                    static_cast<int64_t>(nBricks_.x) * nBricks_.y * nBricks_.z * det_.np;
-                windows_ = std::make_unique<DeviceBuffer>(sizeof(RayWindow) * nwin);
-                launchBrickWindows(dPoses_, vol_, det_, make_int3(kSlab, kSlab, bz), nBricks_,
-                                   windows_->as<RayWindow>(), nullptr, tables.map());
-                setKnob(kKnobAdjointChunks, defaultChunks());
+                adjointChunks_ = defaultChunks();
                 ELSA_CUDA(cudaDeviceSynchronize());
             }
 
@@ -530,6 +581,22 @@ namespace elsa_b200
 
             void adjoint(const float* y, float* x, cudaStream_t s) override
             {
+                if (scatter_) {
+                    const int64_t nrays = rangeSize_;
+                    const unsigned blocks =
+                        static_cast<unsigned>((nrays + kScatterThreads - 1) / kScatterThreads);
+                    ELSA_CUDA(cudaMemsetAsync(x, 0, sizeof(float) * domainSize_, s));
+                    if (vol_.dim == 3)
+                        siddonScatterKernel<3><<<blocks, kScatterThreads, 0, s>>>(
+                            rays_->as<SiddonRay>(), nrays, y, vol_, binary_, x);
+                    else
+                        siddonScatterKernel<2><<<blocks, kScatterThreads, 0, s>>>(
+                            rays_->as<SiddonRay>(), nrays, y, vol_, binary_, x);
+                    ELSA_LAUNCH_CHECK("siddonScatterKernel");
+                    return;
+                }
+                if (!cpState_)
+                    throw Error(ELSA_ERROR_LOGIC, "SiddonsMethod: brick-owner adjoint not built");
                 const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
                 const int per = (det_.np + adjointChunks_ - 1) / adjointChunks_;
                 const int used = (det_.np + per - 1) / per;
@@ -564,7 +631,7 @@ namespace elsa_b200
                 case 6: // kernel launches per forward call
                     return 1;
                 case 7: // kernel launches per adjoint call (with view chunks: + the chunk sum)
-                    return adjointChunks_ > 1 ? 2 : 1;
+                    return (!scatter_ && adjointChunks_ > 1) ? 2 : 1;
                 default:
                     return -1;
                 }
@@ -573,6 +640,8 @@ namespace elsa_b200
             std::vector<int> knobCandidates(int knob) const override
             {
                 if (knob == kKnobAdjointChunks) {
+                    if (scatter_)
+                        return {}; // chunks only exist in the brick-owner adjoint
                     // partial volumes limited to 4 GiB
                     const int64_t byMemory =
                         std::max<int64_t>(1, (int64_t(1) << 32) / (4 * domainSize_));
@@ -582,6 +651,8 @@ namespace elsa_b200
                 }
                 if (knob == kKnobForwardThreads)
                     return {64, 128, 256, 512};
+                if (knob == kKnobAdjointScatter)
+                    return classSpacing_ > 0 ? std::vector<int>{0, 1} : std::vector<int>{1};
                 return {};
             }
 
@@ -591,6 +662,8 @@ namespace elsa_b200
                     return adjointChunks_;
                 if (knob == kKnobForwardThreads)
                     return forwardThreads_;
+                if (knob == kKnobAdjointScatter)
+                    return scatter_;
                 return -1;
             }
 
@@ -608,18 +681,66 @@ namespace elsa_b200
                     forwardThreads_ = value;
                     return;
                 }
+                if (knob == kKnobAdjointScatter) {
+                    if (value == 0)
+                        buildOwner();
+                    else
+                        releaseOwner();
+                    scatter_ = value;
+                } else {
+                    adjointChunks_ = value;
+                }
+                // the partial volumes exist only while the brick-owner adjoint uses chunks
                 const size_t need = sizeof(float) * static_cast<size_t>(domainSize_) *
-                                    static_cast<size_t>(value);
-                if (value <= 1)
+                                    static_cast<size_t>(adjointChunks_);
+                if (scatter_ || adjointChunks_ <= 1)
                     partial_.reset();
                 else if (!partial_ || partial_->bytes() < need) {
                     partial_.reset();
                     partial_ = std::make_unique<DeviceBuffer>(need);
                 }
-                adjointChunks_ = value;
             }
 
         private:
+            // Per-(ray, slab) checkpoints (16 + 4 bytes per ray and slab: about 20 GB at
+            // 256^3 / 360 x 384^2) and per-(brick, view) ray windows of the brick-owner adjoint,
+            // built when that adjoint is selected and released when the scatter adjoint is.
+            void buildOwner()
+            {
+                if (cpState_)
+                    return;
+                const int64_t nrays = rangeSize_;
+                const int threads = 256;
+                const unsigned blocks = static_cast<unsigned>((nrays + threads - 1) / threads);
+                cpState_ = std::make_unique<DeviceBuffer>(sizeof(float4) * nrays * cpRows_);
+                cpVoxel_ = std::make_unique<DeviceBuffer>(sizeof(unsigned) * nrays * cpRows_);
+                if (vol_.dim == 3)
+                    siddonCheckpointKernel<3><<<blocks, threads>>>(
+                        rays_->as<SiddonRay>(), nrays, vol_, cpRows_, cpState_->as<float4>(),
+                        cpVoxel_->as<unsigned>(), nullptr);
+                else
+                    siddonCheckpointKernel<2><<<blocks, threads>>>(
+                        rays_->as<SiddonRay>(), nrays, vol_, cpRows_, cpState_->as<float4>(),
+                        cpVoxel_->as<unsigned>(), nullptr);
+                ELSA_LAUNCH_CHECK("siddonCheckpointKernel");
+                const int bz = vol_.dim == 3 ? kSlab : 1;
+                const int64_t nwin =
+                    static_cast<int64_t>(nBricks_.x) * nBricks_.y * nBricks_.z * det_.np;
+                windows_ = std::make_unique<DeviceBuffer>(sizeof(RayWindow) * nwin);
+                CurvedTables tables(vol_.dim, det_, curved_);
+                launchBrickWindows(dPoses_, vol_, det_, make_int3(kSlab, kSlab, bz), nBricks_,
+                                   windows_->as<RayWindow>(), nullptr, tables.map());
+                ELSA_CUDA(cudaDeviceSynchronize());
+            }
+
+            void releaseOwner()
+            {
+                ELSA_CUDA(cudaDeviceSynchronize());
+                cpState_.reset();
+                cpVoxel_.reset();
+                windows_.reset();
+            }
+
             // View chunks: enough for bricks x chunks to reach kAdjointWarpsPerSm one-warp CTAs
             // per SM and at least kMinAdjointChunks, within kChunkMemory of partial volumes
             // (256^3 / 360 views: 103.8 ms with 1 chunk, 85.5 with 32).
@@ -635,8 +756,10 @@ namespace elsa_b200
 
             std::unique_ptr<DeviceBuffer> partial_; // adjoint: per view-chunk partial volumes
             int adjointChunks_ = 1;
+            int scatter_ = 1; // the atomic scatter adjoint by default (2.6x faster at 256^3)
             int forwardThreads_ = kForwardThreads;
             int binary_ = 0;
+            CurvedDetector curved_;
             std::unique_ptr<DeviceBuffer> rays_, cpState_, cpVoxel_, viewAxes_, windows_;
             int cpRows_ = 0;
             int classSpacing_ = 0;

@@ -89,7 +89,7 @@ namespace elsa_b200
         if (!force && tuneCacheGet(key, cached)) {
             for (int k = 0; k < kKnobCount; ++k) {
                 const std::vector<int> cand = p.knobCandidates(k);
-                if (cached[k] >= 1 && std::find(cand.begin(), cand.end(), cached[k]) != cand.end())
+                if (cached[k] >= 0 && std::find(cand.begin(), cand.end(), cached[k]) != cand.end())
                     p.setKnob(k, cached[k]);
                 res.values[k] = p.knob(k);
             }

@@ -65,9 +65,10 @@ def test_batch_matches_plain(cuda, oracle, solver_kind):
 def _compare(kinds, xs_plain, xs_batch):
     import elsa_b200
     for (kind, _), a, b in zip(kinds, xs_plain, xs_batch):
-        if kind in (elsa_b200.PROJECTOR_JOSEPH, elsa_b200.PROJECTOR_SIDDON):
+        if kind == elsa_b200.PROJECTOR_JOSEPH:
             assert bool((a == b).all()), kind
         else:
+            # Siddon's default adjoint scatters with atomics: the order of its additions varies
             assert float((a - b).norm() / a.norm()) <= 1e-4, kind
 
 

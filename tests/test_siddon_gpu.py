@@ -83,15 +83,55 @@ def test_siddon_adjointness_and_determinism(cuda, oracle, name):
     rng = np.random.default_rng(12)
     x = rng.uniform(0, 1, int(np.prod(c["vol"]))).astype(np.float32)
     y = rng.uniform(0, 1, int(np.prod(det))).astype(np.float32)
-    Ax, Aty = _gpu_pair(cuda, proj, x, y)
+    import elsa_b200
+    Ax, Aty = _gpu_pair(cuda, proj, x, y)  # the default scatter adjoint
     lhs = float(Ax.astype(np.float64) @ y)
     rhs = float(x.astype(np.float64) @ Aty)
     assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
+    # the brick-owner adjoint is bit-reproducible; the forward always is
+    proj.set_knob(elsa_b200.KNOB_ADJOINT_SCATTER, 0)
+    Ax1, Aty1 = _gpu_pair(cuda, proj, x, y)
     Ax2, Aty2 = _gpu_pair(cuda, proj, x, y)
-    assert np.array_equal(Aty.view(np.uint32), Aty2.view(np.uint32))
+    assert np.array_equal(Aty1.view(np.uint32), Aty2.view(np.uint32))
     assert np.array_equal(Ax.view(np.uint32), Ax2.view(np.uint32))
+    assert rel_l2(Aty, Aty1) <= 1e-6
     # visit count agrees with the oracle's crossing count
     assert proj.info(2) == oracle.siddon_visit_count(c["vol"], det, poses)
+
+
+@pytest.mark.parametrize("binary", [False, True])
+@pytest.mark.parametrize("name", sorted(CONFIGS))
+def test_scatter_adjoint_parity(cuda, oracle, name, binary):
+    """The atomic-scatter adjoint (knob ADJOINT_SCATTER = 1) against the oracle and the
+    deterministic brick-owner adjoint: the same sums in another order."""
+    import elsa_b200
+    c = CONFIGS[name]
+    poses, det = oracle.circle_trajectory(c["vol"], c["views"], c.get("arc", 360), c["s2c"],
+                                          c["c2d"], c["det"])
+    kind = elsa_b200.PROJECTOR_BINARY if binary else elsa_b200.PROJECTOR_SIDDON
+    proj = elsa_b200.Projector(kind, c["vol"], det, poses)
+    rng = np.random.default_rng(13)
+    x = rng.uniform(0, 1, int(np.prod(c["vol"]))).astype(np.float32)
+    y = rng.uniform(0, 1, int(np.prod(det))).astype(np.float32)
+    y[::7] = 0.0  # rays with nothing to add are skipped
+    assert proj.knob(elsa_b200.KNOB_ADJOINT_SCATTER) == 1 and proj.info(7) == 1  # default
+    assert proj.knob_candidates(elsa_b200.KNOB_ADJOINT_CHUNKS) == []
+    _, a_scatter = _gpu_pair(cuda, proj, x, y)
+    proj.set_knob(elsa_b200.KNOB_ADJOINT_SCATTER, 0)  # builds the brick-owner adjoint
+    assert proj.knob_candidates(elsa_b200.KNOB_ADJOINT_CHUNKS)
+    _, a_owner = _gpu_pair(cuda, proj, x, y)
+    adj = oracle.binary_adjoint if binary else oracle.siddon_adjoint
+    ref = adj(y, c["vol"], det, poses)
+    assert rel_l2(a_scatter, ref) <= PARITY, name
+    assert rel_l2(a_scatter, a_owner) <= 1e-6, name
+    assert rel_l2(a_owner, ref) <= PARITY, name
+    # back to scatter (the owner's buffers are released) and once more to the owner
+    proj.set_knob(elsa_b200.KNOB_ADJOINT_SCATTER, 1)
+    _, a_again = _gpu_pair(cuda, proj, x, y)
+    assert rel_l2(a_again, a_scatter) <= 1e-6, name
+    proj.set_knob(elsa_b200.KNOB_ADJOINT_SCATTER, 0)
+    _, a_back = _gpu_pair(cuda, proj, x, y)
+    assert np.array_equal(a_back.view(np.uint32), a_owner.view(np.uint32))
 
 
 def test_siddon_cgls(cuda, oracle):

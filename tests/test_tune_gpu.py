@@ -60,7 +60,7 @@ def test_every_knob_value_is_the_same_operator(cuda, oracle, name):
     assert rel_l2(f0, rf) <= PARITY and rel_l2(a0, ra) <= PARITY
     tunable = 0
     for knob in (elsa_b200.KNOB_FORWARD_THREADS, elsa_b200.KNOB_ADJOINT_CHUNKS,
-                 elsa_b200.KNOB_ADJOINT_THREADS):
+                 elsa_b200.KNOB_ADJOINT_THREADS, elsa_b200.KNOB_ADJOINT_SCATTER):
         cands = proj.knob_candidates(knob)
         if not cands:
             continue
@@ -77,8 +77,8 @@ def test_every_knob_value_is_the_same_operator(cuda, oracle, name):
                 assert np.array_equal(f, f0), (name, v)
             if knob == elsa_b200.KNOB_ADJOINT_THREADS:
                 assert np.array_equal(a, a0), (name, v)
-            if knob == elsa_b200.KNOB_ADJOINT_CHUNKS:
-                # only the order of adding the chunks' partial volumes changes
+            if knob in (elsa_b200.KNOB_ADJOINT_CHUNKS, elsa_b200.KNOB_ADJOINT_SCATTER):
+                # only the order of the additions changes
                 assert rel_l2(a, a0) <= 1e-6, (name, v)
         proj.set_knob(knob, default)
         with pytest.raises(elsa_b200.InvalidArgumentError):
@@ -95,7 +95,7 @@ def test_autotune_and_cache(cuda, oracle, name):
     s = cuda.cuda.current_stream().cuda_stream
     values, hit = proj.autotune(s)
     assert not hit
-    for k, key in enumerate(("forward_threads", "adjoint_chunks", "adjoint_threads")):
+    for k, key in enumerate(elsa_b200._capi.KNOB_NAMES):
         cands = proj.knob_candidates(k)
         if cands:
             assert values[key] in cands
