@@ -19,13 +19,18 @@
 // Forward: one thread per ray, samples gathered through the read-only cache (the volume is
 // L2-resident: 67 MB at 256^3 against a 126 MB L2).
 //
-// Adjoint: atomic-free and deterministic. Each CTA owns one brick of the volume in shared memory
+// Adjoint (default): atomic-free and deterministic. Each CTA owns one brick of the volume in shared memory
 // for all views. For every view it visits the rays of the brick's detector window one
 // conflict-free class at a time: rays whose pixel indices are congruent modulo m stay more than
 // two voxels apart on every plane (m is validated per geometry at construction), so their
 // bilinear taps never overlap and the threads update shared memory without atomics. Each thread
 // walks one ray through the brick; classes are separated by barriers. Every voxel receives its
 // contributions in a fixed order, with exactly the positions and weights of the forward kernel.
+// The launch knob kKnobAdjointScatter = 1 selects a thread-per-ray scatter instead (the forward's
+// sample loop with atomic adds to the four taps): faster in 2D, slower in 3D, where four global
+// atomics per sample exceed what the L2 sustains. A shared-memory variant (several warps per
+// brick adding with shared atomics, no ray classes) measured 65.5 ms against 54.8 ms at
+// 256^3 / 360 views and was dropped.
 #include "joseph_tma.cuh"
 #include "projector.hpp"
 #include "raysetup.cuh"
@@ -133,6 +138,67 @@ namespace elsa_b200
                 }
             }
             y[r] = R.len * acc;
+        }
+
+        // Adjoint by atomic scatter: the forward's sample loop, one thread per ray, adding
+        // y[r] * len * (tap weight) to the in-volume taps of every sample (x zeroed beforehand);
+        // the tap values are those of the brick-owner adjoint, the order of the additions varies.
+        template <int DIM>
+        __global__ void __launch_bounds__(kMaxForwardThreads)
+            josephScatterKernel(const JosephRay* __restrict__ rays, int64_t nrays,
+                                const float* __restrict__ y, VolumeShape vol,
+                                float* __restrict__ x)
+        {
+            const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (r >= nrays)
+                return;
+            const JosephRay R = rays[r];
+            if (R.n == 0)
+                return;
+            const float yl = __ldg(y + r) * R.len;
+            if (yl == 0.0f)
+                return;
+            const int g = R.meta & 3;
+            const int dir = (R.meta & 4) ? -1 : 1;
+            int a, b;
+            nonDrivingAxes(g, a, b);
+            const int64_t plane = static_cast<int64_t>(vol.n[0]) * vol.n[1];
+            const int64_t sg = g == 0 ? 1 : (g == 1 ? vol.n[0] : plane);
+            const int64_t sa = a == 0 ? 1 : (a == 1 ? vol.n[0] : plane);
+            const int ng = g == 0 ? vol.n[0] : (g == 1 ? vol.n[1] : vol.n[2]);
+            const int na = a == 0 ? vol.n[0] : (a == 1 ? vol.n[1] : vol.n[2]);
+            const int64_t sb = DIM == 3 ? (b == 1 ? vol.n[0] : plane) : 0;
+            const int nb = DIM == 3 ? (b == 1 ? vol.n[1] : vol.n[2]) : 1;
+            float pa = R.pa, pb = R.pb;
+            int k = R.k0;
+            for (int j = 0; j < R.n; ++j, k += dir, pa = __fadd_rn(pa, R.sa),
+                     pb = __fadd_rn(pb, R.sb)) {
+                if (static_cast<unsigned>(k) >= static_cast<unsigned>(ng))
+                    continue;
+                Weights w;
+                tapWeights(pa, pb, w);
+                float* base = x + k * sg;
+                const bool a0 = static_cast<unsigned>(w.ia) < static_cast<unsigned>(na);
+                const bool a1 = static_cast<unsigned>(w.ia + 1) < static_cast<unsigned>(na);
+                if (DIM == 2) {
+                    if (a0)
+                        atomicAdd(base + w.ia * sa, yl * w.wa);
+                    if (a1)
+                        atomicAdd(base + (w.ia + 1) * sa, yl * w.cwa);
+                } else {
+                    const bool b0 = static_cast<unsigned>(w.ib) < static_cast<unsigned>(nb);
+                    const bool b1 = static_cast<unsigned>(w.ib + 1) < static_cast<unsigned>(nb);
+                    float* p0 = base + w.ia * sa + w.ib * sb;
+                    if (a0 && b0)
+                        atomicAdd(p0, yl * (w.wa * w.wb));
+                    if (a1 && b0)
+                        atomicAdd(p0 + sa, yl * (w.cwa * w.wb));
+                    if (a0 && b1)
+                        atomicAdd(p0 + sb, yl * (w.wa * w.cwb));
+                    if (a1 && b1)
+                        atomicAdd(p0 + sa + sb, yl * (w.cwa * w.cwb));
+                }
+            }
         }
 
         // Detector window of every (brick, view): projection of the brick grown by one voxel,
@@ -1115,6 +1181,20 @@ namespace elsa_b200
 
             void adjoint(const float* y, float* x, cudaStream_t s) override
             {
+                if (scatter_) {
+                    const int64_t nrays = rangeSize_;
+                    const unsigned blocks =
+                        static_cast<unsigned>((nrays + kForwardThreads - 1) / kForwardThreads);
+                    ELSA_CUDA(cudaMemsetAsync(x, 0, sizeof(float) * domainSize_, s));
+                    if (vol_.dim == 3)
+                        josephScatterKernel<3><<<blocks, kForwardThreads, 0, s>>>(dRays_, nrays, y,
+                                                                                 vol_, x);
+                    else
+                        josephScatterKernel<2><<<blocks, kForwardThreads, 0, s>>>(dRays_, nrays, y,
+                                                                                 vol_, x);
+                    ELSA_LAUNCH_CHECK("josephScatterKernel");
+                    return;
+                }
                 const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
                 float* partial = partial_ ? partial_->as<float>() : nullptr;
                 if (vol_.dim == 3)
@@ -1140,6 +1220,8 @@ namespace elsa_b200
                 }
                 if (knob == kKnobForwardThreads && !tma_)
                     return {64, 128, 256, 512};
+                if (knob == kKnobAdjointScatter)
+                    return {0, 1};
                 return {};
             }
 
@@ -1149,6 +1231,8 @@ namespace elsa_b200
                     return adjointChunks_;
                 if (knob == kKnobForwardThreads)
                     return tma_ ? -1 : forwardThreads_;
+                if (knob == kKnobAdjointScatter)
+                    return scatter_;
                 return -1;
             }
 
@@ -1164,6 +1248,10 @@ namespace elsa_b200
                 }
                 if (knob == kKnobForwardThreads) {
                     forwardThreads_ = value;
+                    return;
+                }
+                if (knob == kKnobAdjointScatter) {
+                    scatter_ = value;
                     return;
                 }
                 const size_t need = sizeof(float) * static_cast<size_t>(domainSize_) *
@@ -1193,13 +1281,15 @@ namespace elsa_b200
                 case 6: // kernel launches per forward call
                     return tma_ ? tma_->launchesPerForward() : 1;
                 case 7: // kernel launches per adjoint call (with view chunks: + the chunk sum)
-                    return adjointChunks_ > 1 ? 2 : 1;
+                    return (!scatter_ && adjointChunks_ > 1) ? 2 : 1;
                 default:
                     return -1;
                 }
             }
 
         private:
+            int scatter_ = 0; // 1: atomic scatter adjoint (2D: 512^2 / 720 views 1.74 ms
+                              // against 2.00; 3D 256^3 / 360 views 92 ms against 54.8)
             JosephRay* dRays_ = nullptr;
             unsigned* dViewAxes_ = nullptr;
             RayWindow* dWindows_ = nullptr;
