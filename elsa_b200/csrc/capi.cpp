@@ -219,9 +219,16 @@ static elsa_status projectorCreate(int32_t kind, int32_t dim, const int64_t* vol
         std::memcpy(pv.data(), poses, sizeof(elsa_b200::PoseRecord) * pv.size());
         auto handle = std::make_unique<elsa_projector>();
         switch (kind) {
-        case ELSA_PROJECTOR_JOSEPH:
-            handle->impl = elsa_b200::makeJosephProjector(vol, det, pv, curved);
+        case ELSA_PROJECTOR_JOSEPH: {
+            require(numParams <= 1, "JosephsMethod: too many parameters");
+            const bool fast = numParams >= 1 && params[0] != 0.0f;
+            if (fast && curved.enabled())
+                throw elsa_b200::Error(ELSA_ERROR_NOT_SUPPORTED,
+                                       "JosephsMethodCUDA: the fast adjoint needs a planar "
+                                       "detector");
+            handle->impl = elsa_b200::makeJosephProjector(vol, det, pv, curved, fast);
             break;
+        }
         case ELSA_PROJECTOR_SIDDON:
             handle->impl = elsa_b200::makeSiddonProjector(vol, det, pv, false, curved);
             break;

@@ -201,6 +201,100 @@ namespace elsa_b200
             }
         }
 
+        // elsa's default CUDA adjoint (JosephsMethodCUDA with fast = true,
+        // TraverseJosephsCUDA.cu:218-287): a voxel-driven backprojection, not the transpose of the
+        // forward. For voxel centre c and view p: pixel = B_p (c - o_p) with B_p the leading
+        // DIM x DIM block of the projection matrix and o_p = -Binv_p p4_p, divided by its last
+        // coordinate; the sinogram is read through a layered texture (linear filtering, border
+        // addressing) and the views are summed in order. The float operations are the reference
+        // kernel's: its x coordinates come from 32 lanes per (y, z) row, lane t taking voxels
+        // t + 32 s and advancing the first difference by adding 32 once per step s (voxels past
+        // the last multiple of 32 computed directly), and its matrix-vector product
+        // ((b0 r0 + b1 r1) + b2 r2, Matrix.cuh:12-32) is contracted as fma(b2, r2, fma(b0, r0,
+        // b1 r1)). The layout is the reference's too, a row per 32 lanes, but with kRows rows per
+        // block and the sums of kChunk steps in registers instead of shared memory.
+        template <int DIM>
+        __device__ __forceinline__ float fastSample(cudaTextureObject_t sino, const float* T,
+                                                    float r0, float r1, float r2, int p)
+        {
+            if (DIM == 3) {
+                const float q0 = __fmaf_rn(T[6], r2, __fmaf_rn(T[0], r0, __fmul_rn(T[3], r1)));
+                const float q1 = __fmaf_rn(T[7], r2, __fmaf_rn(T[1], r0, __fmul_rn(T[4], r1)));
+                const float q2 = __fmaf_rn(T[8], r2, __fmaf_rn(T[2], r0, __fmul_rn(T[5], r1)));
+                return tex2DLayered<float>(sino, __fdiv_rn(q0, q2), __fdiv_rn(q1, q2), p);
+            }
+            const float q0 = __fmaf_rn(T[0], r0, __fmul_rn(T[2], r1));
+            const float q1 = __fmaf_rn(T[1], r0, __fmul_rn(T[3], r1));
+            return tex1DLayered<float>(sino, __fdiv_rn(q0, q1), p);
+        }
+
+        constexpr int kFastRows = 4;   // (y, z) rows per block of the fast adjoint
+        constexpr int kFastChunk = 8;  // steps per lane summed in registers at once
+
+        template <int DIM>
+        __global__ void __launch_bounds__(32 * kFastRows)
+            josephFastAdjointKernel(cudaTextureObject_t sino, const float* __restrict__ table,
+                                    int np, VolumeShape vol, float* __restrict__ x)
+        {
+            constexpr int kT = DIM == 3 ? 12 : 6; // block (column-major) + origin
+            extern __shared__ float tab[];        // kT floats per view
+            for (int i = threadIdx.y * 32 + threadIdx.x; i < kT * np; i += 32 * kFastRows)
+                tab[i] = table[i];
+            __syncthreads();
+            const int lane = threadIdx.x;
+            const int row = blockIdx.x * kFastRows + threadIdx.y;
+            const int nrows = vol.n[1] * (DIM == 3 ? vol.n[2] : 1);
+            if (row >= nrows)
+                return;
+            // rows z fastest, as the reference's grid: neighbouring blocks then read neighbouring
+            // detector rows of a view through the texture cache
+            const int nz = DIM == 3 ? vol.n[2] : 1;
+            const int zi = row % nz, yi = row / nz;
+            const int nsteps = vol.n[0] / 32, rem = vol.n[0] - nsteps * 32;
+            const float c1 = static_cast<float>(yi) + 0.5f;
+            const float c2 = static_cast<float>(zi) + 0.5f;
+            float* out = x + static_cast<int64_t>(vol.n[0]) * (yi + static_cast<int64_t>(vol.n[1]) * zi);
+            const float c0 = static_cast<float>(lane) + 0.5f;
+            for (int s0 = 0; s0 < nsteps; s0 += kFastChunk) {
+                const int cnt = min(kFastChunk, nsteps - s0);
+                float acc[kFastChunk];
+#pragma unroll
+                for (int k = 0; k < kFastChunk; ++k)
+                    acc[k] = 0.0f;
+                for (int p = 0; p < np; ++p) {
+                    const float* T = tab + kT * p;
+                    float r0 = __fsub_rn(c0, T[DIM * DIM]);
+                    for (int s = 0; s < s0; ++s)
+                        r0 = __fadd_rn(r0, 32.0f);
+                    const float r1 = __fsub_rn(c1, T[DIM * DIM + 1]);
+                    const float r2 = DIM == 3 ? __fsub_rn(c2, T[11]) : 0.0f;
+#pragma unroll
+                    for (int k = 0; k < kFastChunk; ++k) {
+                        if (k < cnt)
+                            acc[k] = __fadd_rn(acc[k], fastSample<DIM>(sino, T, r0, r1, r2, p));
+                        r0 = __fadd_rn(r0, 32.0f);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < kFastChunk; ++k)
+                    if (k < cnt)
+                        out[lane + 32 * (s0 + k)] = acc[k];
+            }
+            if (lane < rem) {
+                const int xi = nsteps * 32 + lane;
+                const float cr = static_cast<float>(xi) + 0.5f;
+                float acc = 0.0f;
+                for (int p = 0; p < np; ++p) {
+                    const float* T = tab + kT * p;
+                    const float r0 = __fsub_rn(cr, T[DIM * DIM]);
+                    const float r1 = __fsub_rn(c1, T[DIM * DIM + 1]);
+                    const float r2 = DIM == 3 ? __fsub_rn(c2, T[11]) : 0.0f;
+                    acc = __fadd_rn(acc, fastSample<DIM>(sino, T, r0, r1, r2, p));
+                }
+                out[xi] = acc;
+            }
+        }
+
         // Detector window of every (brick, view): projection of the brick grown by one voxel,
         // plus one pixel of margin. Falls back to the whole detector when a corner lies behind
         // the source.
@@ -1038,9 +1132,12 @@ namespace elsa_b200
         class JosephProjector final : public Projector
         {
         public:
+            // fast: elsa's unmatched `fast` adjoint (JosephsMethodCUDA.h:60-67) instead of the
+            // matched one
             JosephProjector(const VolumeShape& vol, const DetectorShape& det,
-                            const std::vector<PoseRecord>& poses, const CurvedDetector& curved)
-                : Projector(0, vol, det, poses), curved_(vol.dim, det, curved)
+                            const std::vector<PoseRecord>& poses, const CurvedDetector& curved,
+                            bool fast)
+                : Projector(0, vol, det, poses), curved_(vol.dim, det, curved), fast_(fast)
             {
                 const int64_t nrays = rangeSize_;
                 ELSA_CUDA(cudaMalloc(&dRays_, sizeof(JosephRay) * nrays));
@@ -1072,6 +1169,17 @@ namespace elsa_b200
                         classSpacing_ = m;
                         break;
                     }
+                if (fast_) {
+                    buildFastAdjoint();
+                    if (vol_.dim == 3) {
+                        std::vector<float> hp(poses_.size() * kPoseFloats);
+                        std::memcpy(hp.data(), poses_.data(), sizeof(float) * hp.size());
+                        tma_ = std::make_unique<JosephForwardTma>(vol_, det_, hp, dRays_);
+                    }
+                    ELSA_CUDA(cudaDeviceSynchronize());
+                    curved_.release();
+                    return;
+                }
                 if (classSpacing_ == 0)
                     throw Error(ELSA_ERROR_NOT_SUPPORTED,
                                 "JosephsMethod: neighbouring detector rays pass within two voxels "
@@ -1155,8 +1263,75 @@ namespace elsa_b200
                                      cudaMemcpyHostToDevice));
             }
 
+            // The fast adjoint's per-view table (leading block of P, column-major, and the ray
+            // origin -Binv p4 as JosephsMethodCUDA.cpp:80-84 computes it, in float, k-sums in
+            // order) and the layered sinogram array it reads through a texture.
+            void buildFastAdjoint()
+            {
+                const int d = vol_.dim;
+                const int kT = d == 3 ? 12 : 6;
+                std::vector<float> table(static_cast<size_t>(kT) * det_.np);
+                for (int p = 0; p < det_.np; ++p) {
+                    const float* P = poses_[p].v;
+                    const float* Pinv = poses_[p].v + kPoseOffPinv;
+                    float* T = table.data() + static_cast<size_t>(kT) * p;
+                    for (int c = 0; c < d; ++c)
+                        for (int r = 0; r < d; ++r)
+                            T[d * c + r] = P[(d + 1) * r + c];
+                    for (int r = 0; r < d; ++r) {
+                        float s = 0.0f;
+                        for (int c = 0; c < d; ++c)
+                            s += Pinv[d * r + c] * P[(d + 1) * c + d];
+                        T[d * d + r] = -s;
+                    }
+                }
+                // the kernel keeps the table in shared memory; the limit attribute only grows, as
+                // for the brick-owner adjoints (shared by every projector of the process)
+                const int need = static_cast<int>(sizeof(float) * table.size());
+                if (need > 227 * 1024)
+                    throw Error(ELSA_ERROR_NOT_SUPPORTED,
+                                "JosephsMethodCUDA: too many poses for the fast adjoint");
+                {
+                    static std::mutex mu;
+                    std::lock_guard<std::mutex> lock(mu);
+                    cudaFuncAttributes attr{};
+                    const void* fn = d == 3 ? reinterpret_cast<const void*>(
+                                                  josephFastAdjointKernel<3>)
+                                            : reinterpret_cast<const void*>(
+                                                  josephFastAdjointKernel<2>);
+                    ELSA_CUDA(cudaFuncGetAttributes(&attr, fn));
+                    if (need > attr.maxDynamicSharedSizeBytes)
+                        ELSA_CUDA(cudaFuncSetAttribute(
+                            fn, cudaFuncAttributeMaxDynamicSharedMemorySize, need));
+                }
+                fastTable_ = std::make_unique<DeviceBuffer>(sizeof(float) * table.size());
+                ELSA_CUDA(cudaMemcpy(fastTable_->as<float>(), table.data(),
+                                     sizeof(float) * table.size(), cudaMemcpyHostToDevice));
+                const cudaChannelFormatDesc fd =
+                    cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
+                const cudaExtent ext =
+                    make_cudaExtent(det_.nu, d == 3 ? det_.nv : 0, det_.np);
+                ELSA_CUDA(cudaMalloc3DArray(&fastArray_, &fd, ext, cudaArrayLayered));
+                cudaResourceDesc res;
+                std::memset(&res, 0, sizeof(res));
+                res.resType = cudaResourceTypeArray;
+                res.res.array.array = fastArray_;
+                cudaTextureDesc tex;
+                std::memset(&tex, 0, sizeof(tex));
+                tex.addressMode[0] = tex.addressMode[1] = tex.addressMode[2] =
+                    cudaAddressModeBorder;
+                tex.filterMode = cudaFilterModeLinear;
+                tex.readMode = cudaReadModeElementType;
+                tex.normalizedCoords = 0;
+                ELSA_CUDA(cudaCreateTextureObject(&fastTex_, &res, &tex, nullptr));
+            }
+
             ~JosephProjector() override
             {
+                if (fastTex_)
+                    cudaDestroyTextureObject(fastTex_);
+                if (fastArray_)
+                    cudaFreeArray(fastArray_);
                 cudaFree(dRays_);
                 cudaFree(dViewAxes_);
                 cudaFree(dWindows_);
@@ -1181,6 +1356,31 @@ namespace elsa_b200
 
             void adjoint(const float* y, float* x, cudaStream_t s) override
             {
+                if (fast_) {
+                    // the sinogram into the layered array (JosephsMethodCUDA.cpp:234-240 copies
+                    // the host data there on every call)
+                    const int d = vol_.dim;
+                    cudaMemcpy3DParms prm = {};
+                    prm.srcPtr = make_cudaPitchedPtr(const_cast<float*>(y), sizeof(float) * det_.nu,
+                                                     det_.nu, d == 3 ? det_.nv : 1);
+                    prm.dstArray = fastArray_;
+                    prm.extent = make_cudaExtent(det_.nu, d == 3 ? det_.nv : 1, det_.np);
+                    prm.kind = cudaMemcpyDeviceToDevice;
+                    ELSA_CUDA(cudaMemcpy3DAsync(&prm, s));
+                    const int64_t rows =
+                        static_cast<int64_t>(vol_.n[1]) * (d == 3 ? vol_.n[2] : 1);
+                    const dim3 grid(static_cast<unsigned>((rows + kFastRows - 1) / kFastRows));
+                    const dim3 block(32, kFastRows);
+                    const size_t smem = sizeof(float) * (d == 3 ? 12 : 6) * det_.np;
+                    if (d == 3)
+                        josephFastAdjointKernel<3><<<grid, block, smem, s>>>(
+                            fastTex_, fastTable_->as<float>(), det_.np, vol_, x);
+                    else
+                        josephFastAdjointKernel<2><<<grid, block, smem, s>>>(
+                            fastTex_, fastTable_->as<float>(), det_.np, vol_, x);
+                    ELSA_LAUNCH_CHECK("josephFastAdjointKernel");
+                    return;
+                }
                 if (scatter_) {
                     const int64_t nrays = rangeSize_;
                     const unsigned blocks =
@@ -1210,6 +1410,8 @@ namespace elsa_b200
 
             std::vector<int> knobCandidates(int knob) const override
             {
+                if (fast_ && knob != kKnobForwardThreads)
+                    return {}; // the fast adjoint has no adjoint knobs
                 if (knob == kKnobAdjointChunks) {
                     // partial volumes limited to 4 GiB
                     const int64_t byMemory =
@@ -1281,13 +1483,17 @@ namespace elsa_b200
                 case 6: // kernel launches per forward call
                     return tma_ ? tma_->launchesPerForward() : 1;
                 case 7: // kernel launches per adjoint call (with view chunks: + the chunk sum)
-                    return (!scatter_ && adjointChunks_ > 1) ? 2 : 1;
+                    return (!fast_ && !scatter_ && adjointChunks_ > 1) ? 2 : 1;
                 default:
                     return -1;
                 }
             }
 
         private:
+            bool fast_ = false; // elsa's unmatched fast adjoint
+            cudaArray_t fastArray_ = nullptr;
+            cudaTextureObject_t fastTex_ = 0;
+            std::unique_ptr<DeviceBuffer> fastTable_;
             int scatter_ = 0; // 1: atomic scatter adjoint (2D: 512^2 / 720 views 1.74 ms
                               // against 2.00; 3D 256^3 / 360 views 92 ms against 54.8)
             JosephRay* dRays_ = nullptr;
@@ -1345,8 +1551,8 @@ namespace elsa_b200
     std::unique_ptr<Projector> makeJosephProjector(const VolumeShape& vol,
                                                    const DetectorShape& det,
                                                    const std::vector<PoseRecord>& poses,
-                                                   const CurvedDetector& curved)
+                                                   const CurvedDetector& curved, bool fast)
     {
-        return std::make_unique<JosephProjector>(vol, det, poses, curved);
+        return std::make_unique<JosephProjector>(vol, det, poses, curved, fast);
     }
 } // namespace elsa_b200

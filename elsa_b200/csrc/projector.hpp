@@ -103,7 +103,8 @@ namespace elsa_b200
     std::unique_ptr<Projector> makeJosephProjector(const VolumeShape& vol,
                                                    const DetectorShape& det,
                                                    const std::vector<PoseRecord>& poses,
-                                                   const CurvedDetector& curved = {});
+                                                   const CurvedDetector& curved = {},
+                                                   bool fast = false);
     // binary: BinaryMethod, the Siddon visits with weight 1 (projectors/BinaryMethod.cpp)
     std::unique_ptr<Projector> makeSiddonProjector(const VolumeShape& vol,
                                                    const DetectorShape& det,

@@ -304,10 +304,22 @@ class LinearOperator:
 
 
 class JosephsMethodCUDA(LinearOperator):
-    """JosephsMethodCUDA(volume, detector, fast=True): the matched, deterministic adjoint is used
-    for both settings of `fast` (elsa's fast adjoint is an unmatched approximation)."""
+    """JosephsMethodCUDA(volume, detector, fast=False). fast=False: the matched, deterministic
+    adjoint (the transpose of the forward, as elsa's CPU JosephsMethod). fast=True: elsa's
+    `fast` adjoint, a voxel-driven backprojection through a texture that is not the transpose
+    (JosephsMethodCUDA.h:60-67). elsa's own default is fast=True; here the matched adjoint is the
+    default, since the solvers assume a transpose."""
 
-    def __init__(self, volumeDescriptor, detectorDescriptor, fast=True):
+    def __init__(self, volumeDescriptor, detectorDescriptor, fast=False):
+        super().__init__(_capi.PROJECTOR_JOSEPH, volumeDescriptor, detectorDescriptor,
+                         [1.0] if fast else [])
+
+
+class JosephsMethod(LinearOperator):
+    """JosephsMethod(volume, detector): elsa's CPU Joseph projector (matched adjoint), on the
+    device."""
+
+    def __init__(self, volumeDescriptor, detectorDescriptor):
         super().__init__(_capi.PROJECTOR_JOSEPH, volumeDescriptor, detectorDescriptor)
 
 
@@ -371,7 +383,8 @@ class PhaseContrastBSplineVoxelProjectorCUDA(LinearOperator):
 
 # pyelsa aliases: the names without the CUDA suffix (CPU projectors in elsa) and the f-suffixed
 # float instantiations resolve to the same device operators
-JosephsMethod = JosephsMethodCUDAf = JosephsMethodCUDA
+JosephsMethodCUDAf = JosephsMethodCUDA
+JosephsMethodf = JosephsMethod
 SiddonsMethod = SiddonsMethodCUDAf = SiddonsMethodCUDA
 BinaryMethodf = BinaryMethod
 BlobProjectorf, BSplineProjectorf = BlobProjector, BSplineProjector

@@ -41,7 +41,12 @@ typedef enum elsa_status {
 } elsa_status;
 
 typedef enum elsa_projector_kind {
-    /* JosephsMethod / JosephsMethodCUDA (matched adjoint), projectors/JosephsMethod.cpp:37-198 */
+    /* JosephsMethod / JosephsMethodCUDA, projectors/JosephsMethod.cpp:37-198. params[0] = fast
+     * (default 0): 0 = the matched adjoint (the transpose of the forward, as JosephsMethod and
+     * JosephsMethodCUDA(..., fast = false)); 1 = JosephsMethodCUDA's `fast` adjoint
+     * (JosephsMethodCUDA.h:60-67, TraverseJosephsCUDA.cu:218-287), a voxel-driven backprojection
+     * through a texture with linear filtering that is not the transpose (the reference's
+     * default; planar detectors only). */
     ELSA_PROJECTOR_JOSEPH = 0,
     /* SiddonsMethod / SiddonsMethodCUDA, projectors/SiddonsMethod.cpp:76-124 with
      * projectors/TraverseAABB.cpp:6-184 */

@@ -382,8 +382,21 @@ namespace elsa_b200
 
         template <typename data_t>
         struct JosephsMethodCUDA : LinearOperator<data_t> {
+            // fast: elsa's unmatched `fast` adjoint (JosephsMethodCUDA.h:60-67). elsa defaults to
+            // it; here the matched adjoint (the transpose, as the CPU JosephsMethod) is the
+            // default, since the solvers assume a transpose.
             JosephsMethodCUDA(const VolumeDescriptor& v, const PlanarDetectorDescriptor& d,
-                              bool /*fast: the matched adjoint is always used*/ = true)
+                              bool fast = false)
+                : LinearOperator<data_t>(v, d, ELSA_PROJECTOR_JOSEPH,
+                                         fast ? std::vector<float>{1.0f} : std::vector<float>{})
+            {
+            }
+        };
+
+        // projectors/JosephsMethod.h: the matched Joseph projector
+        template <typename data_t>
+        struct JosephsMethod : LinearOperator<data_t> {
+            JosephsMethod(const VolumeDescriptor& v, const PlanarDetectorDescriptor& d)
                 : LinearOperator<data_t>(v, d, ELSA_PROJECTOR_JOSEPH)
             {
             }

@@ -3,14 +3,17 @@ harness refcuda.cu; built by oracle/ref_cuda/build.py). TEST INFRASTRUCTURE ONLY
 import ctypes
 import os
 
-from .build import LIB
+# built by oracle/ref_cuda/build.py (not imported here, so that `python -m` runs it cleanly)
+LIB = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "_ref",
+                   "librefcuda.so")
 
 SYMBOLS = ["refcuda_last_error", "refcuda_create", "refcuda_destroy",
            "refcuda_joseph_upload_volume", "refcuda_joseph_forward",
            "refcuda_joseph_download_sinogram", "refcuda_joseph_upload_sinogram",
            "refcuda_joseph_adjoint_fast", "refcuda_joseph_download_volume",
            "refcuda_siddon_forward", "refcuda_siddon_adjoint", "refcuda_voxel_set_lut",
-           "refcuda_voxel_forward", "refcuda_voxel_adjoint"]
+           "refcuda_voxel_forward", "refcuda_voxel_adjoint", "refcuda2d_create",
+           "refcuda2d_destroy", "refcuda2d_joseph_adjoint_fast"]
 
 _lib = None
 
@@ -37,6 +40,9 @@ def lib():
         L.refcuda_voxel_set_lut.argtypes = [vp, vp, i32, f]
         L.refcuda_voxel_forward.argtypes = [vp, i32, vp, vp]
         L.refcuda_voxel_adjoint.argtypes = [vp, i32, vp, vp]
+        L.refcuda2d_create.argtypes = [vp, vp, vp, ctypes.POINTER(vp)]
+        L.refcuda2d_destroy.argtypes = [vp]
+        L.refcuda2d_joseph_adjoint_fast.argtypes = [vp, vp, vp]
         _lib = L
     return _lib
 
@@ -101,3 +107,28 @@ class RefProjectors:
 
     def voxel_adjoint(self, y_ptr, x_ptr, differential=False):
         check(lib().refcuda_voxel_adjoint(self.h, int(differential), y_ptr, x_ptr))
+
+
+class RefJoseph2D:
+    """The reference's 2D Joseph `fast` adjoint (TraverseJosephsCUDA<float, 2>) for one fan-beam
+    geometry (device pointers in and out, legacy default stream)."""
+
+    def __init__(self, vol, det, poses):
+        import numpy as np
+        self._keep = (np.ascontiguousarray(vol, np.int64), np.ascontiguousarray(det, np.int64),
+                      np.ascontiguousarray(poses, np.float32))
+        h = ctypes.c_void_p()
+        check(lib().refcuda2d_create(self._keep[0].ctypes.data, self._keep[1].ctypes.data,
+                                     self._keep[2].ctypes.data, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().refcuda2d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def joseph_adjoint_fast(self, y_ptr, x_ptr):
+        check(lib().refcuda2d_joseph_adjoint_fast(self.h, y_ptr, x_ptr))

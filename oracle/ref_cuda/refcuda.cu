@@ -403,4 +403,103 @@ int refcuda_voxel_adjoint(refcuda* h, int32_t differential, const float* y, floa
     });
 }
 
+// ---- 2D Joseph fast adjoint (JosephsMethodCUDA.cpp:300-335) ------------------------------------
+
+struct refcuda2d {
+    unsigned nx = 0, ny = 0, nu = 0, np = 0;
+    cudaPitchedPtr origins{}, proj{}, volPitched{};
+    cudaArray_t sinoArray = nullptr;
+    cudaTextureObject_t sinoTex = 0;
+    ~refcuda2d()
+    {
+        if (sinoTex)
+            cudaDestroyTextureObject(sinoTex);
+        if (sinoArray)
+            cudaFreeArray(sinoArray);
+        for (void* p : {origins.ptr, proj.ptr, volPitched.ptr})
+            if (p)
+                cudaFree(p);
+    }
+};
+
+// vol = (nx, ny), det = (nu, np), poses: np host 2D pose records (P 2x3 at 0, Pinv 3x2 at 12)
+int refcuda2d_create(const int64_t* vol, const int64_t* det, const float* poses, refcuda2d** out)
+{
+    *out = nullptr;
+    auto* h = new refcuda2d();
+    const int rc = guard([&] {
+        h->nx = unsigned(vol[0]), h->ny = unsigned(vol[1]);
+        h->nu = unsigned(det[0]), h->np = unsigned(det[1]);
+        const unsigned np = h->np;
+        std::vector<float> pblk(4 * size_t(np)), ro(2 * size_t(np));
+        for (unsigned i = 0; i < np; ++i) {
+            const float* q = poses + size_t(i) * kPoseFloats;
+            for (int c = 0; c < 2; ++c)
+                for (int r = 0; r < 2; ++r)
+                    pblk[4 * i + 2 * c + r] = q[3 * r + c];
+            for (int r = 0; r < 2; ++r) {
+                float s = 0.0f;
+                for (int c = 0; c < 2; ++c)
+                    s += q[12 + 2 * r + c] * q[3 * c + 2];
+                ro[2 * i + r] = -s;
+            }
+        }
+        ck(cudaMallocPitch(&h->origins.ptr, &h->origins.pitch, 2 * sizeof(float), np),
+           "cudaMallocPitch");
+        ck(cudaMemcpy2D(h->origins.ptr, h->origins.pitch, ro.data(), 2 * sizeof(float),
+                        2 * sizeof(float), np, cudaMemcpyHostToDevice),
+           "cudaMemcpy2D");
+        ck(cudaMalloc3D(&h->proj, make_cudaExtent(2 * sizeof(float), 2, np)), "cudaMalloc3D");
+        for (unsigned i = 0; i < np; ++i)
+            ck(cudaMemcpy2D(static_cast<char*>(h->proj.ptr) + size_t(i) * h->proj.pitch * 2,
+                            h->proj.pitch, pblk.data() + 4 * size_t(i), 2 * sizeof(float),
+                            2 * sizeof(float), 2, cudaMemcpyHostToDevice),
+               "cudaMemcpy2D");
+        const cudaChannelFormatDesc fd = cudaCreateChannelDesc(32, 0, 0, 0,
+                                                               cudaChannelFormatKindFloat);
+        // a layered 1D array is a 3D array of height 0 (JosephsMethodCUDA.cpp:504-512)
+        ck(cudaMalloc3DArray(&h->sinoArray, &fd, make_cudaExtent(h->nu, 0, np), cudaArrayLayered),
+           "cudaMalloc3DArray");
+        h->sinoTex = makeTexture(h->sinoArray, true);
+        ck(cudaMallocPitch(&h->volPitched.ptr, &h->volPitched.pitch, h->nx * sizeof(float),
+                           h->ny),
+           "cudaMallocPitch");
+    });
+    if (rc) {
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return 0;
+}
+
+int refcuda2d_destroy(refcuda2d* h)
+{
+    delete h;
+    return 0;
+}
+
+// y (device, nu * np) -> x (device, nx * ny): sinogram upload, fast adjoint kernel, copy out
+int refcuda2d_joseph_adjoint_fast(refcuda2d* h, const float* y, float* x)
+{
+    return guard([&] {
+        cudaMemcpy3DParms p = {};
+        p.srcPtr = make_cudaPitchedPtr(const_cast<float*>(y), h->nu * sizeof(float), h->nu, 1);
+        p.dstArray = h->sinoArray;
+        p.extent = make_cudaExtent(h->nu, 1, h->np);
+        p.kind = cudaMemcpyDeviceToDevice;
+        ck(cudaMemcpy3DAsync(&p, 0), "cudaMemcpy3DAsync");
+        const dim3 volumeDims(1, h->ny, h->nx);
+        elsa::TraverseJosephsCUDA<float, 2>::traverseAdjointFast(
+            volumeDims, elsa::TraverseJosephsCUDA<float, 2>::MAX_THREADS_PER_BLOCK,
+            static_cast<int8_t*>(h->volPitched.ptr), h->volPitched.pitch, h->sinoTex,
+            static_cast<int8_t*>(h->origins.ptr), uint32_t(h->origins.pitch),
+            static_cast<int8_t*>(h->proj.ptr), uint32_t(h->proj.pitch), h->np);
+        ck(cudaGetLastError(), "traverseAdjointFast 2D");
+        ck(cudaMemcpy2DAsync(x, h->nx * sizeof(float), h->volPitched.ptr, h->volPitched.pitch,
+                             h->nx * sizeof(float), h->ny, cudaMemcpyDeviceToDevice, 0),
+           "cudaMemcpy2DAsync");
+    });
+}
+
 } // extern "C"

@@ -139,3 +139,37 @@ def test_2d_adjoint_after_smaller_projector(cuda, oracle):
     ys = rng.uniform(0, 1, small.range_size).astype(np.float32)
     _, bps = _gpu_pair(cuda, small, x, ys)
     assert rel_l2(bps, oracle.joseph_adjoint(ys, vol, small_det, small_poses)) <= PARITY
+
+
+@pytest.mark.parametrize("vol,det,views", [((48, 40, 36), [64, 56], 30), ((100, 72), [150], 90)])
+def test_fast_adjoint_mode(cuda, oracle, vol, det, views):
+    """JosephsMethodCUDA(..., fast = true): the forward is unchanged, the adjoint is elsa's
+    voxel-driven texture backprojection (not the transpose: compared loosely with the matched
+    one here; tests/test_reference_cuda.py pins it on the reference's own kernel)."""
+    import elsa_b200
+    poses, dd = oracle.circle_trajectory(vol, views, 360, 10.0 * vol[0], 2.5 * vol[0], det)
+    matched = _projector(vol, dd, poses)
+    fast = elsa_b200.Projector(elsa_b200.PROJECTOR_JOSEPH, vol, dd, poses, [1.0])
+    rng = np.random.default_rng(21)
+    x = rng.uniform(0, 1, int(np.prod(vol))).astype(np.float32)
+    y = rng.uniform(0, 1, int(np.prod(dd))).astype(np.float32)
+    f0, a0 = _gpu_pair(cuda, matched, x, y)
+    f1, a1 = _gpu_pair(cuda, fast, x, y)
+    assert np.array_equal(f0.view(np.uint32), f1.view(np.uint32))
+    assert np.all(np.isfinite(a1))
+    assert np.corrcoef(a0.astype(np.float64), a1.astype(np.float64))[0, 1] > 0.7
+    _, a2 = _gpu_pair(cuda, fast, x, y)  # no atomics: bit-reproducible
+    assert np.array_equal(a1.view(np.uint32), a2.view(np.uint32))
+    assert fast.knob_candidates(elsa_b200.KNOB_ADJOINT_CHUNKS) == []
+    assert fast.knob_candidates(elsa_b200.KNOB_ADJOINT_SCATTER) == []
+    assert fast.info(7) == 1
+
+
+def test_fast_adjoint_arguments(cuda, oracle):
+    import elsa_b200
+    poses, dd = oracle.circle_trajectory((16, 16, 16), 8, 360, 160, 40, [24, 24])
+    with pytest.raises(elsa_b200.InvalidArgumentError):
+        elsa_b200.Projector(elsa_b200.PROJECTOR_JOSEPH, (16, 16, 16), dd, poses, [1.0, 0.0])
+    with pytest.raises(elsa_b200.ElsaError):
+        elsa_b200.Projector(elsa_b200.PROJECTOR_JOSEPH, (16, 16, 16), dd, poses, [1.0],
+                            curved=(0.5, 200.0))

@@ -128,6 +128,17 @@ def test_reference_cuda_agreement(cuda, oracle):
         out["joseph_fwd"] = rel_l2(rAx.cpu().numpy(), Ax.cpu().numpy())
         a, b = rAty.cpu().numpy().astype(np.float64), Aty.cpu().numpy().astype(np.float64)
         out["joseph_fast_adj_corr"] = float(np.corrcoef(a, b)[0, 1])
+        # this library's fast mode (JosephsMethodCUDA(..., fast = true)) against the reference's
+        # fast kernel: the same float operations and texture reads
+        Aty_fast = torch.empty(int(np.prod(vol)), device="cuda")
+        fastp = elsa_b200.Projector(elsa_b200.PROJECTOR_JOSEPH, vol, det, poses, [1.0])
+        fastp.apply_adjoint_ptr(y.data_ptr(), Aty_fast.data_ptr(),
+                                torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        mine, theirs = Aty_fast.cpu().numpy(), rAty.cpu().numpy()
+        out["joseph_fast_adj_vs_ours"] = rel_l2(mine, theirs)
+        out["joseph_fast_adj_bits_differing"] = int(np.count_nonzero(
+            mine.view(np.uint32) != theirs.view(np.uint32)))
         # blob voxel projector, absorption and phase contrast: the reference's CUDA kernels
         # against a restatement of their own formula, and against this library (which follows
         # the CPU path's footprint walk)
@@ -152,10 +163,39 @@ def test_reference_cuda_agreement(cuda, oracle):
     assert all(np.isfinite(v) for v in out.values()), out
     assert out["siddon_fwd"] <= 1e-3 and out["siddon_adj"] <= 1e-3, out
     assert out["joseph_fwd"] <= 5e-2 and out["joseph_fast_adj_corr"] >= 0.7, out
+    assert out["joseph_fast_adj_vs_ours"] <= 1e-6, out
     for k in ("blob", "phase_blob"):
         # float32 footprint bounds and weights against the float64 restatement; the phase
         # contrast weights change sign across the footprint, so their sum cancels more
         assert out[k + "_fwd_vs_formula"] <= 5e-3 and out[k + "_adj_vs_formula"] <= 5e-3, out
+
+
+@pytest.mark.gpu
+def test_reference_cuda_fast_adjoint_2d(cuda, oracle):
+    """The 2D fast adjoint (1D layered texture) against the reference's 2D kernel, with a volume
+    edge that is not a multiple of 32 (the reference's remainder launch)."""
+    ref_cuda = _ref()
+    import elsa_b200
+    torch = cuda
+    vol, views = (100, 72), 90
+    poses, det = oracle.circle_trajectory(vol, views, 360, 1000, 250, [150])
+    rng = np.random.default_rng(6)
+    y = _dev(torch, rng.uniform(0, 1, int(np.prod(det))))
+    mine = torch.empty(int(np.prod(vol)), device="cuda")
+    theirs = torch.empty(int(np.prod(vol)), device="cuda")
+    p = elsa_b200.Projector(elsa_b200.PROJECTOR_JOSEPH, vol, det, poses, [1.0])
+    p.apply_adjoint_ptr(y.data_ptr(), mine.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    R = ref_cuda.RefJoseph2D(vol, det, poses)
+    try:
+        R.joseph_adjoint_fast(y.data_ptr(), theirs.data_ptr())
+        torch.cuda.synchronize()
+    finally:
+        R.close()
+    a, b = mine.cpu().numpy(), theirs.cpu().numpy()
+    err = rel_l2(a, b)
+    print(json.dumps({"joseph2d_fast_adj_vs_ours": err, "bits_differing":
+                      int(np.count_nonzero(a.view(np.uint32) != b.view(np.uint32)))}))
+    assert err <= 1e-6
 
 
 def _median_ms(torch, fn, reps=5, warm=2):
@@ -219,6 +259,10 @@ def test_reference_cuda_timing(cuda, oracle, tmp_path):
                     torch, lambda: R.joseph_adjoint_fast(y.data_ptr(), Aty.data_ptr()))
                 rec["joseph_ref_fast_adj_kernel"] = _median_ms(
                     torch, lambda: R.joseph_adjoint_fast(y.data_ptr(), Aty.data_ptr(), True))
+                fastp = elsa_b200.Projector(elsa_b200.PROJECTOR_JOSEPH, vol, det, poses, [1.0])
+                rec["joseph_ours_fast_adj"] = _median_ms(
+                    torch, lambda: fastp.apply_adjoint_ptr(y.data_ptr(), Aty.data_ptr(), s))
+                del fastp
                 rec["siddon_ref_fwd"] = _median_ms(
                     torch, lambda: R.siddon_forward(x.data_ptr(), Ax.data_ptr()), reps=3)
                 rec["siddon_ref_adj"] = _median_ms(
