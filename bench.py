@@ -393,6 +393,9 @@ SECONDARY = {
     "joseph2d128": ("JOSEPH", (128, 128), 180, [182], None, 1000, 250),
     "binary2d128": ("BINARY", (128, 128), 180, [182], None, 1000, 250),
     "rayblob64": ("RAY_BLOB", (64, 64, 64), 60, [96, 96], [2.0, 10.83, 2.0], 640, 160),
+    # JosephsMethodCUDA(..., fast = true): the TMA forward and elsa's voxel-driven adjoint
+    "joseph256fast": ("JOSEPH", (256, 256, 256), 360, [384, 384], [1.0], 2560, 640),
+    "joseph2d512": ("JOSEPH", (512, 512), 720, [730], None, 5120, 1280),
 }
 
 
