@@ -139,14 +139,33 @@ namespace elsa_b200
             return t * fb + (1.0f - t) * fa;
         }
 
-        template <int DIM>
+        // Fast (forward only): the distance as n2 * rsqrt(n2) and the lerp as one fma, within a
+        // few ulp of the reference's weights; the forward's sums are reordered by atomics
+        // anyway, while the adjoint keeps every float operation of the reference.
+        template <int DIM, bool Fast = false>
         __device__ __forceinline__ float voxelWeight(const float* lut, const VoxelParams& vp,
                                                      float d0, float d1)
         {
             float n2 = d0 * d0;
             if (DIM == 3)
-                n2 = n2 + d1 * d1;
-            const float v = lutAt(lut, vp.radius, vp.invRadius, sqrtf(n2));
+                n2 = Fast ? __fmaf_rn(d1, d1, n2) : n2 + d1 * d1;
+            float v;
+            if (Fast) {
+                const float dist = n2 > 0.0f ? __fmul_rn(n2, rsqrtf(n2)) : 0.0f;
+                const float q = vp.invRadius != 0.0f ? dist * vp.invRadius : dist / vp.radius;
+                const float index = q * static_cast<float>(kVoxelLutSize - 1);
+                if (index < 0.0f || index > static_cast<float>(kVoxelLutSize - 1)) {
+                    v = 0.0f;
+                } else {
+                    const float af = floorf(index);
+                    const int a = static_cast<int>(af);
+                    const int b = a + (index > af ? 1 : 0);
+                    const float fa = lut[a];
+                    v = __fmaf_rn(index - af, lut[b] - fa, fa);
+                }
+            } else {
+                v = lutAt(lut, vp.radius, vp.invRadius, sqrtf(n2));
+            }
             if (vp.weightKind == 0)
                 return v;
             if (DIM == 2)
@@ -158,13 +177,16 @@ namespace elsa_b200
         // index within the pose, u, v, d0, d1) with (u, v) the pixel's unwrapped detector
         // coordinates (u may leave [0, nu) where the reference's linear index wraps into the
         // next row; visitBox rejects such footprints for the shared patch).
-        template <int DIM, class Fn>
+        // Fast (forward only): divisions by the scaling s replaced by a multiplication with 1 / s.
+        template <int DIM, bool Fast = false, class Fn>
         __device__ __forceinline__ void visitFootprint(const Footprint& f, const VoxelParams& vp,
                                                        Fn fn)
         {
+            const float invS = Fast ? 1.0f / f.s : 0.0f;
+            auto scaled = [&](float d) { return Fast ? __fmul_rn(d, invS) : d / f.s; };
             if (DIM == 2) {
                 for (int u = f.lo0; u <= f.hi0; ++u)
-                    fn(u, u, 0, (f.c0 - static_cast<float>(u)) / f.s, 0.0f);
+                    fn(u, u, 0, scaled(f.c0 - static_cast<float>(u)), 0.0f);
                 return;
             }
             const int ext0 = f.hi0 - f.lo0 + 1, ext1 = f.hi1 - f.lo1 + 1;
@@ -178,10 +200,10 @@ namespace elsa_b200
             float cur0 = static_cast<float>(f.lo0), cur1 = static_cast<float>(f.lo1);
             int u = f.lo0, v = f.lo1;
             for (int r = 0; r < rows; ++r) {
-                const float d1 = (f.c1 - cur1) / f.s;
+                const float d1 = scaled(f.c1 - cur1);
                 for (int c = 0; c < cols; ++c) {
                     if (lin >= 0 && lin < npix)
-                        fn(lin, u, v, (f.c0 - cur0) / f.s, d1);
+                        fn(lin, u, v, scaled(f.c0 - cur0), d1);
                     lin += 1;
                     u += 1;
                     cur0 = cur0 + 1.0f;
@@ -313,8 +335,9 @@ namespace elsa_b200
             __syncthreads();
             if (active) {
                 const bool toPatch = usePatch && boxed;
-                visitFootprint<DIM>(f, vp, [&](int64_t pix, int pu_, int pv_, float d0, float d1) {
-                    const float w = voxelWeight<DIM>(lut, vp, d0, d1);
+                visitFootprint<DIM, true>(f, vp, [&](int64_t pix, int pu_, int pv_, float d0,
+                                                     float d1) {
+                    const float w = voxelWeight<DIM, true>(lut, vp, d0, d1);
                     const float c = xv * w;
                     if (toPatch) {
                         // a boxed footprint stays inside its rows: the unwrapped coordinates
