@@ -89,6 +89,13 @@ int main(int argc, char** argv)
         save(dir + "/curved.f32", Ac.apply(x).toHost());
         save(dir + "/curved_coords.f32", curved->getPlanarCoords());
 
+        // JosephsMethodCUDA(..., fast = true): elsa's unmatched adjoint, the same forward
+        JosephsMethodCUDA<float> Afast(*vol, *sino, true);
+        if (Afast.apply(x).toHost() != b.toHost())
+            throw elsa_b200::Error(ELSA_ERROR_LOGIC, "fast flag changed the forward");
+        save(dir + "/fast_adjoint.f32", Afast.applyAdjoint(b).toHost());
+        save(dir + "/matched_adjoint.f32", JosephsMethod<float>(*vol, *sino).applyAdjoint(b).toHost());
+
         // image files: the sinogram through EDF and MHD, a slice as PGM
         EDF::write(b, dir + "/sino.edf");
         MHD::write(b, dir + "/sino.mhd", dir + "/sino.raw");

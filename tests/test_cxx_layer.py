@@ -93,6 +93,11 @@ def test_cxx_layer_runs(cuda, oracle, tmp_path):
                                   np.asarray(coords, np.float32).ravel())
     ref = oracle.joseph(xf, vol, det, poses, coords=coords)
     assert rel_l2(_load(tmp_path, "curved.f32"), ref) <= 1e-5
+    # the fast flag: elsa's unmatched adjoint, close to but not the matched one
+    fast, matched = _load(tmp_path, "fast_adjoint.f32"), _load(tmp_path, "matched_adjoint.f32")
+    assert rel_l2(matched, oracle.joseph_adjoint(b, vol, det, poses)) <= 1e-5
+    assert not np.array_equal(fast, matched)
+    assert np.corrcoef(fast.astype(np.float64), matched.astype(np.float64))[0, 1] > 0.7
     # image files written by the C++ layer read back here
     data, dims, spacing, _ = elsa_b200.edf_read(str(tmp_path / "sino.edf"))
     assert dims == [36, 36, 30] and np.array_equal(data, b)

@@ -194,3 +194,27 @@ def test_pyelsa_image_files(cuda, oracle, tmp_path):
     assert back.getDataDescriptor() == vol and np.array_equal(np.asarray(back), arr)
     elsa.PGM.write(dc, str(tmp_path / "a.pgm"))
     assert open(tmp_path / "a.pgm").read().startswith("P2\n11 17\n255\n")
+
+
+def test_pyelsa_fast_flag(cuda, oracle):
+    """JosephsMethodCUDA(..., fast=True) is elsa's unmatched fast adjoint (the C ABI's Joseph
+    parameter 1); JosephsMethod and the default JosephsMethodCUDA are the matched operator."""
+    import elsa_b200
+    elsa, vol, sino = _setup(oracle)
+    rng = np.random.default_rng(4)
+    y = rng.uniform(0, 1, tuple(sino.shape)).astype(np.float32)
+    fast = elsa.JosephsMethodCUDA(vol, sino, fast=True)
+    matched = elsa.JosephsMethodCUDA(vol, sino)
+    cpu_name = elsa.JosephsMethod(vol, sino)
+    a_fast = np.asarray(fast.applyAdjoint(y)).ravel()
+    a_matched = np.asarray(matched.applyAdjoint(y)).ravel()
+    assert np.array_equal(a_matched, np.asarray(cpu_name.applyAdjoint(y)).ravel())
+    p = elsa_b200.Projector(elsa_b200.PROJECTOR_JOSEPH, list(vol.shape), list(sino.shape),
+                            sino.poses, [1.0])
+    yd = cuda.from_numpy(np.ascontiguousarray(y).reshape(-1, order="F")).cuda()
+    out = cuda.empty(p.domain_size, device="cuda")
+    p.apply_adjoint_ptr(yd.data_ptr(), out.data_ptr(), cuda.cuda.current_stream().cuda_stream)
+    cuda.cuda.synchronize()
+    a_fast_x_fastest = np.asarray(fast.applyAdjoint(y)).ravel(order="F")
+    assert np.array_equal(a_fast_x_fastest, out.cpu().numpy())
+    assert not np.array_equal(a_fast, a_matched)
