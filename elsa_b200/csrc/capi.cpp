@@ -26,6 +26,19 @@ struct elsa_projector {
     std::unique_ptr<elsa_b200::Projector> impl;
     // lazily allocated staging buffers of the host-buffer entry points
     std::unique_ptr<elsa_b200::DeviceBuffer> hostIn, hostOut;
+    // streams (compute, copy) and per-group events of the pipelined host-buffer entry points;
+    // blocking streams, so they order with the legacy default stream as a synchronous copy does
+    cudaStream_t hostCompute = nullptr, hostCopy = nullptr;
+    std::vector<cudaEvent_t> hostEvents;
+    ~elsa_projector()
+    {
+        for (cudaEvent_t e : hostEvents)
+            cudaEventDestroy(e);
+        if (hostCompute)
+            cudaStreamDestroy(hostCompute);
+        if (hostCopy)
+            cudaStreamDestroy(hostCopy);
+    }
 };
 
 namespace
@@ -498,6 +511,52 @@ static void hostApply(elsa_projector* p, const float* in, float* out, bool adjoi
     }
     float* din = p->hostIn->as<float>();
     float* dout = p->hostOut->as<float>();
+    elsa_b200::Projector& P = *p->impl;
+    const int groups = adjoint ? P.adjointGroups() : P.forwardGroups();
+    if (groups > 1) {
+        // Pipelined: the forward's finished view groups are copied out while later groups run;
+        // the adjoint's view groups are copied in while earlier groups run.
+        if (!p->hostCompute) {
+            ELSA_CUDA(cudaStreamCreate(&p->hostCompute));
+            ELSA_CUDA(cudaStreamCreate(&p->hostCopy));
+        }
+        while (static_cast<int>(p->hostEvents.size()) < groups) {
+            cudaEvent_t e = nullptr;
+            ELSA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            p->hostEvents.push_back(e);
+        }
+        cudaStream_t sc = p->hostCompute, sx = p->hostCopy;
+        const int64_t view = P.rangeSize() / P.detector().np;
+        if (!adjoint) {
+            ELSA_CUDA(cudaMemcpyAsync(din, in, sizeof(float) * nin, cudaMemcpyHostToDevice, sc));
+            P.prepareForward(din, sc);
+            for (int g = 0; g < groups; ++g) {
+                P.forwardGroup(din, dout, g, groups, sc);
+                ELSA_CUDA(cudaEventRecord(p->hostEvents[g], sc));
+                ELSA_CUDA(cudaStreamWaitEvent(sx, p->hostEvents[g], 0));
+                const auto v = P.forwardGroupViews(g, groups);
+                ELSA_CUDA(cudaMemcpyAsync(out + v.first * view, dout + v.first * view,
+                                          sizeof(float) * (v.second - v.first) * view,
+                                          cudaMemcpyDeviceToHost, sx));
+            }
+            ELSA_CUDA(cudaStreamSynchronize(sx));
+        } else {
+            for (int g = 0; g < groups; ++g) {
+                const auto v = P.adjointGroupViews(g, groups);
+                ELSA_CUDA(cudaMemcpyAsync(din + v.first * view, in + v.first * view,
+                                          sizeof(float) * (v.second - v.first) * view,
+                                          cudaMemcpyHostToDevice, sx));
+                ELSA_CUDA(cudaEventRecord(p->hostEvents[g], sx));
+                ELSA_CUDA(cudaStreamWaitEvent(sc, p->hostEvents[g], 0));
+                P.adjointGroup(din, g, groups, sc);
+            }
+            P.adjointFinish(dout, sc);
+            ELSA_CUDA(cudaMemcpyAsync(out, dout, sizeof(float) * nout, cudaMemcpyDeviceToHost,
+                                      sc));
+            ELSA_CUDA(cudaStreamSynchronize(sc));
+        }
+        return;
+    }
     ELSA_CUDA(cudaMemcpy(din, in, sizeof(float) * nin, cudaMemcpyHostToDevice));
     if (adjoint)
         p->impl->adjoint(din, dout, nullptr);

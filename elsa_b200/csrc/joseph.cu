@@ -1049,10 +1049,11 @@ namespace elsa_b200
                                     const RayWindow* __restrict__ windows,
                                     const unsigned* __restrict__ viewAxes, VolumeShape vol,
                                     DetectorShape det, int m, int3 nBricks, int viewsPerChunk,
-                                    float* __restrict__ x)
+                                    float* __restrict__ x, int chunkBase)
         {
-            // blockIdx.y selects a chunk of views, as in the 2D kernel: with several chunks the
-            // brick goes to x + chunk * nvox and sumChunksKernel adds the chunks in order
+            // chunkBase + blockIdx.y selects a chunk of views, as in the 2D kernel: with several
+            // chunks the brick goes to x + chunk * nvox and sumChunksKernel adds the chunks in
+            // order
             using L = WarpBrick<BX, BY>;
             __shared__ float acc[L::kPlane * BZ + 1]; // + dummy word for taps outside
             const int lane = threadIdx.x;
@@ -1063,7 +1064,8 @@ namespace elsa_b200
             for (int i = lane; i < L::kPlane * BZ; i += 32)
                 acc[i] = 0.0f;
             __syncwarp();
-            const int pBegin = blockIdx.y * viewsPerChunk;
+            const int chunk = chunkBase + static_cast<int>(blockIdx.y);
+            const int pBegin = chunk * viewsPerChunk;
             const int pEnd = min(det.np, pBegin + viewsPerChunk);
             for (int p = pBegin; p < pEnd; ++p) {
                 const RayWindow w = windows[static_cast<int64_t>(p) * nb + bi];
@@ -1081,7 +1083,7 @@ namespace elsa_b200
                                                  org0, org1, org2);
             }
             const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
-            float* out = x + blockIdx.y * nvox;
+            float* out = x + static_cast<int64_t>(chunk) * nvox;
             for (int i = lane; i < BX * BY * BZ; i += 32) {
                 const int lx = i % BX, ly = (i / BX) % BY, lz = i / (BX * BY);
                 const int gx = org0 + lx, gy = org1 + ly, gz = org2 + lz;
@@ -1116,13 +1118,24 @@ namespace elsa_b200
             {
                 const int per = (det.np + nc - 1) / nc;
                 const int used = (det.np + per - 1) / per;
-                const dim3 grid(static_cast<unsigned>(nbricks), static_cast<unsigned>(used));
-                josephAdjointWarpKernel<BX, BY, BZ, CPD><<<grid, 32, 0, s>>>(
-                    rays, cps, nrays, y, win, axes, vol, det, m, nb, per,
-                    used > 1 ? partial : x);
+                launchChunks(nbricks, 0, used, per, s, rays, cps, nrays, y, win, axes, vol, det,
+                             m, nb, used > 1 ? partial : x);
                 if (used > 1)
                     launchSumChunks(partial, used,
                                     static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2], x, s);
+            }
+            // chunks [c0, c1) of `per` views each, into out + chunk * nvox
+            static void launchChunks(int nbricks, int c0, int c1, int per, cudaStream_t s,
+                                     const JosephRay* rays, const float2* cps, int64_t nrays,
+                                     const float* y, const RayWindow* win, const unsigned* axes,
+                                     VolumeShape vol, DetectorShape det, int m, int3 nb,
+                                     float* out)
+            {
+                if (c1 <= c0)
+                    return;
+                const dim3 grid(static_cast<unsigned>(nbricks), static_cast<unsigned>(c1 - c0));
+                josephAdjointWarpKernel<BX, BY, BZ, CPD><<<grid, 32, 0, s>>>(
+                    rays, cps, nrays, y, win, axes, vol, det, m, nb, per, out, c0);
             }
         };
 
@@ -1406,6 +1419,55 @@ namespace elsa_b200
                                       dWindows_, dViewAxes_, vol_, det_, classSpacing_, nBricks_,
                                       x, partial);
                 ELSA_LAUNCH_CHECK("josephAdjointKernel");
+            }
+
+            // Host-buffer pipelining: kHostGroups groups of views for the TMA forward; for the
+            // chunked 3D brick-owner adjoint, groups of whole view chunks.
+            static constexpr int kHostGroups = 4;
+            int forwardGroups() const override
+            {
+                return tma_ && det_.np >= kHostGroups ? kHostGroups : 0;
+            }
+            void prepareForward(const float* x, cudaStream_t s) override { tma_->prepare(x, s); }
+            void forwardGroup(const float* x, float* y, int g, int G, cudaStream_t s) override
+            {
+                const auto v = forwardGroupViews(g, G);
+                tma_->forwardViews(x, y, v.first, v.second, s);
+            }
+            int usedChunks() const
+            {
+                const int per = (det_.np + adjointChunks_ - 1) / adjointChunks_;
+                return (det_.np + per - 1) / per;
+            }
+            int adjointGroups() const override
+            {
+                if (fast_ || scatter_ || vol_.dim != 3 || !partial_)
+                    return 0;
+                return usedChunks() >= kHostGroups ? kHostGroups : 0;
+            }
+            std::pair<int, int> adjointGroupViews(int g, int G) const override
+            {
+                const int per = (det_.np + adjointChunks_ - 1) / adjointChunks_;
+                const int used = usedChunks();
+                const int c0 = static_cast<int>(static_cast<int64_t>(used) * g / G);
+                const int c1 = static_cast<int>(static_cast<int64_t>(used) * (g + 1) / G);
+                return {std::min(det_.np, c0 * per), std::min(det_.np, c1 * per)};
+            }
+            void adjointGroup(const float* y, int g, int G, cudaStream_t s) override
+            {
+                const int per = (det_.np + adjointChunks_ - 1) / adjointChunks_;
+                const int used = usedChunks();
+                const int c0 = static_cast<int>(static_cast<int64_t>(used) * g / G);
+                const int c1 = static_cast<int>(static_cast<int64_t>(used) * (g + 1) / G);
+                Adjoint3d::launchChunks(nBricks_.x * nBricks_.y * nBricks_.z, c0, c1, per, s,
+                                        dRays_, dCheckpoints_, rangeSize_, y, dWindows_,
+                                        dViewAxes_, vol_, det_, classSpacing_, nBricks_,
+                                        partial_->as<float>());
+                ELSA_LAUNCH_CHECK("josephAdjointWarpKernel");
+            }
+            void adjointFinish(float* x, cudaStream_t s) override
+            {
+                launchSumChunks(partial_->as<float>(), usedChunks(), domainSize_, x, s);
             }
 
             std::vector<int> knobCandidates(int knob) const override

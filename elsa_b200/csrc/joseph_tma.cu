@@ -281,12 +281,12 @@ namespace elsa_b200
                              const int2* __restrict__ origins, int maxChunks,
                              const float* __restrict__ x, VolumeShape vol, DetectorShape det,
                              int tilesU, int tilesV, int3 fastAxis, float* __restrict__ y,
-                             unsigned* __restrict__ error)
+                             unsigned* __restrict__ error, int tileBase)
         {
             extern __shared__ __align__(128) float stage[];
             __shared__ __align__(8) uint64_t full[NS];
             __shared__ int abortFlag;
-            const int tile = blockIdx.x;
+            const int tile = tileBase + blockIdx.x; // tiles are view-major
             const int p = tile / (tilesU * tilesV);
             const int tu = tile % tilesU, tv = (tile / tilesU) % tilesV;
             const int u = tu * TU + threadIdx.x % TU, v = tv * TV + threadIdx.x / TU;
@@ -495,6 +495,12 @@ namespace elsa_b200
 
     void JosephForwardTma::forward(const float* x, float* y, cudaStream_t s)
     {
+        prepare(x, s);
+        forwardViews(x, y, 0, det_.np, s);
+    }
+
+    void JosephForwardTma::prepare(const float* x, cudaStream_t s)
+    {
         for (int g = 0; g < 3; ++g) {
             if (!present_[g])
                 continue;
@@ -502,9 +508,18 @@ namespace elsa_b200
                                                   dLayouts_[g]);
             ELSA_LAUNCH_CHECK("permuteKernel");
         }
-        forwardTmaKernel<<<static_cast<unsigned>(nTiles_), NT, NS * kStageBytes, s>>>(
+    }
+
+    void JosephForwardTma::forwardViews(const float* x, float* y, int p0, int p1, cudaStream_t s)
+    {
+        const int64_t perView = static_cast<int64_t>(tilesU_) * tilesV_;
+        const int64_t count = perView * (p1 - p0);
+        if (count <= 0)
+            return;
+        forwardTmaKernel<<<static_cast<unsigned>(count), NT, NS * kStageBytes, s>>>(
             maps_[0], maps_[1], maps_[2], dRays_, dTiles_, dChunkOrigins_, maxChunks_, x, vol_,
-            det_, tilesU_, tilesV_, make_int3(fast_[0], fast_[1], fast_[2]), y, dError_);
+            det_, tilesU_, tilesV_, make_int3(fast_[0], fast_[1], fast_[2]), y, dError_,
+            static_cast<int>(perView * p0));
         ELSA_LAUNCH_CHECK("forwardTmaKernel");
     }
 

@@ -35,6 +35,9 @@ namespace elsa_b200
         JosephForwardTma& operator=(const JosephForwardTma&) = delete;
 
         void forward(const float* x, float* y, cudaStream_t s);
+        // forward() in two parts: the permuted copies of x, then the rays of views [p0, p1)
+        void prepare(const float* x, cudaStream_t s);
+        void forwardViews(const float* x, float* y, int p0, int p1, cudaStream_t s);
         // Fraction of tiles that take the gather fallback, and the error word (0 = fine;
         // synchronizes).
         double fallbackFraction() const { return fallbackFraction_; }

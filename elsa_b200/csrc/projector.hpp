@@ -11,6 +11,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <utility>
 #include <vector>
 
 #include "geometry.hpp"
@@ -87,6 +88,41 @@ namespace elsa_b200
             return -1;
         }
         virtual void setKnob(int knob, int value);
+
+        // Pipelining of the host-buffer entry points (optional). forwardGroups() > 1: after
+        // prepareForward(x), forwardGroup(x, y, g, G) writes the rays of the views
+        // [forwardGroupViews(g, G)), so that finished groups can be copied out while later ones
+        // run. adjointGroups() > 1: adjointGroup(y, g, G) adds the views
+        // [adjointGroupViews(g, G)) (only those must be on the device yet), adjointFinish(x)
+        // writes the result. The views of the groups partition [0, np) in order.
+        virtual int forwardGroups() const { return 0; }
+        virtual int adjointGroups() const { return 0; }
+        virtual std::pair<int, int> forwardGroupViews(int g, int G) const
+        {
+            return {static_cast<int>(static_cast<int64_t>(det_.np) * g / G),
+                    static_cast<int>(static_cast<int64_t>(det_.np) * (g + 1) / G)};
+        }
+        virtual std::pair<int, int> adjointGroupViews(int g, int G) const
+        {
+            return forwardGroupViews(g, G);
+        }
+        virtual void prepareForward(const float* x, cudaStream_t s)
+        {
+            (void)x;
+            (void)s;
+        }
+        virtual void forwardGroup(const float* x, float* y, int g, int G, cudaStream_t s)
+        {
+            (void)x, (void)y, (void)g, (void)G, (void)s;
+        }
+        virtual void adjointGroup(const float* y, int g, int G, cudaStream_t s)
+        {
+            (void)y, (void)g, (void)G, (void)s;
+        }
+        virtual void adjointFinish(float* x, cudaStream_t s)
+        {
+            (void)x, (void)s;
+        }
 
     protected:
         Projector(int kind, const VolumeShape& vol, const DetectorShape& det,

@@ -94,8 +94,13 @@ def test_joseph_adjointness_and_determinism(cuda, oracle, name):
     assert np.array_equal(Ax.view(np.uint32), Ax2.view(np.uint32))
 
 
-def test_joseph_host_entry_points(cuda, oracle):
-    poses, det = oracle.circle_trajectory((32, 32, 32), 20, 360, 320, 80, [48, 48])
+@pytest.mark.parametrize("views", [3, 20, 30])
+def test_joseph_host_entry_points(cuda, oracle, views):
+    """Host-buffer entry points: with enough views the 3D operator pipelines the copies of view
+    groups with the kernels; the results equal the device entry points bit for bit (also with a
+    one-chunk adjoint, which takes the plain path)."""
+    import elsa_b200
+    poses, det = oracle.circle_trajectory((32, 32, 32), views, 360, 320, 80, [48, 48])
     proj = _projector((32, 32, 32), det, poses)
     rng = np.random.default_rng(3)
     x = rng.uniform(0, 1, 32 ** 3).astype(np.float32)
@@ -103,6 +108,13 @@ def test_joseph_host_entry_points(cuda, oracle):
     Ax, Aty = _gpu_pair(cuda, proj, x, y)
     assert np.array_equal(proj.apply_host(x), Ax)
     assert np.array_equal(proj.apply_adjoint_host(y), Aty)
+    xp = cuda.from_numpy(x).pin_memory().numpy()  # page-locked buffers take the async copies
+    yp = cuda.from_numpy(y).pin_memory().numpy()
+    assert np.array_equal(proj.apply_host(xp), Ax)
+    assert np.array_equal(proj.apply_adjoint_host(yp), Aty)
+    proj.set_knob(elsa_b200.KNOB_ADJOINT_CHUNKS, 1)
+    _, Aty1 = _gpu_pair(cuda, proj, x, y)
+    assert np.array_equal(proj.apply_adjoint_host(y), Aty1)
 
 
 @pytest.mark.slow
