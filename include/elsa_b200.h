@@ -235,7 +235,11 @@ elsa_status elsa_projector_apply_adjoint(elsa_projector* projector, const float*
 
 /* Host-buffer variants, synchronous: copy the input to the device, run, copy the output back
  * (the call pattern of the reference's CUDA projectors, which copy in and out on every apply,
- * JosephsMethodCUDA.cpp:132-214). */
+ * JosephsMethodCUDA.cpp:132-214). For the 3D Joseph operator (matched adjoint in view chunks)
+ * the copies of the sinogram overlap the kernels: the forward copies finished groups of views
+ * out while later groups run, the adjoint copies groups of views in while earlier groups run
+ * (page-locked host buffers let the copies run asynchronously). Results equal the device-buffer
+ * entry points bit for bit. */
 elsa_status elsa_projector_apply_host(elsa_projector* projector, const float* x, float* y);
 elsa_status elsa_projector_apply_adjoint_host(elsa_projector* projector, const float* y,
                                               float* x);
