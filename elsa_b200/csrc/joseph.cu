@@ -1422,11 +1422,30 @@ namespace elsa_b200
             }
 
             // Host-buffer pipelining: kHostGroups groups of views for the TMA forward; for the
-            // chunked 3D brick-owner adjoint, groups of whole view chunks.
+            // chunked 3D brick-owner adjoint, groups of whole view chunks. Only the copy of the
+            // forward's last group and of the adjoint's first group are not overlapped with a
+            // kernel, so those groups are small: the forward's groups hold 30/30/30/10 % of
+            // the views, the adjoint's first group one view chunk and the rest thirds.
             static constexpr int kHostGroups = 4;
             int forwardGroups() const override
             {
-                return tma_ && det_.np >= kHostGroups ? kHostGroups : 0;
+                return tma_ && det_.np >= 10 ? kHostGroups : 0;
+            }
+            std::pair<int, int> forwardGroupViews(int g, int G) const override
+            {
+                static constexpr int kEnd[kHostGroups + 1] = {0, 30, 60, 90, 100};
+                (void)G;
+                return {static_cast<int>(static_cast<int64_t>(det_.np) * kEnd[g] / 100),
+                        static_cast<int>(static_cast<int64_t>(det_.np) * kEnd[g + 1] / 100)};
+            }
+            // first chunk of adjoint group g (g = 0 .. kHostGroups)
+            int groupChunk(int g) const
+            {
+                const int used = usedChunks();
+                if (g == 0)
+                    return 0;
+                return 1 + static_cast<int>(static_cast<int64_t>(used - 1) * (g - 1) /
+                                            (kHostGroups - 1));
             }
             void prepareForward(const float* x, cudaStream_t s) override { tma_->prepare(x, s); }
             void forwardGroup(const float* x, float* y, int g, int G, cudaStream_t s) override
@@ -1447,18 +1466,16 @@ namespace elsa_b200
             }
             std::pair<int, int> adjointGroupViews(int g, int G) const override
             {
+                (void)G;
                 const int per = (det_.np + adjointChunks_ - 1) / adjointChunks_;
-                const int used = usedChunks();
-                const int c0 = static_cast<int>(static_cast<int64_t>(used) * g / G);
-                const int c1 = static_cast<int>(static_cast<int64_t>(used) * (g + 1) / G);
-                return {std::min(det_.np, c0 * per), std::min(det_.np, c1 * per)};
+                return {std::min(det_.np, groupChunk(g) * per),
+                        std::min(det_.np, groupChunk(g + 1) * per)};
             }
             void adjointGroup(const float* y, int g, int G, cudaStream_t s) override
             {
+                (void)G;
                 const int per = (det_.np + adjointChunks_ - 1) / adjointChunks_;
-                const int used = usedChunks();
-                const int c0 = static_cast<int>(static_cast<int64_t>(used) * g / G);
-                const int c1 = static_cast<int>(static_cast<int64_t>(used) * (g + 1) / G);
+                const int c0 = groupChunk(g), c1 = groupChunk(g + 1);
                 Adjoint3d::launchChunks(nBricks_.x * nBricks_.y * nBricks_.z, c0, c1, per, s,
                                         dRays_, dCheckpoints_, rangeSize_, y, dWindows_,
                                         dViewAxes_, vol_, det_, classSpacing_, nBricks_,
