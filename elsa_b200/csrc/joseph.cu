@@ -1320,6 +1320,13 @@ namespace elsa_b200
                 fastTable_ = std::make_unique<DeviceBuffer>(sizeof(float) * table.size());
                 ELSA_CUDA(cudaMemcpy(fastTable_->as<float>(), table.data(),
                                      sizeof(float) * table.size(), cudaMemcpyHostToDevice));
+                cudaDeviceProp prop{};
+                ELSA_CUDA(cudaGetDeviceProperties(&prop, device_));
+                const int* lim = d == 3 ? prop.maxTexture2DLayered : prop.maxTexture1DLayered;
+                if (det_.nu > lim[0] || (d == 3 && det_.nv > lim[1]) || det_.np > lim[d - 1])
+                    throw Error(ELSA_ERROR_NOT_SUPPORTED,
+                                "JosephsMethodCUDA: the fast adjoint's layered texture cannot "
+                                "hold this detector (size or number of poses)");
                 const cudaChannelFormatDesc fd =
                     cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
                 const cudaExtent ext =
