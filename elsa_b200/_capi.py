@@ -229,6 +229,9 @@ class Projector:
         if ps.size != POSE_FLOATS * self.det_dims[-1]:
             raise InvalidArgumentError(1, "pose array does not match the number of poses")
         prm = np.ascontiguousarray(params if params is not None else [], np.float32)
+        # False for JosephsMethodCUDA's `fast` adjoint (Joseph parameter 1), which is not the
+        # transpose of the forward
+        self.matched = not (int(kind) == PROJECTOR_JOSEPH and prm.size > 0 and prm[0] != 0)
         h = ctypes.c_void_p()
         self.curved = None if curved is None else (float(curved[0]), float(curved[1]))
         if self.curved is None:

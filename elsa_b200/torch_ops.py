@@ -4,8 +4,11 @@
 native matched adjoint (the adjoint is the exact transpose of the forward, so gradients are exact
 up to float rounding). ``x`` is a CUDA float32 tensor whose last dimension holds the volume
 (x fastest); leading dimensions are a batch. ``op`` is an ``elsa_b200.Projector`` or a
-``elsa_b200.pyelsa`` operator.
+``elsa_b200.pyelsa`` operator. With JosephsMethodCUDA's ``fast`` adjoint (not the transpose) the
+gradients are only approximate; a warning says so once per operator.
 """
+import warnings
+
 import torch
 
 __all__ = ["project", "backproject", "Projection"]
@@ -39,6 +42,12 @@ class _Project(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, op, adjoint):
         ctx.op, ctx.adjoint = op, adjoint
+        native = _native(op)
+        if not getattr(native, "matched", True) and not getattr(native, "_warned", False):
+            native._warned = True
+            warnings.warn("this operator's adjoint is JosephsMethodCUDA's fast backprojection, "
+                          "not the transpose of the forward: gradients are approximate",
+                          RuntimeWarning, stacklevel=3)
         return _run(op, x, adjoint)
 
     @staticmethod

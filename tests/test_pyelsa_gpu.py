@@ -218,3 +218,23 @@ def test_pyelsa_fast_flag(cuda, oracle):
     a_fast_x_fastest = np.asarray(fast.applyAdjoint(y)).ravel(order="F")
     assert np.array_equal(a_fast_x_fastest, out.cpu().numpy())
     assert not np.array_equal(a_fast, a_matched)
+
+
+def test_autograd_warns_for_the_fast_adjoint(cuda, oracle):
+    """Gradients through JosephsMethodCUDA(..., fast=True) use its unmatched backprojection: the
+    torch op says so (once per operator); the matched operator stays silent."""
+    import warnings
+
+    from elsa_b200.torch_ops import project
+    elsa, vol, sino = _setup(oracle, n=16, views=8, det=24)
+    fast = elsa.JosephsMethodCUDA(vol, sino, fast=True)
+    matched = elsa.JosephsMethodCUDA(vol, sino)
+    assert not fast.native.matched and matched.native.matched
+    x = cuda.rand(16 ** 3, device="cuda", requires_grad=True)
+    with warnings.catch_warnings(record=True) as caught:
+        warnings.simplefilter("always")
+        project(x, matched).sum().backward()
+        assert not caught
+        project(x, fast).sum().backward()
+        project(x, fast).sum().backward()
+    assert len([w for w in caught if issubclass(w.category, RuntimeWarning)]) == 1
