@@ -231,10 +231,13 @@ def test_autograd_warns_for_the_fast_adjoint(cuda, oracle):
     matched = elsa.JosephsMethodCUDA(vol, sino)
     assert not fast.native.matched and matched.native.matched
     x = cuda.rand(16 ** 3, device="cuda", requires_grad=True)
+    def ours(caught):
+        return [w for w in caught if "fast backprojection" in str(w.message)]
+
     with warnings.catch_warnings(record=True) as caught:
         warnings.simplefilter("always")
         project(x, matched).sum().backward()
-        assert not caught
+        assert not ours(caught)
         project(x, fast).sum().backward()
         project(x, fast).sum().backward()
-    assert len([w for w in caught if issubclass(w.category, RuntimeWarning)]) == 1
+    assert len(ours(caught)) == 1
