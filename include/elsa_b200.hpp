@@ -348,6 +348,19 @@ namespace elsa_b200
                 return hit != 0;
             }
 
+            // launch knobs (ELSA_KNOB_*, elsa_projector_get_knob / _set_knob): e.g.
+            // setKnob(ELSA_KNOB_ADJOINT_SCATTER, 0) selects Siddon's bit-reproducible adjoint
+            int32_t getKnob(int32_t knob) const
+            {
+                int32_t v = -1;
+                check(elsa_projector_get_knob(handle_.get(), knob, &v));
+                return v;
+            }
+            void setKnob(int32_t knob, int32_t value)
+            {
+                check(elsa_projector_set_knob(handle_.get(), knob, value));
+            }
+
             const DataDescriptor& getDomainDescriptor() const { return *domain_; }
             const DataDescriptor& getRangeDescriptor() const { return *range_; }
             elsa_projector* handle() const { return handle_.get(); }

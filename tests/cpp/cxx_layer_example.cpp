@@ -72,6 +72,15 @@ int main(int argc, char** argv)
         for (size_t i = 0; i < blocks.size(); ++i)
             save(dir + "/block" + std::to_string(i) + ".f32", blocks[i].toHost());
 
+        // Siddon with its bit-reproducible brick-owner adjoint instead of the atomic scatter
+        SiddonsMethodCUDA<float> S(*vol, *sino);
+        const auto scatterAdj = S.applyAdjoint(b).toHost();
+        S.setKnob(ELSA_KNOB_ADJOINT_SCATTER, 0);
+        if (S.getKnob(ELSA_KNOB_ADJOINT_SCATTER) != 0)
+            throw elsa_b200::Error(ELSA_ERROR_LOGIC, "knob not set");
+        save(dir + "/siddon_adj_scatter.f32", scatterAdj);
+        save(dir + "/siddon_adj_owner.f32", S.applyAdjoint(b).toHost());
+
         // BinaryMethod and the ray-driven blob / B-spline projectors (forward of the phantom)
         BinaryMethod<float> binary(*vol, *sino);
         save(dir + "/binary.f32", binary.apply(x).toHost());

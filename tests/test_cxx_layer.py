@@ -87,6 +87,10 @@ def test_cxx_layer_runs(cuda, oracle, tmp_path):
     ref = oracle.lut_project(False, xf, vol, det, poses, oracle.bspline_lut(3, 2),
                              oracle.bspline_support(2), 2)
     assert rel_l2(_load(tmp_path, "raybspline.f32"), ref) <= 1e-5
+    # Siddon's two adjoints: the same sums in another order
+    ref = oracle.siddon_adjoint(b, vol, det, poses)
+    for name in ("siddon_adj_scatter.f32", "siddon_adj_owner.f32"):
+        assert rel_l2(_load(tmp_path, name), ref) <= 1e-5, name
     # the curved detector
     coords = oracle.curved_coords(3, 36, 36, 0.6, 300.0)
     np.testing.assert_array_equal(_load(tmp_path, "curved_coords.f32"),
