@@ -47,6 +47,9 @@
 #ifndef ELSA_ADJ_MIN_BLOCKS
 #define ELSA_ADJ_MIN_BLOCKS 1 // resident one-warp blocks per SM asked of the register allocator
 #endif
+#ifndef ELSA_ADJ_BATCH
+#define ELSA_ADJ_BATCH 2 // class rays per lane fetched together (3D adjoint; at 256^3 / 360 views 1: 64.0 ms, 2: 54.9, 3: 55.3, 4: 60.8)
+#endif
 #ifndef ELSA_SPLAT_UNROLL
 #define ELSA_SPLAT_UNROLL 2 // unroll factor of the adjoint's per-sample loop (1: 72.8 ms, 2: 63.4 ms, 4: 68.9 ms at 256^3)
 #endif
@@ -990,7 +993,7 @@ namespace elsa_b200
                     // up to kBatch class rays per lane are fetched together (record,
                     // checkpoint and detector value are independent loads: the brick is one
                     // checkpoint slab deep, so the checkpoint row is known up front)
-                    constexpr int kBatch = 2;
+                    constexpr int kBatch = ELSA_ADJ_BATCH;
                     const int64_t cpRow = static_cast<int64_t>(orgG / CPD + 1) * nrays;
                     for (int base = lane; base < total; base += 32 * kBatch) {
                         JosephRay Rb[kBatch];
