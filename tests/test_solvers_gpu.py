@@ -117,15 +117,6 @@ def _cg_bound(x32, x64, hist32, hist64):
             max(1e-3 * hist32[-1], 4.0 * abs(hist32[-1] - hist64[-1])))
 
 
-def _assert_cg_close(x, x32, x64):
-    """The device iterate is within the CG_TOL bound of the FP32 oracle, or at least as close to
-    the FP64 oracle as the FP32 oracle is (times 2). The second form covers ill-conditioned cases
-    where the FP32 oracle's own run-to-run variation (its adjoint adds with OpenMP atomics) is of
-    the size of the bound."""
-    e32, e64, spread = rel_l2(x, x32), rel_l2(x, x64), rel_l2(x32, x64)
-    assert e32 <= max(CG_TOL, 4.0 * spread) or e64 <= 2.0 * spread, (e32, e64, spread)
-
-
 def _run_solver(torch, proj, kind, b_np, iterations, params=(), x0=None, chunks=1):
     import elsa_b200
     b = torch.from_numpy(np.ascontiguousarray(b_np, np.float32)).cuda()
@@ -187,9 +178,23 @@ def test_cgls_parity(cuda, oracle, name):
     # damped, warm start from a seeded random x0
     x0 = np.random.default_rng(3).random(n).astype(np.float32)
     x, _, _ = _run_solver(cuda, proj, elsa_b200.SOLVER_CGLS, b, 8, params=(2.0, 1e-4), x0=x0)
-    xr, hr = S.cgls(A, At, b, n, 8, x0=x0, eps=2.0)
+    # The FP32 oracle's own result varies from run to run here (its adjoint adds with OpenMP
+    # atomics; on fan2d_64 eight runs landed 2.4e-4 to 1.3e-3 from the FP64 oracle, the
+    # single-threaded, deterministic run 8.7e-4): the device must be as close to the FP64 oracle
+    # as twice the farthest of three FP32 oracle runs (one single-threaded), or within CG_TOL of
+    # one of them.
     x64, h64 = S.cgls(A64, At64, b, n, 8, x0=x0, eps=2.0, dtype=np.float64)
-    _assert_cg_close(x, xr, x64)
+    threads = oracle.num_threads()
+    oracle.set_num_threads(1)
+    try:
+        runs = [S.cgls(A, At, b, n, 8, x0=x0, eps=2.0)[0]]
+    finally:
+        oracle.set_num_threads(threads)
+    runs += [S.cgls(A, At, b, n, 8, x0=x0, eps=2.0)[0] for _ in range(2)]
+    worst = max(rel_l2(xr, x64) for xr in runs)
+    e32 = min(rel_l2(x, xr) for xr in runs)
+    assert e32 <= CG_TOL or rel_l2(x, x64) <= max(CG_TOL, 2.0 * worst), (e32, rel_l2(x, x64),
+                                                                            worst)
 
 
 def test_cgls_tolerance_stops(cuda, oracle):
