@@ -129,6 +129,53 @@ def cpu_baseline_sample(views_in_sample, vol, poses, det, x):
     return 2.0 * np.prod(vol) * len(idx) / dt / 1e9, dt, O.num_threads()
 
 
+PARITY_VIEWS = (0, 45, 90, 135, 180, 225, 270, 315)
+
+
+def parity_block(torch, proj, vol, poses, det, x_true):
+    """Relative L2 of the benchmarked operator (the same projector handle, its kernels, view
+    chunks and knobs) against the FP32 and FP64 oracle on a fixed subset of the views, outside the
+    timed region. Forward: the rows of the subset's views of A x_true. Adjoint: A^T y with y
+    seeded U(0,1) on the subset's views and zero on all others, which equals the oracle's adjoint
+    over the subset's views alone."""
+    from oracle import oracle as O
+    O.build()
+    idx = np.array(PARITY_VIEWS)
+    view = int(det[0]) * int(det[1])
+    sub = np.ascontiguousarray(poses[idx])
+    dsub = np.array([det[0], det[1], len(idx)])
+    s = torch.cuda.current_stream().cuda_stream
+    xt = torch.from_numpy(np.ascontiguousarray(x_true).ravel()).cuda()
+    Ax = torch.empty(proj.range_size, dtype=torch.float32, device="cuda")
+    proj.apply_ptr(xt.data_ptr(), Ax.data_ptr(), s)
+    ysub = np.random.default_rng(2).uniform(0, 1, len(idx) * view).astype(np.float32)
+    yfull = np.zeros(proj.range_size, np.float32)
+    for i, v in enumerate(idx):
+        yfull[v * view:(v + 1) * view] = ysub[i * view:(i + 1) * view]
+    yd = torch.from_numpy(yfull).cuda()
+    Aty = torch.empty(proj.domain_size, dtype=torch.float32, device="cuda")
+    proj.apply_adjoint_ptr(yd.data_ptr(), Aty.data_ptr(), s)
+    torch.cuda.synchronize()
+    fwd = Ax.cpu().numpy().reshape(-1, view)[idx].ravel()
+    adj = Aty.cpu().numpy()
+    del xt, Ax, yd, Aty
+
+    def rel(a, b):
+        a, b = np.asarray(a, np.float64).ravel(), np.asarray(b, np.float64).ravel()
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    f32 = O.joseph(x_true, vol, dsub, sub)
+    a32 = O.joseph_adjoint(ysub, vol, dsub, sub)
+    f64 = O.joseph(x_true.astype(np.float64), vol, dsub, sub, dtype=np.float64)
+    a64 = O.joseph_adjoint(ysub.astype(np.float64), vol, dsub, sub, dtype=np.float64)
+    return {"views": [int(v) for v in idx], "bound": 1e-5,
+            "forward_vs_f32": rel(fwd, f32), "forward_vs_f64": rel(fwd, f64),
+            "adjoint_vs_f32": rel(adj, a32), "adjoint_vs_f64": rel(adj, a64),
+            "oracle_f32_vs_f64": {"forward": rel(f32, f64), "adjoint": rel(a32, a64)},
+            "how": "the benchmarked projector handle; oracle on the listed views; "
+                   "x = modified Shepp-Logan, y = U(0,1) seed 2 on those views"}
+
+
 def _traffic_from_profiles():
     """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "joseph_cone256_traffic.json")
@@ -235,7 +282,7 @@ def run_elsa(args):
     h2d = 4 * (proj.domain_size + proj.range_size)
     d2h = 4 * (proj.range_size + proj.domain_size)
 
-    # roofline of the dominant kernel (algorithmic gather bytes)
+    # roofline of the dominant kernel: algorithmic gather bytes 4 (N_vol + N_sino) + 16 S per pass
     samples = proj.info(2)
     bytes_per_pass = 4.0 * (proj.domain_size + proj.range_size) + 16.0 * samples
     fwd_avg, adj_avg = fwd_ms / max(timed, 1), adj_ms / max(timed, 1)
@@ -276,6 +323,8 @@ def run_elsa(args):
         "gpu_launches": (proj.info(6) + proj.info(7) + VECTOR_LAUNCHES_PER_STEP) * args.steps,
         "clocks": clock_info,
     }
+    if rank == 0 and not args.no_parity:
+        out["parity"] = parity_block(torch, proj, vol, poses, det, x_true)
     if rank == 0 and world == 1 and not args.no_batched:
         out["batched"] = batched_vs_plain(torch, elsa_b200, phantoms)
     if rank == 0 and world == 1 and args.batched_full:
@@ -487,6 +536,8 @@ def main():
                          "this arm, about 10 s on 16 host threads; for --impl reference as many "
                          "as keep the whole run near 90 s, 4 to 60)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the parity block (oracle check of the benchmarked operator)")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-vs-plain small-problem measurement")
     ap.add_argument("--batched-full", action="store_true",

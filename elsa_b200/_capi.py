@@ -83,6 +83,7 @@ SIGNATURES = {
     "elsa_projector_destroy": (_st, [_vp]),
     "elsa_projector_sizes": (_st, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "elsa_projector_info": (_st, [_vp, _i32, ctypes.POINTER(_i64)]),
+    "elsa_projector_wait_test": (_st, [_vp, _i64, _i32]),
     "elsa_projector_get_knob": (_st, [_vp, _i32, ctypes.POINTER(_i32)]),
     "elsa_projector_knob_candidates": (_st, [_vp, _i32, _vp, _i32, ctypes.POINTER(_i32)]),
     "elsa_projector_set_knob": (_st, [_vp, _i32, _i32]),
@@ -256,6 +257,10 @@ class Projector:
         v = ctypes.c_int64()
         call("elsa_projector_info", self._h, int(key), ctypes.byref(v))
         return v.value
+
+    def wait_test(self, wait_cycles, withhold_copies):
+        """Test hook of the bounded device waits (elsa_projector_wait_test)."""
+        call("elsa_projector_wait_test", self._h, int(wait_cycles), int(bool(withhold_copies)))
 
     def knob(self, knob):
         """Current value of a launch knob (KNOB_*), -1 when this projector does not use it."""

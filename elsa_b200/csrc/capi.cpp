@@ -32,12 +32,21 @@ struct elsa_projector {
     std::vector<cudaEvent_t> hostEvents;
     ~elsa_projector()
     {
+        // streams and events belong to the projector's device: destroy them with it current
+        int prev = -1;
+        const bool any = hostCompute || hostCopy || !hostEvents.empty();
+        if (any && impl && cudaGetDevice(&prev) == cudaSuccess && prev != impl->device())
+            cudaSetDevice(impl->device());
+        else
+            prev = -1;
         for (cudaEvent_t e : hostEvents)
             cudaEventDestroy(e);
         if (hostCompute)
             cudaStreamDestroy(hostCompute);
         if (hostCopy)
             cudaStreamDestroy(hostCopy);
+        if (prev >= 0)
+            cudaSetDevice(prev);
     }
 };
 
@@ -372,6 +381,18 @@ elsa_status elsa_projector_info(const elsa_projector* p, int32_t key, int64_t* v
     });
 }
 
+elsa_status elsa_projector_wait_test(elsa_projector* p, int64_t waitCycles, int32_t withholdCopies)
+{
+    return guarded([&] {
+        require(p, "elsa_projector_wait_test: null argument");
+        onDevice(p);
+        if (!p->impl->setWaitTest(waitCycles, withholdCopies != 0))
+            throw elsa_b200::Error(ELSA_ERROR_NOT_SUPPORTED,
+                                   "elsa_projector_wait_test: this projector has no bounded "
+                                   "device waits");
+    });
+}
+
 elsa_status elsa_projector_get_knob(const elsa_projector* p, int32_t knob, int32_t* value)
 {
     return guarded([&] {
@@ -527,6 +548,7 @@ static void hostApply(elsa_projector* p, const float* in, float* out, bool adjoi
         }
         cudaStream_t sc = p->hostCompute, sx = p->hostCopy;
         const int64_t view = P.rangeSize() / P.detector().np;
+        try {
         if (!adjoint) {
             ELSA_CUDA(cudaMemcpyAsync(din, in, sizeof(float) * nin, cudaMemcpyHostToDevice, sc));
             P.prepareForward(din, sc);
@@ -555,6 +577,13 @@ static void hostApply(elsa_projector* p, const float* in, float* out, bool adjoi
                                       sc));
             ELSA_CUDA(cudaStreamSynchronize(sc));
         }
+        } catch (...) {
+            // copies into or out of the caller's buffers may still be queued: finish them
+            // before the error returns, so that no late copy touches a buffer the caller reuses
+            cudaStreamSynchronize(sc);
+            cudaStreamSynchronize(sx);
+            throw;
+        }
         return;
     }
     ELSA_CUDA(cudaMemcpy(din, in, sizeof(float) * nin, cudaMemcpyHostToDevice));
@@ -581,13 +610,37 @@ elsa_status elsa_projector_apply_adjoint_host(elsa_projector* p, const float* y,
     });
 }
 
+namespace
+{
+    // The partial sums of one reduction, taken from the device's stream-ordered memory pool on
+    // the call's stream and returned to it on the same stream: no device-wide synchronization
+    // (as cudaMalloc/cudaFree have), no wait on the host, and calls on different streams get
+    // separate buffers.
+    class StreamPartials
+    {
+    public:
+        explicit StreamPartials(cudaStream_t s) : s_(s)
+        {
+            ELSA_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p_),
+                                      sizeof(double) * elsa_b200::kReduceBlocks, s_));
+        }
+        ~StreamPartials() { cudaFreeAsync(p_, s_); }
+        StreamPartials(const StreamPartials&) = delete;
+        StreamPartials& operator=(const StreamPartials&) = delete;
+        double* get() const { return p_; }
+
+    private:
+        cudaStream_t s_;
+        double* p_ = nullptr;
+    };
+} // namespace
+
 elsa_status elsa_dot(const float* x, const float* y, int64_t n, double* result, void* stream)
 {
     return guarded([&] {
         require(result && n >= 0 && ((x && y) || n == 0), "elsa_dot: invalid argument");
-        elsa_b200::DeviceBuffer partials(sizeof(double) * elsa_b200::kReduceBlocks);
-        elsa_b200::launchDot(x, y, n, partials.as<double>(), result, asStream(stream));
-        ELSA_CUDA(cudaStreamSynchronize(asStream(stream)));
+        StreamPartials partials(asStream(stream));
+        elsa_b200::launchDot(x, y, n, partials.get(), result, asStream(stream));
     });
 }
 
@@ -601,9 +654,8 @@ elsa_status elsa_squared_l2_norm(const float* x, int64_t n, double* result, void
 {
     return guarded([&] {
         require(result && n >= 0 && (x || n == 0), "elsa_squared_l2_norm: invalid argument");
-        elsa_b200::DeviceBuffer partials(sizeof(double) * elsa_b200::kReduceBlocks);
-        elsa_b200::launchSquaredNorm(x, n, partials.as<double>(), result, asStream(stream));
-        ELSA_CUDA(cudaStreamSynchronize(asStream(stream)));
+        StreamPartials partials(asStream(stream));
+        elsa_b200::launchSquaredNorm(x, n, partials.get(), result, asStream(stream));
     });
 }
 

@@ -1556,6 +1556,14 @@ namespace elsa_b200
                 adjointChunks_ = value;
             }
 
+            bool setWaitTest(long long cycles, bool withhold) override
+            {
+                if (!tma_)
+                    return false;
+                tma_->setWaitTest(cycles, withhold);
+                return true;
+            }
+
             int64_t info(int key) const override
             {
                 switch (key) {

@@ -12,8 +12,11 @@
 // box; tiles whose rays disagree on axis or direction, or do not fit the box, use the per-ray
 // gather (the same arithmetic as josephForwardKernel).
 //
-// All waits on mbarriers are bounded (about one second of clock cycles); on timeout the CTA
-// records an error word and returns.
+// All waits on mbarriers are bounded (about one second of clock cycles by default); on timeout the
+// CTA records bit 0 of the error word, waits (bounded again) for the copies it has issued and
+// not yet consumed, and returns. For tests of that path, setWaitTest() shortens the limit and can
+// withhold the copies (the barriers then expect bytes that never arrive), so the waits run out
+// without any fault.
 #include "joseph_tma.cuh"
 
 #include <cudaTypedefs.h>
@@ -33,7 +36,6 @@ namespace elsa_b200
         constexpr int kStageFloats = BW * BH * BD;
         constexpr unsigned kStageBytes = kStageFloats * sizeof(float);
         constexpr int kFlagFallback = 8;
-        constexpr long long kWaitCycles = 2000000000LL; // ~1 s at 2 GHz
 
         __device__ __forceinline__ int floorDivI(int a, int b)
         {
@@ -72,14 +74,14 @@ namespace elsa_b200
             return ok != 0;
         }
 
-        // Bounded wait; false on timeout.
-        __device__ __forceinline__ bool mbarWait(uint64_t* bar, unsigned parity)
+        // Bounded wait of at most `limit` clock cycles; false on timeout.
+        __device__ __forceinline__ bool mbarWait(uint64_t* bar, unsigned parity, long long limit)
         {
             if (mbarTryWait(bar, parity))
                 return true;
             const long long t0 = clock64();
             while (!mbarTryWait(bar, parity)) {
-                if (clock64() - t0 > kWaitCycles)
+                if (clock64() - t0 > limit)
                     return false;
             }
             return true;
@@ -281,7 +283,8 @@ namespace elsa_b200
                              const int2* __restrict__ origins, int maxChunks,
                              const float* __restrict__ x, VolumeShape vol, DetectorShape det,
                              int tilesU, int tilesV, int3 fastAxis, float* __restrict__ y,
-                             unsigned* __restrict__ error, int tileBase)
+                             unsigned* __restrict__ error, int tileBase, long long waitCycles,
+                             int withhold)
         {
             extern __shared__ __align__(128) float stage[];
             __shared__ __align__(8) uint64_t full[NS];
@@ -324,16 +327,18 @@ namespace elsa_b200
                 const int2 o = org[ch];
                 const int gOrg = dir > 0 ? T.kStart + ch * BD : T.kStart - ch * BD - (BD - 1);
                 mbarExpectTx(&full[s], kStageBytes);
-                tmaLoad3d(stage + s * kStageFloats, map, o.x, o.y, gOrg, &full[s]);
+                if (!withhold) // test mode: the barrier waits for bytes that never come
+                    tmaLoad3d(stage + s * kStageFloats, map, o.x, o.y, gOrg, &full[s]);
             };
             if (threadIdx.x == 0)
                 for (int ch = 0; ch < NS && ch < T.nChunks; ++ch)
                     issue(ch);
             float acc = 0.0f;
             float pf = c.pf, ps = c.ps;
+            int failed = -1; // chunk whose wait timed out
             for (int ch = 0; ch < T.nChunks; ++ch) {
                 const int s = ch % NS;
-                const bool ready = mbarWait(&full[s], (ch / NS) & 1);
+                const bool ready = mbarWait(&full[s], (ch / NS) & 1, waitCycles);
                 if (!ready) {
                     atomicOr(error, 1u);
                     abortFlag = 1;
@@ -361,10 +366,20 @@ namespace elsa_b200
                     }
                 }
                 __syncthreads();
-                if (abortFlag)
-                    break; // a copy never completed: leave without issuing more
+                if (abortFlag) { // a copy never completed: issue no more
+                    failed = ch;
+                    break;
+                }
                 if (threadIdx.x == 0 && ch + NS < T.nChunks)
                     issue(ch + NS);
+            }
+            if (failed >= 0) {
+                // chunks failed .. failed + NS - 1 were issued and not consumed: give their
+                // copies a bounded time to land before the CTA's shared memory goes away
+                if (threadIdx.x == 0)
+                    for (int ch = failed; ch < failed + NS && ch < T.nChunks; ++ch)
+                        mbarWait(&full[ch % NS], (ch / NS) & 1, waitCycles);
+                __syncthreads();
             }
             if (valid)
                 y[r] = c.n > 0 ? R.len * acc : 0.0f;
@@ -519,8 +534,16 @@ namespace elsa_b200
         forwardTmaKernel<<<static_cast<unsigned>(count), NT, NS * kStageBytes, s>>>(
             maps_[0], maps_[1], maps_[2], dRays_, dTiles_, dChunkOrigins_, maxChunks_, x, vol_,
             det_, tilesU_, tilesV_, make_int3(fast_[0], fast_[1], fast_[2]), y, dError_,
-            static_cast<int>(perView * p0));
+            static_cast<int>(perView * p0), waitCycles_, withhold_ ? 1 : 0);
         ELSA_LAUNCH_CHECK("forwardTmaKernel");
+    }
+
+    void JosephForwardTma::setWaitTest(long long cycles, bool withhold)
+    {
+        ELSA_CUDA(cudaDeviceSynchronize()); // no launch of the old setting in flight
+        waitCycles_ = cycles > 0 ? cycles : kDefaultWaitCycles;
+        withhold_ = withhold;
+        ELSA_CUDA(cudaMemset(dError_, 0, sizeof(unsigned)));
     }
 
     unsigned JosephForwardTma::errorWord() const

@@ -48,6 +48,11 @@ namespace elsa_b200
             return 1 + (present_[0] ? 1 : 0) + (present_[1] ? 1 : 0) + (present_[2] ? 1 : 0);
         }
         unsigned errorWord() const;
+        // Test hook for the bounded waits: limit them to `cycles` clock cycles (<= 0: the
+        // default, about one second) and, with `withhold`, issue no copies, so every wait runs
+        // out and sets bit 0 of the error word. Clears the error word.
+        void setWaitTest(long long cycles, bool withhold);
+        static constexpr long long kDefaultWaitCycles = 2000000000LL; // ~1 s at 2 GHz
 
     private:
         VolumeShape vol_;
@@ -65,5 +70,7 @@ namespace elsa_b200
         std::array<int, 3> padFast_{{0, 0, 0}};
         std::array<CUtensorMap, 3> maps_{};
         double fallbackFraction_ = 0.0;
+        long long waitCycles_ = kDefaultWaitCycles;
+        bool withhold_ = false;
     };
 } // namespace elsa_b200

@@ -18,6 +18,9 @@
 //   array and may return wrong sums; order them on one stream.
 // * The device address of the array is looked up once per device (cudaGetSymbolAddress) by the
 //   first call made with that device current; make that first call before any stream capture.
+//   The address is kept for the life of the process: after a cudaDeviceReset (or anything else
+//   that re-creates the device's primary context) the module may load elsewhere, so this entry
+//   point does not support a device reset after its first call on that device.
 #include "internal.cuh"
 #include "vecops.cuh"
 

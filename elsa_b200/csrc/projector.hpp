@@ -88,6 +88,13 @@ namespace elsa_b200
             return -1;
         }
         virtual void setKnob(int knob, int value);
+        // Test hook of the bounded device waits (elsa_projector_wait_test): false when this
+        // projector has none.
+        virtual bool setWaitTest(long long cycles, bool withhold)
+        {
+            (void)cycles, (void)withhold;
+            return false;
+        }
 
         // Pipelining of the host-buffer entry points (optional). forwardGroups() > 1: after
         // prepareForward(x), forwardGroup(x, y, g, G) writes the rays of the views

@@ -21,7 +21,11 @@ __all__ = ["view_block", "NativeVectorOps", "TorchVectorOps", "ShardedCGNE"]
 
 
 def view_block(num_views, rank, world):
-    """Contiguous block [lo, hi) of views for `rank`; blocks differ in size by at most one."""
+    """Contiguous block [lo, hi) of views for `rank`; blocks differ in size by at most one.
+    Every rank needs at least one view: ValueError when there are more ranks than views."""
+    if int(world) > int(num_views):
+        raise ValueError("view sharding needs at least one view per rank: %d views for %d ranks"
+                         % (int(num_views), int(world)))
     base, extra = divmod(int(num_views), int(world))
     lo = rank * base + min(rank, extra)
     return lo, lo + base + (1 if rank < extra else 0)

@@ -170,6 +170,18 @@ elsa_status elsa_projector_sizes(const elsa_projector* projector, int64_t* domai
  * projector, 6 / 7 = kernel launches per forward / adjoint call. */
 elsa_status elsa_projector_info(const elsa_projector* projector, int32_t key, int64_t* value);
 
+/* Test hook of the bounded device waits (no counterpart in the reference, whose kernels do not
+ * wait on one another). The TMA-staged Joseph forward (3D) waits on shared-memory barriers for its
+ * volume copies; every wait gives up after a limit (about one second of clock cycles), records
+ * bit 0 of the error word (elsa_projector_info key 3), waits (bounded again) for the copies it
+ * issued and returns, so the GPU context stays usable. This call sets the limit to waitCycles
+ * clock cycles (<= 0: the default) and, with withholdCopies != 0, makes the forward issue no
+ * copies, so that every wait runs out: a test of that path without any fault. The forward's
+ * output is then undefined. Clears the error word; synchronizes the device. Returns
+ * ELSA_ERROR_NOT_SUPPORTED for projectors without bounded waits. */
+elsa_status elsa_projector_wait_test(elsa_projector* projector, int64_t waitCycles,
+                                     int32_t withholdCopies);
+
 /* Launch parameters ("knobs") of a projector. None of them changes the operator: every value
  * computes the same forward and adjoint up to float rounding (adjoint view chunks only change
  * the order in which per-chunk partial volumes are added). The reference has no counterpart;
@@ -223,7 +235,14 @@ elsa_status elsa_tune_cache_put(const char* key, const int32_t* values);
 elsa_status elsa_tune_cache_get(const char* key, int32_t* values, int32_t* found);
 
 /* y = A x on device buffers. Replaces LinearOperator::apply(x, Ax), core/LinearOperator.cpp:94-98
- * -> XrayProjector::applyImpl -> JosephsMethodCUDA::forward, JosephsMethodCUDA.cpp:132-214. */
+ * -> XrayProjector::applyImpl -> JosephsMethodCUDA::forward, JosephsMethodCUDA.cpp:132-214.
+ * Asynchronous on `stream`.
+ * Concurrency: a projector owns device scratch that its applies write (the TMA forward's
+ * permuted copies of x, the adjoint's per-view-chunk partial volumes, staging buffers of the
+ * host-buffer entry points). Applies of ONE projector must therefore be ordered: issue them on
+ * one stream, or order the streams with events. Different projectors (also of the same geometry)
+ * may run concurrently on any streams. The reference's CUDA projectors are not reentrant either
+ * (they share the device and synchronize it on every call). */
 elsa_status elsa_projector_apply(elsa_projector* projector, const float* x, float* y,
                                  void* stream);
 
@@ -248,8 +267,12 @@ elsa_status elsa_projector_apply_adjoint_host(elsa_projector* projector, const f
  * Vector operations on device float buffers; scalar results are float64 in device memory
  * ------------------------------------------------------------------------------------------- */
 
-/* *result = <x, y>. Replaces DataContainer::dot, core/DataContainer.cpp:403-417
- * (storage/reductions/DotProduct.h:24-47). */
+/* *result = <x, y>, accumulated in float64 in a fixed order (bit-reproducible). Replaces
+ * DataContainer::dot, core/DataContainer.cpp:403-417 (storage/reductions/DotProduct.h:24-47).
+ * result is device memory; the call is asynchronous on `stream` (read the result after the
+ * stream's work). Its partial sums come from the device's stream-ordered memory pool
+ * (cudaMallocAsync / cudaFreeAsync on `stream`), which neither synchronizes the device nor waits
+ * on the host. */
 elsa_status elsa_dot(const float* x, const float* y, int64_t n, double* result, void* stream);
 
 /* Largest n accepted by elsa_dot_no_alloc. */
@@ -263,11 +286,13 @@ elsa_status elsa_dot(const float* x, const float* y, int64_t n, double* result, 
  * ELSA_ERROR_INVALID_ARGUMENT). result is device memory; the call is asynchronous on `stream`.
  * All calls on a device share the array: calls that may run at the same time on the GPU race and
  * must be ordered on one stream. The first call on a device looks up the array's device address;
- * make that first call before any stream capture. */
+ * make that first call before any stream capture. The address is kept for the life of the
+ * process, so a device reset (cudaDeviceReset) after that first call is not supported. */
 elsa_status elsa_dot_no_alloc(const float* x, const float* y, int64_t n, double* result,
                               void* stream);
 
-/* *result = |x|_2^2. Replaces DataContainer::squaredL2Norm (storage/reductions/L2.h:15-49). */
+/* *result = |x|_2^2, like elsa_dot (float64, asynchronous, result in device memory). Replaces
+ * DataContainer::squaredL2Norm (storage/reductions/L2.h:15-49). */
 elsa_status elsa_squared_l2_norm(const float* x, int64_t n, double* result, void* stream);
 
 /* out = a*x + b*y. Replaces lincomb(a, x, b, y, out), core/DataContainer.cpp:1075-1108

@@ -641,6 +641,40 @@ namespace orc
         }
     }
 
+    // ------------------------------------------------------------------------------------------
+    // Adjoint accumulation in a fixed order. The reference adds every contribution with
+    // `omp atomic` (JosephsMethod.cpp:180-186, SiddonsMethod.cpp:119), so its float sums change
+    // from run to run. Here the rays are split into `chunks` contiguous ranges, a number that
+    // depends on the problem size only; one thread scatters each range, in ray order, into a
+    // partial volume of its own, and the partial volumes are added in range order. The result is
+    // the same for every thread count and every run.
+    // ------------------------------------------------------------------------------------------
+    template <typename data_t, class RayFn>
+    static void orderedScatter(index_t nrays, index_t nvol, data_t* out, RayFn rayFn)
+    {
+        const index_t bytes = std::max<index_t>(1, nvol * static_cast<index_t>(sizeof(data_t)));
+        index_t chunks = std::min<index_t>(32, std::max<index_t>(1, (index_t(1) << 31) / bytes));
+        chunks = std::min<index_t>(chunks, std::max<index_t>(1, nrays));
+        std::fill(out, out + nvol, data_t(0));
+        std::vector<data_t> partial(static_cast<size_t>((chunks - 1) * nvol), data_t(0));
+#pragma omp parallel for schedule(dynamic, 1)
+        for (index_t c = 0; c < chunks; ++c) {
+            data_t* dst = c == 0 ? out : partial.data() + (c - 1) * nvol;
+            const index_t lo = nrays * c / chunks, hi = nrays * (c + 1) / chunks;
+            for (index_t ir = lo; ir < hi; ++ir)
+                rayFn(ir, dst);
+        }
+        if (chunks > 1) {
+#pragma omp parallel for schedule(static)
+            for (index_t v = 0; v < nvol; ++v) {
+                data_t s = out[v];
+                for (index_t c = 1; c < chunks; ++c)
+                    s += partial[static_cast<size_t>((c - 1) * nvol + v)];
+                out[v] = s;
+            }
+        }
+    }
+
     // mode 0: reference position update (pos += step each step, DrivingDirectionTraversal.cpp:265)
     // mode 1: pos_j = fma(j, step, pos_0) (one rounding; used to isolate the accumulation drift)
     template <typename data_t, bool adjoint>
@@ -658,10 +692,8 @@ namespace orc
             nvol *= volDims[i];
         }
         const index_t nrays = (dim == 2 ? detDims[0] : detDims[0] * detDims[1]) * numPoses;
-        if (adjoint)
-            std::fill(out, out + nvol, data_t(0));
-#pragma omp parallel for schedule(dynamic, 256)
-        for (index_t ir = 0; ir < nrays; ++ir) {
+        // one ray; the adjoint adds into dst (a partial volume of orderedScatter)
+        auto ray = [&](index_t ir, data_t* dst) {
             const Ray r = rayForIndex(poses.data(), dim, detDims, ir, coords);
             DDTraversal tr = ddSetup(boxMax, dim, r);
             const data_t L = static_cast<data_t>(tr.length);
@@ -675,9 +707,7 @@ namespace orc
                 if (adjoint) {
                     const data_t y = in[ir];
                     josephTaps(pos, tr.driving, dim, volDims, [&](index_t idx, float wt) {
-                        const data_t v = y * L * static_cast<data_t>(wt);
-#pragma omp atomic
-                        out[idx] += v;
+                        dst[idx] += y * L * static_cast<data_t>(wt);
                     });
                 } else {
                     josephTaps(pos, tr.driving, dim, volDims, [&](index_t idx, float wt) {
@@ -690,7 +720,14 @@ namespace orc
             }
             if (!adjoint)
                 out[ir] = acc;
+        };
+        if (adjoint) {
+            orderedScatter<data_t>(nrays, nvol, out, ray);
+            return;
         }
+#pragma omp parallel for schedule(dynamic, 256)
+        for (index_t ir = 0; ir < nrays; ++ir)
+            ray(ir, nullptr);
     }
 
     // ------------------------------------------------------------------------------------------
@@ -715,12 +752,10 @@ namespace orc
             nvol *= volDims[i];
         }
         const index_t nrays = (dim == 2 ? detDims[0] : detDims[0] * detDims[1]) * numPoses;
-        if (adjoint)
-            std::fill(out, out + nvol, data_t(0));
         const float EPS = std::numeric_limits<float>::epsilon();
         const float MAXF = std::numeric_limits<float>::max();
-#pragma omp parallel for schedule(dynamic, 256)
-        for (index_t ir = 0; ir < nrays; ++ir) {
+        // one ray; the adjoint adds into dst (a partial volume of orderedScatter)
+        auto ray = [&](index_t ir, data_t* dst) {
             const Ray r = rayForIndex(poses.data(), dim, detDims, ir, coords);
             data_t acc = 0;
             float tmin, tmax;
@@ -786,16 +821,12 @@ namespace orc
                             ++visits[ir];
                         if (binary) {
                             if (adjoint) {
-                                const data_t v = in[ir];
-#pragma omp atomic
-                                out[idx] += v;
+                                dst[idx] += in[ir];
                             } else {
                                 acc += in[idx];
                             }
                         } else if (adjoint) {
-                            const data_t v = in[ir] * static_cast<data_t>(weight);
-#pragma omp atomic
-                            out[idx] += v;
+                            dst[idx] += in[ir] * static_cast<data_t>(weight);
                         } else {
                             acc += in[idx] * static_cast<data_t>(weight);
                         }
@@ -807,7 +838,14 @@ namespace orc
             }
             if (!adjoint)
                 out[ir] = acc;
+        };
+        if (adjoint) {
+            orderedScatter<data_t>(nrays, nvol, out, ray);
+            return;
         }
+#pragma omp parallel for schedule(dynamic, 256)
+        for (index_t ir = 0; ir < nrays; ++ir)
+            ray(ir, nullptr);
     }
 
     // ------------------------------------------------------------------------------------------
@@ -1041,10 +1079,8 @@ namespace orc
         for (int i = 0; i < dim; ++i)
             nvol *= volDims[i];
         const index_t nrays = (dim == 2 ? detDims[0] : detDims[0] * detDims[1]) * numPoses;
-        if (adjoint)
-            std::fill(out, out + nvol, data_t(0));
-#pragma omp parallel for schedule(dynamic, 64)
-        for (index_t ir = 0; ir < nrays; ++ir) {
+        // one ray; the adjoint adds into dst (a partial volume of orderedScatter)
+        auto ray = [&](index_t ir, data_t* dst) {
             const Ray r = rayForIndex(poses.data(), dim, detDims, ir);
             if (adjoint) {
                 const data_t y = in[ir];
@@ -1052,9 +1088,7 @@ namespace orc
                        [&](index_t idx, float wt) {
                            if (idx < 0 || idx >= nvol)
                                return;
-                           const data_t v = static_cast<data_t>(wt) * y;
-#pragma omp atomic
-                           out[idx] += v;
+                           dst[idx] += static_cast<data_t>(wt) * y;
                        });
             } else {
                 data_t acc = 0;
@@ -1066,7 +1100,14 @@ namespace orc
                        });
                 out[ir] = acc;
             }
+        };
+        if (adjoint) {
+            orderedScatter<data_t>(nrays, nvol, out, ray);
+            return;
         }
+#pragma omp parallel for schedule(dynamic, 64)
+        for (index_t ir = 0; ir < nrays; ++ir)
+            ray(ir, nullptr);
     }
 
     // ------------------------------------------------------------------------------------------

@@ -4,14 +4,16 @@ ProjectVoxelsCUDA.cu), compiled from the reference sources where they lie, with 
 headers in shim/ and the host harness refcuda.cu. TEST INFRASTRUCTURE ONLY: the library lets the
 GPU tests time the reference's kernels beside this library's on the same device.
 
-Run here (where the reference tree exists): python -m oracle.ref_cuda.build
-The built library travels with the repository snapshot; the reference tree is not needed to load
-it."""
+Run where the reference tree exists: ELSA_REFERENCE_DIR=<root of the reference checkout>
+python -m oracle.ref_cuda.build (the recipe looks for <root>/elsa/projectors_cuda/...; without the
+variable it looks at the checkout location of the build container). The built library travels
+with the repository snapshot; the reference tree is not needed to load it."""
 import os
 import subprocess
 import sys
 
-REFERENCE = "/root/reference/elsa"
+# root of the reference checkout (its elsa/ source tree), for this build recipe only
+REFERENCE = os.path.join(os.environ.get("ELSA_REFERENCE_DIR", "/root/reference"), "elsa")
 _HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(os.path.dirname(_HERE), "_ref")
 LIB = os.path.join(OUT_DIR, "librefcuda.so")

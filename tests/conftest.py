@@ -39,3 +39,18 @@ def cuda():
     from elsa_b200 import build
     build.build()
     return torch
+
+
+def record_parity(case, **fields):
+    """Append one parity result (relative L2 distances, bounds) as a JSON line to the file named
+    by ELSA_PARITY_RECORD; a no-op when it is unset. The committed parity record is made from
+    these lines."""
+    import json
+    path = os.environ.get("ELSA_PARITY_RECORD")
+    if not path:
+        return
+    entry = {"case": case}
+    for k, v in fields.items():
+        entry[k] = float(v) if isinstance(v, (np.floating, np.integer)) else v
+    with open(path, "a") as f:
+        f.write(json.dumps(entry, sort_keys=True) + "\n")

@@ -2,7 +2,7 @@
 tests/golden/shepp_logan_2d_16.json.
 
 Reads elsa/generators/tests/test_Phantoms.cpp:145-187 as text (the `expected` vector, x fastest).
-Usage: python tests/golden/make_phantom_goldens.py [reference_root]
+Usage: python tests/golden/make_phantom_goldens.py <reference_root>
 """
 import json
 import os
@@ -13,7 +13,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: %s <root of the reference checkout>" % sys.argv[0])
+    root = sys.argv[1]
     path = os.path.join(root, "elsa", "generators", "tests", "test_Phantoms.cpp")
     src = open(path).read()
     at = src.index('TEST_CASE_TEMPLATE("Phantoms: Drawing a 2d Shepp-Logan phantom"')

@@ -7,7 +7,7 @@ Reads the reference test sources as text (C++ doctest files; nothing is compiled
                                                  {2.5, 5, 7.5, 10.83}, m in {1, 2}, s = i/100
   elsa/projectors/tests/test_BlobGradientHelper.cpp  the same arrays (used there as expected[i]/s)
 
-Usage: python tests/golden/make_voxel_goldens.py [reference_root]
+Usage: python tests/golden/make_voxel_goldens.py <reference_root>
 """
 import json
 import os
@@ -81,7 +81,9 @@ def derivative_goldens(src):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: %s <root of the reference checkout>" % sys.argv[0])
+    root = sys.argv[1]
     tests = os.path.join(root, "elsa", "projectors", "tests")
     with open(os.path.join(tests, "test_Luts.cpp")) as f:
         luts = lut_goldens(f.read())

@@ -185,3 +185,29 @@ def test_fast_adjoint_arguments(cuda, oracle):
     with pytest.raises(elsa_b200.ElsaError):
         elsa_b200.Projector(elsa_b200.PROJECTOR_JOSEPH, (16, 16, 16), dd, poses, [1.0],
                             curved=(0.5, 200.0))
+
+
+def test_bounded_wait_runs_out(cuda, oracle):
+    """The TMA forward's barrier waits are bounded: with the copies withheld and a short limit
+    every wait runs out, the kernel records bit 0 of the error word and returns, and the context
+    stays usable: the next forward (copies restored) is correct and leaves the word at 0."""
+    import elsa_b200
+    vol = (32, 32, 32)
+    poses, det = oracle.circle_trajectory(vol, 24, 360, 320, 80, [48, 48])
+    proj = _projector(vol, det, poses)
+    rng = np.random.default_rng(8)
+    x = rng.uniform(0, 1, 32 ** 3).astype(np.float32)
+    y = rng.uniform(0, 1, int(np.prod(det))).astype(np.float32)
+    assert proj.info(3) == 0
+    proj.wait_test(20000, True)  # ~10 microseconds per wait, no copies issued
+    _gpu_pair(cuda, proj, x, y)
+    assert proj.info(3) & 1
+    proj.wait_test(0, False)  # default limit, copies issued; clears the error word
+    assert proj.info(3) == 0
+    Ax, _ = _gpu_pair(cuda, proj, x, y)
+    assert proj.info(3) == 0
+    assert rel_l2(Ax, oracle.joseph(x, vol, det, poses)) <= PARITY
+    # projectors without bounded waits refuse the hook
+    siddon = elsa_b200.Projector(elsa_b200.PROJECTOR_SIDDON, vol, det, poses)
+    with pytest.raises(elsa_b200.ElsaError):
+        siddon.wait_test(20000, True)

@@ -128,3 +128,27 @@ def test_accumulated_positions_matter(oracle):
     y0 = oracle.joseph(x, vol, dd, poses, mode=0)
     y1 = oracle.joseph(x, vol, dd, poses, mode=1)
     assert rel_l2(y1, y0) > 1e-6
+
+
+def test_oracle_adjoints_deterministic(oracle):
+    """The oracle's adjoints add their contributions in a fixed order (ray ranges scattered into
+    partial volumes, summed in range order): the same bits for every thread count and run."""
+    vol = (20, 24, 28)
+    poses, det = oracle.circle_trajectory(vol, 12, 360, 200, 50, [32, 30])
+    y = np.random.default_rng(4).uniform(0, 1, int(np.prod(det))).astype(np.float32)
+    fns = [lambda: oracle.joseph_adjoint(y, vol, det, poses),
+           lambda: oracle.siddon_adjoint(y, vol, det, poses),
+           lambda: oracle.binary_adjoint(y, vol, det, poses),
+           lambda: oracle.joseph_adjoint(y.astype(np.float64), vol, det, poses,
+                                         dtype=np.float64)]
+    threads = oracle.num_threads()
+    try:
+        oracle.set_num_threads(1)
+        single = [f() for f in fns]
+        oracle.set_num_threads(max(2, threads))
+        multi = [f() for f in fns]
+        again = [f() for f in fns]
+    finally:
+        oracle.set_num_threads(threads)
+    for a, b, c in zip(single, multi, again):
+        assert np.array_equal(a, b) and np.array_equal(b, c)

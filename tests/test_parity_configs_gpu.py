@@ -1,0 +1,319 @@
+"""Parity at the full sizes of the benchmark configurations, through the C ABI, against the
+deterministic FP32 oracle, with the distance to the FP64 oracle stated for every result.
+
+* cone-beam 256^3, 360 views over 360 degrees, 384^2 detector, source-centre 2560,
+  centre-detector 640: Joseph forward and adjoint on all views, the seeded U(0,1) adjoint dot
+  test, Siddon forward and adjoint on a view subset, and 30 CGNE iterations (the first against
+  the oracle, all of them through properties that hold at any size);
+* fan-beam 128^2, 180 views, 1000 / 250, 182 pixels, modified Shepp-Logan plus seeded Gaussian
+  noise sigma = 0.01 on the sinogram: 20 iterations of CGNE, CGLS, FGM, OGM and SQS;
+* cone-beam 128^3 of 20 seeded random ellipsoids, 180 views, 192^2 detector: blob, B-spline and
+  both phase-contrast voxel projectors, forward and adjoint, on every fourth view.
+
+Each result is appended to the parity record (conftest.record_parity) when ELSA_PARITY_RECORD
+names a file.
+"""
+import numpy as np
+import pytest
+
+from conftest import record_parity, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+PARITY = 1e-5  # relative L2 vs the FP32 CPU path (elsa's isApprox, testHelpers.h:190-206)
+
+
+def _apply(torch, proj, x_np, adjoint=False):
+    src = torch.from_numpy(np.ascontiguousarray(x_np, np.float32).ravel()).cuda()
+    n = proj.domain_size if adjoint else proj.range_size
+    out = torch.full((n,), np.nan, dtype=torch.float32, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    if adjoint:
+        proj.apply_adjoint_ptr(src.data_ptr(), out.data_ptr(), s)
+    else:
+        proj.apply_ptr(src.data_ptr(), out.data_ptr(), s)
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+# ------------------------------------------------------------------------------------------------
+# cone-beam 256^3 / 360 views / 384^2
+# ------------------------------------------------------------------------------------------------
+CONE256 = dict(vol=(256, 256, 256), views=360, s2c=2560, c2d=640, det=[384, 384])
+
+
+@pytest.fixture(scope="module")
+def cone256(oracle):
+    c = CONE256
+    poses, det = oracle.circle_trajectory(c["vol"], c["views"], 360, c["s2c"], c["c2d"],
+                                          c["det"])
+    return c["vol"], poses, det
+
+
+def _joseph(vol, det, poses):
+    import elsa_b200
+    return elsa_b200.Projector(elsa_b200.PROJECTOR_JOSEPH, vol, det, poses)
+
+
+@pytest.mark.slow
+def test_cone256_joseph_all_views(cuda, oracle, cone256):
+    from elsa_b200 import phantoms
+    vol, poses, det = cone256
+    proj = _joseph(vol, det, poses)
+    x = phantoms.modified_shepp_logan(vol)
+    y = np.random.default_rng(2).uniform(0, 1, int(np.prod(det))).astype(np.float32)
+    Ax = _apply(cuda, proj, x)
+    Aty = _apply(cuda, proj, y, adjoint=True)
+    assert proj.info(3) == 0  # no timed-out pipeline wait
+    del proj
+    f32, a32 = oracle.joseph(x, vol, det, poses), oracle.joseph_adjoint(y, vol, det, poses)
+    e_f, e_a = rel_l2(Ax, f32), rel_l2(Aty, a32)
+    f64 = oracle.joseph(x.astype(np.float64), vol, det, poses, dtype=np.float64)
+    a64 = oracle.joseph_adjoint(y.astype(np.float64), vol, det, poses, dtype=np.float64)
+    fields = dict(fwd_gpu_f32=e_f, fwd_gpu_f64=rel_l2(Ax, f64), fwd_f32_f64=rel_l2(f32, f64),
+                  adj_gpu_f32=e_a, adj_gpu_f64=rel_l2(Aty, a64), adj_f32_f64=rel_l2(a32, a64),
+                  bound=PARITY)
+    record_parity("cone256_joseph_360_views", **fields)
+    print(fields)
+    assert e_f <= PARITY
+    assert e_a <= PARITY
+
+
+def test_cone256_adjoint_dot(cuda, cone256):
+    """<A x, y> = <x, A^T y> with x, y ~ U(0,1) (seeds 1 and 2), dots in float64 on the host."""
+    vol, poses, det = cone256
+    proj = _joseph(vol, det, poses)
+    x = np.random.default_rng(1).uniform(0, 1, int(np.prod(vol))).astype(np.float32)
+    y = np.random.default_rng(2).uniform(0, 1, int(np.prod(det))).astype(np.float32)
+    Ax = _apply(cuda, proj, x).astype(np.float64)
+    Aty = _apply(cuda, proj, y, adjoint=True).astype(np.float64)
+    lhs, rhs = float(Ax @ y), float(x.astype(np.float64) @ Aty)
+    rel = abs(lhs - rhs) / abs(lhs)
+    record_parity("cone256_joseph_adjoint_dot", rel_diff=rel, bound=1e-6)
+    assert rel <= 1e-6, (lhs, rhs)
+
+
+SIDDON_VIEWS = np.arange(0, 360, 15)  # 24 of the 360 poses
+
+
+@pytest.mark.slow
+def test_cone256_siddon_view_subset(cuda, oracle, cone256):
+    import elsa_b200
+    from elsa_b200 import phantoms
+    vol, poses, det = cone256
+    sub = np.ascontiguousarray(poses[SIDDON_VIEWS])
+    dsub = np.array([det[0], det[1], len(SIDDON_VIEWS)])
+    x = phantoms.modified_shepp_logan(vol)
+    y = np.random.default_rng(2).uniform(0, 1, int(np.prod(dsub))).astype(np.float32)
+    fields = {}
+    for scheme in (0, 1):  # the default scheme, then the other adjoint scheme (same operator)
+        proj = elsa_b200.Projector(elsa_b200.PROJECTOR_SIDDON, vol, dsub, sub)
+        if scheme:
+            other = 1 - proj.knob(elsa_b200.KNOB_ADJOINT_SCATTER)
+            proj.set_knob(elsa_b200.KNOB_ADJOINT_SCATTER, other)
+        Ax = _apply(cuda, proj, x)
+        Aty = _apply(cuda, proj, y, adjoint=True)
+        fields["scheme%d" % scheme] = (Ax, Aty)
+        del proj
+    f32, a32 = oracle.siddon(x, vol, dsub, sub), oracle.siddon_adjoint(y, vol, dsub, sub)
+    f64 = oracle.siddon(x.astype(np.float64), vol, dsub, sub, dtype=np.float64)
+    a64 = oracle.siddon_adjoint(y.astype(np.float64), vol, dsub, sub, dtype=np.float64)
+    Ax, Aty = fields["scheme0"]
+    Ax1, Aty1 = fields["scheme1"]
+    rec = dict(fwd_gpu_f32=rel_l2(Ax, f32), fwd_gpu_f64=rel_l2(Ax, f64),
+               fwd_f32_f64=rel_l2(f32, f64), adj_gpu_f32=rel_l2(Aty, a32),
+               adj_gpu_f64=rel_l2(Aty, a64), adj_f32_f64=rel_l2(a32, a64),
+               adj_other_scheme_f32=rel_l2(Aty1, a32), views=len(SIDDON_VIEWS), bound=PARITY)
+    record_parity("cone256_siddon_24_views", **rec)
+    print(rec)
+    assert np.array_equal(Ax, Ax1)
+    assert rec["fwd_gpu_f32"] <= PARITY
+    assert rec["adj_gpu_f32"] <= PARITY
+    assert rec["adj_other_scheme_f32"] <= PARITY
+
+
+@pytest.mark.slow
+def test_cone256_cgne_30(cuda, oracle, cone256):
+    """30 CGNE iterations at full size. With b = A x_true, CGNE minimises |A (x - x_true)| =
+    |b - A x| over growing Krylov spaces, so |b - A x_k| must not increase; the recurrence
+    residual |r_k|^2 must track the true |A^T (b - A x_k)|^2; the first iterate x_1 =
+    alpha A^T b is checked against the oracle."""
+    import elsa_b200
+    from elsa_b200 import phantoms
+    torch = cuda
+    vol, poses, det = cone256
+    proj = _joseph(vol, det, poses)
+    xt = phantoms.modified_shepp_logan(vol)
+    b = _apply(torch, proj, xt)
+    bd = torch.from_numpy(b).cuda()
+    x = torch.zeros(proj.domain_size, dtype=torch.float32, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    solver = elsa_b200.Solver(elsa_b200.SOLVER_CGNE, proj, bd.data_ptr(), x.data_ptr(), stream=s)
+    Ax = torch.empty(proj.range_size, dtype=torch.float32, device="cuda")
+    data_res, x1 = [], None
+    for k in range(30):
+        solver.iterate(1, s)
+        proj.apply_ptr(x.data_ptr(), Ax.data_ptr(), s)
+        torch.cuda.synchronize()
+        data_res.append(float(torch.sum((bd.double() - Ax.double()) ** 2)))
+        if k == 0:
+            x1 = x.cpu().numpy()
+    rec_res = solver.squared_residual(s)
+    g = torch.empty(proj.domain_size, dtype=torch.float32, device="cuda")
+    diff = (bd - Ax).contiguous()
+    proj.apply_adjoint_ptr(diff.data_ptr(), g.data_ptr(), s)
+    torch.cuda.synchronize()
+    true_res = float(torch.sum(g.double() ** 2))
+    solver.close()
+    del proj
+    # oracle first iterate: x_1 = (|A^T b|^2 / |A A^T b|^2) A^T b (CGNE.cpp:50-73 with x0 = 0)
+    atb = oracle.joseph_adjoint(b, vol, det, poses).astype(np.float64)
+    aatb = oracle.joseph(atb.astype(np.float32), vol, det, poses).astype(np.float64)
+    alpha = np.float32(float(atb @ atb) / float(aatb @ aatb))
+    x1_ref = (alpha * atb.astype(np.float32)).astype(np.float32)
+    e1 = rel_l2(x1, x1_ref)
+    rises = [data_res[i + 1] / data_res[i] - 1.0 for i in range(29)]
+    rec = dict(x1_gpu_f32=e1, data_residual_first=data_res[0], data_residual_last=data_res[-1],
+               worst_relative_rise=max(rises), recurrence_vs_true_residual=abs(rec_res - true_res)
+               / true_res, bound=PARITY)
+    record_parity("cone256_cgne_30", **rec)
+    print(rec)
+    assert e1 <= PARITY
+    assert max(rises) <= 1e-4  # non-increasing up to float32 rounding of the data residual
+    assert data_res[-1] < 0.05 * data_res[0]
+    assert abs(rec_res - true_res) <= 0.05 * true_res
+
+
+# ------------------------------------------------------------------------------------------------
+# fan-beam 128^2 / 180 views / 182 pixels, noisy sinogram, 20 iterations
+# ------------------------------------------------------------------------------------------------
+FAN128 = dict(vol=(128, 128), views=180, s2c=1000, c2d=250, det=[182])
+
+# Fixed bounds per solver on the relative L2 distance between the device iterate and the FP32
+# oracle's after 20 iterations; both sides are deterministic, so the distance is one number,
+# recorded with the FP32-FP64 distance in the parity record. CG-type recurrences amplify the
+# last-bit differences of the projectors (device and oracle sum in different orders).
+SOLVER_BOUNDS = {"cgne": 1e-4, "cgls": 1e-4, "fgm": 1e-4, "ogm": 1e-4, "sqs": 1e-4}
+
+
+@pytest.fixture(scope="module")
+def fan128(oracle):
+    from elsa_b200 import phantoms
+    c = FAN128
+    poses, det = oracle.circle_trajectory(c["vol"], c["views"], 360, c["s2c"], c["c2d"],
+                                          c["det"])
+    x = np.asarray(phantoms.modified_shepp_logan(tuple(reversed(c["vol"]))), np.float32)
+    b = oracle.joseph(x.ravel(), c["vol"], det, poses).ravel()
+    b = (b + phantoms.gaussian_noise(b.shape, 0.01, seed=0)).astype(np.float32)
+    return c["vol"], poses, det, b
+
+
+def _solve(torch, proj, kind, b_np, iterations):
+    import elsa_b200
+    b = torch.from_numpy(np.ascontiguousarray(b_np, np.float32)).cuda()
+    x = torch.zeros(proj.domain_size, dtype=torch.float32, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    solver = elsa_b200.Solver(kind, proj, b.data_ptr(), x.data_ptr(), stream=s)
+    solver.iterate(iterations, s)
+    torch.cuda.synchronize()
+    out = x.cpu().numpy()
+    solver.close()
+    return out
+
+
+@pytest.mark.parametrize("name", sorted(SOLVER_BOUNDS))
+def test_fan128_solvers_20(cuda, oracle, fan128, name):
+    import elsa_b200
+    from oracle import solvers as S
+    vol, poses, det, b = fan128
+    proj = _joseph(vol, det, poses)
+    n = int(np.prod(vol))
+    kind = {"cgne": elsa_b200.SOLVER_CGNE, "cgls": elsa_b200.SOLVER_CGLS,
+            "fgm": elsa_b200.SOLVER_FGM, "ogm": elsa_b200.SOLVER_OGM,
+            "sqs": elsa_b200.SOLVER_SQS}[name]
+    x = _solve(cuda, proj, kind, b, 20)
+    A = lambda v: oracle.joseph(v, vol, det, poses).ravel()  # noqa: E731
+    At = lambda v: oracle.joseph_adjoint(v, vol, det, poses).ravel()  # noqa: E731
+    A64 = lambda v: oracle.joseph(np.asarray(v, np.float64), vol, det, poses,  # noqa: E731
+                                  dtype=np.float64).ravel()
+    At64 = lambda v: oracle.joseph_adjoint(np.asarray(v, np.float64), vol, det,  # noqa: E731
+                                           poses, dtype=np.float64).ravel()
+    if name == "cgne":
+        xr, _ = S.cgne(A, At, b, n, 20)
+        x64, _ = S.cgne(A64, At64, b, n, 20, dtype=np.float64)
+    elif name == "cgls":
+        xr, _ = S.cgls(A, At, b, n, 20)
+        x64, _ = S.cgls(A64, At64, b, n, 20, dtype=np.float64)
+    elif name == "sqs":
+        xr = S.sqs(A, At, b, n, 20)[0]
+        x64 = S.sqs(A64, At64, b, n, 20, dtype=np.float64)[0]
+    else:
+        xr = getattr(S, name)(A, At, b, n, 20)[0]
+        x64 = getattr(S, name)(A64, At64, b, n, 20, dtype=np.float64)[0]
+    rec = dict(gpu_f32=rel_l2(x, xr), gpu_f64=rel_l2(x, x64), f32_f64=rel_l2(xr, x64),
+               bound=SOLVER_BOUNDS[name])
+    record_parity("fan128_%s_20" % name, **rec)
+    print(name, rec)
+    assert rec["gpu_f32"] <= SOLVER_BOUNDS[name]
+
+
+def test_fan128_joseph(cuda, oracle, fan128):
+    vol, poses, det, b = fan128
+    from elsa_b200 import phantoms
+    proj = _joseph(vol, det, poses)
+    x = np.asarray(phantoms.modified_shepp_logan(tuple(reversed(vol))), np.float32)
+    Ax = _apply(cuda, proj, x)
+    Atb = _apply(cuda, proj, b, adjoint=True)
+    f32, a32 = oracle.joseph(x, vol, det, poses), oracle.joseph_adjoint(b, vol, det, poses)
+    f64 = oracle.joseph(x.astype(np.float64), vol, det, poses, dtype=np.float64)
+    a64 = oracle.joseph_adjoint(b.astype(np.float64), vol, det, poses, dtype=np.float64)
+    rec = dict(fwd_gpu_f32=rel_l2(Ax, f32), fwd_gpu_f64=rel_l2(Ax, f64),
+               fwd_f32_f64=rel_l2(f32, f64), adj_gpu_f32=rel_l2(Atb, a32),
+               adj_gpu_f64=rel_l2(Atb, a64), adj_f32_f64=rel_l2(a32, a64), bound=PARITY)
+    record_parity("fan128_joseph", **rec)
+    assert rec["fwd_gpu_f32"] <= PARITY
+    assert rec["adj_gpu_f32"] <= PARITY
+
+
+# ------------------------------------------------------------------------------------------------
+# cone-beam 128^3 random ellipsoids / 180 views / 192^2: the voxel projectors
+# ------------------------------------------------------------------------------------------------
+VOXEL_KINDS = {"blob": 2, "bspline": 3, "phase_blob": 4, "phase_bspline": 5}
+VOXEL_VIEWS = np.arange(0, 180, 4)  # 45 of the 180 poses
+
+
+@pytest.fixture(scope="module")
+def cone128_ellipsoids(oracle):
+    from elsa_b200 import phantoms
+    vol = (128, 128, 128)
+    poses, det = oracle.circle_trajectory(vol, 180, 360, 1280.0, 320.0, [192, 192])
+    sub = np.ascontiguousarray(poses[VOXEL_VIEWS])
+    dsub = np.array([192, 192, len(VOXEL_VIEWS)])
+    x = phantoms.random_ellipsoids(128, 20, seed=0)
+    y = np.random.default_rng(3).uniform(0, 1, int(np.prod(dsub))).astype(np.float32)
+    return vol, sub, dsub, x, y
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("name", sorted(VOXEL_KINDS))
+def test_cone128_voxel_projectors(cuda, oracle, cone128_ellipsoids, name):
+    import elsa_b200
+    vol, poses, det, x, y = cone128_ellipsoids
+    params = (2.0, 10.83, 2.0) if name.endswith("blob") else (2.0,)
+    proj = elsa_b200.Projector(VOXEL_KINDS[name], vol, det, poses, params)
+    Ax = _apply(cuda, proj, x)
+    Aty = _apply(cuda, proj, y, adjoint=True)
+    del proj
+    lut, support, wk = oracle.voxel_lut(name, 3)
+    f32 = oracle.voxel_project(False, x, vol, det, poses, lut, support, wk, 0)
+    a32 = oracle.voxel_project(True, y, vol, det, poses, lut, support, wk, 0)
+    f64 = oracle.voxel_project(False, x, vol, det, poses, lut, support, wk, 0, np.float64)
+    a64 = oracle.voxel_project(True, y, vol, det, poses, lut, support, wk, 0, np.float64)
+    rec = dict(fwd_gpu_f32=rel_l2(Ax, f32), fwd_gpu_f64=rel_l2(Ax, f64),
+               fwd_f32_f64=rel_l2(f32, f64), adj_gpu_f32=rel_l2(Aty, a32),
+               adj_gpu_f64=rel_l2(Aty, a64), adj_f32_f64=rel_l2(a32, a64),
+               views=len(VOXEL_VIEWS), bound=PARITY)
+    record_parity("cone128_ellipsoids_%s_45_views" % name, **rec)
+    print(name, rec)
+    assert rec["fwd_gpu_f32"] <= PARITY
+    assert rec["adj_gpu_f32"] <= PARITY

@@ -58,12 +58,14 @@ def _rank_main(rank, world, port, out_path):
 
 def test_view_block_partition():
     from elsa_b200.sharded import view_block
-    for n, w in ((360, 8), (17, 4), (5, 5), (3, 4)):
+    for n, w in ((360, 8), (17, 4), (5, 5), (3, 3)):
         blocks = [view_block(n, r, w) for r in range(w)]
         assert blocks[0][0] == 0 and blocks[-1][1] == n
         assert all(blocks[i][1] == blocks[i + 1][0] for i in range(w - 1))
         sizes = [hi - lo for lo, hi in blocks]
-        assert max(sizes) - min(sizes) <= 1
+        assert max(sizes) - min(sizes) <= 1 and min(sizes) >= 1
+    with pytest.raises(ValueError, match="at least one view per rank"):
+        view_block(3, 0, 4)
 
 
 def test_sharded_cgne_two_gloo_ranks(tmp_path):

@@ -3,17 +3,19 @@
 cudaMalloc/cudaFree synchronize the device, so a caller inside a latency-bound loop, or a host
 that routes all device memory through its own pool, cannot let the library allocate per call.
 elsa_dot_no_alloc keeps its partial sums in a fixed device array instead. This file checks it
-against elsa_dot through the C ABI, on two calls in a row (the shared array keeps the previous
-call's contents, which must not leak into the next result), and that sizes beyond the array's
-limit are refused. The file name sorts last so that a run stopping at the first failure has run
+against elsa_dot through the C ABI and against numpy's float64 sum, on two calls in a row (the
+shared array keeps the previous call's contents, which must not leak into the next result), that
+sizes beyond the array's limit are refused, and that its translation unit references no
+allocation routine. The file name sorts last so that a run stopping at the first failure has run
 every other test before it.
 """
 import ctypes
+import os
+import shutil
+import subprocess
 
 import numpy as np
 import pytest
-
-pytestmark = pytest.mark.gpu
 
 # Both entry points sum float products in float64, in different orders; the tolerance is the one
 # the vector-op tests use against a float64 numpy reference (1e-13 of sum |x_i y_i|).
@@ -31,6 +33,7 @@ def _dot(torch, name, x, y, n, offset=0):
     return float(res.cpu().numpy()[0])
 
 
+@pytest.mark.gpu
 @pytest.mark.parametrize("n, offset", [(0, 0), (1, 0), (4097, 1), ((1 << 20) + 3, 0),
                                        (16777216, 0)])
 def test_no_alloc_matches_dot_twice(cuda, n, offset):
@@ -43,11 +46,13 @@ def test_no_alloc_matches_dot_twice(cuda, n, offset):
         y = torch.from_numpy(ys).cuda()
         ref = _dot(torch, "elsa_dot", x, y, n, offset)
         got = _dot(torch, "elsa_dot_no_alloc", x, y, n, offset)
-        scale = max(1.0, float(np.dot(np.abs(xs[offset:].astype(np.float64)),
-                                      np.abs(ys[offset:].astype(np.float64)))))
+        x64, y64 = xs[offset:].astype(np.float64), ys[offset:].astype(np.float64)
+        scale = max(1.0, float(np.dot(np.abs(x64), np.abs(y64))))
         assert abs(got - ref) <= REL * scale, (call, got, ref)
+        assert abs(got - float(np.dot(x64, y64))) <= REL * scale, (call, got)
 
 
+@pytest.mark.gpu
 def test_no_alloc_refuses_oversize(cuda):
     import elsa_b200
     from elsa_b200 import _capi
@@ -60,3 +65,22 @@ def test_no_alloc_refuses_oversize(cuda):
         _capi.call("elsa_dot_no_alloc", ctypes.c_void_p(x.data_ptr()),
                    ctypes.c_void_p(x.data_ptr()), too_big, ctypes.c_void_p(res.data_ptr()),
                    ctypes.c_void_p(0))
+
+
+def test_no_alloc_unit_references_no_allocator():
+    """The translation unit of elsa_dot_no_alloc names no allocating CUDA runtime routine, so no
+    code path of the entry point can allocate (its C ABI wrapper only forwards to it)."""
+    from elsa_b200 import build
+    build.build()
+    nm = shutil.which("nm")
+    if nm is None:
+        pytest.skip("nm is not installed")
+    obj = os.path.join(build.BUILD, "noalloc.cu.o")
+    out = subprocess.run([nm, "-u", "-C", obj], capture_output=True, text=True, check=True).stdout
+    undefined = [line.split()[-1] for line in out.splitlines() if line.strip()]
+    allocators = ("cudaMalloc", "cudaFree", "cudaMallocAsync", "cudaFreeAsync", "cudaMallocManaged",
+                  "cudaMallocHost", "cudaHostAlloc", "cuMemAlloc", "cuMemCreate")
+    bad = [u for u in undefined if any(u == a or u.startswith(a + "_") or u.startswith(a + "(")
+                                       for a in allocators)]
+    assert not bad, bad
+    assert any("cudaGetSymbolAddress" in u for u in undefined)
