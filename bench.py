@@ -119,6 +119,7 @@ def cpu_baseline_sample(views_in_sample, vol, poses, det, x):
     the views: forward + adjoint. Returns (GUPS, seconds, threads)."""
     from oracle import oracle as O
     O.build()
+    O.set_adjoint_atomic(True)  # time the reference's own scheme (omp atomic adds)
     idx = np.linspace(0, poses.shape[0] - 1, views_in_sample).round().astype(int)
     p = np.ascontiguousarray(poses[idx])
     d = np.array([det[0], det[1], len(idx)])
@@ -126,6 +127,7 @@ def cpu_baseline_sample(views_in_sample, vol, poses, det, x):
     y = O.joseph(x, vol, d, p)
     O.joseph_adjoint(y, vol, d, p)
     dt = time.perf_counter() - t0
+    O.set_adjoint_atomic(False)
     return 2.0 * np.prod(vol) * len(idx) / dt / 1e9, dt, O.num_threads()
 
 

@@ -63,6 +63,16 @@ namespace elsa_b200
         constexpr int kSplatUnroll = ELSA_SPLAT_UNROLL;
         constexpr int kMinClass = 2;
         constexpr int kMaxClass = 8;
+        // Joseph brick windows: the brick grown by half a voxel (the reach of a bilinear tap)
+        // plus slack for the accumulated-position drift (at most n steps of half an ulp of a
+        // coordinate below n: n^2 2^-24 voxel, 0.004 at n = 256), doubled, and 0.05 voxel for the
+        // rounding of the float rays; 0.05 pixel of margin for the projection of the corners.
+        inline float windowGrow(const VolumeShape& vol)
+        {
+            const float n = static_cast<float>(std::max(vol.n[0], std::max(vol.n[1], vol.n[2])));
+            return 0.55f + 2.0f * n * n * 5.9604645e-8f;
+        }
+        constexpr float kWindowPixelMargin = 0.05f;
 
         struct Weights {
             int ia, ib;
@@ -316,9 +326,17 @@ namespace elsa_b200
             return lo;
         }
 
+        // grow > 0 (tight mode, flat detectors): the window holds exactly the pixels whose
+        // centres lie in the projection of the brick grown by `grow` voxels on every side, plus
+        // `pixMargin` pixels (the float rays deviate from the exact pixel-centre rays by far less
+        // than both). A Joseph sample on driving plane k touches the brick only if its position
+        // lies within half a voxel of the brick in both non-driving axes (taps floor(p - 0.5)
+        // and floor(p - 0.5) + 1), so grow = 0.5 plus the accumulated-position slack suffices.
+        // grow = 0: the conservative window (brick grown by one voxel, one pixel of margin).
         __global__ void josephWindowKernel(const float* __restrict__ poses, VolumeShape vol,
                                            DetectorShape det, int3 brick, int3 nBricks,
-                                           CurvedMap cm, RayWindow* __restrict__ out)
+                                           CurvedMap cm, float grow, float pixMargin,
+                                           RayWindow* __restrict__ out)
         {
             const int nb = nBricks.x * nBricks.y * nBricks.z;
             const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -329,12 +347,14 @@ namespace elsa_b200
             const float* P = poses + static_cast<int64_t>(p) * 40;
             const int bxi = bi % nBricks.x, byi = (bi / nBricks.x) % nBricks.y,
                       bzi = bi / (nBricks.x * nBricks.y);
-            const float lo0 = static_cast<float>(bxi * brick.x - 1);
-            const float lo1 = static_cast<float>(byi * brick.y - 1);
-            const float lo2 = static_cast<float>(bzi * brick.z - 1);
-            const float hi0 = static_cast<float>(bxi * brick.x + brick.x + 1);
-            const float hi1 = static_cast<float>(byi * brick.y + brick.y + 1);
-            const float hi2 = static_cast<float>(bzi * brick.z + brick.z + 1);
+            const bool tight = grow > 0.0f && !cm.planarU;
+            const float g = tight ? grow : 1.0f;
+            const float lo0 = static_cast<float>(bxi * brick.x) - g;
+            const float lo1 = static_cast<float>(byi * brick.y) - g;
+            const float lo2 = static_cast<float>(bzi * brick.z) - g;
+            const float hi0 = static_cast<float>(bxi * brick.x + brick.x) + g;
+            const float hi1 = static_cast<float>(byi * brick.y + brick.y) + g;
+            const float hi2 = static_cast<float>(bzi * brick.z + brick.z) + g;
             float umin = 1e30f, umax = -1e30f, vmin = 1e30f, vmax = -1e30f;
             bool behind = false;
             const int corners = vol.dim == 3 ? 8 : 4;
@@ -387,6 +407,21 @@ namespace elsa_b200
                 } else {
                     w.v0 = 0, w.v1 = 0;
                 }
+            } else if (tight) {
+                // pixels whose centres i + 0.5 lie in [umin - margin, umax + margin]
+                const float uLo = fmaxf(ceilf(umin - 0.5f - pixMargin), -1.0f);
+                const float uHi = fminf(floorf(umax - 0.5f + pixMargin), static_cast<float>(det.nu));
+                w.u0 = max(0, static_cast<int>(uLo));
+                w.u1 = min(det.nu - 1, static_cast<int>(uHi));
+                if (vol.dim == 3) {
+                    const float vLo = fmaxf(ceilf(vmin - 0.5f - pixMargin), -1.0f);
+                    const float vHi =
+                        fminf(floorf(vmax - 0.5f + pixMargin), static_cast<float>(det.nv));
+                    w.v0 = max(0, static_cast<int>(vLo));
+                    w.v1 = min(det.nv - 1, static_cast<int>(vHi));
+                } else {
+                    w.v0 = 0, w.v1 = 0;
+                }
             } else {
                 // pixel i has its centre at i + 0.5
                 const float uLo = fmaxf(floorf(umin - 0.5f) - 1.0f, -1.0f);
@@ -404,6 +439,67 @@ namespace elsa_b200
                 }
             }
             out[t] = w;
+        }
+
+        // Check of the brick windows (test support, elsa_projector_info key 8): every tap of
+        // every sample must lie in a brick whose window for the ray's view contains the ray.
+        // Counts the taps that violate this.
+        __global__ void josephWindowCheckKernel(const JosephRay* __restrict__ rays,
+                                                const RayWindow* __restrict__ windows,
+                                                VolumeShape vol, DetectorShape det, int3 brick,
+                                                int3 nBricks,
+                                                unsigned long long* __restrict__ misses)
+        {
+            const int64_t nrays = static_cast<int64_t>(det.nu) * det.nv * det.np;
+            const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (r >= nrays)
+                return;
+            const JosephRay R = rays[r];
+            if (R.n == 0)
+                return;
+            const int u = static_cast<int>(r % det.nu);
+            const int v = static_cast<int>((r / det.nu) % det.nv);
+            const int p = static_cast<int>(r / (static_cast<int64_t>(det.nu) * det.nv));
+            const int nb = nBricks.x * nBricks.y * nBricks.z;
+            const int g = R.meta & 3;
+            const int dir = (R.meta & 4) ? -1 : 1;
+            int a, b;
+            nonDrivingAxes(g, a, b);
+            const int bext[3] = {brick.x, brick.y, brick.z};
+            float pa = R.pa, pb = R.pb;
+            int k = R.k0;
+            unsigned long long bad = 0;
+            int lastBrick = -1;
+            for (int j = 0; j < R.n; ++j, k += dir, pa = __fadd_rn(pa, R.sa),
+                     pb = __fadd_rn(pb, R.sb)) {
+                const int ia = static_cast<int>(floorf(__fsub_rn(pa, 0.5f)));
+                const int ib = static_cast<int>(floorf(__fsub_rn(pb, 0.5f)));
+                for (int t = 0; t < (vol.dim == 3 ? 4 : 2); ++t) {
+                    int c[3];
+                    c[g] = k;
+                    c[a] = ia + (t & 1);
+                    if (vol.dim == 3)
+                        c[b] = ib + (t >> 1);
+                    else
+                        c[2] = 0;
+                    bool in = true;
+                    for (int i = 0; i < vol.dim; ++i)
+                        in = in && c[i] >= 0 && c[i] < vol.n[i];
+                    if (!in)
+                        continue;
+                    const int bi = c[0] / bext[0] + nBricks.x *
+                                   (c[1] / bext[1] + nBricks.y * (vol.dim == 3 ? c[2] / bext[2] : 0));
+                    if (bi == lastBrick)
+                        continue;
+                    const RayWindow w = windows[static_cast<int64_t>(p) * nb + bi];
+                    if (u < w.u0 || u > w.u1 || v < w.v0 || v > w.v1)
+                        ++bad;
+                    else
+                        lastBrick = bi;
+                }
+            }
+            if (bad)
+                atomicAdd(misses, bad);
         }
 
         // Approximate non-driving position of ray R on driving plane k (pos0 + j*step). It
@@ -1226,7 +1322,8 @@ namespace elsa_b200
                     static_cast<int64_t>(nBricks_.x) * nBricks_.y * nBricks_.z * det_.np;
                 ELSA_CUDA(cudaMalloc(&dWindows_, sizeof(RayWindow) * nwin));
                 josephWindowKernel<<<static_cast<unsigned>((nwin + 255) / 256), 256>>>(
-                    dPoses_, vol_, det_, brick_, nBricks_, curved_.map(), dWindows_);
+                    dPoses_, vol_, det_, brick_, nBricks_, curved_.map(), windowGrow(vol_),
+                    kWindowPixelMargin, dWindows_);
                 ELSA_LAUNCH_CHECK("josephWindowKernel");
                 setKnob(kKnobAdjointChunks, defaultChunks());
                 if (vol_.dim == 3) {
@@ -1581,12 +1678,31 @@ namespace elsa_b200
                     return tma_ ? tma_->launchesPerForward() : 1;
                 case 7: // kernel launches per adjoint call (with view chunks: + the chunk sum)
                     return (!fast_ && !scatter_ && adjointChunks_ > 1) ? 2 : 1;
+                case 8: // taps outside the windows of their bricks (test support; synchronizes)
+                    return windowMisses();
                 default:
                     return -1;
                 }
             }
 
         private:
+            int64_t windowMisses() const
+            {
+                if (!dWindows_)
+                    return -1;
+                DeviceBuffer count(sizeof(unsigned long long));
+                ELSA_CUDA(cudaMemset(count.as<unsigned long long>(), 0, sizeof(unsigned long long)));
+                const int64_t nrays = rangeSize_;
+                josephWindowCheckKernel<<<static_cast<unsigned>((nrays + 255) / 256), 256>>>(
+                    dRays_, dWindows_, vol_, det_, brick_, nBricks_,
+                    count.as<unsigned long long>());
+                ELSA_LAUNCH_CHECK("josephWindowCheckKernel");
+                unsigned long long h = 0;
+                ELSA_CUDA(cudaMemcpy(&h, count.as<unsigned long long>(), sizeof(h),
+                                     cudaMemcpyDeviceToHost));
+                return static_cast<int64_t>(h);
+            }
+
             bool fast_ = false; // elsa's unmatched fast adjoint
             cudaArray_t fastArray_ = nullptr;
             cudaTextureObject_t fastTex_ = 0;
@@ -1631,7 +1747,7 @@ namespace elsa_b200
         if (nwin == 0)
             return;
         josephWindowKernel<<<static_cast<unsigned>((nwin + 255) / 256), 256, 0, s>>>(
-            poses, vol, det, brick, nBricks, cm, out);
+            poses, vol, det, brick, nBricks, cm, 0.0f, 0.0f, out);
         ELSA_LAUNCH_CHECK("josephWindowKernel");
     }
 

@@ -649,9 +649,25 @@ namespace orc
     // partial volume of its own, and the partial volumes are added in range order. The result is
     // the same for every thread count and every run.
     // ------------------------------------------------------------------------------------------
+    // When set (oracle_set_adjoint_atomic), the adjoints add with `omp atomic` straight into the
+    // output as the reference does: the reference's speed, not its order. Only the CPU-baseline
+    // timing uses it; parity checks use the fixed order.
+    static bool gAtomicAdjoint = false;
+
     template <typename data_t, class RayFn>
     static void orderedScatter(index_t nrays, index_t nvol, data_t* out, RayFn rayFn)
     {
+        if (gAtomicAdjoint) {
+            std::fill(out, out + nvol, data_t(0));
+            auto add = [out](index_t idx, data_t v) {
+#pragma omp atomic
+                out[idx] += v;
+            };
+#pragma omp parallel for schedule(dynamic, 256)
+            for (index_t ir = 0; ir < nrays; ++ir)
+                rayFn(ir, add);
+            return;
+        }
         const index_t bytes = std::max<index_t>(1, nvol * static_cast<index_t>(sizeof(data_t)));
         index_t chunks = std::min<index_t>(32, std::max<index_t>(1, (index_t(1) << 31) / bytes));
         chunks = std::min<index_t>(chunks, std::max<index_t>(1, nrays));
@@ -660,9 +676,10 @@ namespace orc
 #pragma omp parallel for schedule(dynamic, 1)
         for (index_t c = 0; c < chunks; ++c) {
             data_t* dst = c == 0 ? out : partial.data() + (c - 1) * nvol;
+            auto add = [dst](index_t idx, data_t v) { dst[idx] += v; };
             const index_t lo = nrays * c / chunks, hi = nrays * (c + 1) / chunks;
             for (index_t ir = lo; ir < hi; ++ir)
-                rayFn(ir, dst);
+                rayFn(ir, add);
         }
         if (chunks > 1) {
 #pragma omp parallel for schedule(static)
@@ -692,8 +709,8 @@ namespace orc
             nvol *= volDims[i];
         }
         const index_t nrays = (dim == 2 ? detDims[0] : detDims[0] * detDims[1]) * numPoses;
-        // one ray; the adjoint adds into dst (a partial volume of orderedScatter)
-        auto ray = [&](index_t ir, data_t* dst) {
+        // one ray; the adjoint adds through add(index, value) (orderedScatter)
+        auto ray = [&](index_t ir, auto& add) {
             const Ray r = rayForIndex(poses.data(), dim, detDims, ir, coords);
             DDTraversal tr = ddSetup(boxMax, dim, r);
             const data_t L = static_cast<data_t>(tr.length);
@@ -707,7 +724,7 @@ namespace orc
                 if (adjoint) {
                     const data_t y = in[ir];
                     josephTaps(pos, tr.driving, dim, volDims, [&](index_t idx, float wt) {
-                        dst[idx] += y * L * static_cast<data_t>(wt);
+                        add(idx, y * L * static_cast<data_t>(wt));
                     });
                 } else {
                     josephTaps(pos, tr.driving, dim, volDims, [&](index_t idx, float wt) {
@@ -725,9 +742,10 @@ namespace orc
             orderedScatter<data_t>(nrays, nvol, out, ray);
             return;
         }
+        auto none = [](index_t, data_t) {};
 #pragma omp parallel for schedule(dynamic, 256)
         for (index_t ir = 0; ir < nrays; ++ir)
-            ray(ir, nullptr);
+            ray(ir, none);
     }
 
     // ------------------------------------------------------------------------------------------
@@ -754,8 +772,8 @@ namespace orc
         const index_t nrays = (dim == 2 ? detDims[0] : detDims[0] * detDims[1]) * numPoses;
         const float EPS = std::numeric_limits<float>::epsilon();
         const float MAXF = std::numeric_limits<float>::max();
-        // one ray; the adjoint adds into dst (a partial volume of orderedScatter)
-        auto ray = [&](index_t ir, data_t* dst) {
+        // one ray; the adjoint adds through add(index, value) (orderedScatter)
+        auto ray = [&](index_t ir, auto& add) {
             const Ray r = rayForIndex(poses.data(), dim, detDims, ir, coords);
             data_t acc = 0;
             float tmin, tmax;
@@ -821,12 +839,12 @@ namespace orc
                             ++visits[ir];
                         if (binary) {
                             if (adjoint) {
-                                dst[idx] += in[ir];
+                                add(idx, in[ir]);
                             } else {
                                 acc += in[idx];
                             }
                         } else if (adjoint) {
-                            dst[idx] += in[ir] * static_cast<data_t>(weight);
+                            add(idx, in[ir] * static_cast<data_t>(weight));
                         } else {
                             acc += in[idx] * static_cast<data_t>(weight);
                         }
@@ -843,9 +861,10 @@ namespace orc
             orderedScatter<data_t>(nrays, nvol, out, ray);
             return;
         }
+        auto none = [](index_t, data_t) {};
 #pragma omp parallel for schedule(dynamic, 256)
         for (index_t ir = 0; ir < nrays; ++ir)
-            ray(ir, nullptr);
+            ray(ir, none);
     }
 
     // ------------------------------------------------------------------------------------------
@@ -1079,8 +1098,8 @@ namespace orc
         for (int i = 0; i < dim; ++i)
             nvol *= volDims[i];
         const index_t nrays = (dim == 2 ? detDims[0] : detDims[0] * detDims[1]) * numPoses;
-        // one ray; the adjoint adds into dst (a partial volume of orderedScatter)
-        auto ray = [&](index_t ir, data_t* dst) {
+        // one ray; the adjoint adds through add(index, value) (orderedScatter)
+        auto ray = [&](index_t ir, auto& add) {
             const Ray r = rayForIndex(poses.data(), dim, detDims, ir);
             if (adjoint) {
                 const data_t y = in[ir];
@@ -1088,7 +1107,7 @@ namespace orc
                        [&](index_t idx, float wt) {
                            if (idx < 0 || idx >= nvol)
                                return;
-                           dst[idx] += static_cast<data_t>(wt) * y;
+                           add(idx, static_cast<data_t>(wt) * y);
                        });
             } else {
                 data_t acc = 0;
@@ -1105,9 +1124,10 @@ namespace orc
             orderedScatter<data_t>(nrays, nvol, out, ray);
             return;
         }
+        auto none = [](index_t, data_t) {};
 #pragma omp parallel for schedule(dynamic, 64)
         for (index_t ir = 0; ir < nrays; ++ir)
-            ray(ir, nullptr);
+            ray(ir, none);
     }
 
     // ------------------------------------------------------------------------------------------
@@ -1146,6 +1166,11 @@ extern "C" {
 int oracle_num_threads(void)
 {
     return omp_get_max_threads();
+}
+
+void oracle_set_adjoint_atomic(int on)
+{
+    orc::gAtomicAdjoint = on != 0;
 }
 
 void oracle_set_num_threads(int n)

@@ -48,6 +48,7 @@ def lib():
         c_int, c_i64, c_f = ctypes.c_int, ctypes.c_int64, ctypes.c_float
         L.oracle_num_threads.restype = c_int
         L.oracle_set_num_threads.argtypes = [c_int]
+        L.oracle_set_adjoint_atomic.argtypes = [c_int]
         L.oracle_geometry2d.argtypes = [c_f, c_f, c_f, _f32p, _f32p, _f32p, _f32p, c_f, _f32p,
                                         _f32p]
         L.oracle_geometry3d.argtypes = [c_f, c_f, _f32p, _f32p, _f32p, _f32p, c_f, c_f, c_f,
@@ -102,6 +103,12 @@ def _f32(a):
 
 def set_num_threads(n):
     lib().oracle_set_num_threads(int(n))
+
+
+def set_adjoint_atomic(on):
+    """True: the adjoints add with `omp atomic` as the reference does (its speed, a run-dependent
+    order; for CPU-baseline timing only). False (the default): the fixed, deterministic order."""
+    lib().oracle_set_adjoint_atomic(1 if on else 0)
 
 
 def num_threads():

@@ -71,6 +71,7 @@ def test_joseph_parity(cuda, oracle, name):
     print("%s: fwd %.3g adj %.3g (vs f64 fwd %.3g), fallback tiles %d ppm"
           % (name, e_fwd, e_adj, rel_l2(Ax, d_Ax), proj.info(4)))
     assert proj.info(3) == 0  # no timed-out pipeline wait
+    assert proj.info(8) == 0  # every tap lies in a brick whose ray window holds its ray
     assert e_fwd <= PARITY
     assert e_adj <= PARITY
 

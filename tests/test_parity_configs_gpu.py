@@ -65,6 +65,7 @@ def test_cone256_joseph_all_views(cuda, oracle, cone256):
     Ax = _apply(cuda, proj, x)
     Aty = _apply(cuda, proj, y, adjoint=True)
     assert proj.info(3) == 0  # no timed-out pipeline wait
+    misses = proj.info(8)  # taps outside the ray windows of their bricks (must be none)
     del proj
     f32, a32 = oracle.joseph(x, vol, det, poses), oracle.joseph_adjoint(y, vol, det, poses)
     e_f, e_a = rel_l2(Ax, f32), rel_l2(Aty, a32)
@@ -72,9 +73,10 @@ def test_cone256_joseph_all_views(cuda, oracle, cone256):
     a64 = oracle.joseph_adjoint(y.astype(np.float64), vol, det, poses, dtype=np.float64)
     fields = dict(fwd_gpu_f32=e_f, fwd_gpu_f64=rel_l2(Ax, f64), fwd_f32_f64=rel_l2(f32, f64),
                   adj_gpu_f32=e_a, adj_gpu_f64=rel_l2(Aty, a64), adj_f32_f64=rel_l2(a32, a64),
-                  bound=PARITY)
+                  bound=PARITY, window_misses=misses)
     record_parity("cone256_joseph_360_views", **fields)
     print(fields)
+    assert misses == 0
     assert e_f <= PARITY
     assert e_a <= PARITY
 
@@ -191,9 +193,11 @@ FAN128 = dict(vol=(128, 128), views=180, s2c=1000, c2d=250, det=[182])
 
 # Fixed bounds per solver on the relative L2 distance between the device iterate and the FP32
 # oracle's after 20 iterations; both sides are deterministic, so the distance is one number,
-# recorded with the FP32-FP64 distance in the parity record. CG-type recurrences amplify the
-# last-bit differences of the projectors (device and oracle sum in different orders).
-SOLVER_BOUNDS = {"cgne": 1e-4, "cgls": 1e-4, "fgm": 1e-4, "ogm": 1e-4, "sqs": 1e-4}
+# recorded with the FP32-FP64 distance in the parity record. FGM, OGM and SQS meet 1e-5. CGNE
+# and CGLS amplify the last-bit differences of the projectors (device and oracle sum in different
+# orders): measured on a B200, CGNE 6.1e-5 and CGLS 3.6e-5 from the FP32 oracle, while the FP32
+# oracle itself lies 1.2e-2 from the FP64 oracle; their bounds are about three times that.
+SOLVER_BOUNDS = {"cgne": 2e-4, "cgls": 1e-4, "fgm": 1e-5, "ogm": 1e-5, "sqs": 1e-5}
 
 
 @pytest.fixture(scope="module")
