@@ -8,9 +8,10 @@ One step is one CGNE iteration (solvers/CGNE.cpp:50-73 of elsa): a forward proje
 adjoint and the fused float64 vector updates, enqueued through the C ABI (elsa_solver_iterate).
 `value` counts the voxel-view updates of the forward + adjoint pass per second (GUPS = 2 * N_vox *
 N_views per step). `e2e` is the same metric through the host-buffer entry points (the reference's
-call pattern: volume in, sinogram out, sinogram in, volume out, every apply). Under torchrun every
-rank runs its own replica of the problem (the cone-beam problem has no exchange step at this size)
-and `value` is the sum over ranks, timed as the max over ranks.
+call pattern: volume in, sinogram out, sinogram in, volume out, every apply). Under torchrun the
+one 256^3 problem is split by views over the ranks (strong scaling): every CGNE iteration applies
+each rank's block of views and all-reduces one volume over NCCL; `value` is the whole problem's
+rate, timed as the max over ranks.
 
 `--impl reference` times the CPU restatement of elsa's own algorithm (oracle/, the reference
 C++ library cannot be built here: Eigen 3.4 is absent) on the host cores, on a bounded subset of
@@ -199,18 +200,123 @@ def _apply_size(args):
                                  % (n, 3 * n // 2, 3 * n // 2))
 
 
+def run_sharded(args):
+    """N > 1: one 256^3 problem, its views split into N contiguous blocks, one per rank; every
+    CGNE iteration applies each rank's block (native kernels) and all-reduces the volume
+    A^T A c over NCCL on the solver stream (strong scaling: the total work is fixed)."""
+    import ctypes
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    import elsa_b200
+    from elsa_b200 import _capi, phantoms
+    from elsa_b200.sharded import ShardedCGNE, native_split, view_block
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if "MASTER_ADDR" not in os.environ:  # --sharded without torchrun: a group of one rank
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(sk.getsockname()[1]),
+                              RANK="0", WORLD_SIZE="1")
+    os.environ.setdefault("NCCL_DEBUG", "INFO")  # NCCL's init log (transport, NVLS) on stderr
+    os.environ.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", local))
+    _apply_size(args)
+    vol = tuple(WORKLOAD["volume"])
+    poses, det = elsa_b200.circle_trajectory(vol, WORKLOAD["views"], 360,
+                                             WORKLOAD["source_to_center"],
+                                             WORKLOAD["center_to_detector"], WORKLOAD["detector"])
+    split, proj, (lo, hi) = native_split(elsa_b200.PROJECTOR_JOSEPH, vol, poses, det, rank,
+                                         world)
+    x_true = phantoms.modified_shepp_logan(vol)
+    stream = torch.cuda.current_stream().cuda_stream
+    xt = torch.from_numpy(x_true.ravel()).cuda()
+    b = torch.empty(proj.range_size, dtype=torch.float32, device="cuda")
+    proj.apply_ptr(xt.data_ptr(), b.data_ptr(), stream)
+    solver = ShardedCGNE(split, b)
+    solver.begin()
+    solver.iterate(args.warmup)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    hist = solver.iterate(args.steps)
+    end.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    ms = start.elapsed_time(end)
+    clock_info = clocks.stop()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    updates = 2.0 * np.prod(vol) * WORKLOAD["views"]  # the whole problem's fwd + adj per step
+    value = updates * args.steps / (ms / 1e3) / 1e9
+
+    # end to end: every rank's host-buffer forward + adjoint of its block (pinned buffers)
+    xh = torch.from_numpy(x_true.ravel()).pin_memory().numpy()
+    yh = torch.empty(proj.range_size, dtype=torch.float32).pin_memory().numpy()
+    bh = torch.empty(proj.domain_size, dtype=torch.float32).pin_memory().numpy()
+
+    def e2e_step():
+        _capi.call("elsa_projector_apply_host", proj.handle, _capi.np_ptr(xh), _capi.np_ptr(yh))
+        _capi.call("elsa_projector_apply_adjoint_host", proj.handle, _capi.np_ptr(yh),
+                   _capi.np_ptr(bh))
+
+    e2e_steps = max(2, min(args.steps, 5))
+    e2e_step()
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = updates * e2e_steps / float(t.item()) / 1e9
+    res = [float(v) for v in hist.cpu()]
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (modified Shepp-Logan 3D phantom, b = A x)",
+        "config": dict(WORKLOAD, parallelism="views sharded over %d ranks, NCCL all-reduce of "
+                                             "A^T A c per CGNE iteration" % world,
+                       views_per_rank=[hi_ - lo_ for lo_, hi_ in
+                                       (view_block(WORKLOAD["views"], r, world)
+                                        for r in range(world))],
+                       l2="working set > L2"),
+        "cg_iters_per_s": round(1e3 * args.steps / ms, 3),
+        "cg_residual_sq": [res[0], res[-1]] if res else [],
+        "e2e": {"value": round(e2e_value, 3), "unit": "GUPS",
+                "h2d_bytes_per_step": 4 * (proj.domain_size + proj.range_size),
+                "d2h_bytes_per_step": 4 * (proj.range_size + proj.domain_size),
+                "timing": "host wall clock, max over ranks, every rank its block"},
+        "gpu_launches": (proj.info(6) + proj.info(7) + VECTOR_LAUNCHES_PER_STEP) * args.steps,
+        "clocks": clock_info,
+    }
+    split.close()
+    dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
 def run_elsa(args):
     import torch
     import elsa_b200
     from elsa_b200 import phantoms
 
     world, rank, local = _dist()
+    if world > 1 or args.sharded:
+        run_sharded(args)
+        return
     torch.cuda.set_device(local)
     dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     _apply_size(args)
     vol = tuple(WORKLOAD["volume"])
@@ -538,6 +644,8 @@ def main():
                          "this arm, about 10 s on 16 host threads; for --impl reference as many "
                          "as keep the whole run near 90 s, 4 to 60)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sharded", action="store_true",
+                    help="run the view-sharded solver (the N > 1 path) also on one GPU")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the parity block (oracle check of the benchmarked operator)")
     ap.add_argument("--no-batched", action="store_true",

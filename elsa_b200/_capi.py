@@ -84,6 +84,15 @@ SIGNATURES = {
     "elsa_projector_sizes": (_st, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "elsa_projector_info": (_st, [_vp, _i32, ctypes.POINTER(_i64)]),
     "elsa_projector_wait_test": (_st, [_vp, _i64, _i32]),
+    "elsa_projector_apply_batch": (_st, [_vp, _vp, _i64, _vp, _i64, _i32, _vp]),
+    "elsa_cgne_split_create": (_st, [_vp, _vp, ctypes.POINTER(_vp)]),
+    "elsa_cgne_split_backproject": (_st, [_vp, _vp, _vp, _vp]),
+    "elsa_cgne_split_begin": (_st, [_vp, _vp, _vp]),
+    "elsa_cgne_split_normal": (_st, [_vp, _vp, _vp]),
+    "elsa_cgne_split_update": (_st, [_vp, _vp, _vp]),
+    "elsa_cgne_split_residual": (_st, [_vp, _vp, _vp]),
+    "elsa_cgne_split_destroy": (_st, [_vp]),
+    "elsa_projector_apply_adjoint_batch": (_st, [_vp, _vp, _i64, _vp, _i64, _i32, _vp]),
     "elsa_projector_get_knob": (_st, [_vp, _i32, ctypes.POINTER(_i32)]),
     "elsa_projector_knob_candidates": (_st, [_vp, _i32, _vp, _i32, ctypes.POINTER(_i32)]),
     "elsa_projector_set_knob": (_st, [_vp, _i32, _i32]),
@@ -296,6 +305,17 @@ class Projector:
     def apply_adjoint_ptr(self, y_ptr, x_ptr, stream=None):
         call("elsa_projector_apply_adjoint", self._h, ctypes.c_void_p(y_ptr),
              ctypes.c_void_p(x_ptr), ctypes.c_void_p(stream or 0))
+
+    def apply_batch_ptr(self, x_ptr, x_stride, y_ptr, y_stride, batch, stream=None):
+        """y + b y_stride = A (x + b x_stride) for b < batch (strides in floats)."""
+        call("elsa_projector_apply_batch", self._h, ctypes.c_void_p(x_ptr), int(x_stride),
+             ctypes.c_void_p(y_ptr), int(y_stride), int(batch), ctypes.c_void_p(stream or 0))
+
+    def apply_adjoint_batch_ptr(self, y_ptr, y_stride, x_ptr, x_stride, batch, stream=None):
+        """x + b x_stride = A^T (y + b y_stride) for b < batch (strides in floats)."""
+        call("elsa_projector_apply_adjoint_batch", self._h, ctypes.c_void_p(y_ptr),
+             int(y_stride), ctypes.c_void_p(x_ptr), int(x_stride), int(batch),
+             ctypes.c_void_p(stream or 0))
 
     def apply_host(self, x):
         x = np.ascontiguousarray(x, np.float32).reshape(-1)

@@ -22,6 +22,11 @@ struct elsa_solver {
     int device = 0;
 };
 
+struct elsa_cgne_split {
+    std::unique_ptr<elsa_b200::SplitCgne> impl;
+    int device = 0;
+};
+
 struct elsa_projector {
     std::unique_ptr<elsa_b200::Projector> impl;
     // lazily allocated staging buffers of the host-buffer entry points
@@ -520,6 +525,33 @@ elsa_status elsa_projector_apply_adjoint(elsa_projector* p, const float* y, floa
     });
 }
 
+elsa_status elsa_projector_apply_batch(elsa_projector* p, const float* x, int64_t xStride,
+                                       float* y, int64_t yStride, int32_t batch, void* stream)
+{
+    return guarded([&] {
+        require(p && batch >= 0 && (batch == 0 || (x && y)),
+                "elsa_projector_apply_batch: invalid argument");
+        require(batch <= 1 || (xStride >= p->impl->domainSize() && yStride >= p->impl->rangeSize()),
+                "elsa_projector_apply_batch: strides must not make the elements overlap");
+        onDevice(p);
+        p->impl->forwardBatch(x, xStride, y, yStride, batch, asStream(stream));
+    });
+}
+
+elsa_status elsa_projector_apply_adjoint_batch(elsa_projector* p, const float* y, int64_t yStride,
+                                               float* x, int64_t xStride, int32_t batch,
+                                               void* stream)
+{
+    return guarded([&] {
+        require(p && batch >= 0 && (batch == 0 || (x && y)),
+                "elsa_projector_apply_adjoint_batch: invalid argument");
+        require(batch <= 1 || (xStride >= p->impl->domainSize() && yStride >= p->impl->rangeSize()),
+                "elsa_projector_apply_adjoint_batch: strides must not make the elements overlap");
+        onDevice(p);
+        p->impl->adjointBatch(y, yStride, x, xStride, batch, asStream(stream));
+    });
+}
+
 static void hostApply(elsa_projector* p, const float* in, float* out, bool adjoint)
 {
     onDevice(p);
@@ -677,6 +709,88 @@ elsa_status elsa_cgne_solve(elsa_projector* p, const float* b, float* x, int32_t
         elsa_b200::SolverWorkspace ws(p->impl->domainSize(), p->impl->rangeSize());
         elsa_b200::cgneSolve(*p->impl, b, x, iterations, useX0 != 0, ws, asStream(stream));
         ELSA_CUDA(cudaStreamSynchronize(asStream(stream)));
+    });
+}
+
+elsa_status elsa_cgne_split_create(elsa_projector* p, float* x, elsa_cgne_split** out)
+{
+    return guarded([&] {
+        require(out != nullptr, "elsa_cgne_split_create: null output handle");
+        *out = nullptr;
+        require(p && x, "elsa_cgne_split_create: null argument");
+        onDevice(p);
+        auto h = std::make_unique<elsa_cgne_split>();
+        h->device = p->impl->device();
+        h->impl = std::make_unique<elsa_b200::SplitCgne>(*p->impl, x);
+        *out = h.release();
+    });
+}
+
+namespace
+{
+    void onSplitDevice(const elsa_cgne_split* c)
+    {
+        int cur = 0;
+        ELSA_CUDA(cudaGetDevice(&cur));
+        if (cur != c->device)
+            ELSA_CUDA(cudaSetDevice(c->device));
+    }
+} // namespace
+
+elsa_status elsa_cgne_split_backproject(elsa_cgne_split* c, const float* b, float* atb,
+                                        void* stream)
+{
+    return guarded([&] {
+        require(c && b && atb, "elsa_cgne_split_backproject: null argument");
+        onSplitDevice(c);
+        c->impl->backprojectData(b, atb, asStream(stream));
+    });
+}
+
+elsa_status elsa_cgne_split_begin(elsa_cgne_split* c, const float* atb, void* stream)
+{
+    return guarded([&] {
+        require(c && atb, "elsa_cgne_split_begin: null argument");
+        onSplitDevice(c);
+        c->impl->begin(atb, asStream(stream));
+    });
+}
+
+elsa_status elsa_cgne_split_normal(elsa_cgne_split* c, float* q, void* stream)
+{
+    return guarded([&] {
+        require(c && q, "elsa_cgne_split_normal: null argument");
+        onSplitDevice(c);
+        c->impl->applyNormal(q, asStream(stream));
+    });
+}
+
+elsa_status elsa_cgne_split_update(elsa_cgne_split* c, const float* q, void* stream)
+{
+    return guarded([&] {
+        require(c && q, "elsa_cgne_split_update: null argument");
+        onSplitDevice(c);
+        c->impl->update(q, asStream(stream));
+    });
+}
+
+elsa_status elsa_cgne_split_residual(const elsa_cgne_split* c, double* result, void* stream)
+{
+    return guarded([&] {
+        require(c && result, "elsa_cgne_split_residual: null argument");
+        ELSA_CUDA(cudaMemcpyAsync(result, c->impl->squaredResidualDevice(), sizeof(double),
+                                  cudaMemcpyDeviceToDevice, asStream(stream)));
+    });
+}
+
+elsa_status elsa_cgne_split_destroy(elsa_cgne_split* c)
+{
+    return guarded([&] {
+        if (c) {
+            onSplitDevice(c);
+            ELSA_CUDA(cudaDeviceSynchronize()); // no update in flight uses the workspace
+        }
+        delete c;
     });
 }
 

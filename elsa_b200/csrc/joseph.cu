@@ -50,6 +50,15 @@
 #ifndef ELSA_ADJ_BATCH
 #define ELSA_ADJ_BATCH 2 // class rays per lane fetched together (3D adjoint; at 256^3 / 360 views 1: 64.0 ms, 2: 54.9, 3: 55.3, 4: 60.8)
 #endif
+#ifndef ELSA_AXIS_TD
+#define ELSA_AXIS_TD 8 // depth along the driving axis of the 3D adjoint's axis bricks
+#endif
+#ifndef ELSA_AXIS_TA
+#define ELSA_AXIS_TA 32 // edge along the first non-driving axis
+#endif
+#ifndef ELSA_AXIS_TB
+#define ELSA_AXIS_TB 16 // edge along the second non-driving axis
+#endif
 #ifndef ELSA_SPLAT_UNROLL
 #define ELSA_SPLAT_UNROLL 2 // unroll factor of the adjoint's per-sample loop (1: 72.8 ms, 2: 63.4 ms, 4: 68.9 ms at 256^3)
 #endif
@@ -447,7 +456,7 @@ namespace elsa_b200
         __global__ void josephWindowCheckKernel(const JosephRay* __restrict__ rays,
                                                 const RayWindow* __restrict__ windows,
                                                 VolumeShape vol, DetectorShape det, int3 brick,
-                                                int3 nBricks,
+                                                int3 nBricks, int onlyAxis,
                                                 unsigned long long* __restrict__ misses)
         {
             const int64_t nrays = static_cast<int64_t>(det.nu) * det.nv * det.np;
@@ -455,7 +464,7 @@ namespace elsa_b200
             if (r >= nrays)
                 return;
             const JosephRay R = rays[r];
-            if (R.n == 0)
+            if (R.n == 0 || (onlyAxis >= 0 && (R.meta & 3) != onlyAxis))
                 return;
             const int u = static_cast<int>(r % det.nu);
             const int v = static_cast<int>((r / det.nu) % det.nv);
@@ -907,6 +916,7 @@ namespace elsa_b200
         constexpr int kAdjoint3dWarpsPerSm = ELSA_ADJ3D_WARPS_PER_SM;
         constexpr int kMinAdjointChunks = 32;                // default floor of the view chunks
         constexpr int64_t kChunkMemory = int64_t(1) << 31;   // default partial-volume budget
+        constexpr int64_t kBatchPartialMemory = int64_t(8) << 30; // batched adjoints: up to 8 GiB
 
         template <int DIM, int BX, int BY, int BZ, int CPD, int NW>
         struct AdjointConfig {
@@ -1238,6 +1248,232 @@ namespace elsa_b200
             }
         };
 
+        // ---------------------------------------------------------------------------------------
+        // 3D adjoint on axis bricks. The rays of one view all step along about the same axis G, so
+        // the volume is cut, per driving axis present, into bricks that are TD planes deep along G
+        // and TA x TB voxels across (a < b the other two axes). A ray crossing such a brick keeps
+        // most of its TD samples inside it (a 16^3 brick loses half of the samples of oblique rays
+        // to its sides), and the window of a brick, the pixels whose centres lie in the projection
+        // of the brick grown by half a voxel, holds few rays that miss it. One warp owns a brick
+        // in shared memory for a chunk of views and splats the window's rays class by class, as
+        // the 16^3 warp kernel does. Across the rays the brick keeps a halo of two voxels on every
+        // side: tap indices are clamped into it instead of tested, and the halo is not written out.
+        // ---------------------------------------------------------------------------------------
+        constexpr int kAxisHalo = 2;
+
+        template <int TD, int TA, int TB>
+        struct AxisBrick {
+            static constexpr int kRow = TA + 2 * kAxisHalo;  // words per row along a (fastest)
+            static constexpr int kRows = TB + 2 * kAxisHalo; // rows along b
+            static constexpr int kPlaneMin = kRow * kRows;
+            // plane stride congruent to 1 modulo 32: lanes one plane apart use other banks
+            static constexpr int kPlane = kPlaneMin + ((33 - kPlaneMin % 32) % 32);
+            static constexpr int kWords = kPlane * TD;
+            static constexpr int kOrigin = kAxisHalo * kRow + kAxisHalo; // word of (a, b) = (0, 0)
+        };
+
+        // Word of the bilinear footprint of position (pa, pb) on `plane` (the brick word of
+        // a = b = 0 on that plane) and the reference's weights (JosephsMethod.cpp:37-52); tap
+        // indices outside the brick are clamped into the halo.
+        template <int TA, int TB, int ROW>
+        __device__ __forceinline__ float* axisTap(float* plane, float pa, float pb, int orgA,
+                                                  int orgB, float& wa, float& cwa, float& wb,
+                                                  float& cwb)
+        {
+            const float fa = floorf(__fsub_rn(pa, 0.5f));
+            const float fb = floorf(__fsub_rn(pb, 0.5f));
+            cwa = __fsub_rn(__fsub_rn(pa, fa), 0.5f);
+            cwb = __fsub_rn(__fsub_rn(pb, fb), 0.5f);
+            wa = __fsub_rn(1.0f, cwa);
+            wb = __fsub_rn(1.0f, cwb);
+            const int la = min(max(static_cast<int>(fa) - orgA, -kAxisHalo), TA);
+            const int lb = min(max(static_cast<int>(fb) - orgB, -kAxisHalo), TB);
+            return plane + lb * ROW + la;
+        }
+
+        // Samples jLo..jHi of ray R (position cp at sample jLo, on brick plane t0) into the brick.
+        // Software-pipelined: the footprint of sample j+1 (always on another plane) is read before
+        // the sums of sample j are written back.
+        template <int TD, int TA, int TB>
+        __device__ __forceinline__ void axisSplat(float* acc, const JosephRay& R, float yl,
+                                                  float2 cp, int jLo, int jHi, int t0, int orgA,
+                                                  int orgB)
+        {
+            using L = AxisBrick<TD, TA, TB>;
+            constexpr int ROW = L::kRow;
+            const int dPlane = ((R.meta & 4) ? -1 : 1) * L::kPlane;
+            float* plane = acc + L::kOrigin + t0 * L::kPlane;
+            float pa = cp.x, pb = cp.y;
+            float wa, cwa, wb, cwb;
+            float* q = axisTap<TA, TB, ROW>(plane, pa, pb, orgA, orgB, wa, cwa, wb, cwb);
+            float v0 = q[0], v1 = q[1], v2 = q[ROW], v3 = q[ROW + 1];
+            float ya = yl * wa, yc = yl * cwa;
+#pragma unroll kSplatUnroll
+            for (int j = jLo; j < jHi; ++j) {
+                plane += dPlane;
+                pa = __fadd_rn(pa, R.sa);
+                pb = __fadd_rn(pb, R.sb);
+                float wa2, cwa2, wb2, cwb2;
+                float* q2 = axisTap<TA, TB, ROW>(plane, pa, pb, orgA, orgB, wa2, cwa2, wb2, cwb2);
+                const float n0 = q2[0], n1 = q2[1], n2 = q2[ROW], n3 = q2[ROW + 1];
+                q[0] = v0 + ya * wb;
+                q[1] = v1 + yc * wb;
+                q[ROW] = v2 + ya * cwb;
+                q[ROW + 1] = v3 + yc * cwb;
+                q = q2;
+                v0 = n0, v1 = n1, v2 = n2, v3 = n3;
+                ya = yl * wa2, yc = yl * cwa2;
+                wb = wb2, cwb = cwb2;
+            }
+            q[0] = v0 + ya * wb;
+            q[1] = v1 + yc * wb;
+            q[ROW] = v2 + ya * cwb;
+            q[ROW + 1] = v3 + yc * cwb;
+        }
+
+        // One view for an axis brick of grid G: m x m ray classes separated by __syncwarp; lane i
+        // takes class rays i, i + 32, ... (u fastest within the class grid).
+        template <int G, int TD, int TA, int TB, int CPD>
+        __device__ __forceinline__ void axisView(float* acc, const RayWindow& w, int p, int m,
+                                                 const JosephRay* __restrict__ rays,
+                                                 const float2* __restrict__ cps, int64_t nrays,
+                                                 const float* __restrict__ y,
+                                                 const DetectorShape& det, int orgG, int orgA,
+                                                 int orgB)
+        {
+            const int kLo = orgG, kHi = orgG + TD - 1;
+            const int slabLo = (orgG / CPD) * CPD, slabHi = slabLo + CPD - 1;
+            const int64_t cpRow = static_cast<int64_t>(orgG / CPD + 1) * nrays;
+            const int lane = threadIdx.x & 31;
+            const int64_t viewBase = static_cast<int64_t>(det.nu) * det.nv * p;
+            for (int ov = 0; ov < m; ++ov) {
+                const int vStart = w.v0 + ov;
+                const int nvc = vStart <= w.v1 ? (w.v1 - vStart) / m + 1 : 0;
+                for (int ou = 0; ou < m; ++ou) {
+                    const int uStart = w.u0 + ou;
+                    const int nuc = uStart <= w.u1 ? (w.u1 - uStart) / m + 1 : 0;
+                    const int total = nuc * nvc;
+                    const float invNuc = nuc > 0 ? 1.0f / static_cast<float>(nuc) : 0.0f;
+                    constexpr int kBatch = ELSA_ADJ_BATCH;
+                    for (int base = lane; base < total; base += 32 * kBatch) {
+                        JosephRay Rb[kBatch];
+                        float2 cpb[kBatch];
+                        float yb[kBatch];
+#pragma unroll
+                        for (int q = 0; q < kBatch; ++q) {
+                            const int i = base + 32 * q;
+                            Rb[q].n = 0;
+                            if (i < total) {
+                                // i / nuc by a float reciprocal: exact for i < 2^20, nuc < 2^11
+                                const int iv =
+                                    static_cast<int>((static_cast<float>(i) + 0.5f) * invNuc);
+                                const int iu = i - iv * nuc;
+                                const int64_t r = viewBase + (uStart + iu * m) +
+                                                  static_cast<int64_t>(det.nu) * (vStart + iv * m);
+                                Rb[q] = rays[r];
+                                cpb[q] = __ldg(cps + cpRow + r);
+                                yb[q] = __ldg(y + r);
+                            }
+                        }
+#pragma unroll
+                        for (int q = 0; q < kBatch; ++q) {
+                            const JosephRay& R = Rb[q];
+                            if (R.n == 0 || (R.meta & 3) != G)
+                                continue;
+                            int jLo, jHi;
+                            if (!sampleRange(R, kLo, kHi, jLo, jHi))
+                                continue;
+                            // the checkpoint holds the position at the ray's first sample in the
+                            // slab; a brick thinner than the slab advances it to its own planes
+                            float2 cp = cpb[q];
+                            if (TD < CPD) {
+                                int jS0, jS1;
+                                sampleRange(R, slabLo, slabHi, jS0, jS1);
+                                for (int j = jS0; j < jLo; ++j) {
+                                    cp.x = __fadd_rn(cp.x, R.sa);
+                                    cp.y = __fadd_rn(cp.y, R.sb);
+                                }
+                            }
+                            const int dir = (R.meta & 4) ? -1 : 1;
+                            const int t0 = R.k0 + jLo * dir - orgG;
+                            axisSplat<TD, TA, TB>(acc, R, yb[q] * R.len, cp, jLo, jHi, t0, orgA,
+                                                  orgB);
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+
+        // Brick edges of grid G in volume axis order (x, y, z).
+        template <int G, int TD, int TA, int TB>
+        __host__ __device__ constexpr int axisBrickEdge(int axis)
+        {
+            return axis == G ? TD : (axis == (G == 0 ? 1 : 0) ? TA : TB);
+        }
+
+        // One warp per axis brick of grid G and per chunk entry (blockIdx.y): chunk entry e of
+        // the grid covers views [chunks[e].x * per, ...) and writes its partial volume
+        // chunks[e].y (or x itself when the adjoint has a single partial).
+        template <int G, int TD, int TA, int TB, int CPD>
+        __global__ void __launch_bounds__(32, ELSA_ADJ_MIN_BLOCKS)
+            josephAdjointAxisKernel(const JosephRay* __restrict__ rays,
+                                    const float2* __restrict__ checkpoints, int64_t nrays,
+                                    const float* __restrict__ y,
+                                    const RayWindow* __restrict__ windows,
+                                    const unsigned* __restrict__ viewAxes,
+                                    const int2* __restrict__ chunks, int entryBase,
+                                    int viewsPerChunk, VolumeShape vol, DetectorShape det, int m,
+                                    int3 nBricks, float* __restrict__ out, int64_t yStride,
+                                    int64_t outStride)
+        {
+            // blockIdx.z: batch element (sinogram y + b yStride, partial volumes out + b outStride)
+            y += blockIdx.z * yStride;
+            out += blockIdx.z * outStride;
+            using L = AxisBrick<TD, TA, TB>;
+            __shared__ float acc[L::kWords];
+            constexpr int EX = axisBrickEdge<G, TD, TA, TB>(0);
+            constexpr int EY = axisBrickEdge<G, TD, TA, TB>(1);
+            constexpr int EZ = axisBrickEdge<G, TD, TA, TB>(2);
+            const int lane = threadIdx.x;
+            const int bi = blockIdx.x;
+            const int org[3] = {(bi % nBricks.x) * EX, ((bi / nBricks.x) % nBricks.y) * EY,
+                                (bi / (nBricks.x * nBricks.y)) * EZ};
+            int a, b;
+            nonDrivingAxes(G, a, b);
+            const int orgG = org[G], orgA = org[a], orgB = org[b];
+            const int nb = nBricks.x * nBricks.y * nBricks.z;
+            for (int i = lane; i < L::kWords; i += 32)
+                acc[i] = 0.0f;
+            __syncwarp();
+            const int2 entry = chunks[entryBase + blockIdx.y];
+            const int pBegin = entry.x * viewsPerChunk;
+            const int pEnd = min(det.np, pBegin + viewsPerChunk);
+            for (int p = pBegin; p < pEnd; ++p) {
+                if (!(viewAxes[p] & (1u << G)))
+                    continue;
+                const RayWindow w = windows[static_cast<int64_t>(p) * nb + bi];
+                if (w.u0 > w.u1 || w.v0 > w.v1)
+                    continue;
+                axisView<G, TD, TA, TB, CPD>(acc, w, p, m, rays, checkpoints, nrays, y, det,
+                                             orgG, orgA, orgB);
+            }
+            __syncwarp();
+            const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
+            float* dst = out + static_cast<int64_t>(entry.y) * nvox;
+            for (int i = lane; i < TD * TA * TB; i += 32) {
+                // i runs x fastest over the brick's voxels
+                const int lx = i % EX, ly = (i / EX) % EY, lz = i / (EX * EY);
+                const int gx = org[0] + lx, gy = org[1] + ly, gz = org[2] + lz;
+                if (gx < vol.n[0] && gy < vol.n[1] && gz < vol.n[2]) {
+                    const int l[3] = {lx, ly, lz};
+                    dst[gx + static_cast<int64_t>(vol.n[0]) *
+                                 (gy + static_cast<int64_t>(vol.n[1]) * gz)] =
+                        acc[L::kOrigin + l[G] * L::kPlane + l[b] * L::kRow + l[a]];
+                }
+            }
+        }
+
         using Adjoint3d = WarpAdjointConfig<16, 16, ELSA_ADJ_BZ, 16>;
         using Adjoint2d = AdjointConfig<2, 64, 64, 1, 64, 8>;
 
@@ -1300,9 +1536,7 @@ namespace elsa_b200
 
                 int cpd;
                 if (vol_.dim == 3) {
-                    brick_ = Adjoint3d::brick();
-                    cpd = Adjoint3d::kCheckpointDepth;
-                    Adjoint3d::prepare(det_.np);
+                    cpd = kAxisCheckpointDepth;
                 } else {
                     brick_ = Adjoint2d::brick();
                     cpd = Adjoint2d::kCheckpointDepth;
@@ -1315,16 +1549,20 @@ namespace elsa_b200
                                                             dCheckpoints_);
                 ELSA_LAUNCH_CHECK("josephCheckpointKernel");
 
-                nBricks_ = make_int3((vol_.n[0] + brick_.x - 1) / brick_.x,
-                                     (vol_.n[1] + brick_.y - 1) / brick_.y,
-                                     (vol_.n[2] + brick_.z - 1) / brick_.z);
-                const int64_t nwin =
-                    static_cast<int64_t>(nBricks_.x) * nBricks_.y * nBricks_.z * det_.np;
-                ELSA_CUDA(cudaMalloc(&dWindows_, sizeof(RayWindow) * nwin));
-                josephWindowKernel<<<static_cast<unsigned>((nwin + 255) / 256), 256>>>(
-                    dPoses_, vol_, det_, brick_, nBricks_, curved_.map(), windowGrow(vol_),
-                    kWindowPixelMargin, dWindows_);
-                ELSA_LAUNCH_CHECK("josephWindowKernel");
+                if (vol_.dim == 3) {
+                    buildAxisGrids();
+                } else {
+                    nBricks_ = make_int3((vol_.n[0] + brick_.x - 1) / brick_.x,
+                                         (vol_.n[1] + brick_.y - 1) / brick_.y,
+                                         (vol_.n[2] + brick_.z - 1) / brick_.z);
+                    const int64_t nwin =
+                        static_cast<int64_t>(nBricks_.x) * nBricks_.y * nBricks_.z * det_.np;
+                    ELSA_CUDA(cudaMalloc(&dWindows_, sizeof(RayWindow) * nwin));
+                    josephWindowKernel<<<static_cast<unsigned>((nwin + 255) / 256), 256>>>(
+                        dPoses_, vol_, det_, brick_, nBricks_, curved_.map(), windowGrow(vol_),
+                        kWindowPixelMargin, dWindows_);
+                    ELSA_LAUNCH_CHECK("josephWindowKernel");
+                }
                 setKnob(kKnobAdjointChunks, defaultChunks());
                 if (vol_.dim == 3) {
                     std::vector<float> hp(poses_.size() * kPoseFloats);
@@ -1515,17 +1753,67 @@ namespace elsa_b200
                     ELSA_LAUNCH_CHECK("josephScatterKernel");
                     return;
                 }
+                if (vol_.dim == 3) {
+                    const int used = usedChunks();
+                    float* out = axisPartials_ > 1 ? partial_->as<float>() : x;
+                    launchAxisChunks(0, used, y, out, s);
+                    if (axisPartials_ > 1)
+                        launchSumChunks(partial_->as<float>(), axisPartials_, domainSize_, x, s);
+                    return;
+                }
                 const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
                 float* partial = partial_ ? partial_->as<float>() : nullptr;
-                if (vol_.dim == 3)
-                    Adjoint3d::launch(nb, adjointChunks_, s, dRays_, dCheckpoints_, rangeSize_, y,
-                                      dWindows_, dViewAxes_, vol_, det_, classSpacing_, nBricks_,
-                                      x, partial);
-                else
-                    Adjoint2d::launch(nb, adjointChunks_, s, dRays_, dCheckpoints_, rangeSize_, y,
-                                      dWindows_, dViewAxes_, vol_, det_, classSpacing_, nBricks_,
-                                      x, partial);
+                Adjoint2d::launch(nb, adjointChunks_, s, dRays_, dCheckpoints_, rangeSize_, y,
+                                  dWindows_, dViewAxes_, vol_, det_, classSpacing_, nBricks_, x,
+                                  partial);
                 ELSA_LAUNCH_CHECK("josephAdjointKernel");
+            }
+
+            // Batched applies (3D matched operator): one launch per kernel for all volumes,
+            // sharing the ray tables; every batch element is computed exactly as by a single
+            // apply (same kernels, chunks and summation order).
+            void forwardBatch(const float* x, int64_t xs, float* y, int64_t ys, int batch,
+                              cudaStream_t s) override
+            {
+                if (!tma_) {
+                    Projector::forwardBatch(x, xs, y, ys, batch, s);
+                    return;
+                }
+                tma_->forwardBatch(x, xs, y, ys, batch, s);
+            }
+            void adjointBatch(const float* y, int64_t ys, float* x, int64_t xs, int batch,
+                              cudaStream_t s) override
+            {
+                if (batch <= 0)
+                    return;
+                if (fast_ || scatter_ || vol_.dim != 3) {
+                    Projector::adjointBatch(y, ys, x, xs, batch, s);
+                    return;
+                }
+                const int used = usedChunks();
+                if (axisPartials_ <= 1) {
+                    launchAxisChunks(0, used, y, x, s, batch, ys, xs);
+                    return;
+                }
+                // partial volumes for as many batch elements as fit in kBatchPartialMemory
+                const int64_t perElem = static_cast<int64_t>(axisPartials_) * domainSize_;
+                const int fit = static_cast<int>(std::max<int64_t>(
+                    1, std::min<int64_t>(batch, kBatchPartialMemory / (4 * perElem))));
+                const size_t need = sizeof(float) * static_cast<size_t>(perElem) * fit;
+                if (partial_->bytes() < need) {
+                    ELSA_CUDA(cudaStreamSynchronize(s)); // no launch in flight reads the old one
+                    ELSA_CUDA(cudaDeviceSynchronize());
+                    partial_.reset();
+                    partial_ = std::make_unique<DeviceBuffer>(need);
+                }
+                for (int b0 = 0; b0 < batch; b0 += fit) {
+                    const int nb = std::min(fit, batch - b0);
+                    launchAxisChunks(0, used, y + b0 * ys, partial_->as<float>(), s, nb, ys,
+                                     perElem);
+                    for (int b = 0; b < nb; ++b)
+                        launchSumChunks(partial_->as<float>() + b * perElem, axisPartials_,
+                                        domainSize_, x + (b0 + b) * xs, s);
+                }
             }
 
             // Host-buffer pipelining: kHostGroups groups of views for the TMA forward; for the
@@ -1567,7 +1855,7 @@ namespace elsa_b200
             }
             int adjointGroups() const override
             {
-                if (fast_ || scatter_ || vol_.dim != 3 || !partial_)
+                if (fast_ || scatter_ || vol_.dim != 3 || axisPartials_ <= 1)
                     return 0;
                 return usedChunks() >= kHostGroups ? kHostGroups : 0;
             }
@@ -1581,17 +1869,11 @@ namespace elsa_b200
             void adjointGroup(const float* y, int g, int G, cudaStream_t s) override
             {
                 (void)G;
-                const int per = (det_.np + adjointChunks_ - 1) / adjointChunks_;
-                const int c0 = groupChunk(g), c1 = groupChunk(g + 1);
-                Adjoint3d::launchChunks(nBricks_.x * nBricks_.y * nBricks_.z, c0, c1, per, s,
-                                        dRays_, dCheckpoints_, rangeSize_, y, dWindows_,
-                                        dViewAxes_, vol_, det_, classSpacing_, nBricks_,
-                                        partial_->as<float>());
-                ELSA_LAUNCH_CHECK("josephAdjointWarpKernel");
+                launchAxisChunks(groupChunk(g), groupChunk(g + 1), y, partial_->as<float>(), s);
             }
             void adjointFinish(float* x, cudaStream_t s) override
             {
-                launchSumChunks(partial_->as<float>(), usedChunks(), domainSize_, x, s);
+                launchSumChunks(partial_->as<float>(), axisPartials_, domainSize_, x, s);
             }
 
             std::vector<int> knobCandidates(int knob) const override
@@ -1642,15 +1924,16 @@ namespace elsa_b200
                     scatter_ = value;
                     return;
                 }
+                adjointChunks_ = value;
+                const int volumes = vol_.dim == 3 ? buildAxisEntries() : value;
                 const size_t need = sizeof(float) * static_cast<size_t>(domainSize_) *
-                                    static_cast<size_t>(value);
-                if (value <= 1)
+                                    static_cast<size_t>(volumes);
+                if (volumes <= 1)
                     partial_.reset();
                 else if (!partial_ || partial_->bytes() < need) {
                     partial_.reset();
                     partial_ = std::make_unique<DeviceBuffer>(need);
                 }
-                adjointChunks_ = value;
             }
 
             bool setWaitTest(long long cycles, bool withhold) override
@@ -1666,7 +1949,14 @@ namespace elsa_b200
                 switch (key) {
                 case 0:
                     return classSpacing_;
-                case 1:
+                case 1: // bricks of the matched adjoint (3D: over the axis grids)
+                    if (vol_.dim == 3) {
+                        int64_t n = 0;
+                        for (const AxisGrid& g : grids_)
+                            if (g.present)
+                                n += static_cast<int64_t>(g.nb.x) * g.nb.y * g.nb.z;
+                        return n;
+                    }
                     return nBricks_.x * nBricks_.y * nBricks_.z;
                 case 2:
                     return sampleCount_;
@@ -1676,8 +1966,17 @@ namespace elsa_b200
                     return tma_ ? static_cast<int64_t>(tma_->fallbackFraction() * 1e6) : -1;
                 case 6: // kernel launches per forward call
                     return tma_ ? tma_->launchesPerForward() : 1;
-                case 7: // kernel launches per adjoint call (with view chunks: + the chunk sum)
-                    return (!fast_ && !scatter_ && adjointChunks_ > 1) ? 2 : 1;
+                case 7: // kernel launches per adjoint call (3D: one per axis grid; with
+                        // several partial volumes: + the chunk sum)
+                    if (fast_ || scatter_)
+                        return 1;
+                    if (vol_.dim == 3) {
+                        int n = 0;
+                        for (const AxisGrid& g : grids_)
+                            n += g.present && g.entryEnd > g.entryBegin ? 1 : 0;
+                        return n + (axisPartials_ > 1 ? 1 : 0);
+                    }
+                    return adjointChunks_ > 1 ? 2 : 1;
                 case 8: // taps outside the windows of their bricks (test support; synchronizes)
                     return windowMisses();
                 default:
@@ -1688,14 +1987,23 @@ namespace elsa_b200
         private:
             int64_t windowMisses() const
             {
-                if (!dWindows_)
+                if (fast_ || (vol_.dim == 2 && !dWindows_))
                     return -1;
                 DeviceBuffer count(sizeof(unsigned long long));
                 ELSA_CUDA(cudaMemset(count.as<unsigned long long>(), 0, sizeof(unsigned long long)));
                 const int64_t nrays = rangeSize_;
-                josephWindowCheckKernel<<<static_cast<unsigned>((nrays + 255) / 256), 256>>>(
-                    dRays_, dWindows_, vol_, det_, brick_, nBricks_,
-                    count.as<unsigned long long>());
+                const unsigned blocks = static_cast<unsigned>((nrays + 255) / 256);
+                if (vol_.dim == 3) {
+                    for (int g = 0; g < 3; ++g)
+                        if (grids_[g].present)
+                            josephWindowCheckKernel<<<blocks, 256>>>(
+                                dRays_, grids_[g].windows->as<RayWindow>(), vol_, det_,
+                                grids_[g].edge, grids_[g].nb, g, count.as<unsigned long long>());
+                } else {
+                    josephWindowCheckKernel<<<blocks, 256>>>(dRays_, dWindows_, vol_, det_,
+                                                             brick_, nBricks_, -1,
+                                                             count.as<unsigned long long>());
+                }
                 ELSA_LAUNCH_CHECK("josephWindowCheckKernel");
                 unsigned long long h = 0;
                 ELSA_CUDA(cudaMemcpy(&h, count.as<unsigned long long>(), sizeof(h),
@@ -1728,13 +2036,155 @@ namespace elsa_b200
             // the adjoint takes 63.4 ms with 1 chunk, 55.5 with 8 and 54.8 with 16-32.
             int defaultChunks() const
             {
-                const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
-                const int fill = vol_.dim == 2 ? Adjoint2d::chunks(nb, det_.np)
-                                               : Adjoint3d::chunks(nb, det_.np);
+                int fill;
+                if (vol_.dim == 2) {
+                    fill = Adjoint2d::chunks(nBricks_.x * nBricks_.y * nBricks_.z, det_.np);
+                } else {
+                    // bricks x chunks of the smallest present grid reach kAdjoint3dWarpsPerSm
+                    // one-warp CTAs per SM (each grid sees about its share of the views)
+                    int64_t nb = 0;
+                    for (const AxisGrid& g : grids_)
+                        if (g.present)
+                            nb = std::max<int64_t>(nb, static_cast<int64_t>(g.nb.x) * g.nb.y *
+                                                           g.nb.z);
+                    const int64_t want = (kAdjoint3dWarpsPerSm * 148 + nb - 1) / std::max<int64_t>(nb, 1);
+                    fill = static_cast<int>(std::min<int64_t>(det_.np, std::max<int64_t>(1, want)));
+                }
+                // partial volumes within kChunkMemory: the 3D adjoint writes one per (chunk,
+                // axis grid) pair, so leave room for the chunks whose views drive along two axes
                 const int64_t cap = std::max<int64_t>(1, kChunkMemory / (4 * domainSize_));
+                const int64_t capChunks = vol_.dim == 3 ? std::max<int64_t>(1, cap * 7 / 8) : cap;
                 return static_cast<int>(std::min<int64_t>(
-                    std::min<int64_t>(det_.np, cap), std::max(fill, kMinAdjointChunks)));
+                    std::min<int64_t>(det_.np, capChunks), std::max(fill, kMinAdjointChunks)));
             }
+
+            // ---- 3D matched adjoint on axis bricks ----
+            static constexpr int kAxisTD = ELSA_AXIS_TD, kAxisTA = ELSA_AXIS_TA,
+                                 kAxisTB = ELSA_AXIS_TB;
+            static constexpr int kAxisCheckpointDepth = 16;
+            static_assert(kAxisCheckpointDepth % kAxisTD == 0,
+                          "axis bricks are a whole fraction of a checkpoint slab deep");
+            struct AxisGrid {
+                bool present = false;
+                int3 edge{}, nb{}; // brick edges and brick counts in volume axis order
+                std::unique_ptr<DeviceBuffer> windows; // [view][brick]
+                int entryBegin = 0, entryEnd = 0;      // this grid's (chunk, partial) entries
+            };
+            AxisGrid grids_[3];
+            std::vector<unsigned> viewAxesHost_;
+            std::vector<int2> entries_;                 // (chunk, partial volume), grid-major
+            std::unique_ptr<DeviceBuffer> dEntries_;
+            int axisPartials_ = 0;                      // partial volumes of the 3D adjoint
+
+            static int3 axisEdge(int g)
+            {
+                const int e[3] = {g == 0 ? kAxisTD : kAxisTA, g == 1 ? kAxisTD : (g == 0 ? kAxisTA : kAxisTB),
+                                  g == 2 ? kAxisTD : kAxisTB};
+                return make_int3(e[0], e[1], e[2]);
+            }
+
+            // Brick grids and windows for every driving axis of the geometry.
+            void buildAxisGrids()
+            {
+                viewAxesHost_.resize(det_.np);
+                ELSA_CUDA(cudaMemcpy(viewAxesHost_.data(), dViewAxes_, sizeof(unsigned) * det_.np,
+                                     cudaMemcpyDeviceToHost));
+                for (int g = 0; g < 3; ++g) {
+                    AxisGrid& G = grids_[g];
+                    G.present = std::any_of(viewAxesHost_.begin(), viewAxesHost_.end(),
+                                            [g](unsigned a) { return (a >> g) & 1u; });
+                    if (!G.present)
+                        continue;
+                    G.edge = axisEdge(g);
+                    G.nb = make_int3((vol_.n[0] + G.edge.x - 1) / G.edge.x,
+                                     (vol_.n[1] + G.edge.y - 1) / G.edge.y,
+                                     (vol_.n[2] + G.edge.z - 1) / G.edge.z);
+                    const int64_t nwin = static_cast<int64_t>(G.nb.x) * G.nb.y * G.nb.z * det_.np;
+                    G.windows = std::make_unique<DeviceBuffer>(sizeof(RayWindow) * nwin);
+                    josephWindowKernel<<<static_cast<unsigned>((nwin + 255) / 256), 256>>>(
+                        dPoses_, vol_, det_, G.edge, G.nb, curved_.map(), windowGrow(vol_),
+                        kWindowPixelMargin, G.windows->as<RayWindow>());
+                    ELSA_LAUNCH_CHECK("josephWindowKernel");
+                }
+            }
+
+            // (chunk, partial volume) entries of every grid for adjointChunks_ view chunks: chunk
+            // c covers views [c per, (c + 1) per); a grid takes the chunks holding a view that
+            // drives along its axis. Partial volumes are numbered by (chunk, axis), the order in
+            // which the chunk sum adds them. Returns the number of partial volumes.
+            int buildAxisEntries()
+            {
+                const int per = (det_.np + adjointChunks_ - 1) / adjointChunks_;
+                const int used = (det_.np + per - 1) / per;
+                std::vector<std::vector<int2>> byGrid(3);
+                int next = 0;
+                for (int c = 0; c < used; ++c) {
+                    for (int g = 0; g < 3; ++g) {
+                        if (!grids_[g].present)
+                            continue;
+                        bool any = false;
+                        for (int p = c * per; p < std::min(det_.np, (c + 1) * per) && !any; ++p)
+                            any = (viewAxesHost_[p] >> g) & 1u;
+                        if (any)
+                            byGrid[g].push_back(make_int2(c, next++));
+                    }
+                }
+                entries_.clear();
+                for (int g = 0; g < 3; ++g) {
+                    grids_[g].entryBegin = static_cast<int>(entries_.size());
+                    entries_.insert(entries_.end(), byGrid[g].begin(), byGrid[g].end());
+                    grids_[g].entryEnd = static_cast<int>(entries_.size());
+                }
+                if (next == 1) // one partial: the kernel writes x itself
+                    for (auto& e : entries_)
+                        e.y = 0;
+                dEntries_ = std::make_unique<DeviceBuffer>(sizeof(int2) * std::max<size_t>(1, entries_.size()));
+                if (!entries_.empty())
+                    ELSA_CUDA(cudaMemcpy(dEntries_->as<int2>(), entries_.data(),
+                                         sizeof(int2) * entries_.size(), cudaMemcpyHostToDevice));
+                axisPartials_ = next;
+                return next;
+            }
+
+            // The axis-brick kernels for view chunks [c0, c1), writing their partial volumes into
+            // out (x itself when there is a single partial volume); `batch` sinograms
+            // y + b yStride into out + b outStride.
+            void launchAxisChunks(int c0, int c1, const float* y, float* out, cudaStream_t s,
+                                  int batch = 1, int64_t yStride = 0, int64_t outStride = 0)
+            {
+                const int per = (det_.np + adjointChunks_ - 1) / adjointChunks_;
+                for (int g = 0; g < 3; ++g) {
+                    const AxisGrid& G = grids_[g];
+                    if (!G.present)
+                        continue;
+                    int e0 = G.entryBegin, e1 = G.entryBegin;
+                    for (int e = G.entryBegin; e < G.entryEnd; ++e) {
+                        if (entries_[e].x < c0)
+                            e0 = e + 1;
+                        if (entries_[e].x < c1)
+                            e1 = e + 1;
+                    }
+                    if (e1 <= e0)
+                        continue;
+                    const dim3 grid(static_cast<unsigned>(G.nb.x * G.nb.y * G.nb.z),
+                                    static_cast<unsigned>(e1 - e0), static_cast<unsigned>(batch));
+                    const RayWindow* win = G.windows->as<RayWindow>();
+                    const int2* ent = dEntries_->as<int2>();
+#define ELSA_AXIS_LAUNCH(G_)                                                                     \
+    josephAdjointAxisKernel<G_, kAxisTD, kAxisTA, kAxisTB, kAxisCheckpointDepth><<<grid, 32, 0, s>>>( \
+        dRays_, dCheckpoints_, rangeSize_, y, win, dViewAxes_, ent, e0, per, vol_, det_,          \
+        classSpacing_, G.nb, out, yStride, outStride)
+                    if (g == 0)
+                        ELSA_AXIS_LAUNCH(0);
+                    else if (g == 1)
+                        ELSA_AXIS_LAUNCH(1);
+                    else
+                        ELSA_AXIS_LAUNCH(2);
+#undef ELSA_AXIS_LAUNCH
+                    ELSA_LAUNCH_CHECK("josephAdjointAxisKernel");
+                }
+            }
+
             int3 brick_{}, nBricks_{};
         };
     } // namespace

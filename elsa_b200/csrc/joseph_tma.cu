@@ -87,23 +87,29 @@ namespace elsa_b200
             return true;
         }
 
-        __device__ __forceinline__ void tmaLoad3d(float* dst, const CUtensorMap* map, int c0,
-                                                  int c1, int c2, uint64_t* bar)
+        // Box (c0, c1, c2) of batch element c3 of the permuted copies (a 4D tensor map whose
+        // slowest dimension is the batch element; the box is one element deep there).
+        __device__ __forceinline__ void tmaLoad4d(float* dst, const CUtensorMap* map, int c0,
+                                                  int c1, int c2, int c3, uint64_t* bar)
         {
             asm volatile(
-                "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-                " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smemAddr(dst)),
-                "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2),
+                "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smemAddr(dst)),
+                "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
                 "r"(smemAddr(bar))
                 : "memory");
         }
 
         // out[(k * nSlow + s) * padFast + f] = x(axis values), zero in the padding columns.
+        // blockIdx.y: batch element (x + b xStride into copy b of out)
         __global__ void permuteKernel(const float* __restrict__ x, VolumeShape vol, int g, int sAx,
-                                      int fAx, int padFast, float* __restrict__ out)
+                                      int fAx, int padFast, float* __restrict__ out,
+                                      int64_t xStride)
         {
             const int nf = vol.n[fAx], ns = vol.n[sAx], ng = vol.n[g];
             const int64_t total = static_cast<int64_t>(padFast) * ns * ng;
+            x += blockIdx.y * xStride;
+            out += blockIdx.y * total;
             const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
             for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
                  i < total; i += stride) {
@@ -284,8 +290,12 @@ namespace elsa_b200
                              const float* __restrict__ x, VolumeShape vol, DetectorShape det,
                              int tilesU, int tilesV, int3 fastAxis, float* __restrict__ y,
                              unsigned* __restrict__ error, int tileBase, long long waitCycles,
-                             int withhold)
+                             int withhold, int64_t xStride, int64_t yStride)
         {
+            // blockIdx.y: batch element (volume x + b xStride, sinogram y + b yStride)
+            const int batch = static_cast<int>(blockIdx.y);
+            x += batch * xStride;
+            y += batch * yStride;
             extern __shared__ __align__(128) float stage[];
             __shared__ __align__(8) uint64_t full[NS];
             __shared__ int abortFlag;
@@ -328,7 +338,7 @@ namespace elsa_b200
                 const int gOrg = dir > 0 ? T.kStart + ch * BD : T.kStart - ch * BD - (BD - 1);
                 mbarExpectTx(&full[s], kStageBytes);
                 if (!withhold) // test mode: the barrier waits for bytes that never come
-                    tmaLoad3d(stage + s * kStageFloats, map, o.x, o.y, gOrg, &full[s]);
+                    tmaLoad4d(stage + s * kStageFloats, map, o.x, o.y, gOrg, batch, &full[s]);
             };
             if (threadIdx.x == 0)
                 for (int ch = 0; ch < NS && ch < T.nChunks; ++ch)
@@ -472,20 +482,43 @@ namespace elsa_b200
             }
         }
         fallbackFraction_ = live + fallback ? double(fallback) / double(live + fallback) : 0.0;
+        for (int g = 0; g < 3; ++g)
+            if (present_[g])
+                padFast_[g] = (vol.n[fast_[g]] + 3) / 4 * 4;
+        ensureBatch(1);
+        ELSA_CUDA(cudaFuncSetAttribute(forwardTmaKernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(NS * kStageBytes)));
+    }
+
+    // Permuted copies for `batch` volumes and their tensor maps (4D: fast, slow, driving axis,
+    // batch element). Grows only; growing waits for the device, since launches in flight read
+    // the old copies.
+    void JosephForwardTma::ensureBatch(int batch)
+    {
+        if (batch <= batchCap_)
+            return;
+        if (batchCap_ > 0)
+            ELSA_CUDA(cudaDeviceSynchronize());
         auto encode = tensorMapEncoder();
         for (int g = 0; g < 3; ++g) {
             if (!present_[g])
                 continue;
-            const int nf = vol.n[fast_[g]], ns = vol.n[slow_[g]], ng = vol.n[g];
-            padFast_[g] = (nf + 3) / 4 * 4;
-            ELSA_CUDA(cudaMalloc(&dLayouts_[g], sizeof(float) * padFast_[g] * ns * ng));
-            const cuuint64_t dims[3] = {static_cast<cuuint64_t>(nf), static_cast<cuuint64_t>(ns),
-                                        static_cast<cuuint64_t>(ng)};
-            const cuuint64_t strides[2] = {static_cast<cuuint64_t>(padFast_[g]) * 4,
-                                           static_cast<cuuint64_t>(padFast_[g]) * ns * 4};
-            const cuuint32_t box[3] = {BW, BH, BD};
-            const cuuint32_t estr[3] = {1, 1, 1};
-            const CUresult rc = encode(&maps_[g], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+            const int nf = vol_.n[fast_[g]], ns = vol_.n[slow_[g]], ng = vol_.n[g];
+            if (dLayouts_[g])
+                ELSA_CUDA(cudaFree(dLayouts_[g]));
+            dLayouts_[g] = nullptr;
+            ELSA_CUDA(cudaMalloc(&dLayouts_[g],
+                                 sizeof(float) * padFast_[g] * ns * ng * static_cast<size_t>(batch)));
+            const cuuint64_t dims[4] = {static_cast<cuuint64_t>(nf), static_cast<cuuint64_t>(ns),
+                                        static_cast<cuuint64_t>(ng),
+                                        static_cast<cuuint64_t>(batch)};
+            const cuuint64_t strides[3] = {static_cast<cuuint64_t>(padFast_[g]) * 4,
+                                           static_cast<cuuint64_t>(padFast_[g]) * ns * 4,
+                                           static_cast<cuuint64_t>(padFast_[g]) * ns * ng * 4};
+            const cuuint32_t box[4] = {BW, BH, BD, 1};
+            const cuuint32_t estr[4] = {1, 1, 1, 1};
+            const CUresult rc = encode(&maps_[g], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
                                        dLayouts_[g], dims, strides, box, estr,
                                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -493,9 +526,7 @@ namespace elsa_b200
             if (rc != CUDA_SUCCESS)
                 throw Error(ELSA_ERROR_CUDA, "cuTensorMapEncodeTiled failed");
         }
-        ELSA_CUDA(cudaFuncSetAttribute(forwardTmaKernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(NS * kStageBytes)));
+        batchCap_ = batch;
     }
 
     JosephForwardTma::~JosephForwardTma()
@@ -514,27 +545,39 @@ namespace elsa_b200
         forwardViews(x, y, 0, det_.np, s);
     }
 
-    void JosephForwardTma::prepare(const float* x, cudaStream_t s)
+    void JosephForwardTma::forwardBatch(const float* x, int64_t xStride, float* y,
+                                        int64_t yStride, int batch, cudaStream_t s)
+    {
+        if (batch <= 0)
+            return;
+        ensureBatch(batch);
+        prepare(x, s, batch, xStride);
+        forwardViews(x, y, 0, det_.np, s, batch, xStride, yStride);
+    }
+
+    void JosephForwardTma::prepare(const float* x, cudaStream_t s, int batch, int64_t xStride)
     {
         for (int g = 0; g < 3; ++g) {
             if (!present_[g])
                 continue;
-            permuteKernel<<<148 * 8, 256, 0, s>>>(x, vol_, g, slow_[g], fast_[g], padFast_[g],
-                                                  dLayouts_[g]);
+            permuteKernel<<<dim3(148 * 8, static_cast<unsigned>(batch)), 256, 0, s>>>(
+                x, vol_, g, slow_[g], fast_[g], padFast_[g], dLayouts_[g], xStride);
             ELSA_LAUNCH_CHECK("permuteKernel");
         }
     }
 
-    void JosephForwardTma::forwardViews(const float* x, float* y, int p0, int p1, cudaStream_t s)
+    void JosephForwardTma::forwardViews(const float* x, float* y, int p0, int p1, cudaStream_t s,
+                                        int batch, int64_t xStride, int64_t yStride)
     {
         const int64_t perView = static_cast<int64_t>(tilesU_) * tilesV_;
         const int64_t count = perView * (p1 - p0);
         if (count <= 0)
             return;
-        forwardTmaKernel<<<static_cast<unsigned>(count), NT, NS * kStageBytes, s>>>(
+        forwardTmaKernel<<<dim3(static_cast<unsigned>(count), static_cast<unsigned>(batch)), NT,
+                           NS * kStageBytes, s>>>(
             maps_[0], maps_[1], maps_[2], dRays_, dTiles_, dChunkOrigins_, maxChunks_, x, vol_,
             det_, tilesU_, tilesV_, make_int3(fast_[0], fast_[1], fast_[2]), y, dError_,
-            static_cast<int>(perView * p0), waitCycles_, withhold_ ? 1 : 0);
+            static_cast<int>(perView * p0), waitCycles_, withhold_ ? 1 : 0, xStride, yStride);
         ELSA_LAUNCH_CHECK("forwardTmaKernel");
     }
 

@@ -35,9 +35,13 @@ namespace elsa_b200
         JosephForwardTma& operator=(const JosephForwardTma&) = delete;
 
         void forward(const float* x, float* y, cudaStream_t s);
+        // batch volumes x + b xStride into sinograms y + b yStride, b < batch, in one launch
+        void forwardBatch(const float* x, int64_t xStride, float* y, int64_t yStride, int batch,
+                          cudaStream_t s);
         // forward() in two parts: the permuted copies of x, then the rays of views [p0, p1)
-        void prepare(const float* x, cudaStream_t s);
-        void forwardViews(const float* x, float* y, int p0, int p1, cudaStream_t s);
+        void prepare(const float* x, cudaStream_t s, int batch = 1, int64_t xStride = 0);
+        void forwardViews(const float* x, float* y, int p0, int p1, cudaStream_t s,
+                          int batch = 1, int64_t xStride = 0, int64_t yStride = 0);
         // Fraction of tiles that take the gather fallback, and the error word (0 = fine;
         // synchronizes).
         double fallbackFraction() const { return fallbackFraction_; }
@@ -72,5 +76,7 @@ namespace elsa_b200
         double fallbackFraction_ = 0.0;
         long long waitCycles_ = kDefaultWaitCycles;
         bool withhold_ = false;
+        int batchCap_ = 0; // volumes the permuted copies hold
+        void ensureBatch(int batch);
     };
 } // namespace elsa_b200

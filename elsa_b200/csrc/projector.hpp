@@ -66,6 +66,20 @@ namespace elsa_b200
         virtual ~Projector();
         virtual void forward(const float* x, float* y, cudaStream_t stream) = 0;
         virtual void adjoint(const float* y, float* x, cudaStream_t stream) = 0;
+        // `batch` applies on x + b xStride -> y + b yStride (adjoint: y + b yStride ->
+        // x + b xStride), each exactly as a single apply computes it; the default loops.
+        virtual void forwardBatch(const float* x, int64_t xStride, float* y, int64_t yStride,
+                                  int batch, cudaStream_t stream)
+        {
+            for (int b = 0; b < batch; ++b)
+                forward(x + b * xStride, y + b * yStride, stream);
+        }
+        virtual void adjointBatch(const float* y, int64_t yStride, float* x, int64_t xStride,
+                                  int batch, cudaStream_t stream)
+        {
+            for (int b = 0; b < batch; ++b)
+                adjoint(y + b * yStride, x + b * xStride, stream);
+        }
 
         int64_t domainSize() const { return domainSize_; }
         int64_t rangeSize() const { return rangeSize_; }

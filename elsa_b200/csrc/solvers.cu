@@ -194,6 +194,54 @@ namespace elsa_b200
         launchCgDirection(r, c, n, S, s);            // c = r + beta c
     }
 
+    SplitCgne::SplitCgne(Projector& A, float* x) : A_(A), x_(x), ws_(A.domainSize(), A.rangeSize())
+    {
+    }
+
+    void SplitCgne::backprojectData(const float* b, float* atb, cudaStream_t s)
+    {
+        A_.adjoint(b, atb, s);
+    }
+
+    void SplitCgne::begin(const float* atb, cudaStream_t s)
+    {
+        const int64_t n = A_.domainSize();
+        float* r = ws_.vol0.as<float>();
+        float* c = ws_.vol1.as<float>();
+        SolverScalars* S = ws_.scalars.as<SolverScalars>();
+        ELSA_CUDA(cudaMemsetAsync(S, 0, sizeof(SolverScalars), s));
+        launchFill(x_, 0.0f, n, s);
+        ELSA_CUDA(cudaMemcpyAsync(r, atb, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+        ELSA_CUDA(cudaMemcpyAsync(c, atb, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+        launchSquaredNorm(r, n, ws_.partials.as<double>(), &S->kold, s);
+    }
+
+    void SplitCgne::applyNormal(float* q, cudaStream_t s)
+    {
+        float* c = ws_.vol1.as<float>();
+        float* sino = ws_.sino0.as<float>();
+        A_.forward(c, sino, s);
+        A_.adjoint(sino, q, s);
+    }
+
+    void SplitCgne::update(const float* q, cudaStream_t s)
+    {
+        const int64_t n = A_.domainSize();
+        float* r = ws_.vol0.as<float>();
+        float* c = ws_.vol1.as<float>();
+        double* partials = ws_.partials.as<double>();
+        SolverScalars* S = ws_.scalars.as<SolverScalars>();
+        launchDot(c, q, n, partials, &S->den, s);     // <c, sum_r A_r^T A_r c>
+        launchCgStep(x_, r, c, q, n, S, partials, s); // x += a c, r -= a q, |r|^2 partials
+        launchCgFinishNorm(partials, S, s);           // k, beta = k/kold, kold = k
+        launchCgDirection(r, c, n, S, s);             // c = r + beta c
+    }
+
+    const double* SplitCgne::squaredResidualDevice() const
+    {
+        return &ws_.scalars.as<SolverScalars>()->kold;
+    }
+
     void cgneSolve(Projector& A, const float* b, float* x, int iterations, bool useX0,
                    SolverWorkspace& ws, cudaStream_t s)
     {

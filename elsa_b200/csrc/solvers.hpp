@@ -146,6 +146,29 @@ namespace elsa_b200
         void sqsIterate(int iterations, cudaStream_t s);
     };
 
+    // CGNE split around the reduction of its normal-operator results, for solves whose
+    // projector is spread over ranks by views (A = [A_0; A_1; ...], A^T A = sum_r A_r^T A_r):
+    // every rank computes its local A_r^T b and A_r^T A_r c into caller buffers, the caller sums
+    // them across the ranks in place (an all-reduce), and every rank then performs the same
+    // update, so all ranks hold identical x, r, c and scalars. Scalars stay in device memory; no
+    // call waits on the host. solvers/CGNE.cpp:20-78 with x0 = 0.
+    class SplitCgne
+    {
+    public:
+        SplitCgne(Projector& A, float* x);
+        void backprojectData(const float* b, float* atb, cudaStream_t s); // atb = A_r^T b_r
+        void begin(const float* atb, cudaStream_t s); // x = 0, r = c = atb (reduced), kold = |r|^2
+        void applyNormal(float* q, cudaStream_t s);   // q = A_r^T A_r c
+        void update(const float* q, cudaStream_t s);  // alpha, x, r, beta, c from the reduced q
+        const double* squaredResidualDevice() const;  // |r|^2 of the last update (device)
+        Projector& op() { return A_; }
+
+    private:
+        Projector& A_;
+        float* x_;
+        SolverWorkspace ws_;
+    };
+
     // Runs `iterations` iterations of every session, each as its CUDA graph, spread round-robin
     // over `streams` concurrent streams (the sessions must use distinct projectors and buffers);
     // returns when all have finished.

@@ -3,21 +3,23 @@
 Every rank holds the whole volume and the poses [lo, hi) of its block of views; A = [A_0; A_1; ...]
 stacks the ranks' projectors. CGNE (solvers/CGNE.cpp:20-78) works on volume-sized vectors only,
 so the one exchange per iteration is the sum A^T A c = sum_r A_r^T A_r c: an all-reduce of one
-volume (67 MB at 256^3, ~0.1 ms over NVLink against ~78 ms of projection). The right-hand side
-A^T b is all-reduced once. The all-reduce hands every rank the same sum, so the replicated vectors
-(x, r, c) and the scalars computed from them stay identical on all ranks without further
+volume (67 MB at 256^3, about 0.1 ms over NVLink against tens of ms of projection). The right-hand
+side A^T b is all-reduced once. The all-reduce hands every rank the same sum, so the replicated
+vectors (x, r, c) and the scalars computed from them stay identical on all ranks without further
 exchange.
 
-With the "nccl" backend the vectors are CUDA tensors and the projections and vector updates run
-the native kernels (C ABI); with "gloo" the same code runs on CPU tensors with caller-supplied
-projections (used by the tests).
+The iteration runs through a "split" CGNE whose two halves surround the all-reduce: with CUDA
+tensors NativeSplitCGNE (the C ABI's elsa_cgne_split_*: native projections and fused vector
+updates, scalars in device memory, no host synchronisation per iteration; the all-reduce is NCCL
+on the same stream), on CPU tensors TorchSplitCGNE (caller-supplied projections, used by the
+gloo tests).
 """
 import ctypes
 
 import numpy as np
 import torch
 
-__all__ = ["view_block", "NativeVectorOps", "TorchVectorOps", "ShardedCGNE"]
+__all__ = ["view_block", "TorchSplitCGNE", "NativeSplitCGNE", "ShardedCGNE", "native_split"]
 
 
 def view_block(num_views, rank, world):
@@ -31,103 +33,135 @@ def view_block(num_views, rank, world):
     return lo, lo + base + (1 if rank < extra else 0)
 
 
-class TorchVectorOps:
-    """Vector operations on torch tensors (CPU testing; float64 inner products)."""
+class TorchSplitCGNE:
+    """The split CGNE in torch operations around caller-supplied projections forward(x) -> local
+    sinogram block and adjoint(y) -> volume (any device; float64 scalars kept as tensors)."""
 
-    @staticmethod
-    def dot(a, b):
-        return float(torch.dot(a.double(), b.double()))
+    def __init__(self, forward, adjoint, domain_size, device="cpu"):
+        self.forward, self.adjoint = forward, adjoint
+        n = int(domain_size)
+        self.x = torch.zeros(n, dtype=torch.float32, device=device)
+        self.r = torch.zeros_like(self.x)
+        self.c = torch.zeros_like(self.x)
+        self.kold = torch.zeros((), dtype=torch.float64, device=device)
 
-    @staticmethod
-    def lincomb(a, x, b, y, out):
-        out.copy_((a * x + b * y).to(out.dtype))
+    def backproject(self, b, atb):
+        atb.copy_(self.adjoint(b))
+
+    def begin(self, atb):
+        self.x.zero_()
+        self.r.copy_(atb)
+        self.c.copy_(atb)
+        self.kold = torch.dot(self.r.double(), self.r.double())
+
+    def normal(self, q):
+        q.copy_(self.adjoint(self.forward(self.c)))
+
+    def update(self, q):
+        alpha = (self.kold / torch.dot(self.c.double(), q.double())).float()
+        self.x.add_(alpha * self.c)
+        self.r.sub_(alpha * q)
+        k = torch.dot(self.r.double(), self.r.double())
+        beta = (k / self.kold).float()
+        self.c.mul_(beta).add_(self.r)
+        self.kold = k
+
+    def residual(self):
+        return self.kold.clone()
 
 
-class NativeVectorOps:
-    """The C ABI's fused vector operations on CUDA tensors (float64 inner products)."""
+class NativeSplitCGNE:
+    """The split CGNE of the C ABI (elsa_cgne_split_*) on a rank's projector; x is a CUDA tensor
+    it owns. Every call is asynchronous on torch's current stream."""
 
-    def __init__(self):
+    def __init__(self, projector):
         from . import _capi
         self._capi = _capi
-        self._res = torch.empty(1, dtype=torch.float64, device="cuda")
+        self.projector = projector
+        self.x = torch.zeros(projector.domain_size, dtype=torch.float32, device="cuda")
+        h = ctypes.c_void_p()
+        _capi.call("elsa_cgne_split_create", projector.handle, ctypes.c_void_p(self.x.data_ptr()),
+                   ctypes.byref(h))
+        self._h = h
 
     def _stream(self):
         return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
-    def dot(self, a, b):
-        self._capi.call("elsa_dot", ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(b.data_ptr()),
-                        a.numel(), ctypes.c_void_p(self._res.data_ptr()), self._stream())
-        return float(self._res.item())
+    def backproject(self, b, atb):
+        self._capi.call("elsa_cgne_split_backproject", self._h, ctypes.c_void_p(b.data_ptr()),
+                        ctypes.c_void_p(atb.data_ptr()), self._stream())
 
-    def lincomb(self, a, x, b, y, out):
-        self._capi.call("elsa_lincomb", ctypes.c_float(a), ctypes.c_void_p(x.data_ptr()),
-                        ctypes.c_float(b), ctypes.c_void_p(y.data_ptr()),
-                        ctypes.c_void_p(out.data_ptr()), x.numel(), self._stream())
+    def begin(self, atb):
+        self._capi.call("elsa_cgne_split_begin", self._h, ctypes.c_void_p(atb.data_ptr()),
+                        self._stream())
+
+    def normal(self, q):
+        self._capi.call("elsa_cgne_split_normal", self._h, ctypes.c_void_p(q.data_ptr()),
+                        self._stream())
+
+    def update(self, q):
+        self._capi.call("elsa_cgne_split_update", self._h, ctypes.c_void_p(q.data_ptr()),
+                        self._stream())
+
+    def residual(self):
+        out = torch.empty((), dtype=torch.float64, device="cuda")
+        self._capi.call("elsa_cgne_split_residual", self._h, ctypes.c_void_p(out.data_ptr()),
+                        self._stream())
+        return out
+
+    def close(self):
+        if self._h:
+            self._capi.call("elsa_cgne_split_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class ShardedCGNE:
     """CGNE on A^T A x = A^T b with A split by views over the ranks of `group`.
 
-    forward(x) -> local sinogram block, adjoint(y) -> volume: this rank's projector (for the
-    native path: an elsa_b200.Projector built on the rank's poses, see `native_ops`).
-    b_local: this rank's block of measurements."""
+    split: this rank's split CGNE (NativeSplitCGNE on its block's projector, or TorchSplitCGNE);
+    b_local: this rank's block of measurements (a tensor on the split's device)."""
 
-    def __init__(self, forward, adjoint, b_local, domain_size, ops=None, group=None):
+    def __init__(self, split, b_local, group=None):
         import torch.distributed as dist
         self.dist = dist
         self.group = group
-        self.forward, self.adjoint = forward, adjoint
-        self.ops = ops or TorchVectorOps()
-        self.n = int(domain_size)
+        self.split = split
         self.b = b_local
 
-    def _normal(self, v):
-        q = self.adjoint(self.forward(v))
-        self.dist.all_reduce(q, group=self.group)  # sum over the view blocks
-        return q
+    def begin(self):
+        atb = torch.empty_like(self.split.x)
+        self.split.backproject(self.b, atb)
+        self.dist.all_reduce(atb, group=self.group)  # sum over the view blocks
+        self.split.begin(atb)
+        self._q = torch.empty_like(self.split.x)
 
-    def solve(self, iterations, x0=None):
-        like = self.b
-        x = torch.zeros(self.n, dtype=torch.float32, device=like.device) if x0 is None else \
-            x0.clone()
-        atb = self.adjoint(self.b)
-        self.dist.all_reduce(atb, group=self.group)
-        r = atb.clone()
-        if x0 is not None:
-            ata_x = self._normal(x)
-            self.ops.lincomb(1.0, r, -1.0, ata_x, r)
-        c = r.clone()
-        kold = self.ops.dot(r, r)
-        history = []
+    def iterate(self, iterations):
+        """Enqueue `iterations` iterations; returns the |r|^2 after each as a float64 tensor on
+        the split's device (no host synchronisation)."""
+        hist = []
         for _ in range(int(iterations)):
-            q = self._normal(c)
-            alpha = float(np.float32(kold / self.ops.dot(c, q)))
-            self.ops.lincomb(1.0, x, alpha, c, x)
-            self.ops.lincomb(1.0, r, -alpha, q, r)
-            k = self.ops.dot(r, r)
-            beta = float(np.float32(k / kold))
-            self.ops.lincomb(1.0, r, beta, c, c)
-            kold = k
-            history.append(k)
-        return x, history
+            self.split.normal(self._q)
+            self.dist.all_reduce(self._q, group=self.group)
+            self.split.update(self._q)
+            hist.append(self.split.residual())
+        return torch.stack(hist) if hist else torch.zeros(0, dtype=torch.float64)
+
+    def solve(self, iterations):
+        self.begin()
+        hist = self.iterate(iterations)
+        return self.split.x, [float(v) for v in hist.cpu()]
 
 
-def native_ops(kind, vol_dims, poses, det_dims, rank, world, params=None):
-    """(forward, adjoint, projector, (lo, hi)) for this rank's block of views, running the native
-    kernels on CUDA tensors."""
+def native_split(kind, vol_dims, poses, det_dims, rank, world, params=None):
+    """(NativeSplitCGNE, projector, (lo, hi)) for this rank's block of views."""
     from . import _capi
     lo, hi = view_block(len(poses), rank, world)
     det = list(det_dims[:-1]) + [hi - lo]
     proj = _capi.Projector(kind, vol_dims, det, np.ascontiguousarray(poses[lo:hi]), params)
-
-    def forward(x):
-        y = torch.empty(proj.range_size, dtype=torch.float32, device="cuda")
-        proj.apply_ptr(x.data_ptr(), y.data_ptr(), torch.cuda.current_stream().cuda_stream)
-        return y
-
-    def adjoint(y):
-        x = torch.empty(proj.domain_size, dtype=torch.float32, device="cuda")
-        proj.apply_adjoint_ptr(y.data_ptr(), x.data_ptr(), torch.cuda.current_stream().cuda_stream)
-        return x
-
-    return forward, adjoint, proj, (lo, hi)
+    return NativeSplitCGNE(proj), proj, (lo, hi)

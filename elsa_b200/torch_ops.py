@@ -30,11 +30,12 @@ def _run(op, inp, adjoint):
     flat = inp.contiguous().reshape(-1, n_in)
     out = torch.empty(flat.shape[0], n_out, dtype=torch.float32, device=inp.device)
     stream = torch.cuda.current_stream(inp.device).cuda_stream
-    for i in range(flat.shape[0]):
-        if adjoint:
-            op.apply_adjoint_ptr(flat[i].data_ptr(), out[i].data_ptr(), stream)
-        else:
-            op.apply_ptr(flat[i].data_ptr(), out[i].data_ptr(), stream)
+    # the whole batch in one call (one launch per kernel for the 3D Joseph operator)
+    if adjoint:
+        op.apply_adjoint_batch_ptr(flat.data_ptr(), n_in, out.data_ptr(), n_out,
+                                   flat.shape[0], stream)
+    else:
+        op.apply_batch_ptr(flat.data_ptr(), n_in, out.data_ptr(), n_out, flat.shape[0], stream)
     return out.reshape(*inp.shape[:-1], n_out)
 
 

@@ -84,6 +84,7 @@ typedef enum elsa_projector_kind {
 #define ELSA_FOOTPRINT_RECTANGLE 1
 
 typedef struct elsa_projector elsa_projector;
+typedef struct elsa_cgne_split elsa_cgne_split;
 
 /* Message of the last failed call on this thread ("" if none). */
 const char* elsa_last_error(void);
@@ -252,6 +253,21 @@ elsa_status elsa_projector_apply(elsa_projector* projector, const float* x, floa
 elsa_status elsa_projector_apply_adjoint(elsa_projector* projector, const float* y, float* x,
                                          void* stream);
 
+/* Batched applies on device buffers: for b < batch, y + b yStride = A (x + b xStride)
+ * (elsa_projector_apply_batch) or x + b xStride = A^T (y + b yStride)
+ * (elsa_projector_apply_adjoint_batch); strides in floats, at least the element sizes. Each
+ * element equals what the single-volume entry point computes, bit for bit. The 3D Joseph
+ * operator runs the whole batch in one launch per kernel, sharing its ray tables; the other
+ * operators apply the elements in turn. No reference counterpart: elsa applies one DataContainer
+ * at a time (LinearOperator::apply, core/LinearOperator.cpp:94-98); this serves batched
+ * (differentiable) reconstruction. Same concurrency rule as the single applies. */
+elsa_status elsa_projector_apply_batch(elsa_projector* projector, const float* x,
+                                       int64_t xStride, float* y, int64_t yStride, int32_t batch,
+                                       void* stream);
+elsa_status elsa_projector_apply_adjoint_batch(elsa_projector* projector, const float* y,
+                                               int64_t yStride, float* x, int64_t xStride,
+                                               int32_t batch, void* stream);
+
 /* Host-buffer variants, synchronous: copy the input to the device, run, copy the output back
  * (the call pattern of the reference's CUDA projectors, which copy in and out on every apply,
  * JosephsMethodCUDA.cpp:132-214). For the 3D Joseph operator (matched adjoint in view chunks)
@@ -348,6 +364,29 @@ typedef enum elsa_solver_kind {
      * Ordered subsets and a preconditioner: elsa_sqs_create. */
     ELSA_SOLVER_SQS = 7
 } elsa_solver_kind;
+
+/* CGNE split around the reduction of its normal-operator results (view-sharded solves over
+ * several GPUs, one process each; no reference counterpart: multi-GPU solves are a stated goal
+ * of elsa's roadmap, ROADMAP.md:48-50). With A = [A_0; A_1; ...] by blocks of views,
+ * A^T A = sum_r A_r^T A_r: every rank holds the whole volume and its block's projector
+ * (created on its poses), computes its local volumes into caller buffers, the caller sums them
+ * across the ranks in place (e.g. an NCCL all-reduce on the same stream), and every rank then
+ * performs the same update, so all ranks hold identical x and scalars. Per solve:
+ *   elsa_cgne_split_backproject(c, b_r, atb)  atb = A_r^T b_r;   all-reduce atb
+ *   elsa_cgne_split_begin(c, atb)             x = 0, r = d = atb, |r|^2
+ * per iteration:
+ *   elsa_cgne_split_normal(c, q)              q = A_r^T A_r d;   all-reduce q
+ *   elsa_cgne_split_update(c, q)              alpha, x, r, beta, d (solvers/CGNE.cpp:50-73)
+ * Scalars stay in device memory and no call waits on the host. elsa_cgne_split_residual copies
+ * the current |r|^2 (float64) to device memory `result`. x is the caller's volume buffer. */
+elsa_status elsa_cgne_split_create(elsa_projector* projector, float* x, elsa_cgne_split** out);
+elsa_status elsa_cgne_split_backproject(elsa_cgne_split* cgne, const float* b, float* atb,
+                                        void* stream);
+elsa_status elsa_cgne_split_begin(elsa_cgne_split* cgne, const float* atb, void* stream);
+elsa_status elsa_cgne_split_normal(elsa_cgne_split* cgne, float* q, void* stream);
+elsa_status elsa_cgne_split_update(elsa_cgne_split* cgne, const float* q, void* stream);
+elsa_status elsa_cgne_split_residual(const elsa_cgne_split* cgne, double* result, void* stream);
+elsa_status elsa_cgne_split_destroy(elsa_cgne_split* cgne);
 
 /* Set up a solver run: allocate its scratch, compute the initial residual (x is zeroed unless
  * use_x0 != 0). b (range) and x (domain) are device buffers that must stay valid until

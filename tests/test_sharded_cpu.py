@@ -28,7 +28,7 @@ def _problem():
 def _rank_main(rank, world, port, out_path):
     import torch
     import torch.distributed as dist
-    from elsa_b200.sharded import ShardedCGNE, view_block
+    from elsa_b200.sharded import ShardedCGNE, TorchSplitCGNE, view_block
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
@@ -46,7 +46,7 @@ def _rank_main(rank, world, port, out_path):
         def adj(y):
             return torch.from_numpy(O.joseph_adjoint(y.numpy(), vol, dloc, ploc))
 
-        solver = ShardedCGNE(fwd, adj, b_loc, int(np.prod(vol)))
+        solver = ShardedCGNE(TorchSplitCGNE(fwd, adj, int(np.prod(vol))), b_loc)
         x, hist = solver.solve(6)
         if rank == 0:
             np.savez(out_path, x=x.numpy(), hist=np.array(hist))
