@@ -89,7 +89,31 @@ def build(force=False, verbose=False):
                 sys.stderr.write(err)
     if force or jobs or _stale(LIB, objs):
         _compile([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
+    build_pyelsa(force)
     return LIB
+
+
+def build_pyelsa(force=False):
+    """The pybind11 module elsa_b200._pyelsa (csrc/pyelsa_ext.cpp over include/elsa_b200.hpp),
+    linked against libelsa_b200.so beside it. Skipped when pybind11 is not installed."""
+    try:
+        import pybind11
+    except ImportError:
+        return None
+    import sysconfig
+    src = os.path.join(CSRC, "pyelsa_ext.cpp")
+    out = os.path.join(HERE, "_pyelsa" + sysconfig.get_config_var("EXT_SUFFIX"))
+    deps = [src, LIB, os.path.join(ROOT, "include", "elsa_b200.hpp"),
+            os.path.join(ROOT, "include", "elsa_b200.h")]
+    if not force and not _stale(out, deps):
+        return out
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fvisibility=hidden",
+           "-I" + pybind11.get_include(), "-I" + sysconfig.get_paths()["include"],
+           "-I" + os.path.join(ROOT, "include"), "-I/usr/local/cuda/include", src,
+           "-o", out, "-L" + HERE, "-lelsa_b200", "-Wl,-rpath,$ORIGIN",
+           "-L/usr/local/cuda/lib64", "-lcudart"]
+    _compile(cmd)
+    return out
 
 
 if __name__ == "__main__":

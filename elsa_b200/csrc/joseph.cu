@@ -53,11 +53,11 @@
 #ifndef ELSA_AXIS_TD
 #define ELSA_AXIS_TD 8 // depth along the driving axis of the 3D adjoint's axis bricks
 #endif
-#ifndef ELSA_AXIS_TA
-#define ELSA_AXIS_TA 32 // edge along the first non-driving axis
+#ifndef ELSA_AXIS_TW
+#define ELSA_AXIS_TW 32 // edge along the non-driving axis over which a detector row's rays spread
 #endif
-#ifndef ELSA_AXIS_TB
-#define ELSA_AXIS_TB 16 // edge along the second non-driving axis
+#ifndef ELSA_AXIS_TV
+#define ELSA_AXIS_TV 16 // edge along the other non-driving axis
 #endif
 #ifndef ELSA_SPLAT_UNROLL
 #define ELSA_SPLAT_UNROLL 2 // unroll factor of the adjoint's per-sample loop (1: 72.8 ms, 2: 63.4 ms, 4: 68.9 ms at 256^3)
@@ -1261,21 +1261,34 @@ namespace elsa_b200
         // ---------------------------------------------------------------------------------------
         constexpr int kAxisHalo = 2;
 
-        template <int TD, int TA, int TB>
+        // Shared-memory brick of TD planes (along G) of TV rows x TW columns. Columns run along
+        // the non-driving axis over which the rays of a detector row spread (the warp's lanes
+        // spread along it, so stride 1 there keeps their taps in different banks), rows along the
+        // other one; both carry the halo.
+        template <int TD, int TW, int TV>
         struct AxisBrick {
-            static constexpr int kRow = TA + 2 * kAxisHalo;  // words per row along a (fastest)
-            static constexpr int kRows = TB + 2 * kAxisHalo; // rows along b
+            static constexpr int kRow = TW + 2 * kAxisHalo;  // words per row (stride 1 axis)
+            static constexpr int kRows = TV + 2 * kAxisHalo; // rows per plane
             static constexpr int kPlaneMin = kRow * kRows;
             // plane stride congruent to 1 modulo 32: lanes one plane apart use other banks
             static constexpr int kPlane = kPlaneMin + ((33 - kPlaneMin % 32) % 32);
             static constexpr int kWords = kPlane * TD;
-            static constexpr int kOrigin = kAxisHalo * kRow + kAxisHalo; // word of (a, b) = (0, 0)
+        };
+
+        // Axis roles of an axis brick: non-driving axes a < b of G; UB: the columns run along b
+        // (else along a). Edges and word strides along a and b.
+        template <int TD, bool UB, int TW, int TV>
+        struct AxisRolesAB {
+            using L = AxisBrick<TD, TW, TV>;
+            static constexpr int EA = UB ? TV : TW, EB = UB ? TW : TV;
+            static constexpr int SA = UB ? L::kRow : 1, SB = UB ? 1 : L::kRow;
+            static constexpr int kOrigin = kAxisHalo * (SA + SB); // word of (a, b) = (0, 0)
         };
 
         // Word of the bilinear footprint of position (pa, pb) on `plane` (the brick word of
         // a = b = 0 on that plane) and the reference's weights (JosephsMethod.cpp:37-52); tap
         // indices outside the brick are clamped into the halo.
-        template <int TA, int TB, int ROW>
+        template <int EA, int EB, int SA, int SB>
         __device__ __forceinline__ float* axisTap(float* plane, float pa, float pb, int orgA,
                                                   int orgB, float& wa, float& cwa, float& wb,
                                                   float& cwb)
@@ -1286,27 +1299,28 @@ namespace elsa_b200
             cwb = __fsub_rn(__fsub_rn(pb, fb), 0.5f);
             wa = __fsub_rn(1.0f, cwa);
             wb = __fsub_rn(1.0f, cwb);
-            const int la = min(max(static_cast<int>(fa) - orgA, -kAxisHalo), TA);
-            const int lb = min(max(static_cast<int>(fb) - orgB, -kAxisHalo), TB);
-            return plane + lb * ROW + la;
+            const int la = min(max(static_cast<int>(fa) - orgA, -kAxisHalo), EA);
+            const int lb = min(max(static_cast<int>(fb) - orgB, -kAxisHalo), EB);
+            return plane + la * SA + lb * SB;
         }
 
         // Samples jLo..jHi of ray R (position cp at sample jLo, on brick plane t0) into the brick.
         // Software-pipelined: the footprint of sample j+1 (always on another plane) is read before
         // the sums of sample j are written back.
-        template <int TD, int TA, int TB>
+        template <int TD, bool UB, int TW, int TV>
         __device__ __forceinline__ void axisSplat(float* acc, const JosephRay& R, float yl,
                                                   float2 cp, int jLo, int jHi, int t0, int orgA,
                                                   int orgB)
         {
-            using L = AxisBrick<TD, TA, TB>;
-            constexpr int ROW = L::kRow;
+            using L = AxisBrick<TD, TW, TV>;
+            using AR = AxisRolesAB<TD, UB, TW, TV>;
+            constexpr int SA = AR::SA, SB = AR::SB;
             const int dPlane = ((R.meta & 4) ? -1 : 1) * L::kPlane;
-            float* plane = acc + L::kOrigin + t0 * L::kPlane;
+            float* plane = acc + AR::kOrigin + t0 * L::kPlane;
             float pa = cp.x, pb = cp.y;
             float wa, cwa, wb, cwb;
-            float* q = axisTap<TA, TB, ROW>(plane, pa, pb, orgA, orgB, wa, cwa, wb, cwb);
-            float v0 = q[0], v1 = q[1], v2 = q[ROW], v3 = q[ROW + 1];
+            float* q = axisTap<AR::EA, AR::EB, SA, SB>(plane, pa, pb, orgA, orgB, wa, cwa, wb, cwb);
+            float v0 = q[0], v1 = q[SA], v2 = q[SB], v3 = q[SA + SB];
             float ya = yl * wa, yc = yl * cwa;
 #pragma unroll kSplatUnroll
             for (int j = jLo; j < jHi; ++j) {
@@ -1314,26 +1328,27 @@ namespace elsa_b200
                 pa = __fadd_rn(pa, R.sa);
                 pb = __fadd_rn(pb, R.sb);
                 float wa2, cwa2, wb2, cwb2;
-                float* q2 = axisTap<TA, TB, ROW>(plane, pa, pb, orgA, orgB, wa2, cwa2, wb2, cwb2);
-                const float n0 = q2[0], n1 = q2[1], n2 = q2[ROW], n3 = q2[ROW + 1];
+                float* q2 = axisTap<AR::EA, AR::EB, SA, SB>(plane, pa, pb, orgA, orgB, wa2, cwa2,
+                                                           wb2, cwb2);
+                const float n0 = q2[0], n1 = q2[SA], n2 = q2[SB], n3 = q2[SA + SB];
                 q[0] = v0 + ya * wb;
-                q[1] = v1 + yc * wb;
-                q[ROW] = v2 + ya * cwb;
-                q[ROW + 1] = v3 + yc * cwb;
+                q[SA] = v1 + yc * wb;
+                q[SB] = v2 + ya * cwb;
+                q[SA + SB] = v3 + yc * cwb;
                 q = q2;
                 v0 = n0, v1 = n1, v2 = n2, v3 = n3;
                 ya = yl * wa2, yc = yl * cwa2;
                 wb = wb2, cwb = cwb2;
             }
             q[0] = v0 + ya * wb;
-            q[1] = v1 + yc * wb;
-            q[ROW] = v2 + ya * cwb;
-            q[ROW + 1] = v3 + yc * cwb;
+            q[SA] = v1 + yc * wb;
+            q[SB] = v2 + ya * cwb;
+            q[SA + SB] = v3 + yc * cwb;
         }
 
         // One view for an axis brick of grid G: m x m ray classes separated by __syncwarp; lane i
         // takes class rays i, i + 32, ... (u fastest within the class grid).
-        template <int G, int TD, int TA, int TB, int CPD>
+        template <int G, int TD, bool UB, int TW, int TV, int CPD>
         __device__ __forceinline__ void axisView(float* acc, const RayWindow& w, int p, int m,
                                                  const JosephRay* __restrict__ rays,
                                                  const float2* __restrict__ cps, int64_t nrays,
@@ -1396,8 +1411,8 @@ namespace elsa_b200
                             }
                             const int dir = (R.meta & 4) ? -1 : 1;
                             const int t0 = R.k0 + jLo * dir - orgG;
-                            axisSplat<TD, TA, TB>(acc, R, yb[q] * R.len, cp, jLo, jHi, t0, orgA,
-                                                  orgB);
+                            axisSplat<TD, UB, TW, TV>(acc, R, yb[q] * R.len, cp, jLo, jHi, t0,
+                                                      orgA, orgB);
                         }
                     }
                     __syncwarp();
@@ -1406,16 +1421,16 @@ namespace elsa_b200
         }
 
         // Brick edges of grid G in volume axis order (x, y, z).
-        template <int G, int TD, int TA, int TB>
+        template <int G, int TD, bool UB, int TW, int TV>
         __host__ __device__ constexpr int axisBrickEdge(int axis)
         {
-            return axis == G ? TD : (axis == (G == 0 ? 1 : 0) ? TA : TB);
+            return axis == G ? TD : (axis == (G == 0 ? 1 : 0) ? (UB ? TV : TW) : (UB ? TW : TV));
         }
 
         // One warp per axis brick of grid G and per chunk entry (blockIdx.y): chunk entry e of
         // the grid covers views [chunks[e].x * per, ...) and writes its partial volume
         // chunks[e].y (or x itself when the adjoint has a single partial).
-        template <int G, int TD, int TA, int TB, int CPD>
+        template <int G, int TD, bool UB, int TW, int TV, int CPD>
         __global__ void __launch_bounds__(32, ELSA_ADJ_MIN_BLOCKS)
             josephAdjointAxisKernel(const JosephRay* __restrict__ rays,
                                     const float2* __restrict__ checkpoints, int64_t nrays,
@@ -1430,11 +1445,12 @@ namespace elsa_b200
             // blockIdx.z: batch element (sinogram y + b yStride, partial volumes out + b outStride)
             y += blockIdx.z * yStride;
             out += blockIdx.z * outStride;
-            using L = AxisBrick<TD, TA, TB>;
+            using L = AxisBrick<TD, TW, TV>;
+            using AR = AxisRolesAB<TD, UB, TW, TV>;
             __shared__ float acc[L::kWords];
-            constexpr int EX = axisBrickEdge<G, TD, TA, TB>(0);
-            constexpr int EY = axisBrickEdge<G, TD, TA, TB>(1);
-            constexpr int EZ = axisBrickEdge<G, TD, TA, TB>(2);
+            constexpr int EX = axisBrickEdge<G, TD, UB, TW, TV>(0);
+            constexpr int EY = axisBrickEdge<G, TD, UB, TW, TV>(1);
+            constexpr int EZ = axisBrickEdge<G, TD, UB, TW, TV>(2);
             const int lane = threadIdx.x;
             const int bi = blockIdx.x;
             const int org[3] = {(bi % nBricks.x) * EX, ((bi / nBricks.x) % nBricks.y) * EY,
@@ -1455,13 +1471,13 @@ namespace elsa_b200
                 const RayWindow w = windows[static_cast<int64_t>(p) * nb + bi];
                 if (w.u0 > w.u1 || w.v0 > w.v1)
                     continue;
-                axisView<G, TD, TA, TB, CPD>(acc, w, p, m, rays, checkpoints, nrays, y, det,
-                                             orgG, orgA, orgB);
+                axisView<G, TD, UB, TW, TV, CPD>(acc, w, p, m, rays, checkpoints, nrays, y, det,
+                                                 orgG, orgA, orgB);
             }
             __syncwarp();
             const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
             float* dst = out + static_cast<int64_t>(entry.y) * nvox;
-            for (int i = lane; i < TD * TA * TB; i += 32) {
+            for (int i = lane; i < TD * TW * TV; i += 32) {
                 // i runs x fastest over the brick's voxels
                 const int lx = i % EX, ly = (i / EX) % EY, lz = i / (EX * EY);
                 const int gx = org[0] + lx, gy = org[1] + ly, gz = org[2] + lz;
@@ -1469,7 +1485,7 @@ namespace elsa_b200
                     const int l[3] = {lx, ly, lz};
                     dst[gx + static_cast<int64_t>(vol.n[0]) *
                                  (gy + static_cast<int64_t>(vol.n[1]) * gz)] =
-                        acc[L::kOrigin + l[G] * L::kPlane + l[b] * L::kRow + l[a]];
+                        acc[AR::kOrigin + l[G] * L::kPlane + l[a] * AR::SA + l[b] * AR::SB];
                 }
             }
         }
@@ -2059,13 +2075,14 @@ namespace elsa_b200
             }
 
             // ---- 3D matched adjoint on axis bricks ----
-            static constexpr int kAxisTD = ELSA_AXIS_TD, kAxisTA = ELSA_AXIS_TA,
-                                 kAxisTB = ELSA_AXIS_TB;
+            static constexpr int kAxisTD = ELSA_AXIS_TD, kAxisTW = ELSA_AXIS_TW,
+                                 kAxisTV = ELSA_AXIS_TV;
             static constexpr int kAxisCheckpointDepth = 16;
             static_assert(kAxisCheckpointDepth % kAxisTD == 0,
                           "axis bricks are a whole fraction of a checkpoint slab deep");
             struct AxisGrid {
                 bool present = false;
+                bool ub = false;   // columns (the wide, stride-1 edge) along b instead of a
                 int3 edge{}, nb{}; // brick edges and brick counts in volume axis order
                 std::unique_ptr<DeviceBuffer> windows; // [view][brick]
                 int entryBegin = 0, entryEnd = 0;      // this grid's (chunk, partial) entries
@@ -2076,10 +2093,14 @@ namespace elsa_b200
             std::unique_ptr<DeviceBuffer> dEntries_;
             int axisPartials_ = 0;                      // partial volumes of the 3D adjoint
 
-            static int3 axisEdge(int g)
+            static int3 axisEdge(int g, bool ub)
             {
-                const int e[3] = {g == 0 ? kAxisTD : kAxisTA, g == 1 ? kAxisTD : (g == 0 ? kAxisTA : kAxisTB),
-                                  g == 2 ? kAxisTD : kAxisTB};
+                int a, b;
+                nonDrivingAxes(g, a, b);
+                int e[3];
+                e[g] = kAxisTD;
+                e[a] = ub ? kAxisTV : kAxisTW;
+                e[b] = ub ? kAxisTW : kAxisTV;
                 return make_int3(e[0], e[1], e[2]);
             }
 
@@ -2095,7 +2116,16 @@ namespace elsa_b200
                                             [g](unsigned a) { return (a >> g) & 1u; });
                     if (!G.present)
                         continue;
-                    G.edge = axisEdge(g);
+                    // columns along the axis over which a detector row's rays spread, by a vote
+                    // of the views driving along g (bit 4+g of a view's axis word: along b)
+                    int alongB = 0, votes = 0;
+                    for (unsigned w : viewAxesHost_)
+                        if ((w >> g) & 1u) {
+                            ++votes;
+                            alongB += (w >> (4 + g)) & 1u;
+                        }
+                    G.ub = 2 * alongB > votes;
+                    G.edge = axisEdge(g, G.ub);
                     G.nb = make_int3((vol_.n[0] + G.edge.x - 1) / G.edge.x,
                                      (vol_.n[1] + G.edge.y - 1) / G.edge.y,
                                      (vol_.n[2] + G.edge.z - 1) / G.edge.z);
@@ -2170,16 +2200,26 @@ namespace elsa_b200
                                     static_cast<unsigned>(e1 - e0), static_cast<unsigned>(batch));
                     const RayWindow* win = G.windows->as<RayWindow>();
                     const int2* ent = dEntries_->as<int2>();
-#define ELSA_AXIS_LAUNCH(G_)                                                                     \
-    josephAdjointAxisKernel<G_, kAxisTD, kAxisTA, kAxisTB, kAxisCheckpointDepth><<<grid, 32, 0, s>>>( \
-        dRays_, dCheckpoints_, rangeSize_, y, win, dViewAxes_, ent, e0, per, vol_, det_,          \
-        classSpacing_, G.nb, out, yStride, outStride)
-                    if (g == 0)
-                        ELSA_AXIS_LAUNCH(0);
-                    else if (g == 1)
-                        ELSA_AXIS_LAUNCH(1);
-                    else
-                        ELSA_AXIS_LAUNCH(2);
+#define ELSA_AXIS_LAUNCH(G_, UB_)                                                                \
+    josephAdjointAxisKernel<G_, kAxisTD, UB_, kAxisTW, kAxisTV, kAxisCheckpointDepth>             \
+        <<<grid, 32, 0, s>>>(dRays_, dCheckpoints_, rangeSize_, y, win, dViewAxes_, ent, e0, per,  \
+                             vol_, det_, classSpacing_, G.nb, out, yStride, outStride)
+                    if (g == 0) {
+                        if (G.ub)
+                            ELSA_AXIS_LAUNCH(0, true);
+                        else
+                            ELSA_AXIS_LAUNCH(0, false);
+                    } else if (g == 1) {
+                        if (G.ub)
+                            ELSA_AXIS_LAUNCH(1, true);
+                        else
+                            ELSA_AXIS_LAUNCH(1, false);
+                    } else {
+                        if (G.ub)
+                            ELSA_AXIS_LAUNCH(2, true);
+                        else
+                            ELSA_AXIS_LAUNCH(2, false);
+                    }
 #undef ELSA_AXIS_LAUNCH
                     ELSA_LAUNCH_CHECK("josephAdjointAxisKernel");
                 }
