@@ -434,13 +434,14 @@ def run_elsa(args):
     if rank == 0 and not args.no_parity:
         out["parity"] = parity_block(torch, proj, vol, poses, det, x_true)
     if rank == 0 and world == 1 and not args.no_batched:
-        out["batched"] = batched_vs_plain(torch, elsa_b200, phantoms)
-    if rank == 0 and world == 1 and args.batched_full:
-        # the full batched workload: 64 instances, edges {64, ..., 256}, 60-360 views, 50
-        # CG iterations each (several minutes; not part of the default run)
-        out["batched_full"] = batched_vs_plain(torch, elsa_b200, phantoms, instances=64,
-                                               iterations=50, edges=(64, 96, 128, 192, 256),
-                                               views=(60, 360))
+        # the batched workload: 64 seeded instances, edges {64, 96, 128, 192, 256}, 60-360
+        # views, detector 1.5 x edge, 50 CGNE iterations each (--batched-small: a reduced set)
+        if args.batched_small:
+            out["batched"] = batched_vs_plain(torch, elsa_b200, phantoms)
+        else:
+            out["batched"] = batched_vs_plain(torch, elsa_b200, phantoms, instances=64,
+                                              iterations=50, edges=(64, 96, 128, 192, 256),
+                                              views=(60, 360))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         gups, dt, cores = cpu_baseline_sample(args.cpu_views, vol, poses, det, x_true)
         out["cpu_baseline"] = {"value": round(gups, 5), "unit": "GUPS", "cores": cores,
@@ -470,6 +471,7 @@ def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, st
         specs.append((n, nv))
     t_plain = t_batch = 0.0
     waves = 0
+    per_edge = {}  # plain form: seconds spent on the instances of each volume edge
     i = 0
     while i < len(specs):
         problems = []
@@ -508,11 +510,17 @@ def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, st
         for sol in plain:  # warm-up of every kernel shape
             sol.iterate(1, s)
         torch.cuda.synchronize()
+        marks = [torch.cuda.Event(enable_timing=True) for _ in range(len(plain) + 1)]
         t0 = time.perf_counter()
-        for sol in plain:
+        marks[0].record()
+        for k, sol in enumerate(plain):
             sol.iterate(iterations, s)
+            marks[k + 1].record()
         torch.cuda.synchronize()
         t_plain += time.perf_counter() - t0
+        for k, (proj, _) in enumerate(problems):
+            edge = int(proj.vol_dims[0])
+            per_edge[edge] = per_edge.get(edge, 0.0) + marks[k].elapsed_time(marks[k + 1]) / 1e3
         for sol in plain:
             sol.close()
         del xs, plain
@@ -535,6 +543,9 @@ def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, st
             "plain_recon_per_s": round(instances / t_plain, 3),
             "batched_recon_per_s": round(instances / t_batch, 3),
             "speedup": round(t_plain / t_batch, 3),
+            "plain_seconds_by_edge": {str(k): round(v, 3) for k, v in sorted(per_edge.items())},
+            "instances_by_edge": {str(e): sum(1 for n, _ in specs if n == e)
+                                  for e in sorted(set(n for n, _ in specs))},
             "timing": "host wall clock around synchronized device work, graph capture included"}
 
 
@@ -650,9 +661,9 @@ def main():
                     help="skip the parity block (oracle check of the benchmarked operator)")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-vs-plain small-problem measurement")
-    ap.add_argument("--batched-full", action="store_true",
-                    help="also time the full batched workload (64 reconstructions of edges "
-                         "64-256, 60-360 views, 50 CG iterations each; several minutes)")
+    ap.add_argument("--batched-small", action="store_true",
+                    help="time the batched-vs-plain leg on a reduced set (12 instances of edges "
+                         "64-128, 60-180 views, 10 iterations) instead of the 64-instance one")
     ap.add_argument("--secondary", default=None,
                     help="time other projector workloads instead ('all' or a comma list of: %s)"
                          % ", ".join(SECONDARY))

@@ -177,12 +177,13 @@ namespace elsa_b200
                                                 const std::vector<PoseRecord>& poses,
                                                 const VoxelLut& lut, int support);
 
-    // Detector window of every (brick, view) for the brick-owner adjoints: the projection of the
-    // brick grown by one voxel, plus one pixel (joseph.cu). Windows are indexed view * nBricks +
-    // brick.
+    // Detector window of every (brick, view) for the brick-owner adjoints (joseph.cu). grow > 0
+    // (flat detectors): the pixels whose centres lie in the projection of the brick grown by
+    // `grow` voxels, plus `pixMargin` pixels; grow = 0 (and curved detectors): the projection of
+    // the brick grown by one voxel, plus one pixel. Windows are indexed view * nBricks + brick.
     void launchBrickWindows(const float* poses, const VolumeShape& vol, const DetectorShape& det,
                             int3 brick, int3 nBricks, RayWindow* out, cudaStream_t s,
-                            CurvedMap cm = {});
+                            CurvedMap cm = {}, float grow = 0.0f, float pixMargin = 0.0f);
 
     // x[v] = sum over c = 0 .. chunks-1 of partial[c * nvox + v], added in chunk order
     // (joseph.cu).

@@ -46,6 +46,8 @@ namespace elsa_b200
         constexpr int kMinAdjointChunks = 32;   // default floor of the view chunks
         constexpr int64_t kChunkMemory = int64_t(1) << 31; // default partial-volume budget
         constexpr int kSlab = 16; // brick edge = checkpoint slab depth
+        constexpr float kWindowSlack = 0.1f;       // voxels around a brick in its ray window
+        constexpr float kWindowPixelMargin = 0.05f; // pixels around the projected brick
         constexpr int kMinClass = 2;
         constexpr int kMaxClass = 8;
         constexpr int kActive = 256;
@@ -336,6 +338,69 @@ namespace elsa_b200
         }
 
         // Shared-memory brick of one warp (x stride 1, row stride 17, plane stride = 1 mod 32).
+        // Check of the brick windows (test support, elsa_projector_info key 8): every visited
+        // voxel must lie in a brick whose window for the ray's view contains the ray. Counts the
+        // visits that violate this.
+        template <int DIM>
+        __global__ void siddonWindowCheckKernel(const SiddonRay* __restrict__ rays,
+                                                const RayWindow* __restrict__ windows,
+                                                VolumeShape vol, DetectorShape det, int3 brick,
+                                                int3 nBricks, unsigned long long* __restrict__ misses)
+        {
+            const int64_t nrays = static_cast<int64_t>(det.nu) * det.nv * det.np;
+            const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (r >= nrays)
+                return;
+            const SiddonRay R = rays[r];
+            if (!(R.meta & kActive))
+                return;
+            const int u = static_cast<int>(r % det.nu);
+            const int v = static_cast<int>((r / det.nu) % det.nv);
+            const int p = static_cast<int>(r / (static_cast<int64_t>(det.nu) * det.nv));
+            const int nb = nBricks.x * nBricks.y * nBricks.z;
+            const int g = R.meta & 3;
+            int c0, c1, c2;
+            entryVoxel(g, R.kFirst, R.cur[0], R.cur[1], c0, c1, c2);
+            const int s0 = axisStep(R.meta, 0), s1 = axisStep(R.meta, 1), s2 = axisStep(R.meta, 2);
+            float T0 = R.T[0], T1 = R.T[1], T2 = R.T[2];
+            const int maxVisits = vol.n[0] + vol.n[1] + (DIM == 3 ? vol.n[2] : 0) + 3;
+            unsigned long long bad = 0;
+            int lastBrick = -1;
+            for (int it = 0; it < maxVisits; ++it) {
+                const int o0 = c0, o1 = c1, o2 = DIM == 3 ? c2 : 0; // the voxel of this visit
+                bool m0, m1, m2;
+                nextCrossing<DIM>(T0, T1, T2, m0, m1, m2);
+                if (m0) {
+                    c0 += s0;
+                    T0 = __fadd_rn(T0, R.tDelta[0]);
+                }
+                if (m1) {
+                    c1 += s1;
+                    T1 = __fadd_rn(T1, R.tDelta[1]);
+                }
+                if (m2) {
+                    c2 += s2;
+                    T2 = __fadd_rn(T2, R.tDelta[2]);
+                }
+                const int bi = o0 / brick.x + nBricks.x * (o1 / brick.y + nBricks.y * (o2 / brick.z));
+                if (bi != lastBrick) {
+                    const RayWindow w = windows[static_cast<int64_t>(p) * nb + bi];
+                    if (u < w.u0 || u > w.u1 || v < w.v0 || v > w.v1)
+                        ++bad;
+                    else
+                        lastBrick = bi;
+                }
+                const bool inside =
+                    static_cast<unsigned>(c0) < static_cast<unsigned>(vol.n[0]) &&
+                    static_cast<unsigned>(c1) < static_cast<unsigned>(vol.n[1]) &&
+                    (DIM < 3 || static_cast<unsigned>(c2) < static_cast<unsigned>(vol.n[2]));
+                if (!inside)
+                    break;
+            }
+            if (bad)
+                atomicAdd(misses, bad);
+        }
+
         template <int DIM>
         struct SiddonBrick {
             static constexpr int kBz = DIM == 3 ? kSlab : 1;
@@ -632,9 +697,36 @@ namespace elsa_b200
                     return 1;
                 case 7: // kernel launches per adjoint call (with view chunks: + the chunk sum)
                     return (!scatter_ && adjointChunks_ > 1) ? 2 : 1;
+                case 8: // visits outside the windows of their bricks (brick-owner adjoint only;
+                        // test support; synchronizes)
+                    return windowMisses();
                 default:
                     return -1;
                 }
+            }
+
+            int64_t windowMisses() const
+            {
+                if (!windows_)
+                    return -1;
+                DeviceBuffer count(sizeof(unsigned long long));
+                ELSA_CUDA(cudaMemset(count.as<unsigned long long>(), 0, sizeof(unsigned long long)));
+                const int64_t nrays = rangeSize_;
+                const unsigned blocks = static_cast<unsigned>((nrays + 255) / 256);
+                const int bz = vol_.dim == 3 ? kSlab : 1;
+                if (vol_.dim == 3)
+                    siddonWindowCheckKernel<3><<<blocks, 256>>>(
+                        rays_->as<SiddonRay>(), windows_->as<RayWindow>(), vol_, det_,
+                        make_int3(kSlab, kSlab, bz), nBricks_, count.as<unsigned long long>());
+                else
+                    siddonWindowCheckKernel<2><<<blocks, 256>>>(
+                        rays_->as<SiddonRay>(), windows_->as<RayWindow>(), vol_, det_,
+                        make_int3(kSlab, kSlab, bz), nBricks_, count.as<unsigned long long>());
+                ELSA_LAUNCH_CHECK("siddonWindowCheckKernel");
+                unsigned long long h = 0;
+                ELSA_CUDA(cudaMemcpy(&h, count.as<unsigned long long>(), sizeof(h),
+                                     cudaMemcpyDeviceToHost));
+                return static_cast<int64_t>(h);
             }
 
             std::vector<int> knobCandidates(int knob) const override
@@ -728,8 +820,11 @@ namespace elsa_b200
                     static_cast<int64_t>(nBricks_.x) * nBricks_.y * nBricks_.z * det_.np;
                 windows_ = std::make_unique<DeviceBuffer>(sizeof(RayWindow) * nwin);
                 CurvedTables tables(vol_.dim, det_, curved_);
+                // Siddon visits exactly the voxels a ray crosses: the window is the projection
+                // of the brick itself, grown by kWindowSlack for the rounding of the float rays
                 launchBrickWindows(dPoses_, vol_, det_, make_int3(kSlab, kSlab, bz), nBricks_,
-                                   windows_->as<RayWindow>(), nullptr, tables.map());
+                                   windows_->as<RayWindow>(), nullptr, tables.map(),
+                                   kWindowSlack, kWindowPixelMargin);
                 ELSA_CUDA(cudaDeviceSynchronize());
             }
 

@@ -90,6 +90,7 @@ def test_siddon_adjointness_and_determinism(cuda, oracle, name):
     assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
     # the brick-owner adjoint is bit-reproducible; the forward always is
     proj.set_knob(elsa_b200.KNOB_ADJOINT_SCATTER, 0)
+    assert proj.info(8) == 0  # every visit lies in a brick whose ray window holds its ray
     Ax1, Aty1 = _gpu_pair(cuda, proj, x, y)
     Ax2, Aty2 = _gpu_pair(cuda, proj, x, y)
     assert np.array_equal(Aty1.view(np.uint32), Aty2.view(np.uint32))
