@@ -457,8 +457,9 @@ def run_elsa(args):
 def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, streams=8,
                      seed=5, edges=(64, 96, 128), views=(60, 180), free_floor_gb=24.0):
     """Many independent reconstructions: one at a time (each solver's iterations enqueued on one
-    stream, one problem after the other) against elsa_solve_batch (every solver's iterations as
-    a CUDA graph, problems spread over concurrent streams). Seeded instances with volume edges
+    stream, one problem after the other) against the batched solver elsa_batch_cgne (one CUDA
+    graph for the whole batch; `batched_recon_per_s`), and against elsa_solve_batch (every
+    solver's iterations as its own CUDA graph, problems spread over concurrent streams). Seeded instances with volume edges
     drawn from `edges`, views uniform in `views`, a detector of 1.5 x edge and a modified
     Shepp-Logan phantom. Instances are built in waves that leave `free_floor_gb` of device
     memory free; each wave is timed both ways and the times are summed. Projector and solver
@@ -469,7 +470,7 @@ def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, st
         n = int(rng.choice(list(edges)))
         nv = int(rng.integers(views[0], views[1] + 1))
         specs.append((n, nv))
-    t_plain = t_batch = 0.0
+    t_plain = t_batch = t_graphs = 0.0
     waves = 0
     per_edge = {}  # plain form: seconds spent on the instances of each volume edge
     i = 0
@@ -528,12 +529,29 @@ def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, st
         elsa_b200.solve_batch(batch, 1, streams)  # captures the one-iteration graphs (warm-up)
         t0 = time.perf_counter()
         elsa_b200.solve_batch(batch, iterations, streams)  # captures + runs the timed graphs
-        t_batch += time.perf_counter() - t0
+        t_graphs += time.perf_counter() - t0
         for sol in batch:
             sol.close()
+        del xs2, batch
+        # the batched solver: forwards side by side, all adjoints in one launch per axis grid,
+        # batched vector updates, the whole iteration one CUDA graph
+        st = torch.cuda.Stream()
+        xs3 = [torch.zeros(p.domain_size, dtype=torch.float32, device="cuda")
+               for p, _ in problems]
+        with torch.cuda.stream(st):
+            bc = elsa_b200.BatchCGNE([p for p, _ in problems], [b.data_ptr() for _, b in problems],
+                                     [x.data_ptr() for x in xs3], st.cuda_stream)
+            bc.iterate_graph(1, st.cuda_stream)  # warm-up of every kernel shape
+        st.synchronize()
+        t0 = time.perf_counter()
+        with torch.cuda.stream(st):
+            bc.iterate_graph(iterations, st.cuda_stream)  # captures + runs the timed graph
+        st.synchronize()
+        t_batch += time.perf_counter() - t0
+        bc.close()
         for proj, _ in problems:
             proj.close()
-        del xs2, batch, problems
+        del xs3, problems
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
     return {"instances": instances, "iterations": iterations, "streams": streams,
@@ -543,6 +561,10 @@ def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, st
             "plain_recon_per_s": round(instances / t_plain, 3),
             "batched_recon_per_s": round(instances / t_batch, 3),
             "speedup": round(t_plain / t_batch, 3),
+            "batched_form": "elsa_batch_cgne: forwards side by side, all adjoints in one launch "
+                            "per axis grid over an instance table, batched vector updates, the "
+                            "iterations one CUDA graph",
+            "concurrent_graphs_recon_per_s": round(instances / t_graphs, 3),
             "plain_seconds_by_edge": {str(k): round(v, 3) for k, v in sorted(per_edge.items())},
             "instances_by_edge": {str(e): sum(1 for n, _ in specs if n == e)
                                   for e in sorted(set(n for n, _ in specs))},

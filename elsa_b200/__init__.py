@@ -6,7 +6,7 @@ a C ABI, include/elsa_b200.h). Importing this package does not need a GPU; calli
 does, and fails loudly when the library is missing.
 """
 from . import _capi  # noqa: F401
-from ._capi import (ElsaError, InvalidArgumentError, Projector, Solver,  # noqa: F401
+from ._capi import (ElsaError, InvalidArgumentError, Projector, Solver, BatchCGNE,  # noqa: F401
                     voxel_lut, PROJECTOR_BLOB, PROJECTOR_BSPLINE, PROJECTOR_PHASE_CONTRAST_BLOB,
                     PROJECTOR_PHASE_CONTRAST_BSPLINE, FOOTPRINT_REFERENCE, FOOTPRINT_RECTANGLE,
                     circle_trajectory, pose_2d, pose_3d, power_iterations, solve_batch, POSE_FLOATS,
@@ -21,7 +21,7 @@ from ._capi import (ElsaError, InvalidArgumentError, Projector, Solver,  # noqa:
                     edf_write, mhd_read, mhd_write, pgm_write, PROJECTOR_BINARY,
                     curved_detector_coords, PROJECTOR_RAY_BLOB, PROJECTOR_RAY_BSPLINE)
 
-__all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "voxel_lut",
+__all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "BatchCGNE", "voxel_lut",
            "PROJECTOR_BLOB", "PROJECTOR_BSPLINE", "PROJECTOR_PHASE_CONTRAST_BLOB",
            "PROJECTOR_PHASE_CONTRAST_BSPLINE", "FOOTPRINT_REFERENCE", "FOOTPRINT_RECTANGLE",
            "circle_trajectory",

@@ -85,6 +85,11 @@ SIGNATURES = {
     "elsa_projector_info": (_st, [_vp, _i32, ctypes.POINTER(_i64)]),
     "elsa_projector_wait_test": (_st, [_vp, _i64, _i32]),
     "elsa_projector_apply_batch": (_st, [_vp, _vp, _i64, _vp, _i64, _i32, _vp]),
+    "elsa_batch_cgne_create": (_st, [_vp, _vp, _vp, _i32, _vp, ctypes.POINTER(_vp)]),
+    "elsa_batch_cgne_iterate": (_st, [_vp, _i32, _vp]),
+    "elsa_batch_cgne_iterate_graph": (_st, [_vp, _i32, _vp]),
+    "elsa_batch_cgne_residuals": (_st, [_vp, _vp, _vp]),
+    "elsa_batch_cgne_destroy": (_st, [_vp]),
     "elsa_cgne_split_create": (_st, [_vp, _vp, ctypes.POINTER(_vp)]),
     "elsa_cgne_split_backproject": (_st, [_vp, _vp, _vp, _vp]),
     "elsa_cgne_split_begin": (_st, [_vp, _vp, _vp]),
@@ -486,6 +491,45 @@ def power_iterations(projector, iterations=5, stream=None):
     call("elsa_power_iterations", projector.handle, int(iterations), ctypes.c_void_p(stream or 0),
          ctypes.byref(v))
     return v.value
+
+
+class BatchCGNE:
+    """Owning handle of an elsa_batch_cgne: CGNE on many 3D Joseph operators advanced together
+    (x0 = 0); b_ptrs / x_ptrs are device buffers that must outlive the batch."""
+
+    def __init__(self, projectors, b_ptrs, x_ptrs, stream=None):
+        n = len(projectors)
+        self._keep = list(projectors)
+        ops = (ctypes.c_void_p * n)(*[p.handle.value for p in projectors])
+        bs = (ctypes.c_void_p * n)(*[int(v) for v in b_ptrs])
+        xs = (ctypes.c_void_p * n)(*[int(v) for v in x_ptrs])
+        h = ctypes.c_void_p()
+        call("elsa_batch_cgne_create", ops, bs, xs, n, ctypes.c_void_p(stream or 0),
+             ctypes.byref(h))
+        self._h = h
+        self.size = n
+
+    def iterate(self, iterations, stream=None):
+        call("elsa_batch_cgne_iterate", self._h, int(iterations), ctypes.c_void_p(stream or 0))
+
+    def iterate_graph(self, iterations, stream):
+        call("elsa_batch_cgne_iterate_graph", self._h, int(iterations), ctypes.c_void_p(stream))
+
+    def squared_residuals(self, stream=None):
+        out = np.zeros(self.size, np.float64)
+        call("elsa_batch_cgne_residuals", self._h, np_ptr(out), ctypes.c_void_p(stream or 0))
+        return out
+
+    def close(self):
+        if self._h:
+            call("elsa_batch_cgne_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Solver:

@@ -22,6 +22,11 @@ struct elsa_solver {
     int device = 0;
 };
 
+struct elsa_batch_cgne {
+    std::unique_ptr<elsa_b200::BatchedCgne> impl;
+    int device = 0;
+};
+
 struct elsa_cgne_split {
     std::unique_ptr<elsa_b200::SplitCgne> impl;
     int device = 0;
@@ -709,6 +714,82 @@ elsa_status elsa_cgne_solve(elsa_projector* p, const float* b, float* x, int32_t
         elsa_b200::SolverWorkspace ws(p->impl->domainSize(), p->impl->rangeSize());
         elsa_b200::cgneSolve(*p->impl, b, x, iterations, useX0 != 0, ws, asStream(stream));
         ELSA_CUDA(cudaStreamSynchronize(asStream(stream)));
+    });
+}
+
+elsa_status elsa_batch_cgne_create(elsa_projector* const* projectors, const float* const* b,
+                                   float* const* x, int32_t count, void* stream,
+                                   elsa_batch_cgne** out)
+{
+    return guarded([&] {
+        require(out != nullptr, "elsa_batch_cgne_create: null output handle");
+        *out = nullptr;
+        require(count > 0 && projectors && b && x, "elsa_batch_cgne_create: invalid argument");
+        std::vector<elsa_b200::Projector*> ops;
+        std::vector<const float*> bs;
+        std::vector<float*> xs;
+        for (int32_t i = 0; i < count; ++i) {
+            require(projectors[i] && b[i] && x[i], "elsa_batch_cgne_create: null instance");
+            require(projectors[i]->impl->device() == projectors[0]->impl->device(),
+                    "elsa_batch_cgne_create: all projectors must be on one device");
+            ops.push_back(projectors[i]->impl.get());
+            bs.push_back(b[i]);
+            xs.push_back(x[i]);
+        }
+        onDevice(projectors[0]);
+        auto h = std::make_unique<elsa_batch_cgne>();
+        h->device = projectors[0]->impl->device();
+        h->impl = std::make_unique<elsa_b200::BatchedCgne>(ops, bs, xs, asStream(stream));
+        *out = h.release();
+    });
+}
+
+namespace
+{
+    void onBatchDevice(const elsa_batch_cgne* h)
+    {
+        int cur = 0;
+        ELSA_CUDA(cudaGetDevice(&cur));
+        if (cur != h->device)
+            ELSA_CUDA(cudaSetDevice(h->device));
+    }
+} // namespace
+
+elsa_status elsa_batch_cgne_iterate(elsa_batch_cgne* h, int32_t iterations, void* stream)
+{
+    return guarded([&] {
+        require(h && iterations >= 0, "elsa_batch_cgne_iterate: invalid argument");
+        onBatchDevice(h);
+        h->impl->iterate(iterations, asStream(stream));
+    });
+}
+
+elsa_status elsa_batch_cgne_iterate_graph(elsa_batch_cgne* h, int32_t iterations, void* stream)
+{
+    return guarded([&] {
+        require(h && iterations >= 0, "elsa_batch_cgne_iterate_graph: invalid argument");
+        onBatchDevice(h);
+        h->impl->iterateGraph(iterations, asStream(stream));
+    });
+}
+
+elsa_status elsa_batch_cgne_residuals(elsa_batch_cgne* h, double* out, void* stream)
+{
+    return guarded([&] {
+        require(h && out, "elsa_batch_cgne_residuals: null argument");
+        onBatchDevice(h);
+        h->impl->squaredResiduals(out, asStream(stream));
+    });
+}
+
+elsa_status elsa_batch_cgne_destroy(elsa_batch_cgne* h)
+{
+    return guarded([&] {
+        if (h) {
+            onBatchDevice(h);
+            ELSA_CUDA(cudaDeviceSynchronize()); // nothing in flight uses the workspaces
+        }
+        delete h;
     });
 }
 

@@ -906,6 +906,25 @@ namespace elsa_b200
             x[v] = s;
         }
 
+        // sumChunksKernel for many volumes: blockIdx.y selects (partials, count, nvox, out)
+        struct SumChunksEntry {
+            const float* partial;
+            int chunks;
+            int64_t nvox;
+            float* x;
+        };
+        __global__ void sumChunksManyKernel(const SumChunksEntry* __restrict__ e)
+        {
+            const SumChunksEntry E = e[blockIdx.y];
+            for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+                 v < E.nvox; v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+                float s = E.partial[v];
+                for (int c = 1; c < E.chunks; ++c)
+                    s = s + E.partial[c * E.nvox + v];
+                E.x[v] = s;
+            }
+        }
+
 #ifndef ELSA_ADJ2D_CTAS_PER_SM
 #define ELSA_ADJ2D_CTAS_PER_SM 16
 #endif
@@ -1259,15 +1278,23 @@ namespace elsa_b200
         // the 16^3 warp kernel does. Across the rays the brick keeps a halo of two voxels on every
         // side: tap indices are clamped into it instead of tested, and the halo is not written out.
         // ---------------------------------------------------------------------------------------
-        constexpr int kAxisHalo = 2;
+#ifndef ELSA_AXIS_HALO
+#define ELSA_AXIS_HALO 2 // halo of the axis bricks (0: no halo, taps outside are predicated off)
+#endif
+        constexpr int kAxisHalo = ELSA_AXIS_HALO;
+        static_assert(kAxisHalo == 0 || kAxisHalo == 2, "halo of 0 or 2 voxels");
 
         // Shared-memory brick of TD planes (along G) of TV rows x TW columns. Columns run along
         // the non-driving axis over which the rays of a detector row spread (the warp's lanes
         // spread along it, so stride 1 there keeps their taps in different banks), rows along the
         // other one; both carry the halo.
+#ifndef ELSA_AXIS_ROWPAD
+#define ELSA_AXIS_ROWPAD (ELSA_AXIS_HALO == 0 ? 1 : 0) // extra words per row (bank spread)
+#endif
         template <int TD, int TW, int TV>
         struct AxisBrick {
-            static constexpr int kRow = TW + 2 * kAxisHalo;  // words per row (stride 1 axis)
+            // words per row (stride 1 axis)
+            static constexpr int kRow = TW + 2 * kAxisHalo + ELSA_AXIS_ROWPAD;
             static constexpr int kRows = TV + 2 * kAxisHalo; // rows per plane
             static constexpr int kPlaneMin = kRow * kRows;
             // plane stride congruent to 1 modulo 32: lanes one plane apart use other banks
@@ -1304,6 +1331,29 @@ namespace elsa_b200
             return plane + la * SA + lb * SB;
         }
 
+        // Without a halo: the word offset of the footprint on its plane and a mask of the taps
+        // inside the brick (bit t: tap (a + (t & 1), b + (t >> 1))).
+        template <int EA, int EB, int SA, int SB>
+        __device__ __forceinline__ int axisTapMasked(float pa, float pb, int orgA, int orgB,
+                                                     float& wa, float& cwa, float& wb, float& cwb,
+                                                     unsigned& mask)
+        {
+            const float fa = floorf(__fsub_rn(pa, 0.5f));
+            const float fb = floorf(__fsub_rn(pb, 0.5f));
+            cwa = __fsub_rn(__fsub_rn(pa, fa), 0.5f);
+            cwb = __fsub_rn(__fsub_rn(pb, fb), 0.5f);
+            wa = __fsub_rn(1.0f, cwa);
+            wb = __fsub_rn(1.0f, cwb);
+            const int la = static_cast<int>(fa) - orgA, lb = static_cast<int>(fb) - orgB;
+            const bool a0 = static_cast<unsigned>(la) < static_cast<unsigned>(EA);
+            const bool a1 = static_cast<unsigned>(la + 1) < static_cast<unsigned>(EA);
+            const bool b0 = static_cast<unsigned>(lb) < static_cast<unsigned>(EB);
+            const bool b1 = static_cast<unsigned>(lb + 1) < static_cast<unsigned>(EB);
+            mask = (a0 && b0 ? 1u : 0u) | (a1 && b0 ? 2u : 0u) | (a0 && b1 ? 4u : 0u) |
+                   (a1 && b1 ? 8u : 0u);
+            return la * SA + lb * SB;
+        }
+
         // Samples jLo..jHi of ray R (position cp at sample jLo, on brick plane t0) into the brick.
         // Software-pipelined: the footprint of sample j+1 (always on another plane) is read before
         // the sums of sample j are written back.
@@ -1315,6 +1365,53 @@ namespace elsa_b200
             using L = AxisBrick<TD, TW, TV>;
             using AR = AxisRolesAB<TD, UB, TW, TV>;
             constexpr int SA = AR::SA, SB = AR::SB;
+            if constexpr (kAxisHalo == 0) {
+                const int dPlane = ((R.meta & 4) ? -1 : 1) * L::kPlane;
+                int plane = t0 * L::kPlane;
+                float pa = cp.x, pb = cp.y;
+                float wa, cwa, wb, cwb;
+                unsigned mk;
+                int o = plane + axisTapMasked<AR::EA, AR::EB, SA, SB>(pa, pb, orgA, orgB, wa, cwa,
+                                                                       wb, cwb, mk);
+                float v0 = (mk & 1u) ? acc[o] : 0.0f, v1 = (mk & 2u) ? acc[o + SA] : 0.0f;
+                float v2 = (mk & 4u) ? acc[o + SB] : 0.0f, v3 = (mk & 8u) ? acc[o + SA + SB] : 0.0f;
+                float ya = yl * wa, yc = yl * cwa;
+#pragma unroll kSplatUnroll
+                for (int j = jLo; j < jHi; ++j) {
+                    plane += dPlane;
+                    pa = __fadd_rn(pa, R.sa);
+                    pb = __fadd_rn(pb, R.sb);
+                    float wa2, cwa2, wb2, cwb2;
+                    unsigned mk2;
+                    const int o2 = plane + axisTapMasked<AR::EA, AR::EB, SA, SB>(
+                                               pa, pb, orgA, orgB, wa2, cwa2, wb2, cwb2, mk2);
+                    const float n0 = (mk2 & 1u) ? acc[o2] : 0.0f;
+                    const float n1 = (mk2 & 2u) ? acc[o2 + SA] : 0.0f;
+                    const float n2 = (mk2 & 4u) ? acc[o2 + SB] : 0.0f;
+                    const float n3 = (mk2 & 8u) ? acc[o2 + SA + SB] : 0.0f;
+                    if (mk & 1u)
+                        acc[o] = v0 + ya * wb;
+                    if (mk & 2u)
+                        acc[o + SA] = v1 + yc * wb;
+                    if (mk & 4u)
+                        acc[o + SB] = v2 + ya * cwb;
+                    if (mk & 8u)
+                        acc[o + SA + SB] = v3 + yc * cwb;
+                    o = o2, mk = mk2;
+                    v0 = n0, v1 = n1, v2 = n2, v3 = n3;
+                    ya = yl * wa2, yc = yl * cwa2;
+                    wb = wb2, cwb = cwb2;
+                }
+                if (mk & 1u)
+                    acc[o] = v0 + ya * wb;
+                if (mk & 2u)
+                    acc[o + SA] = v1 + yc * wb;
+                if (mk & 4u)
+                    acc[o + SB] = v2 + ya * cwb;
+                if (mk & 8u)
+                    acc[o + SA + SB] = v3 + yc * cwb;
+                return;
+            }
             const int dPlane = ((R.meta & 4) ? -1 : 1) * L::kPlane;
             float* plane = acc + AR::kOrigin + t0 * L::kPlane;
             float pa = cp.x, pb = cp.y;
@@ -1427,32 +1524,45 @@ namespace elsa_b200
             return axis == G ? TD : (axis == (G == 0 ? 1 : 0) ? (UB ? TV : TW) : (UB ? TW : TV));
         }
 
-        // One warp per axis brick of grid G and per chunk entry (blockIdx.y): chunk entry e of
-        // the grid covers views [chunks[e].x * per, ...) and writes its partial volume
-        // chunks[e].y (or x itself when the adjoint has a single partial).
+        // Shape of the axis bricks (depth along the driving axis, columns, rows) and the
+        // checkpoint slab depth of the 3D operator.
+        constexpr int kAxisTD = ELSA_AXIS_TD, kAxisTW = ELSA_AXIS_TW, kAxisTV = ELSA_AXIS_TV;
+        constexpr int kAxisCheckpointDepth = 16;
+        static_assert(kAxisCheckpointDepth % kAxisTD == 0,
+                      "axis bricks are a whole fraction of a checkpoint slab deep");
+
+        // What one axis-brick adjoint launch works on: the operator's tables, the sinogram y,
+        // the grid's windows and (chunk, partial volume) entries, and where partial volumes go.
+        struct AxisJob {
+            const JosephRay* rays;
+            const float2* checkpoints;
+            int64_t nrays;
+            const float* y;
+            const RayWindow* windows; // this grid's windows, [view][brick]
+            const unsigned* viewAxes;
+            const int2* chunks; // this grid's entries (chunk, partial volume)
+            int entries;
+            int viewsPerChunk;
+            VolumeShape vol;
+            DetectorShape det;
+            int m;
+            int3 nBricks;
+            float* out;       // partial volume k at out + k * nvox (x itself for one partial)
+            int64_t itemBase; // batched launches: first block of this job
+        };
+
+        // One warp: brick bi of grid G, chunk entry e (views [chunks[e].x * per, ...)), written
+        // to the entry's partial volume.
         template <int G, int TD, bool UB, int TW, int TV, int CPD>
-        __global__ void __launch_bounds__(32, ELSA_ADJ_MIN_BLOCKS)
-            josephAdjointAxisKernel(const JosephRay* __restrict__ rays,
-                                    const float2* __restrict__ checkpoints, int64_t nrays,
-                                    const float* __restrict__ y,
-                                    const RayWindow* __restrict__ windows,
-                                    const unsigned* __restrict__ viewAxes,
-                                    const int2* __restrict__ chunks, int entryBase,
-                                    int viewsPerChunk, VolumeShape vol, DetectorShape det, int m,
-                                    int3 nBricks, float* __restrict__ out, int64_t yStride,
-                                    int64_t outStride)
+        __device__ __forceinline__ void axisBrickWork(const AxisJob& J, int bi, int e, float* acc)
         {
-            // blockIdx.z: batch element (sinogram y + b yStride, partial volumes out + b outStride)
-            y += blockIdx.z * yStride;
-            out += blockIdx.z * outStride;
             using L = AxisBrick<TD, TW, TV>;
             using AR = AxisRolesAB<TD, UB, TW, TV>;
-            __shared__ float acc[L::kWords];
             constexpr int EX = axisBrickEdge<G, TD, UB, TW, TV>(0);
             constexpr int EY = axisBrickEdge<G, TD, UB, TW, TV>(1);
             constexpr int EZ = axisBrickEdge<G, TD, UB, TW, TV>(2);
             const int lane = threadIdx.x;
-            const int bi = blockIdx.x;
+            const int3 nBricks = J.nBricks;
             const int org[3] = {(bi % nBricks.x) * EX, ((bi / nBricks.x) % nBricks.y) * EY,
                                 (bi / (nBricks.x * nBricks.y)) * EZ};
             int a, b;
@@ -1462,21 +1572,22 @@ namespace elsa_b200
             for (int i = lane; i < L::kWords; i += 32)
                 acc[i] = 0.0f;
             __syncwarp();
-            const int2 entry = chunks[entryBase + blockIdx.y];
-            const int pBegin = entry.x * viewsPerChunk;
-            const int pEnd = min(det.np, pBegin + viewsPerChunk);
+            const int2 entry = J.chunks[e];
+            const int pBegin = entry.x * J.viewsPerChunk;
+            const int pEnd = min(J.det.np, pBegin + J.viewsPerChunk);
             for (int p = pBegin; p < pEnd; ++p) {
-                if (!(viewAxes[p] & (1u << G)))
+                if (!(J.viewAxes[p] & (1u << G)))
                     continue;
-                const RayWindow w = windows[static_cast<int64_t>(p) * nb + bi];
+                const RayWindow w = J.windows[static_cast<int64_t>(p) * nb + bi];
                 if (w.u0 > w.u1 || w.v0 > w.v1)
                     continue;
-                axisView<G, TD, UB, TW, TV, CPD>(acc, w, p, m, rays, checkpoints, nrays, y, det,
-                                                 orgG, orgA, orgB);
+                axisView<G, TD, UB, TW, TV, CPD>(acc, w, p, J.m, J.rays, J.checkpoints, J.nrays,
+                                                 J.y, J.det, orgG, orgA, orgB);
             }
             __syncwarp();
+            const VolumeShape& vol = J.vol;
             const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
-            float* dst = out + static_cast<int64_t>(entry.y) * nvox;
+            float* dst = J.out + static_cast<int64_t>(entry.y) * nvox;
             for (int i = lane; i < TD * TW * TV; i += 32) {
                 // i runs x fastest over the brick's voxels
                 const int lx = i % EX, ly = (i / EX) % EY, lz = i / (EX * EY);
@@ -1488,6 +1599,43 @@ namespace elsa_b200
                         acc[AR::kOrigin + l[G] * L::kPlane + l[a] * AR::SA + l[b] * AR::SB];
                 }
             }
+        }
+
+        // One warp per axis brick of grid G (blockIdx.x) and chunk entry (entryBase +
+        // blockIdx.y); blockIdx.z: batch element (sinogram y + b yStride, partial volumes
+        // out + b outStride).
+        template <int G, int TD, bool UB, int TW, int TV, int CPD>
+        __global__ void __launch_bounds__(32, ELSA_ADJ_MIN_BLOCKS)
+            josephAdjointAxisKernel(AxisJob J, int entryBase, int64_t yStride, int64_t outStride)
+        {
+            __shared__ float acc[AxisBrick<TD, TW, TV>::kWords];
+            J.y += blockIdx.z * yStride;
+            J.out += blockIdx.z * outStride;
+            axisBrickWork<G, TD, UB, TW, TV, CPD>(J, blockIdx.x, entryBase + blockIdx.y, acc);
+        }
+
+        // Many operators in one launch (batched solves): block k belongs to the job whose
+        // [itemBase, itemBase + bricks x entries) holds k; within it, brick k % bricks and entry
+        // k / bricks, exactly the work of that operator's own launch.
+        template <int G, int TD, bool UB, int TW, int TV, int CPD>
+        __global__ void __launch_bounds__(32, ELSA_ADJ_MIN_BLOCKS)
+            josephAdjointAxisManyKernel(const AxisJob* __restrict__ jobs, int njobs)
+        {
+            __shared__ float acc[AxisBrick<TD, TW, TV>::kWords];
+            const int64_t k = blockIdx.x;
+            int lo = 0, hi = njobs - 1; // last job with itemBase <= k
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (jobs[mid].itemBase <= k)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            const AxisJob J = jobs[lo];
+            const int nb = J.nBricks.x * J.nBricks.y * J.nBricks.z;
+            const int64_t local = k - J.itemBase;
+            axisBrickWork<G, TD, UB, TW, TV, CPD>(J, static_cast<int>(local % nb),
+                                                  static_cast<int>(local / nb), acc);
         }
 
         using Adjoint3d = WarpAdjointConfig<16, 16, ELSA_ADJ_BZ, 16>;
@@ -2075,11 +2223,7 @@ namespace elsa_b200
             }
 
             // ---- 3D matched adjoint on axis bricks ----
-            static constexpr int kAxisTD = ELSA_AXIS_TD, kAxisTW = ELSA_AXIS_TW,
-                                 kAxisTV = ELSA_AXIS_TV;
-            static constexpr int kAxisCheckpointDepth = 16;
-            static_assert(kAxisCheckpointDepth % kAxisTD == 0,
-                          "axis bricks are a whole fraction of a checkpoint slab deep");
+
             struct AxisGrid {
                 bool present = false;
                 bool ub = false;   // columns (the wide, stride-1 edge) along b instead of a
@@ -2176,6 +2320,53 @@ namespace elsa_b200
                 return next;
             }
 
+        public:
+            // This operator's share of a batched adjoint (planJosephAdjointMany): its axis-brick
+            // jobs keyed by (grid, column axis), and its chunk sum (chunks <= 1: none).
+            bool batchable() const
+            {
+                return vol_.dim == 3 && !fast_ && !scatter_ && dCheckpoints_ != nullptr;
+            }
+            void appendAxisJobs(const float* y, float* x, std::vector<AxisJob> (&jobs)[6],
+                                std::vector<SumChunksEntry>& sums) const
+            {
+                float* out = axisPartials_ > 1 ? partial_->as<float>() : x;
+                for (int g = 0; g < 3; ++g) {
+                    const AxisGrid& G = grids_[g];
+                    if (!G.present || G.entryEnd <= G.entryBegin)
+                        continue;
+                    jobs[2 * g + (G.ub ? 1 : 0)].push_back(axisJob(g, y, out));
+                }
+                if (axisPartials_ > 1)
+                    sums.push_back(SumChunksEntry{partial_->as<float>(), axisPartials_,
+                                                  domainSize_, x});
+            }
+
+        private:
+            // The axis-brick job of grid g on sinogram y into out (entries indexed from the grid's
+            // first entry; itemBase left to batched callers).
+            AxisJob axisJob(int g, const float* y, float* out) const
+            {
+                const AxisGrid& G = grids_[g];
+                AxisJob J{};
+                J.rays = dRays_;
+                J.checkpoints = dCheckpoints_;
+                J.nrays = rangeSize_;
+                J.y = y;
+                J.windows = G.windows->as<RayWindow>();
+                J.viewAxes = dViewAxes_;
+                J.chunks = dEntries_->as<int2>() + G.entryBegin;
+                J.entries = G.entryEnd - G.entryBegin;
+                J.viewsPerChunk = (det_.np + adjointChunks_ - 1) / adjointChunks_;
+                J.vol = vol_;
+                J.det = det_;
+                J.m = classSpacing_;
+                J.nBricks = G.nb;
+                J.out = out;
+                J.itemBase = 0;
+                return J;
+            }
+
             // The axis-brick kernels for view chunks [c0, c1), writing their partial volumes into
             // out (x itself when there is a single partial volume); `batch` sinograms
             // y + b yStride into out + b outStride.
@@ -2198,12 +2389,10 @@ namespace elsa_b200
                         continue;
                     const dim3 grid(static_cast<unsigned>(G.nb.x * G.nb.y * G.nb.z),
                                     static_cast<unsigned>(e1 - e0), static_cast<unsigned>(batch));
-                    const RayWindow* win = G.windows->as<RayWindow>();
-                    const int2* ent = dEntries_->as<int2>();
+                    const AxisJob J = axisJob(g, y, out);
 #define ELSA_AXIS_LAUNCH(G_, UB_)                                                                \
     josephAdjointAxisKernel<G_, kAxisTD, UB_, kAxisTW, kAxisTV, kAxisCheckpointDepth>             \
-        <<<grid, 32, 0, s>>>(dRays_, dCheckpoints_, rangeSize_, y, win, dViewAxes_, ent, e0, per,  \
-                             vol_, det_, classSpacing_, G.nb, out, yStride, outStride)
+        <<<grid, 32, 0, s>>>(J, e0 - G.entryBegin, yStride, outStride)
                     if (g == 0) {
                         if (G.ub)
                             ELSA_AXIS_LAUNCH(0, true);
@@ -2249,6 +2438,91 @@ namespace elsa_b200
         sumChunksKernel<<<static_cast<unsigned>((nvox + 255) / 256), 256, 0, s>>>(partial, chunks,
                                                                                   nvox, x);
         ELSA_LAUNCH_CHECK("sumChunksKernel");
+    }
+
+    class AdjointManyPlan
+    {
+    public:
+        std::unique_ptr<DeviceBuffer> jobs[6]; // per (grid, column axis)
+        int64_t items[6] = {0, 0, 0, 0, 0, 0};
+        int counts[6] = {0, 0, 0, 0, 0, 0};
+        std::unique_ptr<DeviceBuffer> sums;
+        int sumCount = 0;
+        int64_t maxVox = 0;
+    };
+
+    std::shared_ptr<AdjointManyPlan> planJosephAdjointMany(const std::vector<Projector*>& ops,
+                                                           const std::vector<const float*>& ys,
+                                                           const std::vector<float*>& xs)
+    {
+        if (ops.size() != ys.size() || ops.size() != xs.size())
+            throw Error(ELSA_ERROR_INVALID_ARGUMENT, "planJosephAdjointMany: size mismatch");
+        std::vector<AxisJob> jobs[6];
+        std::vector<SumChunksEntry> sums;
+        auto plan = std::make_shared<AdjointManyPlan>();
+        for (size_t i = 0; i < ops.size(); ++i) {
+            const auto* J = dynamic_cast<const JosephProjector*>(ops[i]);
+            if (!J || !J->batchable())
+                throw Error(ELSA_ERROR_NOT_SUPPORTED,
+                            "batched adjoints take 3D Joseph operators with the matched "
+                            "brick-owner adjoint only");
+            J->appendAxisJobs(ys[i], xs[i], jobs, sums);
+            plan->maxVox = std::max(plan->maxVox, J->domainSize());
+        }
+        for (int k = 0; k < 6; ++k) {
+            int64_t base = 0;
+            for (AxisJob& j : jobs[k]) {
+                j.itemBase = base;
+                base += static_cast<int64_t>(j.nBricks.x) * j.nBricks.y * j.nBricks.z * j.entries;
+            }
+            if (base >= (int64_t(1) << 31))
+                throw Error(ELSA_ERROR_NOT_SUPPORTED, "planJosephAdjointMany: too many bricks");
+            plan->items[k] = base;
+            plan->counts[k] = static_cast<int>(jobs[k].size());
+            if (!jobs[k].empty()) {
+                plan->jobs[k] = std::make_unique<DeviceBuffer>(sizeof(AxisJob) * jobs[k].size());
+                ELSA_CUDA(cudaMemcpy(plan->jobs[k]->as<AxisJob>(), jobs[k].data(),
+                                     sizeof(AxisJob) * jobs[k].size(), cudaMemcpyHostToDevice));
+            }
+        }
+        plan->sumCount = static_cast<int>(sums.size());
+        if (!sums.empty()) {
+            plan->sums = std::make_unique<DeviceBuffer>(sizeof(SumChunksEntry) * sums.size());
+            ELSA_CUDA(cudaMemcpy(plan->sums->as<SumChunksEntry>(), sums.data(),
+                                 sizeof(SumChunksEntry) * sums.size(), cudaMemcpyHostToDevice));
+        }
+        return plan;
+    }
+
+    void runJosephAdjointMany(const AdjointManyPlan& plan, cudaStream_t s)
+    {
+        constexpr int TD = kAxisTD, TW = kAxisTW, TV = kAxisTV, CPD = kAxisCheckpointDepth;
+        for (int k = 0; k < 6; ++k) {
+            if (plan.items[k] == 0)
+                continue;
+            const unsigned grid = static_cast<unsigned>(plan.items[k]);
+            const AxisJob* jobs = plan.jobs[k]->as<AxisJob>();
+            const int n = plan.counts[k];
+#define ELSA_AXIS_MANY(G_, UB_)                                                                   \
+    josephAdjointAxisManyKernel<G_, TD, UB_, TW, TV, CPD><<<grid, 32, 0, s>>>(jobs, n)
+            switch (k) {
+            case 0: ELSA_AXIS_MANY(0, false); break;
+            case 1: ELSA_AXIS_MANY(0, true); break;
+            case 2: ELSA_AXIS_MANY(1, false); break;
+            case 3: ELSA_AXIS_MANY(1, true); break;
+            case 4: ELSA_AXIS_MANY(2, false); break;
+            default: ELSA_AXIS_MANY(2, true); break;
+            }
+#undef ELSA_AXIS_MANY
+            ELSA_LAUNCH_CHECK("josephAdjointAxisManyKernel");
+        }
+        if (plan.sumCount > 0) {
+            const int64_t blocks = std::min<int64_t>((plan.maxVox + 255) / 256, 148 * 8);
+            sumChunksManyKernel<<<dim3(static_cast<unsigned>(blocks),
+                                       static_cast<unsigned>(plan.sumCount)),
+                                  256, 0, s>>>(plan.sums->as<SumChunksEntry>());
+            ELSA_LAUNCH_CHECK("sumChunksManyKernel");
+        }
     }
 
     std::unique_ptr<Projector> makeJosephProjector(const VolumeShape& vol,

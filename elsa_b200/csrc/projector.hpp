@@ -185,6 +185,17 @@ namespace elsa_b200
                             int3 brick, int3 nBricks, RayWindow* out, cudaStream_t s,
                             CurvedMap cm = {}, float grow = 0.0f, float pixMargin = 0.0f);
 
+    // Matched 3D Joseph adjoints of many projectors in one launch per driving-axis grid (batched
+    // solves): plan once for fixed sinogram and volume buffers, then run on a stream. Every
+    // projector's result equals its own adjoint() bit for bit (same bricks, view chunks and
+    // summation order). Throws ELSA_ERROR_NOT_SUPPORTED unless every projector is a 3D matched
+    // Joseph operator with its brick-owner adjoint.
+    class AdjointManyPlan;
+    std::shared_ptr<AdjointManyPlan> planJosephAdjointMany(const std::vector<Projector*>& ops,
+                                                           const std::vector<const float*>& ys,
+                                                           const std::vector<float*>& xs);
+    void runJosephAdjointMany(const AdjointManyPlan& plan, cudaStream_t s);
+
     // x[v] = sum over c = 0 .. chunks-1 of partial[c * nvox + v], added in chunk order
     // (joseph.cu).
     void launchSumChunks(const float* partial, int chunks, int64_t nvox, float* x,

@@ -697,6 +697,132 @@ namespace elsa_b200
         ELSA_CUDA(cudaGraphLaunch(graph_, s));
     }
 
+    BatchedCgne::BatchedCgne(std::vector<Projector*> ops, std::vector<const float*> b,
+                             std::vector<float*> x, cudaStream_t s)
+        : ops_(std::move(ops)), x_(std::move(x))
+    {
+        const size_t n = ops_.size();
+        if (n == 0 || b.size() != n || x_.size() != n)
+            throw Error(ELSA_ERROR_INVALID_ARGUMENT, "BatchedCgne: invalid instance lists");
+        scalars_ = std::make_unique<DeviceBuffer>(sizeof(SolverScalars) * n);
+        ELSA_CUDA(cudaMemsetAsync(scalars_->as<SolverScalars>(), 0, sizeof(SolverScalars) * n, s));
+        std::vector<const float*> sinos;
+        std::vector<float*> qs;
+        std::vector<CgBatchEntry> entries(n);
+        for (size_t i = 0; i < n; ++i) {
+            Projector& A = *ops_[i];
+            const int64_t dn = A.domainSize();
+            maxN_ = std::max(maxN_, dn);
+            r_.push_back(std::make_unique<DeviceBuffer>(sizeof(float) * dn));
+            c_.push_back(std::make_unique<DeviceBuffer>(sizeof(float) * dn));
+            q_.push_back(std::make_unique<DeviceBuffer>(sizeof(float) * dn));
+            sino_.push_back(std::make_unique<DeviceBuffer>(sizeof(float) * A.rangeSize()));
+            partials_.push_back(std::make_unique<DeviceBuffer>(sizeof(double) * kReduceBlocks));
+            sinos.push_back(sino_.back()->as<float>());
+            qs.push_back(q_.back()->as<float>());
+            SolverScalars* S = scalars_->as<SolverScalars>() + i;
+            entries[i] = CgBatchEntry{x_[i], r_[i]->as<float>(), c_[i]->as<float>(),
+                                      q_[i]->as<float>(), dn, S, partials_[i]->as<double>()};
+        }
+        plan_ = planJosephAdjointMany(ops_, sinos, qs); // checks that every operator qualifies
+        entries_ = std::make_unique<DeviceBuffer>(sizeof(CgBatchEntry) * n);
+        ELSA_CUDA(cudaMemcpy(entries_->as<CgBatchEntry>(), entries.data(),
+                             sizeof(CgBatchEntry) * n, cudaMemcpyHostToDevice));
+        // the begin of cgneBegin (x0 = 0): r = A^T b, x = 0, c = r, kold = |r|^2
+        for (size_t i = 0; i < n; ++i) {
+            const int64_t dn = ops_[i]->domainSize();
+            float* r = r_[i]->as<float>();
+            ops_[i]->adjoint(b[i], r, s);
+            launchFill(x_[i], 0.0f, dn, s);
+            ELSA_CUDA(cudaMemcpyAsync(c_[i]->as<float>(), r, sizeof(float) * dn,
+                                      cudaMemcpyDeviceToDevice, s));
+            launchSquaredNorm(r, dn, partials_[i]->as<double>(),
+                              &(scalars_->as<SolverScalars>() + i)->kold, s);
+        }
+        for (int k = 0; k < kSideStreams; ++k) {
+            ELSA_CUDA(cudaStreamCreateWithFlags(&side_[k], cudaStreamNonBlocking));
+            ELSA_CUDA(cudaEventCreateWithFlags(&join_[k], cudaEventDisableTiming));
+        }
+        ELSA_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+    }
+
+    BatchedCgne::~BatchedCgne()
+    {
+        if (graph_)
+            cudaGraphExecDestroy(graph_);
+        for (int k = 0; k < kSideStreams; ++k) {
+            if (side_[k]) {
+                cudaStreamSynchronize(side_[k]);
+                cudaStreamDestroy(side_[k]);
+            }
+            if (join_[k])
+                cudaEventDestroy(join_[k]);
+        }
+        if (fork_)
+            cudaEventDestroy(fork_);
+    }
+
+    void BatchedCgne::step(cudaStream_t s)
+    {
+        // forwards: instance i on side stream i mod kSideStreams, joined before the adjoints
+        ELSA_CUDA(cudaEventRecord(fork_, s));
+        for (int k = 0; k < kSideStreams; ++k)
+            ELSA_CUDA(cudaStreamWaitEvent(side_[k], fork_, 0));
+        for (size_t i = 0; i < ops_.size(); ++i)
+            ops_[i]->forward(c_[i]->as<float>(), sino_[i]->as<float>(), side_[i % kSideStreams]);
+        for (int k = 0; k < kSideStreams; ++k) {
+            ELSA_CUDA(cudaEventRecord(join_[k], side_[k]));
+            ELSA_CUDA(cudaStreamWaitEvent(s, join_[k], 0));
+        }
+        runJosephAdjointMany(*plan_, s); // q_i = A_i^T A_i c_i
+        launchCgneUpdateBatch(entries_->as<CgBatchEntry>(), size(), maxN_, s);
+    }
+
+    void BatchedCgne::iterate(int iterations, cudaStream_t s)
+    {
+        for (int it = 0; it < iterations; ++it)
+            step(s);
+    }
+
+    void BatchedCgne::iterateGraph(int iterations, cudaStream_t s)
+    {
+        if (s == nullptr || s == cudaStreamLegacy)
+            throw Error(ELSA_ERROR_INVALID_ARGUMENT,
+                        "batched solver graphs need an explicitly created stream");
+        if (!graph_ || graphIterations_ != iterations) {
+            if (graph_) {
+                ELSA_CUDA(cudaGraphExecDestroy(graph_));
+                graph_ = nullptr;
+            }
+            cudaGraph_t g = nullptr;
+            ELSA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            try {
+                iterate(iterations, s);
+            } catch (...) {
+                cudaStreamEndCapture(s, &g);
+                if (g)
+                    cudaGraphDestroy(g);
+                throw;
+            }
+            ELSA_CUDA(cudaStreamEndCapture(s, &g));
+            const cudaError_t e = cudaGraphInstantiate(&graph_, g, 0);
+            cudaGraphDestroy(g);
+            ELSA_CUDA(e);
+            graphIterations_ = iterations;
+        }
+        ELSA_CUDA(cudaGraphLaunch(graph_, s));
+    }
+
+    void BatchedCgne::squaredResiduals(double* out, cudaStream_t s)
+    {
+        std::vector<SolverScalars> h(ops_.size());
+        ELSA_CUDA(cudaMemcpyAsync(h.data(), scalars_->as<SolverScalars>(),
+                                  sizeof(SolverScalars) * h.size(), cudaMemcpyDeviceToHost, s));
+        ELSA_CUDA(cudaStreamSynchronize(s));
+        for (size_t i = 0; i < h.size(); ++i)
+            out[i] = h[i].kold;
+    }
+
     void solveBatch(SolverSession* const* sessions, int n, int iterations, int streams)
     {
         if (n < 0 || iterations < 0 || streams < 1 || streams > 64)

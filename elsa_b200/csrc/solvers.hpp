@@ -169,6 +169,39 @@ namespace elsa_b200
         SolverWorkspace ws_;
     };
 
+    // Many CGNE solves (x0 = 0) on 3D Joseph operators advanced together: per iteration every
+    // operator's forward (fanned out over side streams), then all matched adjoints in one launch
+    // per driving-axis grid (planJosephAdjointMany), then all vector updates in five launches
+    // (launchCgneUpdateBatch). Every instance's iterates equal those of its own SolverSession
+    // bit for bit. iterateGraph captures the batched iterations as one CUDA graph.
+    class BatchedCgne
+    {
+    public:
+        BatchedCgne(std::vector<Projector*> ops, std::vector<const float*> b,
+                    std::vector<float*> x, cudaStream_t s);
+        ~BatchedCgne();
+        BatchedCgne(const BatchedCgne&) = delete;
+        BatchedCgne& operator=(const BatchedCgne&) = delete;
+        void iterate(int iterations, cudaStream_t s);
+        void iterateGraph(int iterations, cudaStream_t s);
+        void squaredResiduals(double* out, cudaStream_t s); // |r|^2 per instance; synchronizes
+        int size() const { return static_cast<int>(ops_.size()); }
+
+    private:
+        static constexpr int kSideStreams = 4;
+        std::vector<Projector*> ops_;
+        std::vector<float*> x_;
+        std::vector<std::unique_ptr<DeviceBuffer>> r_, c_, q_, sino_, partials_;
+        std::unique_ptr<DeviceBuffer> scalars_, entries_;
+        std::shared_ptr<AdjointManyPlan> plan_;
+        int64_t maxN_ = 0;
+        cudaStream_t side_[kSideStreams] = {};
+        cudaEvent_t fork_ = nullptr, join_[kSideStreams] = {};
+        cudaGraphExec_t graph_ = nullptr;
+        int graphIterations_ = -1;
+        void step(cudaStream_t s);
+    };
+
     // Runs `iterations` iterations of every session, each as its CUDA graph, spread round-robin
     // over `streams` concurrent streams (the sessions must use distinct projectors and buffers);
     // returns when all have finished.

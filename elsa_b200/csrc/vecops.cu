@@ -31,9 +31,22 @@ namespace elsa_b200
         // Each thread handles float4 chunks i = tid, tid + T, ... (T = total threads), plus a
         // scalar tail; fixed assignment -> fixed summation order.
         template <bool kSquare>
+        __device__ __forceinline__ void partialDot(const float* __restrict__ x,
+                                                   const float* __restrict__ y, int64_t n,
+                                                   double* __restrict__ partials);
+
+        template <bool kSquare>
         __global__ void __launch_bounds__(kReduceThreads)
             partialDotKernel(const float* __restrict__ x, const float* __restrict__ y, int64_t n,
                              double* __restrict__ partials)
+        {
+            partialDot<kSquare>(x, y, n, partials);
+        }
+
+        template <bool kSquare>
+        __device__ __forceinline__ void partialDot(const float* __restrict__ x,
+                                                   const float* __restrict__ y, int64_t n,
+                                                   double* __restrict__ partials)
         {
             const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
             const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
@@ -116,10 +129,25 @@ namespace elsa_b200
                 x[i] *= v;
         }
 
+        __device__ __forceinline__ void cgStep(float* __restrict__ x, float* __restrict__ r,
+                                               const float* __restrict__ c,
+                                               const float* __restrict__ q, int64_t n,
+                                               const SolverScalars* S,
+                                               double* __restrict__ partials);
+
         __global__ void __launch_bounds__(kReduceThreads)
             cgStepKernel(float* __restrict__ x, float* __restrict__ r, const float* __restrict__ c,
                          const float* __restrict__ q, int64_t n, const SolverScalars* S,
                          double* __restrict__ partials)
+        {
+            cgStep(x, r, c, q, n, S, partials);
+        }
+
+        __device__ __forceinline__ void cgStep(float* __restrict__ x, float* __restrict__ r,
+                                               const float* __restrict__ c,
+                                               const float* __restrict__ q, int64_t n,
+                                               const SolverScalars* S,
+                                               double* __restrict__ partials)
         {
             const float alpha = static_cast<float>(S->kold / S->den);
             const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -163,6 +191,53 @@ namespace elsa_b200
             const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
             for (int64_t i = tid; i < n; i += T)
                 c[i] = r[i] + beta * c[i];
+        }
+
+        // batched CGNE update: blockIdx.y selects the instance, blockIdx.x is the block of
+        // the single-instance launch
+        __global__ void __launch_bounds__(kReduceThreads)
+            dotManyKernel(const CgBatchEntry* __restrict__ e)
+        {
+            const CgBatchEntry E = e[blockIdx.y];
+            partialDot<false>(E.c, E.q, E.n, E.partials);
+        }
+
+        __global__ void __launch_bounds__(kReduceThreads)
+            finishDenManyKernel(const CgBatchEntry* __restrict__ e)
+        {
+            const CgBatchEntry E = e[blockIdx.y];
+            const double s = sumPartials(E.partials);
+            if (threadIdx.x == 0)
+                E.S->den = s;
+        }
+
+        __global__ void __launch_bounds__(kReduceThreads)
+            cgStepManyKernel(const CgBatchEntry* __restrict__ e)
+        {
+            const CgBatchEntry E = e[blockIdx.y];
+            cgStep(E.x, E.r, E.c, E.q, E.n, E.S, E.partials);
+        }
+
+        __global__ void __launch_bounds__(kReduceThreads)
+            cgFinishNormManyKernel(const CgBatchEntry* __restrict__ e)
+        {
+            const CgBatchEntry E = e[blockIdx.y];
+            const double s = sumPartials(E.partials);
+            if (threadIdx.x == 0) {
+                E.S->k = s;
+                E.S->beta = s / E.S->kold;
+                E.S->kold = s;
+            }
+        }
+
+        __global__ void cgDirectionManyKernel(const CgBatchEntry* __restrict__ e)
+        {
+            const CgBatchEntry E = e[blockIdx.y];
+            const float beta = static_cast<float>(E.S->beta);
+            const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            const int64_t T = static_cast<int64_t>(gridDim.x) * blockDim.x;
+            for (int64_t i = tid; i < E.n; i += T)
+                E.c[i] = E.r[i] + beta * E.c[i];
         }
 
         unsigned gridFor(int64_t n)
@@ -238,6 +313,20 @@ namespace elsa_b200
     {
         cgDirectionKernel<<<gridFor(n), 256, 0, s>>>(r, c, n, S);
         ELSA_LAUNCH_CHECK("cgDirection");
+    }
+
+    void launchCgneUpdateBatch(const CgBatchEntry* entries, int count, int64_t maxN,
+                               cudaStream_t s)
+    {
+        if (count <= 0)
+            return;
+        const unsigned nb = static_cast<unsigned>(count);
+        dotManyKernel<<<dim3(kReduceBlocks, nb), kReduceThreads, 0, s>>>(entries);
+        finishDenManyKernel<<<dim3(1, nb), kReduceThreads, 0, s>>>(entries);
+        cgStepManyKernel<<<dim3(kReduceBlocks, nb), kReduceThreads, 0, s>>>(entries);
+        cgFinishNormManyKernel<<<dim3(1, nb), kReduceThreads, 0, s>>>(entries);
+        cgDirectionManyKernel<<<dim3(gridFor(maxN), nb), 256, 0, s>>>(entries);
+        ELSA_LAUNCH_CHECK("cgneUpdateBatch");
     }
 } // namespace elsa_b200
 

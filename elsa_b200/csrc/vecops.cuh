@@ -37,6 +37,25 @@ namespace elsa_b200
         float lo, hi, sigma;
     };
 
+    // One CG instance of a batched solve: x, r, c (direction), q (normal-operator result), the
+    // element count, its scalars and its kReduceBlocks partial sums.
+    struct CgBatchEntry {
+        float* x;
+        float* r;
+        float* c;
+        const float* q;
+        int64_t n;
+        SolverScalars* S;
+        double* partials;
+    };
+
+    // The CGNE update (dot <c, q> -> den, step, norm, direction) of `count` instances in five
+    // launches; every instance runs the blocks and summation order of the single-instance
+    // launches (launchDot, launchCgStep, launchCgFinishNorm, launchCgDirection), so its results
+    // are bit-identical to theirs. entries: device array; maxN: largest n.
+    void launchCgneUpdateBatch(const CgBatchEntry* entries, int count, int64_t maxN,
+                               cudaStream_t s);
+
     // partials: device buffer of kReduceBlocks doubles.
     void launchDot(const float* x, const float* y, int64_t n, double* partials, double* result,
                    cudaStream_t s);

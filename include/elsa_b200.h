@@ -85,6 +85,7 @@ typedef enum elsa_projector_kind {
 
 typedef struct elsa_projector elsa_projector;
 typedef struct elsa_cgne_split elsa_cgne_split;
+typedef struct elsa_batch_cgne elsa_batch_cgne;
 
 /* Message of the last failed call on this thread ("" if none). */
 const char* elsa_last_error(void);
@@ -364,6 +365,25 @@ typedef enum elsa_solver_kind {
      * Ordered subsets and a preconditioner: elsa_sqs_create. */
     ELSA_SOLVER_SQS = 7
 } elsa_solver_kind;
+
+/* Many CGNE solves advanced together (a batch of reconstructions of uneven size; no reference
+ * counterpart: elsa solves one problem at a time, CGNE.cpp:20-78 per DataContainer). Instance i
+ * solves A_i^T A_i x_i = A_i^T b_i from x_i = 0 with its own operator (a 3D Joseph projector
+ * with the matched adjoint; others return ELSA_ERROR_NOT_SUPPORTED), b_i and x_i device
+ * buffers. Per iteration the instances' forwards run concurrently, all adjoints run in one
+ * launch per driving-axis grid over an instance table, and all vector updates in five launches;
+ * every x_i equals what a single elsa_solver session computes, bit for bit.
+ * elsa_batch_cgne_iterate_graph captures the batched iterations as one CUDA graph (stream must
+ * be an explicitly created stream). residuals: count doubles |r_i|^2 in host memory
+ * (synchronizes). The projectors must outlive the batch; each belongs to one batch at a time. */
+elsa_status elsa_batch_cgne_create(elsa_projector* const* projectors, const float* const* b,
+                                   float* const* x, int32_t count, void* stream,
+                                   elsa_batch_cgne** out);
+elsa_status elsa_batch_cgne_iterate(elsa_batch_cgne* batch, int32_t iterations, void* stream);
+elsa_status elsa_batch_cgne_iterate_graph(elsa_batch_cgne* batch, int32_t iterations,
+                                          void* stream);
+elsa_status elsa_batch_cgne_residuals(elsa_batch_cgne* batch, double* residuals, void* stream);
+elsa_status elsa_batch_cgne_destroy(elsa_batch_cgne* batch);
 
 /* CGNE split around the reduction of its normal-operator results (view-sharded solves over
  * several GPUs, one process each; no reference counterpart: multi-GPU solves are a stated goal

@@ -82,3 +82,52 @@ def test_graph_needs_created_stream(cuda, oracle):
     st = torch.cuda.Stream()
     sol.iterate_graph(2, st.cuda_stream)
     st.synchronize()
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batched_cgne_matches_plain_sessions(cuda, oracle, graph):
+    """elsa_batch_cgne (forwards side by side, every adjoint in one launch per axis grid over an
+    instance table, vector updates batched): each instance's iterate equals that of its own
+    CGNE session bit for bit, also across further iterations and as one CUDA graph."""
+    import elsa_b200
+    torch = cuda
+    J = elsa_b200.PROJECTOR_JOSEPH
+    kinds = [(J, 24), (J, 40), (J, 16), (J, 32), (J, 24), (J, 48)]
+    insts = _instances(oracle, torch, kinds)
+    xs_plain, plain = _solvers(torch, insts, 0)
+    s = torch.cuda.current_stream().cuda_stream
+    for sol in plain:
+        sol.iterate(5, s)
+    torch.cuda.synchronize()
+    xs = [torch.full((p.domain_size,), np.nan, device="cuda") for p, _ in insts]
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        batch = elsa_b200.BatchCGNE([p for p, _ in insts], [b.data_ptr() for _, b in insts],
+                                    [x.data_ptr() for x in xs], st.cuda_stream)
+        (batch.iterate_graph if graph else batch.iterate)(5, st.cuda_stream)
+    st.synchronize()
+    for a, b in zip(xs_plain, xs):
+        assert bool((a == b).all())
+    res = batch.squared_residuals(st.cuda_stream)
+    for r, sol in zip(res, plain):
+        assert r == sol.squared_residual(s)
+    with torch.cuda.stream(st):
+        (batch.iterate_graph if graph else batch.iterate)(3, st.cuda_stream)
+    st.synchronize()
+    for sol in plain:
+        sol.iterate(3, s)
+    torch.cuda.synchronize()
+    for a, b in zip(xs_plain, xs):
+        assert bool((a == b).all())
+    batch.close()
+
+
+def test_batched_cgne_refuses_other_operators(cuda, oracle):
+    import elsa_b200
+    torch = cuda
+    insts = _instances(oracle, torch, [(elsa_b200.PROJECTOR_JOSEPH, 16),
+                                       (elsa_b200.PROJECTOR_SIDDON, 16)])
+    xs = [torch.zeros(p.domain_size, device="cuda") for p, _ in insts]
+    with pytest.raises(elsa_b200.ElsaError):
+        elsa_b200.BatchCGNE([p for p, _ in insts], [b.data_ptr() for _, b in insts],
+                            [x.data_ptr() for x in xs])
