@@ -400,10 +400,23 @@ def run_elsa(args):
     achieved = bytes_per_pass / (dom_ms / 1e3) / 1e9
     traffic = None
     prof = _traffic_from_profiles()
-    if prof and prof.get("kernel") == dominant:
+    if prof and (prof.get("kernel") != dominant or prof.get("workload") != WORKLOAD["workload"]):
+        prof = None  # the committed capture is of another kernel or workload
+    if prof:
         traffic = prof.get("dram_bytes_per_launch")
     compulsory = 4.0 * (proj.domain_size + proj.range_size)
     pair_achieved = 2.0 * bytes_per_pass / ((fwd_avg + adj_avg) / 1e3) / 1e9
+    # issue-rate ceiling of the dominant kernel: its warp instructions per sample (ncu, on a
+    # smaller case of the same geometry family) x samples / (148 SMs x 4 schedulers x clock)
+    issue = None
+    wips = prof.get("warp_inst_per_sample") if prof else None
+    if wips:
+        mhz = (clock_info or {}).get("sm_mhz") or 1965.0
+        ceiling_ms = wips * samples / (148 * 4 * mhz * 1e6) * 1e3
+        issue = {"warp_inst_per_sample": wips, "sm_mhz": mhz,
+                 "ceiling_ms": round(ceiling_ms, 3),
+                 "frac": round(ceiling_ms / dom_ms, 4),
+                 "source": prof.get("warp_inst_source")}
 
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "GUPS", "n_gpus": world,
@@ -411,8 +424,9 @@ def run_elsa(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (modified Shepp-Logan 3D phantom, b = A x)",
         "config": dict(WORKLOAD, parallelism="replicas" if world > 1 else "single GPU",
-                       l2="working set > L2 (1.7 GB ray table + 8 GB checkpoints + 212 MB "
-                          "sinogram per step)"),
+                       l2="no flush; every pass streams the %d-ray table with its slab "
+                          "checkpoints and the %.0f MB sinogram, together > L2 (126 MB)"
+                          % (proj.range_size, 4e-6 * proj.range_size)),
         "cg_iters_per_s": round(1e3 / ms_per_step, 3),
         "forward_ms": round(fwd_avg, 4), "adjoint_ms": round(adj_avg, 4),
         "cg_residual_sq": [res0, res1],
@@ -427,7 +441,10 @@ def run_elsa(args):
                      # forward + matched adjoint together: two passes of gather bytes over
                      # the sum of the two kernels' mean durations
                      "forward_back_achieved": round(pair_achieved, 1),
-                     "forward_back_frac": round(pair_achieved / peak, 4)},
+                     "forward_back_frac": round(pair_achieved / peak, 4),
+                     # the kernels are bound by instruction issue, not by DRAM (traffic is a
+                     # small fraction of the gather bytes): the issue-rate ceiling beside it
+                     "issue": issue},
         "gpu_launches": (proj.info(6) + proj.info(7) + VECTOR_LAUNCHES_PER_STEP) * args.steps,
         "clocks": clock_info,
     }
@@ -454,6 +471,58 @@ def run_elsa(args):
         print(json.dumps(out))
 
 
+def reference_form_cgne(torch, proj, b, iterations):
+    """CGNE in the reference's per-instance form: solvers/CGNE.cpp:20-78 over the operator's
+    apply / applyAdjoint, every operator application and vector operation its own call, and every
+    scalar (c.Ac and |r|^2 of the recurrence, and |r|, |c| of the log line the reference formats
+    each iteration) read back to the host before the next step, as DataContainer::dot and
+    squaredL2Norm return host values. Device-resident data (no host copies per apply)."""
+    import ctypes
+    from elsa_b200 import _capi
+    s = torch.cuda.current_stream().cuda_stream
+    n = proj.domain_size
+    x = torch.zeros(n, device="cuda")
+    r = torch.empty(n, device="cuda")
+    c = torch.empty(n, device="cuda")
+    ac = torch.empty(n, device="cuda")
+    atb = torch.empty(n, device="cuda")
+    tmp = torch.empty(proj.range_size, device="cuda")
+    res = torch.empty(1, dtype=torch.float64, device="cuda")
+
+    def dot(u, v):
+        _capi.call("elsa_dot", u.data_ptr(), v.data_ptr(), n, res.data_ptr(), s)
+        return res.item()
+
+    def sq(u):
+        _capi.call("elsa_squared_l2_norm", u.data_ptr(), n, res.data_ptr(), s)
+        return res.item()
+
+    def lin(a, u, bb, v, out):
+        _capi.call("elsa_lincomb", ctypes.c_float(a), u.data_ptr(), ctypes.c_float(bb),
+                   v.data_ptr(), out.data_ptr(), n, s)
+
+    def normal(u, out):  # (A^T A) u
+        proj.apply_ptr(u.data_ptr(), tmp.data_ptr(), s)
+        proj.apply_adjoint_ptr(tmp.data_ptr(), out.data_ptr(), s)
+
+    proj.apply_adjoint_ptr(b.data_ptr(), atb.data_ptr(), s)  # A^T b
+    normal(x, r)                                             # r = A^T b - A^T A x
+    lin(-1.0, r, 1.0, atb, r)
+    lin(1.0, r, 0.0, r, c)                                   # c = r
+    kold = sq(r)
+    for _ in range(iterations):
+        normal(c, ac)
+        alpha = kold / dot(c, ac)
+        lin(1.0, x, alpha, c, x)
+        lin(1.0, r, -alpha, ac, r)
+        k = sq(r)
+        beta = k / kold
+        lin(1.0, r, beta, c, c)
+        kold = k
+        sq(r), sq(c)  # the norms of the per-iteration log line
+    return x
+
+
 def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, streams=8,
                      seed=5, edges=(64, 96, 128), views=(60, 180), free_floor_gb=24.0):
     """Many independent reconstructions: one at a time (each solver's iterations enqueued on one
@@ -470,7 +539,7 @@ def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, st
         n = int(rng.choice(list(edges)))
         nv = int(rng.integers(views[0], views[1] + 1))
         specs.append((n, nv))
-    t_plain = t_batch = t_graphs = 0.0
+    t_plain = t_batch = t_graphs = t_ref = 0.0
     waves = 0
     per_edge = {}  # plain form: seconds spent on the instances of each volume edge
     i = 0
@@ -506,6 +575,15 @@ def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, st
             torch.cuda.synchronize()
             return xs, sols
 
+        # the reference's per-instance form, one problem after the other
+        reference_form_cgne(torch, problems[0][0], problems[0][1], 1)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for proj, b in problems:
+            reference_form_cgne(torch, proj, b, iterations)
+        torch.cuda.synchronize()
+        t_ref += time.perf_counter() - t0
+        torch.cuda.empty_cache()
         xs, plain = make()
         s = torch.cuda.current_stream().cuda_stream
         for sol in plain:  # warm-up of every kernel shape
@@ -561,6 +639,17 @@ def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, st
             "plain_recon_per_s": round(instances / t_plain, 3),
             "batched_recon_per_s": round(instances / t_batch, 3),
             "speedup": round(t_plain / t_batch, 3),
+            "plain_form": "this library's CGNE sessions one at a time: device-resident scalars, "
+                          "every iteration enqueued without a host round trip",
+            "reference_form_recon_per_s": round(instances / t_ref, 3),
+            "speedup_vs_reference_form": round(t_ref / t_batch, 3),
+            "reference_form": "CGNE.cpp's loop one problem at a time on this library's kernels: "
+                              "one call per operator application and vector operation, four "
+                              "scalars read back to the host per iteration",
+            # the instances of edge <= 128 are the only ones that leave the GPU idle on their
+            # own; if batching made them free the gain would still be bounded by their share
+            "small_instance_share": round(sum(v for k, v in per_edge.items() if k <= 128)
+                                          / max(sum(per_edge.values()), 1e-9), 4),
             "batched_form": "elsa_batch_cgne: forwards side by side, all adjoints in one launch "
                             "per axis grid over an instance table, batched vector updates, the "
                             "iterations one CUDA graph",

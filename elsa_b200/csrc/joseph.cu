@@ -41,23 +41,20 @@
 #include <cmath>
 #include <cstring>
 
-#ifndef ELSA_ADJ_BZ
-#define ELSA_ADJ_BZ 16 // z depth of the 3D adjoint's warp brick (x and y: one checkpoint slab)
-#endif
 #ifndef ELSA_ADJ_MIN_BLOCKS
 #define ELSA_ADJ_MIN_BLOCKS 1 // resident one-warp blocks per SM asked of the register allocator
 #endif
 #ifndef ELSA_ADJ_BATCH
-#define ELSA_ADJ_BATCH 2 // class rays per lane fetched together (3D adjoint; at 256^3 / 360 views 1: 64.0 ms, 2: 54.9, 3: 55.3, 4: 60.8)
+#define ELSA_ADJ_BATCH 2 // class rays per lane fetched together by the 3D adjoint (2 was fastest at 256^3 / 360 views)
 #endif
 #ifndef ELSA_AXIS_TD
-#define ELSA_AXIS_TD 8 // depth along the driving axis of the 3D adjoint's axis bricks
+#define ELSA_AXIS_TD 16 // depth along the driving axis of the 3D adjoint's axis bricks
 #endif
 #ifndef ELSA_AXIS_TW
 #define ELSA_AXIS_TW 32 // edge along the non-driving axis over which a detector row's rays spread
 #endif
 #ifndef ELSA_AXIS_TV
-#define ELSA_AXIS_TV 8 // edge along the other non-driving axis (256^3: 8: 38.9 ms, 16: 41.6 ms)
+#define ELSA_AXIS_TV 8 // edge along the other non-driving axis
 #endif
 #ifndef ELSA_SPLAT_UNROLL
 #define ELSA_SPLAT_UNROLL 2 // unroll factor of the adjoint's per-sample loop (1: 72.8 ms, 2: 63.4 ms, 4: 68.9 ms at 256^3)
@@ -994,292 +991,23 @@ namespace elsa_b200
             }
         };
 
-        // Shared-memory brick of one warp: x stride 1, row stride BX + 1, plane stride chosen
-        // congruent to 1 modulo 32, so the 8 x 4 patch of class rays a warp walks at once spreads
-        // over the banks for both x- and z-driving rays.
-        template <int BX, int BY>
-        struct WarpBrick {
-            static constexpr int kRow = BX + 1;
-            static constexpr int kPlaneMin = kRow * BY;
-            static constexpr int kPlane = kPlaneMin + ((33 - kPlaneMin % 32) % 32);
-        };
-
-        template <int G, int BX, int BY, int BZ>
-        struct WarpRoles {
-            using L = WarpBrick<BX, BY>;
-            static constexpr int strG = G == 0 ? 1 : (G == 1 ? L::kRow : L::kPlane);
-            static constexpr int extG = G == 0 ? BX : (G == 1 ? BY : BZ);
-            static constexpr int strA = G == 0 ? L::kRow : 1;
-            static constexpr int extA = G == 0 ? BY : BX;
-            static constexpr int strB = G == 2 ? L::kRow : L::kPlane;
-            static constexpr int extB = G == 2 ? BY : BZ;
-        };
-
-        // Bilinear footprint of one sample in the warp brick: four word addresses (taps outside
-        // the brick point at a dummy word past the brick) and their weights.
-        template <int G, int BX, int BY, int BZ>
-        __device__ __forceinline__ void warpTaps(float* plane, float* dummy, float pa, float pb,
-                                                 int orgA, int orgB, float* (&adr)[4],
-                                                 float (&wt)[4])
-        {
-            using AR = WarpRoles<G, BX, BY, BZ>;
-            Weights w;
-            tapWeights(pa, pb, w);
-            const int ia = w.ia - orgA, ib = w.ib - orgB;
-            const bool a0 = static_cast<unsigned>(ia) < static_cast<unsigned>(AR::extA);
-            const bool a1 = static_cast<unsigned>(ia + 1) < static_cast<unsigned>(AR::extA);
-            const bool b0 = static_cast<unsigned>(ib) < static_cast<unsigned>(AR::extB);
-            const bool b1 = static_cast<unsigned>(ib + 1) < static_cast<unsigned>(AR::extB);
-            float* q = plane + ia * AR::strA + ib * AR::strB;
-            adr[0] = (a0 && b0) ? q : dummy;
-            adr[1] = (a1 && b0) ? q + AR::strA : dummy;
-            adr[2] = (a0 && b1) ? q + AR::strB : dummy;
-            adr[3] = (a1 && b1) ? q + AR::strA + AR::strB : dummy;
-            wt[0] = w.wa * w.wb;
-            wt[1] = w.cwa * w.wb;
-            wt[2] = w.wa * w.cwb;
-            wt[3] = w.cwa * w.cwb;
-        }
-
-        // Walk samples jLo..jHi of ray R (position cp at sample jLo) through the brick. The loop
-        // is software-pipelined: the taps of sample j+1 (always on another plane) are read
-        // before the sums of sample j are written back.
-        template <int G, int BX, int BY, int BZ>
-        __device__ __forceinline__ void warpSplat(float* acc, float* dummy, const JosephRay& R,
-                                                  float yl, float2 cp, int jLo, int jHi,
-                                                  int orgG, int orgA, int orgB)
-        {
-            using AR = WarpRoles<G, BX, BY, BZ>;
-            const int dir = (R.meta & 4) ? -1 : 1;
-            float pa = cp.x, pb = cp.y;
-            float* plane = acc + (R.k0 + jLo * dir - orgG) * AR::strG;
-            const int dPlane = dir * AR::strG;
-            float* adr[4];
-            float wt[4], val[4];
-            warpTaps<G, BX, BY, BZ>(plane, dummy, pa, pb, orgA, orgB, adr, wt);
-#pragma unroll
-            for (int t = 0; t < 4; ++t)
-                val[t] = *adr[t];
-#pragma unroll kSplatUnroll
-            for (int j = jLo; j < jHi; ++j) {
-                plane += dPlane;
-                pa = __fadd_rn(pa, R.sa);
-                pb = __fadd_rn(pb, R.sb);
-                float* adr2[4];
-                float wt2[4], val2[4];
-                warpTaps<G, BX, BY, BZ>(plane, dummy, pa, pb, orgA, orgB, adr2, wt2);
-#pragma unroll
-                for (int t = 0; t < 4; ++t)
-                    val2[t] = *adr2[t];
-#pragma unroll
-                for (int t = 0; t < 4; ++t)
-                    *adr[t] = val[t] + yl * wt[t];
-#pragma unroll
-                for (int t = 0; t < 4; ++t) {
-                    adr[t] = adr2[t];
-                    wt[t] = wt2[t];
-                    val[t] = val2[t];
-                }
-            }
-#pragma unroll
-            for (int t = 0; t < 4; ++t)
-                *adr[t] = val[t] + yl * wt[t];
-        }
-
-        // One (view, driving axis G) for a warp-owned brick: M x M ray classes, separated by
-        // __syncwarp; lane i takes class rays i, i + 32, ... (u fastest within the class grid).
-        template <int G, int BX, int BY, int BZ, int CPD>
-        __device__ __forceinline__ void warpView(float* acc, const RayWindow& w, int p, int m,
-                                                 const JosephRay* __restrict__ rays,
-                                                 const float2* __restrict__ cps, int64_t nrays,
-                                                 const float* __restrict__ y,
-                                                 const DetectorShape& det, int org0, int org1,
-                                                 int org2)
-        {
-            using AR = WarpRoles<G, BX, BY, BZ>;
-            const int orgG = G == 0 ? org0 : (G == 1 ? org1 : org2);
-            const int orgA = G == 0 ? org1 : org0;
-            const int orgB = G == 2 ? org1 : org2;
-            const int kLo = orgG, kHi = orgG + AR::extG - 1;
-            // a brick thinner than a checkpoint slab along G starts its rays from the slab's
-            // checkpoint and advances them to the brick's first plane
-            constexpr bool kPartialSlab = AR::extG < CPD;
-            const int slabLo = (orgG / CPD) * CPD, slabHi = slabLo + CPD - 1;
-            const int lane = threadIdx.x & 31;
-            const int64_t viewBase = static_cast<int64_t>(det.nu) * det.nv * p;
-            for (int ov = 0; ov < m; ++ov) {
-                const int vStart = w.v0 + ov;
-                const int nvc = vStart <= w.v1 ? (w.v1 - vStart) / m + 1 : 0;
-                for (int ou = 0; ou < m; ++ou) {
-                    const int uStart = w.u0 + ou;
-                    const int nuc = uStart <= w.u1 ? (w.u1 - uStart) / m + 1 : 0;
-                    const int total = nuc * nvc;
-                    const float invNuc = nuc > 0 ? 1.0f / static_cast<float>(nuc) : 0.0f;
-                    // up to kBatch class rays per lane are fetched together (record,
-                    // checkpoint and detector value are independent loads: the brick is one
-                    // checkpoint slab deep, so the checkpoint row is known up front)
-                    constexpr int kBatch = ELSA_ADJ_BATCH;
-                    const int64_t cpRow = static_cast<int64_t>(orgG / CPD + 1) * nrays;
-                    for (int base = lane; base < total; base += 32 * kBatch) {
-                        JosephRay Rb[kBatch];
-                        float2 cpb[kBatch];
-                        float yb[kBatch];
-#pragma unroll
-                        for (int q = 0; q < kBatch; ++q) {
-                            const int i = base + 32 * q;
-                            Rb[q].n = 0;
-                            if (i < total) {
-                                // i / nuc by a float reciprocal: exact for i < 2^20, nuc < 2^11
-                                const int iv =
-                                    static_cast<int>((static_cast<float>(i) + 0.5f) * invNuc);
-                                const int iu = i - iv * nuc;
-                                const int64_t r = viewBase + (uStart + iu * m) +
-                                                  static_cast<int64_t>(det.nu) * (vStart + iv * m);
-                                Rb[q] = rays[r];
-                                cpb[q] = __ldg(cps + cpRow + r);
-                                yb[q] = __ldg(y + r);
-                            }
-                        }
-#pragma unroll
-                        for (int q = 0; q < kBatch; ++q) {
-                            const JosephRay& R = Rb[q];
-                            if (R.n == 0 || (R.meta & 3) != G)
-                                continue;
-                            int jLo, jHi;
-                            if (!sampleRange(R, kLo, kHi, jLo, jHi))
-                                continue;
-                            float2 cp = cpb[q];
-                            if (kPartialSlab) {
-                                int jS0, jS1;
-                                sampleRange(R, slabLo, slabHi, jS0, jS1);
-                                for (int j = jS0; j < jLo; ++j) {
-                                    cp.x = __fadd_rn(cp.x, R.sa);
-                                    cp.y = __fadd_rn(cp.y, R.sb);
-                                }
-                            }
-                            warpSplat<G, BX, BY, BZ>(acc, acc + WarpBrick<BX, BY>::kPlane * BZ,
-                                                     R, yb[q] * R.len, cp, jLo, jHi, orgG,
-                                                     orgA, orgB);
-                        }
-                    }
-                    __syncwarp();
-                }
-            }
-        }
-
-        // 3D adjoint: one warp per brick of BX x BY x BZ voxels; the brick accumulates every
-        // view in a fixed order (view, axis, class, lane round) and is written once.
-        template <int BX, int BY, int BZ, int CPD>
-        __global__ void __launch_bounds__(32, ELSA_ADJ_MIN_BLOCKS)
-            josephAdjointWarpKernel(const JosephRay* __restrict__ rays,
-                                    const float2* __restrict__ checkpoints, int64_t nrays,
-                                    const float* __restrict__ y,
-                                    const RayWindow* __restrict__ windows,
-                                    const unsigned* __restrict__ viewAxes, VolumeShape vol,
-                                    DetectorShape det, int m, int3 nBricks, int viewsPerChunk,
-                                    float* __restrict__ x, int chunkBase)
-        {
-            // chunkBase + blockIdx.y selects a chunk of views, as in the 2D kernel: with several
-            // chunks the brick goes to x + chunk * nvox and sumChunksKernel adds the chunks in
-            // order
-            using L = WarpBrick<BX, BY>;
-            __shared__ float acc[L::kPlane * BZ + 1]; // + dummy word for taps outside
-            const int lane = threadIdx.x;
-            const int bi = blockIdx.x;
-            const int org0 = (bi % nBricks.x) * BX, org1 = ((bi / nBricks.x) % nBricks.y) * BY,
-                      org2 = (bi / (nBricks.x * nBricks.y)) * BZ;
-            const int nb = nBricks.x * nBricks.y * nBricks.z;
-            for (int i = lane; i < L::kPlane * BZ; i += 32)
-                acc[i] = 0.0f;
-            __syncwarp();
-            const int chunk = chunkBase + static_cast<int>(blockIdx.y);
-            const int pBegin = chunk * viewsPerChunk;
-            const int pEnd = min(det.np, pBegin + viewsPerChunk);
-            for (int p = pBegin; p < pEnd; ++p) {
-                const RayWindow w = windows[static_cast<int64_t>(p) * nb + bi];
-                if (w.u0 > w.u1 || w.v0 > w.v1)
-                    continue;
-                const unsigned ax = viewAxes[p];
-                if (ax & 1u)
-                    warpView<0, BX, BY, BZ, CPD>(acc, w, p, m, rays, checkpoints, nrays, y, det,
-                                                 org0, org1, org2);
-                if (ax & 2u)
-                    warpView<1, BX, BY, BZ, CPD>(acc, w, p, m, rays, checkpoints, nrays, y, det,
-                                                 org0, org1, org2);
-                if (ax & 4u)
-                    warpView<2, BX, BY, BZ, CPD>(acc, w, p, m, rays, checkpoints, nrays, y, det,
-                                                 org0, org1, org2);
-            }
-            const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
-            float* out = x + static_cast<int64_t>(chunk) * nvox;
-            for (int i = lane; i < BX * BY * BZ; i += 32) {
-                const int lx = i % BX, ly = (i / BX) % BY, lz = i / (BX * BY);
-                const int gx = org0 + lx, gy = org1 + ly, gz = org2 + lz;
-                if (gx < vol.n[0] && gy < vol.n[1] && gz < vol.n[2])
-                    out[gx + static_cast<int64_t>(vol.n[0]) *
-                                 (gy + static_cast<int64_t>(vol.n[1]) * gz)] =
-                        acc[lz * L::kPlane + ly * L::kRow + lx];
-            }
-        }
-
-        template <int BX, int BY, int BZ, int CPD>
-        struct WarpAdjointConfig {
-            static constexpr int kCheckpointDepth = CPD;
-            static_assert(BX == CPD && BY == CPD && BZ <= CPD && CPD % BZ == 0,
-                          "a warp brick is one checkpoint slab deep along x and y and a whole "
-                          "fraction of one along z");
-            static int3 brick() { return make_int3(BX, BY, BZ); }
-            static void prepare(int) {}
-            // View chunks so that bricks x chunks reach kAdjoint3dWarpsPerSm one-warp CTAs per
-            // SM (about two waves of the 11 bricks that fit in shared memory at once); a 256^3
-            // volume has 4096 bricks and keeps one chunk.
-            static int chunks(int nbricks, int np)
-            {
-                const int want = (kAdjoint3dWarpsPerSm * 148 + nbricks - 1) / nbricks;
-                return want < 1 ? 1 : (want > np ? np : want);
-            }
-            // nc view chunks; partial: scratch of nc volumes (unused with one chunk)
-            static void launch(int nbricks, int nc, cudaStream_t s, const JosephRay* rays,
-                               const float2* cps, int64_t nrays, const float* y,
-                               const RayWindow* win, const unsigned* axes, VolumeShape vol,
-                               DetectorShape det, int m, int3 nb, float* x, float* partial)
-            {
-                const int per = (det.np + nc - 1) / nc;
-                const int used = (det.np + per - 1) / per;
-                launchChunks(nbricks, 0, used, per, s, rays, cps, nrays, y, win, axes, vol, det,
-                             m, nb, used > 1 ? partial : x);
-                if (used > 1)
-                    launchSumChunks(partial, used,
-                                    static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2], x, s);
-            }
-            // chunks [c0, c1) of `per` views each, into out + chunk * nvox
-            static void launchChunks(int nbricks, int c0, int c1, int per, cudaStream_t s,
-                                     const JosephRay* rays, const float2* cps, int64_t nrays,
-                                     const float* y, const RayWindow* win, const unsigned* axes,
-                                     VolumeShape vol, DetectorShape det, int m, int3 nb,
-                                     float* out)
-            {
-                if (c1 <= c0)
-                    return;
-                const dim3 grid(static_cast<unsigned>(nbricks), static_cast<unsigned>(c1 - c0));
-                josephAdjointWarpKernel<BX, BY, BZ, CPD><<<grid, 32, 0, s>>>(
-                    rays, cps, nrays, y, win, axes, vol, det, m, nb, per, out, c0);
-            }
-        };
-
         // ---------------------------------------------------------------------------------------
         // 3D adjoint on axis bricks. The rays of one view all step along about the same axis G, so
         // the volume is cut, per driving axis present, into bricks that are TD planes deep along G
         // and TA x TB voxels across (a < b the other two axes). A ray crossing such a brick keeps
         // most of its TD samples inside it (a 16^3 brick loses half of the samples of oblique rays
         // to its sides), and the window of a brick, the pixels whose centres lie in the projection
-        // of the brick grown by half a voxel, holds few rays that miss it. One warp owns a brick
-        // in shared memory for a chunk of views and splats the window's rays class by class, as
-        // the 16^3 warp kernel does. Across the rays the brick keeps a halo of two voxels on every
-        // side: tap indices are clamped into it instead of tested, and the halo is not written out.
+        // of the brick grown by about half a voxel, holds few rays that miss it. One warp owns a
+        // brick in shared memory for a chunk of views and splats the window's rays class by class:
+        // rays of one class are more than two voxels apart, so no two lanes add to one word at
+        // once and the brick needs no atomics. A tap outside the brick is predicated off (the
+        // neighbouring brick owns it); with ELSA_AXIS_HALO 2 the brick instead carries a two-voxel
+        // halo into which tap indices are clamped, and the halo is not written out.
         // ---------------------------------------------------------------------------------------
 #ifndef ELSA_AXIS_HALO
-#define ELSA_AXIS_HALO 2 // halo of the axis bricks (0: no halo, taps outside are predicated off)
+// halo of the axis bricks: 0, taps outside the brick predicated off (256^3: 35.9 ms); 2, taps
+// clamped into a two-voxel halo (38.9 ms with 8-deep bricks, whose halo costs occupancy)
+#define ELSA_AXIS_HALO 0
 #endif
         constexpr int kAxisHalo = ELSA_AXIS_HALO;
         static_assert(kAxisHalo == 0 || kAxisHalo == 2, "halo of 0 or 2 voxels");
@@ -1288,6 +1016,9 @@ namespace elsa_b200
         // the non-driving axis over which the rays of a detector row spread (the warp's lanes
         // spread along it, so stride 1 there keeps their taps in different banks), rows along the
         // other one; both carry the halo.
+#ifndef ELSA_AXIS_PLANE_ODD
+#define ELSA_AXIS_PLANE_ODD 0 // 1: pad the plane stride to 1 modulo 32 (256^3: 35.8 ms, 0: 33.5 ms)
+#endif
 #ifndef ELSA_AXIS_ROWPAD
 #define ELSA_AXIS_ROWPAD (ELSA_AXIS_HALO == 0 ? 1 : 0) // extra words per row (bank spread)
 #endif
@@ -1297,8 +1028,10 @@ namespace elsa_b200
             static constexpr int kRow = TW + 2 * kAxisHalo + ELSA_AXIS_ROWPAD;
             static constexpr int kRows = TV + 2 * kAxisHalo; // rows per plane
             static constexpr int kPlaneMin = kRow * kRows;
-            // plane stride congruent to 1 modulo 32: lanes one plane apart use other banks
-            static constexpr int kPlane = kPlaneMin + ((33 - kPlaneMin % 32) % 32);
+            // plane stride unpadded (smaller bricks, more of them resident per SM), or congruent
+            // to 1 modulo 32 with ELSA_AXIS_PLANE_ODD 1 (lanes one plane apart in other banks)
+            static constexpr int kPlane =
+                ELSA_AXIS_PLANE_ODD ? kPlaneMin + ((33 - kPlaneMin % 32) % 32) : kPlaneMin;
             static constexpr int kWords = kPlane * TD;
         };
 
@@ -1495,8 +1228,9 @@ namespace elsa_b200
                             int jLo, jHi;
                             if (!sampleRange(R, kLo, kHi, jLo, jHi))
                                 continue;
-                            // the checkpoint holds the position at the ray's first sample in the
-                            // slab; a brick thinner than the slab advances it to its own planes
+                            // the checkpoint holds the position at the ray's first sample in
+                            // the slab; a brick thinner than the slab advances it to its own
+                            // planes
                             float2 cp = cpb[q];
                             if (TD < CPD) {
                                 int jS0, jS1;
@@ -1638,7 +1372,6 @@ namespace elsa_b200
                                                   static_cast<int>(local / nb), acc);
         }
 
-        using Adjoint3d = WarpAdjointConfig<16, 16, ELSA_ADJ_BZ, 16>;
         using Adjoint2d = AdjointConfig<2, 64, 64, 1, 64, 8>;
 
         class JosephProjector final : public Projector
@@ -2373,7 +2106,6 @@ namespace elsa_b200
             void launchAxisChunks(int c0, int c1, const float* y, float* out, cudaStream_t s,
                                   int batch = 1, int64_t yStride = 0, int64_t outStride = 0)
             {
-                const int per = (det_.np + adjointChunks_ - 1) / adjointChunks_;
                 for (int g = 0; g < 3; ++g) {
                     const AxisGrid& G = grids_[g];
                     if (!G.present)

@@ -345,14 +345,15 @@ namespace elsa_b200
         __global__ void siddonWindowCheckKernel(const SiddonRay* __restrict__ rays,
                                                 const RayWindow* __restrict__ windows,
                                                 VolumeShape vol, DetectorShape det, int3 brick,
-                                                int3 nBricks, unsigned long long* __restrict__ misses)
+                                                int3 nBricks, int onlyAxis,
+                                                unsigned long long* __restrict__ misses)
         {
             const int64_t nrays = static_cast<int64_t>(det.nu) * det.nv * det.np;
             const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
             if (r >= nrays)
                 return;
             const SiddonRay R = rays[r];
-            if (!(R.meta & kActive))
+            if (!(R.meta & kActive) || (onlyAxis >= 0 && (R.meta & 3) != onlyAxis))
                 return;
             const int u = static_cast<int>(r % det.nu);
             const int v = static_cast<int>((r / det.nu) % det.nv);
@@ -563,6 +564,188 @@ namespace elsa_b200
             }
         }
 
+        // ---------------------------------------------------------------------------------------
+        // 3D brick-owner adjoint on axis bricks: per driving axis G present, bricks one checkpoint
+        // slab (kSlab planes) deep along G, kAxisTW voxels along the non-driving axis over which
+        // the rays of a detector row spread (the columns: stride 1 in shared memory, the lanes
+        // spread along it) and kAxisTV along the other. A ray crossing a brick keeps most of its
+        // visits inside it, and a warp's taps fall into different banks. Visits outside the brick
+        // across the rays are predicated off. As the 16^3 kernel: one warp per (brick, chunk
+        // entry), the window's rays class by class, each lane replaying one ray's visits of the
+        // slab from its checkpoint.
+        // ---------------------------------------------------------------------------------------
+        constexpr int kAxisTW = 32, kAxisTV = 8;
+
+        struct SiddonAxisBrick {
+            static constexpr int kRow = kAxisTW + 1; // columns (+1: rows land in other banks)
+            static constexpr int kPlaneMin = kRow * kAxisTV;
+            static constexpr int kPlane = kPlaneMin + ((33 - kPlaneMin % 32) % 32);
+            static constexpr int kWords = kPlane * kSlab;
+        };
+
+        // Brick edges of grid G (UB: columns along b) in volume axis order.
+        template <int G, bool UB>
+        __host__ __device__ constexpr int siddonAxisEdge(int axis)
+        {
+            return axis == G ? kSlab
+                             : (axis == (G == 0 ? 1 : 0) ? (UB ? kAxisTV : kAxisTW)
+                                                         : (UB ? kAxisTW : kAxisTV));
+        }
+
+        struct SiddonAxisJob {
+            const SiddonRay* rays;
+            const float4* cpState;
+            const unsigned* cpVoxel;
+            int64_t nrays;
+            const float* y;
+            const RayWindow* windows;
+            const unsigned* viewAxes;
+            const int2* chunks;
+            int viewsPerChunk;
+            VolumeShape vol;
+            DetectorShape det;
+            int m;
+            int3 nBricks;
+            int binary;
+            float* out;
+        };
+
+        // Replays the visits of one ray inside the slab [kLo, kLo + kSlab) along G from its
+        // checkpoint and adds y * weight to the visits inside the axis brick.
+        template <int G, bool UB>
+        __device__ __forceinline__ void splatAxisSegment(float* acc, float3 tDelta, int meta,
+                                                         int kFirst, float4 cp, unsigned cpv,
+                                                         float yv, int kLo, int orgA, int orgB,
+                                                         const VolumeShape& vol, int binary)
+        {
+            using L = SiddonAxisBrick;
+            constexpr int EA = UB ? kAxisTV : kAxisTW, EB = UB ? kAxisTW : kAxisTV;
+            constexpr int SA = UB ? L::kRow : 1, SB = UB ? 1 : L::kRow;
+            int a, b;
+            nonDrivingAxes(G, a, b);
+            const int dirG = ((meta >> (2 + G)) & 1) ? -1 : 1;
+            const int kg = dirG > 0 ? max(kLo, kFirst) : min(kLo + kSlab - 1, kFirst);
+            int c0, c1, c2;
+            entryVoxel(G, kg, static_cast<int>(cpv & 0xffffu), static_cast<int>(cpv >> 16), c0,
+                       c1, c2);
+            const int s0 = axisStep(meta, 0), s1 = axisStep(meta, 1), s2 = axisStep(meta, 2);
+            float T0 = cp.x, T1 = cp.y, T2 = cp.z;
+            float tEntry = cp.w;
+            for (int it = 0; it < 3 * kSlab + 3; ++it) {
+                bool m0, m1, m2;
+                const float tExit = nextCrossing<3>(T0, T1, T2, m0, m1, m2);
+                const int c[3] = {c0, c1, c2};
+                const int lg = c[G] - kLo, la = c[a] - orgA, lb = c[b] - orgB;
+                if (static_cast<unsigned>(la) < static_cast<unsigned>(EA) &&
+                    static_cast<unsigned>(lb) < static_cast<unsigned>(EB)) {
+                    float* adr = acc + lg * L::kPlane + la * SA + lb * SB;
+                    const float w = binary ? 1.0f : __fsub_rn(tExit, tEntry);
+                    *adr = __fadd_rn(*adr, __fmul_rn(yv, w));
+                }
+                if (m0) {
+                    c0 += s0;
+                    T0 = __fadd_rn(T0, tDelta.x);
+                }
+                if (m1) {
+                    c1 += s1;
+                    T1 = __fadd_rn(T1, tDelta.y);
+                }
+                if (m2) {
+                    c2 += s2;
+                    T2 = __fadd_rn(T2, tDelta.z);
+                }
+                const bool inside =
+                    static_cast<unsigned>(c0) < static_cast<unsigned>(vol.n[0]) &&
+                    static_cast<unsigned>(c1) < static_cast<unsigned>(vol.n[1]) &&
+                    static_cast<unsigned>(c2) < static_cast<unsigned>(vol.n[2]);
+                const int cg = G == 0 ? c0 : (G == 1 ? c1 : c2);
+                if (!inside || cg < kLo || cg >= kLo + kSlab)
+                    break;
+                tEntry = tExit;
+            }
+        }
+
+        template <int G, bool UB>
+        __global__ void __launch_bounds__(32)
+            siddonAxisKernel(SiddonAxisJob J, int entryBase)
+        {
+            using L = SiddonAxisBrick;
+            __shared__ float acc[L::kWords];
+            constexpr int EX = siddonAxisEdge<G, UB>(0), EY = siddonAxisEdge<G, UB>(1),
+                          EZ = siddonAxisEdge<G, UB>(2);
+            constexpr int SA = UB ? L::kRow : 1, SB = UB ? 1 : L::kRow;
+            const int lane = threadIdx.x;
+            const int bi = blockIdx.x;
+            const int3 nb3 = J.nBricks;
+            const int org[3] = {(bi % nb3.x) * EX, ((bi / nb3.x) % nb3.y) * EY,
+                                (bi / (nb3.x * nb3.y)) * EZ};
+            int a, b;
+            nonDrivingAxes(G, a, b);
+            const int kLo = org[G], kHi = kLo + kSlab - 1;
+            const int nb = nb3.x * nb3.y * nb3.z;
+            for (int i = lane; i < L::kWords; i += 32)
+                acc[i] = 0.0f;
+            __syncwarp();
+            const int2 entry = J.chunks[entryBase + blockIdx.y];
+            const int pBegin = entry.x * J.viewsPerChunk;
+            const int pEnd = min(J.det.np, pBegin + J.viewsPerChunk);
+            const int64_t cpRow = static_cast<int64_t>(kLo / kSlab + 1) * J.nrays;
+            const int m = J.m;
+            for (int p = pBegin; p < pEnd; ++p) {
+                if (!(J.viewAxes[p] & (1u << G)))
+                    continue;
+                const RayWindow w = J.windows[static_cast<int64_t>(p) * nb + bi];
+                if (w.u0 > w.u1 || w.v0 > w.v1)
+                    continue;
+                const int64_t viewBase = static_cast<int64_t>(J.det.nu) * J.det.nv * p;
+                for (int ov = 0; ov < m; ++ov) {
+                    const int vStart = w.v0 + ov;
+                    const int nvc = vStart <= w.v1 ? (w.v1 - vStart) / m + 1 : 0;
+                    for (int ou = 0; ou < m; ++ou) {
+                        const int uStart = w.u0 + ou;
+                        const int nuc = uStart <= w.u1 ? (w.u1 - uStart) / m + 1 : 0;
+                        const int total = nuc * nvc;
+                        for (int i = lane; i < total; i += 32) {
+                            const int iv = i / nuc;
+                            const int iu = i - iv * nuc;
+                            const int64_t r = viewBase + (uStart + iu * m) +
+                                              static_cast<int64_t>(J.det.nu) * (vStart + iv * m);
+                            const int4* rp = reinterpret_cast<const int4*>(J.rays + r);
+                            const int4 q0 = __ldg(rp);     // tDelta[3], meta
+                            const int4 q1 = __ldg(rp + 1); // kFirst, kLast, cur[2]
+                            const int meta = q0.w;
+                            if (!(meta & kActive) || (meta & 3) != G)
+                                continue;
+                            if (max(q1.x, q1.y) < kLo || min(q1.x, q1.y) > kHi)
+                                continue;
+                            const float3 td =
+                                make_float3(__int_as_float(q0.x), __int_as_float(q0.y),
+                                            __int_as_float(q0.z));
+                            splatAxisSegment<G, UB>(acc, td, meta, q1.x,
+                                                    __ldg(J.cpState + cpRow + r),
+                                                    __ldg(J.cpVoxel + cpRow + r), __ldg(J.y + r),
+                                                    kLo, org[a], org[b], J.vol, J.binary);
+                        }
+                        __syncwarp();
+                    }
+                }
+            }
+            __syncwarp();
+            const VolumeShape& vol = J.vol;
+            const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
+            float* dst = J.out + static_cast<int64_t>(entry.y) * nvox;
+            for (int i = lane; i < EX * EY * EZ; i += 32) {
+                const int lx = i % EX, ly = (i / EX) % EY, lz = i / (EX * EY);
+                const int gx = org[0] + lx, gy = org[1] + ly, gz = org[2] + lz;
+                if (gx < vol.n[0] && gy < vol.n[1] && gz < vol.n[2]) {
+                    const int l[3] = {lx, ly, lz};
+                    dst[gx + static_cast<int64_t>(vol.n[0]) *
+                                 (gy + static_cast<int64_t>(vol.n[1]) * gz)] =
+                        acc[l[G] * L::kPlane + l[a] * SA + l[b] * SB];
+                }
+            }
+        }
+
         class SiddonProjector final : public Projector
         {
         public:
@@ -662,21 +845,65 @@ namespace elsa_b200
                 }
                 if (!cpState_)
                     throw Error(ELSA_ERROR_LOGIC, "SiddonsMethod: brick-owner adjoint not built");
+                if (vol_.dim == 3) {
+                    float* out = axisPartials_ > 1 ? partial_->as<float>() : x;
+                    const int per = (det_.np + adjointChunks_ - 1) / adjointChunks_;
+                    for (int g = 0; g < 3; ++g) {
+                        const SiddonGrid& G = grids_[g];
+                        if (!G.present || G.entryEnd <= G.entryBegin)
+                            continue;
+                        SiddonAxisJob J{};
+                        J.rays = rays_->as<SiddonRay>();
+                        J.cpState = cpState_->as<float4>();
+                        J.cpVoxel = cpVoxel_->as<unsigned>();
+                        J.nrays = rangeSize_;
+                        J.y = y;
+                        J.windows = G.windows->as<RayWindow>();
+                        J.viewAxes = viewAxes_->as<unsigned>();
+                        J.chunks = dEntries_->as<int2>() + G.entryBegin;
+                        J.viewsPerChunk = per;
+                        J.vol = vol_;
+                        J.det = det_;
+                        J.m = classSpacing_;
+                        J.nBricks = G.nb;
+                        J.binary = binary_;
+                        J.out = out;
+                        const dim3 grid(static_cast<unsigned>(G.nb.x * G.nb.y * G.nb.z),
+                                        static_cast<unsigned>(G.entryEnd - G.entryBegin));
+#define ELSA_SIDDON_AXIS(G_, UB_) siddonAxisKernel<G_, UB_><<<grid, 32, 0, s>>>(J, 0)
+                        if (g == 0) {
+                            if (G.ub)
+                                ELSA_SIDDON_AXIS(0, true);
+                            else
+                                ELSA_SIDDON_AXIS(0, false);
+                        } else if (g == 1) {
+                            if (G.ub)
+                                ELSA_SIDDON_AXIS(1, true);
+                            else
+                                ELSA_SIDDON_AXIS(1, false);
+                        } else {
+                            if (G.ub)
+                                ELSA_SIDDON_AXIS(2, true);
+                            else
+                                ELSA_SIDDON_AXIS(2, false);
+                        }
+#undef ELSA_SIDDON_AXIS
+                        ELSA_LAUNCH_CHECK("siddonAxisKernel");
+                    }
+                    if (axisPartials_ > 1)
+                        launchSumChunks(partial_->as<float>(), axisPartials_, domainSize_, x, s);
+                    return;
+                }
                 const int nb = nBricks_.x * nBricks_.y * nBricks_.z;
                 const int per = (det_.np + adjointChunks_ - 1) / adjointChunks_;
                 const int used = (det_.np + per - 1) / per;
                 const dim3 grid(static_cast<unsigned>(nb), static_cast<unsigned>(used));
                 float* out = used > 1 ? partial_->as<float>() : x;
-                if (vol_.dim == 3)
-                    siddonAdjointKernel<3><<<grid, 32, 0, s>>>(
-                        rays_->as<SiddonRay>(), cpState_->as<float4>(), cpVoxel_->as<unsigned>(),
-                        rangeSize_, y, windows_->as<RayWindow>(), viewAxes_->as<unsigned>(), vol_,
-                        det_, classSpacing_, nBricks_, per, binary_, out);
-                else
-                    siddonAdjointKernel<2><<<grid, 32, 0, s>>>(
-                        rays_->as<SiddonRay>(), cpState_->as<float4>(), cpVoxel_->as<unsigned>(),
-                        rangeSize_, y, windows_->as<RayWindow>(), viewAxes_->as<unsigned>(), vol_,
-                        det_, classSpacing_, nBricks_, per, binary_, out);
+                // 2D: square bricks (3D volumes take the axis bricks above)
+                siddonAdjointKernel<2><<<grid, 32, 0, s>>>(
+                    rays_->as<SiddonRay>(), cpState_->as<float4>(), cpVoxel_->as<unsigned>(),
+                    rangeSize_, y, windows_->as<RayWindow>(), viewAxes_->as<unsigned>(), vol_,
+                    det_, classSpacing_, nBricks_, per, binary_, out);
                 ELSA_LAUNCH_CHECK("siddonAdjointKernel");
                 if (used > 1)
                     launchSumChunks(partial_->as<float>(), used, domainSize_, x, s);
@@ -687,7 +914,14 @@ namespace elsa_b200
                 switch (key) {
                 case 0:
                     return classSpacing_;
-                case 1:
+                case 1: // bricks of the brick-owner adjoint (3D: over the axis grids)
+                    if (vol_.dim == 3) {
+                        int64_t n = 0;
+                        for (const SiddonGrid& g : grids_)
+                            if (g.present)
+                                n += static_cast<int64_t>(g.nb.x) * g.nb.y * g.nb.z;
+                        return n;
+                    }
                     return static_cast<int64_t>(nBricks_.x) * nBricks_.y * nBricks_.z;
                 case 2:
                     return visits_;
@@ -695,8 +929,17 @@ namespace elsa_b200
                     return 0;
                 case 6: // kernel launches per forward call
                     return 1;
-                case 7: // kernel launches per adjoint call (with view chunks: + the chunk sum)
-                    return (!scatter_ && adjointChunks_ > 1) ? 2 : 1;
+                case 7: // kernel launches per adjoint call (brick owner in 3D: one per axis
+                        // grid; with several partial volumes: + the chunk sum)
+                    if (scatter_)
+                        return 1;
+                    if (vol_.dim == 3) {
+                        int n = 0;
+                        for (const SiddonGrid& g : grids_)
+                            n += g.present && g.entryEnd > g.entryBegin ? 1 : 0;
+                        return n + (axisPartials_ > 1 ? 1 : 0);
+                    }
+                    return adjointChunks_ > 1 ? 2 : 1;
                 case 8: // visits outside the windows of their bricks (brick-owner adjoint only;
                         // test support; synchronizes)
                     return windowMisses();
@@ -707,7 +950,7 @@ namespace elsa_b200
 
             int64_t windowMisses() const
             {
-                if (!windows_)
+                if (!cpState_)
                     return -1;
                 DeviceBuffer count(sizeof(unsigned long long));
                 ELSA_CUDA(cudaMemset(count.as<unsigned long long>(), 0, sizeof(unsigned long long)));
@@ -715,13 +958,19 @@ namespace elsa_b200
                 const unsigned blocks = static_cast<unsigned>((nrays + 255) / 256);
                 const int bz = vol_.dim == 3 ? kSlab : 1;
                 if (vol_.dim == 3)
-                    siddonWindowCheckKernel<3><<<blocks, 256>>>(
-                        rays_->as<SiddonRay>(), windows_->as<RayWindow>(), vol_, det_,
-                        make_int3(kSlab, kSlab, bz), nBricks_, count.as<unsigned long long>());
+                    for (int g = 0; g < 3; ++g) {
+                        if (!grids_[g].present)
+                            continue;
+                        siddonWindowCheckKernel<3><<<blocks, 256>>>(
+                            rays_->as<SiddonRay>(), grids_[g].windows->as<RayWindow>(), vol_,
+                            det_, grids_[g].edge, grids_[g].nb, g,
+                            count.as<unsigned long long>());
+                    }
                 else
                     siddonWindowCheckKernel<2><<<blocks, 256>>>(
                         rays_->as<SiddonRay>(), windows_->as<RayWindow>(), vol_, det_,
-                        make_int3(kSlab, kSlab, bz), nBricks_, count.as<unsigned long long>());
+                        make_int3(kSlab, kSlab, bz), nBricks_, -1,
+                        count.as<unsigned long long>());
                 ELSA_LAUNCH_CHECK("siddonWindowCheckKernel");
                 unsigned long long h = 0;
                 ELSA_CUDA(cudaMemcpy(&h, count.as<unsigned long long>(), sizeof(h),
@@ -782,10 +1031,14 @@ namespace elsa_b200
                 } else {
                     adjointChunks_ = value;
                 }
-                // the partial volumes exist only while the brick-owner adjoint uses chunks
+                // the partial volumes exist only while the brick-owner adjoint uses chunks (3D:
+                // one per (chunk, axis grid) pair)
+                int volumes = adjointChunks_;
+                if (!scatter_ && vol_.dim == 3)
+                    volumes = buildAxisEntries();
                 const size_t need = sizeof(float) * static_cast<size_t>(domainSize_) *
-                                    static_cast<size_t>(adjointChunks_);
-                if (scatter_ || adjointChunks_ <= 1)
+                                    static_cast<size_t>(volumes);
+                if (scatter_ || volumes <= 1)
                     partial_.reset();
                 else if (!partial_ || partial_->bytes() < need) {
                     partial_.reset();
@@ -815,11 +1068,16 @@ namespace elsa_b200
                         rays_->as<SiddonRay>(), nrays, vol_, cpRows_, cpState_->as<float4>(),
                         cpVoxel_->as<unsigned>(), nullptr);
                 ELSA_LAUNCH_CHECK("siddonCheckpointKernel");
+                CurvedTables tables(vol_.dim, det_, curved_);
+                if (vol_.dim == 3) {
+                    buildAxisGrids(tables.map());
+                    ELSA_CUDA(cudaDeviceSynchronize());
+                    return;
+                }
                 const int bz = vol_.dim == 3 ? kSlab : 1;
                 const int64_t nwin =
                     static_cast<int64_t>(nBricks_.x) * nBricks_.y * nBricks_.z * det_.np;
                 windows_ = std::make_unique<DeviceBuffer>(sizeof(RayWindow) * nwin);
-                CurvedTables tables(vol_.dim, det_, curved_);
                 // Siddon visits exactly the voxels a ray crosses: the window is the projection
                 // of the brick itself, grown by kWindowSlack for the rounding of the float rays
                 launchBrickWindows(dPoses_, vol_, det_, make_int3(kSlab, kSlab, bz), nBricks_,
@@ -834,6 +1092,115 @@ namespace elsa_b200
                 cpState_.reset();
                 cpVoxel_.reset();
                 windows_.reset();
+                for (SiddonGrid& g : grids_)
+                    g = SiddonGrid{};
+                dEntries_.reset();
+                axisPartials_ = 0;
+            }
+
+            // ---- 3D brick-owner adjoint on axis bricks ----
+            struct SiddonGrid {
+                bool present = false;
+                bool ub = false; // columns along b instead of a
+                int3 edge{}, nb{};
+                std::unique_ptr<DeviceBuffer> windows;
+                int entryBegin = 0, entryEnd = 0;
+            };
+            SiddonGrid grids_[3];
+            std::vector<unsigned> viewAxesHost_;
+            std::vector<int2> entries_;
+            std::unique_ptr<DeviceBuffer> dEntries_;
+            int axisPartials_ = 0;
+
+            // Per view and driving axis g: true when neighbouring pixels of the centre detector
+            // row spread more along b than along a on the planes of g.
+            bool rowAlongB(int p, int g) const
+            {
+                const float* P = poses_[p].v + kPoseOffPinv;
+                const float uc = det_.nu / 2 + 0.5f, vc = det_.nv / 2 + 0.5f;
+                float D[3], E[3];
+                for (int i = 0; i < 3; ++i) {
+                    D[i] = P[i * 3] * uc + P[i * 3 + 1] * vc + P[i * 3 + 2];
+                    E[i] = P[i * 3] * (uc + 1.0f) + P[i * 3 + 1] * vc + P[i * 3 + 2];
+                }
+                int a, b;
+                nonDrivingAxes(g, a, b);
+                if (std::fabs(D[g]) == 0.0f || std::fabs(E[g]) == 0.0f)
+                    return false;
+                const float da = std::fabs(E[a] / std::fabs(E[g]) - D[a] / std::fabs(D[g]));
+                const float db = std::fabs(E[b] / std::fabs(E[g]) - D[b] / std::fabs(D[g]));
+                return db > da;
+            }
+
+            void buildAxisGrids(CurvedMap cm)
+            {
+                viewAxesHost_.resize(det_.np);
+                ELSA_CUDA(cudaMemcpy(viewAxesHost_.data(), viewAxes_->as<unsigned>(),
+                                     sizeof(unsigned) * det_.np, cudaMemcpyDeviceToHost));
+                for (int g = 0; g < 3; ++g) {
+                    SiddonGrid& G = grids_[g];
+                    int votes = 0, alongB = 0;
+                    for (int p = 0; p < det_.np; ++p)
+                        if ((viewAxesHost_[p] >> g) & 1u) {
+                            ++votes;
+                            alongB += rowAlongB(p, g) ? 1 : 0;
+                        }
+                    G.present = votes > 0;
+                    if (!G.present)
+                        continue;
+                    G.ub = 2 * alongB > votes;
+                    int a, b;
+                    nonDrivingAxes(g, a, b);
+                    int e[3];
+                    e[g] = kSlab;
+                    e[a] = G.ub ? kAxisTV : kAxisTW;
+                    e[b] = G.ub ? kAxisTW : kAxisTV;
+                    G.edge = make_int3(e[0], e[1], e[2]);
+                    G.nb = make_int3((vol_.n[0] + e[0] - 1) / e[0], (vol_.n[1] + e[1] - 1) / e[1],
+                                     (vol_.n[2] + e[2] - 1) / e[2]);
+                    const int64_t nwin = static_cast<int64_t>(G.nb.x) * G.nb.y * G.nb.z * det_.np;
+                    G.windows = std::make_unique<DeviceBuffer>(sizeof(RayWindow) * nwin);
+                    launchBrickWindows(dPoses_, vol_, det_, G.edge, G.nb,
+                                       G.windows->as<RayWindow>(), nullptr, cm, kWindowSlack,
+                                       kWindowPixelMargin);
+                }
+            }
+
+            // (chunk, partial volume) entries per grid for adjointChunks_ view chunks (the
+            // chunks holding a view that drives along the grid's axis), partial volumes numbered
+            // by (chunk, axis); returns their number.
+            int buildAxisEntries()
+            {
+                const int per = (det_.np + adjointChunks_ - 1) / adjointChunks_;
+                const int used = (det_.np + per - 1) / per;
+                std::vector<std::vector<int2>> byGrid(3);
+                int next = 0;
+                for (int c = 0; c < used; ++c)
+                    for (int g = 0; g < 3; ++g) {
+                        if (!grids_[g].present)
+                            continue;
+                        bool any = false;
+                        for (int p = c * per; p < std::min(det_.np, (c + 1) * per) && !any; ++p)
+                            any = (viewAxesHost_[p] >> g) & 1u;
+                        if (any)
+                            byGrid[g].push_back(make_int2(c, next++));
+                    }
+                entries_.clear();
+                for (int g = 0; g < 3; ++g) {
+                    grids_[g].entryBegin = static_cast<int>(entries_.size());
+                    entries_.insert(entries_.end(), byGrid[g].begin(), byGrid[g].end());
+                    grids_[g].entryEnd = static_cast<int>(entries_.size());
+                }
+                if (next == 1)
+                    for (auto& e : entries_)
+                        e.y = 0;
+                dEntries_ = std::make_unique<DeviceBuffer>(sizeof(int2) *
+                                                           std::max<size_t>(1, entries_.size()));
+                if (!entries_.empty())
+                    ELSA_CUDA(cudaMemcpy(dEntries_->as<int2>(), entries_.data(),
+                                         sizeof(int2) * entries_.size(), cudaMemcpyHostToDevice));
+                axisPartials_ = next;
+                return next;
             }
 
             // View chunks: enough for bricks x chunks to reach kAdjointWarpsPerSm one-warp CTAs

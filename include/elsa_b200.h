@@ -169,7 +169,9 @@ elsa_status elsa_projector_sizes(const elsa_projector* projector, int64_t* domai
  * 2 = samples per forward pass (sum over rays of the Joseph step count), 3 = error word of the
  * device pipeline (0 = no timed-out wait; synchronizes), 4 = detector tiles on the gather
  * fallback of the staged forward, in parts per million, 5 = footprint mode of a voxel
- * projector, 6 / 7 = kernel launches per forward / adjoint call. */
+ * projector, 6 / 7 = kernel launches per forward / adjoint call, 8 = samples (Joseph taps, Siddon
+ * visits) of the brick-owner adjoint that fall outside the window of the brick that owns them
+ * (0 = every brick's ray list is complete; runs a check kernel and synchronizes). */
 elsa_status elsa_projector_info(const elsa_projector* projector, int32_t key, int64_t* value);
 
 /* Test hook of the bounded device waits (no counterpart in the reference, whose kernels do not
