@@ -45,7 +45,7 @@
 #define ELSA_ADJ_MIN_BLOCKS 1 // resident one-warp blocks per SM asked of the register allocator
 #endif
 #ifndef ELSA_ADJ_BATCH
-#define ELSA_ADJ_BATCH 2 // class rays per lane fetched together by the 3D adjoint (2 was fastest at 256^3 / 360 views)
+#define ELSA_ADJ_BATCH 3 // class rays per lane fetched together by the adjoints (3D axis bricks at 256^3 / 360 views: 1: 37.5 ms, 2: 33.5, 3: 33.0)
 #endif
 #ifndef ELSA_AXIS_TD
 #define ELSA_AXIS_TD 16 // depth along the driving axis of the 3D adjoint's axis bricks
