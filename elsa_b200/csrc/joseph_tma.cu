@@ -36,6 +36,21 @@ namespace elsa_b200
         constexpr int kStageFloats = BW * BH * BD;
         constexpr unsigned kStageBytes = kStageFloats * sizeof(float);
         constexpr int kFlagFallback = 8;
+#ifndef ELSA_FWD_FULLCHUNK
+#define ELSA_FWD_FULLCHUNK 0
+#endif
+#ifndef ELSA_FWD_NOCLAMP
+#define ELSA_FWD_NOCLAMP 0
+#endif
+
+        // Tap index of a box edge of E words. The box origins come from the same accumulated
+        // positions (tileSetupKernel), so i is in [0, E - 2] by construction; the clamp only
+        // guards against a disagreement between the two kernels.
+        template <int E>
+        __device__ __forceinline__ int boxIndex(int i)
+        {
+            return ELSA_FWD_NOCLAMP ? i : min(max(i, 0), E - 2);
+        }
 
         __device__ __forceinline__ int floorDivI(int a, int b)
         {
@@ -356,6 +371,27 @@ namespace elsa_b200
                 const int2 o = org[ch];
                 const float* buf = stage + s * kStageFloats;
                 const int jBase = ch * BD - c.t0;
+#if ELSA_FWD_FULLCHUNK
+                // chunks in which every ray of the warp has all BD samples: no per-sample test
+                if (__all_sync(0xffffffffu, ready && jBase >= 0 && jBase + BD <= c.n)) {
+#pragma unroll
+                    for (int kk = 0; kk < BD; ++kk) {
+                        const float ff = floorf(__fsub_rn(pf, 0.5f));
+                        const float fs = floorf(__fsub_rn(ps, 0.5f));
+                        const float cwf = __fsub_rn(__fsub_rn(pf, ff), 0.5f);
+                        const float cws = __fsub_rn(__fsub_rn(ps, fs), 0.5f);
+                        const float wf = __fsub_rn(1.0f, cwf), ws = __fsub_rn(1.0f, cws);
+                        const int lf = boxIndex<BW>(static_cast<int>(ff) - o.x);
+                        const int ls = boxIndex<BH>(static_cast<int>(fs) - o.y);
+                        const int lk = dir > 0 ? kk : BD - 1 - kk;
+                        const float* q = buf + (lk * BH + ls) * BW + lf;
+                        const float v00 = q[0], v10 = q[1], v01 = q[BW], v11 = q[BW + 1];
+                        acc += ws * (wf * v00 + cwf * v10) + cws * (wf * v01 + cwf * v11);
+                        pf = __fadd_rn(pf, c.sf);
+                        ps = __fadd_rn(ps, c.ss);
+                    }
+                } else
+#endif
 #pragma unroll
                 for (int kk = 0; kk < BD; ++kk) {
                     const int j = jBase + kk;
@@ -365,8 +401,8 @@ namespace elsa_b200
                         const float cwf = __fsub_rn(__fsub_rn(pf, ff), 0.5f);
                         const float cws = __fsub_rn(__fsub_rn(ps, fs), 0.5f);
                         const float wf = __fsub_rn(1.0f, cwf), ws = __fsub_rn(1.0f, cws);
-                        const int lf = min(max(static_cast<int>(ff) - o.x, 0), BW - 2);
-                        const int ls = min(max(static_cast<int>(fs) - o.y, 0), BH - 2);
+                        const int lf = boxIndex<BW>(static_cast<int>(ff) - o.x);
+                        const int ls = boxIndex<BH>(static_cast<int>(fs) - o.y);
                         const int lk = dir > 0 ? kk : BD - 1 - kk;
                         const float* q = buf + (lk * BH + ls) * BW + lf;
                         const float v00 = q[0], v10 = q[1], v01 = q[BW], v11 = q[BW + 1];

@@ -575,11 +575,20 @@ namespace elsa_b200
         // slab from its checkpoint.
         // ---------------------------------------------------------------------------------------
         constexpr int kAxisTW = 32, kAxisTV = 8;
+#ifndef ELSA_SIDDON_AXIS_BATCH
+#define ELSA_SIDDON_AXIS_BATCH 3 // class rays per lane whose records are fetched together
+#endif
+#ifndef ELSA_SIDDON_PLANE_ODD
+#define ELSA_SIDDON_PLANE_ODD 0 // 1: plane stride padded to 1 modulo 32
+#endif
+        constexpr int kSiddonAxisBatch = ELSA_SIDDON_AXIS_BATCH;
 
         struct SiddonAxisBrick {
             static constexpr int kRow = kAxisTW + 1; // columns (+1: rows land in other banks)
             static constexpr int kPlaneMin = kRow * kAxisTV;
-            static constexpr int kPlane = kPlaneMin + ((33 - kPlaneMin % 32) % 32);
+            // unpadded planes keep the brick at 16.9 KB (12 resident per SM instead of 11)
+            static constexpr int kPlane =
+                ELSA_SIDDON_PLANE_ODD ? kPlaneMin + ((33 - kPlaneMin % 32) % 32) : kPlaneMin;
             static constexpr int kWords = kPlane * kSlab;
         };
 
@@ -631,17 +640,24 @@ namespace elsa_b200
             const int s0 = axisStep(meta, 0), s1 = axisStep(meta, 1), s2 = axisStep(meta, 2);
             float T0 = cp.x, T1 = cp.y, T2 = cp.z;
             float tEntry = cp.w;
+            // software-pipelined: the word of a visit is read before the sum of the previous
+            // visit (always another voxel) is written back
+            int prevOff = 0;
+            float prevVal = 0.0f, prevW = 0.0f;
+            bool prevIn = false;
             for (int it = 0; it < 3 * kSlab + 3; ++it) {
                 bool m0, m1, m2;
                 const float tExit = nextCrossing<3>(T0, T1, T2, m0, m1, m2);
                 const int c[3] = {c0, c1, c2};
                 const int lg = c[G] - kLo, la = c[a] - orgA, lb = c[b] - orgB;
-                if (static_cast<unsigned>(la) < static_cast<unsigned>(EA) &&
-                    static_cast<unsigned>(lb) < static_cast<unsigned>(EB)) {
-                    float* adr = acc + lg * L::kPlane + la * SA + lb * SB;
-                    const float w = binary ? 1.0f : __fsub_rn(tExit, tEntry);
-                    *adr = __fadd_rn(*adr, __fmul_rn(yv, w));
-                }
+                const bool in = static_cast<unsigned>(la) < static_cast<unsigned>(EA) &&
+                                static_cast<unsigned>(lb) < static_cast<unsigned>(EB);
+                const int off = lg * L::kPlane + la * SA + lb * SB;
+                const float val = in ? acc[off] : 0.0f;
+                if (prevIn)
+                    acc[prevOff] = __fadd_rn(prevVal, __fmul_rn(yv, prevW));
+                prevOff = off, prevVal = val, prevIn = in;
+                prevW = binary ? 1.0f : __fsub_rn(tExit, tEntry);
                 if (m0) {
                     c0 += s0;
                     T0 = __fadd_rn(T0, tDelta.x);
@@ -663,6 +679,8 @@ namespace elsa_b200
                     break;
                 tEntry = tExit;
             }
+            if (prevIn)
+                acc[prevOff] = __fadd_rn(prevVal, __fmul_rn(yv, prevW));
         }
 
         template <int G, bool UB>
@@ -705,26 +723,49 @@ namespace elsa_b200
                         const int uStart = w.u0 + ou;
                         const int nuc = uStart <= w.u1 ? (w.u1 - uStart) / m + 1 : 0;
                         const int total = nuc * nvc;
-                        for (int i = lane; i < total; i += 32) {
-                            const int iv = i / nuc;
-                            const int iu = i - iv * nuc;
-                            const int64_t r = viewBase + (uStart + iu * m) +
-                                              static_cast<int64_t>(J.det.nu) * (vStart + iv * m);
-                            const int4* rp = reinterpret_cast<const int4*>(J.rays + r);
-                            const int4 q0 = __ldg(rp);     // tDelta[3], meta
-                            const int4 q1 = __ldg(rp + 1); // kFirst, kLast, cur[2]
-                            const int meta = q0.w;
-                            if (!(meta & kActive) || (meta & 3) != G)
-                                continue;
-                            if (max(q1.x, q1.y) < kLo || min(q1.x, q1.y) > kHi)
-                                continue;
-                            const float3 td =
-                                make_float3(__int_as_float(q0.x), __int_as_float(q0.y),
-                                            __int_as_float(q0.z));
-                            splatAxisSegment<G, UB>(acc, td, meta, q1.x,
-                                                    __ldg(J.cpState + cpRow + r),
-                                                    __ldg(J.cpVoxel + cpRow + r), __ldg(J.y + r),
-                                                    kLo, org[a], org[b], J.vol, J.binary);
+                        const float invNuc = nuc > 0 ? 1.0f / static_cast<float>(nuc) : 0.0f;
+                        constexpr int kB = kSiddonAxisBatch;
+                        for (int base = lane; base < total; base += 32 * kB) {
+                            // the records of kB class rays first, then their visits in turn
+                            int4 q0[kB], q1[kB];
+                            float4 cps[kB];
+                            unsigned cpvs[kB];
+                            float ys[kB];
+#pragma unroll
+                            for (int q = 0; q < kB; ++q) {
+                                const int i = base + 32 * q;
+                                q0[q].w = 0;
+                                if (i < total) {
+                                    // i / nuc by a float reciprocal: exact for i < 2^20,
+                                    // nuc < 2^11
+                                    const int iv = static_cast<int>(
+                                        (static_cast<float>(i) + 0.5f) * invNuc);
+                                    const int iu = i - iv * nuc;
+                                    const int64_t r =
+                                        viewBase + (uStart + iu * m) +
+                                        static_cast<int64_t>(J.det.nu) * (vStart + iv * m);
+                                    const int4* rp = reinterpret_cast<const int4*>(J.rays + r);
+                                    q0[q] = __ldg(rp);     // tDelta[3], meta
+                                    q1[q] = __ldg(rp + 1); // kFirst, kLast, cur[2]
+                                    cps[q] = __ldg(J.cpState + cpRow + r);
+                                    cpvs[q] = __ldg(J.cpVoxel + cpRow + r);
+                                    ys[q] = __ldg(J.y + r);
+                                }
+                            }
+#pragma unroll
+                            for (int q = 0; q < kB; ++q) {
+                                const int meta = q0[q].w;
+                                if (!(meta & kActive) || (meta & 3) != G)
+                                    continue;
+                                if (max(q1[q].x, q1[q].y) < kLo || min(q1[q].x, q1[q].y) > kHi)
+                                    continue;
+                                const float3 td = make_float3(__int_as_float(q0[q].x),
+                                                              __int_as_float(q0[q].y),
+                                                              __int_as_float(q0[q].z));
+                                splatAxisSegment<G, UB>(acc, td, meta, q1[q].x, cps[q], cpvs[q],
+                                                        ys[q], kLo, org[a], org[b], J.vol,
+                                                        J.binary);
+                            }
                         }
                         __syncwarp();
                     }
