@@ -39,6 +39,9 @@ namespace elsa_b200
         constexpr int kVoxelThreads = 256;      // forward: one thread per brick voxel; adjoint default
         constexpr int kMaxAdjointThreads = 512; // largest adjoint block the autotuner may choose
         constexpr int kPatchWords = 2304; // 9 KB shared detector patch (48 x 48 pixels)
+#ifndef ELSA_VOXEL_ADJ_FAST
+#define ELSA_VOXEL_ADJ_FAST 0
+#endif
 
         struct VoxelParams {
             int dim;
@@ -218,7 +221,7 @@ namespace elsa_b200
 
         // Adjoint: x[v] = sum over poses and footprint pixels of w * y[pixel], in the reference's
         // order (VoxelComputation.h:152-183). One thread per voxel, x fastest within a block.
-        template <int DIM>
+        template <int DIM, bool Fast = (ELSA_VOXEL_ADJ_FAST != 0)>
         __global__ void __launch_bounds__(kMaxAdjointThreads)
             voxelAdjointKernel(const float* __restrict__ poses, int np,
                                const float* __restrict__ lutIn, VoxelParams vp, VolumeShape vol,
@@ -243,8 +246,9 @@ namespace elsa_b200
                 const Footprint f = footprint<DIM>(poses + static_cast<int64_t>(p) * 40, ix, iy,
                                                    iz, vp);
                 const float* view = y + p * npix;
-                visitFootprint<DIM>(f, vp, [&](int64_t pix, int pu_, int pv_, float d0, float d1) {
-                    const float w = voxelWeight<DIM>(lut, vp, d0, d1);
+                visitFootprint<DIM, Fast>(f, vp, [&](int64_t pix, int pu_, int pv_, float d0,
+                                                     float d1) {
+                    const float w = voxelWeight<DIM, Fast>(lut, vp, d0, d1);
                     acc = acc + w * __ldg(view + pix);
                 });
             }
