@@ -27,7 +27,8 @@ namespace elsa_b200
         kKnobAdjointChunks = 1,  // view chunks of a brick-owner adjoint (partial volumes)
         kKnobAdjointThreads = 2, // voxels per block of a thread-per-voxel adjoint kernel
         kKnobAdjointScatter = 3, // 0: deterministic brick-owner adjoint, 1: atomic scatter
-        kKnobCount = 4
+        kKnobExactWeights = 4,   // voxel adjoint: 0 the forward's weights, 1 the reference's
+        kKnobCount = 5
     };
 
     // A curved (cylindrical) detector: opening angle (radian) and source-to-detector distance

@@ -69,13 +69,12 @@ namespace elsa_b200
         __device__ __forceinline__ float nextCrossing(float T0, float T1, float T2, bool& m0,
                                                       bool& m1, bool& m2)
         {
-            float tm = T0;
-            tm = (T1 < tm) ? T1 : tm;
-            if (DIM == 3)
-                tm = (T2 < tm) ? T2 : tm;
-            m0 = (T0 <= T1) && (DIM < 3 || T0 <= T2);
-            m1 = (T1 <= T0) && (DIM < 3 || T1 <= T2);
-            m2 = DIM == 3 && (T2 <= T0) && (T2 <= T1);
+            // an axis crosses when its T is the minimum (T0 <= T1 && T0 <= T2 and so on: the T
+            // are never NaN, FLT_MAX for an axis the ray does not cross)
+            const float tm = DIM == 3 ? fminf(T0, fminf(T1, T2)) : fminf(T0, T1);
+            m0 = T0 == tm;
+            m1 = T1 == tm;
+            m2 = DIM == 3 && T2 == tm;
             return tm;
         }
 
@@ -574,7 +573,10 @@ namespace elsa_b200
         // entry), the window's rays class by class, each lane replaying one ray's visits of the
         // slab from its checkpoint.
         // ---------------------------------------------------------------------------------------
-        constexpr int kAxisTW = 32, kAxisTV = 8;
+#ifndef ELSA_SIDDON_AXIS_TV
+#define ELSA_SIDDON_AXIS_TV 8 // rows of a Siddon axis brick
+#endif
+        constexpr int kAxisTW = 32, kAxisTV = ELSA_SIDDON_AXIS_TV;
 #ifndef ELSA_SIDDON_AXIS_BATCH
 #define ELSA_SIDDON_AXIS_BATCH 1 // class rays per lane whose records are fetched together
                                  // (256^3 / 360 views: 1: 44.6 ms, 2: 50.6, 3: 50.3; the
@@ -642,6 +644,12 @@ namespace elsa_b200
             const int s0 = axisStep(meta, 0), s1 = axisStep(meta, 1), s2 = axisStep(meta, 2);
             float T0 = cp.x, T1 = cp.y, T2 = cp.z;
             float tEntry = cp.w;
+            // the walk stays inside the volume and the slab: along G the two tests are one,
+            // kLo <= cg < min(kLo + kSlab, n_G)
+            const int nA = a == 0 ? vol.n[0] : (a == 1 ? vol.n[1] : vol.n[2]);
+            const int nB = b == 1 ? vol.n[1] : vol.n[2];
+            const int nG = G == 0 ? vol.n[0] : (G == 1 ? vol.n[1] : vol.n[2]);
+            const unsigned spanG = static_cast<unsigned>(min(kLo + kSlab, nG) - kLo);
             // software-pipelined: the word of a visit is read before the sum of the previous
             // visit (always another voxel) is written back
             int prevOff = 0;
@@ -672,12 +680,10 @@ namespace elsa_b200
                     c2 += s2;
                     T2 = __fadd_rn(T2, tDelta.z);
                 }
-                const bool inside =
-                    static_cast<unsigned>(c0) < static_cast<unsigned>(vol.n[0]) &&
-                    static_cast<unsigned>(c1) < static_cast<unsigned>(vol.n[1]) &&
-                    static_cast<unsigned>(c2) < static_cast<unsigned>(vol.n[2]);
-                const int cg = G == 0 ? c0 : (G == 1 ? c1 : c2);
-                if (!inside || cg < kLo || cg >= kLo + kSlab)
+                const int cn[3] = {c0, c1, c2};
+                if (static_cast<unsigned>(cn[a]) >= static_cast<unsigned>(nA) ||
+                    static_cast<unsigned>(cn[b]) >= static_cast<unsigned>(nB) ||
+                    static_cast<unsigned>(cn[G] - kLo) >= spanG)
                     break;
                 tEntry = tExit;
             }
@@ -853,6 +859,18 @@ namespace elsa_b200
                 nBricks_ = make_int3((vol_.n[0] + kSlab - 1) / kSlab,
                                      (vol_.n[1] + kSlab - 1) / kSlab, (vol_.n[2] + bz - 1) / bz);
                 adjointChunks_ = defaultChunks();
+                // The deterministic brick-owner adjoint is the default wherever it exists (a
+                // valid class spacing) and its per-(ray, slab) checkpoints (20 B each: about
+                // 20 GB at 256^3 / 360 x 384^2) take at most a quarter of the device's memory and
+                // half of what is free; otherwise the atomic scatter.
+                if (classSpacing_ > 0) {
+                    size_t freeBytes = 0, totalBytes = 0;
+                    ELSA_CUDA(cudaMemGetInfo(&freeBytes, &totalBytes));
+                    const double need = 20.0 * static_cast<double>(nrays) * cpRows_;
+                    if (need <= 0.25 * static_cast<double>(totalBytes) &&
+                        need <= 0.5 * static_cast<double>(freeBytes))
+                        setKnob(kKnobAdjointScatter, 0);
+                }
                 ELSA_CUDA(cudaDeviceSynchronize());
             }
 
@@ -1261,7 +1279,7 @@ namespace elsa_b200
 
             std::unique_ptr<DeviceBuffer> partial_; // adjoint: per view-chunk partial volumes
             int adjointChunks_ = 1;
-            int scatter_ = 1; // the atomic scatter adjoint by default (2.6x faster at 256^3)
+            int scatter_ = 1; // until the constructor selects the brick owner (see there)
             int forwardThreads_ = kForwardThreads;
             int binary_ = 0;
             CurvedDetector curved_;

@@ -39,9 +39,6 @@ namespace elsa_b200
         constexpr int kVoxelThreads = 256;      // forward: one thread per brick voxel; adjoint default
         constexpr int kMaxAdjointThreads = 512; // largest adjoint block the autotuner may choose
         constexpr int kPatchWords = 2304; // 9 KB shared detector patch (48 x 48 pixels)
-#ifndef ELSA_VOXEL_ADJ_FAST
-#define ELSA_VOXEL_ADJ_FAST 0
-#endif
 
         struct VoxelParams {
             int dim;
@@ -145,7 +142,11 @@ namespace elsa_b200
         // Fast (forward only): the distance as n2 * rsqrt(n2) and the lerp as one fma, within a
         // few ulp of the reference's weights; the forward's sums are reordered by atomics
         // anyway, while the adjoint keeps every float operation of the reference.
-        template <int DIM, bool Fast = false>
+        // WK: weight kind (-1: read vp.weightKind; 0 classic, 1 differential). The fast lerp
+        // always reads lut[a + 1]: the staged table carries one padding entry, and at an integer
+        // index the factor (index - a) is 0, so the result equals the reference's
+        // lut[a] + 0 * (lut[ceil] - lut[a]).
+        template <int DIM, bool Fast = false, int WK = -1>
         __device__ __forceinline__ float voxelWeight(const float* lut, const VoxelParams& vp,
                                                      float d0, float d1)
         {
@@ -157,19 +158,19 @@ namespace elsa_b200
                 const float dist = n2 > 0.0f ? __fmul_rn(n2, rsqrtf(n2)) : 0.0f;
                 const float q = vp.invRadius != 0.0f ? dist * vp.invRadius : dist / vp.radius;
                 const float index = q * static_cast<float>(kVoxelLutSize - 1);
-                if (index < 0.0f || index > static_cast<float>(kVoxelLutSize - 1)) {
+                if (!(index <= static_cast<float>(kVoxelLutSize - 1))) { // index >= 0 here
                     v = 0.0f;
                 } else {
                     const float af = floorf(index);
                     const int a = static_cast<int>(af);
-                    const int b = a + (index > af ? 1 : 0);
                     const float fa = lut[a];
-                    v = __fmaf_rn(index - af, lut[b] - fa, fa);
+                    v = __fmaf_rn(index - af, lut[a + 1] - fa, fa);
                 }
             } else {
                 v = lutAt(lut, vp.radius, vp.invRadius, sqrtf(n2));
             }
-            if (vp.weightKind == 0)
+            const int wk = WK >= 0 ? WK : vp.weightKind;
+            if (wk == 0)
                 return v;
             if (DIM == 2)
                 return v * static_cast<float>((0.0f < d0) - (d0 < 0.0f));
@@ -219,40 +220,40 @@ namespace elsa_b200
             }
         }
 
-        // Adjoint: x[v] = sum over poses and footprint pixels of w * y[pixel], in the reference's
-        // order (VoxelComputation.h:152-183). One thread per voxel, x fastest within a block.
-        template <int DIM, bool Fast = (ELSA_VOXEL_ADJ_FAST != 0)>
-        __global__ void __launch_bounds__(kMaxAdjointThreads)
-            voxelAdjointKernel(const float* __restrict__ poses, int np,
-                               const float* __restrict__ lutIn, VoxelParams vp, VolumeShape vol,
-                               const float* __restrict__ y, float* __restrict__ x)
+        // visitFootprint for a footprint whose visited pixels lie inside the detector (visitBox
+        // true): the same pixels in the same order with the same offsets (Fast), without the
+        // linear index. In the reference loop with a sheared block, rows past the detector's
+        // last row are where the linear index would leave the view: they are not visited.
+        template <int DIM, class Fn>
+        __device__ __forceinline__ void visitFootprintInside(const Footprint& f,
+                                                             const VoxelParams& vp, Fn fn)
         {
-            __shared__ float lut[kVoxelLutSize];
-            for (int i = threadIdx.x; i < kVoxelLutSize; i += blockDim.x)
-                lut[i] = lutIn[i];
-            __syncthreads();
-            const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
-            const int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-            if (v >= nvox)
+            const float invS = 1.0f / f.s;
+            if (DIM == 2) {
+                for (int u = f.lo0; u <= f.hi0; ++u)
+                    fn(u, 0, __fmul_rn(f.c0 - static_cast<float>(u), invS), 0.0f);
                 return;
-            const int ix = static_cast<int>(v % vol.n[0]);
-            const int iy = static_cast<int>((v / vol.n[0]) % vol.n[1]);
-            const int iz = DIM == 3 ? static_cast<int>(v / (static_cast<int64_t>(vol.n[0]) *
-                                                            vol.n[1]))
-                                    : 0;
-            const int64_t npix = static_cast<int64_t>(vp.nu) * vp.nv;
-            float acc = 0.0f;
-            for (int p = 0; p < np; ++p) {
-                const Footprint f = footprint<DIM>(poses + static_cast<int64_t>(p) * 40, ix, iy,
-                                                   iz, vp);
-                const float* view = y + p * npix;
-                visitFootprint<DIM, Fast>(f, vp, [&](int64_t pix, int pu_, int pv_, float d0,
-                                                     float d1) {
-                    const float w = voxelWeight<DIM, Fast>(lut, vp, d0, d1);
-                    acc = acc + w * __ldg(view + pix);
-                });
             }
-            x[v] = acc;
+            const int ext0 = f.hi0 - f.lo0 + 1, ext1 = f.hi1 - f.lo1 + 1;
+            if (ext0 <= 0 || ext1 <= 0)
+                return;
+            const bool ref = vp.mode == static_cast<int>(FootprintMode::Reference);
+            const int rows = min(ref ? ext0 : ext1, vp.nv - f.lo1);
+            const int cols = ref ? ext1 : ext0;
+            float cur0 = static_cast<float>(f.lo0), cur1 = static_cast<float>(f.lo1);
+            int u = f.lo0, v = f.lo1;
+            for (int r = 0; r < rows; ++r) {
+                const float d1 = __fmul_rn(f.c1 - cur1, invS);
+                for (int c = 0; c < cols; ++c) {
+                    fn(u, v, __fmul_rn(f.c0 - cur0, invS), d1);
+                    u += 1;
+                    cur0 = cur0 + 1.0f;
+                }
+                u -= ext0;
+                v += 1;
+                cur0 = cur0 - static_cast<float>(ext0);
+                cur1 = cur1 + 1.0f;
+            }
         }
 
         // Bounding box (u0, u1, v0, v1) of the pixels a footprint visits; false when the visit
@@ -277,17 +278,75 @@ namespace elsa_b200
             return u0 >= 0 && u1 < vp.nu;
         }
 
+        // visitBox's test alone: the footprint's visited pixels stay inside the detector's rows.
+        template <int DIM>
+        __device__ __forceinline__ bool footprintInside(const Footprint& f, const VoxelParams& vp)
+        {
+            const int ext0 = f.hi0 - f.lo0 + 1, ext1 = f.hi1 - f.lo1 + 1;
+            if (DIM == 2 || vp.mode != static_cast<int>(FootprintMode::Reference) ||
+                ext0 == ext1)
+                return true;
+            const int shift = (ext0 - 1) * (ext1 - ext0);
+            return f.lo0 + min(0, shift) >= 0 && f.lo0 + max(0, shift) + ext1 - 1 < vp.nu;
+        }
+
+        // Adjoint: x[v] = sum over poses and footprint pixels of w * y[pixel], in the reference's
+        // order (VoxelComputation.h:152-183). One thread per voxel, x fastest within a block.
+        // Fast: the forward's weights (the default); otherwise the reference's float
+        // operations, bit-identical to its CPU loop.
+        template <int DIM, bool Fast, int WK>
+        __global__ void __launch_bounds__(kMaxAdjointThreads, 2)
+            voxelAdjointKernel(const float* __restrict__ poses, int np,
+                               const float* __restrict__ lutIn, VoxelParams vp, VolumeShape vol,
+                               const float* __restrict__ y, float* __restrict__ x)
+        {
+            __shared__ float lut[kVoxelLutSize + 1]; // + 1 padding entry for the fast lerp
+            for (int i = threadIdx.x; i <= kVoxelLutSize; i += blockDim.x)
+                lut[i] = lutIn[min(i, kVoxelLutSize - 1)];
+            __syncthreads();
+            const int64_t nvox = static_cast<int64_t>(vol.n[0]) * vol.n[1] * vol.n[2];
+            const int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (v >= nvox)
+                return;
+            const int ix = static_cast<int>(v % vol.n[0]);
+            const int iy = static_cast<int>((v / vol.n[0]) % vol.n[1]);
+            const int iz = DIM == 3 ? static_cast<int>(v / (static_cast<int64_t>(vol.n[0]) *
+                                                            vol.n[1]))
+                                    : 0;
+            const int64_t npix = static_cast<int64_t>(vp.nu) * vp.nv;
+            float acc = 0.0f;
+            for (int p = 0; p < np; ++p) {
+                const Footprint f = footprint<DIM>(poses + static_cast<int64_t>(p) * 40, ix, iy,
+                                                   iz, vp);
+                const float* view = y + p * npix;
+                if (Fast && footprintInside<DIM>(f, vp)) {
+                    // the same pixels in the same order, without the linear index
+                    visitFootprintInside<DIM>(f, vp, [&](int pu_, int pv_, float d0, float d1) {
+                        const float w = voxelWeight<DIM, true, WK>(lut, vp, d0, d1);
+                        acc = acc + w * __ldg(view + pv_ * vp.nu + pu_);
+                    });
+                    continue;
+                }
+                visitFootprint<DIM, Fast>(f, vp, [&](int64_t pix, int pu_, int pv_, float d0,
+                                                     float d1) {
+                    const float w = voxelWeight<DIM, Fast, WK>(lut, vp, d0, d1);
+                    acc = acc + w * __ldg(view + pix);
+                });
+            }
+            x[v] = acc;
+        }
+
         // Forward: one CTA per (brick of voxels, pose). Voxels splat into a shared patch of the
         // detector (shared atomics); the patch is added to the sinogram with global atomics.
         // Voxels whose footprint leaves the patch add to the sinogram directly.
-        template <int DIM, int BX, int BY, int BZ>
+        template <int DIM, int BX, int BY, int BZ, int WK>
         __global__ void __launch_bounds__(kVoxelThreads)
             voxelForwardKernel(const float* __restrict__ poses, const float* __restrict__ lutIn,
                                VoxelParams vp, VolumeShape vol, int3 nBricks,
                                const float* __restrict__ x, float* __restrict__ y)
         {
             static_assert(BX * BY * BZ == kVoxelThreads, "one thread per brick voxel");
-            __shared__ float lut[kVoxelLutSize];
+            __shared__ float lut[kVoxelLutSize + 1]; // + 1 padding entry for the fast lerp
             __shared__ float patch[kPatchWords];
             __shared__ int box[4]; // u0, -u1, v0, -v1 (atomicMin on all four)
             const int p = blockIdx.y;
@@ -297,8 +356,8 @@ namespace elsa_b200
             const int tx = threadIdx.x % BX, ty = (threadIdx.x / BX) % BY,
                       tz = threadIdx.x / (BX * BY);
             const int ix = bx * BX + tx, iy = by * BY + ty, iz = bz * BZ + tz;
-            for (int i = threadIdx.x; i < kVoxelLutSize; i += blockDim.x)
-                lut[i] = lutIn[i];
+            for (int i = threadIdx.x; i <= kVoxelLutSize; i += blockDim.x)
+                lut[i] = lutIn[min(i, kVoxelLutSize - 1)];
             if (threadIdx.x < 4)
                 box[threadIdx.x] = INT_MAX;
             __syncthreads();
@@ -338,19 +397,20 @@ namespace elsa_b200
             }
             __syncthreads();
             if (active) {
-                const bool toPatch = usePatch && boxed;
-                visitFootprint<DIM, true>(f, vp, [&](int64_t pix, int pu_, int pv_, float d0,
-                                                     float d1) {
-                    const float w = voxelWeight<DIM, true>(lut, vp, d0, d1);
-                    const float c = xv * w;
-                    if (toPatch) {
-                        // a boxed footprint stays inside its rows: the unwrapped coordinates
-                        // are the pixel's own
-                        atomicAdd(&patch[(pv_ - bv0) * pw + (pu_ - bu0)], c);
-                    } else {
-                        atomicAdd(view + pix, c);
-                    }
-                });
+                if (usePatch && boxed) {
+                    // a boxed footprint stays inside the detector and its rows: no linear
+                    // index to test
+                    visitFootprintInside<DIM>(f, vp, [&](int pu_, int pv_, float d0, float d1) {
+                        const float w = voxelWeight<DIM, true, WK>(lut, vp, d0, d1);
+                        atomicAdd(&patch[(pv_ - bv0) * pw + (pu_ - bu0)], xv * w);
+                    });
+                } else {
+                    visitFootprint<DIM, true>(f, vp, [&](int64_t pix, int pu_, int pv_, float d0,
+                                                         float d1) {
+                        const float w = voxelWeight<DIM, true, WK>(lut, vp, d0, d1);
+                        atomicAdd(view + pix, xv * w);
+                    });
+                }
             }
             if (usePatch) {
                 __syncthreads();
@@ -398,8 +458,12 @@ namespace elsa_b200
                 ELSA_CUDA(cudaMemsetAsync(y, 0, sizeof(float) * rangeSize_, s));
                 const dim3 grid(static_cast<unsigned>(nBricks_.x * nBricks_.y * nBricks_.z),
                                 static_cast<unsigned>(det_.np));
-                voxelForwardKernel<DIM, kBX, kBY, kBZ><<<grid, kVoxelThreads, 0, s>>>(
-                    dPoses_, lut_.as<float>(), vp_, vol_, nBricks_, x, y);
+                if (vp_.weightKind == 0)
+                    voxelForwardKernel<DIM, kBX, kBY, kBZ, 0><<<grid, kVoxelThreads, 0, s>>>(
+                        dPoses_, lut_.as<float>(), vp_, vol_, nBricks_, x, y);
+                else
+                    voxelForwardKernel<DIM, kBX, kBY, kBZ, 1><<<grid, kVoxelThreads, 0, s>>>(
+                        dPoses_, lut_.as<float>(), vp_, vol_, nBricks_, x, y);
                 ELSA_LAUNCH_CHECK("voxelForwardKernel");
             }
 
@@ -407,8 +471,21 @@ namespace elsa_b200
             {
                 const unsigned blocks =
                     static_cast<unsigned>((domainSize_ + adjointThreads_ - 1) / adjointThreads_);
-                voxelAdjointKernel<DIM><<<blocks, adjointThreads_, 0, s>>>(
-                    dPoses_, det_.np, lut_.as<float>(), vp_, vol_, y, x);
+#define ELSA_VOXEL_ADJOINT(FAST_, WK_)                                                      \
+    voxelAdjointKernel<DIM, FAST_, WK_><<<blocks, adjointThreads_, 0, s>>>(                    \
+        dPoses_, det_.np, lut_.as<float>(), vp_, vol_, y, x)
+                if (exactWeights_) {
+                    if (vp_.weightKind == 0)
+                        ELSA_VOXEL_ADJOINT(false, 0);
+                    else
+                        ELSA_VOXEL_ADJOINT(false, 1);
+                } else {
+                    if (vp_.weightKind == 0)
+                        ELSA_VOXEL_ADJOINT(true, 0);
+                    else
+                        ELSA_VOXEL_ADJOINT(true, 1);
+                }
+#undef ELSA_VOXEL_ADJOINT
                 ELSA_LAUNCH_CHECK("voxelAdjointKernel");
             }
 
@@ -432,12 +509,18 @@ namespace elsa_b200
             {
                 if (knob == kKnobAdjointThreads)
                     return {64, 128, 256, 512};
+                if (knob == kKnobExactWeights)
+                    return {0, 1};
                 return {};
             }
 
             int knob(int knob) const override
             {
-                return knob == kKnobAdjointThreads ? adjointThreads_ : -1;
+                if (knob == kKnobAdjointThreads)
+                    return adjointThreads_;
+                if (knob == kKnobExactWeights)
+                    return exactWeights_;
+                return -1;
             }
 
             void setKnob(int knob, int value) override
@@ -447,11 +530,17 @@ namespace elsa_b200
                     throw Error(ELSA_ERROR_INVALID_ARGUMENT,
                                 "voxel projector: value " + std::to_string(value) +
                                     " is not a candidate of knob " + std::to_string(knob));
-                adjointThreads_ = value;
+                if (knob == kKnobExactWeights)
+                    exactWeights_ = value;
+                else
+                    adjointThreads_ = value;
             }
 
         private:
             int adjointThreads_ = kVoxelThreads; // voxels per block of the gather adjoint
+            // 0: the adjoint uses the forward's weights (128^3 blob: 21.7 ms); 1: the reference's
+            // float operations, bit-identical to elsa's CPU loop (26.0 ms)
+            int exactWeights_ = 0;
             // forward bricks: 8 x 8 x 4 voxels in 3D, 16 x 16 in 2D (one thread per voxel)
             static constexpr int kBX = DIM == 3 ? 8 : 16;
             static constexpr int kBY = DIM == 3 ? 8 : 16;

@@ -197,10 +197,20 @@ elsa_status elsa_projector_wait_test(elsa_projector* projector, int64_t waitCycl
 /* Adjoint scheme of Joseph (matched adjoint), Siddon and BinaryMethod: 0 = deterministic
  * brick-owner kernel (bit-reproducible), 1 = thread-per-ray atomic scatter, the reference's own
  * scheme (SiddonsMethod.cpp:119 `omp atomic`, TraverseSiddonsCUDA.cu atomicAdd): the same sums
- * in an order that varies from run to run. Defaults: 1 for Siddon / BinaryMethod (2.6x faster at
- * 256^3), 0 for Joseph (the scatter is faster only in 2D). */
+ * in an order that varies from run to run. Default 0 for Joseph; for Siddon / BinaryMethod 0 when
+ * the brick owner exists for the geometry (a valid class spacing) and its checkpoint tables
+ * (20 bytes per ray and 16-plane slab, about 20 GB at 256^3 / 360 x 384^2) take at most a quarter
+ * of the device's memory and half of the free memory at creation, else 1. At 256^3 the Siddon
+ * brick owner takes 1.27x the scatter's time. */
 #define ELSA_KNOB_ADJOINT_SCATTER 3
-#define ELSA_KNOB_COUNT 4
+/* Weights of the voxel projectors' adjoint (blob, B-spline and their phase-contrast forms):
+ * 0 = the forward's weights (distance as n2 * rsqrt(n2), scaling applied as a multiplication by
+ * 1 / s, the table lerp as one fma; within a few ulp of the reference's, and forward and adjoint
+ * then use the same weights), 1 = the reference's float operations (VoxelComputation.h:55-185),
+ * the adjoint bit-identical to elsa's CPU loop. Default 0 (1.2x faster). Either way the adjoint
+ * is deterministic. */
+#define ELSA_KNOB_EXACT_WEIGHTS 4
+#define ELSA_KNOB_COUNT 5
 
 /* Current value of `knob` (-1: the projector does not use it). */
 elsa_status elsa_projector_get_knob(const elsa_projector* projector, int32_t knob,

@@ -84,7 +84,9 @@ def test_siddon_adjointness_and_determinism(cuda, oracle, name):
     x = rng.uniform(0, 1, int(np.prod(c["vol"]))).astype(np.float32)
     y = rng.uniform(0, 1, int(np.prod(det))).astype(np.float32)
     import elsa_b200
-    Ax, Aty = _gpu_pair(cuda, proj, x, y)  # the default scatter adjoint
+    assert proj.knob(elsa_b200.KNOB_ADJOINT_SCATTER) == 0  # default: the brick owner
+    proj.set_knob(elsa_b200.KNOB_ADJOINT_SCATTER, 1)
+    Ax, Aty = _gpu_pair(cuda, proj, x, y)  # the scatter adjoint
     lhs = float(Ax.astype(np.float64) @ y)
     rhs = float(x.astype(np.float64) @ Aty)
     assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
@@ -115,7 +117,9 @@ def test_scatter_adjoint_parity(cuda, oracle, name, binary):
     x = rng.uniform(0, 1, int(np.prod(c["vol"]))).astype(np.float32)
     y = rng.uniform(0, 1, int(np.prod(det))).astype(np.float32)
     y[::7] = 0.0  # rays with nothing to add are skipped
-    assert proj.knob(elsa_b200.KNOB_ADJOINT_SCATTER) == 1 and proj.info(7) == 1  # default
+    assert proj.knob(elsa_b200.KNOB_ADJOINT_SCATTER) == 0  # default: the brick owner
+    proj.set_knob(elsa_b200.KNOB_ADJOINT_SCATTER, 1)  # releases the owner's tables
+    assert proj.info(7) == 1
     assert proj.knob_candidates(elsa_b200.KNOB_ADJOINT_CHUNKS) == []
     _, a_scatter = _gpu_pair(cuda, proj, x, y)
     proj.set_knob(elsa_b200.KNOB_ADJOINT_SCATTER, 0)  # builds the brick-owner adjoint

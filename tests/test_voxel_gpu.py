@@ -60,18 +60,23 @@ def test_voxel_parity(cuda, oracle, cfg, name, mode):
     rng = np.random.default_rng(21)
     x = rng.uniform(0, 1, int(np.prod(vol))).astype(np.float32)
     y = rng.uniform(0, 1, int(np.prod(det))).astype(np.float32)
+    import elsa_b200
     Ax, Aty = _pair(cuda, proj, x, y)
     lut, support, wk = oracle.voxel_lut(name, len(vol))
     ref_Ax = oracle.voxel_project(False, x, vol, det, poses, lut, support, wk, mode)
     ref_Aty = oracle.voxel_project(True, y, vol, det, poses, lut, support, wk, mode)
     d_Ax = oracle.voxel_project(False, x, vol, det, poses, lut, support, wk, mode, np.float64)
     e_fwd, e_adj = rel_l2(Ax, ref_Ax), rel_l2(Aty, ref_Aty)
-    mism = int(np.count_nonzero(Aty.view(np.uint32) != ref_Aty.view(np.uint32)))
-    print("%s %s mode %d: fwd %.3g adj %.3g (fwd vs f64 %.3g), adjoint bit mismatches %d"
-          % (cfg, name, mode, e_fwd, e_adj, rel_l2(Ax, d_Ax), mism))
+    # with exact weights the adjoint gathers in the reference's order with the reference's float
+    # operations: bit-identical to the CPU loop
+    assert proj.knob(elsa_b200.KNOB_EXACT_WEIGHTS) == 0  # default: the forward's weights
+    proj.set_knob(elsa_b200.KNOB_EXACT_WEIGHTS, 1)
+    _, Aty_exact = _pair(cuda, proj, x, y)
+    mism = int(np.count_nonzero(Aty_exact.view(np.uint32) != ref_Aty.view(np.uint32)))
+    print("%s %s mode %d: fwd %.3g adj %.3g (fwd vs f64 %.3g), exact-weight adjoint bit "
+          "mismatches %d" % (cfg, name, mode, e_fwd, e_adj, rel_l2(Ax, d_Ax), mism))
     assert e_fwd <= PARITY
     assert e_adj <= PARITY
-    # the adjoint gathers in the reference's order with the reference's float operations
     assert mism == 0
 
 
