@@ -34,6 +34,22 @@ namespace elsa_b200
     // accumulated in float, pa_{j+1} = pa_j + sa (one rounding per step), exactly like elsa's
     // CPU traversal (projectors/DrivingDirectionTraversal.cpp:265). Kernels that start a ray in
     // the middle read the accumulated position from the slab checkpoints.
+    // floor(x) as a float and as an int for |x| < 2^22, on the FMA and integer pipes instead of
+    // the conversion pipe (the "magic number" rounding method): x + 1.5 * 2^23 rounded toward
+    // -infinity lies in [2^23, 2^24), where the floats are exactly the integers, so it equals
+    // 1.5 * 2^23 + floor(x); subtracting the constant back is exact, and the integer is the
+    // difference of the two bit patterns (0x4B400000 is the pattern of 1.5 * 2^23). x = -0 does
+    // not occur where this is used (x = p - 0.5 rounds to +0 at p = 0.5).
+#ifdef __CUDACC__
+    __device__ __forceinline__ float floorSmall(float x, int& i)
+    {
+        constexpr float kMagic = 12582912.0f; // 1.5 * 2^23
+        const float t = __fadd_rd(x, kMagic);
+        i = __float_as_int(t) - 0x4B400000;
+        return __fsub_rn(t, kMagic);
+    }
+#endif
+
     struct __align__(16) JosephRay {
         float pa, pb, sa, sb;
         float len; // |step| = intersection length per sample

@@ -1071,13 +1071,15 @@ namespace elsa_b200
                                                      float& wa, float& cwa, float& wb, float& cwb,
                                                      unsigned& mask)
         {
+            // (floorSmall here, instead of floorf and a conversion: 256^3 33.3 ms against 32.9)
             const float fa = floorf(__fsub_rn(pa, 0.5f));
             const float fb = floorf(__fsub_rn(pb, 0.5f));
+            const int ia = static_cast<int>(fa), ib = static_cast<int>(fb);
             cwa = __fsub_rn(__fsub_rn(pa, fa), 0.5f);
             cwb = __fsub_rn(__fsub_rn(pb, fb), 0.5f);
             wa = __fsub_rn(1.0f, cwa);
             wb = __fsub_rn(1.0f, cwb);
-            const int la = static_cast<int>(fa) - orgA, lb = static_cast<int>(fb) - orgB;
+            const int la = ia - orgA, lb = ib - orgB;
             const bool a0 = static_cast<unsigned>(la) < static_cast<unsigned>(EA);
             const bool a1 = static_cast<unsigned>(la + 1) < static_cast<unsigned>(EA);
             const bool b0 = static_cast<unsigned>(lb) < static_cast<unsigned>(EB);
