@@ -691,6 +691,13 @@ def run_secondary(args):
         kind, vol, views, det, params, s2c, c2d = SECONDARY[name]
         poses, dd = elsa_b200.circle_trajectory(vol, views, 360, s2c, c2d, det)
         p = elsa_b200.Projector(getattr(elsa_b200, "PROJECTOR_" + kind), vol, dd, poses, params)
+        knobs = {}
+        for kv in args.knob or []:  # e.g. exact_weights=1, adjoint_scatter=1
+            k, v = kv.split("=")
+            knob = elsa_b200._capi.KNOB_NAMES.index(k)
+            if p.knob_candidates(knob):
+                p.set_knob(knob, int(v))
+                knobs[k] = int(v)
         x = torch.rand(p.domain_size, device="cuda")
         y = torch.rand(p.range_size, device="cuda")
         oy, ox = torch.empty_like(y), torch.empty_like(x)
@@ -713,7 +720,7 @@ def run_secondary(args):
         out["secondary"][name] = {
             "volume": [int(v) for v in vol], "views": int(views),
             "detector": [int(v) for v in dd[:-1]],
-            "forward_ms": round(fwd, 3), "adjoint_ms": round(adj, 3),
+            "forward_ms": round(fwd, 3), "adjoint_ms": round(adj, 3), "knobs": knobs,
             "gups": round(2 * nvox * views / ((fwd + adj) / 1e3) / 1e9, 3)}
         p.close()
     print(json.dumps(out))
@@ -778,6 +785,11 @@ def main():
     ap.add_argument("--secondary", default=None,
                     help="time other projector workloads instead ('all' or a comma list of: %s)"
                          % ", ".join(SECONDARY))
+    ap.add_argument("--knob", action="append",
+                    help="with --secondary: set a projector knob, name=value (names: %s); "
+                         "repeatable, ignored where the projector lacks the knob"
+                         % ", ".join(("forward_threads", "adjoint_chunks", "adjoint_threads",
+                                      "adjoint_scatter", "exact_weights")))
     ap.add_argument("--size", type=int, default=256,
                     help="volume edge (profiling only; the benchmark workload is 256)")
     args = ap.parse_args()
