@@ -582,6 +582,9 @@ namespace elsa_b200
                                  // (256^3 / 360 views: 1: 44.6 ms, 2: 50.6, 3: 50.3; the
                                  // records of the next ray prefetched instead: 44.4 ms)
 #endif
+#ifndef ELSA_SIDDON_NOZERO
+#define ELSA_SIDDON_NOZERO 0
+#endif
 #ifndef ELSA_SIDDON_PLANE_ODD
 #define ELSA_SIDDON_PLANE_ODD 0 // 1: plane stride padded to 1 modulo 32
 #endif
@@ -663,7 +666,13 @@ namespace elsa_b200
                 const bool in = static_cast<unsigned>(la) < static_cast<unsigned>(EA) &&
                                 static_cast<unsigned>(lb) < static_cast<unsigned>(EB);
                 const int off = lg * L::kPlane + la * SA + lb * SB;
+#if ELSA_SIDDON_NOZERO
+                float val; // read only where used: its store carries the same flag
+                if (in)
+                    val = acc[off];
+#else
                 const float val = in ? acc[off] : 0.0f;
+#endif
                 if (prevIn)
                     acc[prevOff] = __fadd_rn(prevVal, __fmul_rn(yv, prevW));
                 prevOff = off, prevVal = val, prevIn = in;

@@ -539,7 +539,7 @@ namespace elsa_b200
         private:
             int adjointThreads_ = kVoxelThreads; // voxels per block of the gather adjoint
             // 0: the adjoint uses the forward's weights (128^3 blob: 21.7 ms); 1: the reference's
-            // float operations, bit-identical to elsa's CPU loop (26.0 ms)
+            // float operations, bit-identical to elsa's CPU loop (24.1 ms)
             int exactWeights_ = 0;
             // forward bricks: 8 x 8 x 4 voxels in 3D, 16 x 16 in 2D (one thread per voxel)
             static constexpr int kBX = DIM == 3 ? 8 : 16;

@@ -207,7 +207,7 @@ elsa_status elsa_projector_wait_test(elsa_projector* projector, int64_t waitCycl
  * 0 = the forward's weights (distance as n2 * rsqrt(n2), scaling applied as a multiplication by
  * 1 / s, the table lerp as one fma; within a few ulp of the reference's, and forward and adjoint
  * then use the same weights), 1 = the reference's float operations (VoxelComputation.h:55-185),
- * the adjoint bit-identical to elsa's CPU loop. Default 0 (1.2x faster). Either way the adjoint
+ * the adjoint bit-identical to elsa's CPU loop. Default 0 (1.4x faster). Either way the adjoint
  * is deterministic. */
 #define ELSA_KNOB_EXACT_WEIGHTS 4
 #define ELSA_KNOB_COUNT 5
