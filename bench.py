@@ -663,6 +663,7 @@ def batched_vs_plain(torch, elsa_b200, phantoms, instances=12, iterations=10, st
 SECONDARY = {
     # name: (projector kind, volume, views, detector, params, source-centre, centre-detector)
     "siddon256": ("SIDDON", (256, 256, 256), 360, [384, 384], None, 2560, 640),
+    "siddon128": ("SIDDON", (128, 128, 128), 360, [192, 192], None, 1280, 320),
     "blob128": ("BLOB", (128, 128, 128), 180, [192, 192], [2.0, 10.83, 2.0], 1280, 320),
     "bspline128": ("BSPLINE", (128, 128, 128), 180, [192, 192], [2.0], 1280, 320),
     "phase_blob128": ("PHASE_CONTRAST_BLOB", (128, 128, 128), 180, [192, 192],

@@ -1016,9 +1016,6 @@ namespace elsa_b200
         // the non-driving axis over which the rays of a detector row spread (the warp's lanes
         // spread along it, so stride 1 there keeps their taps in different banks), rows along the
         // other one; both carry the halo.
-#ifndef ELSA_AXIS_NOZERO
-#define ELSA_AXIS_NOZERO 0
-#endif
 #ifndef ELSA_AXIS_PLANE_ODD
 #define ELSA_AXIS_PLANE_ODD 0 // 1: pad the plane stride to 1 modulo 32 (256^3: 35.8 ms, 0: 33.5 ms)
 #endif
@@ -1123,24 +1120,10 @@ namespace elsa_b200
                     unsigned mk2;
                     const int o2 = plane + axisTapMasked<AR::EA, AR::EB, SA, SB>(
                                                pa, pb, orgA, orgB, wa2, cwa2, wb2, cwb2, mk2);
-#if ELSA_AXIS_NOZERO
-                    // a masked tap's word is neither read nor used: its store below carries the
-                    // same mask bit
-                    float n0, n1, n2, n3;
-                    if (mk2 & 1u)
-                        n0 = acc[o2];
-                    if (mk2 & 2u)
-                        n1 = acc[o2 + SA];
-                    if (mk2 & 4u)
-                        n2 = acc[o2 + SB];
-                    if (mk2 & 8u)
-                        n3 = acc[o2 + SA + SB];
-#else
                     const float n0 = (mk2 & 1u) ? acc[o2] : 0.0f;
                     const float n1 = (mk2 & 2u) ? acc[o2 + SA] : 0.0f;
                     const float n2 = (mk2 & 4u) ? acc[o2 + SB] : 0.0f;
                     const float n3 = (mk2 & 8u) ? acc[o2 + SA + SB] : 0.0f;
-#endif
                     if (mk & 1u)
                         acc[o] = v0 + ya * wb;
                     if (mk & 2u)

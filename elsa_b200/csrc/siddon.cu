@@ -583,7 +583,7 @@ namespace elsa_b200
                                  // records of the next ray prefetched instead: 44.4 ms)
 #endif
 #ifndef ELSA_SIDDON_NOZERO
-#define ELSA_SIDDON_NOZERO 0
+#define ELSA_SIDDON_NOZERO 1 // 256^3 owner: 39.5 ms, against 41.3 ms reading 0 into skipped words
 #endif
 #ifndef ELSA_SIDDON_PLANE_ODD
 #define ELSA_SIDDON_PLANE_ODD 0 // 1: plane stride padded to 1 modulo 32

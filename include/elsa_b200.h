@@ -201,7 +201,7 @@ elsa_status elsa_projector_wait_test(elsa_projector* projector, int64_t waitCycl
  * the brick owner exists for the geometry (a valid class spacing) and its checkpoint tables
  * (20 bytes per ray and 16-plane slab, about 20 GB at 256^3 / 360 x 384^2) take at most a quarter
  * of the device's memory and half of the free memory at creation, else 1. At 256^3 the Siddon
- * brick owner takes 1.27x the scatter's time. */
+ * brick owner takes 1.22x the scatter's time. */
 #define ELSA_KNOB_ADJOINT_SCATTER 3
 /* Weights of the voxel projectors' adjoint (blob, B-spline and their phase-contrast forms):
  * 0 = the forward's weights (distance as n2 * rsqrt(n2), scaling applied as a multiplication by
