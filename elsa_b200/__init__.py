@@ -14,6 +14,7 @@ from ._capi import (ElsaError, InvalidArgumentError, Projector, Solver, BatchCGN
                     SOLVER_LANDWEBER, SOLVER_APGD, SOLVER_SIRT, SOLVER_FGM,
                     SOLVER_OGM, PROX_IDENTITY, PROX_BOX, PROX_L1, KNOB_FORWARD_THREADS,
                     KNOB_ADJOINT_CHUNKS, KNOB_ADJOINT_THREADS, KNOB_ADJOINT_SCATTER, KNOB_EXACT_WEIGHTS,
+                    KNOB_CHECKPOINT_DEPTH,
                     tune_cache_size,
                     tune_cache_clear, tune_cache_save, tune_cache_load, tune_cache_put,
                     tune_cache_get, SOLVER_SQS, SUBSET_ROUND_ROBIN,
@@ -30,7 +31,7 @@ __all__ = ["ElsaError", "InvalidArgumentError", "Projector", "Solver", "BatchCGN
            "SOLVER_SIRT", "SOLVER_FGM", "SOLVER_OGM",
            "PROX_IDENTITY",
            "PROX_BOX", "PROX_L1", "KNOB_FORWARD_THREADS", "KNOB_ADJOINT_CHUNKS",
-           "KNOB_ADJOINT_THREADS", "KNOB_ADJOINT_SCATTER", "KNOB_EXACT_WEIGHTS", "tune_cache_size", "tune_cache_clear", "tune_cache_save",
+           "KNOB_ADJOINT_THREADS", "KNOB_ADJOINT_SCATTER", "KNOB_EXACT_WEIGHTS", "KNOB_CHECKPOINT_DEPTH", "tune_cache_size", "tune_cache_clear", "tune_cache_save",
            "tune_cache_load", "tune_cache_put", "tune_cache_get", "SOLVER_SQS",
            "SUBSET_ROUND_ROBIN", "SUBSET_ROTATIONAL_CLUSTERING", "subset_split", "gather_views",
            "edf_read", "edf_write", "mhd_read", "mhd_write", "pgm_write", "PROJECTOR_BINARY",

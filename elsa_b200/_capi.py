@@ -50,9 +50,10 @@ KNOB_ADJOINT_CHUNKS = 1
 KNOB_ADJOINT_THREADS = 2
 KNOB_ADJOINT_SCATTER = 3
 KNOB_EXACT_WEIGHTS = 4
-KNOB_COUNT = 5
+KNOB_CHECKPOINT_DEPTH = 5
+KNOB_COUNT = 6
 KNOB_NAMES = ("forward_threads", "adjoint_chunks", "adjoint_threads", "adjoint_scatter",
-              "exact_weights")
+              "exact_weights", "checkpoint_depth")
 
 IO_MAX_DIMS = 8
 IO_TYPES = ("int8", "uint8", "int16", "uint16", "int32", "uint32", "float32", "float64")

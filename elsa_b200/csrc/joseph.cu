@@ -37,6 +37,7 @@
 #include "solvers.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <cmath>
 #include <cstring>
@@ -1182,15 +1183,22 @@ namespace elsa_b200
         // takes class rays i, i + 32, ... (u fastest within the class grid).
         template <int G, int TD, bool UB, int TW, int TV, int CPD>
         __device__ __forceinline__ void axisView(float* acc, const RayWindow& w, int p, int m,
-                                                 const JosephRay* __restrict__ rays,
+                                                 int cpdShift, const JosephRay* __restrict__ rays,
                                                  const float2* __restrict__ cps, int64_t nrays,
                                                  const float* __restrict__ y,
                                                  const DetectorShape& det, int orgG, int orgA,
                                                  int orgB)
         {
+            // Checkpoint slabs of CPD planes, or of 2^cpdShift planes when CPD is 0 (the
+            // deeper slabs that save memory). A brick that does not start at its ray's first
+            // sample in the slab catches up from the checkpoint by exact additions.
             const int kLo = orgG, kHi = orgG + TD - 1;
-            const int slabLo = (orgG / CPD) * CPD, slabHi = slabLo + CPD - 1;
-            const int64_t cpRow = static_cast<int64_t>(orgG / CPD + 1) * nrays;
+            const int shift = CPD > 0 ? 0 : cpdShift;
+            const int slabLo = CPD > 0 ? (orgG / CPD) * CPD : (orgG >> shift) << shift;
+            const int slabHi = slabLo + (CPD > 0 ? CPD : 1 << shift) - 1;
+            const bool catchUp = CPD > 0 ? TD < CPD : (1 << shift) > TD;
+            const int64_t cpRow =
+                static_cast<int64_t>((CPD > 0 ? orgG / CPD : orgG >> shift) + 1) * nrays;
             const int lane = threadIdx.x & 31;
             const int64_t viewBase = static_cast<int64_t>(det.nu) * det.nv * p;
             for (int ov = 0; ov < m; ++ov) {
@@ -1234,7 +1242,7 @@ namespace elsa_b200
                             // the slab; a brick thinner than the slab advances it to its own
                             // planes
                             float2 cp = cpb[q];
-                            if (TD < CPD) {
+                            if (catchUp) {
                                 int jS0, jS1;
                                 sampleRange(R, slabLo, slabHi, jS0, jS1);
                                 for (int j = jS0; j < jLo; ++j) {
@@ -1263,7 +1271,7 @@ namespace elsa_b200
         // Shape of the axis bricks (depth along the driving axis, columns, rows) and the
         // checkpoint slab depth of the 3D operator.
         constexpr int kAxisTD = ELSA_AXIS_TD, kAxisTW = ELSA_AXIS_TW, kAxisTV = ELSA_AXIS_TV;
-        constexpr int kAxisCheckpointDepth = 16;
+        constexpr int kAxisCheckpointDepth = 16; // the smallest checkpoint slab of the 3D adjoint
         static_assert(kAxisCheckpointDepth % kAxisTD == 0,
                       "axis bricks are a whole fraction of a checkpoint slab deep");
 
@@ -1282,6 +1290,7 @@ namespace elsa_b200
             VolumeShape vol;
             DetectorShape det;
             int m;
+            int cpdShift; // checkpoint slabs of 2^cpdShift planes
             int3 nBricks;
             float* out;       // partial volume k at out + k * nvox (x itself for one partial)
             int64_t itemBase; // batched launches: first block of this job
@@ -1317,7 +1326,8 @@ namespace elsa_b200
                 const RayWindow w = J.windows[static_cast<int64_t>(p) * nb + bi];
                 if (w.u0 > w.u1 || w.v0 > w.v1)
                     continue;
-                axisView<G, TD, UB, TW, TV, CPD>(acc, w, p, J.m, J.rays, J.checkpoints, J.nrays,
+                axisView<G, TD, UB, TW, TV, CPD>(acc, w, p, J.m, J.cpdShift, J.rays,
+                                                 J.checkpoints, J.nrays,
                                                  J.y, J.det, orgG, orgA, orgB);
             }
             __syncwarp();
@@ -1435,18 +1445,13 @@ namespace elsa_b200
 
                 int cpd;
                 if (vol_.dim == 3) {
-                    cpd = kAxisCheckpointDepth;
+                    cpd = defaultCheckpointDepth();
                 } else {
                     brick_ = Adjoint2d::brick();
                     cpd = Adjoint2d::kCheckpointDepth;
                     Adjoint2d::prepare(det_.np);
                 }
-                const int maxDim = std::max(vol_.n[0], std::max(vol_.n[1], vol_.n[2]));
-                cpStride_ = maxDim / cpd + 3;
-                ELSA_CUDA(cudaMalloc(&dCheckpoints_, sizeof(float2) * nrays * cpStride_));
-                josephCheckpointKernel<<<blocks, threads>>>(dRays_, nrays, cpd, cpStride_,
-                                                            dCheckpoints_);
-                ELSA_LAUNCH_CHECK("josephCheckpointKernel");
+                buildCheckpoints(cpd);
 
                 if (vol_.dim == 3) {
                     buildAxisGrids();
@@ -1791,11 +1796,27 @@ namespace elsa_b200
                     return {64, 128, 256, 512};
                 if (knob == kKnobAdjointScatter)
                     return {0, 1};
+                if (knob == kKnobCheckpointDepth && vol_.dim == 3) {
+                    // depths whose table takes at most an eighth of the device's memory, and
+                    // the current one
+                    size_t freeBytes = 0, totalBytes = 0;
+                    ELSA_CUDA(cudaMemGetInfo(&freeBytes, &totalBytes));
+                    const int maxDim = std::max(vol_.n[0], std::max(vol_.n[1], vol_.n[2]));
+                    std::vector<int> c;
+                    for (int cpd = kAxisCheckpointDepth; cpd <= 128; cpd *= 2)
+                        if (cpd == (1 << cpdShift_) ||
+                            8.0 * static_cast<double>(rangeSize_) * (maxDim / cpd + 3) <=
+                                static_cast<double>(totalBytes) / 8.0)
+                            c.push_back(cpd);
+                    return c;
+                }
                 return {};
             }
 
             int knob(int knob) const override
             {
+                if (knob == kKnobCheckpointDepth)
+                    return vol_.dim == 3 && !fast_ ? 1 << cpdShift_ : -1;
                 if (knob == kKnobAdjointChunks)
                     return adjointChunks_;
                 if (knob == kKnobForwardThreads)
@@ -1815,12 +1836,20 @@ namespace elsa_b200
                                 "JosephsMethod: value " + std::to_string(value) +
                                     " is not a candidate of knob " + std::to_string(knob));
                 }
+                if (batchRefs_.load() > 0 && knob != kKnobForwardThreads)
+                    throw Error(ELSA_ERROR_INVALID_ARGUMENT,
+                                "JosephsMethod: a batched solver holds this operator's adjoint "
+                                "tables; destroy it before changing an adjoint knob");
                 if (knob == kKnobForwardThreads) {
                     forwardThreads_ = value;
                     return;
                 }
                 if (knob == kKnobAdjointScatter) {
                     scatter_ = value;
+                    return;
+                }
+                if (knob == kKnobCheckpointDepth) {
+                    buildCheckpoints(value);
                     return;
                 }
                 adjointChunks_ = value;
@@ -1833,6 +1862,45 @@ namespace elsa_b200
                     partial_.reset();
                     partial_ = std::make_unique<DeviceBuffer>(need);
                 }
+            }
+
+            // Checkpoint slab depth of the 3D adjoint by default: the smallest of 16, 32, 64, 128
+            // planes whose table (8 bytes per ray and slab) takes at most an eighth of the
+            // device's memory (256^3 / 360 x 384^2: 16 planes, 8.1 GB; 512^3 / 720 x 768^2: 128
+            // planes, 15 GB instead of 119 GB). Deeper slabs cost catch-up additions from the
+            // slab's checkpoint to a brick's first plane; the results are the same.
+            int defaultCheckpointDepth() const
+            {
+                size_t freeBytes = 0, totalBytes = 0;
+                ELSA_CUDA(cudaMemGetInfo(&freeBytes, &totalBytes));
+                const int maxDim = std::max(vol_.n[0], std::max(vol_.n[1], vol_.n[2]));
+                int cpd = kAxisCheckpointDepth;
+                while (cpd < 128 && 8.0 * static_cast<double>(rangeSize_) * (maxDim / cpd + 3) >
+                                        static_cast<double>(totalBytes) / 8.0)
+                    cpd *= 2;
+                return cpd;
+            }
+
+            // (Re)builds the slab checkpoints for slabs of cpd planes.
+            void buildCheckpoints(int cpd)
+            {
+                if (dCheckpoints_ != nullptr) {
+                    ELSA_CUDA(cudaDeviceSynchronize()); // no adjoint may still read the table
+                    ELSA_CUDA(cudaFree(dCheckpoints_));
+                    dCheckpoints_ = nullptr;
+                }
+                int shift = 0;
+                while ((1 << shift) < cpd)
+                    ++shift;
+                cpdShift_ = shift;
+                const int maxDim = std::max(vol_.n[0], std::max(vol_.n[1], vol_.n[2]));
+                const int64_t nrays = rangeSize_;
+                cpStride_ = maxDim / cpd + 3;
+                ELSA_CUDA(cudaMalloc(&dCheckpoints_, sizeof(float2) * nrays * cpStride_));
+                const unsigned blocks = static_cast<unsigned>((nrays + 255) / 256);
+                josephCheckpointKernel<<<blocks, 256>>>(dRays_, nrays, cpd, cpStride_,
+                                                        dCheckpoints_);
+                ELSA_LAUNCH_CHECK("josephCheckpointKernel");
             }
 
             bool setWaitTest(long long cycles, bool withhold) override
@@ -1921,6 +1989,13 @@ namespace elsa_b200
             RayWindow* dWindows_ = nullptr;
             float2* dCheckpoints_ = nullptr;
             int cpStride_ = 0;
+            int cpdShift_ = 4; // checkpoint slabs of 2^cpdShift_ planes (3D)
+
+        public:
+            // batched adjoint plans holding pointers into this operator's tables
+            mutable std::atomic<int> batchRefs_{0};
+
+        private:
             int classSpacing_ = 0;
             int64_t sampleCount_ = 0;
             std::unique_ptr<JosephForwardTma> tma_;
@@ -2096,6 +2171,7 @@ namespace elsa_b200
                 J.vol = vol_;
                 J.det = det_;
                 J.m = classSpacing_;
+                J.cpdShift = cpdShift_;
                 J.nBricks = G.nb;
                 J.out = out;
                 J.itemBase = 0;
@@ -2124,9 +2200,18 @@ namespace elsa_b200
                     const dim3 grid(static_cast<unsigned>(G.nb.x * G.nb.y * G.nb.z),
                                     static_cast<unsigned>(e1 - e0), static_cast<unsigned>(batch));
                     const AxisJob J = axisJob(g, y, out);
+                    // slabs of kAxisCheckpointDepth planes: the depth fixed at compile time;
+                    // deeper ones (CPD 0): read from the job
+                    const bool deep = (1 << cpdShift_) != kAxisCheckpointDepth;
 #define ELSA_AXIS_LAUNCH(G_, UB_)                                                                \
-    josephAdjointAxisKernel<G_, kAxisTD, UB_, kAxisTW, kAxisTV, kAxisCheckpointDepth>             \
-        <<<grid, 32, 0, s>>>(J, e0 - G.entryBegin, yStride, outStride)
+    do {                                                                                         \
+        if (deep)                                                                                \
+            josephAdjointAxisKernel<G_, kAxisTD, UB_, kAxisTW, kAxisTV, 0>                       \
+                <<<grid, 32, 0, s>>>(J, e0 - G.entryBegin, yStride, outStride);                  \
+        else                                                                                     \
+            josephAdjointAxisKernel<G_, kAxisTD, UB_, kAxisTW, kAxisTV, kAxisCheckpointDepth>     \
+                <<<grid, 32, 0, s>>>(J, e0 - G.entryBegin, yStride, outStride);                  \
+    } while (0)
                     if (g == 0) {
                         if (G.ub)
                             ELSA_AXIS_LAUNCH(0, true);
@@ -2183,6 +2268,14 @@ namespace elsa_b200
         std::unique_ptr<DeviceBuffer> sums;
         int sumCount = 0;
         int64_t maxVox = 0;
+        bool deep = false; // some instance uses checkpoint slabs deeper than kAxisCheckpointDepth
+        // operators whose tables the jobs point into: their adjoint knobs stay fixed meanwhile
+        std::vector<const JosephProjector*> holds;
+        ~AdjointManyPlan()
+        {
+            for (const JosephProjector* J : holds)
+                --J->batchRefs_;
+        }
     };
 
     std::shared_ptr<AdjointManyPlan> planJosephAdjointMany(const std::vector<Projector*>& ops,
@@ -2201,7 +2294,10 @@ namespace elsa_b200
                             "batched adjoints take 3D Joseph operators with the matched "
                             "brick-owner adjoint only");
             J->appendAxisJobs(ys[i], xs[i], jobs, sums);
+            ++J->batchRefs_;
+            plan->holds.push_back(J);
             plan->maxVox = std::max(plan->maxVox, J->domainSize());
+            plan->deep = plan->deep || J->knob(kKnobCheckpointDepth) != kAxisCheckpointDepth;
         }
         for (int k = 0; k < 6; ++k) {
             int64_t base = 0;
@@ -2238,7 +2334,12 @@ namespace elsa_b200
             const AxisJob* jobs = plan.jobs[k]->as<AxisJob>();
             const int n = plan.counts[k];
 #define ELSA_AXIS_MANY(G_, UB_)                                                                   \
-    josephAdjointAxisManyKernel<G_, TD, UB_, TW, TV, CPD><<<grid, 32, 0, s>>>(jobs, n)
+    do {                                                                                         \
+        if (plan.deep)                                                                           \
+            josephAdjointAxisManyKernel<G_, TD, UB_, TW, TV, 0><<<grid, 32, 0, s>>>(jobs, n);    \
+        else                                                                                     \
+            josephAdjointAxisManyKernel<G_, TD, UB_, TW, TV, CPD><<<grid, 32, 0, s>>>(jobs, n);  \
+    } while (0)
             switch (k) {
             case 0: ELSA_AXIS_MANY(0, false); break;
             case 1: ELSA_AXIS_MANY(0, true); break;

@@ -28,7 +28,8 @@ namespace elsa_b200
         kKnobAdjointThreads = 2, // voxels per block of a thread-per-voxel adjoint kernel
         kKnobAdjointScatter = 3, // 0: deterministic brick-owner adjoint, 1: atomic scatter
         kKnobExactWeights = 4,   // voxel adjoint: 0 the forward's weights, 1 the reference's
-        kKnobCount = 5
+        kKnobCheckpointDepth = 5, // planes per checkpoint slab of the 3D Joseph adjoint
+        kKnobCount = 6
     };
 
     // A curved (cylindrical) detector: opening angle (radian) and source-to-detector distance

@@ -210,7 +210,14 @@ elsa_status elsa_projector_wait_test(elsa_projector* projector, int64_t waitCycl
  * the adjoint bit-identical to elsa's CPU loop. Default 0 (1.4x faster). Either way the adjoint
  * is deterministic. */
 #define ELSA_KNOB_EXACT_WEIGHTS 4
-#define ELSA_KNOB_COUNT 5
+/* Planes per checkpoint slab of the 3D Joseph matched adjoint: 16, 32, 64 or 128. The adjoint
+ * replays every ray from its exact accumulated position at the slab's first sample (8 bytes per
+ * ray and slab); deeper slabs need less memory and add catch-up additions to bricks inside a
+ * slab, with the same results bit for bit. Default: the smallest depth whose table takes at most
+ * an eighth of the device's memory (16 at 256^3 / 360 x 384^2, 8.1 GB). Setting it rebuilds the
+ * table (synchronizes the device). */
+#define ELSA_KNOB_CHECKPOINT_DEPTH 5
+#define ELSA_KNOB_COUNT 6
 
 /* Current value of `knob` (-1: the projector does not use it). */
 elsa_status elsa_projector_get_knob(const elsa_projector* projector, int32_t knob,

@@ -131,3 +131,37 @@ def test_batched_cgne_refuses_other_operators(cuda, oracle):
     with pytest.raises(elsa_b200.ElsaError):
         elsa_b200.BatchCGNE([p for p, _ in insts], [b.data_ptr() for _, b in insts],
                             [x.data_ptr() for x in xs])
+
+
+def test_batched_cgne_deep_checkpoints_and_knob_guard(cuda, oracle):
+    """Instances with deeper checkpoint slabs (less memory) batch like the others: the same
+    iterates as their plain sessions. While a batch holds an operator its adjoint knobs are
+    fixed (the batch points into its tables); closing the batch releases them."""
+    import elsa_b200
+    torch = cuda
+    J = elsa_b200.PROJECTOR_JOSEPH
+    insts = _instances(oracle, torch, [(J, 24), (J, 40), (J, 32)])
+    insts[1][0].set_knob(elsa_b200.KNOB_CHECKPOINT_DEPTH, 64)
+    insts[2][0].set_knob(elsa_b200.KNOB_CHECKPOINT_DEPTH, 32)
+    xs_plain, plain = _solvers(torch, insts, 0)
+    s = torch.cuda.current_stream().cuda_stream
+    for sol in plain:
+        sol.iterate(4, s)
+    torch.cuda.synchronize()
+    xs = [torch.zeros(p.domain_size, device="cuda") for p, _ in insts]
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        batch = elsa_b200.BatchCGNE([p for p, _ in insts], [b.data_ptr() for _, b in insts],
+                                    [x.data_ptr() for x in xs], st.cuda_stream)
+        batch.iterate(4, st.cuda_stream)
+    st.synchronize()
+    for a, b in zip(xs_plain, xs):
+        assert bool((a == b).all())
+    for p, _ in insts:
+        with pytest.raises(elsa_b200.InvalidArgumentError):
+            p.set_knob(elsa_b200.KNOB_CHECKPOINT_DEPTH, 128)
+    batch.close()
+    for sol in plain:
+        sol.close()
+    insts[0][0].set_knob(elsa_b200.KNOB_CHECKPOINT_DEPTH, 128)  # released
+    assert insts[0][0].knob(elsa_b200.KNOB_CHECKPOINT_DEPTH) == 128

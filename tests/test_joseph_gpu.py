@@ -212,3 +212,38 @@ def test_bounded_wait_runs_out(cuda, oracle):
     siddon = elsa_b200.Projector(elsa_b200.PROJECTOR_SIDDON, vol, det, poses)
     with pytest.raises(elsa_b200.ElsaError):
         siddon.wait_test(20000, True)
+
+
+@pytest.mark.parametrize("vol,det,views", [((48, 48, 48), [72, 72], 36),
+                                           ((40, 56, 72), [88, 64], 25)])
+def test_checkpoint_depth_same_adjoint(cuda, oracle, vol, det, views):
+    """Deeper checkpoint slabs (knob CHECKPOINT_DEPTH: less memory) give the same 3D matched
+    adjoint bit for bit, in single and batched launches: a brick inside a slab catches up from the
+    slab's checkpoint with the same float additions the ray would have made."""
+    import elsa_b200
+    torch = cuda
+    n = max(vol)
+    poses, dd = oracle.circle_trajectory(vol, views, 360, 10.0 * n, 2.5 * n, det)
+    proj = _projector(vol, dd, poses)
+    assert proj.knob(elsa_b200.KNOB_CHECKPOINT_DEPTH) == 16  # small problem: the default
+    assert proj.knob_candidates(elsa_b200.KNOB_CHECKPOINT_DEPTH) == [16, 32, 64, 128]
+    rng = np.random.default_rng(17)
+    x = rng.uniform(0, 1, int(np.prod(vol))).astype(np.float32)
+    y = rng.uniform(0, 1, proj.range_size).astype(np.float32)
+    _, a16 = _gpu_pair(torch, proj, x, y)
+    assert rel_l2(a16, oracle.joseph_adjoint(y, vol, dd, poses)) <= PARITY
+    s = torch.cuda.current_stream().cuda_stream
+    yb = torch.from_numpy(np.stack([y, y[::-1].copy()])).cuda()
+    for cpd in (32, 64, 128):
+        proj.set_knob(elsa_b200.KNOB_CHECKPOINT_DEPTH, cpd)
+        assert proj.knob(elsa_b200.KNOB_CHECKPOINT_DEPTH) == cpd
+        assert proj.info(8) == 0
+        _, a = _gpu_pair(torch, proj, x, y)
+        assert np.array_equal(a.view(np.uint32), a16.view(np.uint32)), cpd
+        out = torch.full((2, proj.domain_size), np.nan, device="cuda")
+        proj.apply_adjoint_batch_ptr(yb.data_ptr(), proj.range_size, out.data_ptr(),
+                                     proj.domain_size, 2, s)
+        torch.cuda.synchronize()
+        assert np.array_equal(out[0].cpu().numpy().view(np.uint32), a16.view(np.uint32)), cpd
+    with pytest.raises(elsa_b200.InvalidArgumentError):
+        proj.set_knob(elsa_b200.KNOB_CHECKPOINT_DEPTH, 24)

@@ -61,7 +61,7 @@ def test_every_knob_value_is_the_same_operator(cuda, oracle, name):
     tunable = 0
     for knob in (elsa_b200.KNOB_FORWARD_THREADS, elsa_b200.KNOB_ADJOINT_CHUNKS,
                  elsa_b200.KNOB_ADJOINT_THREADS, elsa_b200.KNOB_ADJOINT_SCATTER,
-                 elsa_b200.KNOB_EXACT_WEIGHTS):
+                 elsa_b200.KNOB_EXACT_WEIGHTS, elsa_b200.KNOB_CHECKPOINT_DEPTH):
         cands = proj.knob_candidates(knob)
         if not cands:
             continue
@@ -76,7 +76,7 @@ def test_every_knob_value_is_the_same_operator(cuda, oracle, name):
             if knob == elsa_b200.KNOB_FORWARD_THREADS:
                 # the block size changes nothing in a thread-per-ray forward
                 assert np.array_equal(f, f0), (name, v)
-            if knob == elsa_b200.KNOB_ADJOINT_THREADS:
+            if knob in (elsa_b200.KNOB_ADJOINT_THREADS, elsa_b200.KNOB_CHECKPOINT_DEPTH):
                 assert np.array_equal(a, a0), (name, v)
             if knob in (elsa_b200.KNOB_ADJOINT_CHUNKS, elsa_b200.KNOB_ADJOINT_SCATTER):
                 # only the order of the additions changes
