@@ -790,7 +790,7 @@ def main():
                     help="with --secondary: set a projector knob, name=value (names: %s); "
                          "repeatable, ignored where the projector lacks the knob"
                          % ", ".join(("forward_threads", "adjoint_chunks", "adjoint_threads",
-                                      "adjoint_scatter", "exact_weights")))
+                                      "adjoint_scatter", "exact_weights", "checkpoint_depth")))
     ap.add_argument("--size", type=int, default=256,
                     help="volume edge (profiling only; the benchmark workload is 256)")
     args = ap.parse_args()
