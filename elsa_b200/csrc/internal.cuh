@@ -41,6 +41,61 @@ namespace elsa_b200
     // difference of the two bit patterns (0x4B400000 is the pattern of 1.5 * 2^23). x = -0 does
     // not occur where this is used (x = p - 0.5 rounds to +0 at p = 0.5).
 #ifdef __CUDACC__
+    // Packed two-wide FP32 arithmetic of sm_100 (add/sub/mul/fma .f32x2): two IEEE operations
+    // with the stated rounding in one instruction, on a register pair.
+    __device__ __forceinline__ unsigned long long pack2(float2 a)
+    {
+        unsigned long long r;
+        asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+        return r;
+    }
+    __device__ __forceinline__ float2 unpack2(unsigned long long r)
+    {
+        float2 a;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+        return a;
+    }
+    __device__ __forceinline__ float2 add2(float2 a, float2 b)
+    {
+        unsigned long long r;
+        asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)));
+        return unpack2(r);
+    }
+    __device__ __forceinline__ float2 add2Down(float2 a, float2 b) // rounded toward -infinity
+    {
+        unsigned long long r;
+        asm("add.rm.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)));
+        return unpack2(r);
+    }
+    __device__ __forceinline__ float2 sub2(float2 a, float2 b)
+    {
+        unsigned long long r;
+        asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)));
+        return unpack2(r);
+    }
+    __device__ __forceinline__ float2 mul2(float2 a, float2 b)
+    {
+        unsigned long long r;
+        asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)));
+        return unpack2(r);
+    }
+    __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) // a * b + c, one rounding
+    {
+        unsigned long long r;
+        asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)), "l"(pack2(c)));
+        return unpack2(r);
+    }
+
+    // floorSmall of both components.
+    __device__ __forceinline__ float2 floorSmall2(float2 x, int& i0, int& i1)
+    {
+        constexpr float kMagic = 12582912.0f; // 1.5 * 2^23
+        const float2 t = add2Down(x, make_float2(kMagic, kMagic));
+        i0 = __float_as_int(t.x) - 0x4B400000;
+        i1 = __float_as_int(t.y) - 0x4B400000;
+        return sub2(t, make_float2(kMagic, kMagic));
+    }
+
     __device__ __forceinline__ float floorSmall(float x, int& i)
     {
         constexpr float kMagic = 12582912.0f; // 1.5 * 2^23
