@@ -39,6 +39,9 @@ namespace elsa_b200
         constexpr int kVoxelThreads = 256;      // forward: one thread per brick voxel; adjoint default
         constexpr int kMaxAdjointThreads = 512; // largest adjoint block the autotuner may choose
         constexpr int kPatchWords = 2304; // 9 KB shared detector patch (48 x 48 pixels)
+#ifndef ELSA_VOXEL_PAIRS
+#define ELSA_VOXEL_PAIRS 0 // 1: footprint pixels in pairs on the packed two-wide FP32 path
+#endif
 
         struct VoxelParams {
             int dim;
@@ -177,6 +180,41 @@ namespace elsa_b200
             return v * d0;
         }
 
+        // voxelWeight<DIM, true, WK> of two pixels of one footprint row (d0 pair, shared d1) on
+        // the packed two-wide FP32 instructions: the same operations and roundings per pixel.
+        template <int DIM, int WK>
+        __device__ __forceinline__ float2 voxelWeight2(const float* lut, const VoxelParams& vp,
+                                                       float2 d0, float d1)
+        {
+            float2 n2 = mul2(d0, d0);
+            if (DIM == 3)
+                n2 = fma2(make_float2(d1, d1), make_float2(d1, d1), n2);
+            float2 dist = mul2(n2, make_float2(rsqrtf(n2.x), rsqrtf(n2.y)));
+            dist.x = n2.x > 0.0f ? dist.x : 0.0f;
+            dist.y = n2.y > 0.0f ? dist.y : 0.0f;
+            const float2 q = vp.invRadius != 0.0f
+                                 ? mul2(dist, make_float2(vp.invRadius, vp.invRadius))
+                                 : make_float2(dist.x / vp.radius, dist.y / vp.radius);
+            constexpr float kTop = static_cast<float>(kVoxelLutSize - 1);
+            const float2 index = mul2(q, make_float2(kTop, kTop));
+            // index >= 0 and far below 2^22 (a footprint reaches a few supports at most)
+            int a0, a1;
+            const float2 af = floorSmall2(index, a0, a1);
+            const bool in0 = index.x <= kTop, in1 = index.y <= kTop;
+            const float2 fa = make_float2(in0 ? lut[a0] : 0.0f, in1 ? lut[a1] : 0.0f);
+            const float2 fb = make_float2(in0 ? lut[a0 + 1] : 0.0f, in1 ? lut[a1 + 1] : 0.0f);
+            float2 v = fma2(sub2(index, af), sub2(fb, fa), fa);
+            v.x = in0 ? v.x : 0.0f;
+            v.y = in1 ? v.y : 0.0f;
+            const int wk = WK >= 0 ? WK : vp.weightKind;
+            if (wk == 0)
+                return v;
+            if (DIM == 2)
+                return make_float2(v.x * static_cast<float>((0.0f < d0.x) - (d0.x < 0.0f)),
+                                   v.y * static_cast<float>((0.0f < d0.y) - (d0.y < 0.0f)));
+            return mul2(v, d0);
+        }
+
         // Visits the footprint pixels of one voxel in the reference's order; fn(linear pixel
         // index within the pose, u, v, d0, d1) with (u, v) the pixel's unwrapped detector
         // coordinates (u may leave [0, nu) where the reference's linear index wraps into the
@@ -213,6 +251,57 @@ namespace elsa_b200
                     cur0 = cur0 + 1.0f;
                 }
                 lin += vp.nu - ext0;
+                u -= ext0;
+                v += 1;
+                cur0 = cur0 - static_cast<float>(ext0);
+                cur1 = cur1 + 1.0f;
+            }
+        }
+
+        // visitFootprintInside with the pixels of a row taken in pairs: fn2(u, v, (d0, d0'), d1)
+        // for pixels u and u + 1, fn1 for the last pixel of an odd row; the same pixels, order
+        // and offsets.
+        template <int DIM, class Fn2, class Fn1>
+        __device__ __forceinline__ void visitFootprintInsidePairs(const Footprint& f,
+                                                                  const VoxelParams& vp, Fn2 fn2,
+                                                                  Fn1 fn1)
+        {
+            const float invS = 1.0f / f.s;
+            const float2 inv2 = make_float2(invS, invS);
+            const float2 c2 = make_float2(f.c0, f.c0);
+            if (DIM == 2) {
+                int u = f.lo0;
+                for (; u + 1 <= f.hi0; u += 2)
+                    fn2(u, 0, mul2(sub2(c2, make_float2(static_cast<float>(u),
+                                                        static_cast<float>(u + 1))),
+                                   inv2),
+                        0.0f);
+                if (u <= f.hi0)
+                    fn1(u, 0, __fmul_rn(f.c0 - static_cast<float>(u), invS), 0.0f);
+                return;
+            }
+            const int ext0 = f.hi0 - f.lo0 + 1, ext1 = f.hi1 - f.lo1 + 1;
+            if (ext0 <= 0 || ext1 <= 0)
+                return;
+            const bool ref = vp.mode == static_cast<int>(FootprintMode::Reference);
+            const int rows = min(ref ? ext0 : ext1, vp.nv - f.lo1);
+            const int cols = ref ? ext1 : ext0;
+            float cur0 = static_cast<float>(f.lo0), cur1 = static_cast<float>(f.lo1);
+            int u = f.lo0, v = f.lo1;
+            for (int r = 0; r < rows; ++r) {
+                const float d1 = __fmul_rn(f.c1 - cur1, invS);
+                int c = 0;
+                for (; c + 1 < cols; c += 2) {
+                    fn2(u, v, mul2(sub2(c2, make_float2(cur0, cur0 + 1.0f)), inv2), d1);
+                    u += 2;
+                    cur0 = cur0 + 1.0f;
+                    cur0 = cur0 + 1.0f;
+                }
+                if (c < cols) {
+                    fn1(u, v, __fmul_rn(f.c0 - cur0, invS), d1);
+                    u += 1;
+                    cur0 = cur0 + 1.0f;
+                }
                 u -= ext0;
                 v += 1;
                 cur0 = cur0 - static_cast<float>(ext0);
@@ -321,10 +410,25 @@ namespace elsa_b200
                 const float* view = y + p * npix;
                 if (Fast && footprintInside<DIM>(f, vp)) {
                     // the same pixels in the same order, without the linear index
+#if ELSA_VOXEL_PAIRS
+                    visitFootprintInsidePairs<DIM>(
+                        f, vp,
+                        [&](int pu_, int pv_, float2 d0, float d1) {
+                            const float2 w = voxelWeight2<DIM, WK>(lut, vp, d0, d1);
+                            const float* yp = view + pv_ * vp.nu + pu_;
+                            acc = acc + w.x * __ldg(yp);
+                            acc = acc + w.y * __ldg(yp + 1);
+                        },
+                        [&](int pu_, int pv_, float d0, float d1) {
+                            const float w = voxelWeight<DIM, true, WK>(lut, vp, d0, d1);
+                            acc = acc + w * __ldg(view + pv_ * vp.nu + pu_);
+                        });
+#else
                     visitFootprintInside<DIM>(f, vp, [&](int pu_, int pv_, float d0, float d1) {
                         const float w = voxelWeight<DIM, true, WK>(lut, vp, d0, d1);
                         acc = acc + w * __ldg(view + pv_ * vp.nu + pu_);
                     });
+#endif
                     continue;
                 }
                 visitFootprint<DIM, Fast>(f, vp, [&](int64_t pix, int pu_, int pv_, float d0,
@@ -400,10 +504,26 @@ namespace elsa_b200
                 if (usePatch && boxed) {
                     // a boxed footprint stays inside the detector and its rows: no linear
                     // index to test
+#if ELSA_VOXEL_PAIRS
+                    visitFootprintInsidePairs<DIM>(
+                        f, vp,
+                        [&](int pu_, int pv_, float2 d0, float d1) {
+                            const float2 c = mul2(make_float2(xv, xv),
+                                                  voxelWeight2<DIM, WK>(lut, vp, d0, d1));
+                            float* pp = &patch[(pv_ - bv0) * pw + (pu_ - bu0)];
+                            atomicAdd(pp, c.x);
+                            atomicAdd(pp + 1, c.y);
+                        },
+                        [&](int pu_, int pv_, float d0, float d1) {
+                            const float w = voxelWeight<DIM, true, WK>(lut, vp, d0, d1);
+                            atomicAdd(&patch[(pv_ - bv0) * pw + (pu_ - bu0)], xv * w);
+                        });
+#else
                     visitFootprintInside<DIM>(f, vp, [&](int pu_, int pv_, float d0, float d1) {
                         const float w = voxelWeight<DIM, true, WK>(lut, vp, d0, d1);
                         atomicAdd(&patch[(pv_ - bv0) * pw + (pu_ - bu0)], xv * w);
                     });
+#endif
                 } else {
                     visitFootprint<DIM, true>(f, vp, [&](int64_t pix, int pu_, int pv_, float d0,
                                                          float d1) {
