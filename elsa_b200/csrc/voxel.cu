@@ -39,8 +39,14 @@ namespace elsa_b200
         constexpr int kVoxelThreads = 256;      // forward: one thread per brick voxel; adjoint default
         constexpr int kMaxAdjointThreads = 512; // largest adjoint block the autotuner may choose
         constexpr int kPatchWords = 2304; // 9 KB shared detector patch (48 x 48 pixels)
-#ifndef ELSA_VOXEL_PAIRS
-#define ELSA_VOXEL_PAIRS 0 // 1: footprint pixels in pairs on the packed two-wide FP32 path
+// Footprint pixels in pairs on the packed two-wide FP32 path (blob / B-spline 128^3 adjoint:
+// 17.5 -> 16.6 / 16.1 ms; the forward: blob unchanged, B-spline 24.5 -> 25.0 ms, phase-contrast
+// blob 26.7 -> 25.6 ms, so the forward keeps single pixels by default)
+#ifndef ELSA_VOXEL_PAIRS_ADJ
+#define ELSA_VOXEL_PAIRS_ADJ 1
+#endif
+#ifndef ELSA_VOXEL_PAIRS_FWD
+#define ELSA_VOXEL_PAIRS_FWD 0
 #endif
 
         struct VoxelParams {
@@ -410,7 +416,7 @@ namespace elsa_b200
                 const float* view = y + p * npix;
                 if (Fast && footprintInside<DIM>(f, vp)) {
                     // the same pixels in the same order, without the linear index
-#if ELSA_VOXEL_PAIRS
+#if ELSA_VOXEL_PAIRS_ADJ
                     visitFootprintInsidePairs<DIM>(
                         f, vp,
                         [&](int pu_, int pv_, float2 d0, float d1) {
@@ -504,7 +510,7 @@ namespace elsa_b200
                 if (usePatch && boxed) {
                     // a boxed footprint stays inside the detector and its rows: no linear
                     // index to test
-#if ELSA_VOXEL_PAIRS
+#if ELSA_VOXEL_PAIRS_FWD
                     visitFootprintInsidePairs<DIM>(
                         f, vp,
                         [&](int pu_, int pv_, float2 d0, float d1) {
