@@ -7,7 +7,7 @@ from kat_cases import joseph_cases
 
 pytestmark = pytest.mark.gpu
 
-PARITY = 1e-5  # relative L2 vs the FP32 CPU path (north-star criterion)
+PARITY = 1e-5  # relative L2 vs the FP32 CPU path (the parity bound)
 
 
 def _gpu_pair(torch, proj, x_np, y_np):
