@@ -41,12 +41,13 @@ namespace elsa_b200
         constexpr int kPatchWords = 2304; // 9 KB shared detector patch (48 x 48 pixels)
 // Footprint pixels in pairs on the packed two-wide FP32 path (blob / B-spline 128^3 adjoint:
 // 17.5 -> 16.6 / 16.1 ms; the forward: blob unchanged, B-spline 24.5 -> 25.0 ms, phase-contrast
-// blob 26.7 -> 25.6 ms, so the forward keeps single pixels by default)
+// blob / B-spline 26.7 -> 25.6 / 25.8 -> 25.1 ms, so the forward pairs pixels for the
+// phase-contrast (differential) weights only)
 #ifndef ELSA_VOXEL_PAIRS_ADJ
 #define ELSA_VOXEL_PAIRS_ADJ 1
 #endif
 #ifndef ELSA_VOXEL_PAIRS_FWD
-#define ELSA_VOXEL_PAIRS_FWD 0
+#define ELSA_VOXEL_PAIRS_FWD 2 // 0: never, 1: always, 2: differential weights only
 #endif
 
         struct VoxelParams {
@@ -510,26 +511,28 @@ namespace elsa_b200
                 if (usePatch && boxed) {
                     // a boxed footprint stays inside the detector and its rows: no linear
                     // index to test
-#if ELSA_VOXEL_PAIRS_FWD
-                    visitFootprintInsidePairs<DIM>(
-                        f, vp,
-                        [&](int pu_, int pv_, float2 d0, float d1) {
-                            const float2 c = mul2(make_float2(xv, xv),
-                                                  voxelWeight2<DIM, WK>(lut, vp, d0, d1));
-                            float* pp = &patch[(pv_ - bv0) * pw + (pu_ - bu0)];
-                            atomicAdd(pp, c.x);
-                            atomicAdd(pp + 1, c.y);
-                        },
-                        [&](int pu_, int pv_, float d0, float d1) {
+                    constexpr bool kFwdPairs =
+                        ELSA_VOXEL_PAIRS_FWD == 1 || (ELSA_VOXEL_PAIRS_FWD == 2 && WK == 1);
+                    if constexpr (kFwdPairs) {
+                        visitFootprintInsidePairs<DIM>(
+                            f, vp,
+                            [&](int pu_, int pv_, float2 d0, float d1) {
+                                const float2 c = mul2(make_float2(xv, xv),
+                                                      voxelWeight2<DIM, WK>(lut, vp, d0, d1));
+                                float* pp = &patch[(pv_ - bv0) * pw + (pu_ - bu0)];
+                                atomicAdd(pp, c.x);
+                                atomicAdd(pp + 1, c.y);
+                            },
+                            [&](int pu_, int pv_, float d0, float d1) {
+                                const float w = voxelWeight<DIM, true, WK>(lut, vp, d0, d1);
+                                atomicAdd(&patch[(pv_ - bv0) * pw + (pu_ - bu0)], xv * w);
+                            });
+                    } else {
+                        visitFootprintInside<DIM>(f, vp, [&](int pu_, int pv_, float d0, float d1) {
                             const float w = voxelWeight<DIM, true, WK>(lut, vp, d0, d1);
                             atomicAdd(&patch[(pv_ - bv0) * pw + (pu_ - bu0)], xv * w);
                         });
-#else
-                    visitFootprintInside<DIM>(f, vp, [&](int pu_, int pv_, float d0, float d1) {
-                        const float w = voxelWeight<DIM, true, WK>(lut, vp, d0, d1);
-                        atomicAdd(&patch[(pv_ - bv0) * pw + (pu_ - bu0)], xv * w);
-                    });
-#endif
+                    }
                 } else {
                     visitFootprint<DIM, true>(f, vp, [&](int64_t pix, int pu_, int pv_, float d0,
                                                          float d1) {
