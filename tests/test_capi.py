@@ -37,6 +37,36 @@ def test_library_exports_header(capi):
     assert declared == set(capi.SIGNATURES)
 
 
+def _header_constants():
+    """ELSA_* integer constants of include/*.h: #define values and enumerators."""
+    consts = {}
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        for name, value in re.findall(r"#define\s+ELSA_([A-Z0-9_]+)\s+(-?\d+)\b", text):
+            consts[name] = int(value)
+        for name, value in re.findall(r"\bELSA_([A-Z0-9_]+)\s*=\s*(-?\d+)", text):
+            consts[name] = int(value)
+    return consts
+
+
+def test_python_constants_match_header(capi):
+    """Every constant the Python bindings mirror (projector and solver kinds, knobs, footprint
+    modes, status codes, ...) has the header's value, and the knob names cover every knob."""
+    consts = _header_constants()
+    assert consts["KNOB_COUNT"] == capi.KNOB_COUNT == len(capi.KNOB_NAMES)
+    mirrored = 0
+    for name, value in consts.items():
+        short = name[len("ERROR_"):] if name.startswith("ERROR_") else name
+        for candidate in (name, short):
+            if hasattr(capi, candidate) and isinstance(getattr(capi, candidate), int):
+                assert getattr(capi, candidate) == value, name
+                mirrored += 1
+                break
+    assert mirrored >= 25, mirrored
+    for k, knob in enumerate(capi.KNOB_NAMES):
+        assert consts["KNOB_" + knob.upper()] == k
+
+
 def test_geometry_bit_identical_to_oracle(capi, oracle):
     for args in [([128, 128], 180, 360, 1000, 250, [182]),
                  ([256, 256, 256], 360, 360, 2560, 640, [384, 384]),
