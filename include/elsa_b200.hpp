@@ -349,7 +349,8 @@ namespace elsa_b200
             }
 
             // launch knobs (ELSA_KNOB_*, elsa_projector_get_knob / _set_knob): e.g.
-            // setKnob(ELSA_KNOB_ADJOINT_SCATTER, 0) selects Siddon's bit-reproducible adjoint
+            // setKnob(ELSA_KNOB_ADJOINT_SCATTER, 1) selects Siddon's atomic scatter adjoint
+            // instead of the bit-reproducible brick owner
             int32_t getKnob(int32_t knob) const
             {
                 int32_t v = -1;

@@ -72,8 +72,10 @@ int main(int argc, char** argv)
         for (size_t i = 0; i < blocks.size(); ++i)
             save(dir + "/block" + std::to_string(i) + ".f32", blocks[i].toHost());
 
-        // Siddon with its bit-reproducible brick-owner adjoint instead of the atomic scatter
+        // Siddon with the atomic scatter adjoint, then with its bit-reproducible brick owner
+        // (the default)
         SiddonsMethodCUDA<float> S(*vol, *sino);
+        S.setKnob(ELSA_KNOB_ADJOINT_SCATTER, 1);
         const auto scatterAdj = S.applyAdjoint(b).toHost();
         S.setKnob(ELSA_KNOB_ADJOINT_SCATTER, 0);
         if (S.getKnob(ELSA_KNOB_ADJOINT_SCATTER) != 0)
